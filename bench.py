@@ -1,0 +1,314 @@
+"""Benchmark: RBE + LJ/Coulomb atom-steps/s on the 200k-atom LJ electrolyte.
+
+A step is one NVE velocity-Verlet MD step (NVEensemble::Solve): half kick,
+drift with periodic wrap and skin check, neighbor rebuild when needed, the RBL
+real-space force (hashed shell batch, r_core 2.5, cut_off 5, skin 0.3), RBE
+k-space with P = 100 Philox-sampled k-vectors, and the second half kick.
+
+value      mixed form (fixed-point positions, FP32 SFU phases, FP64 reductions
+           and integrator), state resident on the GPU.
+fp64_plain the plain FP64 form of the same step on the same GPU.
+e2e        mixed form through rbx_engine_step_host: host x, v in (pinned), one
+           step, x, v, F out, every step.
+roofline   the fused RBL filter + pair-force kernel against measured HBM
+           bandwidth; its algorithmic bytes per launch are the candidate
+           indices read (4 B each) plus 44 B of per-atom traffic (count,
+           atom record, type, two hash keys, force out).
+cpu_baseline  the FP64 host oracle (same step, OpenMP over all host cores).
+
+--impl reference runs the reference path on the host: RBMD's hot-path kernels
+exist only as CUDA, so the reference arm is the FP64 host restatement of the
+same RBE + RBL step (the oracle), timed on this box's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RBE+LJ atom-steps/s @200k atoms: mixed vs FP64 plain at <=1e-5 rel force err"
+UNIT = "atom-steps/s"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}",
+                                      f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    return ws, rank
+
+
+def _init_pg(ws, backend):
+    import datetime
+
+    import torch.distributed as dist
+
+    if ws > 1 and not dist.is_initialized():
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def cpu_baseline(n, p, steps, warmup):
+    from oracle import oracle as O
+    from rbmd_b200 import systems
+
+    s = systems.lj_electrolyte(n, seed=2024, kspace_p=p)
+    eng = O.Engine(s, seed=99)
+    eng.compute_forces(0)
+    eng.step(warmup)
+    t0 = time.perf_counter()
+    eng.step(steps)
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"N={n} LJ electrolyte, P={p}, {steps} velocity-Verlet steps after "
+                      f"{warmup} warm-up (FP64 host restatement, OpenMP)"}
+
+
+def run_reference(args):
+    ws, rank = _dist()
+    if rank != 0:
+        return 0
+    base = cpu_baseline(args.n, args.p, max(1, args.steps), max(1, args.warmup))
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": args.n / base["value"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"lj_electrolyte N={args.n} rho*=0.8 RBL(r_core 2.5, cut_off 5,"
+                                   f" skin 0.3) + RBE(P={args.p}, alpha=0.16)",
+                       "global_batch": args.n, "parallelism": "host cores"},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    from rbmd_b200 import rbx, systems
+
+    ws, rank = _dist()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = _init_pg(ws, "nccl")
+    n, p = args.n, args.p
+    s = systems.lj_electrolyte(n, seed=2024 + rank, kspace_p=p)
+
+    # ---- accuracy of the mixed form vs plain FP64 on the same state and samples
+    err = {}
+    if rank == 0:
+        from oracle import oracle as O
+
+        m = O.rbe_sample_philox(O.Box.make(s["lo"], s["hi"]), s["params"]["alpha"], p, 5, 0)
+        parts = {}
+        for prec in (rbx.PLAIN_FP64, rbx.MIXED):
+            e = rbx.Engine(s, precision=prec, device=local)
+            e.set_k_samples(*m)
+            e.compute_forces(0)
+            fp, fk = e.force_parts()
+            parts[prec] = (fp + fk, fp, fk, e.stats())
+            e.close()
+        err = {"force": systems.rel_rms(parts[1][0], parts[0][0]),
+               "pair": systems.rel_rms(parts[1][1], parts[0][1]),
+               "kspace": systems.rel_rms(parts[1][2], parts[0][2]),
+               "energy_kspace": abs(parts[1][3].e_kspace - parts[0][3].e_kspace) /
+               abs(parts[0][3].e_kspace)}
+
+    def timed(precision, steps, warmup, profile=False):
+        e = rbx.Engine(s, precision=precision, seed=77 + rank, device=local)
+        e.compute_forces(0)
+        e.step(warmup)
+        if profile:
+            e.set_profiling(True)
+        st = torch.cuda.ExternalStream(e.stream)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        if dist and ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = rbx.launch_count()
+        ev0.record(st)
+        e.step(steps)
+        ev1.record(st)
+        torch.cuda.synchronize()
+        launches = rbx.launch_count() - l0
+        ms = ev0.elapsed_time(ev1)
+        if dist and ws > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        phases = e.phase_ms() if profile else None
+        stats = e.stats()
+        return e, ms, launches, phases, stats
+
+    # ---- plain FP64 form
+    e64, ms64, _, ph64, _ = timed(rbx.PLAIN_FP64, args.steps, args.warmup, profile=True)
+    e64.close()
+    # ---- mixed form (headline), clocks sampled during the timed region
+    with ClockSampler(local) as clk:
+        em, ms, launches, _, stats = timed(rbx.MIXED, args.steps, args.warmup)
+    em.close()
+    # per-phase device times of the mixed step (separate profiled run)
+    em2, _, _, phm, stats2 = timed(rbx.MIXED, args.steps, args.warmup, profile=True)
+    em2.close()
+
+    # ---- end to end through the host-buffer C-ABI call
+    e2 = rbx.Engine(s, precision=rbx.MIXED, seed=5, device=local)
+    e2.compute_forces(0)
+    xin = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
+    vin = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
+    xo = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
+    vo = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
+    fo = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
+    xin[:] = s["pos"].T
+    vin[:] = s["vel"].T
+    for _ in range(args.warmup):
+        e2.step_host(xin, vin, xo, vo, fo)
+        xin[:], vin[:] = xo, vo
+    if dist and ws > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2.step_host(xin, vin, xo, vo, fo)
+        xin[:], vin[:] = xo, vo
+    e2e_s = time.perf_counter() - t0
+    if dist and ws > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2.close()
+
+    if rank != 0:
+        if dist and ws > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    value = ws * n * args.steps / (ms / 1e3)
+    v64 = ws * n * args.steps / (ms64 / 1e3)
+    peaks, peak_src = _peaks()
+    # roofline of the fused RBL kernel (phase 2 of the profiled mixed step)
+    cand_per_atom = stats2.candidates / n
+    alg_bytes = n * (4.0 * cand_per_atom + 44.0)
+    t_pair = phm[2] / 1e3
+    achieved = alg_bytes / t_pair / 1e9
+    roof = {"kernel": "k_rbl_fused_mixed", "bound": "hbm", "achieved": achieved,
+            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+            "peak_source": peak_src, "traffic": None,
+            "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": phm[2]}
+    base = cpu_baseline(n, p, 2, 1) if not args.no_cpu_baseline else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "mixed(u32 fixed-point, f32 SFU, f64 "
+                                                         "reductions/integrator)",
+        "data": "synthetic",
+        "config": {"workload": f"lj_electrolyte N={n} rho*=0.8 10% ions, RBL(r_core 2.5, cut_off "
+                               f"5, skin 0.3, p=100, freq={stats.selection_frequency}) + RBE(P={p},"
+                               " alpha=0.16), NVE dt=0.005",
+                   "global_batch": ws * n, "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (candidate list "
+                         f"{stats.candidates * 4 / 1e6:.0f} MB)"},
+        "fp64_plain": {"value": v64, "ms_per_step": ms64 / args.steps, "phase_ms": ph64},
+        "mixed_over_fp64": value / v64,
+        "mixed_error_vs_fp64": err,
+        "phase_ms_mixed": {"kick_drift": phm[0], "skin_rebuild": phm[1], "real_space": phm[2],
+                           "kspace": phm[3]},
+        "rebuilds_per_step": stats.rebuilds / max(1, stats.steps + 1),
+        "e2e": {"value": ws * n * args.steps / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": 6 * 8 * n, "d2h_bytes_per_step": 9 * 8 * n},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "clocks": clk.summary(),
+        "cpu_baseline": base,
+    }
+    print(json.dumps(line), flush=True)
+    if dist and ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=200000)
+    ap.add_argument("--p", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,311 @@
+/*
+ * rbx.h -- C ABI of the B200-native (sm_100a) RBE + LJ/erfc-Coulomb force
+ * engine, a drop-in for RBMD 2.0's src/force (LJ/CUT/COUL/LONG + RBE k-space)
+ * and src/neighbor_list (linked cells, full Verlet list, RBL core/shell lists).
+ *
+ * Conventions
+ *  - Every function returns an rbx_status (0 = RBX_OK); rbx_last_error() gives
+ *    the message of the last failure on the calling thread.  No C++ exception
+ *    crosses this boundary.
+ *  - Op-level functions take caller-owned DEVICE pointers (FP64 SoA, int32
+ *    ids, the reference's rbmd::Real / rbmd::Id layout) and a cudaStream_t
+ *    passed as void*; they enqueue work and return without synchronising
+ *    unless stated.  Argument order follows the reference functor each one
+ *    replaces (file:line given per entry, relative to the RBMD source tree).
+ *  - Engine-level functions (rbx_engine_*) own their device memory and run
+ *    the whole force evaluation / velocity-Verlet step on one GPU.
+ *  - The library has no CPU fallback: without a usable sm_100 device every
+ *    compute entry fails with RBX_ERR_DEVICE.
+ */
+#ifndef RBX_H
+#define RBX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RBX_VERSION 1
+
+typedef enum {
+  RBX_OK = 0,
+  RBX_ERR_INVALID = 1,   /* bad argument or configuration */
+  RBX_ERR_CUDA = 2,      /* CUDA runtime / launch error */
+  RBX_ERR_CAPACITY = 3,  /* a device list overflowed its capacity */
+  RBX_ERR_NOMEM = 4,     /* device or host allocation failed */
+  RBX_ERR_DEVICE = 5,    /* no usable sm_100 device */
+  RBX_ERR_CONFIG = 6,    /* JSON key missing / unsupported value */
+  RBX_ERR_SAMPLER = 7    /* k-sampler could not draw a non-zero vector */
+} rbx_status;
+
+/* Orthogonal periodic box: Box::_coord_min/_coord_max
+ * (src/data_manager/include/model/box.h:5-49). */
+typedef struct {
+  double lo[3];
+  double hi[3];
+} rbx_box;
+
+const char* rbx_last_error(void);
+int rbx_version(void);
+/* Number of kernel launches this thread issued through the library so far. */
+uint64_t rbx_launch_count(void);
+
+/* ------------------------------------------------------------------------ */
+/* Host-side helpers                                                         */
+/* ------------------------------------------------------------------------ */
+
+/* S = prod_d H_d - 1.  Replaces ComputeRbeGaussianSum
+ * (src/force/src/kspace_calculator.cpp:68-78). */
+int rbx_rbe_gauss_sum(const rbx_box* box, double alpha, double* S);
+
+/* RBL selection frequency ("pice_num").  Replaces
+ * RblFullNeighborListBuilder::GetRblParams
+ * (src/neighbor_list/src/neighbor_list_builder/rbl_full_neighbor_list_builder.cpp:193-228). */
+int rbx_rbl_params(int n_global, const rbx_box* box, double r_core,
+                   double cut_off, int neighbor_sample_num, int* freq);
+
+/* ------------------------------------------------------------------------ */
+/* k-space ops (device pointers)                                             */
+/* ------------------------------------------------------------------------ */
+
+/* Counter-based (Philox4x32-10) draw of P integer k-vectors m != 0 from the
+ * RBE importance density P(m) ~ exp(-(2 pi m/L)^2/(4 alpha)); writes
+ * m_x/m_y/m_z as doubles.  Replaces the host Metropolis-Hastings sampler
+ * RBEPSAMPLE::Fetch_P_Sample (src/common/RBEPSample.h:150-188) called from
+ * KSpaceCalculator::RBEInit (src/force/src/kspace_calculator.cpp:671-715). */
+int rbx_rbe_sample(const rbx_box* box, double alpha, int p, uint64_t seed,
+                   int64_t step, double* p_sample_x, double* p_sample_y,
+                   double* p_sample_z, void* stream);
+
+/* Re/Im rho(k_p) = sum_j q_j {cos,sin}(k_p . r_j).  Replaces
+ * ComputePnumberChargeStructureFactorOp (kspace_calculator_op.h:106-121,
+ * kernel kspace_calculator_op.hip.cu:238-289). Deterministic FP64 reduction. */
+int rbx_rbe_structure_factor(const rbx_box* box, int num_atoms, int p_number,
+                             const double* charge, const double* p_sample_x,
+                             const double* p_sample_y, const double* p_sample_z,
+                             const double* px, const double* py,
+                             const double* pz, double* density_real,
+                             double* density_imag, void* stream);
+
+/* Per-atom RBE force.  Replaces ComputeRBEForceOp (kspace_calculator_op.h:123-135,
+ * kernel kspace_calculator_op.hip.cu:678-738). */
+int rbx_rbe_force(const rbx_box* box, int num_atoms, int p_number, double alpha,
+                  double rbe_sum_gauss, double qqr2e, const double* real_array,
+                  const double* imag_array, const double* charge,
+                  const double* p_sample_x, const double* p_sample_y,
+                  const double* p_sample_z, const double* px, const double* py,
+                  const double* pz, double* fx, double* fy, double* fz,
+                  void* stream);
+
+/* RBE energy and 6-component virial (xx,yy,zz,xy,xz,yz), written to device
+ * memory.  Replaces ComputeRBEForceVirialOp (kernel ComputeRBEVirial0,
+ * kspace_calculator_op.hip.cu:573-674); deterministic order. */
+int rbx_rbe_energy_virial(const rbx_box* box, int p, double alpha,
+                          double rbe_sum_gauss, double qqrd2e, double qsqsum,
+                          double qsum, const double* real_array,
+                          const double* imag_array, const double* p_sample_x,
+                          const double* p_sample_y, const double* p_sample_z,
+                          double* virial_tensor, double* energy, void* stream);
+
+/* Exact Ewald reciprocal force over the kmax box (+ per-atom virial).
+ * Replaces ComputeEwaldForceOp / ComputeKspaceChargeStructureFactorOp
+ * (kspace_calculator_op.hip.cu:176-213, 334-403). rho must hold num_k values;
+ * num_k = (2kx+1)(2ky+1)(2kz+1)-1. energy (device, may be NULL) receives the
+ * reciprocal + self energy of kspace_calculator.cpp:816-907. */
+int rbx_ewald_force(const rbx_box* box, int num_atoms, const int kmax[3],
+                    double alpha, double qqr2e, const double* charge,
+                    const double* px, const double* py, const double* pz,
+                    double* fx, double* fy, double* fz, double* energy,
+                    void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Neighbor-list ops (device pointers)                                       */
+/* ------------------------------------------------------------------------ */
+
+/* Cell grid of edge >= neighbor_cutoff: dims[d] = floor(L_d / neighbor_cutoff).
+ * Returns RBX_ERR_INVALID if a dimension has fewer than 3 cells. */
+int rbx_cell_grid(const rbx_box* box, double neighbor_cutoff, int dims[3]);
+
+/* Bin atoms into cells, stable-sort by cell and give cell ranges.  Replaces
+ * LinkedCell::AssignAtomsToCell + SortAtomsByCellKey + ComputeCellRangesIndices
+ * (src/neighbor_list/src/linked_cell/linked_cell.cpp:428-670,
+ * src/neighbor_list/src/op/rocm/linked_cell_op.hip.cu:57-164).
+ * perm[new] = old index (caller gathers its arrays); cell_start has
+ * ncell + 1 entries.  scratch needs rbx_cells_scratch_bytes(n, ncell) bytes. */
+size_t rbx_cells_scratch_bytes(int n, int ncell);
+int rbx_cells_sort(const rbx_box* box, double neighbor_cutoff, int n,
+                   const double* px, const double* py, const double* pz,
+                   int* perm, int* cell_of_sorted, int* cell_start,
+                   void* scratch, void* stream);
+
+/* Full (i->j and j->i) list of sorted atoms within neighbor_cutoff, j != i,
+ * row-major with a fixed row capacity: nbrs[i*cap + t], count[i] = true count.
+ * *overflow (device int) is set to 1 when some count exceeds cap.  Replaces
+ * Estimate/GenerateFullNeighborListOp (full_neighbor_list_op.hip.cu:177-288)
+ * for cells of edge >= neighbor_cutoff. */
+int rbx_full_list(const rbx_box* box, double neighbor_cutoff, int n,
+                  const double* px, const double* py, const double* pz,
+                  const int* cell_start, int cap, int* count, int* nbrs,
+                  int* overflow, void* stream);
+
+/* Split candidates into the RBL core list (r^2 < core_cutoff_2) and the hashed
+ * shell sample (r^2 < force_cutoff_2, SplitMix64 pair hash % freq == 0).
+ * Same arguments as FilterRblNeighborCandidatesOp
+ * (src/neighbor_list/src/op/rocm/rbl_full_neighbor_list_op.hip.cu:237-334):
+ * candidate CSR [start,end), core rows at core_start[i] with capacity
+ * max_core_neighbor_num[i], shell sample-major random_neighbors[s*n + i]. */
+int rbx_rbl_filter(double core_cutoff_2, double force_cutoff_2, int total_atom_num,
+                   const int* atoms_id, const double* px, const double* py,
+                   const double* pz, const int* candidate_start,
+                   const int* candidate_end, const int* candidate_neighbors,
+                   const int* max_core_neighbor_num, const int* core_start,
+                   int* core_end, int* core_neighbors,
+                   int random_neighbor_capacity, int* random_neighbors,
+                   int* random_neighbors_num,
+                   int* required_random_neighbor_capacity, const rbx_box* box,
+                   int* should_realloc, int selection_frequency,
+                   int sample_epoch, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Pair-force ops (device pointers)                                          */
+/* ------------------------------------------------------------------------ */
+
+/* RBL real-space force: core CSR [start_id, end_id) + sample-major shell list.
+ * Same arguments as LJCutCoulRBLForceOp (lj_cut_coul_kspace_op.h:155-181,
+ * kernel lj_cut_coul_kspace_op.hip.cu:569-683). */
+int rbx_pair_force_rbl(const rbx_box* box, double rs, double rc, int num_atoms,
+                       int neighbor_sample_num, int pice_num, double alpha,
+                       double qqr2e, const int* atoms_type, const double* sigma,
+                       const double* eps, const int* start_id, const int* end_id,
+                       const int* id_verletlist, const int* id_random_neighbor,
+                       const int* random_neighbor_num, const double* charge,
+                       const double* px, const double* py, const double* pz,
+                       double* fx, double* fy, double* fz, void* stream);
+
+/* Subtract the mean force over all atoms, computed on the device (FP64,
+ * deterministic).  Replaces the three thrust::reduce host round trips +
+ * FixRBLForceOp (lj_cut_coul_kspace.cpp:537-563, force_op.hip.cu:9-45).
+ * mean_out (device, 3 doubles) may be NULL. */
+int rbx_fix_rbl_force(int num_atoms, double* fx, double* fy, double* fz,
+                      double* mean_out, void* stream);
+
+/* Verlet real-space force + per-atom virial flat_virial[c*n + i] + energies.
+ * Same arguments as LJCutCoulForceOp (lj_cut_coul_kspace_op.h:117-140, kernel
+ * lj_cut_coul_kspace_op.hip.cu:256-356); total_evdwl / total_ecoul (device)
+ * are overwritten with deterministic sums (the reference accumulates). */
+int rbx_pair_force_verlet(const rbx_box* box, double cut_off, int num_atoms,
+                          double alpha, double qqr2e, const int* atoms_type,
+                          const double* sigma, const double* eps,
+                          const int* start_id, const int* end_id,
+                          const int* id_verletlist, const double* charge,
+                          const double* px, const double* py, const double* pz,
+                          double* fx, double* fy, double* fz,
+                          double* flat_virial, double* total_evdwl,
+                          double* total_ecoul, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Engine: LJCutCoulKspace (src/force/src/lj_cut_coul_kspace.cpp) with its   */
+/* KSpaceCalculator and neighbor builders, plus the NVE velocity-Verlet step */
+/* (NVEensemble::Solve, src/simulate_pipeline/src/nve_ensemble.cpp:59-91).   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct rbx_engine rbx_engine;
+
+typedef enum { RBX_PLAIN_FP64 = 0, RBX_MIXED = 1 } rbx_precision;
+typedef enum { RBX_NEIGHBOR_VERLET = 0, RBX_NEIGHBOR_RBL = 1 } rbx_neighbor_type;
+typedef enum { RBX_COULOMB_NONE = 0, RBX_COULOMB_RBE = 1, RBX_COULOMB_EWALD = 2 } rbx_coulomb_type;
+
+typedef struct {
+  int neighbor_type;        /* hyper_parameters.neighbor.type */
+  double cut_off;           /* hyper_parameters.neighbor.cut_off */
+  double r_core;            /* hyper_parameters.neighbor.r_core (RBL) */
+  double skin;              /* hyper_parameters.neighbor.skin */
+  int neighbor_sample_num;  /* hyper_parameters.neighbor.neighbor_sample_num */
+  int coulomb_type;         /* hyper_parameters.coulomb.type */
+  double alpha;             /* hyper_parameters.coulomb.alpha (= g_ewald^2) */
+  int coulomb_sample_num;   /* hyper_parameters.coulomb.coulomb_sample_num (P) */
+  int kmax[3];              /* hyper_parameters.coulomb.kmax (EWALD) */
+  uint64_t random_seed;     /* hyper_parameters.coulomb.random_seed */
+  double qqr2e;             /* from init_configuration.read_data.unit */
+  double dt;                /* execution.timestep */
+  int precision;            /* rbx_precision */
+  int ntypes;
+  const double* sigma;      /* host, ntypes */
+  const double* eps;        /* host, ntypes */
+  const double* mass;       /* host, ntypes */
+} rbx_params;
+
+/* Engine statistics (host copy). */
+typedef struct {
+  int64_t steps;            /* velocity-Verlet steps taken */
+  int64_t force_calls;      /* force evaluations */
+  int64_t rebuilds;         /* neighbor-list rebuilds */
+  int epoch;                /* RBL hash epoch / k-sample step of the last evaluation */
+  int selection_frequency;  /* RBL pice_num */
+  int candidate_capacity;   /* row capacity of the candidate list */
+  int64_t candidates;       /* candidate pairs in the list at the last rebuild */
+  double e_kspace;          /* last RBE energy (only if requested) */
+  double virial_kspace[6];
+} rbx_stats;
+
+rbx_engine* rbx_engine_create(const rbx_params* params, const rbx_box* box,
+                              int num_atoms, int device);
+/* Build from the reference's JSON keys (hyper_parameters.force_field/neighbor/
+ * coulomb, init_configuration.read_data.unit, execution.timestep) the way
+ * LJCutCoulKspace::Init + KSpaceCalculator::Init do
+ * (src/force/src/lj_cut_coul_kspace.cpp:424-462, kspace_calculator.cpp:159-355),
+ * with the same required-key errors; per-type sigma/eps/mass from host arrays.
+ * charges (host, num_atoms) may be NULL unless alpha is derived from
+ * coulomb.accuracy. precision: rbx_precision. Returns NULL on error. */
+rbx_engine* rbx_engine_create_json(const char* json_text, const rbx_box* box,
+                                   int num_atoms, int ntypes, const double* sigma,
+                                   const double* eps, const double* mass,
+                                   const double* charges, int precision, int device);
+void rbx_engine_destroy(rbx_engine* e);
+
+/* Host arrays in any atom order; the engine keeps its own (cell-sorted) order. */
+int rbx_engine_set_state(rbx_engine* e, const int* gid, const int* type,
+                         const double* charge, const double* px, const double* py,
+                         const double* pz, const double* vx, const double* vy,
+                         const double* vz);
+/* Inject the k-samples used by subsequent evaluations (host, p doubles each);
+ * pass NULL to return to on-device Philox sampling. */
+int rbx_engine_set_k_samples(rbx_engine* e, int p, const double* mx,
+                             const double* my, const double* mz);
+/* Force evaluation at the current positions with the given epoch (RBL hash
+ * epoch and k-sample step), as LJCutCoulKspace::Execute. */
+int rbx_engine_compute_forces(rbx_engine* e, int epoch);
+/* nsteps velocity-Verlet steps, state resident on the device. */
+int rbx_engine_step(rbx_engine* e, int nsteps);
+/* One step end to end from host buffers: copies x, v in (pinned or pageable),
+ * steps once and copies x, v, f out, in gid order of the host arrays given to
+ * rbx_engine_set_state. */
+int rbx_engine_step_host(rbx_engine* e, const double* x_in, const double* v_in,
+                         double* x_out, double* v_out, double* f_out);
+/* Copy the state to host arrays in gid order (index gid-gid_min). Any pointer
+ * may be NULL. f is the last total force (real space + k-space). */
+int rbx_engine_get_state(rbx_engine* e, double* px, double* py, double* pz,
+                         double* vx, double* vy, double* vz, double* fx,
+                         double* fy, double* fz);
+/* Last real-space (after mean removal for RBL) and k-space forces, gid order. */
+int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace);
+/* Last RBL lists as (gid_i, gid_j) pairs; sizes in/out. */
+int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core,
+                             int* shell_pairs, int64_t* n_shell);
+int rbx_engine_get_stats(rbx_engine* e, rbx_stats* out);
+/* Stream the engine launches on (cudaStream_t as void*). */
+void* rbx_engine_stream(rbx_engine* e);
+/* Mean device time per step since profiling was switched on, per phase, in
+ * ms: [0] kick + drift, [1] skin check / rebuild, [2] real space, [3] k-space
+ * (sample, rho, finalize, force + combine + kick). */
+int rbx_engine_phase_ms(rbx_engine* e, float out[4]);
+/* Enable/disable CUDA events around the phases (off by default); resets the
+ * accumulated phase times. */
+int rbx_engine_set_profiling(rbx_engine* e, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RBX_H */

@@ -1,0 +1,1083 @@
+/*
+ * rbx_oracle.c -- FP64 host restatement of RBMD 2.0's RBE + LJ/erfc-Coulomb
+ * hot path (see rbx_oracle.h).  TEST INFRASTRUCTURE: used only by tests/, the
+ * smoke check and bench.py's CPU-baseline leg, as the checker.
+ *
+ * Compiled with -ffp-contract=off so that every distance predicate rounds
+ * exactly like the reference's `POW(dx,2)+POW(dy,2)+POW(dz,2)`
+ * (src/neighbor_list/src/op/full_neighbor_list_op.h:98-106).
+ *
+ * Citations are relative to the RBMD 2.0 source tree.
+ */
+#include "rbx_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* EPSILON under USE_DOUBLE (src/common/rbmd_define.h:46-50). */
+#define ORC_EPSILON 0.0001
+
+static inline double box_len(const orc_box* b, int d) { return b->hi[d] - b->lo[d]; }
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* ========================================================================== */
+/* k-space                                                                    */
+/* ========================================================================== */
+
+/* ComputeRbeGaussianSum, src/force/src/kspace_calculator.cpp:68-78:
+ * S = prod_d H_d - 1, H_d = sqrt(alpha L_d^2/pi) * sum_{m=-10..10} exp(-alpha L_d^2 m^2). */
+double orc_rbe_gauss_sum(const orc_box* box, double alpha) {
+  double h[3] = {0.0, 0.0, 0.0};
+  for (int d = 0; d < 3; ++d) {
+    const double L = box_len(box, d);
+    const double factor = -(alpha * L * L);
+    for (int m = -10; m <= 10; ++m) h[d] += exp((double)(m * m) * factor);
+    h[d] *= sqrt(-(factor) / M_PI);
+  }
+  return h[0] * h[1] * h[2] - 1.0;
+}
+
+/* ComputePnumberChargeStructureFactorOpt,
+ * src/force/src/kspace_calculator_op/rocm/kspace_calculator_op.hip.cu:238-289:
+ * Re rho_p = sum_j q_j cos(k_p.r_j), Im rho_p = sum_j q_j sin(k_p.r_j), k = 2 pi m / L. */
+void orc_rbe_structure_factor(int n, int p, const orc_box* box, const double* q,
+                              const double* x, const double* y, const double* z,
+                              const double* mx, const double* my,
+                              const double* mz, double* re, double* im) {
+  const double Lx = box_len(box, 0), Ly = box_len(box, 1), Lz = box_len(box, 2);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int k = 0; k < p; ++k) {
+    const double kx = 2 * M_PI * mx[k] / Lx;
+    const double ky = 2 * M_PI * my[k] / Ly;
+    const double kz = 2 * M_PI * mz[k] / Lz;
+    double sr = 0.0, si = 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double dot = kx * x[j] + ky * y[j] + kz * z[j];
+      sr += q[j] * cos(dot);
+      si += q[j] * sin(dot);
+    }
+    re[k] = sr;
+    im[k] = si;
+  }
+}
+
+/* ComputeRBEForce + RBEForce, kspace_calculator_op.hip.cu:98-125, 678-738:
+ * F_i = (S/P) sum_p [-4 pi q_i qqr2e / (V k^2)] (cos(k.r_i) Im - sin(k.r_i) Re) k. */
+void orc_rbe_force(int n, int p, const orc_box* box, double S, double qqr2e,
+                   const double* re, const double* im, const double* q,
+                   const double* mx, const double* my, const double* mz,
+                   const double* x, const double* y, const double* z,
+                   double* fx, double* fy, double* fz) {
+  const double Lx = box_len(box, 0), Ly = box_len(box, 1), Lz = box_len(box, 2);
+  const double volume = Lx * Ly * Lz;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    const double factor_a = -4 * M_PI * q[i];
+    for (int k = 0; k < p; ++k) {
+      const double Kx = 2 * M_PI * mx[k] / Lx;
+      const double Ky = 2 * M_PI * my[k] / Ly;
+      const double Kz = 2 * M_PI * mz[k] / Lz;
+      const double k2 = Kx * Kx + Ky * Ky + Kz * Kz;
+      const double dot = Kx * x[i] + Ky * y[i] + Kz * z[i];
+      double f = (factor_a / (volume * k2)) * (cos(dot) * im[k] - sin(dot) * re[k]);
+      f *= qqr2e;
+      sx += f * Kx;
+      sy += f * Ky;
+      sz += f * Kz;
+    }
+    fx[i] = sx * S / p;
+    fy[i] = sy * S / p;
+    fz[i] = sz * S / p;
+  }
+}
+
+/* ComputeRBEVirial0, kspace_calculator_op.hip.cu:573-674 (the path the op uses):
+ * E = qqr2e [ (2 pi S/(P V)) sum |rho|^2/k^2 - sqrt(alpha) sum q^2/sqrt(pi)
+ *             - (pi/2) Q^2/(alpha V) ],
+ * W_ab = qqr2e (2 pi S/(P V)) sum (|rho|^2/k^2)(delta_ab - 2 k_a k_b (1/(4 alpha) + 1/k^2)).
+ * Summed in sample order (the reference's float atomics have no fixed order). */
+void orc_rbe_energy_virial(int p, const orc_box* box, double alpha, double S,
+                           double qqr2e, double qsq, double qsum,
+                           const double* re, const double* im,
+                           const double* mx, const double* my,
+                           const double* mz, double* virial6, double* energy) {
+  const double Lx = box_len(box, 0), Ly = box_len(box, 1), Lz = box_len(box, 2);
+  const double V = Lx * Ly * Lz;
+  const double coef = (2 * M_PI * S) / (p * V);
+  double e = 0.0, w[6] = {0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < p; ++k) {
+    const double kx = 2 * M_PI * mx[k] / Lx;
+    const double ky = 2 * M_PI * my[k] / Ly;
+    const double kz = 2 * M_PI * mz[k] / Lz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double rho2 = re[k] * re[k] + im[k] * im[k];
+    e += coef * rho2 / k2;
+    const double base = coef * rho2 / k2;
+    const double inner = (1.0 / (4 * alpha)) + (1.0 / k2);
+    w[0] += base * (1.0 - 2 * kx * kx * inner);
+    w[1] += base * (1.0 - 2 * ky * ky * inner);
+    w[2] += base * (1.0 - 2 * kz * kz * inner);
+    w[3] += base * (-2 * kx * ky * inner);
+    w[4] += base * (-2 * kx * kz * inner);
+    w[5] += base * (-2 * ky * kz * inner);
+  }
+  const double MY_PIS = 1.77245385090551602729, MY_PI2 = 1.57079632679489661923;
+  e -= sqrt(alpha) * qsq / MY_PIS + MY_PI2 * qsum * qsum / (alpha * V);
+  *energy = e * qqr2e;
+  for (int j = 0; j < 6; ++j) virial6[j] = w[j] * qqr2e;
+}
+
+/* Exact Ewald over the kmax box, the ordering of ExecuteOnKmax /
+ * ComputeKspaceEnergy (kspace_calculator.cpp:816-895). */
+int orc_ewald_num_k(const int kmax[3]) {
+  return (2 * kmax[0] + 1) * (2 * kmax[1] + 1) * (2 * kmax[2] + 1) - 1;
+}
+
+void orc_ewald_kvectors(const int kmax[3], const orc_box* box, double* kx,
+                        double* ky, double* kz) {
+  int idx = 0;
+  for (int i = -kmax[0]; i <= kmax[0]; ++i)
+    for (int j = -kmax[1]; j <= kmax[1]; ++j)
+      for (int k = -kmax[2]; k <= kmax[2]; ++k) {
+        if (i == 0 && j == 0 && k == 0) continue;
+        kx[idx] = 2 * M_PI * i / box_len(box, 0);
+        ky[idx] = 2 * M_PI * j / box_len(box, 1);
+        kz[idx] = 2 * M_PI * k / box_len(box, 2);
+        ++idx;
+      }
+}
+
+/* ComputeKspaceChargeStructureFactor, kspace_calculator_op.hip.cu:176-213. */
+void orc_ewald_structure_factor(int n, int nk, const double* q,
+                                const double* x, const double* y,
+                                const double* z, const double* kx,
+                                const double* ky, const double* kz, double* re,
+                                double* im) {
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int k = 0; k < nk; ++k) {
+    double sr = 0.0, si = 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double dot = kx[k] * x[j] + ky[k] * y[j] + kz[k] * z[j];
+      sr += q[j] * cos(dot);
+      si += q[j] * sin(dot);
+    }
+    re[k] = sr;
+    im[k] = si;
+  }
+}
+
+/* ComputeEwaldForceFlat, kspace_calculator_op.hip.cu:334-403. */
+void orc_ewald_force(int n, int nk, const orc_box* box, double alpha,
+                     double qqr2e, const double* kx, const double* ky,
+                     const double* kz, const double* re, const double* im,
+                     const double* q, const double* x, const double* y,
+                     const double* z, double* fx, double* fy, double* fz) {
+  const double volume = box_len(box, 0) * box_len(box, 1) * box_len(box, 2);
+  const double alpha_inv = 1.0 / alpha;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    const double base = -4.0 * M_PI * q[i];
+    double sx = 0, sy = 0, sz = 0;
+    for (int k = 0; k < nk; ++k) {
+      const double k2 = kx[k] * kx[k] + ky[k] * ky[k] + kz[k] * kz[k];
+      const double dot = -(kx[k] * x[i] + ky[k] * y[i] + kz[k] * z[i]);
+      const double fb = exp(-0.25 * k2 * alpha_inv);
+      double f = base / (volume * k2) * fb * (cos(dot) * im[k] + sin(dot) * re[k]);
+      f *= qqr2e;
+      sx += f * kx[k];
+      sy += f * ky[k];
+      sz += f * kz[k];
+    }
+    fx[i] = sx;
+    fy[i] = sy;
+    fz[i] = sz;
+  }
+}
+
+/* ComputeKspaceEnergy + ComputeSelfEnergy, kspace_calculator.cpp:816-907. */
+double orc_ewald_energy(int nk, const orc_box* box, double alpha, double qqr2e,
+                        double qsq, const double* kx, const double* ky,
+                        const double* kz, const double* re, const double* im) {
+  const double volume = box_len(box, 0) * box_len(box, 1) * box_len(box, 2);
+  double e = 0.0;
+  for (int k = 0; k < nk; ++k) {
+    const double k2 = kx[k] * kx[k] + ky[k] * ky[k] + kz[k] * kz[k];
+    e += exp(-0.25 * k2 / alpha) / k2 * (re[k] * re[k] + im[k] * im[k]);
+  }
+  e = qqr2e * (2 * M_PI / volume) * e;
+  return e + qqr2e * (-sqrt(alpha / M_PI) * qsq);
+}
+
+/* ========================================================================== */
+/* k-vector samplers                                                          */
+/* ========================================================================== */
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+ * as 1, 2, 3", SC'11): 10 rounds of two 32x32->64 multiplies with Weyl key
+ * schedule.  The project's on-device k-sampler uses the same function. */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2],
+                       uint32_t out[4]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+  uint32_t k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    c0 = hi1 ^ c1 ^ k0;
+    c1 = lo1;
+    c2 = hi0 ^ c3 ^ k1;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+/* Discrete Gaussian weights of the RBE importance density along one axis:
+ * P(m) ~ exp(-(2 pi m / L)^2 / (4 alpha)) (RBEPSample.h:98-105), tabulated in
+ * the order m = 0, +1, -1, +2, -2, ... until the weight drops below 1e-20. */
+static int rbe_axis_table(double L, double alpha, double* w, int max_entries,
+                          double* total) {
+  const double c = (M_PI * M_PI) / (alpha * L * L);
+  int cnt = 0;
+  double z = 0.0;
+  for (int m = 0;; ++m) {
+    const double v = exp(-c * (double)m * (double)m);
+    if (m > 0 && v < 1e-20) break;
+    if (cnt + (m == 0 ? 1 : 2) > max_entries) return -1;
+    if (m == 0) {
+      w[cnt++] = v;
+      z += v;
+    } else {
+      w[cnt++] = v;
+      w[cnt++] = v;
+      z += v;
+      z += v;
+    }
+  }
+  *total = z;
+  return cnt;
+}
+
+static inline int rbe_table_pick(const double* w, int cnt, double total, uint64_t u53) {
+  const double target = (double)u53 * (1.0 / 9007199254740992.0) * total;
+  double acc = 0.0;
+  int idx = cnt - 1;
+  for (int t = 0; t < cnt; ++t) {
+    acc += w[t];
+    if (target < acc) {
+      idx = t;
+      break;
+    }
+  }
+  /* idx 0 -> m = 0; odd 2k-1 -> +k; even 2k -> -k */
+  if (idx == 0) return 0;
+  return (idx & 1) ? (idx + 1) / 2 : -(idx / 2);
+}
+
+/* Counter-based RBE k-sampler (the project's replacement of RBEPSample's
+ * Metropolis-Hastings chain, RBEPSample.h:150-188): i.i.d. draws from the same
+ * discrete density, excluding m = (0,0,0).  Counter = (sample, 2*attempt+b,
+ * step_lo, step_hi), key = (seed_lo, seed_hi); three 53-bit uniforms per
+ * attempt drive an inverse-CDF pick per axis.  Returns 0, or -1 if a sample
+ * needed more than 64 attempts or a table overflowed. */
+int orc_rbe_sample_philox(int p, const orc_box* box, double alpha,
+                          uint64_t seed, int64_t step, double* mx, double* my,
+                          double* mz) {
+  enum { MAXT = 4096 };
+  static double w[3][MAXT];
+  double tot[3];
+  int cnt[3];
+  for (int d = 0; d < 3; ++d) {
+    cnt[d] = rbe_axis_table(box_len(box, d), alpha, w[d], MAXT, &tot[d]);
+    if (cnt[d] < 0) return -1;
+  }
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  const uint64_t ustep = (uint64_t)step;
+  for (int s = 0; s < p; ++s) {
+    int ok = 0;
+    for (int a = 0; a < 64 && !ok; ++a) {
+      uint32_t o[8];
+      const uint32_t c0[4] = {(uint32_t)s, (uint32_t)(2 * a), (uint32_t)ustep,
+                              (uint32_t)(ustep >> 32)};
+      const uint32_t c1[4] = {(uint32_t)s, (uint32_t)(2 * a + 1),
+                              (uint32_t)ustep, (uint32_t)(ustep >> 32)};
+      orc_philox4x32_10(c0, key, o);
+      orc_philox4x32_10(c1, key, o + 4);
+      int m[3];
+      for (int d = 0; d < 3; ++d) {
+        const uint64_t u = (((uint64_t)o[2 * d] << 32) | o[2 * d + 1]) >> 11;
+        m[d] = rbe_table_pick(w[d], cnt[d], tot[d], u);
+      }
+      if (m[0] != 0 || m[1] != 0 || m[2] != 0) {
+        mx[s] = m[0];
+        my[s] = m[1];
+        mz[s] = m[2];
+        ok = 1;
+      }
+    }
+    if (!ok) return -1;
+  }
+  return 0;
+}
+
+/* -- restatement of the reference's MH chain (statistical comparison only) -- */
+typedef struct {
+  uint64_t s;
+} orc_rng;
+static inline uint64_t rng_next(orc_rng* r) { /* SplitMix64 stream */
+  uint64_t z = (r->s += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+static inline double rng_uniform(orc_rng* r) {
+  return (double)(rng_next(r) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* FetchSample_1D, RBEPSample.h:124-148 (Box-Muller, U1 >= 1e-6). */
+static double mh_gauss(orc_rng* r, double sigma) {
+  double u1;
+  do {
+    u1 = rng_uniform(r);
+  } while (u1 < 1e-6);
+  const double u2 = rng_uniform(r);
+  return sigma * sqrt(-2.0 * log(u1)) * cos(2 * M_PI * u2);
+}
+
+typedef struct {
+  double alpha, L[3], H[3];
+} mh_ctx;
+
+/* Distribution_P, RBEPSample.h:98-105. */
+static double mh_P(const mh_ctx* c, double x, int d) {
+  const double t = 2 * M_PI * x / c->L[d];
+  return exp(-(t * t) / (4 * c->alpha)) / c->H[d];
+}
+/* Distribution_q, RBEPSample.h:107-122. */
+static double mh_q(const mh_ctx* c, double x, int d) {
+  const double s = sqrt(c->alpha * c->L[d] * c->L[d] / (M_PI * M_PI));
+  if (x == 0 || fabs(x) < 1.0e-13) return erf(0.5 / s);
+  return (erf((0.5 + fabs(x)) / s) - erf((fabs(x) - 0.5) / s)) / 2;
+}
+/* MH_Algorithm, RBEPSample.h:70-97. */
+static double mh_step(const mh_ctx* c, orc_rng* r, double m, double sigma, int d) {
+  const double mw = round(mh_gauss(r, sigma));
+  double prob = (mh_P(c, mw, d) / mh_P(c, m, d)) * (mh_q(c, m, d) / mh_q(c, mw, d));
+  if (prob > 1.0) prob = 1.0;
+  const double u = rng_uniform(r);
+  return (u <= prob) ? mw : m;
+}
+
+/* Fetch_P_Sample, RBEPSample.h:150-188, with sigma from
+ * KSpaceCalculator::RBEInit (kspace_calculator.cpp:697-700). */
+void orc_rbe_sample_mh(int p, const orc_box* box, double alpha, uint64_t seed,
+                       double* mx, double* my, double* mz) {
+  mh_ctx c;
+  c.alpha = alpha;
+  double sig[3];
+  for (int d = 0; d < 3; ++d) {
+    c.L[d] = box_len(box, d);
+    const double factor = -(alpha * c.L[d] * c.L[d]);
+    c.H[d] = 0.0;
+    for (int m = -10; m <= 10; ++m) c.H[d] += exp((double)(m * m) * factor);
+    c.H[d] *= sqrt(-factor / M_PI);
+    sig[d] = sqrt(alpha / 2.0) * c.L[d] / M_PI;
+  }
+  orc_rng r = {seed};
+  const double eps = 1e-6;
+  double x0[3];
+  do {
+    for (int d = 0; d < 3; ++d) x0[d] = round(mh_gauss(&r, sig[d]));
+  } while (fabs(x0[0]) < eps && fabs(x0[1]) < eps && fabs(x0[2]) < eps);
+  mx[0] = x0[0];
+  my[0] = x0[1];
+  mz[0] = x0[2];
+  for (int i = 1; i < p; i++) {
+    double x1[3];
+    for (int d = 0; d < 3; ++d) x1[d] = mh_step(&c, &r, x0[d], sig[d], d);
+    mx[i] = x1[0];
+    my[i] = x1[1];
+    mz[i] = x1[2];
+    x0[0] = x1[0];
+    x0[1] = x1[1];
+    x0[2] = x1[2];
+    if (fabs(x1[0]) < eps && fabs(x1[1]) < eps && fabs(x1[2]) < eps) {
+      i = i - 1;
+      continue;
+    }
+  }
+}
+
+/* ========================================================================== */
+/* Geometry, cells and neighbor lists                                         */
+/* ========================================================================== */
+
+/* MinImageDistance single shift, box.h:51-73. */
+static inline void min_image(const orc_box* b, double* dx, double* dy, double* dz) {
+  const double Lx = box_len(b, 0), Ly = box_len(b, 1), Lz = box_len(b, 2);
+  if (fabs(*dx) > Lx * 0.5) *dx -= (*dx > 0 ? Lx : -Lx);
+  if (fabs(*dy) > Ly * 0.5) *dy -= (*dy > 0 ? Ly : -Ly);
+  if (fabs(*dz) > Lz * 0.5) *dz -= (*dz > 0 ? Lz : -Lz);
+}
+
+/* MinImageDistance_while, box.h:75-97. */
+static inline void min_image_while(const orc_box* b, double* dx, double* dy, double* dz) {
+  const double Lx = box_len(b, 0), Ly = box_len(b, 1), Lz = box_len(b, 2);
+  /* bounded form of the while loop: nearest image by rint */
+  if (fabs(*dx) > Lx * 0.5) *dx -= Lx * rint(*dx / Lx);
+  if (fabs(*dy) > Ly * 0.5) *dy -= Ly * rint(*dy / Ly);
+  if (fabs(*dz) > Lz * 0.5) *dz -= Lz * rint(*dz / Lz);
+}
+
+/* CaculateDistance, full_neighbor_list_op.h:98-106 (i minus j, squared terms
+ * summed left to right without fused multiply-add). */
+double orc_dist2(const orc_box* box, double xi, double yi, double zi, double xj,
+                 double yj, double zj) {
+  double dx = xi - xj, dy = yi - yj, dz = zi - zj;
+  min_image(box, &dx, &dy, &dz);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+/* LinkedCell::Build (linked_cell.cpp:251-411) without halo: per-dimension cell
+ * count floor(L / neighbor_cutoff). */
+int orc_cell_grid(const orc_box* box, double neighbor_cutoff, int dims[3]) {
+  for (int d = 0; d < 3; ++d) {
+    const double nd = floor(box_len(box, d) / neighbor_cutoff);
+    if (!(nd >= 1.0)) return -1;
+    dims[d] = (int)nd;
+  }
+  return dims[0] * dims[1] * dims[2];
+}
+
+/* AssignAtomsToCell (linked_cell_op.hip.cu:57-138, halo width 0), stable sort
+ * by cell (SortAtomsByCellKey, linked_cell.cpp:485-560) and cell ranges
+ * (ComputeCellRangesIndices, linked_cell_op.hip.cu:142-164).
+ * perm[new] = old index; cell_of_sorted[new] = cell id. */
+int orc_cells_sort(int n, const orc_box* box, double neighbor_cutoff,
+                   const double* x, const double* y, const double* z,
+                   int* perm, int* cell_of_sorted, int* cell_start,
+                   int* cell_end) {
+  int dims[3];
+  const int ncell = orc_cell_grid(box, neighbor_cutoff, dims);
+  if (ncell <= 0) return -1;
+  double clen[3], crecip[3];
+  for (int d = 0; d < 3; ++d) {
+    clen[d] = box_len(box, d) / dims[d];
+    crecip[d] = 1.0 / clen[d];
+  }
+  int* cell = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  const double* pos[3] = {x, y, z};
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    int c[3];
+    for (int d = 0; d < 3; ++d) {
+      int v = (int)floor((pos[d][i] - box->lo[d]) * crecip[d]);
+      v = v < 0 ? 0 : v;
+      v = v > dims[d] - 1 ? dims[d] - 1 : v;
+      c[d] = v;
+    }
+    /* one-cell correction against the cell bounds lo + c*len */
+    int cc[3];
+    int inside = 1;
+    for (int d = 0; d < 3; ++d) {
+      const double cmin = c[d] * clen[d] + box->lo[d];
+      const double cmax = (c[d] + 1) * clen[d] + box->lo[d];
+      if (!(cmin <= pos[d][i] && pos[d][i] < cmax)) inside = 0;
+    }
+    if (!inside) {
+      for (int d = 0; d < 3; ++d) {
+        const double cmin = c[d] * clen[d] + box->lo[d];
+        const double cmax = (c[d] + 1) * clen[d] + box->lo[d];
+        cc[d] = c[d];
+        if (pos[d][i] < cmin)
+          cc[d]--;
+        else if (pos[d][i] >= cmax)
+          cc[d]++;
+        cc[d] = cc[d] < 0 ? 0 : (cc[d] > dims[d] - 1 ? dims[d] - 1 : cc[d]);
+      }
+      int ok = 1;
+      for (int d = 0; d < 3; ++d) {
+        const double cmin = cc[d] * clen[d] + box->lo[d];
+        const double cmax = (cc[d] + 1) * clen[d] + box->lo[d];
+        if (!(cmin <= pos[d][i] && pos[d][i] < cmax)) ok = 0;
+      }
+      if (ok) {
+        c[0] = cc[0];
+        c[1] = cc[1];
+        c[2] = cc[2];
+      }
+    }
+    cell[i] = (c[2] * dims[1] + c[1]) * dims[0] + c[0];
+  }
+  /* stable counting sort by cell id */
+  for (int c = 0; c < ncell; ++c) cell_start[c] = 0;
+  for (int i = 0; i < n; ++i) cell_start[cell[i]]++;
+  int acc = 0;
+  for (int c = 0; c < ncell; ++c) {
+    const int t = cell_start[c];
+    cell_start[c] = acc;
+    cell_end[c] = acc;
+    acc += t;
+  }
+  for (int i = 0; i < n; ++i) {
+    const int pos_new = cell_end[cell[i]]++;
+    perm[pos_new] = i;
+    cell_of_sorted[pos_new] = cell[i];
+  }
+  free(cell);
+  return ncell;
+}
+
+/* ComputeFullNeighborStencilCellOnTheFly (full_neighbor_list_op.hip.cu:19-85)
+ * for a whole-domain grid: stencil index s -> offsets (s%3-1, (s/3)%3-1, s/9-1). */
+static inline int stencil_cell(const int dims[3], int cell_idx, int s) {
+  const int ox = s % 3 - 1, oy = (s / 3) % 3 - 1, oz = s / 9 - 1;
+  const int cz = cell_idx / (dims[0] * dims[1]);
+  const int cy = (cell_idx - cz * dims[0] * dims[1]) / dims[0];
+  const int cx = cell_idx - dims[0] * (cy + dims[1] * cz);
+  int nx = (cx + ox) % dims[0];
+  if (nx < 0) nx += dims[0];
+  int ny = (cy + oy) % dims[1];
+  if (ny < 0) ny += dims[1];
+  int nz = (cz + oz) % dims[2];
+  if (nz < 0) nz += dims[2];
+  return (nz * dims[1] + ny) * dims[0] + nx;
+}
+
+/* GenerateFullNeighborListNoWarp (full_neighbor_list_op.hip.cu:227-288) over
+ * sorted atoms: j != i with dist2 < neighbor_cutoff^2.  Row i of nbrs holds up
+ * to cap entries; count[i] is the true count.  Returns the largest count. */
+int64_t orc_full_list(int n, const orc_box* box, double neighbor_cutoff,
+                      const double* x, const double* y, const double* z,
+                      const int* cell_of, const int* cell_start,
+                      const int* cell_end, int cap, int* count, int* nbrs) {
+  int dims[3];
+  if (orc_cell_grid(box, neighbor_cutoff, dims) <= 0) return -1;
+  const double cut2 = neighbor_cutoff * neighbor_cutoff;
+  int64_t maxc = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(max : maxc)
+  for (int i = 0; i < n; ++i) {
+    int cnt = 0;
+    for (int s = 0; s < 27; ++s) {
+      const int nc = stencil_cell(dims, cell_of[i], s);
+      for (int j = cell_start[nc]; j < cell_end[nc]; ++j) {
+        if (j == i) continue;
+        const double d2 = orc_dist2(box, x[i], y[i], z[i], x[j], y[j], z[j]);
+        if (d2 < cut2) {
+          if (cnt < cap && nbrs) nbrs[(size_t)i * cap + cnt] = j;
+          ++cnt;
+        }
+      }
+    }
+    count[i] = cnt;
+    if (cnt > maxc) maxc = cnt;
+  }
+  return maxc;
+}
+
+/* RblFullNeighborListBuilder::GetRblParams (rbl_full_neighbor_list_builder.cpp:193-228). */
+int orc_rbl_params(int n_global, const orc_box* box, double r_core,
+                   double cut_off, int sample_num, int* rs_num, int* rc_num) {
+  const double volume = box_len(box, 0) * box_len(box, 1) * box_len(box, 2);
+  const double rho = (double)n_global / volume;
+  const double coeff = 1.0 + (0.05 / rho - 0.05);
+  const int icoeff = (int)round(coeff);
+  const int rs = (int)(icoeff * rho * ceil(4.0 / 3.0 * M_PI * pow(r_core, 3)) + 1);
+  const int rc = (int)(icoeff * rho * ceil(4.0 / 3.0 * M_PI * pow(cut_off, 3)) + 1);
+  if (rs_num) *rs_num = rs;
+  if (rc_num) *rc_num = rc;
+  const int shell = rc - rs;
+  return shell <= sample_num ? 1 : (int)ceil((double)shell / (double)sample_num);
+}
+
+/* MixRblSampleKey (rbl_full_neighbor_list_op.hip.cu:6-11): SplitMix64 finaliser. */
+uint64_t orc_rbl_mix(uint64_t v) {
+  v += 0x9e3779b97f4a7c15ULL;
+  v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  v = (v ^ (v >> 27)) * 0x94d049bb133111ebULL;
+  return v ^ (v >> 31);
+}
+
+/* RblShellSampleSelected (rbl_full_neighbor_list_op.hip.cu:13-30). */
+int orc_rbl_selected(int freq, int epoch, int gid_i, int gid_j) {
+  if (freq <= 1) return 1;
+  uint64_t key = (uint64_t)(int64_t)epoch;
+  key ^= orc_rbl_mix((uint64_t)(int64_t)gid_i);
+  key ^= orc_rbl_mix((uint64_t)(int64_t)gid_j + 0xd1b54a32d192ed03ULL);
+  return orc_rbl_mix(key) % (uint64_t)freq == 0ULL;
+}
+
+/* FilterRBLNeighborCandidates (rbl_full_neighbor_list_op.hip.cu:237-304) with
+ * the host capacity loops run to completion (FilterCandidateList,
+ * rbl_full_neighbor_list_builder.cpp:416-471): core = r^2 < r_core^2 - EPS,
+ * sampled shell = r^2 < cut_off^2 - EPS and selected.  Row layout as cand. */
+void orc_rbl_filter(int n, const orc_box* box, double r_core, double cut_off,
+                    int freq, int epoch, const int* gid, const double* x,
+                    const double* y, const double* z, int cap,
+                    const int* cand_count, const int* cand, int* core_count,
+                    int* core, int* shell_count, int* shell) {
+  const double core2 = r_core * r_core - ORC_EPSILON;
+  const double force2 = cut_off * cut_off - ORC_EPSILON;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < n; ++i) {
+    int nc = 0, ns = 0;
+    const int* row = cand + (size_t)i * cap;
+    for (int t = 0; t < cand_count[i]; ++t) {
+      const int j = row[t];
+      if (j == i) continue;
+      const double d2 = orc_dist2(box, x[i], y[i], z[i], x[j], y[j], z[j]);
+      if (d2 < core2) {
+        core[(size_t)i * cap + nc++] = j;
+      } else if (d2 < force2 && orc_rbl_selected(freq, epoch, gid[i], gid[j])) {
+        shell[(size_t)i * cap + ns++] = j;
+      }
+    }
+    core_count[i] = nc;
+    shell_count[i] = ns;
+  }
+}
+
+/* ========================================================================== */
+/* Pair forces                                                                */
+/* ========================================================================== */
+
+/* lj126_rs / lj126_rcs (src/force/src/lj_op/rocm/lj_op.hip.cu:40-73) and
+ * CoulCutForce_rs_fix / _rcs_fix (lj_cut_coul_kspace_op.hip.cu:134-194). */
+static inline double lj_force(double eps_ij, double sigma_ij, double d2) {
+  const double s6 = pow(sigma_ij, 6.0);
+  const double d6 = pow(d2, 3.0);
+  const double sd6 = s6 / d6;
+  return -24 * eps_ij * ((2 * sd6 - 1) * sd6) / d2;
+}
+static inline double coul_force(double alpha, double qqr2e, double qi, double qj,
+                                double d2) {
+  const double dis = sqrt(d2);
+  const double erfcx = sqrt(alpha) * dis;
+  const double g = (1.0 - erf(erfcx)) / d2 +
+                   2 * sqrt(alpha) * exp(-alpha * d2) / (sqrt(M_PI) * dis);
+  return -qqr2e * qi * qj * g / dis;
+}
+
+/* ComputeLJCutCoulRBLForce (lj_cut_coul_kspace_op.hip.cu:569-683). */
+void orc_pair_force_rbl(int n, const orc_box* box, double r_core, double cut_off,
+                        int freq, double alpha, double qqr2e, const int* type,
+                        const double* sigma, const double* eps, const double* q,
+                        const double* x, const double* y, const double* z,
+                        int cap, const int* core_count, const int* core,
+                        const int* shell_count, const int* shell, double* fx,
+                        double* fy, double* fz) {
+  const double rs2 = r_core * r_core, rc2 = cut_off * cut_off;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < n; ++i) {
+    const int ti = type[i];
+    const double eps_i = eps[ti], sig_i = sigma[ti], qi = q[i];
+    double sx = 0, sy = 0, sz = 0, cx = 0, cy = 0, cz = 0;
+    for (int t = 0; t < core_count[i]; ++t) {
+      const int j = core[(size_t)i * cap + t];
+      const int tj = type[j];
+      const double eps_ij = sqrt(eps_i * eps[tj]);
+      const double sig_ij = (sig_i + sigma[tj]) / 2;
+      double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+      min_image(box, &dx, &dy, &dz);
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      double f = 0.0;
+      if (d2 < rs2 && d2 > ORC_EPSILON)
+        f = lj_force(eps_ij, sig_ij, d2) + coul_force(alpha, qqr2e, qi, q[j], d2);
+      sx += f * dx;
+      sy += f * dy;
+      sz += f * dz;
+    }
+    for (int t = 0; t < shell_count[i]; ++t) {
+      const int j = shell[(size_t)i * cap + t];
+      const int tj = type[j];
+      const double eps_ij = sqrt(eps_i * eps[tj]);
+      const double sig_ij = (sig_i + sigma[tj]) / 2;
+      double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+      min_image(box, &dx, &dy, &dz);
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      double f = 0.0;
+      if (d2 < rc2 && d2 > rs2)
+        f = freq * lj_force(eps_ij, sig_ij, d2) +
+            freq * coul_force(alpha, qqr2e, qi, q[j], d2);
+      cx += f * dx;
+      cy += f * dy;
+      cz += f * dz;
+    }
+    fx[i] = sx + cx;
+    fy[i] = sy + cy;
+    fz[i] = sz + cz;
+  }
+}
+
+/* LJCutCoulKspace::ComputeLJRBL mean-force removal (lj_cut_coul_kspace.cpp:537-563)
+ * + FixRBLForce (src/force/src/force_op/rocm/force_op.hip.cu:9-45). */
+void orc_fix_rbl(int n, double* fx, double* fy, double* fz, double mean_out[3]) {
+  double s[3] = {0, 0, 0};
+  for (int i = 0; i < n; ++i) {
+    s[0] += fx[i];
+    s[1] += fy[i];
+    s[2] += fz[i];
+  }
+  const double mx = s[0] / n, my = s[1] / n, mz = s[2] / n;
+  for (int i = 0; i < n; ++i) {
+    fx[i] -= mx;
+    fy[i] -= my;
+    fz[i] -= mz;
+  }
+  if (mean_out) {
+    mean_out[0] = mx;
+    mean_out[1] = my;
+    mean_out[2] = mz;
+  }
+}
+
+/* ComputeLJCutCoulForce (lj_cut_coul_kspace_op.hip.cu:256-356) with lj126
+ * (lj_op.hip.cu:18-38), CoulCutForce (lj_cut_coul_kspace_op.hip.cu:108-132)
+ * and ComputeVirial (lj_op.hip.cu:76-88); virial summed over atoms in index
+ * order (Force::ReduceVirial, force.h:24-41). */
+void orc_pair_force_verlet(int n, const orc_box* box, double cut_off,
+                           double alpha, double qqr2e, const int* type,
+                           const double* sigma, const double* eps,
+                           const double* q, const double* x, const double* y,
+                           const double* z, int cap, const int* count,
+                           const int* nbrs, double* fx, double* fy, double* fz,
+                           double* virial6, double* evdwl, double* ecoul) {
+  const double cut2 = cut_off * cut_off;
+  double* vir = (double*)calloc((size_t)6 * (n > 0 ? n : 1), sizeof(double));
+  double* elj = (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+  double* ecl = (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < n; ++i) {
+    const int ti = type[i];
+    double sx = 0, sy = 0, sz = 0, el = 0, ec = 0, w[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = 0; t < count[i]; ++t) {
+      const int j = nbrs[(size_t)i * cap + t];
+      const int tj = type[j];
+      const double eps_ij = sqrt(eps[ti] * eps[tj]);
+      const double sig_ij = (sigma[ti] + sigma[tj]) / 2;
+      double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+      min_image(box, &dx, &dy, &dz);
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      double flj = 0, elj_p = 0, fc = 0, ec_p = 0;
+      if (d2 < cut2) {
+        const double s6 = pow(sig_ij, 6.0);
+        const double d6 = pow(d2, 3.0);
+        const double sd6 = s6 / d6;
+        flj = -24 * eps_ij * ((2 * sd6 - 1) * sd6) / d2;
+        elj_p = 0.5 * (4 * eps_ij * (s6 / d6 - 1) * sd6);
+        const double dis = sqrt(d2);
+        const double erfc_v = erfc(sqrt(alpha) * dis);
+        const double g = erfc_v / d2 + 2 * sqrt(alpha) * exp(-alpha * d2) / (sqrt(M_PI) * dis);
+        fc = -qqr2e * q[i] * q[j] * g / dis;
+        ec_p = qqr2e * (0.5 * q[i] * q[j] * erfc_v / dis);
+      }
+      const double f = flj + fc;
+      sx += f * dx;
+      sy += f * dy;
+      sz += f * dz;
+      el += elj_p;
+      ec += ec_p;
+      w[0] += -0.5 * dx * dx * f;
+      w[1] += -0.5 * dy * dy * f;
+      w[2] += -0.5 * dz * dz * f;
+      w[3] += -0.5 * dx * dy * f;
+      w[4] += -0.5 * dx * dz * f;
+      w[5] += -0.5 * dy * dz * f;
+    }
+    fx[i] = sx;
+    fy[i] = sy;
+    fz[i] = sz;
+    elj[i] = el;
+    ecl[i] = ec;
+    for (int c = 0; c < 6; ++c) vir[(size_t)c * n + i] = w[c];
+  }
+  double tw[6] = {0, 0, 0, 0, 0, 0}, te = 0, tc = 0;
+  for (int i = 0; i < n; ++i) {
+    for (int c = 0; c < 6; ++c) tw[c] += vir[(size_t)c * n + i];
+    te += elj[i];
+    tc += ecl[i];
+  }
+  if (virial6)
+    for (int c = 0; c < 6; ++c) virial6[c] = tw[c];
+  if (evdwl) *evdwl = te;
+  if (ecoul) *ecoul = tc;
+  free(vir);
+  free(elj);
+  free(ecl);
+}
+
+/* DisplacementSq + max reduction (base_neighbor_list_builder.cpp:102-116, 270-283). */
+double orc_max_disp2(int n, const orc_box* box, const double* x,
+                     const double* y, const double* z, const double* x0,
+                     const double* y0, const double* z0) {
+  double m = 0.0;
+#pragma omp parallel for schedule(static) reduction(max : m)
+  for (int i = 0; i < n; ++i) {
+    double dx = x[i] - x0[i], dy = y[i] - y0[i], dz = z[i] - z0[i];
+    min_image_while(box, &dx, &dy, &dz);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 > m) m = d2;
+  }
+  return m;
+}
+
+/* ========================================================================== */
+/* Whole MD step on the host (CPU baseline): NVEensemble::Solve               */
+/* (src/simulate_pipeline/src/nve_ensemble.cpp:59-91) with LJCutCoulKspace::   */
+/* Execute (lj_cut_coul_kspace.cpp:464-471), RBL or Verlet real space.         */
+/* ========================================================================== */
+struct orc_engine {
+  int n, ntypes, use_rbl, p, sample_num, freq, cap, rebuilds, have_cache;
+  orc_box box;
+  double sigma[64], eps[64], mass[64];
+  double cut_off, r_core, skin, alpha, qqr2e, dt, S, qsq, qsum;
+  uint64_t seed;
+  int epoch;
+  int *gid, *type, *perm, *cell, *cstart, *cend, *cand_count, *cand, *core_count, *core,
+      *shell_count, *shell, *itmp;
+  double *q, *x, *y, *z, *vx, *vy, *vz, *fx, *fy, *fz, *x0, *y0, *z0, *tmp;
+  double *kfx, *kfy, *kfz, *mx, *my, *mz, *re, *im;
+  int ncell;
+};
+
+orc_engine* orc_engine_create(int n, const orc_box* box, int ntypes,
+                              const double* sigma, const double* eps,
+                              const double* mass, double cut_off, double r_core,
+                              double skin, int neighbor_sample_num,
+                              double alpha, int kspace_p, double qqr2e,
+                              double dt, uint64_t seed, int use_rbl) {
+  if (n <= 0 || ntypes <= 0 || ntypes > 64) return NULL;
+  orc_engine* e = (orc_engine*)calloc(1, sizeof(orc_engine));
+  e->n = n;
+  e->ntypes = ntypes;
+  e->box = *box;
+  for (int t = 0; t < ntypes; ++t) {
+    e->sigma[t] = sigma[t];
+    e->eps[t] = eps[t];
+    e->mass[t] = mass[t];
+  }
+  e->cut_off = cut_off;
+  e->r_core = r_core;
+  e->skin = skin;
+  e->sample_num = neighbor_sample_num;
+  e->alpha = alpha;
+  e->p = kspace_p;
+  e->qqr2e = qqr2e;
+  e->dt = dt;
+  e->seed = seed;
+  e->use_rbl = use_rbl;
+  e->freq = orc_rbl_params(n, box, r_core, cut_off, neighbor_sample_num, NULL, NULL);
+  e->S = orc_rbe_gauss_sum(box, alpha);
+  int dims[3];
+  e->ncell = orc_cell_grid(box, cut_off + skin, dims);
+  const size_t N = (size_t)n;
+#define A(ptr, T, cnt) ptr = (T*)calloc((cnt), sizeof(T))
+  A(e->gid, int, N); A(e->type, int, N); A(e->perm, int, N); A(e->cell, int, N);
+  A(e->itmp, int, N); A(e->cand_count, int, N); A(e->core_count, int, N);
+  A(e->shell_count, int, N);
+  A(e->cstart, int, e->ncell > 0 ? e->ncell : 1); A(e->cend, int, e->ncell > 0 ? e->ncell : 1);
+  A(e->q, double, N); A(e->x, double, N); A(e->y, double, N); A(e->z, double, N);
+  A(e->vx, double, N); A(e->vy, double, N); A(e->vz, double, N);
+  A(e->fx, double, N); A(e->fy, double, N); A(e->fz, double, N);
+  A(e->x0, double, N); A(e->y0, double, N); A(e->z0, double, N); A(e->tmp, double, N);
+  A(e->kfx, double, N); A(e->kfy, double, N); A(e->kfz, double, N);
+  A(e->mx, double, kspace_p); A(e->my, double, kspace_p); A(e->mz, double, kspace_p);
+  A(e->re, double, kspace_p); A(e->im, double, kspace_p);
+#undef A
+  return e;
+}
+
+void orc_engine_destroy(orc_engine* e) {
+  if (!e) return;
+  void* ptrs[] = {e->gid, e->type, e->perm, e->cell, e->itmp, e->cand_count, e->core_count,
+                  e->shell_count, e->cstart, e->cend, e->q, e->x, e->y, e->z, e->vx, e->vy,
+                  e->vz, e->fx, e->fy, e->fz, e->x0, e->y0, e->z0, e->tmp, e->kfx, e->kfy,
+                  e->kfz, e->mx, e->my, e->mz, e->re, e->im, e->cand, e->core, e->shell};
+  for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
+  free(e);
+}
+
+int orc_engine_set_state(orc_engine* e, const int* gid, const int* type,
+                         const double* q, const double* x, const double* y,
+                         const double* z, const double* vx, const double* vy,
+                         const double* vz) {
+  const size_t N = (size_t)e->n;
+  memcpy(e->gid, gid, N * sizeof(int));
+  memcpy(e->type, type, N * sizeof(int));
+  memcpy(e->q, q, N * sizeof(double));
+  memcpy(e->x, x, N * sizeof(double));
+  memcpy(e->y, y, N * sizeof(double));
+  memcpy(e->z, z, N * sizeof(double));
+  memcpy(e->vx, vx, N * sizeof(double));
+  memcpy(e->vy, vy, N * sizeof(double));
+  memcpy(e->vz, vz, N * sizeof(double));
+  e->qsq = 0;
+  e->qsum = 0;
+  for (int i = 0; i < e->n; ++i) {
+    e->qsq += q[i] * q[i];
+    e->qsum += q[i];
+  }
+  e->have_cache = 0;
+  e->epoch = 0;
+  return 0;
+}
+
+static void permute_d(double* a, const int* perm, double* tmp, int n) {
+  for (int i = 0; i < n; ++i) tmp[i] = a[perm[i]];
+  memcpy(a, tmp, sizeof(double) * (size_t)n);
+}
+static void permute_i(int* a, const int* perm, int* tmp, int n) {
+  for (int i = 0; i < n; ++i) tmp[i] = a[perm[i]];
+  memcpy(a, tmp, sizeof(int) * (size_t)n);
+}
+
+static int engine_rebuild(orc_engine* e) {
+  const int n = e->n;
+  if (orc_cells_sort(n, &e->box, e->cut_off + e->skin, e->x, e->y, e->z, e->perm, e->cell,
+                     e->cstart, e->cend) <= 0)
+    return -1;
+  double* arrs[] = {e->q, e->x, e->y, e->z, e->vx, e->vy, e->vz, e->fx, e->fy, e->fz};
+  for (size_t a = 0; a < sizeof(arrs) / sizeof(arrs[0]); ++a) permute_d(arrs[a], e->perm, e->tmp, n);
+  permute_i(e->gid, e->perm, e->itmp, n);
+  permute_i(e->type, e->perm, e->itmp, n);
+  const int64_t maxc = orc_full_list(n, &e->box, e->cut_off + e->skin, e->x, e->y, e->z,
+                                     e->cell, e->cstart, e->cend, 0, e->cand_count, NULL);
+  if (maxc < 0) return -1;
+  const int cap = (int)(maxc > 0 ? maxc : 1);
+  if (cap > e->cap) {
+    free(e->cand);
+    free(e->core);
+    free(e->shell);
+    e->cand = (int*)malloc(sizeof(int) * (size_t)n * cap);
+    e->core = (int*)malloc(sizeof(int) * (size_t)n * cap);
+    e->shell = (int*)malloc(sizeof(int) * (size_t)n * cap);
+    e->cap = cap;
+  }
+  orc_full_list(n, &e->box, e->cut_off + e->skin, e->x, e->y, e->z, e->cell, e->cstart,
+                e->cend, e->cap, e->cand_count, e->cand);
+  memcpy(e->x0, e->x, sizeof(double) * (size_t)n);
+  memcpy(e->y0, e->y, sizeof(double) * (size_t)n);
+  memcpy(e->z0, e->z, sizeof(double) * (size_t)n);
+  e->have_cache = 1;
+  e->rebuilds++;
+  return 0;
+}
+
+int orc_engine_compute_forces(orc_engine* e, int epoch) {
+  const int n = e->n;
+  const double thr = e->skin * 0.5;
+  int need = !e->have_cache || e->skin <= 0.0;
+  if (!need) {
+    const double md2 = orc_max_disp2(n, &e->box, e->x, e->y, e->z, e->x0, e->y0, e->z0);
+    need = md2 > thr * thr;
+  }
+  if (need && engine_rebuild(e) != 0) return -1;
+  if (e->use_rbl) {
+    orc_rbl_filter(n, &e->box, e->r_core, e->cut_off, e->freq, epoch, e->gid, e->x, e->y, e->z,
+                   e->cap, e->cand_count, e->cand, e->core_count, e->core, e->shell_count,
+                   e->shell);
+    orc_pair_force_rbl(n, &e->box, e->r_core, e->cut_off, e->freq, e->alpha, e->qqr2e, e->type,
+                       e->sigma, e->eps, e->q, e->x, e->y, e->z, e->cap, e->core_count, e->core,
+                       e->shell_count, e->shell, e->fx, e->fy, e->fz);
+    orc_fix_rbl(n, e->fx, e->fy, e->fz, NULL);
+  } else {
+    orc_pair_force_verlet(n, &e->box, e->cut_off, e->alpha, e->qqr2e, e->type, e->sigma, e->eps,
+                          e->q, e->x, e->y, e->z, e->cap, e->cand_count, e->cand, e->fx, e->fy,
+                          e->fz, NULL, NULL, NULL);
+  }
+  if (e->p > 0) {
+    if (orc_rbe_sample_philox(e->p, &e->box, e->alpha, e->seed, epoch, e->mx, e->my, e->mz) != 0)
+      return -1;
+    orc_rbe_structure_factor(n, e->p, &e->box, e->q, e->x, e->y, e->z, e->mx, e->my, e->mz,
+                             e->re, e->im);
+    orc_rbe_force(n, e->p, &e->box, e->S, e->qqr2e, e->re, e->im, e->q, e->mx, e->my, e->mz,
+                  e->x, e->y, e->z, e->kfx, e->kfy, e->kfz);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+      e->fx[i] += e->kfx[i];
+      e->fy[i] += e->kfy[i];
+      e->fz[i] += e->kfz[i];
+    }
+  }
+  return 0;
+}
+
+/* UpdateVelocity (update_velocity_op.hip.cu:5-28, fmt2v = 1) and
+ * UpdatePositionFlag + ApplyPBC (update_position_op.hip.cu:22-46, box.h:133-169). */
+static void engine_kick(orc_engine* e) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < e->n; ++i) {
+    const double m = e->mass[e->type[i]];
+    e->vx[i] += 0.5 * e->fx[i] / m * e->dt;
+    e->vy[i] += 0.5 * e->fy[i] / m * e->dt;
+    e->vz[i] += 0.5 * e->fz[i] / m * e->dt;
+  }
+}
+static void engine_drift(orc_engine* e) {
+  const double L[3] = {box_len(&e->box, 0), box_len(&e->box, 1), box_len(&e->box, 2)};
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < e->n; ++i) {
+    double* p[3] = {&e->x[i], &e->y[i], &e->z[i]};
+    const double v[3] = {e->vx[i], e->vy[i], e->vz[i]};
+    for (int d = 0; d < 3; ++d) {
+      double s = *p[d] + v[d] * e->dt;
+      if (s >= e->box.hi[d]) s -= L[d];
+      if (s < e->box.lo[d]) s += L[d];
+      *p[d] = s;
+    }
+  }
+}
+
+int orc_engine_step(orc_engine* e, int nsteps) {
+  if (!e->have_cache) {
+    if (orc_engine_compute_forces(e, e->epoch) != 0) return -1;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    engine_kick(e);
+    engine_drift(e);
+    e->epoch++;
+    if (orc_engine_compute_forces(e, e->epoch) != 0) return -1;
+    engine_kick(e);
+  }
+  return 0;
+}
+
+int orc_engine_get(orc_engine* e, int* gid, double* x, double* y, double* z,
+                   double* vx, double* vy, double* vz, double* fx, double* fy,
+                   double* fz) {
+  const size_t N = (size_t)e->n;
+  if (gid) memcpy(gid, e->gid, N * sizeof(int));
+  if (x) memcpy(x, e->x, N * sizeof(double));
+  if (y) memcpy(y, e->y, N * sizeof(double));
+  if (z) memcpy(z, e->z, N * sizeof(double));
+  if (vx) memcpy(vx, e->vx, N * sizeof(double));
+  if (vy) memcpy(vy, e->vy, N * sizeof(double));
+  if (vz) memcpy(vz, e->vz, N * sizeof(double));
+  if (fx) memcpy(fx, e->fx, N * sizeof(double));
+  if (fy) memcpy(fy, e->fy, N * sizeof(double));
+  if (fz) memcpy(fz, e->fz, N * sizeof(double));
+  return 0;
+}
+
+int orc_engine_rebuilds(const orc_engine* e) { return e->rebuilds; }

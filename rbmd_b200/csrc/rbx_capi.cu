@@ -1,0 +1,504 @@
+// rbx_capi.cu -- error plumbing and the op-level C ABI (include/rbx.h).
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "rbx.h"
+#include "rbx_common.cuh"
+#include "rbx_kernels.h"
+
+namespace rbx {
+
+static thread_local std::string g_err;
+static std::atomic<uint64_t> g_launches{0};
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
+int check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return RBX_ERR_CUDA;
+  }
+  return RBX_OK;
+}
+
+int sm_count() {
+  static thread_local int cached_dev = -1, cached = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return cached;
+  if (dev != cached_dev) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+      cached = v;
+    cached_dev = dev;
+  }
+  return cached;
+}
+
+int grid_for(long long work, int per_block, int max_blocks) {
+  long long b = (work + per_block - 1) / per_block;
+  if (b > max_blocks) b = max_blocks;
+  return b < 1 ? 1 : (int)b;
+}
+
+// The library runs only on sm_100-class devices; there is no CPU path.
+int require_device() {
+  int dev = 0, count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    set_error("no CUDA device available (librbx has no CPU fallback)");
+    return RBX_ERR_DEVICE;
+  }
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    set_error("cudaGetDevice failed");
+    return RBX_ERR_DEVICE;
+  }
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (major != 10) {
+    set_error("device %d has compute capability %d.x; librbx is built for sm_100a only", dev,
+              major);
+    return RBX_ERR_DEVICE;
+  }
+  return RBX_OK;
+}
+
+// Per-axis inverse-CDF table of the RBE importance density (see the oracle's
+// restatement): order m = 0, +1, -1, +2, -2, ... down to weight 1e-20.
+int rbe_axis_table(double L, double alpha, double* w, int max_entries, double* total) {
+  const double c = (M_PI * M_PI) / (alpha * L * L);
+  int cnt = 0;
+  double z = 0.0;
+  for (int m = 0;; ++m) {
+    const double v = exp(-c * (double)m * (double)m);
+    if (m > 0 && v < 1e-20) break;
+    if (cnt + (m == 0 ? 1 : 2) > max_entries) return -1;
+    if (m == 0) {
+      w[cnt++] = v;
+      z += v;
+    } else {
+      w[cnt++] = v;
+      w[cnt++] = v;
+      z += v;
+      z += v;
+    }
+  }
+  *total = z;
+  return cnt;
+}
+
+double gauss_sum(const rbx_box& b, double alpha) {
+  double h[3] = {0, 0, 0};
+  for (int d = 0; d < 3; ++d) {
+    const double L = b.hi[d] - b.lo[d];
+    const double factor = -(alpha * L * L);
+    for (int m = -10; m <= 10; ++m) h[d] += exp((double)(m * m) * factor);
+    h[d] *= sqrt(-(factor) / M_PI);
+  }
+  return h[0] * h[1] * h[2] - 1.0;
+}
+
+int rbl_freq(int n_global, const rbx_box& b, double r_core, double cut_off, int sample_num) {
+  const double V = (b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]) * (b.hi[2] - b.lo[2]);
+  const double rho = (double)n_global / V;
+  const double coeff = 1.0 + (0.05 / rho - 0.05);
+  const int icoeff = (int)round(coeff);
+  const int rs = (int)(icoeff * rho * ceil(4.0 / 3.0 * M_PI * pow(r_core, 3)) + 1);
+  const int rc = (int)(icoeff * rho * ceil(4.0 / 3.0 * M_PI * pow(cut_off, 3)) + 1);
+  const int shell = rc - rs;
+  return shell <= sample_num ? 1 : (int)ceil((double)shell / (double)sample_num);
+}
+
+static bool valid_box(const rbx_box* b) {
+  if (!b) return false;
+  for (int d = 0; d < 3; ++d)
+    if (!(b->hi[d] - b->lo[d] > 0.0) || !isfinite(b->hi[d] - b->lo[d])) return false;
+  return true;
+}
+
+}  // namespace rbx
+
+using namespace rbx;
+
+#define RBX_CHECK_BOX(b)                           \
+  do {                                             \
+    if (!valid_box(b)) {                           \
+      set_error("invalid box (hi must exceed lo)"); \
+      return RBX_ERR_INVALID;                      \
+    }                                              \
+  } while (0)
+
+#define RBX_TRY(expr)       \
+  do {                      \
+    const int _rc = (expr); \
+    if (_rc) return _rc;    \
+  } while (0)
+
+template <typename T>
+static int async_alloc(T** p, size_t count, cudaStream_t st) {
+  if (count == 0) count = 1;
+  if (cudaMallocAsync((void**)p, sizeof(T) * count, st) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("cudaMallocAsync of %zu bytes failed", sizeof(T) * count);
+    return RBX_ERR_NOMEM;
+  }
+  return RBX_OK;
+}
+
+extern "C" {
+
+const char* rbx_last_error(void) { return g_err.c_str(); }
+int rbx_version(void) { return RBX_VERSION; }
+uint64_t rbx_launch_count(void) { return g_launches.load(); }
+
+int rbx_rbe_gauss_sum(const rbx_box* box, double alpha, double* S) {
+  RBX_CHECK_BOX(box);
+  if (!(alpha > 0.0) || !S) {
+    set_error("rbx_rbe_gauss_sum: alpha must be > 0");
+    return RBX_ERR_INVALID;
+  }
+  *S = gauss_sum(*box, alpha);
+  return RBX_OK;
+}
+
+int rbx_rbl_params(int n_global, const rbx_box* box, double r_core, double cut_off,
+                   int neighbor_sample_num, int* freq) {
+  RBX_CHECK_BOX(box);
+  if (n_global <= 0 || neighbor_sample_num <= 0 || !freq) {
+    set_error("rbx_rbl_params: invalid RBL global density inputs");
+    return RBX_ERR_INVALID;
+  }
+  *freq = rbl_freq(n_global, *box, r_core, cut_off, neighbor_sample_num);
+  return RBX_OK;
+}
+
+int rbx_rbe_sample(const rbx_box* box, double alpha, int p, uint64_t seed, int64_t step,
+                   double* p_sample_x, double* p_sample_y, double* p_sample_z, void* stream) {
+  RBX_CHECK_BOX(box);
+  if (p < 0 || !(alpha > 0.0)) {
+    set_error("rbx_rbe_sample: need p >= 0 and alpha > 0");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  enum { MAXT = 4096 };
+  static thread_local double w[3 * MAXT];
+  int cnt[3];
+  double tot[3];
+  int off = 0;
+  for (int d = 0; d < 3; ++d) {
+    cnt[d] = rbe_axis_table(box->hi[d] - box->lo[d], alpha, w + off, MAXT, &tot[d]);
+    if (cnt[d] < 0) {
+      set_error("rbx_rbe_sample: k-sampler table too large");
+      return RBX_ERR_SAMPLER;
+    }
+    off += cnt[d];
+  }
+  double* dtab = nullptr;
+  int* dstatus = nullptr;
+  RBX_TRY(async_alloc(&dtab, (size_t)off, st));
+  RBX_TRY(async_alloc(&dstatus, 1, st));
+  cudaMemcpyAsync(dtab, w, sizeof(double) * off, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(dstatus, 0, sizeof(int), st);
+  int rc = launch_rbe_sample(p, dtab, cnt, tot, seed, step, p_sample_x, p_sample_y, p_sample_z,
+                             nullptr, dstatus, st);
+  int hstatus = 0;
+  if (!rc) {
+    cudaMemcpyAsync(&hstatus, dstatus, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = check_launch("rbe_sample sync");
+  }
+  cudaFreeAsync(dtab, st);
+  cudaFreeAsync(dstatus, st);
+  if (!rc && hstatus) {
+    set_error("rbx_rbe_sample: a sample needed more than 64 draws to avoid m = 0");
+    return RBX_ERR_SAMPLER;
+  }
+  return rc;
+}
+
+int rbx_rbe_structure_factor(const rbx_box* box, int num_atoms, int p_number,
+                             const double* charge, const double* p_sample_x,
+                             const double* p_sample_y, const double* p_sample_z,
+                             const double* px, const double* py, const double* pz,
+                             double* density_real, double* density_imag, void* stream) {
+  RBX_CHECK_BOX(box);
+  if (num_atoms < 0 || p_number < 0) {
+    set_error("rbx_rbe_structure_factor: negative size");
+    return RBX_ERR_INVALID;
+  }
+  if (p_number == 0) return RBX_OK;
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  const DBox b = make_dbox(*box);
+  const int nb = rbe_partial_blocks(num_atoms);
+  double *pr = nullptr, *pi = nullptr;
+  RBX_TRY(async_alloc(&pr, (size_t)nb * p_number, st));
+  RBX_TRY(async_alloc(&pi, (size_t)nb * p_number, st));
+  int rc = RBX_OK;
+  if (num_atoms > 0) {
+    rc = launch_rbe_rho_partial_f64(b, num_atoms, p_number, p_sample_x, p_sample_y, p_sample_z,
+                                    charge, px, py, pz, pr, pi, nb, st);
+  } else {
+    cudaMemsetAsync(pr, 0, sizeof(double) * nb * p_number, st);
+    cudaMemsetAsync(pi, 0, sizeof(double) * nb * p_number, st);
+  }
+  if (!rc)
+    rc = launch_rbe_finalize(b, p_number, nb, pr, pi, p_sample_x, p_sample_y, p_sample_z, 1.0,
+                             0.0, 1.0, 0.0, 0.0, density_real, density_imag, nullptr, nullptr,
+                             nullptr, 0, nullptr, 0, nullptr, st);
+  cudaFreeAsync(pr, st);
+  cudaFreeAsync(pi, st);
+  return rc;
+}
+
+int rbx_rbe_force(const rbx_box* box, int num_atoms, int p_number, double alpha,
+                  double rbe_sum_gauss, double qqr2e, const double* real_array,
+                  const double* imag_array, const double* charge, const double* p_sample_x,
+                  const double* p_sample_y, const double* p_sample_z, const double* px,
+                  const double* py, const double* pz, double* fx, double* fy, double* fz,
+                  void* stream) {
+  RBX_CHECK_BOX(box);
+  if (num_atoms < 0 || p_number <= 0) {
+    set_error("rbx_rbe_force: need num_atoms >= 0 and p_number > 0");
+    return RBX_ERR_INVALID;
+  }
+  if (num_atoms == 0) return RBX_OK;
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  const DBox b = make_dbox(*box);
+  KTab* tab = nullptr;
+  RBX_TRY(async_alloc(&tab, (size_t)p_number, st));
+  int rc = launch_rbe_finalize(b, p_number, 1, real_array, imag_array, p_sample_x, p_sample_y,
+                               p_sample_z, alpha, rbe_sum_gauss, qqr2e, 0.0, 0.0, nullptr,
+                               nullptr, nullptr, nullptr, tab, 0, nullptr, 0, nullptr, st);
+  if (!rc) {
+    RbeForceOut o;
+    o.f_out_x = fx;
+    o.f_out_y = fy;
+    o.f_out_z = fz;
+    rc = launch_rbe_force_f64(num_atoms, p_number, tab, charge, px, py, pz, o, st);
+  }
+  cudaFreeAsync(tab, st);
+  return rc;
+}
+
+int rbx_rbe_energy_virial(const rbx_box* box, int p, double alpha, double rbe_sum_gauss,
+                          double qqrd2e, double qsqsum, double qsum, const double* real_array,
+                          const double* imag_array, const double* p_sample_x,
+                          const double* p_sample_y, const double* p_sample_z,
+                          double* virial_tensor, double* energy, void* stream) {
+  RBX_CHECK_BOX(box);
+  if (p <= 0 || !virial_tensor || !energy) {
+    set_error("rbx_rbe_energy_virial: need p > 0 and output pointers");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  const DBox b = make_dbox(*box);
+  return launch_rbe_finalize(b, p, 1, real_array, imag_array, p_sample_x, p_sample_y, p_sample_z,
+                             alpha, rbe_sum_gauss, qqrd2e, qsqsum, qsum, nullptr, nullptr, energy,
+                             virial_tensor, nullptr, 0, nullptr, 0, nullptr, (cudaStream_t)stream);
+}
+
+int rbx_ewald_force(const rbx_box* box, int num_atoms, const int kmax[3], double alpha,
+                    double qqr2e, const double* charge, const double* px, const double* py,
+                    const double* pz, double* fx, double* fy, double* fz, double* energy,
+                    void* stream) {
+  RBX_CHECK_BOX(box);
+  if (!kmax || kmax[0] < 0 || kmax[1] < 0 || kmax[2] < 0 || !(alpha > 0.0) || num_atoms < 0) {
+    set_error("rbx_ewald_force: invalid kmax/alpha/num_atoms");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nk = (2 * kmax[0] + 1) * (2 * kmax[1] + 1) * (2 * kmax[2] + 1) - 1;
+  if (nk <= 0) return RBX_OK;
+  double *re = nullptr, *im = nullptr, *kv = nullptr;
+  RBX_TRY(async_alloc(&re, nk, st));
+  RBX_TRY(async_alloc(&im, nk, st));
+  RBX_TRY(async_alloc(&kv, (size_t)3 * nk, st));
+  double qsq = 0.0;
+  int rc = RBX_OK;
+  if (energy && num_atoms > 0) {  // sum q^2 for the self-energy term
+    std::vector<double> hq(num_atoms);
+    rc = cudaMemcpyAsync(hq.data(), charge, sizeof(double) * num_atoms, cudaMemcpyDeviceToHost,
+                         st) == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess
+             ? RBX_OK
+             : check_launch("ewald charge copy");
+    for (int i = 0; i < num_atoms; ++i) qsq += hq[i] * hq[i];
+  }
+  const DBox b = make_dbox(*box);
+  if (!rc)
+    rc = launch_ewald(b, num_atoms, kmax, alpha, qqr2e, qsq, charge, px, py, pz, re, im, kv, fx,
+                      fy, fz, energy, st);
+  cudaFreeAsync(re, st);
+  cudaFreeAsync(im, st);
+  cudaFreeAsync(kv, st);
+  return rc;
+}
+
+int rbx_cell_grid(const rbx_box* box, double neighbor_cutoff, int dims[3]) {
+  RBX_CHECK_BOX(box);
+  if (!(neighbor_cutoff > 0.0) || !dims) {
+    set_error("rbx_cell_grid: invalid neighbor cutoff");
+    return RBX_ERR_INVALID;
+  }
+  for (int d = 0; d < 3; ++d) {
+    const double nd = floor((box->hi[d] - box->lo[d]) / neighbor_cutoff);
+    dims[d] = nd >= 1.0 ? (int)nd : 0;
+    if (dims[d] < 3) {
+      set_error("The current simulation domain is too small for PBC: dimension %d has %d cells "
+                "of edge >= %g (need 3)",
+                d, dims[d], neighbor_cutoff);
+      return RBX_ERR_INVALID;
+    }
+  }
+  return RBX_OK;
+}
+
+size_t rbx_cells_scratch_bytes(int n, int ncell) { return cells_scratch_bytes(n, ncell); }
+
+int rbx_cells_sort(const rbx_box* box, double neighbor_cutoff, int n, const double* px,
+                   const double* py, const double* pz, int* perm, int* cell_of_sorted,
+                   int* cell_start, void* scratch, void* stream) {
+  int dims[3];
+  RBX_TRY(rbx_cell_grid(box, neighbor_cutoff, dims));
+  if (n < 0 || !scratch) {
+    set_error("rbx_cells_sort: invalid n or scratch");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  int* status = nullptr;
+  RBX_TRY(async_alloc(&status, 1, st));
+  cudaMemsetAsync(status, 0, sizeof(int), st);
+  int rc = launch_cells_sort(make_dbox(*box), dims, n, px, py, pz, perm, cell_of_sorted,
+                             cell_start, scratch, status, st);
+  int h = 0;
+  cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = check_launch("cells_sort sync");
+  cudaFreeAsync(status, st);
+  if (!rc && h) {
+    set_error("rbx_cells_sort: a cell holds more than 2048 atoms");
+    return RBX_ERR_CAPACITY;
+  }
+  return rc;
+}
+
+int rbx_full_list(const rbx_box* box, double neighbor_cutoff, int n, const double* px,
+                  const double* py, const double* pz, const int* cell_start, int cap, int* count,
+                  int* nbrs, int* overflow, void* stream) {
+  int dims[3];
+  RBX_TRY(rbx_cell_grid(box, neighbor_cutoff, dims));
+  if (n < 0 || cap <= 0 || !overflow) {
+    set_error("rbx_full_list: invalid n/cap/overflow");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  return launch_full_list(make_dbox(*box), dims, neighbor_cutoff, n, px, py, pz, cell_start, cap,
+                          count, nbrs, overflow, (cudaStream_t)stream);
+}
+
+int rbx_rbl_filter(double core_cutoff_2, double force_cutoff_2, int total_atom_num,
+                   const int* atoms_id, const double* px, const double* py, const double* pz,
+                   const int* candidate_start, const int* candidate_end,
+                   const int* candidate_neighbors, const int* max_core_neighbor_num,
+                   const int* core_start, int* core_end, int* core_neighbors,
+                   int random_neighbor_capacity, int* random_neighbors, int* random_neighbors_num,
+                   int* required_random_neighbor_capacity, const rbx_box* box,
+                   int* should_realloc, int selection_frequency, int sample_epoch, void* stream) {
+  RBX_CHECK_BOX(box);
+  if (total_atom_num < 0 || random_neighbor_capacity < 0) {
+    set_error("rbx_rbl_filter: negative size");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  return launch_ref_rbl_filter(core_cutoff_2, force_cutoff_2, total_atom_num, atoms_id, px, py,
+                               pz, candidate_start, candidate_end, candidate_neighbors,
+                               max_core_neighbor_num, core_start, core_end, core_neighbors,
+                               random_neighbor_capacity, random_neighbors, random_neighbors_num,
+                               required_random_neighbor_capacity, make_dbox(*box), should_realloc,
+                               make_divtest(selection_frequency), sample_epoch,
+                               (cudaStream_t)stream);
+}
+
+int rbx_pair_force_rbl(const rbx_box* box, double rs, double rc, int num_atoms,
+                       int neighbor_sample_num, int pice_num, double alpha, double qqr2e,
+                       const int* atoms_type, const double* sigma, const double* eps,
+                       const int* start_id, const int* end_id, const int* id_verletlist,
+                       const int* id_random_neighbor, const int* random_neighbor_num,
+                       const double* charge, const double* px, const double* py,
+                       const double* pz, double* fx, double* fy, double* fz, void* stream) {
+  (void)neighbor_sample_num;
+  RBX_CHECK_BOX(box);
+  if (num_atoms < 0) {
+    set_error("rbx_pair_force_rbl: negative num_atoms");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  return launch_ref_pair_rbl(make_dbox(*box), rs, rc, num_atoms, pice_num, alpha, qqr2e,
+                             atoms_type, sigma, eps, start_id, end_id, id_verletlist,
+                             id_random_neighbor, random_neighbor_num, charge, px, py, pz, fx, fy,
+                             fz, (cudaStream_t)stream);
+}
+
+int rbx_fix_rbl_force(int num_atoms, double* fx, double* fy, double* fz, double* mean_out,
+                      void* stream) {
+  if (num_atoms <= 0) {
+    set_error("rbx_fix_rbl_force: num_atoms must be > 0");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  double* mean = mean_out;
+  if (!mean) RBX_TRY(async_alloc(&mean, 3, st));
+  int rc = launch_reduce_cols(num_atoms, 1, fx, mean, 1.0 / num_atoms, st);
+  if (!rc) rc = launch_reduce_cols(num_atoms, 1, fy, mean + 1, 1.0 / num_atoms, st);
+  if (!rc) rc = launch_reduce_cols(num_atoms, 1, fz, mean + 2, 1.0 / num_atoms, st);
+  if (!rc) rc = launch_sub_mean(num_atoms, fx, fy, fz, mean, st);
+  if (!mean_out) cudaFreeAsync(mean, st);
+  return rc;
+}
+
+int rbx_pair_force_verlet(const rbx_box* box, double cut_off, int num_atoms, double alpha,
+                          double qqr2e, const int* atoms_type, const double* sigma,
+                          const double* eps, const int* start_id, const int* end_id,
+                          const int* id_verletlist, const double* charge, const double* px,
+                          const double* py, const double* pz, double* fx, double* fy, double* fz,
+                          double* flat_virial, double* total_evdwl, double* total_ecoul,
+                          void* stream) {
+  RBX_CHECK_BOX(box);
+  if (num_atoms < 0) {
+    set_error("rbx_pair_force_verlet: negative num_atoms");
+    return RBX_ERR_INVALID;
+  }
+  if (num_atoms == 0) return RBX_OK;
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  double* epart = nullptr;
+  RBX_TRY(async_alloc(&epart, (size_t)2 * num_atoms, st));
+  int rc = launch_ref_pair_verlet(make_dbox(*box), cut_off, num_atoms, alpha, qqr2e, atoms_type,
+                                  sigma, eps, start_id, end_id, id_verletlist, charge, px, py, pz,
+                                  fx, fy, fz, flat_virial, epart, st);
+  if (!rc && total_evdwl) rc = launch_reduce_cols(num_atoms, 1, epart, total_evdwl, 1.0, st);
+  if (!rc && total_ecoul)
+    rc = launch_reduce_cols(num_atoms, 1, epart + num_atoms, total_ecoul, 1.0, st);
+  cudaFreeAsync(epart, st);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,762 @@
+// rbx_engine.cu -- the engine behind rbx_engine_*: the force evaluation of
+// LJCutCoulKspace::Execute (src/force/src/lj_cut_coul_kspace.cpp:464-471:
+// real space, then KSpaceCalculator::Execute, then SumForces) and the NVE
+// velocity-Verlet step of NVEensemble::Solve
+// (src/simulate_pipeline/src/nve_ensemble.cpp:59-91), with all state resident
+// on one GPU in cell-sorted order.
+//
+// Per step (RBL + RBE): kick, drift(+wrap, +skin check, +fixed point),
+// [rebuild if max displacement > skin/2], fused RBL filter+pair force, Philox
+// k-sample, rho(k) partials, finalize (rho, energy/virial, force table, RBL
+// mean force), k-space force fused with SumForces, the mean removal and the
+// second half kick.  Host syncs per step: one 8-byte read of the displacement
+// maximum.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "rbx.h"
+#include "rbx_common.cuh"
+#include "rbx_engine.h"
+#include "rbx_kernels.h"
+
+namespace rbx {
+int require_device();
+double gauss_sum(const rbx_box& b, double alpha);
+int rbl_freq(int n_global, const rbx_box& b, double r_core, double cut_off, int sample_num);
+}  // namespace rbx
+
+using namespace rbx;
+
+#define ETRY(expr)          \
+  do {                      \
+    const int _rc = (expr); \
+    if (_rc) return _rc;    \
+  } while (0)
+
+static int cuda_ok(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? RBX_ERR_NOMEM : RBX_ERR_CUDA;
+  }
+  return RBX_OK;
+}
+
+template <typename T>
+static int dalloc(T** p, size_t count) {
+  if (count == 0) count = 1;
+  return cuda_ok(cudaMalloc((void**)p, sizeof(T) * count), "cudaMalloc");
+}
+
+rbx_engine::~rbx_engine() {
+  if (device >= 0) cudaSetDevice(device);
+  for (void* ptr : allocs) cudaFree(ptr);
+  if (h_pinned) cudaFreeHost(h_pinned);
+  for (int i = 0; i < 8; ++i)
+    if (ev[i]) cudaEventDestroy(ev[i]);
+  for (cudaEvent_t e : pev) cudaEventDestroy(e);
+  if (st) cudaStreamDestroy(st);
+}
+
+template <typename T>
+int rbx_engine::alloc(T** p, size_t count) {
+  ETRY(dalloc(p, count));
+  allocs.push_back((void*)*p);
+  return RBX_OK;
+}
+
+template <typename T>
+void rbx_engine::release(T*& p) {
+  if (!p) return;
+  auto it = std::find(allocs.begin(), allocs.end(), (void*)p);
+  if (it != allocs.end()) allocs.erase(it);
+  cudaFree(p);
+  p = nullptr;
+}
+
+int rbx_engine::init() {
+  ETRY(cuda_ok(cudaSetDevice(device), "cudaSetDevice"));
+  ETRY(require_device());
+  ETRY(cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate"));
+  dbox = make_dbox(box);
+  const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
+  if (!(prm.cut_off > 0.0) || prm.skin < 0.0 || (rbl && !(prm.r_core > 0.0)) ||
+      (rbl && prm.neighbor_sample_num <= 0)) {
+    set_error("invalid neighbor parameters (cut_off > 0, skin >= 0, r_core > 0, "
+              "neighbor_sample_num > 0 for RBL)");
+    return RBX_ERR_CONFIG;
+  }
+  if (prm.coulomb_type == RBX_COULOMB_RBE && (prm.coulomb_sample_num <= 0 || !(prm.alpha > 0))) {
+    set_error("RBE needs coulomb_sample_num > 0 and alpha > 0");
+    return RBX_ERR_CONFIG;
+  }
+  if (prm.ntypes <= 0 || prm.ntypes > 16) {
+    set_error("ntypes must be in [1, 16]");
+    return RBX_ERR_CONFIG;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (prm.cut_off + prm.skin > 0.5 * dbox.len[d]) {
+      set_error("cut_off + skin (%g) exceeds half the box length (%g) along dimension %d",
+                prm.cut_off + prm.skin, 0.5 * dbox.len[d], d);
+      return RBX_ERR_CONFIG;
+    }
+  ETRY(rbx_cell_grid(&box, prm.cut_off + prm.skin, dims));
+  ncell = dims[0] * dims[1] * dims[2];
+  freq = rbl ? rbl_freq(n, box, prm.r_core, prm.cut_off, prm.neighbor_sample_num) : 1;
+  div = make_divtest(freq);
+  P = prm.coulomb_type == RBX_COULOMB_RBE ? prm.coulomb_sample_num : 0;
+  S = P > 0 ? gauss_sum(box, prm.alpha) : 0.0;
+
+  const size_t N = (size_t)n;
+  double** dptrs[] = {&x, &y, &z, &vx, &vy, &vz, &fx, &fy, &fz, &q, &x0, &y0, &z0,
+                      &fpx, &fpy, &fpz, &fkx, &fky, &fkz, &tmpd};
+  for (double** p : dptrs) ETRY(alloc(p, N));
+  ETRY(alloc(&stage, 9 * N));  // host transfer staging (x,v in; x,v,f out)
+  int** iptrs[] = {&type, &gid, &orig, &tmpi, &perm, &cell_of_sorted, &cand_count};
+  for (int** p : iptrs) ETRY(alloc(p, N));
+  ETRY(alloc(&key_a, N));
+  ETRY(alloc(&key_b, N));
+  ETRY(alloc(&tmpu, N));
+  ETRY(alloc(&atoms, N));
+  ETRY(alloc(&cell_start, (size_t)ncell + 1));
+  ETRY(alloc(&cell_scratch, cells_scratch_bytes(n, ncell)));
+  ETRY(alloc(&dflags, 8));
+  ETRY(alloc(&max_d2, 1));
+  ETRY(alloc(&cand_total, 1));
+  nfpart = rbl_fused_blocks(n);
+  ETRY(alloc(&fpart, (size_t)nfpart * 3));
+  ETRY(alloc(&epart, (size_t)nfpart * 8));
+  ETRY(alloc(&mean, 3));
+  ETRY(alloc(&ek, 1));
+  ETRY(alloc(&virk, 6));
+  ETRY(alloc(&inv_mass, (size_t)prm.ntypes));
+  ETRY(alloc(&lj_eps, (size_t)prm.ntypes * prm.ntypes));
+  ETRY(alloc(&lj_s6, (size_t)prm.ntypes * prm.ntypes));
+  // LJ mixing of ComputeLJCutCoulRBLForce (lj_cut_coul_kspace_op.hip.cu:582-600):
+  // eps_ij = sqrt(eps_i eps_j), sigma_ij = (sigma_i + sigma_j)/2, sigma_ij^6.
+  {
+    const int nt = prm.ntypes;
+    std::vector<double> he(nt * nt), hs(nt * nt), im(nt);
+    for (int a = 0; a < nt; ++a) {
+      im[a] = 1.0 / mass[a];
+      for (int b = 0; b < nt; ++b) {
+        he[a * nt + b] = sqrt(eps[a] * eps[b]);
+        hs[a * nt + b] = pow((sigma[a] + sigma[b]) / 2, 6.0);
+      }
+    }
+    ETRY(cuda_ok(cudaMemcpy(inv_mass, im.data(), sizeof(double) * nt, cudaMemcpyHostToDevice),
+                 "H2D"));
+    ETRY(cuda_ok(cudaMemcpy(lj_eps, he.data(), sizeof(double) * nt * nt, cudaMemcpyHostToDevice),
+                 "H2D"));
+    ETRY(cuda_ok(cudaMemcpy(lj_s6, hs.data(), sizeof(double) * nt * nt, cudaMemcpyHostToDevice),
+                 "H2D"));
+  }
+  if (P > 0) {
+    nparts = rbe_partial_blocks(n);
+    ETRY(alloc(&mx, (size_t)P));
+    ETRY(alloc(&my, (size_t)P));
+    ETRY(alloc(&mz, (size_t)P));
+    ETRY(alloc(&mi, (size_t)3 * P));
+    ETRY(alloc(&part_re, (size_t)nparts * P));
+    ETRY(alloc(&part_im, (size_t)nparts * P));
+    ETRY(alloc(&rho_re, (size_t)P));
+    ETRY(alloc(&rho_im, (size_t)P));
+    ETRY(alloc(&tab, (size_t)P));
+    // Philox sampler tables
+    std::vector<double> w;
+    int off = 0;
+    for (int d = 0; d < 3; ++d) {
+      std::vector<double> t(8192);
+      tcnt[d] = rbe_axis_table(dbox.len[d], prm.alpha, t.data(), 8192, &ttot[d]);
+      if (tcnt[d] < 0) {
+        set_error("k-sampler table too large for this box/alpha");
+        return RBX_ERR_SAMPLER;
+      }
+      w.insert(w.end(), t.begin(), t.begin() + tcnt[d]);
+      off += tcnt[d];
+    }
+    ETRY(alloc(&sample_tables, (size_t)off));
+    ETRY(cuda_ok(cudaMemcpy(sample_tables, w.data(), sizeof(double) * off, cudaMemcpyHostToDevice),
+                 "H2D"));
+  } else {
+    ETRY(alloc(&tab, 1));
+    ETRY(alloc(&mx, 1));
+    ETRY(alloc(&my, 1));
+    ETRY(alloc(&mz, 1));
+  }
+  // candidate capacity from the number density, with headroom (a row that
+  // overflows triggers a regrow and rebuild)
+  const double V = dbox.len[0] * dbox.len[1] * dbox.len[2];
+  const double rcs = prm.cut_off + prm.skin;
+  const double expect = (double)n / V * 4.0 / 3.0 * M_PI * rcs * rcs * rcs;
+  cap = ((int)(1.3 * expect + 64) + 31) / 32 * 32;
+  ETRY(alloc(&cand, N * (size_t)cap));
+  ETRY(cuda_ok(cudaHostAlloc((void**)&h_pinned, 64, cudaHostAllocDefault), "cudaHostAlloc"));
+  for (int i = 0; i < 8; ++i) ETRY(cuda_ok(cudaEventCreate(&ev[i]), "cudaEventCreate"));
+  pp.box = dbox;
+  pp.rs2 = prm.r_core * prm.r_core;
+  pp.rc2 = prm.cut_off * prm.cut_off;
+  pp.core2_list = prm.r_core * prm.r_core - RBX_EPSILON;
+  pp.force2_list = prm.cut_off * prm.cut_off - RBX_EPSILON;
+  pp.alpha = prm.alpha;
+  pp.sqrt_alpha = sqrt(prm.alpha);
+  pp.qqr2e = prm.qqr2e;
+  pp.freq = freq;
+  pp.div = div;
+  pp.ntypes = prm.ntypes;
+  pp.lj_eps = lj_eps;
+  pp.lj_s6 = lj_s6;
+  for (int d = 0; d < 3; ++d) ms.s[d] = dbox.len[d] / 4294967296.0;
+  return RBX_OK;
+}
+
+int rbx_engine::set_state(const int* hgid, const int* htype, const double* hq, const double* hx,
+                          const double* hy, const double* hz, const double* hvx,
+                          const double* hvy, const double* hvz) {
+  cudaSetDevice(device);
+  const size_t N = (size_t)n;
+  for (int i = 0; i < n; ++i)
+    if (htype[i] < 0 || htype[i] >= prm.ntypes) {
+      set_error("atom %d has type %d outside [0, %d)", i, htype[i], prm.ntypes);
+      return RBX_ERR_INVALID;
+    }
+  std::vector<int> horig(N);
+  for (int i = 0; i < n; ++i) horig[i] = i;
+  qsq = 0;
+  qsum = 0;
+  for (int i = 0; i < n; ++i) {
+    qsq += hq[i] * hq[i];
+    qsum += hq[i];
+  }
+  const double* hsrc[] = {hx, hy, hz, hvx, hvy, hvz, hq};
+  double* ddst[] = {x, y, z, vx, vy, vz, q};
+  for (int a = 0; a < 7; ++a)
+    ETRY(cuda_ok(cudaMemcpyAsync(ddst[a], hsrc[a], sizeof(double) * N, cudaMemcpyHostToDevice, st),
+                 "H2D state"));
+  ETRY(cuda_ok(cudaMemcpyAsync(type, htype, sizeof(int) * N, cudaMemcpyHostToDevice, st), "H2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(gid, hgid, sizeof(int) * N, cudaMemcpyHostToDevice, st), "H2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(orig, horig.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st),
+               "H2D"));
+  ETRY(cuda_ok(cudaMemsetAsync(fx, 0, sizeof(double) * N, st), "memset"));
+  ETRY(cuda_ok(cudaMemsetAsync(fy, 0, sizeof(double) * N, st), "memset"));
+  ETRY(cuda_ok(cudaMemsetAsync(fz, 0, sizeof(double) * N, st), "memset"));
+  ETRY(launch_rbl_keys(n, gid, key_a, key_b, st));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "set_state sync"));
+  have_cache = false;
+  have_forces = false;
+  epoch = 0;
+  return RBX_OK;
+}
+
+// Rebuild: cell sort, permute every per-atom array, candidate list.
+int rbx_engine::rebuild() {
+  int* status = dflags;
+  ETRY(cuda_ok(cudaMemsetAsync(dflags, 0, sizeof(int) * 8, st), "memset"));
+  ETRY(cuda_ok(cudaMemsetAsync(cand_total, 0, sizeof(long long), st), "memset"));
+  ETRY(launch_cells_sort(dbox, dims, n, x, y, z, perm, cell_of_sorted, cell_start, cell_scratch,
+                         status, st));
+  double** darr[] = {&x, &y, &z, &vx, &vy, &vz, &fx, &fy, &fz, &q, &fpx, &fpy, &fpz};
+  for (double** a : darr) {
+    ETRY(launch_gather_f64(n, perm, *a, tmpd, st));
+    std::swap(*a, tmpd);
+  }
+  int** iarr[] = {&type, &gid, &orig};
+  for (int** a : iarr) {
+    ETRY(launch_gather_i32(n, perm, *a, tmpi, st));
+    std::swap(*a, tmpi);
+  }
+  unsigned long long** uarr[] = {&key_a, &key_b};
+  for (unsigned long long** a : uarr) {
+    ETRY(launch_gather_u64(n, perm, *a, tmpu, st));
+    std::swap(*a, tmpu);
+  }
+  ETRY(cuda_ok(cudaMemcpyAsync(x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(y0, y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(z0, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
+  if (prm.precision == RBX_MIXED) ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    ETRY(cuda_ok(cudaMemsetAsync(dflags + 1, 0, sizeof(int), st), "memset"));
+    ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
+                          cand_count, cand, dflags + 1, st));
+    int h[2] = {0, 0};
+    ETRY(cuda_ok(cudaMemcpyAsync(h, dflags, sizeof(int) * 2, cudaMemcpyDeviceToHost, st), "D2H"));
+    ETRY(cuda_ok(cudaStreamSynchronize(st), "rebuild sync"));
+    if (h[0]) {
+      set_error("cell sort: a cell holds more than 2048 atoms");
+      return RBX_ERR_CAPACITY;
+    }
+    if (h[1] & 2) {
+      set_error("candidate list: a cell exceeds the staging capacity");
+      return RBX_ERR_CAPACITY;
+    }
+    if (!(h[1] & 1)) {
+      have_cache = true;
+      ++rebuilds;
+      return launch_sum_i32(n, cand_count, cand_total, st);
+    }
+    // grow the row capacity and rebuild the list
+    int maxc = 0;
+    {
+      std::vector<int> hc(n);
+      ETRY(cuda_ok(cudaMemcpy(hc.data(), cand_count, sizeof(int) * n, cudaMemcpyDeviceToHost),
+                   "D2H"));
+      for (int v : hc) maxc = std::max(maxc, v);
+    }
+    release(cand);
+    cap = ((int)(maxc * 1.2) + 31) / 32 * 32;
+    ETRY(alloc(&cand, (size_t)n * cap));
+  }
+  set_error("candidate list capacity did not converge");
+  return RBX_ERR_CAPACITY;
+}
+
+int rbx_engine::check_rebuild(bool disp_from_drift) {
+  if (!have_cache || prm.skin <= 0.0) return rebuild();
+  if (!disp_from_drift) {
+    ETRY(cuda_ok(cudaMemsetAsync(max_d2, 0, sizeof(unsigned long long), st), "memset"));
+    ETRY(launch_max_disp(dbox, n, x, y, z, x0, y0, z0, max_d2, st));
+  }
+  ETRY(cuda_ok(cudaMemcpyAsync(h_pinned, max_d2, sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, st),
+               "D2H"));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "skin check sync"));
+  double d2;
+  memcpy(&d2, h_pinned, sizeof(double));
+  const double thr = prm.skin * 0.5;
+  if (d2 > thr * thr) return rebuild();
+  return RBX_OK;
+}
+
+int rbx_engine::real_space() {
+  const bool mixed = prm.precision == RBX_MIXED;
+  if (prm.neighbor_type == RBX_NEIGHBOR_RBL) {
+    if (mixed)
+      return launch_rbl_fused_mixed(pp, ms, n, atoms, type, key_a, key_b, epoch, cand_count, cand,
+                                    cap, fpx, fpy, fpz, fpart, nfpart, st);
+    return launch_rbl_fused_f64(pp, n, x, y, z, q, type, key_a, key_b, epoch, cand_count, cand,
+                                cap, fpx, fpy, fpz, fpart, nfpart, st);
+  }
+  return launch_verlet_fused_f64(pp, n, x, y, z, q, type, cand_count, cand, cap, fpx, fpy, fpz,
+                                 nullptr, epart, nfpart, st);
+}
+
+int rbx_engine::kspace_and_combine(bool kick) {
+  const bool mixed = prm.precision == RBX_MIXED;
+  const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
+  if (P > 0) {
+    if (!k_injected) {
+      ETRY(cuda_ok(cudaMemsetAsync(dflags + 2, 0, sizeof(int), st), "memset"));
+      ETRY(launch_rbe_sample(P, sample_tables, tcnt, ttot, prm.random_seed, epoch, mx, my, mz,
+                             mixed ? mi : nullptr, dflags + 2, st));
+    }
+    if (mixed)
+      ETRY(launch_rbe_rho_partial_mixed(n, P, mi, atoms, part_re, part_im, nparts, st));
+    else
+      ETRY(launch_rbe_rho_partial_f64(dbox, n, P, mx, my, mz, q, x, y, z, part_re, part_im, nparts,
+                                      st));
+  }
+  ETRY(launch_rbe_finalize(dbox, P, P > 0 ? nparts : 0, part_re, part_im, mx, my, mz, prm.alpha,
+                           S, prm.qqr2e, qsq, qsum, P > 0 ? rho_re : nullptr, rho_im,
+                           P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr, rbl ? nfpart : 0,
+                           fpart, n, rbl ? mean : nullptr, st));
+  RbeForceOut o;
+  o.f_pair_x = fpx;
+  o.f_pair_y = fpy;
+  o.f_pair_z = fpz;
+  o.mean = rbl ? mean : nullptr;
+  o.f_out_x = fx;
+  o.f_out_y = fy;
+  o.f_out_z = fz;
+  if (keep_parts) {
+    o.fk_x = fkx;
+    o.fk_y = fky;
+    o.fk_z = fkz;
+  }
+  if (kick) {
+    o.vx = vx;
+    o.vy = vy;
+    o.vz = vz;
+    o.type = type;
+    o.inv_mass = inv_mass;
+    o.half_dt = 0.5 * prm.dt;
+  }
+  if (mixed)
+    ETRY(launch_rbe_force_mixed(n, P, tab, atoms, o, st));
+  else
+    ETRY(launch_rbe_force_f64(n, P, tab, q, x, y, z, o, st));
+  return RBX_OK;
+}
+
+int rbx_engine::compute_forces(int ep) {
+  cudaSetDevice(device);
+  epoch = ep;
+  ETRY(check_rebuild(false));
+  if (prm.precision == RBX_MIXED) ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
+  ETRY(real_space());
+  ETRY(kspace_and_combine(false));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "compute_forces sync"));
+  ETRY(check_sampler());
+  have_forces = true;
+  ++force_calls;
+  return RBX_OK;
+}
+
+int rbx_engine::check_sampler() {
+  if (P <= 0 || k_injected) return RBX_OK;
+  int h = 0;
+  ETRY(cuda_ok(cudaMemcpy(&h, dflags + 2, sizeof(int), cudaMemcpyDeviceToHost), "D2H"));
+  if (h) {
+    set_error("k-sampler: a sample needed more than 64 draws to avoid m = 0");
+    return RBX_ERR_SAMPLER;
+  }
+  return RBX_OK;
+}
+
+int rbx_engine::step(int nsteps) {
+  cudaSetDevice(device);
+  if (!have_forces) ETRY(compute_forces(epoch));
+  const bool mixed = prm.precision == RBX_MIXED;
+  for (int s = 0; s < nsteps; ++s) {
+    cudaEvent_t* e = nullptr;
+    if (profiling) {
+      if ((size_t)pev_used + 5 > pev.size()) ETRY(flush_profile());
+      while ((size_t)pev_used + 5 > pev.size()) {
+        cudaEvent_t t;
+        ETRY(cuda_ok(cudaEventCreate(&t), "cudaEventCreate"));
+        pev.push_back(t);
+      }
+      e = &pev[pev_used];
+      pev_used += 5;
+      cudaEventRecord(e[0], st);
+    }
+    ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
+    ETRY(cuda_ok(cudaMemsetAsync(max_d2, 0, sizeof(unsigned long long), st), "memset"));
+    ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2,
+                      mixed ? atoms : nullptr, q, st));
+    if (e) cudaEventRecord(e[1], st);
+    ++epoch;
+    ETRY(check_rebuild(true));
+    if (e) cudaEventRecord(e[2], st);
+    ETRY(real_space());
+    if (e) cudaEventRecord(e[3], st);
+    ETRY(kspace_and_combine(true));
+    if (e) cudaEventRecord(e[4], st);
+    ++steps;
+    ++force_calls;
+  }
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "step sync"));
+  if (profiling) ETRY(flush_profile());
+  ETRY(check_sampler());
+  return RBX_OK;
+}
+
+// Fold the recorded per-step phase events into the running totals.
+int rbx_engine::flush_profile() {
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "profile sync"));
+  for (int b = 0; b + 5 <= pev_used; b += 5) {
+    for (int k = 0; k < 4; ++k) {
+      float v = 0.f;
+      ETRY(cuda_ok(cudaEventElapsedTime(&v, pev[b + k], pev[b + k + 1]), "cudaEventElapsedTime"));
+      phase_total[k] += v;
+    }
+    ++phase_steps;
+  }
+  pev_used = 0;
+  return RBX_OK;
+}
+
+// Mean device time per profiled step and phase, in ms.
+int rbx_engine::phase_ms(float out[4]) {
+  if (phase_steps == 0) {
+    set_error("no profiled steps (enable rbx_engine_set_profiling, then step)");
+    return RBX_ERR_INVALID;
+  }
+  for (int k = 0; k < 4; ++k) out[k] = (float)(phase_total[k] / (double)phase_steps);
+  return RBX_OK;
+}
+
+int rbx_engine::get_state(double* hx, double* hy, double* hz, double* hvx, double* hvy,
+                          double* hvz, double* hfx, double* hfy, double* hfz) {
+  cudaSetDevice(device);
+  const double* src[] = {x, y, z, vx, vy, vz, fx, fy, fz};
+  double* dst[] = {hx, hy, hz, hvx, hvy, hvz, hfx, hfy, hfz};
+  for (int a = 0; a < 9; ++a) {
+    if (!dst[a]) continue;
+    ETRY(launch_scatter_f64(n, orig, src[a], stage + (size_t)a * n, st));
+  }
+  for (int a = 0; a < 9; ++a) {
+    if (!dst[a]) continue;
+    ETRY(cuda_ok(cudaMemcpyAsync(dst[a], stage + (size_t)a * n, sizeof(double) * n,
+                                 cudaMemcpyDeviceToHost, st),
+                 "D2H"));
+  }
+  return cuda_ok(cudaStreamSynchronize(st), "get_state sync");
+}
+
+int rbx_engine::step_host(const double* xin, const double* vin, double* xout, double* vout,
+                          double* fout) {
+  cudaSetDevice(device);
+  const size_t N = (size_t)n;
+  // x_in / v_in are [3][n] blocks (x,y,z then vx,vy,vz) in host order
+  ETRY(cuda_ok(cudaMemcpyAsync(stage, xin, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st),
+               "H2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(stage + 3 * N, vin, sizeof(double) * 3 * N, cudaMemcpyHostToDevice,
+                               st),
+               "H2D"));
+  double* dst[] = {x, y, z, vx, vy, vz};
+  for (int a = 0; a < 6; ++a) ETRY(launch_gather_f64(n, orig, stage + a * N, dst[a], st));
+  ETRY(step(1));
+  const double* src[] = {x, y, z, vx, vy, vz, fx, fy, fz};
+  for (int a = 0; a < 9; ++a) ETRY(launch_scatter_f64(n, orig, src[a], stage + a * N, st));
+  ETRY(cuda_ok(cudaMemcpyAsync(xout, stage, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st),
+               "D2H"));
+  ETRY(cuda_ok(cudaMemcpyAsync(vout, stage + 3 * N, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost,
+                               st),
+               "D2H"));
+  ETRY(cuda_ok(cudaMemcpyAsync(fout, stage + 6 * N, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost,
+                               st),
+               "D2H"));
+  return cuda_ok(cudaStreamSynchronize(st), "step_host sync");
+}
+
+int rbx_engine::get_force_parts(double* f_pair, double* f_kspace) {
+  cudaSetDevice(device);
+  if (!keep_parts) {
+    set_error("force parts are not kept; enable with rbx_engine_set_k_samples or a parity run");
+    return RBX_ERR_INVALID;
+  }
+  const size_t N = (size_t)n;
+  // pair part after mean removal: f_total - f_k
+  const double* src[] = {fx, fy, fz, fkx, fky, fkz};
+  for (int a = 0; a < 6; ++a) ETRY(launch_scatter_f64(n, orig, src[a], stage + a * N, st));
+  std::vector<double> h(6 * N);
+  ETRY(cuda_ok(cudaMemcpyAsync(h.data(), stage, sizeof(double) * 6 * N, cudaMemcpyDeviceToHost, st),
+               "D2H"));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "sync"));
+  for (size_t i = 0; i < N; ++i)
+    for (int d = 0; d < 3; ++d) {
+      const double fk = h[(3 + d) * N + i];
+      if (f_kspace) f_kspace[i * 3 + d] = fk;
+      if (f_pair) f_pair[i * 3 + d] = h[d * N + i] - fk;
+    }
+  return RBX_OK;
+}
+
+int rbx_engine::get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs,
+                              int64_t* n_shell) {
+  cudaSetDevice(device);
+  if (prm.neighbor_type != RBX_NEIGHBOR_RBL || !have_cache) {
+    set_error("no RBL lists: engine is not RBL or has not built its lists");
+    return RBX_ERR_INVALID;
+  }
+  int *cc = nullptr, *core = nullptr, *sc = nullptr, *shell = nullptr;
+  const size_t N = (size_t)n;
+  ETRY(dalloc(&cc, N));
+  ETRY(dalloc(&sc, N));
+  ETRY(dalloc(&core, N * cap));
+  ETRY(dalloc(&shell, N * cap));
+  int rc;
+  if (prm.precision == RBX_MIXED) {
+    rc = launch_to_fixed(dbox, n, x, y, z, q, atoms, st);
+    if (!rc)
+      rc = launch_rbl_lists_mixed(pp, ms, n, atoms, key_a, key_b, epoch, cand_count, cand, cap, cc,
+                                  core, sc, shell, st);
+  } else {
+    rc = launch_rbl_lists(pp, n, x, y, z, key_a, key_b, epoch, cand_count, cand, cap, cc, core, sc,
+                          shell, st);
+  }
+  std::vector<int> hcc(N), hsc(N), hcore(N * cap), hshell(N * cap), hgid(N);
+  if (!rc) {
+    cudaMemcpyAsync(hcc.data(), cc, sizeof(int) * N, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hsc.data(), sc, sizeof(int) * N, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hcore.data(), core, sizeof(int) * N * cap, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hshell.data(), shell, sizeof(int) * N * cap, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hgid.data(), gid, sizeof(int) * N, cudaMemcpyDeviceToHost, st);
+    rc = cuda_ok(cudaStreamSynchronize(st), "sync");
+  }
+  cudaFree(cc);
+  cudaFree(sc);
+  cudaFree(core);
+  cudaFree(shell);
+  if (rc) return rc;
+  int64_t tc = 0, ts = 0;
+  for (size_t i = 0; i < N; ++i) {
+    tc += hcc[i];
+    ts += hsc[i];
+  }
+  const int64_t capc = *n_core, caps = *n_shell;
+  *n_core = tc;
+  *n_shell = ts;
+  if (!core_pairs || !shell_pairs) return RBX_OK;  // size query
+  if (capc < tc || caps < ts) {
+    set_error("output arrays too small: need %lld core and %lld shell pairs", (long long)tc,
+              (long long)ts);
+    return RBX_ERR_INVALID;
+  }
+  int64_t a = 0, b = 0;
+  for (size_t i = 0; i < N; ++i) {
+    for (int t = 0; t < hcc[i]; ++t) {
+      core_pairs[2 * a] = hgid[i];
+      core_pairs[2 * a + 1] = hgid[hcore[i * cap + t]];
+      ++a;
+    }
+    for (int t = 0; t < hsc[i]; ++t) {
+      shell_pairs[2 * b] = hgid[i];
+      shell_pairs[2 * b + 1] = hgid[hshell[i * cap + t]];
+      ++b;
+    }
+  }
+  return RBX_OK;
+}
+
+int rbx_engine::set_k_samples(int p, const double* hmx, const double* hmy, const double* hmz) {
+  cudaSetDevice(device);
+  if (!hmx) {
+    k_injected = false;
+    return RBX_OK;
+  }
+  if (p != P) {
+    set_error("injected sample count %d differs from coulomb_sample_num %d", p, P);
+    return RBX_ERR_INVALID;
+  }
+  ETRY(cuda_ok(cudaMemcpyAsync(mx, hmx, sizeof(double) * p, cudaMemcpyHostToDevice, st), "H2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(my, hmy, sizeof(double) * p, cudaMemcpyHostToDevice, st), "H2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(mz, hmz, sizeof(double) * p, cudaMemcpyHostToDevice, st), "H2D"));
+  ETRY(launch_m_to_int(p, mx, my, mz, mi, st));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "sync"));
+  k_injected = true;
+  keep_parts = true;
+  return RBX_OK;
+}
+
+int rbx_engine::get_stats(rbx_stats* s) {
+  cudaSetDevice(device);
+  memset(s, 0, sizeof(*s));
+  s->steps = steps;
+  s->force_calls = force_calls;
+  s->rebuilds = rebuilds;
+  s->epoch = epoch;
+  s->selection_frequency = freq;
+  s->candidate_capacity = cap;
+  if (have_cache)
+    ETRY(cuda_ok(cudaMemcpy(&s->candidates, cand_total, sizeof(long long), cudaMemcpyDeviceToHost),
+                 "D2H"));
+  if (P > 0) {
+    ETRY(cuda_ok(cudaMemcpy(&s->e_kspace, ek, sizeof(double), cudaMemcpyDeviceToHost), "D2H"));
+    ETRY(cuda_ok(cudaMemcpy(s->virial_kspace, virk, sizeof(double) * 6, cudaMemcpyDeviceToHost),
+                 "D2H"));
+  }
+  return RBX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+rbx_engine* rbx_engine_create(const rbx_params* params, const rbx_box* box, int num_atoms,
+                              int device) {
+  if (!params || !box || num_atoms <= 0 || !params->sigma || !params->eps || !params->mass) {
+    set_error("rbx_engine_create: null params/box or num_atoms <= 0");
+    return nullptr;
+  }
+  rbx_engine* e = new rbx_engine();
+  e->prm = *params;
+  e->box = *box;
+  e->n = num_atoms;
+  e->device = device;
+  e->sigma.assign(params->sigma, params->sigma + params->ntypes);
+  e->eps.assign(params->eps, params->eps + params->ntypes);
+  e->mass.assign(params->mass, params->mass + params->ntypes);
+  e->prm.sigma = e->sigma.data();
+  e->prm.eps = e->eps.data();
+  e->prm.mass = e->mass.data();
+  if (e->init() != RBX_OK) {
+    delete e;
+    return nullptr;
+  }
+  return e;
+}
+
+void rbx_engine_destroy(rbx_engine* e) { delete e; }
+
+int rbx_engine_set_state(rbx_engine* e, const int* gid, const int* type, const double* charge,
+                         const double* px, const double* py, const double* pz, const double* vx,
+                         const double* vy, const double* vz) {
+  if (!e || !gid || !type || !charge || !px || !py || !pz || !vx || !vy || !vz) {
+    set_error("rbx_engine_set_state: null argument");
+    return RBX_ERR_INVALID;
+  }
+  return e->set_state(gid, type, charge, px, py, pz, vx, vy, vz);
+}
+
+int rbx_engine_set_k_samples(rbx_engine* e, int p, const double* mx, const double* my,
+                             const double* mz) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->set_k_samples(p, mx, my, mz);
+}
+
+int rbx_engine_compute_forces(rbx_engine* e, int epoch) {
+  if (!e) return RBX_ERR_INVALID;
+  e->keep_parts = true;
+  return e->compute_forces(epoch);
+}
+
+int rbx_engine_step(rbx_engine* e, int nsteps) {
+  if (!e || nsteps < 0) return RBX_ERR_INVALID;
+  return e->step(nsteps);
+}
+
+int rbx_engine_step_host(rbx_engine* e, const double* x_in, const double* v_in, double* x_out,
+                         double* v_out, double* f_out) {
+  if (!e || !x_in || !v_in || !x_out || !v_out || !f_out) {
+    set_error("rbx_engine_step_host: null argument");
+    return RBX_ERR_INVALID;
+  }
+  return e->step_host(x_in, v_in, x_out, v_out, f_out);
+}
+
+int rbx_engine_get_state(rbx_engine* e, double* px, double* py, double* pz, double* vx, double* vy,
+                         double* vz, double* fx, double* fy, double* fz) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->get_state(px, py, pz, vx, vy, vz, fx, fy, fz);
+}
+
+int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->get_force_parts(f_pair, f_kspace);
+}
+
+int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core, int* shell_pairs,
+                             int64_t* n_shell) {
+  if (!e || !n_core || !n_shell) return RBX_ERR_INVALID;
+  return e->get_rbl_pairs(core_pairs, n_core, shell_pairs, n_shell);
+}
+
+int rbx_engine_get_stats(rbx_engine* e, rbx_stats* out) {
+  if (!e || !out) return RBX_ERR_INVALID;
+  return e->get_stats(out);
+}
+
+void* rbx_engine_stream(rbx_engine* e) { return e ? (void*)e->st : nullptr; }
+
+int rbx_engine_phase_ms(rbx_engine* e, float out[4]) {
+  if (!e || !out) return RBX_ERR_INVALID;
+  return e->phase_ms(out);
+}
+
+int rbx_engine_set_profiling(rbx_engine* e, int on) {
+  if (!e) return RBX_ERR_INVALID;
+  e->profiling = on != 0;
+  for (int k = 0; k < 4; ++k) e->phase_total[k] = 0.0;
+  e->phase_steps = 0;
+  e->pev_used = 0;
+  return RBX_OK;
+}
+
+}  // extern "C"

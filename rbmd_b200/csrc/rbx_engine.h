@@ -1,0 +1,109 @@
+// rbx_engine.h -- engine state behind the opaque rbx_engine handle (internal).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "rbx.h"
+#include "rbx_kernels.h"
+
+struct rbx_engine {
+  // configuration
+  rbx_params prm{};
+  std::vector<double> sigma, eps, mass;
+  rbx_box box{};
+  rbx::DBox dbox{};
+  int n = 0;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int dims[3] = {0, 0, 0};
+  int ncell = 0;
+  int freq = 1;
+  rbx::DivTest div{};
+  int P = 0;
+  double S = 0.0, qsq = 0.0, qsum = 0.0;
+  rbx::PairParams pp{};
+  rbx::MixedScale ms{};
+
+  // per-atom device arrays, cell-sorted order
+  double *x = nullptr, *y = nullptr, *z = nullptr;
+  double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  double *fx = nullptr, *fy = nullptr, *fz = nullptr;     // total force
+  double *fpx = nullptr, *fpy = nullptr, *fpz = nullptr;  // real space (before mean removal)
+  double *fkx = nullptr, *fky = nullptr, *fkz = nullptr;  // k-space (kept on request)
+  double *q = nullptr, *x0 = nullptr, *y0 = nullptr, *z0 = nullptr;
+  int *type = nullptr, *gid = nullptr, *orig = nullptr;
+  unsigned long long *key_a = nullptr, *key_b = nullptr;
+  uint4* atoms = nullptr;  // mixed form: {ux, uy, uz, q_f32}
+  double* tmpd = nullptr;
+  int* tmpi = nullptr;
+  unsigned long long* tmpu = nullptr;
+  double* stage = nullptr;  // 9 n doubles for host transfers
+
+  // cells and candidate list
+  int *perm = nullptr, *cell_of_sorted = nullptr, *cell_start = nullptr;
+  void* cell_scratch = nullptr;
+  int cap = 0;
+  int *cand_count = nullptr, *cand = nullptr;
+
+  // reductions, flags
+  int nfpart = 0;
+  double *fpart = nullptr, *epart = nullptr, *mean = nullptr;
+  int* dflags = nullptr;  // [0] cell sort, [1] list overflow, [2] sampler
+  unsigned long long* max_d2 = nullptr;
+  double* inv_mass = nullptr;
+  double *lj_eps = nullptr, *lj_s6 = nullptr;
+  unsigned long long* h_pinned = nullptr;
+
+  // RBE
+  int nparts = 0;
+  double *mx = nullptr, *my = nullptr, *mz = nullptr;
+  int* mi = nullptr;
+  double *part_re = nullptr, *part_im = nullptr, *rho_re = nullptr, *rho_im = nullptr;
+  rbx::KTab* tab = nullptr;
+  double *ek = nullptr, *virk = nullptr;
+  double* sample_tables = nullptr;
+  int tcnt[3] = {0, 0, 0};
+  double ttot[3] = {0, 0, 0};
+
+  // bookkeeping
+  bool have_cache = false, have_forces = false, k_injected = false, keep_parts = false;
+  bool profiling = false;
+  int epoch = 0;
+  long long steps = 0, force_calls = 0, rebuilds = 0;
+  cudaEvent_t ev[8] = {};
+  // accumulated device time per phase while profiling is on
+  std::vector<cudaEvent_t> pev;  // 5 events per profiled step
+  int pev_used = 0;
+  double phase_total[4] = {0, 0, 0, 0};
+  long long phase_steps = 0;
+  long long* cand_total = nullptr;  // device: sum of candidate counts at the last rebuild
+  std::vector<void*> allocs;
+
+  ~rbx_engine();
+  int init();
+  int set_state(const int* gid, const int* type, const double* q, const double* x,
+                const double* y, const double* z, const double* vx, const double* vy,
+                const double* vz);
+  int set_k_samples(int p, const double* mx, const double* my, const double* mz);
+  int rebuild();
+  int check_rebuild(bool disp_from_drift);
+  int real_space();
+  int kspace_and_combine(bool kick);
+  int compute_forces(int epoch);
+  int check_sampler();
+  int step(int nsteps);
+  int step_host(const double* xin, const double* vin, double* xout, double* vout, double* fout);
+  int get_state(double* px, double* py, double* pz, double* vx, double* vy, double* vz,
+                double* fx, double* fy, double* fz);
+  int get_force_parts(double* f_pair, double* f_kspace);
+  int get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs, int64_t* n_shell);
+  int get_stats(rbx_stats* s);
+  int phase_ms(float out[4]);
+  int flush_profile();
+
+  template <typename T>
+  int alloc(T** p, size_t count);
+  template <typename T>
+  void release(T*& p);
+};

@@ -1,0 +1,171 @@
+// rbx_kernels.h -- host launchers of the sm_100a kernels (internal).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rbx_common.cuh"
+
+namespace rbx {
+
+// Per-k force table written by the finalize kernel.
+struct KTab {
+  double kx, ky, kz;
+  double a, b;  // coef * Re rho, coef * Im rho, coef = -4 pi qqr2e S / (P V k^2)
+  int m[4];     // integer m (mixed form)
+};
+
+// Destinations of the RBE force pass.
+struct RbeForceOut {
+  const double* f_pair_x = nullptr;  // add real-space force (combine), or null
+  const double* f_pair_y = nullptr;
+  const double* f_pair_z = nullptr;
+  const double* mean = nullptr;      // subtract this mean from the pair force
+  double* f_out_x = nullptr;
+  double* f_out_y = nullptr;
+  double* f_out_z = nullptr;
+  double* fk_x = nullptr;            // optional copy of the k-space force
+  double* fk_y = nullptr;
+  double* fk_z = nullptr;
+  double* vx = nullptr;              // optional half kick
+  double* vy = nullptr;
+  double* vz = nullptr;
+  const int* type = nullptr;
+  const double* inv_mass = nullptr;
+  double half_dt = 0.0;
+};
+
+// ---- k-space (rbx_rbe.cu) ----
+int rbe_partial_blocks(int n);
+int launch_rbe_rho_partial_f64(const DBox& b, int n, int p, const double* mx, const double* my,
+                               const double* mz, const double* q, const double* x,
+                               const double* y, const double* z, double* part_re,
+                               double* part_im, int nblocks, cudaStream_t st);
+int launch_rbe_rho_partial_mixed(int n, int p, const int* mi, const uint4* atoms,
+                                 double* part_re, double* part_im, int nblocks, cudaStream_t st);
+int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
+                        const double* part_im, const double* mx, const double* my,
+                        const double* mz, double alpha, double S, double qqr2e, double qsq,
+                        double qsum, double* rho_re, double* rho_im, double* energy,
+                        double* virial, KTab* tab, int mean_parts, const double* fpart,
+                        int n_atoms, double* mean_out, cudaStream_t st);
+int launch_rbe_force_f64(int n, int p, const KTab* tab, const double* q, const double* x,
+                         const double* y, const double* z, const RbeForceOut& out,
+                         cudaStream_t st);
+int launch_rbe_force_mixed(int n, int p, const KTab* tab, const uint4* atoms,
+                           const RbeForceOut& out, cudaStream_t st);
+int launch_rbe_sample(int p, const double* tables, const int cnt[3], const double tot[3],
+                      uint64_t seed, int64_t step, double* mx, double* my, double* mz, int* mi,
+                      int* status, cudaStream_t st);
+int launch_m_to_int(int p, const double* mx, const double* my, const double* mz, int* mi,
+                    cudaStream_t st);
+int launch_ewald(const DBox& b, int n, const int kmax[3], double alpha, double qqr2e,
+                 double qsq, const double* q, const double* x, const double* y, const double* z,
+                 double* re, double* im, double* kvec, double* fx, double* fy, double* fz,
+                 double* energy, cudaStream_t st);
+
+// Host-side sampler tables (order m = 0, +1, -1, ...), identical to the oracle's.
+int rbe_axis_table(double L, double alpha, double* w, int max_entries, double* total);
+
+// ---- real space (rbx_pair.cu) ----
+struct PairParams {
+  DBox box;
+  double rs2, rc2;            // force predicates: r_core^2, cut_off^2
+  double core2_list;          // list predicates: r_core^2 - EPS, cut_off^2 - EPS
+  double force2_list;
+  double alpha, sqrt_alpha, qqr2e;
+  int freq;                   // pice_num
+  DivTest div;
+  int ntypes;
+  const double* lj_eps;       // ntypes^2 eps_ij
+  const double* lj_s6;        // ntypes^2 sigma_ij^6
+};
+
+struct MixedScale {
+  double s[3];                // L_d / 2^32
+};
+
+// Fused RBL filter + pair force over a row-major candidate list.
+// fpart (nblocks x 3) receives per-block force sums for the mean removal.
+int rbl_fused_blocks(int n);
+int launch_rbl_fused_f64(const PairParams& pp, int n, const double* x, const double* y,
+                         const double* z, const double* q, const int* type,
+                         const unsigned long long* key_a, const unsigned long long* key_b,
+                         int epoch, const int* cand_count, const int* cand, int cap,
+                         double* fx, double* fy, double* fz, double* fpart, int nblocks,
+                         cudaStream_t st);
+int launch_rbl_fused_mixed(const PairParams& pp, const MixedScale& ms, int n, const uint4* atoms,
+                           const int* type, const unsigned long long* key_a,
+                           const unsigned long long* key_b, int epoch, const int* cand_count,
+                           const int* cand, int cap, double* fx, double* fy, double* fz,
+                           double* fpart, int nblocks, cudaStream_t st);
+// Verlet pair force over the candidate list, cut at cut_off (force predicate).
+int launch_verlet_fused_f64(const PairParams& pp, int n, const double* x, const double* y,
+                            const double* z, const double* q, const int* type,
+                            const int* cand_count, const int* cand, int cap, double* fx,
+                            double* fy, double* fz, double* fpart, double* epart, int nblocks,
+                            cudaStream_t st);
+// Emit RBL lists (engine debugging / parity): core and shell rows (cap stride).
+int launch_rbl_lists(const PairParams& pp, int n, const double* x, const double* y,
+                     const double* z, const unsigned long long* key_a,
+                     const unsigned long long* key_b, int epoch, const int* cand_count,
+                     const int* cand, int cap, int* core_count, int* core, int* shell_count,
+                     int* shell, cudaStream_t st);
+int launch_rbl_lists_mixed(const PairParams& pp, const MixedScale& ms, int n, const uint4* atoms,
+                           const unsigned long long* key_a, const unsigned long long* key_b,
+                           int epoch, const int* cand_count, const int* cand, int cap,
+                           int* core_count, int* core, int* shell_count, int* shell,
+                           cudaStream_t st);
+int launch_rbl_keys(int n, const int* gid, unsigned long long* key_a, unsigned long long* key_b,
+                    cudaStream_t st);
+// Drop-in ops with the reference layouts.
+int launch_ref_rbl_filter(double core2, double force2, int n, const int* gid, const double* x,
+                          const double* y, const double* z, const int* cstart, const int* cend,
+                          const int* cand, const int* core_cap, const int* core_start,
+                          int* core_end, int* core, int shell_cap, int* shell, int* shell_num,
+                          int* required, const DBox& b, int* realloc, const DivTest& div,
+                          int epoch, cudaStream_t st);
+int launch_ref_pair_rbl(const DBox& b, double rs, double rc, int n, int pice_num, double alpha,
+                        double qqr2e, const int* type, const double* sigma, const double* eps,
+                        const int* start, const int* end, const int* core, const int* shell,
+                        const int* shell_num, const double* q, const double* x, const double* y,
+                        const double* z, double* fx, double* fy, double* fz, cudaStream_t st);
+int launch_ref_pair_verlet(const DBox& b, double cut_off, int n, double alpha, double qqr2e,
+                           const int* type, const double* sigma, const double* eps,
+                           const int* start, const int* end, const int* nbrs, const double* q,
+                           const double* x, const double* y, const double* z, double* fx,
+                           double* fy, double* fz, double* flat_virial, double* epart,
+                           cudaStream_t st);
+int launch_sum_i32(int n, const int* src, long long* out, cudaStream_t st);
+int launch_reduce_cols(int n, int ncols, const double* cols, double* out, double scale,
+                       cudaStream_t st);
+int launch_sub_mean(int n, double* fx, double* fy, double* fz, const double* mean,
+                    cudaStream_t st);
+
+// ---- cells, lists, integration (rbx_cells.cu) ----
+int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, const double* y,
+                      const double* z, int* perm, int* cell_of_sorted, int* cell_start,
+                      void* scratch, int* status, cudaStream_t st);
+size_t cells_scratch_bytes(int n, int ncell);
+int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
+                     const double* y, const double* z, const int* cell_start, int cap,
+                     int* count, int* nbrs, int* overflow, cudaStream_t st);
+int launch_gather_f64(int n, const int* perm, const double* src, double* dst, cudaStream_t st);
+int launch_gather_i32(int n, const int* perm, const int* src, int* dst, cudaStream_t st);
+int launch_gather_u64(int n, const int* perm, const unsigned long long* src,
+                      unsigned long long* dst, cudaStream_t st);
+int launch_scatter_f64(int n, const int* idx, const double* src, double* dst, cudaStream_t st);
+int launch_kick(int n, const double* fx, const double* fy, const double* fz, const int* type,
+                const double* inv_mass, double half_dt, double* vx, double* vy, double* vz,
+                cudaStream_t st);
+// Drift + periodic wrap + max displacement since the last build (+ fixed point).
+int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* z,
+                 const double* vx, const double* vy, const double* vz, const double* x0,
+                 const double* y0, const double* z0, unsigned long long* max_d2_bits,
+                 uint4* atoms, const double* q, cudaStream_t st);
+int launch_to_fixed(const DBox& b, int n, const double* x, const double* y, const double* z,
+                    const double* q, uint4* atoms, cudaStream_t st);
+int launch_max_disp(const DBox& b, int n, const double* x, const double* y, const double* z,
+                    const double* x0, const double* y0, const double* z0,
+                    unsigned long long* max_d2_bits, cudaStream_t st);
+
+}  // namespace rbx

@@ -1,0 +1,874 @@
+// rbx_pair.cu -- real-space LJ 12-6 + erfc-Coulomb kernels for sm_100a.
+//
+// Engine path: one fused kernel per step reads the row-major candidate list
+// (cut_off + skin) once, classifies every candidate with the reference's FP64
+// list predicates (core r^2 < r_core^2 - EPS, shell r^2 < cut_off^2 - EPS,
+// SplitMix64 pair hash % freq == 0 -- FilterRBLNeighborCandidates,
+// src/neighbor_list/src/op/rocm/rbl_full_neighbor_list_op.hip.cu:237-304) and
+// evaluates the pair force of ComputeLJCutCoulRBLForce
+// (src/force/src/lj_cut_coul_kspace_op/rocm/lj_cut_coul_kspace_op.hip.cu:569-683)
+// without writing the core/shell lists to HBM.
+//
+// Mapping: one warp per atom i.  Lanes take 32 candidates at a time; pairs that
+// carry a force are compacted into a per-warp shared-memory queue, and the
+// force math runs on full 32-pair batches, so the branchy classification and
+// the expensive erfc/exp math do not diverge against each other.  Per-atom
+// force sums are warp-reduced; per-block force totals (fixed order) feed the
+// RBL mean-force removal.
+#include <math.h>
+
+#include "rbx_common.cuh"
+#include "rbx_kernels.h"
+
+namespace rbx {
+
+constexpr int PAIR_BLOCK = 256;
+constexpr int PAIR_WARPS = PAIR_BLOCK / 32;
+constexpr int QCAP = 64;
+constexpr int MAX_TYPES_SMEM = 16;  // ntypes^2 <= 256 pair entries in shared memory
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// LJ 12-6 force/r (lj126_rs, src/force/src/lj_op/rocm/lj_op.hip.cu:40-54) in FP64.
+__device__ __forceinline__ double lj_f64(double eps_ij, double s6, double d2) {
+  const double d6 = d2 * d2 * d2;
+  const double sd6 = s6 / d6;
+  return -24.0 * eps_ij * ((2.0 * sd6 - 1.0) * sd6) / d2;
+}
+// erfc-Coulomb force/r (CoulCutForce_rs_fix, lj_cut_coul_kspace_op.hip.cu:134-161).
+__device__ __forceinline__ double coul_f64(double alpha, double sqrt_alpha, double qqr2e,
+                                           double qq, double d2) {
+  const double dis = sqrt(d2);
+  const double g = erfc(sqrt_alpha * dis) / d2 +
+                   2.0 * sqrt_alpha * exp(-alpha * d2) / (1.7724538509055160273 * dis);
+  return -qqr2e * qq * g / dis;
+}
+__device__ __forceinline__ float lj_f32(float eps_ij, float s6, float d2) {
+  const float d6 = d2 * d2 * d2;
+  const float sd6 = s6 / d6;
+  return -24.f * eps_ij * ((2.f * sd6 - 1.f) * sd6) / d2;
+}
+__device__ __forceinline__ float coul_f32(float alpha, float sqrt_alpha, float qqr2e, float qq,
+                                          float d2) {
+  const float rinv = rsqrtf(d2);
+  const float dis = d2 * rinv;
+  const float g = erfcf(sqrt_alpha * dis) * (rinv * rinv) +
+                  (2.0f / 1.7724538509055160273f) * sqrt_alpha * expf(-alpha * d2) * rinv;
+  return -qqr2e * qq * g * rinv;
+}
+
+struct TypeTables {
+  double eps[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
+  double s6[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
+};
+
+__device__ __forceinline__ void load_type_tables(TypeTables& t, const PairParams& pp) {
+  const int nt2 = pp.ntypes * pp.ntypes;
+  for (int e = threadIdx.x; e < nt2; e += blockDim.x) {
+    t.eps[e] = pp.lj_eps[e];
+    t.s6[e] = pp.lj_s6[e];
+  }
+  __syncthreads();
+}
+
+// Block partial of the per-atom forces, accumulated by lane 0 of each warp in
+// atom order and combined over warps in warp order.
+__device__ __forceinline__ void write_block_partial(double (*s_acc)[3], double* fpart) {
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int w = 0; w < PAIR_WARPS; ++w) s += s_acc[w][threadIdx.x];
+    fpart[(size_t)blockIdx.x * 3 + threadIdx.x] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plain FP64 fused RBL kernel.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_rbl_fused_f64(PairParams pp, int n, const double* __restrict__ x, const double* __restrict__ y,
+                const double* __restrict__ z, const double* __restrict__ q,
+                const int* __restrict__ type, const unsigned long long* __restrict__ key_a,
+                const unsigned long long* __restrict__ key_b, int epoch,
+                const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
+                double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
+                double* __restrict__ fpart) {
+  __shared__ TypeTables tt;
+  __shared__ double s_dx[PAIR_WARPS][QCAP], s_dy[PAIR_WARPS][QCAP], s_dz[PAIR_WARPS][QCAP];
+  __shared__ int s_j[PAIR_WARPS][QCAP];
+  __shared__ double s_acc[PAIR_WARPS][3];
+  load_type_tables(tt, pp);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = lanemask_lt();
+  double acc0 = 0, acc1 = 0, acc2 = 0;
+  const int nt = pp.ntypes;
+  for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += gridDim.x * PAIR_WARPS) {
+    const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
+    const int ti = type[i];
+    const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
+    const int cnt = cand_count[i];
+    const int* row = cand + (size_t)i * cap;
+    int qn = 0;
+    double fxa = 0, fya = 0, fza = 0;
+    for (int k0 = 0;;) {
+      const bool more = k0 < cnt;
+      bool push = false;
+      int code = 0;
+      double dx = 0, dy = 0, dz = 0;
+      if (more) {
+        const int k = k0 + lane;
+        if (k < cnt) {
+          const int j = __ldg(row + k);
+          if (j != i) {
+            const double xj = __ldg(x + j), yj = __ldg(y + j), zj = __ldg(z + j);
+            // list predicate: i minus j, no FMA (CaculateDistance)
+            const double ex = min_image1(__dsub_rn(xi, xj), pp.box.len[0], pp.box.half[0]);
+            const double ey = min_image1(__dsub_rn(yi, yj), pp.box.len[1], pp.box.half[1]);
+            const double ez = min_image1(__dsub_rn(zi, zj), pp.box.len[2], pp.box.half[2]);
+            const double d2 =
+                __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+            if (d2 < pp.core2_list) {
+              push = d2 < pp.rs2 && d2 > RBX_EPSILON;  // lj126_rs / _rs_fix window
+              code = j;
+            } else if (d2 < pp.force2_list && d2 < pp.rc2 && d2 > pp.rs2) {
+              push = rbl_selected(ea, __ldg(key_b + j), pp.div);  // shell sample
+              code = j | (int)0x80000000;
+            }
+            dx = -ex;  // pair vector r_j - r_i (min image is odd in its argument)
+            dy = -ey;
+            dz = -ez;
+          }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, push);
+        if (push) {
+          const int pos = qn + __popc(m & lt);
+          s_dx[warp][pos] = dx;
+          s_dy[warp][pos] = dy;
+          s_dz[warp][pos] = dz;
+          s_j[warp][pos] = code;
+        }
+        qn += __popc(m);
+        k0 += 32;
+        __syncwarp();
+      }
+      // drain full batches, and the remainder after the last chunk
+      while (qn >= 32 || (!more && qn > 0)) {
+        if (lane < qn) {
+          const int c = s_j[warp][lane];
+          const int j = c & 0x7fffffff;
+          const double ddx = s_dx[warp][lane], ddy = s_dy[warp][lane], ddz = s_dz[warp][lane];
+          const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+          const int tj = __ldg(type + j);
+          const double qq = qi * __ldg(q + j);
+          double f = lj_f64(tt.eps[ti * nt + tj], tt.s6[ti * nt + tj], d2);
+          if (qq != 0.0) f += coul_f64(pp.alpha, pp.sqrt_alpha, pp.qqr2e, qq, d2);
+          if (c < 0) f *= (double)pp.freq;
+          fxa += f * ddx;
+          fya += f * ddy;
+          fza += f * ddz;
+        }
+        __syncwarp();
+        const int rem = qn > 32 ? qn - 32 : 0;
+        if (lane < rem) {
+          s_dx[warp][lane] = s_dx[warp][32 + lane];
+          s_dy[warp][lane] = s_dy[warp][32 + lane];
+          s_dz[warp][lane] = s_dz[warp][32 + lane];
+          s_j[warp][lane] = s_j[warp][32 + lane];
+        }
+        __syncwarp();
+        qn = rem;
+      }
+      if (!more) break;
+    }
+    fxa = warp_sum(fxa);
+    fya = warp_sum(fya);
+    fza = warp_sum(fza);
+    if (lane == 0) {
+      fx[i] = fxa;
+      fy[i] = fya;
+      fz[i] = fza;
+      acc0 += fxa;
+      acc1 += fya;
+      acc2 += fza;
+    }
+  }
+  if (lane == 0) {
+    s_acc[warp][0] = acc0;
+    s_acc[warp][1] = acc1;
+    s_acc[warp][2] = acc2;
+  }
+  if (fpart) write_block_partial(s_acc, fpart);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed fused RBL kernel: atoms as {ux, uy, uz, q_f32}; the pair vector is the
+// exact wrapped integer difference (exact minimum image); list and force
+// windows are decided in FP64 on that vector, the force math runs in FP32.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_rbl_fused_mixed(PairParams pp, MixedScale ms, int n, const uint4* __restrict__ atoms,
+                  const int* __restrict__ type, const unsigned long long* __restrict__ key_a,
+                  const unsigned long long* __restrict__ key_b, int epoch,
+                  const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
+                  double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
+                  double* __restrict__ fpart) {
+  __shared__ TypeTables tt;
+  __shared__ float s_dx[PAIR_WARPS][QCAP], s_dy[PAIR_WARPS][QCAP], s_dz[PAIR_WARPS][QCAP];
+  __shared__ int s_j[PAIR_WARPS][QCAP];
+  __shared__ double s_acc[PAIR_WARPS][3];
+  __shared__ float f_eps[MAX_TYPES_SMEM * MAX_TYPES_SMEM], f_s6[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
+  load_type_tables(tt, pp);
+  for (int e = threadIdx.x; e < pp.ntypes * pp.ntypes; e += blockDim.x) {
+    f_eps[e] = (float)tt.eps[e];
+    f_s6[e] = (float)tt.s6[e];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = lanemask_lt();
+  const float alpha = (float)pp.alpha, sqa = (float)pp.sqrt_alpha, qqr2e = (float)pp.qqr2e;
+  const float ffreq = (float)pp.freq;
+  double acc0 = 0, acc1 = 0, acc2 = 0;
+  const int nt = pp.ntypes;
+  for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += gridDim.x * PAIR_WARPS) {
+    const uint4 ai = atoms[i];
+    const float qi = __uint_as_float(ai.w);
+    const int ti = type[i];
+    const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
+    const int cnt = cand_count[i];
+    const int* row = cand + (size_t)i * cap;
+    int qn = 0;
+    float fxa = 0.f, fya = 0.f, fza = 0.f;
+    for (int k0 = 0;;) {
+      const bool more = k0 < cnt;
+      bool push = false;
+      int code = 0;
+      float dx = 0.f, dy = 0.f, dz = 0.f;
+      if (more) {
+        const int k = k0 + lane;
+        if (k < cnt) {
+          const int j = __ldg(row + k);
+          if (j != i) {
+            const uint4 aj = __ldg(atoms + j);
+            const double ex = (double)(int)(aj.x - ai.x) * ms.s[0];
+            const double ey = (double)(int)(aj.y - ai.y) * ms.s[1];
+            const double ez = (double)(int)(aj.z - ai.z) * ms.s[2];
+            const double d2 =
+                __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+            if (d2 < pp.core2_list) {
+              push = d2 < pp.rs2 && d2 > RBX_EPSILON;
+              code = j;
+            } else if (d2 < pp.force2_list && d2 < pp.rc2 && d2 > pp.rs2) {
+              push = rbl_selected(ea, __ldg(key_b + j), pp.div);
+              code = j | (int)0x80000000;
+            }
+            dx = (float)ex;
+            dy = (float)ey;
+            dz = (float)ez;
+          }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, push);
+        if (push) {
+          const int pos = qn + __popc(m & lt);
+          s_dx[warp][pos] = dx;
+          s_dy[warp][pos] = dy;
+          s_dz[warp][pos] = dz;
+          s_j[warp][pos] = code;
+        }
+        qn += __popc(m);
+        k0 += 32;
+        __syncwarp();
+      }
+      while (qn >= 32 || (!more && qn > 0)) {
+        if (lane < qn) {
+          const int c = s_j[warp][lane];
+          const int j = c & 0x7fffffff;
+          const float ddx = s_dx[warp][lane], ddy = s_dy[warp][lane], ddz = s_dz[warp][lane];
+          const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+          const int tj = __ldg(type + j);
+          const float qq = qi * __uint_as_float(__ldg(&atoms[j].w));
+          float f = lj_f32(f_eps[ti * nt + tj], f_s6[ti * nt + tj], d2);
+          if (qq != 0.f) f += coul_f32(alpha, sqa, qqr2e, qq, d2);
+          if (c < 0) f *= ffreq;
+          fxa = fmaf(f, ddx, fxa);
+          fya = fmaf(f, ddy, fya);
+          fza = fmaf(f, ddz, fza);
+        }
+        __syncwarp();
+        const int rem = qn > 32 ? qn - 32 : 0;
+        if (lane < rem) {
+          s_dx[warp][lane] = s_dx[warp][32 + lane];
+          s_dy[warp][lane] = s_dy[warp][32 + lane];
+          s_dz[warp][lane] = s_dz[warp][32 + lane];
+          s_j[warp][lane] = s_j[warp][32 + lane];
+        }
+        __syncwarp();
+        qn = rem;
+      }
+      if (!more) break;
+    }
+    const double gx = warp_sum((double)fxa), gy = warp_sum((double)fya), gz = warp_sum((double)fza);
+    if (lane == 0) {
+      fx[i] = gx;
+      fy[i] = gy;
+      fz[i] = gz;
+      acc0 += gx;
+      acc1 += gy;
+      acc2 += gz;
+    }
+  }
+  if (lane == 0) {
+    s_acc[warp][0] = acc0;
+    s_acc[warp][1] = acc1;
+    s_acc[warp][2] = acc2;
+  }
+  if (fpart) write_block_partial(s_acc, fpart);
+}
+
+// ---------------------------------------------------------------------------
+// Verlet fused FP64: LJ + erfc-Coulomb for r^2 < cut_off^2 over the candidate
+// list (ComputeLJCutCoulForce, lj_cut_coul_kspace_op.hip.cu:256-356), with
+// per-block energy and virial partials epart[block][8] =
+// {evdwl, ecoul, vxx, vyy, vzz, vxy, vxz, vyz} (ComputeVirial, lj_op.hip.cu:76-88).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_verlet_fused_f64(PairParams pp, int n, const double* __restrict__ x,
+                   const double* __restrict__ y, const double* __restrict__ z,
+                   const double* __restrict__ q, const int* __restrict__ type,
+                   const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
+                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
+                   double* __restrict__ fpart, double* __restrict__ epart) {
+  __shared__ TypeTables tt;
+  __shared__ double s_dx[PAIR_WARPS][QCAP], s_dy[PAIR_WARPS][QCAP], s_dz[PAIR_WARPS][QCAP];
+  __shared__ int s_j[PAIR_WARPS][QCAP];
+  __shared__ double s_acc[PAIR_WARPS][3];
+  __shared__ double s_e[PAIR_WARPS][8];
+  load_type_tables(tt, pp);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = lanemask_lt();
+  double acc0 = 0, acc1 = 0, acc2 = 0;
+  double eacc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int nt = pp.ntypes;
+  for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += gridDim.x * PAIR_WARPS) {
+    const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
+    const int ti = type[i];
+    const int cnt = cand_count[i];
+    const int* row = cand + (size_t)i * cap;
+    int qn = 0;
+    double fxa = 0, fya = 0, fza = 0;
+    double ea[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k0 = 0;;) {
+      const bool more = k0 < cnt;
+      if (more) {
+        bool push = false;
+        int j = 0;
+        double dx = 0, dy = 0, dz = 0;
+        const int k = k0 + lane;
+        if (k < cnt) {
+          j = __ldg(row + k);
+          if (j != i) {
+            dx = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
+            dy = min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
+            dz = min_image1(__ldg(z + j) - zi, pp.box.len[2], pp.box.half[2]);
+            const double d2 =
+                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            push = d2 < pp.rc2;
+          }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, push);
+        if (push) {
+          const int pos = qn + __popc(m & lt);
+          s_dx[warp][pos] = dx;
+          s_dy[warp][pos] = dy;
+          s_dz[warp][pos] = dz;
+          s_j[warp][pos] = j;
+        }
+        qn += __popc(m);
+        k0 += 32;
+        __syncwarp();
+      }
+      while (qn >= 32 || (!more && qn > 0)) {
+        if (lane < qn) {
+          const int j = s_j[warp][lane];
+          const double ddx = s_dx[warp][lane], ddy = s_dy[warp][lane], ddz = s_dz[warp][lane];
+          const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+          const int tj = __ldg(type + j);
+          const double qq = qi * __ldg(q + j);
+          const double e_ij = tt.eps[ti * nt + tj], s6 = tt.s6[ti * nt + tj];
+          const double d6 = d2 * d2 * d2;
+          const double sd6 = s6 / d6;
+          double f = -24.0 * e_ij * ((2.0 * sd6 - 1.0) * sd6) / d2;
+          ea[0] += 0.5 * (4.0 * e_ij * (s6 / d6 - 1.0) * sd6);
+          if (qq != 0.0) {
+            const double dis = sqrt(d2);
+            const double ec = erfc(pp.sqrt_alpha * dis);
+            const double g = ec / d2 + 2.0 * pp.sqrt_alpha * exp(-pp.alpha * d2) /
+                                           (1.7724538509055160273 * dis);
+            f += -pp.qqr2e * qq * g / dis;
+            ea[1] += pp.qqr2e * (0.5 * qq * ec / dis);
+          }
+          fxa += f * ddx;
+          fya += f * ddy;
+          fza += f * ddz;
+          ea[2] += -0.5 * ddx * ddx * f;
+          ea[3] += -0.5 * ddy * ddy * f;
+          ea[4] += -0.5 * ddz * ddz * f;
+          ea[5] += -0.5 * ddx * ddy * f;
+          ea[6] += -0.5 * ddx * ddz * f;
+          ea[7] += -0.5 * ddy * ddz * f;
+        }
+        __syncwarp();
+        const int rem = qn > 32 ? qn - 32 : 0;
+        if (lane < rem) {
+          s_dx[warp][lane] = s_dx[warp][32 + lane];
+          s_dy[warp][lane] = s_dy[warp][32 + lane];
+          s_dz[warp][lane] = s_dz[warp][32 + lane];
+          s_j[warp][lane] = s_j[warp][32 + lane];
+        }
+        __syncwarp();
+        qn = rem;
+      }
+      if (!more) break;
+    }
+    fxa = warp_sum(fxa);
+    fya = warp_sum(fya);
+    fza = warp_sum(fza);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) ea[c] = warp_sum(ea[c]);
+    if (lane == 0) {
+      fx[i] = fxa;
+      fy[i] = fya;
+      fz[i] = fza;
+      acc0 += fxa;
+      acc1 += fya;
+      acc2 += fza;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) eacc[c] += ea[c];
+    }
+  }
+  if (lane == 0) {
+    s_acc[warp][0] = acc0;
+    s_acc[warp][1] = acc1;
+    s_acc[warp][2] = acc2;
+    for (int c = 0; c < 8; ++c) s_e[warp][c] = eacc[c];
+  }
+  if (fpart) write_block_partial(s_acc, fpart);
+  if (epart) {
+    __syncthreads();
+    if (threadIdx.x < 8) {
+      double s = 0.0;
+      for (int w = 0; w < PAIR_WARPS; ++w) s += s_e[w][threadIdx.x];
+      epart[(size_t)blockIdx.x * 8 + threadIdx.x] = s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RBL list emitters (same classification as the fused kernels; rows of cap).
+// Thread per atom: used for parity checks and the drop-in list op, not per step.
+// ---------------------------------------------------------------------------
+__global__ void k_rbl_lists(PairParams pp, int n, const double* __restrict__ x,
+                            const double* __restrict__ y, const double* __restrict__ z,
+                            const unsigned long long* __restrict__ key_a,
+                            const unsigned long long* __restrict__ key_b, int epoch,
+                            const int* __restrict__ cand_count, const int* __restrict__ cand,
+                            int cap, int* __restrict__ core_count, int* __restrict__ core,
+                            int* __restrict__ shell_count, int* __restrict__ shell) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
+  int nc = 0, ns = 0;
+  for (int t = 0; t < cand_count[i]; ++t) {
+    const int j = cand[(size_t)i * cap + t];
+    if (j == i) continue;
+    const double d2 = dist2_list(pp.box, x[i], y[i], z[i], x[j], y[j], z[j]);
+    if (d2 < pp.core2_list)
+      core[(size_t)i * cap + nc++] = j;
+    else if (d2 < pp.force2_list && rbl_selected(ea, key_b[j], pp.div))
+      shell[(size_t)i * cap + ns++] = j;
+  }
+  core_count[i] = nc;
+  shell_count[i] = ns;
+}
+
+__global__ void k_rbl_lists_mixed(PairParams pp, MixedScale ms, int n,
+                                  const uint4* __restrict__ atoms,
+                                  const unsigned long long* __restrict__ key_a,
+                                  const unsigned long long* __restrict__ key_b, int epoch,
+                                  const int* __restrict__ cand_count,
+                                  const int* __restrict__ cand, int cap,
+                                  int* __restrict__ core_count, int* __restrict__ core,
+                                  int* __restrict__ shell_count, int* __restrict__ shell) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
+  const uint4 ai = atoms[i];
+  int nc = 0, ns = 0;
+  for (int t = 0; t < cand_count[i]; ++t) {
+    const int j = cand[(size_t)i * cap + t];
+    if (j == i) continue;
+    const uint4 aj = atoms[j];
+    const double ex = (double)(int)(aj.x - ai.x) * ms.s[0];
+    const double ey = (double)(int)(aj.y - ai.y) * ms.s[1];
+    const double ez = (double)(int)(aj.z - ai.z) * ms.s[2];
+    const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+    if (d2 < pp.core2_list)
+      core[(size_t)i * cap + nc++] = j;
+    else if (d2 < pp.force2_list && rbl_selected(ea, key_b[j], pp.div))
+      shell[(size_t)i * cap + ns++] = j;
+  }
+  core_count[i] = nc;
+  shell_count[i] = ns;
+}
+
+__global__ void k_rbl_keys(int n, const int* __restrict__ gid, unsigned long long* __restrict__ a,
+                           unsigned long long* __restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a[i] = rbl_key_a(gid[i]);
+  b[i] = rbl_key_b(gid[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Drop-in ops with the reference data layouts.
+// ---------------------------------------------------------------------------
+// FilterRBLNeighborCandidates semantics (rbl_full_neighbor_list_op.hip.cu:237-304).
+__global__ void k_ref_rbl_filter(double core2, double force2, int n, const int* __restrict__ gid,
+                                 const double* __restrict__ x, const double* __restrict__ y,
+                                 const double* __restrict__ z, const int* __restrict__ cstart,
+                                 const int* __restrict__ cend, const int* __restrict__ cand,
+                                 const int* __restrict__ core_cap,
+                                 const int* __restrict__ core_start, int* __restrict__ core_end,
+                                 int* __restrict__ core, int shell_cap, int* __restrict__ shell,
+                                 int* __restrict__ shell_num, int* __restrict__ required,
+                                 DBox b, int* __restrict__ realloc, DivTest div, int epoch) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long ea = rbl_key_a(gid[i]) ^ (unsigned long long)(long long)epoch;
+  int nc = 0, ns = 0;
+  const int out0 = core_start[i], ccap = core_cap[i];
+  for (int pos = cstart[i]; pos < cend[i]; ++pos) {
+    const int j = cand[pos];
+    if (j == i) continue;
+    const double d2 = dist2_list(b, x[i], y[i], z[i], x[j], y[j], z[j]);
+    if (d2 < core2) {
+      if (nc < ccap)
+        core[out0 + nc] = j;
+      else
+        atomicOr(realloc, 1);
+      ++nc;
+    } else if (d2 < force2 && rbl_selected(ea, rbl_key_b(gid[j]), div)) {
+      if (ns < shell_cap) shell[(size_t)ns * n + i] = j;
+      ++ns;
+    }
+  }
+  core_end[i] = out0 + (nc < ccap ? nc : ccap);
+  shell_num[i] = ns < shell_cap ? ns : shell_cap;
+  atomicMax(required, ns);
+}
+
+// LJCutCoulRBLForce semantics, warp per atom over core CSR + sample-major shell.
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_ref_pair_rbl(DBox b, double rs2, double rc2, int n, int pice, double alpha, double sqa,
+               double qqr2e, const int* __restrict__ type, const double* __restrict__ sigma,
+               const double* __restrict__ eps, const int* __restrict__ start,
+               const int* __restrict__ end, const int* __restrict__ core,
+               const int* __restrict__ shell, const int* __restrict__ shell_num,
+               const double* __restrict__ q, const double* __restrict__ x,
+               const double* __restrict__ y, const double* __restrict__ z,
+               double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
+  if (i >= n) return;
+  const int ti = type[i];
+  const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
+  const double si = sigma[ti], ei = eps[ti];
+  double s[3] = {0, 0, 0}, c[3] = {0, 0, 0};
+  const int a = start[i], e = end[i], ns = shell_num[i];
+  for (int t = a + lane; t < e; t += 32) {
+    const int j = core[t];
+    const double dx = min_image1(x[j] - xi, b.len[0], b.half[0]);
+    const double dy = min_image1(y[j] - yi, b.len[1], b.half[1]);
+    const double dz = min_image1(z[j] - zi, b.len[2], b.half[2]);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 < rs2 && d2 > RBX_EPSILON) {
+      const double sij = (si + sigma[type[j]]) / 2, eij = sqrt(ei * eps[type[j]]);
+      double f = lj_f64(eij, pow(sij, 6.0), d2);
+      const double qq = qi * q[j];
+      if (qq != 0.0) f += coul_f64(alpha, sqa, qqr2e, qq, d2);
+      s[0] += f * dx;
+      s[1] += f * dy;
+      s[2] += f * dz;
+    }
+  }
+  for (int t = lane; t < ns; t += 32) {
+    const int j = shell[(size_t)t * n + i];
+    const double dx = min_image1(x[j] - xi, b.len[0], b.half[0]);
+    const double dy = min_image1(y[j] - yi, b.len[1], b.half[1]);
+    const double dz = min_image1(z[j] - zi, b.len[2], b.half[2]);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 < rc2 && d2 > rs2) {
+      const double sij = (si + sigma[type[j]]) / 2, eij = sqrt(ei * eps[type[j]]);
+      double f = lj_f64(eij, pow(sij, 6.0), d2);
+      const double qq = qi * q[j];
+      if (qq != 0.0) f += coul_f64(alpha, sqa, qqr2e, qq, d2);
+      f *= (double)pice;
+      c[0] += f * dx;
+      c[1] += f * dy;
+      c[2] += f * dz;
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    s[d] = warp_sum(s[d]);
+    c[d] = warp_sum(c[d]);
+  }
+  if (lane == 0) {
+    fx[i] = s[0] + c[0];
+    fy[i] = s[1] + c[1];
+    fz[i] = s[2] + c[2];
+  }
+}
+
+// LJCutCoulForce semantics (Verlet), warp per atom, per-atom virial columns
+// and per-atom energies epart[2*n] for a deterministic reduction.
+__global__ void __launch_bounds__(PAIR_BLOCK)
+k_ref_pair_verlet(DBox b, double cut2, int n, double alpha, double sqa, double qqr2e,
+                  const int* __restrict__ type, const double* __restrict__ sigma,
+                  const double* __restrict__ eps, const int* __restrict__ start,
+                  const int* __restrict__ end, const int* __restrict__ nbrs,
+                  const double* __restrict__ q, const double* __restrict__ x,
+                  const double* __restrict__ y, const double* __restrict__ z,
+                  double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
+                  double* __restrict__ vir, double* __restrict__ epart) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
+  if (i >= n) return;
+  const int ti = type[i];
+  const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
+  double a[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int t = start[i] + lane; t < end[i]; t += 32) {
+    const int j = nbrs[t];
+    const double dx = min_image1(x[j] - xi, b.len[0], b.half[0]);
+    const double dy = min_image1(y[j] - yi, b.len[1], b.half[1]);
+    const double dz = min_image1(z[j] - zi, b.len[2], b.half[2]);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (!(d2 < cut2)) continue;
+    const double sij = (sigma[ti] + sigma[type[j]]) / 2, eij = sqrt(eps[ti] * eps[type[j]]);
+    const double s6 = pow(sij, 6.0), d6 = d2 * d2 * d2, sd6 = s6 / d6;
+    double f = -24 * eij * ((2 * sd6 - 1) * sd6) / d2;
+    a[3] += 0.5 * (4 * eij * (s6 / d6 - 1) * sd6);
+    const double qq = qi * q[j];
+    if (qq != 0.0) {
+      const double dis = sqrt(d2), ec = erfc(sqa * dis);
+      f += -qqr2e * qq * (ec / d2 + 2 * sqa * exp(-alpha * d2) / (1.7724538509055160273 * dis)) / dis;
+      a[4] += qqr2e * (0.5 * qq * ec / dis);
+    }
+    a[0] += f * dx;
+    a[1] += f * dy;
+    a[2] += f * dz;
+    a[5] += -0.5 * dx * dx * f;
+    a[6] += -0.5 * dy * dy * f;
+    a[7] += -0.5 * dz * dz * f;
+    a[8] += -0.5 * dx * dy * f;
+    a[9] += -0.5 * dx * dz * f;
+    a[10] += -0.5 * dy * dz * f;
+  }
+  for (int c = 0; c < 11; ++c) a[c] = warp_sum(a[c]);
+  if (lane == 0) {
+    fx[i] = a[0];
+    fy[i] = a[1];
+    fz[i] = a[2];
+    if (epart) {
+      epart[i] = a[3];
+      epart[(size_t)n + i] = a[4];
+    }
+    if (vir)
+      for (int c = 0; c < 6; ++c) vir[(size_t)c * n + i] = a[5 + c];
+  }
+}
+
+// Deterministic column sums: out[c] = scale * sum_i cols[c*n + i] (one block per column).
+__global__ void k_reduce_cols(int n, const double* __restrict__ cols, double* __restrict__ out,
+                              double scale) {
+  __shared__ double sh[8];
+  double s = 0.0;
+  const double* col = cols + (size_t)blockIdx.x * n;
+  for (int i = threadIdx.x; i < n; i += 256) s += col[i];
+  s = block_sum_det<256>(s, sh);
+  if (threadIdx.x == 0) out[blockIdx.x] = s * scale;
+}
+
+__global__ void k_sum_i32(int n, const int* __restrict__ src, long long* __restrict__ out) {
+  long long s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += src[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long*)out, (unsigned long long)s);
+}
+
+__global__ void k_sub_mean(int n, double* __restrict__ fx, double* __restrict__ fy,
+                           double* __restrict__ fz, const double* __restrict__ mean) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  fx[i] -= mean[0];
+  fy[i] -= mean[1];
+  fz[i] -= mean[2];
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+int rbl_fused_blocks(int n) {
+  const int target = sm_count() * 8;  // 8 resident 256-thread blocks per SM
+  int b = (n + PAIR_WARPS - 1) / PAIR_WARPS;
+  if (b > target) b = target;
+  return b < 1 ? 1 : b;
+}
+
+int launch_rbl_fused_f64(const PairParams& pp, int n, const double* x, const double* y,
+                         const double* z, const double* q, const int* type,
+                         const unsigned long long* key_a, const unsigned long long* key_b,
+                         int epoch, const int* cand_count, const int* cand, int cap,
+                         double* fx, double* fy, double* fz, double* fpart, int nblocks,
+                         cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_rbl_fused_f64<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, x, y, z, q, type, key_a, key_b, epoch,
+                                                  cand_count, cand, cap, fx, fy, fz, fpart);
+  count_launch();
+  return check_launch("rbl_fused_f64");
+}
+
+int launch_rbl_fused_mixed(const PairParams& pp, const MixedScale& ms, int n, const uint4* atoms,
+                           const int* type, const unsigned long long* key_a,
+                           const unsigned long long* key_b, int epoch, const int* cand_count,
+                           const int* cand, int cap, double* fx, double* fy, double* fz,
+                           double* fpart, int nblocks, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_rbl_fused_mixed<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, ms, n, atoms, type, key_a, key_b, epoch,
+                                                    cand_count, cand, cap, fx, fy, fz, fpart);
+  count_launch();
+  return check_launch("rbl_fused_mixed");
+}
+
+int launch_verlet_fused_f64(const PairParams& pp, int n, const double* x, const double* y,
+                            const double* z, const double* q, const int* type,
+                            const int* cand_count, const int* cand, int cap, double* fx,
+                            double* fy, double* fz, double* fpart, double* epart, int nblocks,
+                            cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_verlet_fused_f64<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, x, y, z, q, type, cand_count, cand,
+                                                     cap, fx, fy, fz, fpart, epart);
+  count_launch();
+  return check_launch("verlet_fused_f64");
+}
+
+int launch_rbl_lists(const PairParams& pp, int n, const double* x, const double* y,
+                     const double* z, const unsigned long long* key_a,
+                     const unsigned long long* key_b, int epoch, const int* cand_count,
+                     const int* cand, int cap, int* core_count, int* core, int* shell_count,
+                     int* shell, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_rbl_lists<<<(n + 127) / 128, 128, 0, st>>>(pp, n, x, y, z, key_a, key_b, epoch, cand_count,
+                                               cand, cap, core_count, core, shell_count, shell);
+  count_launch();
+  return check_launch("rbl_lists");
+}
+
+int launch_rbl_lists_mixed(const PairParams& pp, const MixedScale& ms, int n, const uint4* atoms,
+                           const unsigned long long* key_a, const unsigned long long* key_b,
+                           int epoch, const int* cand_count, const int* cand, int cap,
+                           int* core_count, int* core, int* shell_count, int* shell,
+                           cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_rbl_lists_mixed<<<(n + 127) / 128, 128, 0, st>>>(pp, ms, n, atoms, key_a, key_b, epoch,
+                                                     cand_count, cand, cap, core_count, core,
+                                                     shell_count, shell);
+  count_launch();
+  return check_launch("rbl_lists_mixed");
+}
+
+int launch_rbl_keys(int n, const int* gid, unsigned long long* key_a, unsigned long long* key_b,
+                    cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_rbl_keys<<<(n + 255) / 256, 256, 0, st>>>(n, gid, key_a, key_b);
+  count_launch();
+  return check_launch("rbl_keys");
+}
+
+int launch_ref_rbl_filter(double core2, double force2, int n, const int* gid, const double* x,
+                          const double* y, const double* z, const int* cstart, const int* cend,
+                          const int* cand, const int* core_cap, const int* core_start,
+                          int* core_end, int* core, int shell_cap, int* shell, int* shell_num,
+                          int* required, const DBox& b, int* realloc, const DivTest& div,
+                          int epoch, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_ref_rbl_filter<<<(n + 127) / 128, 128, 0, st>>>(core2, force2, n, gid, x, y, z, cstart, cend,
+                                                    cand, core_cap, core_start, core_end, core,
+                                                    shell_cap, shell, shell_num, required, b,
+                                                    realloc, div, epoch);
+  count_launch();
+  return check_launch("ref_rbl_filter");
+}
+
+int launch_ref_pair_rbl(const DBox& b, double rs, double rc, int n, int pice_num, double alpha,
+                        double qqr2e, const int* type, const double* sigma, const double* eps,
+                        const int* start, const int* end, const int* core, const int* shell,
+                        const int* shell_num, const double* q, const double* x, const double* y,
+                        const double* z, double* fx, double* fy, double* fz, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_ref_pair_rbl<<<(n + PAIR_WARPS - 1) / PAIR_WARPS, PAIR_BLOCK, 0, st>>>(
+      b, rs * rs, rc * rc, n, pice_num, alpha, sqrt(alpha), qqr2e, type, sigma, eps, start, end,
+      core, shell, shell_num, q, x, y, z, fx, fy, fz);
+  count_launch();
+  return check_launch("ref_pair_rbl");
+}
+
+int launch_ref_pair_verlet(const DBox& b, double cut_off, int n, double alpha, double qqr2e,
+                           const int* type, const double* sigma, const double* eps,
+                           const int* start, const int* end, const int* nbrs, const double* q,
+                           const double* x, const double* y, const double* z, double* fx,
+                           double* fy, double* fz, double* flat_virial, double* epart,
+                           cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_ref_pair_verlet<<<(n + PAIR_WARPS - 1) / PAIR_WARPS, PAIR_BLOCK, 0, st>>>(
+      b, cut_off * cut_off, n, alpha, sqrt(alpha), qqr2e, type, sigma, eps, start, end, nbrs, q,
+      x, y, z, fx, fy, fz, flat_virial, epart);
+  count_launch();
+  return check_launch("ref_pair_verlet");
+}
+
+int launch_reduce_cols(int n, int ncols, const double* cols, double* out, double scale,
+                       cudaStream_t st) {
+  if (ncols <= 0) return RBX_OK;
+  k_reduce_cols<<<ncols, 256, 0, st>>>(n, cols, out, scale);
+  count_launch();
+  return check_launch("reduce_cols");
+}
+
+int launch_sum_i32(int n, const int* src, long long* out, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_sum_i32<<<grid_for(n, 256, sm_count() * 4), 256, 0, st>>>(n, src, out);
+  count_launch();
+  return check_launch("sum_i32");
+}
+
+int launch_sub_mean(int n, double* fx, double* fy, double* fz, const double* mean,
+                    cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_sub_mean<<<(n + 255) / 256, 256, 0, st>>>(n, fx, fy, fz, mean);
+  count_launch();
+  return check_launch("sub_mean");
+}
+
+}  // namespace rbx

@@ -1,0 +1,680 @@
+// rbx_rbe.cu -- Random Batch Ewald k-space kernels for sm_100a.
+//
+// Work per step is 2 * N * P (atom, k) phase evaluations: one pass builds the
+// structure factors rho(k_p) = sum_j q_j exp(i k_p . r_j), one pass scatters
+// F_i = q_i sum_p c_p (cos(k_p.r_i) Im rho_p - sin(k_p.r_i) Re rho_p) k_p
+// (src/force/src/kspace_calculator_op/rocm/kspace_calculator_op.hip.cu:98-125,
+// 238-289, 678-738).  Both passes are SFU/issue bound, not HBM bound: the
+// 16-32 B/atom inputs stay in L2.
+//
+// Plain form: FP64 positions, FP64 sincos.
+// Mixed form: 32-bit fixed-point fractional coordinates u = frac((x-lo)/L)*2^32
+// so the phase m.u mod 2^32 is exact integer arithmetic; the angle goes to the
+// SFU (__sincosf) in FP32; per-thread FP32 partial sums are folded with a
+// TwoSum-compensated pair; the cross-block reduction, energy and virial are FP64.
+#include <math.h>
+
+#include "rbx_common.cuh"
+#include "rbx_kernels.h"
+
+namespace rbx {
+
+// ---------------------------------------------------------------------------
+// rho(k) partial sums: block (bx, by) covers atom chunk bx and k-group by.
+// A thread owns RBE_KPT k-vectors {kg*128 + lane + 32*t}; warps of the block
+// take disjoint atom sub-ranges; the block combines its warps in fixed order
+// and writes one partial per k.  No atomics: the result is deterministic.
+// ---------------------------------------------------------------------------
+constexpr int RBE_BLOCK = 256;
+constexpr int RBE_WARPS = RBE_BLOCK / 32;
+constexpr int RBE_KPT = 4;
+constexpr int RBE_KGROUP = 32 * RBE_KPT;  // k-slots per warp
+
+__global__ void __launch_bounds__(RBE_BLOCK)
+k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kzs,
+                      const double* __restrict__ mx, const double* __restrict__ my,
+                      const double* __restrict__ mz, const double* __restrict__ q,
+                      const double* __restrict__ x, const double* __restrict__ y,
+                      const double* __restrict__ z, double* __restrict__ part_re,
+                      double* __restrict__ part_im) {
+  __shared__ double s_re[RBE_WARPS][RBE_KGROUP];
+  __shared__ double s_im[RBE_WARPS][RBE_KGROUP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int kbase = blockIdx.y * RBE_KGROUP;
+  double kx[RBE_KPT], ky[RBE_KPT], kz[RBE_KPT], sr[RBE_KPT], si[RBE_KPT];
+#pragma unroll
+  for (int t = 0; t < RBE_KPT; ++t) {
+    const int k = kbase + lane + 32 * t;
+    const bool ok = k < p;
+    // k = 2 pi m / L, evaluated as (2 pi * m) / L like the reference.
+    kx[t] = ok ? (2 * RBX_PI * mx[k]) / kxs : 0.0;
+    ky[t] = ok ? (2 * RBX_PI * my[k]) / kys : 0.0;
+    kz[t] = ok ? (2 * RBX_PI * mz[k]) / kzs : 0.0;
+    sr[t] = 0.0;
+    si[t] = 0.0;
+  }
+  const int a0 = blockIdx.x * chunk;
+  const int a1 = min(n, a0 + chunk);
+  const int sub = (chunk + RBE_WARPS - 1) / RBE_WARPS;
+  const int w0 = a0 + warp * sub, w1 = min(a1, w0 + sub);
+  for (int j = w0; j < w1; ++j) {
+    const double xj = __ldg(x + j), yj = __ldg(y + j), zj = __ldg(z + j), qj = __ldg(q + j);
+#pragma unroll
+    for (int t = 0; t < RBE_KPT; ++t) {
+      const double dot = kx[t] * xj + ky[t] * yj + kz[t] * zj;
+      double s, c;
+      sincos(dot, &s, &c);
+      sr[t] += qj * c;
+      si[t] += qj * s;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < RBE_KPT; ++t) {
+    s_re[warp][lane + 32 * t] = sr[t];
+    s_im[warp][lane + 32 * t] = si[t];
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < RBE_KGROUP; s += RBE_BLOCK) {
+    const int k = kbase + s;
+    if (k >= p) continue;
+    double r = 0.0, im = 0.0;
+    for (int w = 0; w < RBE_WARPS; ++w) {
+      r += s_re[w][s];
+      im += s_im[w][s];
+    }
+    part_re[(size_t)blockIdx.x * p + k] = r;
+    part_im[(size_t)blockIdx.x * p + k] = im;
+  }
+}
+
+// TwoSum (Knuth): s + e == a + b exactly.
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = a + b;
+  const float bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+// Mixed form.  Atom record: {ux, uy, uz, float bits of q}.  Lanes own k-vectors
+// (integer m), atoms stream through the warp as broadcast loads.  Every
+// RBE_TILE atoms the plain FP32 tile sums are folded into a compensated
+// (hi, lo) pair.
+constexpr int RBE_TILE = 32;
+
+__global__ void __launch_bounds__(RBE_BLOCK)
+k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
+                        const uint4* __restrict__ atoms, double* __restrict__ part_re,
+                        double* __restrict__ part_im) {
+  __shared__ double s_re[RBE_WARPS][RBE_KGROUP];
+  __shared__ double s_im[RBE_WARPS][RBE_KGROUP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int kbase = blockIdx.y * RBE_KGROUP;
+  int m0[RBE_KPT], m1[RBE_KPT], m2[RBE_KPT];
+  float hr[RBE_KPT], lr[RBE_KPT], hi[RBE_KPT], li[RBE_KPT];
+#pragma unroll
+  for (int t = 0; t < RBE_KPT; ++t) {
+    const int k = kbase + lane + 32 * t;
+    const bool ok = k < p;
+    m0[t] = ok ? mi[3 * k] : 0;
+    m1[t] = ok ? mi[3 * k + 1] : 0;
+    m2[t] = ok ? mi[3 * k + 2] : 0;
+    hr[t] = lr[t] = hi[t] = li[t] = 0.f;
+  }
+  const float ang = (float)(2.0 * RBX_PI / 4294967296.0);
+  const int a0 = blockIdx.x * chunk;
+  const int a1 = min(n, a0 + chunk);
+  const int sub = (chunk + RBE_WARPS - 1) / RBE_WARPS;
+  const int w0 = a0 + warp * sub, w1 = min(a1, w0 + sub);
+  for (int jt = w0; jt < w1; jt += RBE_TILE) {
+    const int je = min(w1, jt + RBE_TILE);
+    float tr[RBE_KPT], ti[RBE_KPT];
+#pragma unroll
+    for (int t = 0; t < RBE_KPT; ++t) tr[t] = ti[t] = 0.f;
+    for (int j = jt; j < je; ++j) {
+      const uint4 a = __ldg(atoms + j);
+      const float qj = __uint_as_float(a.w);
+#pragma unroll
+      for (int t = 0; t < RBE_KPT; ++t) {
+        const unsigned ph = (unsigned)m0[t] * a.x + (unsigned)m1[t] * a.y + (unsigned)m2[t] * a.z;
+        float s, c;
+        __sincosf((float)(int)ph * ang, &s, &c);
+        tr[t] = fmaf(qj, c, tr[t]);
+        ti[t] = fmaf(qj, s, ti[t]);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < RBE_KPT; ++t) {
+      float s, e;
+      two_sum(hr[t], tr[t], s, e);
+      hr[t] = s;
+      lr[t] += e;
+      two_sum(hi[t], ti[t], s, e);
+      hi[t] = s;
+      li[t] += e;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < RBE_KPT; ++t) {
+    s_re[warp][lane + 32 * t] = (double)hr[t] + (double)lr[t];
+    s_im[warp][lane + 32 * t] = (double)hi[t] + (double)li[t];
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < RBE_KGROUP; s += RBE_BLOCK) {
+    const int k = kbase + s;
+    if (k >= p) continue;
+    double r = 0.0, im = 0.0;
+    for (int w = 0; w < RBE_WARPS; ++w) {
+      r += s_re[w][s];
+      im += s_im[w][s];
+    }
+    part_re[(size_t)blockIdx.x * p + k] = r;
+    part_im[(size_t)blockIdx.x * p + k] = im;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Finalize (one block): rho_p = sum over blocks in fixed order; optional
+// energy/virial (ComputeRBEVirial0, kspace_calculator_op.hip.cu:573-674) with a
+// deterministic tree; force table tab[p] = {kx, ky, kz, coef*Re, coef*Im} with
+// coef = -4 pi qqr2e S / (P V k^2); optional mean of a force partial array.
+// ---------------------------------------------------------------------------
+constexpr int FIN_BLOCK = 256;
+
+__global__ void __launch_bounds__(FIN_BLOCK)
+k_rbe_finalize(int p, int nparts, const double* __restrict__ part_re,
+               const double* __restrict__ part_im, const double* __restrict__ mx,
+               const double* __restrict__ my, const double* __restrict__ mz, double Lx,
+               double Ly, double Lz, double alpha, double S, double qqr2e, double qsq,
+               double qsum, double* __restrict__ rho_re, double* __restrict__ rho_im,
+               double* __restrict__ energy, double* __restrict__ virial,
+               KTab* __restrict__ tab, int mean_parts, const double* __restrict__ fpart,
+               double n_atoms, double* __restrict__ mean_out) {
+  __shared__ double sh[FIN_BLOCK / 32];
+  const double V = Lx * Ly * Lz;
+  const double coef = (2 * RBX_PI * S) / (p * V);
+  const double fcoef = -4 * RBX_PI * qqr2e * S / p;
+  double e = 0.0, w[6] = {0, 0, 0, 0, 0, 0};
+  for (int k = threadIdx.x; k < p; k += FIN_BLOCK) {
+    double r = 0.0, im = 0.0;
+    for (int b = 0; b < nparts; ++b) {
+      r += part_re[(size_t)b * p + k];
+      im += part_im[(size_t)b * p + k];
+    }
+    if (rho_re) {
+      rho_re[k] = r;
+      rho_im[k] = im;
+    }
+    const double kx = 2 * RBX_PI * mx[k] / Lx;
+    const double ky = 2 * RBX_PI * my[k] / Ly;
+    const double kz = 2 * RBX_PI * mz[k] / Lz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double rho2 = r * r + im * im;
+    const double base = coef * rho2 / k2;
+    e += base;
+    const double inner = (1.0 / (4 * alpha)) + (1.0 / k2);
+    w[0] += base * (1.0 - 2 * kx * kx * inner);
+    w[1] += base * (1.0 - 2 * ky * ky * inner);
+    w[2] += base * (1.0 - 2 * kz * kz * inner);
+    w[3] += base * (-2 * kx * ky * inner);
+    w[4] += base * (-2 * kx * kz * inner);
+    w[5] += base * (-2 * ky * kz * inner);
+    if (tab) {
+      const double c = fcoef / (V * k2);
+      KTab t;
+      t.kx = kx;
+      t.ky = ky;
+      t.kz = kz;
+      t.a = c * r;
+      t.b = c * im;
+      t.m[0] = (int)mx[k];
+      t.m[1] = (int)my[k];
+      t.m[2] = (int)mz[k];
+      t.m[3] = 0;
+      tab[k] = t;
+    }
+  }
+  if (energy) {
+    const double et = block_sum_det<FIN_BLOCK>(e, sh);
+    double wt[6];
+    for (int c = 0; c < 6; ++c) wt[c] = block_sum_det<FIN_BLOCK>(w[c], sh);
+    if (threadIdx.x == 0) {
+      const double MY_PIS = 1.77245385090551602729, MY_PI2 = 1.57079632679489661923;
+      const double etot = et - (sqrt(alpha) * qsq / MY_PIS + MY_PI2 * qsum * qsum / (alpha * V));
+      *energy = etot * qqr2e;
+      for (int c = 0; c < 6; ++c) virial[c] = wt[c] * qqr2e;
+    }
+  }
+  if (mean_out) {
+    for (int d = 0; d < 3; ++d) {
+      double s = 0.0;
+      for (int b = threadIdx.x; b < mean_parts; b += FIN_BLOCK) s += fpart[(size_t)b * 3 + d];
+      s = block_sum_det<FIN_BLOCK>(s, sh);
+      if (threadIdx.x == 0) mean_out[d] = s / n_atoms;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Force scatter.  Thread per atom; the k table is staged in shared memory.
+// Epilogue variants: plain store of F_k, or the fused combine
+// F = F_pair - mean + F_k with the second velocity-Verlet half kick.
+// ---------------------------------------------------------------------------
+constexpr int FRC_BLOCK = 256;
+constexpr int FRC_TABLE = 512;  // k entries staged per pass
+
+struct ForceEpilogue {
+  const double* f_pair_x;  // may be null: store F_k only
+  const double* f_pair_y;
+  const double* f_pair_z;
+  const double* mean;      // may be null
+  double* f_out_x;         // total (or k-space only)
+  double* f_out_y;
+  double* f_out_z;
+  double* fk_x;            // optional copy of the k-space part
+  double* fk_y;
+  double* fk_z;
+  double* vx;              // optional half kick
+  double* vy;
+  double* vz;
+  const int* type;
+  const double* inv_mass;  // per type
+  double half_dt;
+};
+
+__device__ __forceinline__ void force_epilogue(const ForceEpilogue& ep, int i, double fx,
+                                               double fy, double fz) {
+  if (ep.fk_x) {
+    ep.fk_x[i] = fx;
+    ep.fk_y[i] = fy;
+    ep.fk_z[i] = fz;
+  }
+  if (ep.f_pair_x) {
+    double mx = 0, my = 0, mz = 0;
+    if (ep.mean) {
+      mx = ep.mean[0];
+      my = ep.mean[1];
+      mz = ep.mean[2];
+    }
+    fx += ep.f_pair_x[i] - mx;
+    fy += ep.f_pair_y[i] - my;
+    fz += ep.f_pair_z[i] - mz;
+  }
+  ep.f_out_x[i] = fx;
+  ep.f_out_y[i] = fy;
+  ep.f_out_z[i] = fz;
+  if (ep.vx) {
+    const double im = ep.inv_mass[ep.type[i]] * ep.half_dt;
+    ep.vx[i] += fx * im;
+    ep.vy[i] += fy * im;
+    ep.vz[i] += fz * im;
+  }
+}
+
+__global__ void __launch_bounds__(FRC_BLOCK)
+k_rbe_force_f64(int n, int p, const KTab* __restrict__ tab, const double* __restrict__ q,
+                const double* __restrict__ x, const double* __restrict__ y,
+                const double* __restrict__ z, ForceEpilogue ep) {
+  __shared__ KTab s_tab[FRC_TABLE];
+  const int i = blockIdx.x * FRC_BLOCK + threadIdx.x;
+  const bool live = i < n;
+  const double xi = live ? x[i] : 0.0, yi = live ? y[i] : 0.0, zi = live ? z[i] : 0.0;
+  double fx = 0, fy = 0, fz = 0;
+  for (int k0 = 0; k0 < p; k0 += FRC_TABLE) {
+    const int kn = min(FRC_TABLE, p - k0);
+    __syncthreads();
+    for (int s = threadIdx.x; s < kn; s += FRC_BLOCK) s_tab[s] = tab[k0 + s];
+    __syncthreads();
+    if (live) {
+      for (int s = 0; s < kn; ++s) {
+        const KTab t = s_tab[s];
+        const double dot = t.kx * xi + t.ky * yi + t.kz * zi;
+        double sn, cs;
+        sincos(dot, &sn, &cs);
+        const double f = cs * t.b - sn * t.a;
+        fx += f * t.kx;
+        fy += f * t.ky;
+        fz += f * t.kz;
+      }
+    }
+  }
+  if (live) {
+    const double qi = q[i];
+    force_epilogue(ep, i, fx * qi, fy * qi, fz * qi);
+  }
+}
+
+// Mixed-form force table entry (FP32 coefficients, integer m).
+struct KTabF {
+  int m0, m1, m2;
+  float a, b, kx, ky, kz;
+};
+
+__global__ void __launch_bounds__(FRC_BLOCK)
+k_rbe_force_mixed(int n, int p, const KTab* __restrict__ tab, const uint4* __restrict__ atoms,
+                  ForceEpilogue ep) {
+  __shared__ KTabF s_tab[FRC_TABLE];
+  const int i = blockIdx.x * FRC_BLOCK + threadIdx.x;
+  const bool live = i < n;
+  const uint4 a = live ? atoms[i] : make_uint4(0, 0, 0, 0);
+  const float ang = (float)(2.0 * RBX_PI / 4294967296.0);
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  for (int k0 = 0; k0 < p; k0 += FRC_TABLE) {
+    const int kn = min(FRC_TABLE, p - k0);
+    __syncthreads();
+    for (int s = threadIdx.x; s < kn; s += FRC_BLOCK) {
+      const KTab t = tab[k0 + s];
+      KTabF f;
+      f.m0 = t.m[0];
+      f.m1 = t.m[1];
+      f.m2 = t.m[2];
+      f.a = (float)t.a;
+      f.b = (float)t.b;
+      f.kx = (float)t.kx;
+      f.ky = (float)t.ky;
+      f.kz = (float)t.kz;
+      s_tab[s] = f;
+    }
+    __syncthreads();
+    if (live) {
+      for (int s = 0; s < kn; ++s) {
+        const KTabF t = s_tab[s];
+        const unsigned ph = (unsigned)t.m0 * a.x + (unsigned)t.m1 * a.y + (unsigned)t.m2 * a.z;
+        float sn, cs;
+        __sincosf((float)(int)ph * ang, &sn, &cs);
+        const float f = cs * t.b - sn * t.a;
+        fx = fmaf(f, t.kx, fx);
+        fy = fmaf(f, t.ky, fy);
+        fz = fmaf(f, t.kz, fz);
+      }
+    }
+  }
+  if (live) {
+    const double qi = (double)__uint_as_float(a.w);
+    force_epilogue(ep, i, (double)fx * qi, (double)fy * qi, (double)fz * qi);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Philox k-sampler: one thread per sample; per-axis inverse-CDF tables built
+// on the host (order m = 0, +1, -1, +2, -2, ...).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int table_pick(const double* w, int cnt, double total, uint64_t u53) {
+  const double target = (double)u53 * (1.0 / 9007199254740992.0) * total;
+  double acc = 0.0;
+  int idx = cnt - 1;
+  for (int t = 0; t < cnt; ++t) {
+    acc = __dadd_rn(acc, w[t]);
+    if (target < acc) {
+      idx = t;
+      break;
+    }
+  }
+  if (idx == 0) return 0;
+  return (idx & 1) ? (idx + 1) / 2 : -(idx / 2);
+}
+
+__global__ void k_rbe_sample(int p, const double* __restrict__ tables, int c0, int c1, int c2,
+                             double t0, double t1, double t2, uint32_t key0, uint32_t key1,
+                             uint64_t step, double* __restrict__ mx, double* __restrict__ my,
+                             double* __restrict__ mz, int* __restrict__ mi,
+                             int* __restrict__ status) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= p) return;
+  const double* w0 = tables;
+  const double* w1 = tables + c0;
+  const double* w2 = tables + c0 + c1;
+  for (int a = 0; a < 64; ++a) {
+    uint32_t o[8];
+    uint32_t c[4] = {(uint32_t)s, (uint32_t)(2 * a), (uint32_t)step, (uint32_t)(step >> 32)};
+    philox4x32_10(c, key0, key1);
+    o[0] = c[0];
+    o[1] = c[1];
+    o[2] = c[2];
+    o[3] = c[3];
+    uint32_t d[4] = {(uint32_t)s, (uint32_t)(2 * a + 1), (uint32_t)step, (uint32_t)(step >> 32)};
+    philox4x32_10(d, key0, key1);
+    o[4] = d[0];
+    o[5] = d[1];
+    o[6] = d[2];
+    o[7] = d[3];
+    const int m0 = table_pick(w0, c0, t0, ((((uint64_t)o[0]) << 32) | o[1]) >> 11);
+    const int m1 = table_pick(w1, c1, t1, ((((uint64_t)o[2]) << 32) | o[3]) >> 11);
+    const int m2 = table_pick(w2, c2, t2, ((((uint64_t)o[4]) << 32) | o[5]) >> 11);
+    if (m0 != 0 || m1 != 0 || m2 != 0) {
+      if (mx) {
+        mx[s] = m0;
+        my[s] = m1;
+        mz[s] = m2;
+      }
+      if (mi) {
+        mi[3 * s] = m0;
+        mi[3 * s + 1] = m1;
+        mi[3 * s + 2] = m2;
+      }
+      return;
+    }
+  }
+  atomicOr(status, 1);
+}
+
+// Integer copy of injected samples (for the mixed kernels).
+__global__ void k_m_to_int(int p, const double* __restrict__ mx, const double* __restrict__ my,
+                           const double* __restrict__ mz, int* __restrict__ mi) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= p) return;
+  mi[3 * s] = (int)mx[s];
+  mi[3 * s + 1] = (int)my[s];
+  mi[3 * s + 2] = (int)mz[s];
+}
+
+// ---------------------------------------------------------------------------
+// Exact Ewald over the kmax box (oracle support / statistical reference).
+// ---------------------------------------------------------------------------
+__global__ void k_ewald_rho(int n, int nk, int kx_max, int ky_max, int kz_max, double Lx,
+                            double Ly, double Lz, const double* __restrict__ q,
+                            const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, double* __restrict__ re,
+                            double* __restrict__ im, double* __restrict__ kvec) {
+  __shared__ double sh[FIN_BLOCK / 32];
+  const int k = blockIdx.x;
+  // k index -> (i, j, l) in ExecuteOnKmax order, skipping the origin.
+  const int ny = 2 * ky_max + 1, nz = 2 * kz_max + 1;
+  const int center = kx_max * ny * nz + ky_max * nz + kz_max;
+  const int flat = k < center ? k : k + 1;
+  const int ii = flat / (ny * nz) - kx_max;
+  const int jj = (flat / nz) % ny - ky_max;
+  const int ll = flat % nz - kz_max;
+  const double kx = 2 * RBX_PI * ii / Lx, ky = 2 * RBX_PI * jj / Ly, kz = 2 * RBX_PI * ll / Lz;
+  double sr = 0, si = 0;
+  for (int j = threadIdx.x; j < n; j += FIN_BLOCK) {
+    double s, c;
+    sincos(kx * x[j] + ky * y[j] + kz * z[j], &s, &c);
+    sr += q[j] * c;
+    si += q[j] * s;
+  }
+  sr = block_sum_det<FIN_BLOCK>(sr, sh);
+  si = block_sum_det<FIN_BLOCK>(si, sh);
+  if (threadIdx.x == 0) {
+    re[k] = sr;
+    im[k] = si;
+    kvec[3 * k] = kx;
+    kvec[3 * k + 1] = ky;
+    kvec[3 * k + 2] = kz;
+  }
+}
+
+__global__ void k_ewald_force(int n, int nk, double V, double alpha, double qqr2e,
+                              const double* __restrict__ kvec, const double* __restrict__ re,
+                              const double* __restrict__ im, const double* __restrict__ q,
+                              const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, double* __restrict__ fx,
+                              double* __restrict__ fy, double* __restrict__ fz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double base = -4.0 * RBX_PI * q[i];
+  const double ainv = 1.0 / alpha;
+  double sx = 0, sy = 0, sz = 0;
+  for (int k = 0; k < nk; ++k) {
+    const double kx = kvec[3 * k], ky = kvec[3 * k + 1], kz = kvec[3 * k + 2];
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    double s, c;
+    sincos(-(kx * x[i] + ky * y[i] + kz * z[i]), &s, &c);
+    double f = base / (V * k2) * exp(-0.25 * k2 * ainv) * (c * im[k] + s * re[k]);
+    f *= qqr2e;
+    sx += f * kx;
+    sy += f * ky;
+    sz += f * kz;
+  }
+  fx[i] = sx;
+  fy[i] = sy;
+  fz[i] = sz;
+}
+
+__global__ void k_ewald_energy(int nk, double V, double alpha, double qqr2e, double qsq,
+                               const double* __restrict__ kvec, const double* __restrict__ re,
+                               const double* __restrict__ im, double* __restrict__ energy) {
+  __shared__ double sh[FIN_BLOCK / 32];
+  double e = 0;
+  for (int k = threadIdx.x; k < nk; k += FIN_BLOCK) {
+    const double kx = kvec[3 * k], ky = kvec[3 * k + 1], kz = kvec[3 * k + 2];
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    e += exp(-0.25 * k2 / alpha) / k2 * (re[k] * re[k] + im[k] * im[k]);
+  }
+  e = block_sum_det<FIN_BLOCK>(e, sh);
+  if (threadIdx.x == 0) *energy = qqr2e * (2 * RBX_PI / V) * e + qqr2e * (-sqrt(alpha / RBX_PI) * qsq);
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+int rbe_partial_blocks(int n) {
+  // about four waves of 256-thread blocks on the 148 SMs, at least 64 atoms each
+  const int target = sm_count() * 4;
+  int blocks = (n + 63) / 64;
+  if (blocks > target) blocks = target;
+  return blocks < 1 ? 1 : blocks;
+}
+
+int launch_rbe_rho_partial_f64(const DBox& b, int n, int p, const double* mx, const double* my,
+                               const double* mz, const double* q, const double* x,
+                               const double* y, const double* z, double* part_re,
+                               double* part_im, int nblocks, cudaStream_t st) {
+  if (n <= 0 || p <= 0) return RBX_OK;
+  const int chunk = (n + nblocks - 1) / nblocks;
+  dim3 grid(nblocks, (p + RBE_KGROUP - 1) / RBE_KGROUP);
+  k_rbe_rho_partial_f64<<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, b.len[0], b.len[1], b.len[2],
+                                                    mx, my, mz, q, x, y, z, part_re, part_im);
+  count_launch();
+  return check_launch("rbe_rho_partial_f64");
+}
+
+int launch_rbe_rho_partial_mixed(int n, int p, const int* mi, const uint4* atoms,
+                                 double* part_re, double* part_im, int nblocks, cudaStream_t st) {
+  if (n <= 0 || p <= 0) return RBX_OK;
+  const int chunk = (n + nblocks - 1) / nblocks;
+  dim3 grid(nblocks, (p + RBE_KGROUP - 1) / RBE_KGROUP);
+  k_rbe_rho_partial_mixed<<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, mi, atoms, part_re, part_im);
+  count_launch();
+  return check_launch("rbe_rho_partial_mixed");
+}
+
+int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
+                        const double* part_im, const double* mx, const double* my,
+                        const double* mz, double alpha, double S, double qqr2e, double qsq,
+                        double qsum, double* rho_re, double* rho_im, double* energy,
+                        double* virial, KTab* tab, int mean_parts, const double* fpart,
+                        int n_atoms, double* mean_out, cudaStream_t st) {
+  k_rbe_finalize<<<1, FIN_BLOCK, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
+                                          b.len[1], b.len[2], alpha, S, qqr2e, qsq, qsum, rho_re,
+                                          rho_im, energy, virial, tab, mean_parts, fpart,
+                                          (double)n_atoms, mean_out);
+  count_launch();
+  return check_launch("rbe_finalize");
+}
+
+static ForceEpilogue make_ep(const RbeForceOut& o) {
+  ForceEpilogue ep;
+  ep.f_pair_x = o.f_pair_x;
+  ep.f_pair_y = o.f_pair_y;
+  ep.f_pair_z = o.f_pair_z;
+  ep.mean = o.mean;
+  ep.f_out_x = o.f_out_x;
+  ep.f_out_y = o.f_out_y;
+  ep.f_out_z = o.f_out_z;
+  ep.fk_x = o.fk_x;
+  ep.fk_y = o.fk_y;
+  ep.fk_z = o.fk_z;
+  ep.vx = o.vx;
+  ep.vy = o.vy;
+  ep.vz = o.vz;
+  ep.type = o.type;
+  ep.inv_mass = o.inv_mass;
+  ep.half_dt = o.half_dt;
+  return ep;
+}
+
+int launch_rbe_force_f64(int n, int p, const KTab* tab, const double* q, const double* x,
+                         const double* y, const double* z, const RbeForceOut& out,
+                         cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_rbe_force_f64<<<(n + FRC_BLOCK - 1) / FRC_BLOCK, FRC_BLOCK, 0, st>>>(n, p, tab, q, x, y, z,
+                                                                         make_ep(out));
+  count_launch();
+  return check_launch("rbe_force_f64");
+}
+
+int launch_rbe_force_mixed(int n, int p, const KTab* tab, const uint4* atoms,
+                           const RbeForceOut& out, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_rbe_force_mixed<<<(n + FRC_BLOCK - 1) / FRC_BLOCK, FRC_BLOCK, 0, st>>>(n, p, tab, atoms,
+                                                                           make_ep(out));
+  count_launch();
+  return check_launch("rbe_force_mixed");
+}
+
+int launch_rbe_sample(int p, const double* tables, const int cnt[3], const double tot[3],
+                      uint64_t seed, int64_t step, double* mx, double* my, double* mz, int* mi,
+                      int* status, cudaStream_t st) {
+  if (p <= 0) return RBX_OK;
+  k_rbe_sample<<<(p + 127) / 128, 128, 0, st>>>(p, tables, cnt[0], cnt[1], cnt[2], tot[0], tot[1],
+                                                tot[2], (uint32_t)seed, (uint32_t)(seed >> 32),
+                                                (uint64_t)step, mx, my, mz, mi, status);
+  count_launch();
+  return check_launch("rbe_sample");
+}
+
+int launch_m_to_int(int p, const double* mx, const double* my, const double* mz, int* mi,
+                    cudaStream_t st) {
+  if (p <= 0) return RBX_OK;
+  k_m_to_int<<<(p + 127) / 128, 128, 0, st>>>(p, mx, my, mz, mi);
+  count_launch();
+  return check_launch("m_to_int");
+}
+
+int launch_ewald(const DBox& b, int n, const int kmax[3], double alpha, double qqr2e,
+                 double qsq, const double* q, const double* x, const double* y, const double* z,
+                 double* re, double* im, double* kvec, double* fx, double* fy, double* fz,
+                 double* energy, cudaStream_t st) {
+  const int nk = (2 * kmax[0] + 1) * (2 * kmax[1] + 1) * (2 * kmax[2] + 1) - 1;
+  if (nk <= 0) return RBX_OK;
+  k_ewald_rho<<<nk, FIN_BLOCK, 0, st>>>(n, nk, kmax[0], kmax[1], kmax[2], b.len[0], b.len[1],
+                                        b.len[2], q, x, y, z, re, im, kvec);
+  count_launch();
+  int rc = check_launch("ewald_rho");
+  if (rc) return rc;
+  const double V = b.len[0] * b.len[1] * b.len[2];
+  if (n > 0) {
+    k_ewald_force<<<(n + 127) / 128, 128, 0, st>>>(n, nk, V, alpha, qqr2e, kvec, re, im, q, x, y,
+                                                   z, fx, fy, fz);
+    count_launch();
+    rc = check_launch("ewald_force");
+    if (rc) return rc;
+  }
+  if (energy) {
+    k_ewald_energy<<<1, FIN_BLOCK, 0, st>>>(nk, V, alpha, qqr2e, qsq, kvec, re, im, energy);
+    count_launch();
+    rc = check_launch("ewald_energy");
+  }
+  return rc;
+}
+
+}  // namespace rbx

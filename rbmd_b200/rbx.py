@@ -1,0 +1,407 @@
+"""ctypes binding of librbx.so (the C ABI in include/rbx.h).
+
+The engine itself is torch-free C++/CUDA; this module only marshals arguments.
+Op-level wrappers take torch CUDA tensors (device pointers) so tests can drive
+the drop-in kernels exactly as RBMD's op functors are driven.  There is no CPU
+fallback: loading fails loudly when the library is missing, and every compute
+call raises when the library reports an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librbx.so")
+_lib = None
+
+RBX_OK = 0
+PLAIN_FP64 = 0
+MIXED = 1
+NEIGHBOR_VERLET = 0
+NEIGHBOR_RBL = 1
+COULOMB_NONE = 0
+COULOMB_RBE = 1
+COULOMB_EWALD = 2
+
+
+class RbxError(RuntimeError):
+    pass
+
+
+class Box(C.Structure):
+    _fields_ = [("lo", C.c_double * 3), ("hi", C.c_double * 3)]
+
+    @staticmethod
+    def make(lo, hi):
+        b = Box()
+        for d in range(3):
+            b.lo[d] = float(lo[d])
+            b.hi[d] = float(hi[d])
+        return b
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("neighbor_type", C.c_int),
+        ("cut_off", C.c_double),
+        ("r_core", C.c_double),
+        ("skin", C.c_double),
+        ("neighbor_sample_num", C.c_int),
+        ("coulomb_type", C.c_int),
+        ("alpha", C.c_double),
+        ("coulomb_sample_num", C.c_int),
+        ("kmax", C.c_int * 3),
+        ("random_seed", C.c_uint64),
+        ("qqr2e", C.c_double),
+        ("dt", C.c_double),
+        ("precision", C.c_int),
+        ("ntypes", C.c_int),
+        ("sigma", C.POINTER(C.c_double)),
+        ("eps", C.POINTER(C.c_double)),
+        ("mass", C.POINTER(C.c_double)),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int64),
+        ("force_calls", C.c_int64),
+        ("rebuilds", C.c_int64),
+        ("epoch", C.c_int),
+        ("selection_frequency", C.c_int),
+        ("candidate_capacity", C.c_int),
+        ("candidates", C.c_int64),
+        ("e_kspace", C.c_double),
+        ("virial_kspace", C.c_double * 6),
+    ]
+
+
+# Every symbol include/rbx.h declares.
+EXPORTS = [
+    "rbx_last_error", "rbx_version", "rbx_launch_count", "rbx_rbe_gauss_sum", "rbx_rbl_params",
+    "rbx_rbe_sample", "rbx_rbe_structure_factor", "rbx_rbe_force", "rbx_rbe_energy_virial",
+    "rbx_ewald_force", "rbx_cell_grid", "rbx_cells_scratch_bytes", "rbx_cells_sort",
+    "rbx_full_list", "rbx_rbl_filter", "rbx_pair_force_rbl", "rbx_fix_rbl_force",
+    "rbx_pair_force_verlet", "rbx_engine_create", "rbx_engine_create_json",
+    "rbx_engine_destroy", "rbx_engine_set_state", "rbx_engine_set_k_samples",
+    "rbx_engine_compute_forces", "rbx_engine_step", "rbx_engine_step_host",
+    "rbx_engine_get_state", "rbx_engine_get_force_parts", "rbx_engine_get_rbl_pairs",
+    "rbx_engine_get_stats", "rbx_engine_stream", "rbx_engine_phase_ms",
+    "rbx_engine_set_profiling",
+]
+
+
+def lib():
+    """Load librbx.so (built in-tree by rbmd_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RbxError(f"{LIB_PATH} is missing: run `python -m rbmd_b200.build` "
+                       "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+    B = C.POINTER(Box)
+    L.rbx_last_error.restype = C.c_char_p
+    L.rbx_launch_count.restype = C.c_uint64
+    L.rbx_cells_scratch_bytes.restype = C.c_size_t
+    L.rbx_cells_scratch_bytes.argtypes = [ip, ip]
+    L.rbx_rbe_gauss_sum.argtypes = [B, dp, C.POINTER(C.c_double)]
+    L.rbx_rbl_params.argtypes = [ip, B, dp, dp, ip, C.POINTER(C.c_int)]
+    L.rbx_rbe_sample.argtypes = [B, dp, ip, C.c_uint64, C.c_int64, vp, vp, vp, vp]
+    L.rbx_rbe_structure_factor.argtypes = [B, ip, ip] + [vp] * 9 + [vp]
+    L.rbx_rbe_force.argtypes = [B, ip, ip, dp, dp, dp] + [vp] * 12 + [vp]
+    L.rbx_rbe_energy_virial.argtypes = [B, ip, dp, dp, dp, dp, dp] + [vp] * 7 + [vp]
+    L.rbx_ewald_force.argtypes = [B, ip, C.POINTER(C.c_int), dp, dp] + [vp] * 8 + [vp]
+    L.rbx_cell_grid.argtypes = [B, dp, C.POINTER(C.c_int)]
+    L.rbx_cells_sort.argtypes = [B, dp, ip] + [vp] * 7 + [vp]
+    L.rbx_full_list.argtypes = [B, dp, ip, vp, vp, vp, vp, ip, vp, vp, vp, vp]
+    L.rbx_rbl_filter.argtypes = ([dp, dp, ip] + [vp] * 11 + [ip] + [vp] * 3 + [B, vp, ip, ip,
+                                                                                 vp])
+    L.rbx_pair_force_rbl.argtypes = [B, dp, dp, ip, ip, ip, dp, dp] + [vp] * 14 + [vp]
+    L.rbx_fix_rbl_force.argtypes = [ip, vp, vp, vp, vp, vp]
+    L.rbx_pair_force_verlet.argtypes = [B, dp, ip, dp, dp] + [vp] * 15 + [vp]
+    L.rbx_engine_create.restype = vp
+    L.rbx_engine_create.argtypes = [C.POINTER(Params), B, ip, ip]
+    L.rbx_engine_create_json.restype = vp
+    L.rbx_engine_create_json.argtypes = [C.c_char_p, B, ip, ip, vp, vp, vp, vp, ip, ip]
+    L.rbx_engine_destroy.argtypes = [vp]
+    L.rbx_engine_set_state.argtypes = [vp] * 10
+    L.rbx_engine_set_k_samples.argtypes = [vp, ip, vp, vp, vp]
+    L.rbx_engine_compute_forces.argtypes = [vp, ip]
+    L.rbx_engine_step.argtypes = [vp, ip]
+    L.rbx_engine_step_host.argtypes = [vp] * 6
+    L.rbx_engine_get_state.argtypes = [vp] * 10
+    L.rbx_engine_get_force_parts.argtypes = [vp, vp, vp]
+    L.rbx_engine_get_rbl_pairs.argtypes = [vp, vp, C.POINTER(C.c_int64), vp,
+                                           C.POINTER(C.c_int64)]
+    L.rbx_engine_get_stats.argtypes = [vp, C.POINTER(Stats)]
+    L.rbx_engine_stream.restype = vp
+    L.rbx_engine_stream.argtypes = [vp]
+    L.rbx_engine_phase_ms.argtypes = [vp, C.POINTER(C.c_float)]
+    L.rbx_engine_set_profiling.argtypes = [vp, ip]
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().rbx_last_error().decode(errors="replace")
+
+
+def check(rc, what=""):
+    if rc != RBX_OK:
+        raise RbxError(f"{what} failed (status {rc}): {last_error()}")
+
+
+def launch_count() -> int:
+    return int(lib().rbx_launch_count())
+
+
+def _ptr(t):
+    """Device pointer of a torch tensor (or None)."""
+    if t is None:
+        return None
+    return C.c_void_p(t.data_ptr())
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+# ---------------------------------------------------------------------------
+# host helpers
+# ---------------------------------------------------------------------------
+def rbe_gauss_sum(box: Box, alpha: float) -> float:
+    s = C.c_double()
+    check(lib().rbx_rbe_gauss_sum(C.byref(box), alpha, C.byref(s)), "rbx_rbe_gauss_sum")
+    return s.value
+
+
+def rbl_params(n_global, box: Box, r_core, cut_off, sample_num) -> int:
+    f = C.c_int()
+    check(lib().rbx_rbl_params(n_global, C.byref(box), r_core, cut_off, sample_num, C.byref(f)),
+          "rbx_rbl_params")
+    return f.value
+
+
+def cell_grid(box: Box, cutoff: float):
+    dims = (C.c_int * 3)()
+    check(lib().rbx_cell_grid(C.byref(box), cutoff, dims), "rbx_cell_grid")
+    return list(dims)
+
+
+# ---------------------------------------------------------------------------
+# op-level wrappers (torch CUDA tensors in, results written in place)
+# ---------------------------------------------------------------------------
+def rbe_sample(box, alpha, p, seed, step, mx, my, mz, stream=None):
+    check(lib().rbx_rbe_sample(C.byref(box), alpha, p, seed, step, _ptr(mx), _ptr(my), _ptr(mz),
+                               _stream(stream)), "rbx_rbe_sample")
+
+
+def rbe_structure_factor(box, q, mx, my, mz, x, y, z, re, im, stream=None):
+    check(lib().rbx_rbe_structure_factor(C.byref(box), q.numel(), mx.numel(), _ptr(q), _ptr(mx),
+                                         _ptr(my), _ptr(mz), _ptr(x), _ptr(y), _ptr(z), _ptr(re),
+                                         _ptr(im), _stream(stream)), "rbx_rbe_structure_factor")
+
+
+def rbe_force(box, alpha, S, qqr2e, re, im, q, mx, my, mz, x, y, z, fx, fy, fz, stream=None):
+    check(lib().rbx_rbe_force(C.byref(box), q.numel(), mx.numel(), alpha, S, qqr2e, _ptr(re),
+                              _ptr(im), _ptr(q), _ptr(mx), _ptr(my), _ptr(mz), _ptr(x), _ptr(y),
+                              _ptr(z), _ptr(fx), _ptr(fy), _ptr(fz), _stream(stream)),
+          "rbx_rbe_force")
+
+
+def rbe_energy_virial(box, alpha, S, qqr2e, qsq, qsum, re, im, mx, my, mz, virial, energy,
+                      stream=None):
+    check(lib().rbx_rbe_energy_virial(C.byref(box), mx.numel(), alpha, S, qqr2e, qsq, qsum,
+                                      _ptr(re), _ptr(im), _ptr(mx), _ptr(my), _ptr(mz),
+                                      _ptr(virial), _ptr(energy), _stream(stream)),
+          "rbx_rbe_energy_virial")
+
+
+def ewald_force(box, kmax, alpha, qqr2e, q, x, y, z, fx, fy, fz, energy=None, stream=None):
+    km = (C.c_int * 3)(*kmax)
+    check(lib().rbx_ewald_force(C.byref(box), q.numel(), km, alpha, qqr2e, _ptr(q), _ptr(x),
+                                _ptr(y), _ptr(z), _ptr(fx), _ptr(fy), _ptr(fz), _ptr(energy),
+                                _stream(stream)), "rbx_ewald_force")
+
+
+def cells_sort(box, cutoff, x, y, z, perm, cell_of_sorted, cell_start, scratch, stream=None):
+    check(lib().rbx_cells_sort(C.byref(box), cutoff, x.numel(), _ptr(x), _ptr(y), _ptr(z),
+                               _ptr(perm), _ptr(cell_of_sorted), _ptr(cell_start), _ptr(scratch),
+                               _stream(stream)), "rbx_cells_sort")
+
+
+def cells_scratch_bytes(n, ncell) -> int:
+    return int(lib().rbx_cells_scratch_bytes(n, ncell))
+
+
+def full_list(box, cutoff, x, y, z, cell_start, cap, count, nbrs, overflow, stream=None):
+    check(lib().rbx_full_list(C.byref(box), cutoff, x.numel(), _ptr(x), _ptr(y), _ptr(z),
+                              _ptr(cell_start), cap, _ptr(count), _ptr(nbrs), _ptr(overflow),
+                              _stream(stream)), "rbx_full_list")
+
+
+def rbl_filter(core2, force2, gid, x, y, z, cstart, cend, cand, core_cap, core_start, core_end,
+               core, shell_cap, shell, shell_num, required, box, realloc, freq, epoch,
+               stream=None):
+    check(lib().rbx_rbl_filter(core2, force2, gid.numel(), _ptr(gid), _ptr(x), _ptr(y), _ptr(z),
+                               _ptr(cstart), _ptr(cend), _ptr(cand), _ptr(core_cap),
+                               _ptr(core_start), _ptr(core_end), _ptr(core), shell_cap,
+                               _ptr(shell), _ptr(shell_num), _ptr(required), C.byref(box),
+                               _ptr(realloc), freq, epoch, _stream(stream)), "rbx_rbl_filter")
+
+
+def pair_force_rbl(box, rs, rc, sample_num, pice, alpha, qqr2e, typ, sigma, eps, start, end,
+                   core, shell, shell_num, q, x, y, z, fx, fy, fz, stream=None):
+    check(lib().rbx_pair_force_rbl(C.byref(box), rs, rc, q.numel(), sample_num, pice, alpha, qqr2e,
+                                   _ptr(typ), _ptr(sigma), _ptr(eps), _ptr(start), _ptr(end),
+                                   _ptr(core), _ptr(shell), _ptr(shell_num), _ptr(q), _ptr(x),
+                                   _ptr(y), _ptr(z), _ptr(fx), _ptr(fy), _ptr(fz),
+                                   _stream(stream)), "rbx_pair_force_rbl")
+
+
+def fix_rbl_force(fx, fy, fz, mean=None, stream=None):
+    check(lib().rbx_fix_rbl_force(fx.numel(), _ptr(fx), _ptr(fy), _ptr(fz), _ptr(mean),
+                                  _stream(stream)), "rbx_fix_rbl_force")
+
+
+def pair_force_verlet(box, cut_off, alpha, qqr2e, typ, sigma, eps, start, end, nbrs, q, x, y, z,
+                      fx, fy, fz, flat_virial, evdwl, ecoul, stream=None):
+    check(lib().rbx_pair_force_verlet(C.byref(box), cut_off, q.numel(), alpha, qqr2e, _ptr(typ),
+                                      _ptr(sigma), _ptr(eps), _ptr(start), _ptr(end), _ptr(nbrs),
+                                      _ptr(q), _ptr(x), _ptr(y), _ptr(z), _ptr(fx), _ptr(fy),
+                                      _ptr(fz), _ptr(flat_virial), _ptr(evdwl), _ptr(ecoul),
+                                      _stream(stream)), "rbx_pair_force_verlet")
+
+
+# ---------------------------------------------------------------------------
+# engine
+# ---------------------------------------------------------------------------
+class Engine:
+    """LJCutCoulKspace force plugin + NVE velocity-Verlet step on one GPU."""
+
+    def __init__(self, sys: dict, *, precision=PLAIN_FP64, neighbor="RBL", coulomb="RBE",
+                 seed=12345, device=0, json_text: str | None = None):
+        L = lib()
+        self.n = int(sys["n"])
+        self.box = Box.make(sys["lo"], sys["hi"])
+        self._sigma = np.ascontiguousarray(sys["sigma"], dtype=np.float64)
+        self._eps = np.ascontiguousarray(sys["eps"], dtype=np.float64)
+        self._mass = np.ascontiguousarray(sys["mass"], dtype=np.float64)
+        q = np.ascontiguousarray(sys["q"], dtype=np.float64)
+        if json_text is not None:
+            h = L.rbx_engine_create_json(json_text.encode(), C.byref(self.box), self.n,
+                                         len(self._sigma), _np_ptr(self._sigma),
+                                         _np_ptr(self._eps), _np_ptr(self._mass), _np_ptr(q),
+                                         precision, device)
+        else:
+            p = sys["params"]
+            prm = Params()
+            prm.neighbor_type = NEIGHBOR_RBL if neighbor == "RBL" else NEIGHBOR_VERLET
+            prm.cut_off = p["cut_off"]
+            prm.r_core = p["r_core"]
+            prm.skin = p["skin"]
+            prm.neighbor_sample_num = p["neighbor_sample_num"]
+            prm.coulomb_type = {"RBE": COULOMB_RBE, "NONE": COULOMB_NONE}[coulomb]
+            prm.alpha = p["alpha"]
+            prm.coulomb_sample_num = p["kspace_p"]
+            prm.random_seed = seed
+            prm.qqr2e = p["qqr2e"]
+            prm.dt = p["dt"]
+            prm.precision = precision
+            prm.ntypes = len(self._sigma)
+            prm.sigma = self._sigma.ctypes.data_as(C.POINTER(C.c_double))
+            prm.eps = self._eps.ctypes.data_as(C.POINTER(C.c_double))
+            prm.mass = self._mass.ctypes.data_as(C.POINTER(C.c_double))
+            h = L.rbx_engine_create(C.byref(prm), C.byref(self.box), self.n, device)
+        if not h:
+            raise RbxError(f"rbx_engine_create failed: {last_error()}")
+        self._h = C.c_void_p(h)
+        pos = np.ascontiguousarray(sys["pos"], dtype=np.float64)
+        vel = np.ascontiguousarray(sys["vel"], dtype=np.float64)
+        cols = [np.ascontiguousarray(pos[:, d]) for d in range(3)] + \
+               [np.ascontiguousarray(vel[:, d]) for d in range(3)]
+        gid = np.ascontiguousarray(sys["gid"], dtype=np.int32)
+        typ = np.ascontiguousarray(sys["type"], dtype=np.int32)
+        check(L.rbx_engine_set_state(self._h, _np_ptr(gid), _np_ptr(typ), _np_ptr(q),
+                                     *[_np_ptr(c) for c in cols]), "rbx_engine_set_state")
+
+    def set_k_samples(self, mx, my, mz):
+        if mx is None:
+            check(lib().rbx_engine_set_k_samples(self._h, 0, None, None, None), "set_k_samples")
+            return
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (mx, my, mz)]
+        self._kkeep = a
+        check(lib().rbx_engine_set_k_samples(self._h, len(a[0]), *[_np_ptr(v) for v in a]),
+              "rbx_engine_set_k_samples")
+
+    def compute_forces(self, epoch=0):
+        check(lib().rbx_engine_compute_forces(self._h, epoch), "rbx_engine_compute_forces")
+
+    def step(self, nsteps=1):
+        check(lib().rbx_engine_step(self._h, nsteps), "rbx_engine_step")
+
+    def step_host(self, x_in, v_in, x_out, v_out, f_out):
+        """One step from host buffers laid out as [3, n] (x, y, z rows)."""
+        check(lib().rbx_engine_step_host(self._h, _np_ptr(x_in), _np_ptr(v_in), _np_ptr(x_out),
+                                         _np_ptr(v_out), _np_ptr(f_out)), "rbx_engine_step_host")
+
+    def get_state(self):
+        a = [np.zeros(self.n) for _ in range(9)]
+        check(lib().rbx_engine_get_state(self._h, *[_np_ptr(v) for v in a]), "get_state")
+        return {"pos": np.stack(a[0:3], 1), "vel": np.stack(a[3:6], 1),
+                "force": np.stack(a[6:9], 1)}
+
+    def force_parts(self):
+        fp = np.zeros((self.n, 3))
+        fk = np.zeros((self.n, 3))
+        check(lib().rbx_engine_get_force_parts(self._h, _np_ptr(fp), _np_ptr(fk)), "force_parts")
+        return fp, fk
+
+    def rbl_pairs(self):
+        nc, ns = C.c_int64(0), C.c_int64(0)
+        check(lib().rbx_engine_get_rbl_pairs(self._h, None, C.byref(nc), None, C.byref(ns)),
+              "rbl_pairs size")
+        core = np.zeros((max(nc.value, 1), 2), dtype=np.int32)
+        shell = np.zeros((max(ns.value, 1), 2), dtype=np.int32)
+        check(lib().rbx_engine_get_rbl_pairs(self._h, _np_ptr(core), C.byref(nc),
+                                             _np_ptr(shell), C.byref(ns)), "rbl_pairs")
+        return core[:nc.value], shell[:ns.value]
+
+    def stats(self) -> Stats:
+        s = Stats()
+        check(lib().rbx_engine_get_stats(self._h, C.byref(s)), "get_stats")
+        return s
+
+    @property
+    def stream(self) -> int:
+        return int(lib().rbx_engine_stream(self._h) or 0)
+
+    def set_profiling(self, on=True):
+        check(lib().rbx_engine_set_profiling(self._h, int(on)), "set_profiling")
+
+    def phase_ms(self):
+        out = (C.c_float * 4)()
+        check(lib().rbx_engine_phase_ms(self._h, out), "phase_ms")
+        return list(out)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rbx_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

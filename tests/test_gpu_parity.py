@@ -1,0 +1,382 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the FP64 oracle.
+
+Tolerances: bit-exact for lists, batch selection and k-samples; 1e-12 relative
+RMS for plain-FP64 k-space, 1e-10 for plain-FP64 pair forces (the library uses
+erfc where the reference kernel writes 1 - erf); 1e-6 relative RMS for the
+plain-FP64 engine force; 1e-5 for the mixed engine force.
+"""
+import numpy as np
+import pytest
+
+from rbmd_b200 import systems
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(torch, a, dtype=None):
+    a = np.ascontiguousarray(a)
+    if dtype is None:
+        dtype = torch.float64 if a.dtype == np.float64 else torch.int32
+    return torch.as_tensor(a).to(dtype=dtype, device="cuda").contiguous()
+
+
+def _sorted(oracle, s, cutoff):
+    box = oracle.Box.make(s["lo"], s["hi"])
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    perm, cell, cs, ce = oracle.cells_sort(box, cutoff, x, y, z)
+    return box, perm, cell, cs, ce, x[perm], y[perm], z[perm]
+
+
+@pytest.fixture(scope="module")
+def sys4k():
+    return systems.lj_electrolyte(4000, seed=21)
+
+
+@pytest.fixture(scope="module")
+def sys20k():
+    return systems.lj_electrolyte(20000, seed=22)
+
+
+# ---------------------------------------------------------------------------
+# k-space ops
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("p", [1, 100, 400])
+def test_rbe_sample_bit_exact(cuda, rbx, oracle, sys4k, p):
+    s = sys4k
+    for step in (0, 1, 12345):
+        want = oracle.rbe_sample_philox(oracle.Box.make(s["lo"], s["hi"]), 0.16, p, 99, step)
+        m = [cuda.zeros(p, dtype=cuda.float64, device="cuda") for _ in range(3)]
+        rbx.rbe_sample(rbx.Box.make(s["lo"], s["hi"]), 0.16, p, 99, step, *m)
+        cuda.cuda.synchronize()
+        for d in range(3):
+            assert np.array_equal(m[d].cpu().numpy(), want[d])
+        assert not np.any((want[0] == 0) & (want[1] == 0) & (want[2] == 0))
+
+
+@pytest.mark.parametrize("n,p", [(4000, 100), (4000, 400), (20000, 100), (1, 7), (257, 33)])
+def test_rbe_kspace_ops(cuda, rbx, oracle, n, p):
+    s = systems.lj_electrolyte(max(n, 2), seed=n + p)
+    if n == 1:
+        s = {k: (v[:1] if isinstance(v, np.ndarray) and len(v) == 2 else v) for k, v in s.items()}
+        s["n"] = 1
+    box = oracle.Box.make(s["lo"], s["hi"])
+    rbox = rbx.Box.make(s["lo"], s["hi"])
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    m = oracle.rbe_sample_philox(box, 0.16, p, 3, 1)
+    re, im = oracle.rbe_structure_factor(box, s["q"], x, y, z, *m)
+    S = oracle.rbe_gauss_sum(box, 0.16)
+    f = oracle.rbe_force(box, S, 1.0, re, im, s["q"], *m, x, y, z)
+    e, vir = oracle.rbe_energy_virial(box, 0.16, S, 1.0, float((s["q"] ** 2).sum()),
+                                      float(s["q"].sum()), re, im, *m)
+    T = [_t(cuda, a) for a in (s["q"], *m, x, y, z)]
+    dre = cuda.zeros(p, dtype=cuda.float64, device="cuda")
+    dim = cuda.zeros(p, dtype=cuda.float64, device="cuda")
+    rbx.rbe_structure_factor(rbox, T[0], T[1], T[2], T[3], T[4], T[5], T[6], dre, dim)
+    F = [cuda.zeros(len(x), dtype=cuda.float64, device="cuda") for _ in range(3)]
+    rbx.rbe_force(rbox, 0.16, S, 1.0, dre, dim, T[0], T[1], T[2], T[3], T[4], T[5], T[6], *F)
+    dv = cuda.zeros(6, dtype=cuda.float64, device="cuda")
+    de = cuda.zeros(1, dtype=cuda.float64, device="cuda")
+    rbx.rbe_energy_virial(rbox, 0.16, S, 1.0, float((s["q"] ** 2).sum()), float(s["q"].sum()),
+                          dre, dim, T[1], T[2], T[3], dv, de)
+    cuda.cuda.synchronize()
+    scale = np.sqrt((re ** 2 + im ** 2).mean()) + 1e-30
+    assert np.abs(dre.cpu().numpy() - re).max() < 1e-11 * scale * np.sqrt(len(x))
+    assert np.abs(dim.cpu().numpy() - im).max() < 1e-11 * scale * np.sqrt(len(x))
+    got = np.stack([a.cpu().numpy() for a in F], 1)
+    if np.abs(f).max() > 0:
+        assert systems.rel_rms(got, f) < 1e-12
+    assert abs(de.item() - e) <= 1e-12 * abs(e) + 1e-14
+    assert np.allclose(dv.cpu().numpy(), vir, rtol=1e-11, atol=1e-12 * np.abs(vir).max())
+
+
+def test_ewald_force(cuda, rbx, oracle):
+    s = systems.lj_electrolyte(500, seed=5, density=0.5)
+    box = oracle.Box.make(s["lo"], s["hi"])
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    f, e = oracle.ewald_force(box, 0.16, 1.0, [6, 5, 4], s["q"], x, y, z)
+    T = [_t(cuda, a) for a in (s["q"], x, y, z)]
+    F = [cuda.zeros(len(x), dtype=cuda.float64, device="cuda") for _ in range(3)]
+    de = cuda.zeros(1, dtype=cuda.float64, device="cuda")
+    rbx.ewald_force(rbx.Box.make(s["lo"], s["hi"]), [6, 5, 4], 0.16, 1.0, *T, *F, energy=de)
+    cuda.cuda.synchronize()
+    assert systems.rel_rms(np.stack([a.cpu().numpy() for a in F], 1), f) < 1e-12
+    assert abs(de.item() - e) < 1e-11 * abs(e)
+
+
+# ---------------------------------------------------------------------------
+# neighbor ops: bit-exact sets
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n", [4000, 20000])
+def test_cells_and_full_list(cuda, rbx, oracle, n):
+    s = systems.lj_electrolyte(n, seed=n)
+    rc = 5.3
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    rbox = rbx.Box.make(s["lo"], s["hi"])
+    dims = rbx.cell_grid(rbox, rc)
+    ncell = int(np.prod(dims))
+    X = [_t(cuda, a) for a in (x, y, z)]
+    perm = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    cos = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    cst = cuda.zeros(ncell + 1, dtype=cuda.int32, device="cuda")
+    scratch = cuda.zeros(rbx.cells_scratch_bytes(n, ncell), dtype=cuda.uint8, device="cuda")
+    rbx.cells_sort(rbox, rc, *X, perm, cos, cst, scratch)
+    hp = perm.cpu().numpy()
+    assert sorted(hp.tolist()) == list(range(n))
+    hc = cos.cpu().numpy()
+    assert np.all(np.diff(hc) >= 0)
+    hs = cst.cpu().numpy()
+    for c in range(ncell):
+        assert np.all(np.diff(hp[hs[c]:hs[c + 1]]) > 0)  # stable inside a cell
+    xs = [_t(cuda, a[hp]) for a in (x, y, z)]
+    cap = 800
+    cnt = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    nb = cuda.full((n, cap), -1, dtype=cuda.int32, device="cuda")
+    ovf = cuda.zeros(1, dtype=cuda.int32, device="cuda")
+    rbx.full_list(rbox, rc, *xs, cst, cap, cnt, nb, ovf)
+    cuda.cuda.synchronize()
+    assert ovf.item() == 0
+    box = oracle.Box.make(s["lo"], s["hi"])
+    ocnt, orows = oracle.full_list(box, rc, x[hp], y[hp], z[hp], hc, hs[:-1].copy(),
+                                   hs[1:].copy())
+    gc, gn = cnt.cpu().numpy(), nb.cpu().numpy()
+    assert np.array_equal(gc, ocnt)
+    for i in range(n):
+        assert set(gn[i, :gc[i]].tolist()) == set(orows[i, :ocnt[i]].tolist())
+
+
+def test_full_list_overflow_flag(cuda, rbx, sys4k):
+    s = sys4k
+    n = s["n"]
+    rbox = rbx.Box.make(s["lo"], s["hi"])
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    dims = rbx.cell_grid(rbox, 5.3)
+    ncell = int(np.prod(dims))
+    X = [_t(cuda, a) for a in (x, y, z)]
+    perm = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    cos = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    cst = cuda.zeros(ncell + 1, dtype=cuda.int32, device="cuda")
+    scratch = cuda.zeros(rbx.cells_scratch_bytes(n, ncell), dtype=cuda.uint8, device="cuda")
+    rbx.cells_sort(rbox, 5.3, *X, perm, cos, cst, scratch)
+    hp = perm.cpu().numpy()
+    xs = [_t(cuda, a[hp]) for a in (x, y, z)]
+    cnt = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    nb = cuda.zeros((n, 32), dtype=cuda.int32, device="cuda")
+    ovf = cuda.zeros(1, dtype=cuda.int32, device="cuda")
+    rbx.full_list(rbox, 5.3, *xs, cst, 32, cnt, nb, ovf)
+    cuda.cuda.synchronize()
+    assert ovf.item() & 1  # capacity overflow is reported, rows stay in bounds
+    assert cnt.cpu().numpy().max() > 32
+
+
+def _ref_lists(oracle, s, epoch, freq):
+    box, perm, cell, cs, ce, xs, ys, zs = _sorted(oracle, s, 5.3)
+    cnt, rows = oracle.full_list(box, 5.3, xs, ys, zs, cell, cs, ce)
+    gid = s["gid"][perm]
+    cc, core, sc, shell = oracle.rbl_filter(box, 2.5, 5.0, freq, epoch, gid, xs, ys, zs, cnt,
+                                            rows)
+    return box, perm, xs, ys, zs, gid, cnt, rows, cc, core, sc, shell
+
+
+@pytest.mark.parametrize("epoch,freq", [(0, 4), (17, 4), (3, 1), (5, 3)])
+def test_rbl_filter_op_bit_exact(cuda, rbx, oracle, sys4k, epoch, freq):
+    s = sys4k
+    n = s["n"]
+    box, perm, xs, ys, zs, gid, cnt, rows, cc, core, sc, shell = _ref_lists(oracle, s, epoch, freq)
+    cap = rows.shape[1]
+    cstart = np.arange(n, dtype=np.int32) * cap
+    cend = cstart + cnt
+    ccap = np.full(n, cap, dtype=np.int32)
+    T = lambda a: _t(cuda, a)  # noqa: E731
+    core_end = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    dcore = cuda.full((n * cap,), -1, dtype=cuda.int32, device="cuda")
+    shell_cap = cap
+    dshell = cuda.full((shell_cap * n,), -1, dtype=cuda.int32, device="cuda")
+    snum = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    req = cuda.zeros(1, dtype=cuda.int32, device="cuda")
+    realloc = cuda.zeros(1, dtype=cuda.int32, device="cuda")
+    rbx.rbl_filter(2.5 ** 2 - 1e-4, 5.0 ** 2 - 1e-4, T(gid), T(xs), T(ys), T(zs), T(cstart),
+                   T(cend), T(rows.reshape(-1)), T(ccap), T(cstart), core_end, dcore, shell_cap,
+                   dshell, snum, req, rbx.Box.make(s["lo"], s["hi"]), realloc, freq, epoch)
+    cuda.cuda.synchronize()
+    assert realloc.item() == 0
+    hce = core_end.cpu().numpy() - cstart
+    hcore = dcore.cpu().numpy().reshape(n, cap)
+    hsn = snum.cpu().numpy()
+    hsh = dshell.cpu().numpy().reshape(shell_cap, n)
+    assert np.array_equal(hce, cc)
+    assert np.array_equal(hsn, sc)
+    assert req.item() == sc.max()
+    for i in range(n):
+        assert hcore[i, :hce[i]].tolist() == core[i, :cc[i]].tolist()  # same order too
+        assert hsh[:hsn[i], i].tolist() == shell[i, :sc[i]].tolist()
+
+
+# ---------------------------------------------------------------------------
+# pair-force ops
+# ---------------------------------------------------------------------------
+def test_pair_force_rbl_op(cuda, rbx, oracle, sys4k):
+    s = sys4k
+    n = s["n"]
+    box, perm, xs, ys, zs, gid, cnt, rows, cc, core, sc, shell = _ref_lists(oracle, s, 2, 4)
+    typ, q = s["type"][perm], s["q"][perm]
+    want = oracle.pair_force_rbl(box, 2.5, 5.0, 4, 0.16, 1.0, typ, s["sigma"], s["eps"], q, xs,
+                                 ys, zs, cc, core, sc, shell)
+    cap = core.shape[1]
+    start = np.arange(n, dtype=np.int32) * cap
+    sh_sm = np.full((cap, n), -1, dtype=np.int32)
+    for i in range(n):
+        sh_sm[:sc[i], i] = shell[i, :sc[i]]
+    T = lambda a: _t(cuda, a)  # noqa: E731
+    F = [cuda.zeros(n, dtype=cuda.float64, device="cuda") for _ in range(3)]
+    rbx.pair_force_rbl(rbx.Box.make(s["lo"], s["hi"]), 2.5, 5.0, 100, 4, 0.16, 1.0, T(typ),
+                       T(s["sigma"]), T(s["eps"]), T(start), T(start + cc), T(core.reshape(-1)),
+                       T(sh_sm.reshape(-1)), T(sc), T(q), T(xs), T(ys), T(zs), *F)
+    mean = cuda.zeros(3, dtype=cuda.float64, device="cuda")
+    got_raw = np.stack([a.cpu().numpy() for a in F], 1)
+    assert systems.rel_rms(got_raw, want) < 1e-10
+    rbx.fix_rbl_force(*F, mean=mean)
+    cuda.cuda.synchronize()
+    fixed, omean = oracle.fix_rbl(want)
+    assert np.allclose(mean.cpu().numpy(), omean, rtol=1e-9, atol=1e-12)
+    assert systems.rel_rms(np.stack([a.cpu().numpy() for a in F], 1), fixed) < 1e-10
+
+
+def test_pair_force_verlet_op(cuda, rbx, oracle, sys4k):
+    s = sys4k
+    n = s["n"]
+    box, perm, cell, cs, ce, xs, ys, zs = _sorted(oracle, s, 5.3)
+    cnt, rows = oracle.full_list(box, 5.3, xs, ys, zs, cell, cs, ce)
+    typ, q = s["type"][perm], s["q"][perm]
+    f, vir, el, ec = oracle.pair_force_verlet(box, 5.0, 0.16, 1.0, typ, s["sigma"], s["eps"], q,
+                                              xs, ys, zs, cnt, rows)
+    cap = rows.shape[1]
+    start = np.arange(n, dtype=np.int32) * cap
+    T = lambda a: _t(cuda, a)  # noqa: E731
+    F = [cuda.zeros(n, dtype=cuda.float64, device="cuda") for _ in range(3)]
+    fv = cuda.zeros(6 * n, dtype=cuda.float64, device="cuda")
+    e1 = cuda.zeros(1, dtype=cuda.float64, device="cuda")
+    e2 = cuda.zeros(1, dtype=cuda.float64, device="cuda")
+    rbx.pair_force_verlet(rbx.Box.make(s["lo"], s["hi"]), 5.0, 0.16, 1.0, T(typ), T(s["sigma"]),
+                          T(s["eps"]), T(start), T(start + cnt), T(rows.reshape(-1)), T(q), T(xs),
+                          T(ys), T(zs), *F, fv, e1, e2)
+    cuda.cuda.synchronize()
+    assert systems.rel_rms(np.stack([a.cpu().numpy() for a in F], 1), f) < 1e-10
+    assert abs(e1.item() - el) < 1e-10 * abs(el)
+    assert abs(e2.item() - ec) < 1e-10 * abs(ec)
+    assert np.allclose(fv.cpu().numpy().reshape(6, n).sum(1), vir, rtol=1e-10)
+
+
+# ---------------------------------------------------------------------------
+# engine (the per-step fused path)
+# ---------------------------------------------------------------------------
+def _oracle_total(oracle, s, m, epoch):
+    import __graft_entry__ as ge
+
+    if epoch == 0:
+        return ge._oracle_forces(s, m)
+    raise NotImplementedError
+
+
+@pytest.mark.parametrize("n", [4000, 20000])
+def test_engine_forces_fp64_and_mixed(cuda, rbx, oracle, n):
+    s = systems.lj_electrolyte(n, seed=100 + n)
+    box = oracle.Box.make(s["lo"], s["hi"])
+    m = oracle.rbe_sample_philox(box, 0.16, 100, 7, 0)
+    want = _oracle_total(oracle, s, m, 0)
+    for prec, tol in ((rbx.PLAIN_FP64, 1e-9), (rbx.MIXED, 1e-5)):
+        e = rbx.Engine(s, precision=prec)
+        e.set_k_samples(*m)
+        e.compute_forces(epoch=0)
+        got = e.get_state()["force"]
+        err = systems.rel_rms(got, want)
+        assert err < tol, (prec, err)
+        fp, fk = e.force_parts()
+        assert np.abs(fp.mean(0)).max() < 1e-9 * np.abs(fp).mean()  # RBL mean removed
+        e.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_engine_rbl_pairs_bit_exact(cuda, rbx, oracle, sys4k, prec):
+    s = sys4k
+    for epoch in (0, 9):
+        box, perm, xs, ys, zs, gid, cnt, rows, cc, core, sc, shell = _ref_lists(oracle, s, epoch,
+                                                                                4)
+        e = rbx.Engine(s, precision=prec)
+        e.compute_forces(epoch=epoch)
+        gc, gs = e.rbl_pairs()
+        want_c = {(int(gid[i]), int(gid[j])) for i in range(s["n"]) for j in core[i, :cc[i]]}
+        want_s = {(int(gid[i]), int(gid[j])) for i in range(s["n"]) for j in shell[i, :sc[i]]}
+        got_c = set(map(tuple, gc.tolist()))
+        got_s = set(map(tuple, gs.tolist()))
+        if prec == 0:
+            assert got_c == want_c and got_s == want_s
+        else:
+            # fixed-point positions: only pairs within 1e-6 of a list threshold may differ
+            assert len(got_c ^ want_c) <= 2 and len(got_s ^ want_s) <= 2
+        e.close()
+
+
+def test_engine_philox_matches_oracle_engine(cuda, rbx, oracle, sys4k):
+    """Full velocity-Verlet steps with on-device Philox k-samples and RBL
+    batches: the first steps agree with the oracle's step to FP64 round-off."""
+    s = sys4k
+    e = rbx.Engine(s, precision=rbx.PLAIN_FP64, seed=4242)
+    ref = oracle.Engine(s, seed=4242)
+    ref.compute_forces(0)
+    e.compute_forces(0)
+    for k in range(3):
+        e.step(1)
+        ref.step(1)
+        a, b = e.get_state(), ref.get()
+        order = np.argsort(b["gid"])
+        bf = b["force"][order]
+        bp = b["pos"][order]
+        assert systems.rel_rms(a["force"], bf) < 1e-8, k
+        assert np.abs(a["pos"] - bp).max() < 1e-10
+    st = e.stats()
+    assert st.steps == 3 and st.selection_frequency == 4
+
+
+def test_engine_step_host_roundtrip(cuda, rbx, sys4k):
+    s = sys4k
+    e1 = rbx.Engine(s, precision=rbx.MIXED, seed=1)
+    e2 = rbx.Engine(s, precision=rbx.MIXED, seed=1)
+    e1.compute_forces(0)
+    e2.compute_forces(0)
+    n = s["n"]
+    x = np.ascontiguousarray(s["pos"].T)
+    v = np.ascontiguousarray(s["vel"].T)
+    xo, vo, fo = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
+    for _ in range(3):
+        e1.step_host(x, v, xo, vo, fo)
+        x, v = xo.copy(), vo.copy()
+        e2.step(1)
+    st = e2.get_state()
+    assert np.array_equal(st["pos"], xo.T)
+    assert np.array_equal(st["force"], fo.T)
+
+
+def test_engine_json_drop_in(cuda, rbx, sys4k):
+    from tests.test_capi_cpu import JSON_OK
+
+    s = sys4k
+    e = rbx.Engine(s, json_text=JSON_OK)
+    st = e.stats()
+    assert st.selection_frequency == 4
+    e.compute_forces(0)
+    assert np.isfinite(e.get_state()["force"]).all()
+    e.close()
+
+
+def test_engine_energy_conservation_short(cuda, rbx):
+    """Plain-FP64 RBL+RBE dynamics stays finite and the candidate list is
+    rebuilt on the skin criterion."""
+    s = systems.lj_electrolyte(4000, seed=77)
+    e = rbx.Engine(s, precision=rbx.MIXED)
+    e.step(200)
+    st = e.stats()
+    assert st.rebuilds >= 2
+    out = e.get_state()
+    assert np.isfinite(out["pos"]).all() and np.isfinite(out["vel"]).all()
+    T = (out["vel"] ** 2).sum() / (3 * s["n"])
+    assert 0.5 < T < 3.0
