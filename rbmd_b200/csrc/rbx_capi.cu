@@ -79,7 +79,8 @@ int require_device() {
 }
 
 // Per-axis inverse-CDF table of the RBE importance density (see the oracle's
-// restatement): order m = 0, +1, -1, +2, -2, ... down to weight 1e-20.
+// restatement): order m = 0, +1, -1, +2, -2, ... down to weight 1e-20,
+// returned as cumulative sums.
 int rbe_axis_table(double L, double alpha, double* w, int max_entries, double* total) {
   const double c = (M_PI * M_PI) / (alpha * L * L);
   int cnt = 0;
@@ -99,6 +100,12 @@ int rbe_axis_table(double L, double alpha, double* w, int max_entries, double* t
     }
   }
   *total = z;
+  // cumulative form (left-to-right sums, the oracle's scan order)
+  double acc = 0.0;
+  for (int t = 0; t < cnt; ++t) {
+    acc += w[t];
+    w[t] = acc;
+  }
   return cnt;
 }
 

@@ -5,7 +5,9 @@
 // ComputeCellRangesIndices (src/neighbor_list/src/linked_cell/linked_cell.cpp:428-670,
 // src/neighbor_list/src/op/rocm/linked_cell_op.hip.cu:57-164) with a counting
 // sort: atomic histogram, one-block scan, atomic scatter, then a per-cell
-// bitonic sort of the old indices so the order is deterministic and stable.
+// bitonic sort.  Inside a cell atoms are ordered by a 4x4x4 Morton sub-cell
+// code, then by old index (deterministic), so consecutive atoms are close in
+// space: 32-atom chunks have small bounding boxes for the list builder.
 //
 // The candidate list replaces Estimate/GenerateFullNeighborListOp
 // (src/neighbor_list/src/op/rocm/full_neighbor_list_op.hip.cu:177-288): one
@@ -29,16 +31,37 @@ __device__ __forceinline__ int cell_coord(double v, double lo, double inv_edge, 
   return c > dim - 1 ? dim - 1 : c;
 }
 
+// Morton interleave of three 2-bit sub-cell coordinates.
+__device__ __forceinline__ unsigned morton2(unsigned a, unsigned b, unsigned c) {
+  unsigned m = 0;
+#pragma unroll
+  for (int bit = 0; bit < 2; ++bit)
+    m |= ((a >> bit) & 1u) << (3 * bit) | ((b >> bit) & 1u) << (3 * bit + 1) |
+         ((c >> bit) & 1u) << (3 * bit + 2);
+  return m;
+}
+
+constexpr int SUB_SHIFT = 26;  // key = sub-cell code << 26 | old index (n < 2^26)
+
 __global__ void k_cell_assign(DBox b, int dx, int dy, int dz, int n, const double* __restrict__ x,
                               const double* __restrict__ y, const double* __restrict__ z,
-                              int* __restrict__ cell, int* __restrict__ counts) {
+                              int* __restrict__ cell, unsigned* __restrict__ sub,
+                              int* __restrict__ counts) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const double fx = (x[i] - b.lo[0]) * (dx / b.len[0]);
+  const double fy = (y[i] - b.lo[1]) * (dy / b.len[1]);
+  const double fz = (z[i] - b.lo[2]) * (dz / b.len[2]);
   const int cx = cell_coord(x[i], b.lo[0], dx / b.len[0], dx);
   const int cy = cell_coord(y[i], b.lo[1], dy / b.len[1], dy);
   const int cz = cell_coord(z[i], b.lo[2], dz / b.len[2], dz);
   const int c = (cz * dy + cy) * dx + cx;
   cell[i] = c;
+  auto sub4 = [](double f, int c0) {
+    int v = (int)floor((f - c0) * 4.0);
+    return (unsigned)(v < 0 ? 0 : (v > 3 ? 3 : v));
+  };
+  sub[i] = n < (1 << SUB_SHIFT) ? morton2(sub4(fx, cx), sub4(fy, cy), sub4(fz, cz)) : 0u;
   atomicAdd(counts + c, 1);
 }
 
@@ -84,18 +107,19 @@ k_cell_scan(int ncell, const int* __restrict__ counts, int* __restrict__ start,
   if (threadIdx.x == 0) start[ncell] = s_carry;
 }
 
-__global__ void k_cell_scatter(int n, const int* __restrict__ cell, int* __restrict__ fill,
-                               int* __restrict__ tmp) {
+__global__ void k_cell_scatter(int n, const int* __restrict__ cell,
+                               const unsigned* __restrict__ sub, int* __restrict__ fill,
+                               unsigned* __restrict__ tmp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  tmp[atomicAdd(fill + cell[i], 1)] = i;
+  tmp[atomicAdd(fill + cell[i], 1)] = (sub[i] << SUB_SHIFT) | (unsigned)i;
 }
 
-// One block per cell: bitonic sort of the cell's old indices (ascending).
+// One block per cell: bitonic sort of the cell's keys (sub-cell, old index).
 __global__ void __launch_bounds__(512)
-k_cell_segsort(int ncell, const int* __restrict__ start, const int* __restrict__ tmp,
+k_cell_segsort(int ncell, int n, const int* __restrict__ start, const unsigned* __restrict__ tmp,
                int* __restrict__ perm, int* __restrict__ cell_of_sorted, int* __restrict__ status) {
-  __shared__ int s[SEG_MAX];
+  __shared__ unsigned s[SEG_MAX];
   const int c = blockIdx.x;
   const int a = start[c], cnt = start[c + 1] - a;
   if (cnt > SEG_MAX) {
@@ -104,7 +128,7 @@ k_cell_segsort(int ncell, const int* __restrict__ start, const int* __restrict__
   }
   int p2 = 1;
   while (p2 < cnt) p2 <<= 1;
-  for (int t = threadIdx.x; t < p2; t += blockDim.x) s[t] = t < cnt ? tmp[a + t] : 0x7fffffff;
+  for (int t = threadIdx.x; t < p2; t += blockDim.x) s[t] = t < cnt ? tmp[a + t] : 0xffffffffu;
   __syncthreads();
   for (int k = 2; k <= p2; k <<= 1) {
     for (int j = k >> 1; j > 0; j >>= 1) {
@@ -112,7 +136,7 @@ k_cell_segsort(int ncell, const int* __restrict__ start, const int* __restrict__
         const int u = t ^ j;
         if (u > t) {
           const bool up = (t & k) == 0;
-          const int va = s[t], vb = s[u];
+          const unsigned va = s[t], vb = s[u];
           if ((va > vb) == up) {
             s[t] = vb;
             s[u] = va;
@@ -122,18 +146,22 @@ k_cell_segsort(int ncell, const int* __restrict__ start, const int* __restrict__
       __syncthreads();
     }
   }
+  const unsigned mask = n < (1 << SUB_SHIFT) ? (1u << SUB_SHIFT) - 1u : 0xffffffffu;
   for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-    perm[a + t] = s[t];
+    perm[a + t] = (int)(s[t] & mask);
     cell_of_sorted[a + t] = c;
   }
 }
 
 // ---------------------------------------------------------------------------
-// Candidate list: CTA per cell.
+// Candidate list: CTA per cell.  Stencil cells are staged in shared memory,
+// each padded to whole 32-atom chunks; every chunk gets a bounding box, and a
+// centre atom tests only the chunks whose box comes within the cutoff.
 // ---------------------------------------------------------------------------
 constexpr int NL_BLOCK = 256;
 constexpr int NL_WARPS = NL_BLOCK / 32;
-constexpr int NL_STAGE = 2048;   // staged stencil atoms per pass
+constexpr int NL_STAGE = 2048;   // staged stencil slots per pass (multiple of 32)
+constexpr int NL_CHUNKS = NL_STAGE / 32;
 constexpr int NL_CENTER = 1024;  // centre-cell atoms tracked per CTA
 
 __global__ void __launch_bounds__(NL_BLOCK)
@@ -143,8 +171,9 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float lo_band, fl
             int* __restrict__ count, int* __restrict__ nbrs, int* __restrict__ overflow) {
   __shared__ float sx[NL_STAGE], sy[NL_STAGE], sz[NL_STAGE];
   __shared__ int sj[NL_STAGE];
+  __shared__ float bb[6][NL_CHUNKS];  // chunk boxes: min xyz, max xyz
   __shared__ int s_cnt[NL_CENTER];
-  __shared__ int s_cells[27], s_cbeg[27], s_ccnt[27];
+  __shared__ int s_cbeg[27], s_ccnt[27];
   __shared__ double s_shift[27][3];
   const int c = blockIdx.x;
   const int cz = c / (dimx * dimy), cy = (c / dimx) % dimy, cx = c % dimx;
@@ -178,7 +207,6 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float lo_band, fl
       s_shift[s][d] = sh;
     }
     const int cell = (nc[2] * dimy + nc[1]) * dimx + nc[0];
-    s_cells[s] = cell;
     s_cbeg[s] = cell_start[cell];
     s_ccnt[s] = cell_start[cell + 1] - cell_start[cell];
   }
@@ -188,29 +216,54 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float lo_band, fl
   const unsigned lt = (1u << lane) - 1u;
   int s0 = 0;
   while (s0 < 27) {
-    // greedy group of stencil cells that fits the stage
+    // greedy group of stencil cells whose padded sizes fit the stage
     int s1 = s0, tot = 0;
-    while (s1 < 27 && tot + s_ccnt[s1] <= NL_STAGE) {
-      tot += s_ccnt[s1];
+    while (s1 < 27 && tot + ((s_ccnt[s1] + 31) & ~31) <= NL_STAGE) {
+      tot += (s_ccnt[s1] + 31) & ~31;
       ++s1;
     }
     if (s1 == s0) {  // a single cell larger than the stage
       if (threadIdx.x == 0) atomicOr(overflow, 2);
       return;
     }
-    // stage
     int off = 0;
     for (int s = s0; s < s1; ++s) {
-      const int beg = s_cbeg[s], cnt = s_ccnt[s];
+      const int beg = s_cbeg[s], cnt = s_ccnt[s], pad = (cnt + 31) & ~31;
       const double shx = s_shift[s][0] - ox, shy = s_shift[s][1] - oy, shz = s_shift[s][2] - oz;
-      for (int t = threadIdx.x; t < cnt; t += NL_BLOCK) {
-        const int j = beg + t;
-        sx[off + t] = (float)(x[j] + shx);
-        sy[off + t] = (float)(y[j] + shy);
-        sz[off + t] = (float)(z[j] + shz);
-        sj[off + t] = j;
+      for (int t = threadIdx.x; t < pad; t += NL_BLOCK) {
+        if (t < cnt) {
+          const int j = beg + t;
+          sx[off + t] = (float)(x[j] + shx);
+          sy[off + t] = (float)(y[j] + shy);
+          sz[off + t] = (float)(z[j] + shz);
+          sj[off + t] = j;
+        } else {  // padding slot: never within the cutoff
+          sx[off + t] = 1e30f;
+          sy[off + t] = 1e30f;
+          sz[off + t] = 1e30f;
+          sj[off + t] = -1;
+        }
       }
-      off += cnt;
+      off += pad;
+    }
+    __syncthreads();
+    const int nch = tot / 32;
+    for (int ch = warp; ch < nch; ch += NL_WARPS) {
+      const int t = ch * 32 + lane;
+      const bool real = sj[t] >= 0;
+      float lo[3] = {real ? sx[t] : 1e30f, real ? sy[t] : 1e30f, real ? sz[t] : 1e30f};
+      float hi[3] = {real ? sx[t] : -1e30f, real ? sy[t] : -1e30f, real ? sz[t] : -1e30f};
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+          hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+        }
+      if (lane < 3) {
+        bb[lane][ch] = lo[lane];
+        bb[3 + lane][ch] = hi[lane];
+      }
     }
     __syncthreads();
     for (int li = warp; li < ncen; li += NL_WARPS) {
@@ -218,28 +271,37 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float lo_band, fl
       const double xi = x[i], yi = y[i], zi = z[i];
       const float fxi = (float)(xi - ox), fyi = (float)(yi - oy), fzi = (float)(zi - oz);
       int cnt = s_cnt[li];
-      for (int t0 = 0; t0 < tot; t0 += 32) {
-        const int t = t0 + lane;
-        bool in = false;
-        int j = -1;
-        if (t < tot) {
-          j = sj[t];
-          const float dxf = sx[t] - fxi, dyf = sy[t] - fyi, dzf = sz[t] - fzi;
-          const float d2f = dxf * dxf + dyf * dyf + dzf * dzf;
-          if (j != i) {
-            if (d2f < lo_band) {
+      for (int cb = 0; cb < nch; cb += 32) {
+        const int ch = cb + lane;
+        bool near = false;
+        if (ch < nch) {
+          const float gx = fmaxf(0.f, fmaxf(bb[0][ch] - fxi, fxi - bb[3][ch]));
+          const float gy = fmaxf(0.f, fmaxf(bb[1][ch] - fyi, fyi - bb[4][ch]));
+          const float gz = fmaxf(0.f, fmaxf(bb[2][ch] - fzi, fzi - bb[5][ch]));
+          near = gx * gx + gy * gy + gz * gz < hi_band;
+        }
+        unsigned m = __ballot_sync(0xffffffffu, near);
+        while (m) {
+          const int chunk = cb + __ffs(m) - 1;
+          m &= m - 1;
+          const int t = chunk * 32 + lane;
+          const int j = sj[t];
+          bool in = false;
+          if (j >= 0 && j != i) {
+            const float dxf = sx[t] - fxi, dyf = sy[t] - fyi, dzf = sz[t] - fzi;
+            const float d2f = dxf * dxf + dyf * dyf + dzf * dzf;
+            if (d2f < lo_band)
               in = true;
-            } else if (d2f < hi_band) {
+            else if (d2f < hi_band)
               in = dist2_list(b, xi, yi, zi, x[j], y[j], z[j]) < cut2;
-            }
           }
+          const unsigned mm = __ballot_sync(0xffffffffu, in);
+          if (in) {
+            const int pos = cnt + __popc(mm & lt);
+            if (pos < cap) nbrs[(size_t)i * cap + pos] = j;
+          }
+          cnt += __popc(mm);
         }
-        const unsigned m = __ballot_sync(0xffffffffu, in);
-        if (in) {
-          const int pos = cnt + __popc(m & lt);
-          if (pos < cap) nbrs[(size_t)i * cap + pos] = j;
-        }
-        cnt += __popc(m);
       }
       if (lane == 0) s_cnt[li] = cnt;
       __syncwarp();
@@ -371,9 +433,9 @@ __global__ void k_max_disp(DBox b, int n, const double* __restrict__ x,
 // Launchers
 // ---------------------------------------------------------------------------
 size_t cells_scratch_bytes(int n, int ncell) {
-  // counts[ncell] + fill[ncell] + cell[n] + tmp[n], 256-byte aligned pieces
+  // counts[ncell] + fill[ncell] + cell[n] + sub[n] + tmp[n], 256-byte aligned pieces
   auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
-  return al(sizeof(int) * (size_t)ncell) * 2 + al(sizeof(int) * (size_t)n) * 2;
+  return al(sizeof(int) * (size_t)ncell) * 2 + al(sizeof(int) * (size_t)n) * 3;
 }
 
 int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, const double* y,
@@ -388,23 +450,25 @@ int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, 
   p += al(sizeof(int) * (size_t)ncell);
   int* cell = (int*)p;
   p += al(sizeof(int) * (size_t)n);
-  int* tmp = (int*)p;
+  unsigned* sub = (unsigned*)p;
+  p += al(sizeof(int) * (size_t)n);
+  unsigned* tmp = (unsigned*)p;
   if (cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)ncell, st) != cudaSuccess) {
     set_error("cudaMemsetAsync failed in cells_sort");
     return RBX_ERR_CUDA;
   }
   if (n > 0) {
     k_cell_assign<<<(n + 255) / 256, 256, 0, st>>>(b, dims[0], dims[1], dims[2], n, x, y, z, cell,
-                                                   counts);
+                                                   sub, counts);
     count_launch();
   }
   k_cell_scan<<<1, 1024, 0, st>>>(ncell, counts, cell_start, fill);
   count_launch();
   if (n > 0) {
-    k_cell_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, cell, fill, tmp);
+    k_cell_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, cell, sub, fill, tmp);
     count_launch();
   }
-  k_cell_segsort<<<ncell, 512, 0, st>>>(ncell, cell_start, tmp, perm, cell_of_sorted, status);
+  k_cell_segsort<<<ncell, 512, 0, st>>>(ncell, n, cell_start, tmp, perm, cell_of_sorted, status);
   count_launch();
   return check_launch("cells_sort");
 }

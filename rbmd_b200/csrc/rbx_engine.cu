@@ -211,7 +211,19 @@ int rbx_engine::init() {
   pp.ntypes = prm.ntypes;
   pp.lj_eps = lj_eps;
   pp.lj_s6 = lj_s6;
-  for (int d = 0; d < 3; ++d) ms.s[d] = dbox.len[d] / 4294967296.0;
+  for (int d = 0; d < 3; ++d) pp.sf[d] = (float)(dbox.len[d] / 4294967296.0);
+  // fixed-point screens (cubic boxes): the guard band covers the fixed-point
+  // quantisation (< 3 units of L/2^32 per coordinate) with a wide margin
+  pp.cubic = dbox.len[0] == dbox.len[1] && dbox.len[1] == dbox.len[2];
+  if (pp.cubic) {
+    const double L = dbox.len[0];
+    const double band = std::max(1e-5, 128.0 * (L / 4294967296.0) * (rcs + 1.0));
+    pp.sc_eps = make_screen(RBX_EPSILON, L, band);
+    pp.sc_core = make_screen(pp.core2_list, L, band);
+    pp.sc_rs = make_screen(pp.rs2, L, band);
+    pp.sc_force = make_screen(pp.force2_list, L, band);
+    pp.sc_rc = make_screen(pp.rc2, L, band);
+  }
   return RBX_OK;
 }
 
@@ -278,7 +290,7 @@ int rbx_engine::rebuild() {
   ETRY(cuda_ok(cudaMemcpyAsync(x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
   ETRY(cuda_ok(cudaMemcpyAsync(y0, y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
   ETRY(cuda_ok(cudaMemcpyAsync(z0, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
-  if (prm.precision == RBX_MIXED) ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
+  ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
   for (int attempt = 0; attempt < 4; ++attempt) {
     ETRY(cuda_ok(cudaMemsetAsync(dflags + 1, 0, sizeof(int), st), "memset"));
     ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
@@ -334,15 +346,11 @@ int rbx_engine::check_rebuild(bool disp_from_drift) {
 
 int rbx_engine::real_space() {
   const bool mixed = prm.precision == RBX_MIXED;
-  if (prm.neighbor_type == RBX_NEIGHBOR_RBL) {
-    if (mixed)
-      return launch_rbl_fused_mixed(pp, ms, n, atoms, type, key_a, key_b, epoch, cand_count, cand,
-                                    cap, fpx, fpy, fpz, fpart, nfpart, st);
-    return launch_rbl_fused_f64(pp, n, x, y, z, q, type, key_a, key_b, epoch, cand_count, cand,
-                                cap, fpx, fpy, fpz, fpart, nfpart, st);
-  }
-  return launch_verlet_fused_f64(pp, n, x, y, z, q, type, cand_count, cand, cap, fpx, fpy, fpz,
-                                 nullptr, epart, nfpart, st);
+  if (prm.neighbor_type == RBX_NEIGHBOR_RBL)
+    return launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, cand_count,
+                            cand, cap, fpx, fpy, fpz, fpart, nfpart, st);
+  return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, fpx, fpy,
+                                 fpz, nullptr, epart, nfpart, st);
 }
 
 int rbx_engine::kspace_and_combine(bool kick) {
@@ -396,7 +404,7 @@ int rbx_engine::compute_forces(int ep) {
   cudaSetDevice(device);
   epoch = ep;
   ETRY(check_rebuild(false));
-  if (prm.precision == RBX_MIXED) ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
+  ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
   ETRY(real_space());
   ETRY(kspace_and_combine(false));
   ETRY(cuda_ok(cudaStreamSynchronize(st), "compute_forces sync"));
@@ -436,8 +444,7 @@ int rbx_engine::step(int nsteps) {
     }
     ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
     ETRY(cuda_ok(cudaMemsetAsync(max_d2, 0, sizeof(unsigned long long), st), "memset"));
-    ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2,
-                      mixed ? atoms : nullptr, q, st));
+    ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q, st));
     if (e) cudaEventRecord(e[1], st);
     ++epoch;
     ETRY(check_rebuild(true));
@@ -560,16 +567,10 @@ int rbx_engine::get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs
   ETRY(dalloc(&sc, N));
   ETRY(dalloc(&core, N * cap));
   ETRY(dalloc(&shell, N * cap));
-  int rc;
-  if (prm.precision == RBX_MIXED) {
-    rc = launch_to_fixed(dbox, n, x, y, z, q, atoms, st);
-    if (!rc)
-      rc = launch_rbl_lists_mixed(pp, ms, n, atoms, key_a, key_b, epoch, cand_count, cand, cap, cc,
-                                  core, sc, shell, st);
-  } else {
-    rc = launch_rbl_lists(pp, n, x, y, z, key_a, key_b, epoch, cand_count, cand, cap, cc, core, sc,
-                          shell, st);
-  }
+  int rc = launch_to_fixed(dbox, n, x, y, z, q, atoms, st);
+  if (!rc)
+    rc = launch_rbl_lists(pp, n, atoms, x, y, z, key_a, key_b, epoch, cand_count, cand, cap, cc,
+                          core, sc, shell, st);
   std::vector<int> hcc(N), hsc(N), hcore(N * cap), hshell(N * cap), hgid(N);
   if (!rc) {
     cudaMemcpyAsync(hcc.data(), cc, sizeof(int) * N, cudaMemcpyDeviceToHost, st);

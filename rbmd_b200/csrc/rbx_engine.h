@@ -23,7 +23,6 @@ struct rbx_engine {
   int P = 0;
   double S = 0.0, qsq = 0.0, qsum = 0.0;
   rbx::PairParams pp{};
-  rbx::MixedScale ms{};
 
   // per-atom device arrays, cell-sorted order
   double *x = nullptr, *y = nullptr, *z = nullptr;

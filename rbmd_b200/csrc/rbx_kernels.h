@@ -67,6 +67,14 @@ int launch_ewald(const DBox& b, int n, const int kmax[3], double alpha, double q
 int rbe_axis_table(double L, double alpha, double* w, int max_entries, double* total);
 
 // ---- real space (rbx_pair.cu) ----
+// Integer screen of "r^2 < C" on fixed-point |d|^2: true at or below lo, false
+// at or above hi, undecided in between (the FP64 predicate decides).
+struct IntScreen {
+  unsigned long long lo, hi;
+};
+// Build the screen for threshold C (r^2 units) on a cubic box of edge L.
+IntScreen make_screen(double C, double L, double band);
+
 struct PairParams {
   DBox box;
   double rs2, rc2;            // force predicates: r_core^2, cut_off^2
@@ -78,43 +86,34 @@ struct PairParams {
   int ntypes;
   const double* lj_eps;       // ntypes^2 eps_ij
   const double* lj_s6;        // ntypes^2 sigma_ij^6
+  // fixed-point screen (cubic box): |u_j - u_i|^2 against integer thresholds
+  int cubic;
+  float sf[3];                // L_d / 2^32 in FP32 (mixed pair vector)
+  IntScreen sc_eps, sc_core, sc_rs, sc_force, sc_rc;
 };
 
-struct MixedScale {
-  double s[3];                // L_d / 2^32
-};
 
 // Fused RBL filter + pair force over a row-major candidate list.
 // fpart (nblocks x 3) receives per-block force sums for the mean removal.
 int rbl_fused_blocks(int n);
-int launch_rbl_fused_f64(const PairParams& pp, int n, const double* x, const double* y,
-                         const double* z, const double* q, const int* type,
-                         const unsigned long long* key_a, const unsigned long long* key_b,
-                         int epoch, const int* cand_count, const int* cand, int cap,
-                         double* fx, double* fy, double* fz, double* fpart, int nblocks,
-                         cudaStream_t st);
-int launch_rbl_fused_mixed(const PairParams& pp, const MixedScale& ms, int n, const uint4* atoms,
-                           const int* type, const unsigned long long* key_a,
-                           const unsigned long long* key_b, int epoch, const int* cand_count,
-                           const int* cand, int cap, double* fx, double* fy, double* fz,
-                           double* fpart, int nblocks, cudaStream_t st);
+int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
+                     const double* x, const double* y, const double* z, const double* q,
+                     const int* type, const unsigned long long* key_a,
+                     const unsigned long long* key_b, int epoch, const int* cand_count,
+                     const int* cand, int cap, double* fx, double* fy, double* fz, double* fpart,
+                     int nblocks, cudaStream_t st);
 // Verlet pair force over the candidate list, cut at cut_off (force predicate).
-int launch_verlet_fused_f64(const PairParams& pp, int n, const double* x, const double* y,
-                            const double* z, const double* q, const int* type,
+int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, const double* x,
+                            const double* y, const double* z, const double* q, const int* type,
                             const int* cand_count, const int* cand, int cap, double* fx,
                             double* fy, double* fz, double* fpart, double* epart, int nblocks,
                             cudaStream_t st);
-// Emit RBL lists (engine debugging / parity): core and shell rows (cap stride).
-int launch_rbl_lists(const PairParams& pp, int n, const double* x, const double* y,
-                     const double* z, const unsigned long long* key_a,
+// Emit RBL lists (parity checks / export): core and shell rows (cap stride).
+int launch_rbl_lists(const PairParams& pp, int n, const uint4* atoms, const double* x,
+                     const double* y, const double* z, const unsigned long long* key_a,
                      const unsigned long long* key_b, int epoch, const int* cand_count,
                      const int* cand, int cap, int* core_count, int* core, int* shell_count,
                      int* shell, cudaStream_t st);
-int launch_rbl_lists_mixed(const PairParams& pp, const MixedScale& ms, int n, const uint4* atoms,
-                           const unsigned long long* key_a, const unsigned long long* key_b,
-                           int epoch, const int* cand_count, const int* cand, int cap,
-                           int* core_count, int* core, int* shell_count, int* shell,
-                           cudaStream_t st);
 int launch_rbl_keys(int n, const int* gid, unsigned long long* key_a, unsigned long long* key_b,
                     cudaStream_t st);
 // Drop-in ops with the reference layouts.

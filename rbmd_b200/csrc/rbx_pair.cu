@@ -17,6 +17,8 @@
 // RBL mean-force removal.
 #include <math.h>
 
+#include <type_traits>
+
 #include "rbx_common.cuh"
 #include "rbx_kernels.h"
 
@@ -94,86 +96,175 @@ __device__ __forceinline__ void write_block_partial(double (*s_acc)[3], double* 
 }
 
 // ---------------------------------------------------------------------------
-// Plain FP64 fused RBL kernel.
+// Candidate classification shared by both forms.
+//
+// On a cubic box the pair vector in fixed point, d = u_j - u_i (wrapped int32),
+// is the exact minimum image, and s^2 * |d|^2 differs from the FP64 r^2 of the
+// reference predicate by far less than the guard band around each threshold.
+// Each predicate "r^2 < C" is decided in 64-bit integers when |d|^2 is outside
+// [lo, hi]; inside it, the reference's FP64 expression (CaculateDistance:
+// i minus j, min image, no FMA) decides.  The outcome is therefore identical
+// to the FP64 predicate on every pair, in both precision forms.
 // ---------------------------------------------------------------------------
+struct Classified {
+  bool core_active;    // core list and lj126_rs window (r^2 > EPS)
+  bool shell_window;   // shell list and rcs window (r_core^2 < r^2 < cut_off^2)
+};
+
+__device__ __forceinline__ int screen_lt(unsigned long long d2i, const IntScreen& t) {
+  return d2i <= t.lo ? 1 : (d2i >= t.hi ? 0 : -1);
+}
+
+__device__ __forceinline__ Classified classify_exact(double d2, const PairParams& pp) {
+  Classified c;
+  const bool A = d2 < pp.core2_list;
+  c.core_active = A && d2 > RBX_EPSILON;  // d2 < rs2 holds: core2_list < rs2
+  c.shell_window = !A && d2 < pp.force2_list && d2 > pp.rs2;  // force2_list < rc2
+  return c;
+}
+
+__device__ __forceinline__ double exact_d2(const PairParams& pp, const double* __restrict__ x,
+                                           const double* __restrict__ y,
+                                           const double* __restrict__ z, int i, int j) {
+  return dist2_list(pp.box, __ldg(x + i), __ldg(y + i), __ldg(z + i), __ldg(x + j),
+                    __ldg(y + j), __ldg(z + j));
+}
+
+__device__ __forceinline__ Classified classify(const PairParams& pp, const uint4& ai,
+                                               const uint4& aj, const double* __restrict__ x,
+                                               const double* __restrict__ y,
+                                               const double* __restrict__ z, int i, int j) {
+  if (pp.cubic) {
+    const int dx = (int)(aj.x - ai.x), dy = (int)(aj.y - ai.y), dz = (int)(aj.z - ai.z);
+    const unsigned long long d2i = (unsigned long long)((long long)dx * dx) +
+                                   (unsigned long long)((long long)dy * dy) +
+                                   (unsigned long long)((long long)dz * dz);
+    if (d2i >= pp.sc_force.hi) return Classified{false, false};  // beyond the shell
+    const int A = screen_lt(d2i, pp.sc_core), B = screen_lt(d2i, pp.sc_force);
+    const int E = screen_lt(d2i, pp.sc_eps), R = screen_lt(d2i, pp.sc_rs);
+    if ((A | B | E | R) >= 0) {
+      Classified c;
+      c.core_active = A && !E;
+      c.shell_window = !A && B && !R;
+      return c;
+    }
+  }
+  return classify_exact(exact_d2(pp, x, y, z, i, j), pp);
+}
+
+template <typename T>
+struct PairQueue {
+  T dx[PAIR_WARPS][QCAP], dy[PAIR_WARPS][QCAP], dz[PAIR_WARPS][QCAP];
+  int j[PAIR_WARPS][QCAP];
+};
+
+// ---------------------------------------------------------------------------
+// Fused RBL filter + pair force.  MIXED = false: plain FP64 (pair vector and
+// force math in FP64 from the FP64 positions).  MIXED = true: FP32 force math
+// on the exact fixed-point pair vector.
+// ---------------------------------------------------------------------------
+template <bool MIXED>
 __global__ void __launch_bounds__(PAIR_BLOCK)
-k_rbl_fused_f64(PairParams pp, int n, const double* __restrict__ x, const double* __restrict__ y,
-                const double* __restrict__ z, const double* __restrict__ q,
-                const int* __restrict__ type, const unsigned long long* __restrict__ key_a,
-                const unsigned long long* __restrict__ key_b, int epoch,
-                const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
-                double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-                double* __restrict__ fpart) {
+k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
+            const double* __restrict__ y, const double* __restrict__ z,
+            const double* __restrict__ q, const int* __restrict__ type,
+            const unsigned long long* __restrict__ key_a,
+            const unsigned long long* __restrict__ key_b, int epoch,
+            const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
+            double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
+            double* __restrict__ fpart) {
+  using T = typename std::conditional<MIXED, float, double>::type;
   __shared__ TypeTables tt;
-  __shared__ double s_dx[PAIR_WARPS][QCAP], s_dy[PAIR_WARPS][QCAP], s_dz[PAIR_WARPS][QCAP];
-  __shared__ int s_j[PAIR_WARPS][QCAP];
+  __shared__ PairQueue<T> qu;
   __shared__ double s_acc[PAIR_WARPS][3];
+  __shared__ float f_eps[MAX_TYPES_SMEM * MAX_TYPES_SMEM], f_s6[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
   load_type_tables(tt, pp);
+  if (MIXED) {
+    for (int e = threadIdx.x; e < pp.ntypes * pp.ntypes; e += blockDim.x) {
+      f_eps[e] = (float)tt.eps[e];
+      f_s6[e] = (float)tt.s6[e];
+    }
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = lanemask_lt();
   double acc0 = 0, acc1 = 0, acc2 = 0;
   const int nt = pp.ntypes;
   for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += gridDim.x * PAIR_WARPS) {
-    const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
+    const uint4 ai = atoms[i];
+    const double xi = x[i], yi = y[i], zi = z[i];
+    const T qi = MIXED ? (T)__uint_as_float(ai.w) : (T)q[i];
     const int ti = type[i];
     const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
     const int cnt = cand_count[i];
     const int* row = cand + (size_t)i * cap;
     int qn = 0;
-    double fxa = 0, fya = 0, fza = 0;
+    T fxa = 0, fya = 0, fza = 0;
     for (int k0 = 0;;) {
       const bool more = k0 < cnt;
-      bool push = false;
-      int code = 0;
-      double dx = 0, dy = 0, dz = 0;
       if (more) {
         const int k = k0 + lane;
+        bool push = false;
+        int code = 0, j = i;
+        uint4 aj = ai;
         if (k < cnt) {
-          const int j = __ldg(row + k);
+          j = __ldg(row + k);
           if (j != i) {
-            const double xj = __ldg(x + j), yj = __ldg(y + j), zj = __ldg(z + j);
-            // list predicate: i minus j, no FMA (CaculateDistance)
-            const double ex = min_image1(__dsub_rn(xi, xj), pp.box.len[0], pp.box.half[0]);
-            const double ey = min_image1(__dsub_rn(yi, yj), pp.box.len[1], pp.box.half[1]);
-            const double ez = min_image1(__dsub_rn(zi, zj), pp.box.len[2], pp.box.half[2]);
-            const double d2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-            if (d2 < pp.core2_list) {
-              push = d2 < pp.rs2 && d2 > RBX_EPSILON;  // lj126_rs / _rs_fix window
+            aj = __ldg(atoms + j);
+            const Classified c = classify(pp, ai, aj, x, y, z, i, j);
+            if (c.core_active) {
+              push = true;
               code = j;
-            } else if (d2 < pp.force2_list && d2 < pp.rc2 && d2 > pp.rs2) {
-              push = rbl_selected(ea, __ldg(key_b + j), pp.div);  // shell sample
+            } else if (c.shell_window) {
+              push = rbl_selected(ea, __ldg(key_b + j), pp.div);  // shell batch hash
               code = j | (int)0x80000000;
             }
-            dx = -ex;  // pair vector r_j - r_i (min image is odd in its argument)
-            dy = -ey;
-            dz = -ez;
           }
         }
         const unsigned m = __ballot_sync(0xffffffffu, push);
         if (push) {
           const int pos = qn + __popc(m & lt);
-          s_dx[warp][pos] = dx;
-          s_dy[warp][pos] = dy;
-          s_dz[warp][pos] = dz;
-          s_j[warp][pos] = code;
+          T dx, dy, dz;
+          if (MIXED) {  // exact wrapped fixed-point difference r_j - r_i
+            dx = (T)((float)(int)(aj.x - ai.x) * pp.sf[0]);
+            dy = (T)((float)(int)(aj.y - ai.y) * pp.sf[1]);
+            dz = (T)((float)(int)(aj.z - ai.z) * pp.sf[2]);
+          } else {  // r_j - r_i, MinImageDistance (box.h:51-73)
+            dx = (T)min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
+            dy = (T)min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
+            dz = (T)min_image1(__ldg(z + j) - zi, pp.box.len[2], pp.box.half[2]);
+          }
+          qu.dx[warp][pos] = dx;
+          qu.dy[warp][pos] = dy;
+          qu.dz[warp][pos] = dz;
+          qu.j[warp][pos] = code;
         }
         qn += __popc(m);
         k0 += 32;
         __syncwarp();
       }
-      // drain full batches, and the remainder after the last chunk
+      // drain full 32-pair batches, and the remainder after the last chunk
       while (qn >= 32 || (!more && qn > 0)) {
         if (lane < qn) {
-          const int c = s_j[warp][lane];
+          const int c = qu.j[warp][lane];
           const int j = c & 0x7fffffff;
-          const double ddx = s_dx[warp][lane], ddy = s_dy[warp][lane], ddz = s_dz[warp][lane];
-          const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+          const T ddx = qu.dx[warp][lane], ddy = qu.dy[warp][lane], ddz = qu.dz[warp][lane];
           const int tj = __ldg(type + j);
-          const double qq = qi * __ldg(q + j);
-          double f = lj_f64(tt.eps[ti * nt + tj], tt.s6[ti * nt + tj], d2);
-          if (qq != 0.0) f += coul_f64(pp.alpha, pp.sqrt_alpha, pp.qqr2e, qq, d2);
-          if (c < 0) f *= (double)pp.freq;
+          T f;
+          if (MIXED) {
+            const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+            const float qq = (float)qi * __uint_as_float(__ldg(&atoms[j].w));
+            f = lj_f32(f_eps[ti * nt + tj], f_s6[ti * nt + tj], d2);
+            if (qq != 0.f)
+              f += coul_f32((float)pp.alpha, (float)pp.sqrt_alpha, (float)pp.qqr2e, qq, d2);
+            if (c < 0) f *= (float)pp.freq;
+          } else {
+            const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+            const double qq = (double)qi * __ldg(q + j);
+            f = lj_f64(tt.eps[ti * nt + tj], tt.s6[ti * nt + tj], d2);
+            if (qq != 0.0) f += coul_f64(pp.alpha, pp.sqrt_alpha, pp.qqr2e, qq, d2);
+            if (c < 0) f *= (double)pp.freq;
+          }
           fxa += f * ddx;
           fya += f * ddy;
           fza += f * ddz;
@@ -181,143 +272,18 @@ k_rbl_fused_f64(PairParams pp, int n, const double* __restrict__ x, const double
         __syncwarp();
         const int rem = qn > 32 ? qn - 32 : 0;
         if (lane < rem) {
-          s_dx[warp][lane] = s_dx[warp][32 + lane];
-          s_dy[warp][lane] = s_dy[warp][32 + lane];
-          s_dz[warp][lane] = s_dz[warp][32 + lane];
-          s_j[warp][lane] = s_j[warp][32 + lane];
+          qu.dx[warp][lane] = qu.dx[warp][32 + lane];
+          qu.dy[warp][lane] = qu.dy[warp][32 + lane];
+          qu.dz[warp][lane] = qu.dz[warp][32 + lane];
+          qu.j[warp][lane] = qu.j[warp][32 + lane];
         }
         __syncwarp();
         qn = rem;
       }
       if (!more) break;
     }
-    fxa = warp_sum(fxa);
-    fya = warp_sum(fya);
-    fza = warp_sum(fza);
-    if (lane == 0) {
-      fx[i] = fxa;
-      fy[i] = fya;
-      fz[i] = fza;
-      acc0 += fxa;
-      acc1 += fya;
-      acc2 += fza;
-    }
-  }
-  if (lane == 0) {
-    s_acc[warp][0] = acc0;
-    s_acc[warp][1] = acc1;
-    s_acc[warp][2] = acc2;
-  }
-  if (fpart) write_block_partial(s_acc, fpart);
-}
-
-// ---------------------------------------------------------------------------
-// Mixed fused RBL kernel: atoms as {ux, uy, uz, q_f32}; the pair vector is the
-// exact wrapped integer difference (exact minimum image); list and force
-// windows are decided in FP64 on that vector, the force math runs in FP32.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(PAIR_BLOCK)
-k_rbl_fused_mixed(PairParams pp, MixedScale ms, int n, const uint4* __restrict__ atoms,
-                  const int* __restrict__ type, const unsigned long long* __restrict__ key_a,
-                  const unsigned long long* __restrict__ key_b, int epoch,
-                  const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
-                  double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-                  double* __restrict__ fpart) {
-  __shared__ TypeTables tt;
-  __shared__ float s_dx[PAIR_WARPS][QCAP], s_dy[PAIR_WARPS][QCAP], s_dz[PAIR_WARPS][QCAP];
-  __shared__ int s_j[PAIR_WARPS][QCAP];
-  __shared__ double s_acc[PAIR_WARPS][3];
-  __shared__ float f_eps[MAX_TYPES_SMEM * MAX_TYPES_SMEM], f_s6[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
-  load_type_tables(tt, pp);
-  for (int e = threadIdx.x; e < pp.ntypes * pp.ntypes; e += blockDim.x) {
-    f_eps[e] = (float)tt.eps[e];
-    f_s6[e] = (float)tt.s6[e];
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned lt = lanemask_lt();
-  const float alpha = (float)pp.alpha, sqa = (float)pp.sqrt_alpha, qqr2e = (float)pp.qqr2e;
-  const float ffreq = (float)pp.freq;
-  double acc0 = 0, acc1 = 0, acc2 = 0;
-  const int nt = pp.ntypes;
-  for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += gridDim.x * PAIR_WARPS) {
-    const uint4 ai = atoms[i];
-    const float qi = __uint_as_float(ai.w);
-    const int ti = type[i];
-    const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
-    const int cnt = cand_count[i];
-    const int* row = cand + (size_t)i * cap;
-    int qn = 0;
-    float fxa = 0.f, fya = 0.f, fza = 0.f;
-    for (int k0 = 0;;) {
-      const bool more = k0 < cnt;
-      bool push = false;
-      int code = 0;
-      float dx = 0.f, dy = 0.f, dz = 0.f;
-      if (more) {
-        const int k = k0 + lane;
-        if (k < cnt) {
-          const int j = __ldg(row + k);
-          if (j != i) {
-            const uint4 aj = __ldg(atoms + j);
-            const double ex = (double)(int)(aj.x - ai.x) * ms.s[0];
-            const double ey = (double)(int)(aj.y - ai.y) * ms.s[1];
-            const double ez = (double)(int)(aj.z - ai.z) * ms.s[2];
-            const double d2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-            if (d2 < pp.core2_list) {
-              push = d2 < pp.rs2 && d2 > RBX_EPSILON;
-              code = j;
-            } else if (d2 < pp.force2_list && d2 < pp.rc2 && d2 > pp.rs2) {
-              push = rbl_selected(ea, __ldg(key_b + j), pp.div);
-              code = j | (int)0x80000000;
-            }
-            dx = (float)ex;
-            dy = (float)ey;
-            dz = (float)ez;
-          }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, push);
-        if (push) {
-          const int pos = qn + __popc(m & lt);
-          s_dx[warp][pos] = dx;
-          s_dy[warp][pos] = dy;
-          s_dz[warp][pos] = dz;
-          s_j[warp][pos] = code;
-        }
-        qn += __popc(m);
-        k0 += 32;
-        __syncwarp();
-      }
-      while (qn >= 32 || (!more && qn > 0)) {
-        if (lane < qn) {
-          const int c = s_j[warp][lane];
-          const int j = c & 0x7fffffff;
-          const float ddx = s_dx[warp][lane], ddy = s_dy[warp][lane], ddz = s_dz[warp][lane];
-          const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
-          const int tj = __ldg(type + j);
-          const float qq = qi * __uint_as_float(__ldg(&atoms[j].w));
-          float f = lj_f32(f_eps[ti * nt + tj], f_s6[ti * nt + tj], d2);
-          if (qq != 0.f) f += coul_f32(alpha, sqa, qqr2e, qq, d2);
-          if (c < 0) f *= ffreq;
-          fxa = fmaf(f, ddx, fxa);
-          fya = fmaf(f, ddy, fya);
-          fza = fmaf(f, ddz, fza);
-        }
-        __syncwarp();
-        const int rem = qn > 32 ? qn - 32 : 0;
-        if (lane < rem) {
-          s_dx[warp][lane] = s_dx[warp][32 + lane];
-          s_dy[warp][lane] = s_dy[warp][32 + lane];
-          s_dz[warp][lane] = s_dz[warp][32 + lane];
-          s_j[warp][lane] = s_j[warp][32 + lane];
-        }
-        __syncwarp();
-        qn = rem;
-      }
-      if (!more) break;
-    }
-    const double gx = warp_sum((double)fxa), gy = warp_sum((double)fya), gz = warp_sum((double)fza);
+    const double gx = warp_sum((double)fxa), gy = warp_sum((double)fya),
+                 gz = warp_sum((double)fza);
     if (lane == 0) {
       fx[i] = gx;
       fy[i] = gy;
@@ -340,17 +306,18 @@ k_rbl_fused_mixed(PairParams pp, MixedScale ms, int n, const uint4* __restrict__
 // list (ComputeLJCutCoulForce, lj_cut_coul_kspace_op.hip.cu:256-356), with
 // per-block energy and virial partials epart[block][8] =
 // {evdwl, ecoul, vxx, vyy, vzz, vxy, vxz, vyz} (ComputeVirial, lj_op.hip.cu:76-88).
+// The cutoff test uses the integer screen with the FP64 fallback.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(PAIR_BLOCK)
-k_verlet_fused_f64(PairParams pp, int n, const double* __restrict__ x,
-                   const double* __restrict__ y, const double* __restrict__ z,
-                   const double* __restrict__ q, const int* __restrict__ type,
-                   const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
-                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-                   double* __restrict__ fpart, double* __restrict__ epart) {
+k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
+                   const double* __restrict__ x, const double* __restrict__ y,
+                   const double* __restrict__ z, const double* __restrict__ q,
+                   const int* __restrict__ type, const int* __restrict__ cand_count,
+                   const int* __restrict__ cand, int cap, double* __restrict__ fx,
+                   double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart,
+                   double* __restrict__ epart) {
   __shared__ TypeTables tt;
-  __shared__ double s_dx[PAIR_WARPS][QCAP], s_dy[PAIR_WARPS][QCAP], s_dz[PAIR_WARPS][QCAP];
-  __shared__ int s_j[PAIR_WARPS][QCAP];
+  __shared__ PairQueue<double> qu;
   __shared__ double s_acc[PAIR_WARPS][3];
   __shared__ double s_e[PAIR_WARPS][8];
   load_type_tables(tt, pp);
@@ -360,6 +327,7 @@ k_verlet_fused_f64(PairParams pp, int n, const double* __restrict__ x,
   double eacc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const int nt = pp.ntypes;
   for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += gridDim.x * PAIR_WARPS) {
+    const uint4 ai = atoms[i];
     const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
     const int ti = type[i];
     const int cnt = cand_count[i];
@@ -372,26 +340,36 @@ k_verlet_fused_f64(PairParams pp, int n, const double* __restrict__ x,
       if (more) {
         bool push = false;
         int j = 0;
-        double dx = 0, dy = 0, dz = 0;
         const int k = k0 + lane;
         if (k < cnt) {
           j = __ldg(row + k);
           if (j != i) {
-            dx = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
-            dy = min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
-            dz = min_image1(__ldg(z + j) - zi, pp.box.len[2], pp.box.half[2]);
-            const double d2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            push = d2 < pp.rc2;
+            int in = -1;
+            if (pp.cubic) {
+              const uint4 aj = __ldg(atoms + j);
+              const int dx = (int)(aj.x - ai.x), dy = (int)(aj.y - ai.y), dz = (int)(aj.z - ai.z);
+              const unsigned long long d2i = (unsigned long long)((long long)dx * dx) +
+                                             (unsigned long long)((long long)dy * dy) +
+                                             (unsigned long long)((long long)dz * dz);
+              in = screen_lt(d2i, pp.sc_rc);
+            }
+            if (in < 0) {
+              const double ex = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
+              const double ey = min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
+              const double ez = min_image1(__ldg(z + j) - zi, pp.box.len[2], pp.box.half[2]);
+              in = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez)) <
+                   pp.rc2;
+            }
+            push = in;
           }
         }
         const unsigned m = __ballot_sync(0xffffffffu, push);
         if (push) {
           const int pos = qn + __popc(m & lt);
-          s_dx[warp][pos] = dx;
-          s_dy[warp][pos] = dy;
-          s_dz[warp][pos] = dz;
-          s_j[warp][pos] = j;
+          qu.dx[warp][pos] = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
+          qu.dy[warp][pos] = min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
+          qu.dz[warp][pos] = min_image1(__ldg(z + j) - zi, pp.box.len[2], pp.box.half[2]);
+          qu.j[warp][pos] = j;
         }
         qn += __popc(m);
         k0 += 32;
@@ -399,8 +377,8 @@ k_verlet_fused_f64(PairParams pp, int n, const double* __restrict__ x,
       }
       while (qn >= 32 || (!more && qn > 0)) {
         if (lane < qn) {
-          const int j = s_j[warp][lane];
-          const double ddx = s_dx[warp][lane], ddy = s_dy[warp][lane], ddz = s_dz[warp][lane];
+          const int j = qu.j[warp][lane];
+          const double ddx = qu.dx[warp][lane], ddy = qu.dy[warp][lane], ddz = qu.dz[warp][lane];
           const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
           const int tj = __ldg(type + j);
           const double qq = qi * __ldg(q + j);
@@ -430,10 +408,10 @@ k_verlet_fused_f64(PairParams pp, int n, const double* __restrict__ x,
         __syncwarp();
         const int rem = qn > 32 ? qn - 32 : 0;
         if (lane < rem) {
-          s_dx[warp][lane] = s_dx[warp][32 + lane];
-          s_dy[warp][lane] = s_dy[warp][32 + lane];
-          s_dz[warp][lane] = s_dz[warp][32 + lane];
-          s_j[warp][lane] = s_j[warp][32 + lane];
+          qu.dx[warp][lane] = qu.dx[warp][32 + lane];
+          qu.dy[warp][lane] = qu.dy[warp][32 + lane];
+          qu.dz[warp][lane] = qu.dz[warp][32 + lane];
+          qu.j[warp][lane] = qu.j[warp][32 + lane];
         }
         __syncwarp();
         qn = rem;
@@ -474,11 +452,14 @@ k_verlet_fused_f64(PairParams pp, int n, const double* __restrict__ x,
 }
 
 // ---------------------------------------------------------------------------
-// RBL list emitters (same classification as the fused kernels; rows of cap).
-// Thread per atom: used for parity checks and the drop-in list op, not per step.
+// RBL list emitter (same classification as the fused kernels; rows of cap):
+// core = list predicate r^2 < r_core^2 - EPS; shell = hashed
+// r_core^2 - EPS <= r^2 < cut_off^2 - EPS.  Thread per atom: parity checks and
+// the engine's list export, not the per-step path.
 // ---------------------------------------------------------------------------
-__global__ void k_rbl_lists(PairParams pp, int n, const double* __restrict__ x,
-                            const double* __restrict__ y, const double* __restrict__ z,
+__global__ void k_rbl_lists(PairParams pp, int n, const uint4* __restrict__ atoms,
+                            const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z,
                             const unsigned long long* __restrict__ key_a,
                             const unsigned long long* __restrict__ key_b, int epoch,
                             const int* __restrict__ cand_count, const int* __restrict__ cand,
@@ -491,37 +472,7 @@ __global__ void k_rbl_lists(PairParams pp, int n, const double* __restrict__ x,
   for (int t = 0; t < cand_count[i]; ++t) {
     const int j = cand[(size_t)i * cap + t];
     if (j == i) continue;
-    const double d2 = dist2_list(pp.box, x[i], y[i], z[i], x[j], y[j], z[j]);
-    if (d2 < pp.core2_list)
-      core[(size_t)i * cap + nc++] = j;
-    else if (d2 < pp.force2_list && rbl_selected(ea, key_b[j], pp.div))
-      shell[(size_t)i * cap + ns++] = j;
-  }
-  core_count[i] = nc;
-  shell_count[i] = ns;
-}
-
-__global__ void k_rbl_lists_mixed(PairParams pp, MixedScale ms, int n,
-                                  const uint4* __restrict__ atoms,
-                                  const unsigned long long* __restrict__ key_a,
-                                  const unsigned long long* __restrict__ key_b, int epoch,
-                                  const int* __restrict__ cand_count,
-                                  const int* __restrict__ cand, int cap,
-                                  int* __restrict__ core_count, int* __restrict__ core,
-                                  int* __restrict__ shell_count, int* __restrict__ shell) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
-  const uint4 ai = atoms[i];
-  int nc = 0, ns = 0;
-  for (int t = 0; t < cand_count[i]; ++t) {
-    const int j = cand[(size_t)i * cap + t];
-    if (j == i) continue;
-    const uint4 aj = atoms[j];
-    const double ex = (double)(int)(aj.x - ai.x) * ms.s[0];
-    const double ey = (double)(int)(aj.y - ai.y) * ms.s[1];
-    const double ez = (double)(int)(aj.z - ai.z) * ms.s[2];
-    const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+    const double d2 = exact_d2(pp, x, y, z, i, j);
     if (d2 < pp.core2_list)
       core[(size_t)i * cap + nc++] = j;
     else if (d2 < pp.force2_list && rbl_selected(ea, key_b[j], pp.div))
@@ -729,6 +680,17 @@ __global__ void k_sub_mean(int n, double* __restrict__ fx, double* __restrict__ 
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
+IntScreen make_screen(double C, double L, double band) {
+  // |d|^2 * s^2 < C  <=>  |d|^2 < C / s^2, s = L / 2^32; band in r^2 units
+  const long double scale = 18446744073709551616.0L / ((long double)L * (long double)L);
+  const long double K = (long double)C * scale, B = (long double)band * scale;
+  IntScreen t;
+  const long double lo = floorl(K - B), hi = ceill(K + B);
+  t.lo = lo <= 0.0L ? 0ULL : (unsigned long long)lo;
+  t.hi = hi >= 18446744073709551615.0L ? ~0ULL : (unsigned long long)hi;
+  return t;
+}
+
 int rbl_fused_blocks(int n) {
   const int target = sm_count() * 8;  // 8 resident 256-thread blocks per SM
   int b = (n + PAIR_WARPS - 1) / PAIR_WARPS;
@@ -736,66 +698,48 @@ int rbl_fused_blocks(int n) {
   return b < 1 ? 1 : b;
 }
 
-int launch_rbl_fused_f64(const PairParams& pp, int n, const double* x, const double* y,
-                         const double* z, const double* q, const int* type,
-                         const unsigned long long* key_a, const unsigned long long* key_b,
-                         int epoch, const int* cand_count, const int* cand, int cap,
-                         double* fx, double* fy, double* fz, double* fpart, int nblocks,
-                         cudaStream_t st) {
+int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
+                     const double* x, const double* y, const double* z, const double* q,
+                     const int* type, const unsigned long long* key_a,
+                     const unsigned long long* key_b, int epoch, const int* cand_count,
+                     const int* cand, int cap, double* fx, double* fy, double* fz, double* fpart,
+                     int nblocks, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  k_rbl_fused_f64<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, x, y, z, q, type, key_a, key_b, epoch,
-                                                  cand_count, cand, cap, fx, fy, fz, fpart);
+  if (mixed)
+    k_rbl_fused<true><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, key_a,
+                                                      key_b, epoch, cand_count, cand, cap, fx, fy,
+                                                      fz, fpart);
+  else
+    k_rbl_fused<false><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, key_a,
+                                                       key_b, epoch, cand_count, cand, cap, fx, fy,
+                                                       fz, fpart);
   count_launch();
-  return check_launch("rbl_fused_f64");
+  return check_launch(mixed ? "rbl_fused_mixed" : "rbl_fused_f64");
 }
 
-int launch_rbl_fused_mixed(const PairParams& pp, const MixedScale& ms, int n, const uint4* atoms,
-                           const int* type, const unsigned long long* key_a,
-                           const unsigned long long* key_b, int epoch, const int* cand_count,
-                           const int* cand, int cap, double* fx, double* fy, double* fz,
-                           double* fpart, int nblocks, cudaStream_t st) {
-  if (n <= 0) return RBX_OK;
-  k_rbl_fused_mixed<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, ms, n, atoms, type, key_a, key_b, epoch,
-                                                    cand_count, cand, cap, fx, fy, fz, fpart);
-  count_launch();
-  return check_launch("rbl_fused_mixed");
-}
-
-int launch_verlet_fused_f64(const PairParams& pp, int n, const double* x, const double* y,
-                            const double* z, const double* q, const int* type,
+int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, const double* x,
+                            const double* y, const double* z, const double* q, const int* type,
                             const int* cand_count, const int* cand, int cap, double* fx,
                             double* fy, double* fz, double* fpart, double* epart, int nblocks,
                             cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  k_verlet_fused_f64<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, x, y, z, q, type, cand_count, cand,
-                                                     cap, fx, fy, fz, fpart, epart);
+  k_verlet_fused_f64<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, cand_count,
+                                                     cand, cap, fx, fy, fz, fpart, epart);
   count_launch();
   return check_launch("verlet_fused_f64");
 }
 
-int launch_rbl_lists(const PairParams& pp, int n, const double* x, const double* y,
-                     const double* z, const unsigned long long* key_a,
+int launch_rbl_lists(const PairParams& pp, int n, const uint4* atoms, const double* x,
+                     const double* y, const double* z, const unsigned long long* key_a,
                      const unsigned long long* key_b, int epoch, const int* cand_count,
                      const int* cand, int cap, int* core_count, int* core, int* shell_count,
                      int* shell, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  k_rbl_lists<<<(n + 127) / 128, 128, 0, st>>>(pp, n, x, y, z, key_a, key_b, epoch, cand_count,
-                                               cand, cap, core_count, core, shell_count, shell);
+  k_rbl_lists<<<(n + 127) / 128, 128, 0, st>>>(pp, n, atoms, x, y, z, key_a, key_b, epoch,
+                                               cand_count, cand, cap, core_count, core,
+                                               shell_count, shell);
   count_launch();
   return check_launch("rbl_lists");
-}
-
-int launch_rbl_lists_mixed(const PairParams& pp, const MixedScale& ms, int n, const uint4* atoms,
-                           const unsigned long long* key_a, const unsigned long long* key_b,
-                           int epoch, const int* cand_count, const int* cand, int cap,
-                           int* core_count, int* core, int* shell_count, int* shell,
-                           cudaStream_t st) {
-  if (n <= 0) return RBX_OK;
-  k_rbl_lists_mixed<<<(n + 127) / 128, 128, 0, st>>>(pp, ms, n, atoms, key_a, key_b, epoch,
-                                                     cand_count, cand, cap, core_count, core,
-                                                     shell_count, shell);
-  count_launch();
-  return check_launch("rbl_lists_mixed");
 }
 
 int launch_rbl_keys(int n, const int* gid, unsigned long long* key_a, unsigned long long* key_b,

@@ -82,8 +82,8 @@ k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kz
       r += s_re[w][s];
       im += s_im[w][s];
     }
-    part_re[(size_t)blockIdx.x * p + k] = r;
-    part_im[(size_t)blockIdx.x * p + k] = im;
+    part_re[(size_t)k * gridDim.x + blockIdx.x] = r;
+    part_im[(size_t)k * gridDim.x + blockIdx.x] = im;
   }
 }
 
@@ -166,20 +166,22 @@ k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
       r += s_re[w][s];
       im += s_im[w][s];
     }
-    part_re[(size_t)blockIdx.x * p + k] = r;
-    part_im[(size_t)blockIdx.x * p + k] = im;
+    part_re[(size_t)k * gridDim.x + blockIdx.x] = r;
+    part_im[(size_t)k * gridDim.x + blockIdx.x] = im;
   }
 }
 
 // ---------------------------------------------------------------------------
-// Finalize (one block): rho_p = sum over blocks in fixed order; optional
-// energy/virial (ComputeRBEVirial0, kspace_calculator_op.hip.cu:573-674) with a
-// deterministic tree; force table tab[p] = {kx, ky, kz, coef*Re, coef*Im} with
-// coef = -4 pi qqr2e S / (P V k^2); optional mean of a force partial array.
+// Finalize (one block of 1024 threads): rho_p = sum over the k-major partials
+// (one warp per k, fixed tree); optional energy/virial (ComputeRBEVirial0,
+// kspace_calculator_op.hip.cu:573-674) summed over k in fixed order; force
+// table tab[p] = {kx, ky, kz, coef*Re, coef*Im} with coef = -4 pi qqr2e S /
+// (P V k^2); optional mean of a force-partial array (RBL mean removal).
 // ---------------------------------------------------------------------------
 constexpr int FIN_BLOCK = 256;
+constexpr int FIN_WIDE = 1024;
 
-__global__ void __launch_bounds__(FIN_BLOCK)
+__global__ void __launch_bounds__(FIN_WIDE)
 k_rbe_finalize(int p, int nparts, const double* __restrict__ part_re,
                const double* __restrict__ part_im, const double* __restrict__ mx,
                const double* __restrict__ my, const double* __restrict__ mz, double Lx,
@@ -188,66 +190,81 @@ k_rbe_finalize(int p, int nparts, const double* __restrict__ part_re,
                double* __restrict__ energy, double* __restrict__ virial,
                KTab* __restrict__ tab, int mean_parts, const double* __restrict__ fpart,
                double n_atoms, double* __restrict__ mean_out) {
-  __shared__ double sh[FIN_BLOCK / 32];
+  __shared__ double s_e[7][FIN_WIDE / 32];
+  __shared__ double sh[FIN_WIDE / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const double V = Lx * Ly * Lz;
   const double coef = (2 * RBX_PI * S) / (p * V);
   const double fcoef = -4 * RBX_PI * qqr2e * S / p;
-  double e = 0.0, w[6] = {0, 0, 0, 0, 0, 0};
-  for (int k = threadIdx.x; k < p; k += FIN_BLOCK) {
+  // per-warp running sums of the per-k energy/virial terms, k in increasing order
+  double we[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int k = warp; k < p; k += FIN_WIDE / 32) {
     double r = 0.0, im = 0.0;
-    for (int b = 0; b < nparts; ++b) {
-      r += part_re[(size_t)b * p + k];
-      im += part_im[(size_t)b * p + k];
+    const double* pr = part_re + (size_t)k * nparts;
+    const double* pi = part_im + (size_t)k * nparts;
+    for (int b = lane; b < nparts; b += 32) {
+      r += pr[b];
+      im += pi[b];
     }
-    if (rho_re) {
-      rho_re[k] = r;
-      rho_im[k] = im;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      r += __shfl_xor_sync(0xffffffffu, r, o);
+      im += __shfl_xor_sync(0xffffffffu, im, o);
     }
-    const double kx = 2 * RBX_PI * mx[k] / Lx;
-    const double ky = 2 * RBX_PI * my[k] / Ly;
-    const double kz = 2 * RBX_PI * mz[k] / Lz;
-    const double k2 = kx * kx + ky * ky + kz * kz;
-    const double rho2 = r * r + im * im;
-    const double base = coef * rho2 / k2;
-    e += base;
-    const double inner = (1.0 / (4 * alpha)) + (1.0 / k2);
-    w[0] += base * (1.0 - 2 * kx * kx * inner);
-    w[1] += base * (1.0 - 2 * ky * ky * inner);
-    w[2] += base * (1.0 - 2 * kz * kz * inner);
-    w[3] += base * (-2 * kx * ky * inner);
-    w[4] += base * (-2 * kx * kz * inner);
-    w[5] += base * (-2 * ky * kz * inner);
-    if (tab) {
-      const double c = fcoef / (V * k2);
-      KTab t;
-      t.kx = kx;
-      t.ky = ky;
-      t.kz = kz;
-      t.a = c * r;
-      t.b = c * im;
-      t.m[0] = (int)mx[k];
-      t.m[1] = (int)my[k];
-      t.m[2] = (int)mz[k];
-      t.m[3] = 0;
-      tab[k] = t;
+    if (lane == 0) {
+      if (rho_re) {
+        rho_re[k] = r;
+        rho_im[k] = im;
+      }
+      const double kx = 2 * RBX_PI * mx[k] / Lx;
+      const double ky = 2 * RBX_PI * my[k] / Ly;
+      const double kz = 2 * RBX_PI * mz[k] / Lz;
+      const double k2 = kx * kx + ky * ky + kz * kz;
+      const double rho2 = r * r + im * im;
+      const double base = coef * rho2 / k2;
+      const double inner = (1.0 / (4 * alpha)) + (1.0 / k2);
+      we[0] += base;
+      we[1] += base * (1.0 - 2 * kx * kx * inner);
+      we[2] += base * (1.0 - 2 * ky * ky * inner);
+      we[3] += base * (1.0 - 2 * kz * kz * inner);
+      we[4] += base * (-2 * kx * ky * inner);
+      we[5] += base * (-2 * kx * kz * inner);
+      we[6] += base * (-2 * ky * kz * inner);
+      if (tab) {
+        const double c = fcoef / (V * k2);
+        KTab t;
+        t.kx = kx;
+        t.ky = ky;
+        t.kz = kz;
+        t.a = c * r;
+        t.b = c * im;
+        t.m[0] = (int)mx[k];
+        t.m[1] = (int)my[k];
+        t.m[2] = (int)mz[k];
+        t.m[3] = 0;
+        tab[k] = t;
+      }
     }
   }
   if (energy) {
-    const double et = block_sum_det<FIN_BLOCK>(e, sh);
-    double wt[6];
-    for (int c = 0; c < 6; ++c) wt[c] = block_sum_det<FIN_BLOCK>(w[c], sh);
+    if (lane == 0)
+      for (int c = 0; c < 7; ++c) s_e[c][warp] = we[c];
+    __syncthreads();
     if (threadIdx.x == 0) {
+      double t[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int w = 0; w < FIN_WIDE / 32; ++w)
+        for (int c = 0; c < 7; ++c) t[c] += s_e[c][w];
       const double MY_PIS = 1.77245385090551602729, MY_PI2 = 1.57079632679489661923;
-      const double etot = et - (sqrt(alpha) * qsq / MY_PIS + MY_PI2 * qsum * qsum / (alpha * V));
+      const double etot = t[0] - (sqrt(alpha) * qsq / MY_PIS + MY_PI2 * qsum * qsum / (alpha * V));
       *energy = etot * qqr2e;
-      for (int c = 0; c < 6; ++c) virial[c] = wt[c] * qqr2e;
+      for (int c = 0; c < 6; ++c) virial[c] = t[1 + c] * qqr2e;
     }
   }
   if (mean_out) {
     for (int d = 0; d < 3; ++d) {
       double s = 0.0;
-      for (int b = threadIdx.x; b < mean_parts; b += FIN_BLOCK) s += fpart[(size_t)b * 3 + d];
-      s = block_sum_det<FIN_BLOCK>(s, sh);
+      for (int b = threadIdx.x; b < mean_parts; b += FIN_WIDE) s += fpart[(size_t)b * 3 + d];
+      s = block_sum_det<FIN_WIDE>(s, sh);
       if (threadIdx.x == 0) mean_out[d] = s / n_atoms;
     }
   }
@@ -397,17 +414,20 @@ k_rbe_force_mixed(int n, int p, const KTab* __restrict__ tab, const uint4* __res
 // Philox k-sampler: one thread per sample; per-axis inverse-CDF tables built
 // on the host (order m = 0, +1, -1, +2, -2, ...).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int table_pick(const double* w, int cnt, double total, uint64_t u53) {
+// cdf[t] = w[0] + ... + w[t], accumulated left to right on the host exactly as
+// the oracle's linear scan accumulates, so the first t with target < cdf[t]
+// (binary search) is the oracle's pick.
+__device__ __forceinline__ int table_pick(const double* cdf, int cnt, double total, uint64_t u53) {
   const double target = (double)u53 * (1.0 / 9007199254740992.0) * total;
-  double acc = 0.0;
-  int idx = cnt - 1;
-  for (int t = 0; t < cnt; ++t) {
-    acc = __dadd_rn(acc, w[t]);
-    if (target < acc) {
-      idx = t;
-      break;
-    }
+  int lo = 0, hi = cnt - 1;  // first index with target < cdf[idx], else cnt - 1
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (target < cdf[mid])
+      hi = mid;
+    else
+      lo = mid + 1;
   }
+  const int idx = lo;
   if (idx == 0) return 0;
   return (idx & 1) ? (idx + 1) / 2 : -(idx / 2);
 }
@@ -423,22 +443,13 @@ __global__ void k_rbe_sample(int p, const double* __restrict__ tables, int c0, i
   const double* w1 = tables + c0;
   const double* w2 = tables + c0 + c1;
   for (int a = 0; a < 64; ++a) {
-    uint32_t o[8];
     uint32_t c[4] = {(uint32_t)s, (uint32_t)(2 * a), (uint32_t)step, (uint32_t)(step >> 32)};
     philox4x32_10(c, key0, key1);
-    o[0] = c[0];
-    o[1] = c[1];
-    o[2] = c[2];
-    o[3] = c[3];
     uint32_t d[4] = {(uint32_t)s, (uint32_t)(2 * a + 1), (uint32_t)step, (uint32_t)(step >> 32)};
     philox4x32_10(d, key0, key1);
-    o[4] = d[0];
-    o[5] = d[1];
-    o[6] = d[2];
-    o[7] = d[3];
-    const int m0 = table_pick(w0, c0, t0, ((((uint64_t)o[0]) << 32) | o[1]) >> 11);
-    const int m1 = table_pick(w1, c1, t1, ((((uint64_t)o[2]) << 32) | o[3]) >> 11);
-    const int m2 = table_pick(w2, c2, t2, ((((uint64_t)o[4]) << 32) | o[5]) >> 11);
+    const int m0 = table_pick(w0, c0, t0, ((((uint64_t)c[0]) << 32) | c[1]) >> 11);
+    const int m1 = table_pick(w1, c1, t1, ((((uint64_t)c[2]) << 32) | c[3]) >> 11);
+    const int m2 = table_pick(w2, c2, t2, ((((uint64_t)d[0]) << 32) | d[1]) >> 11);
     if (m0 != 0 || m1 != 0 || m2 != 0) {
       if (mx) {
         mx[s] = m0;
@@ -583,7 +594,7 @@ int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
                         double qsum, double* rho_re, double* rho_im, double* energy,
                         double* virial, KTab* tab, int mean_parts, const double* fpart,
                         int n_atoms, double* mean_out, cudaStream_t st) {
-  k_rbe_finalize<<<1, FIN_BLOCK, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
+  k_rbe_finalize<<<1, FIN_WIDE, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
                                           b.len[1], b.len[2], alpha, S, qqr2e, qsq, qsum, rho_re,
                                           rho_im, energy, virial, tab, mean_parts, fpart,
                                           (double)n_atoms, mean_out);
@@ -635,7 +646,7 @@ int launch_rbe_sample(int p, const double* tables, const int cnt[3], const doubl
                       uint64_t seed, int64_t step, double* mx, double* my, double* mz, int* mi,
                       int* status, cudaStream_t st) {
   if (p <= 0) return RBX_OK;
-  k_rbe_sample<<<(p + 127) / 128, 128, 0, st>>>(p, tables, cnt[0], cnt[1], cnt[2], tot[0], tot[1],
+  k_rbe_sample<<<(p + 31) / 32, 32, 0, st>>>(p, tables, cnt[0], cnt[1], cnt[2], tot[0], tot[1],
                                                 tot[2], (uint32_t)seed, (uint32_t)(seed >> 32),
                                                 (uint64_t)step, mx, my, mz, mi, status);
   count_launch();

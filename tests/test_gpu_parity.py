@@ -20,6 +20,18 @@ def _t(torch, a, dtype=None):
     return torch.as_tensor(a).to(dtype=dtype, device="cuda").contiguous()
 
 
+def _subcell_key(x, y, z, lo, hi, dims):
+    """In-cell order of rbx_cells_sort: 4x4x4 Morton sub-cell code, then old index."""
+    code = np.zeros(len(x), dtype=np.int64)
+    for d, v in enumerate((x, y, z)):
+        f = (v - lo[d]) * (dims[d] / (hi[d] - lo[d]))
+        c = np.clip(np.floor(f), 0, dims[d] - 1)
+        sub = np.clip(np.floor((f - c) * 4.0), 0, 3).astype(np.int64)
+        for bit in range(2):
+            code |= ((sub >> bit) & 1) << (3 * bit + d)
+    return (code << 26) | np.arange(len(x))
+
+
 def _sorted(oracle, s, cutoff):
     box = oracle.Box.make(s["lo"], s["hi"])
     x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
@@ -56,8 +68,11 @@ def test_rbe_sample_bit_exact(cuda, rbx, oracle, sys4k, p):
 @pytest.mark.parametrize("n,p", [(4000, 100), (4000, 400), (20000, 100), (1, 7), (257, 33)])
 def test_rbe_kspace_ops(cuda, rbx, oracle, n, p):
     s = systems.lj_electrolyte(max(n, 2), seed=n + p)
-    if n == 1:
-        s = {k: (v[:1] if isinstance(v, np.ndarray) and len(v) == 2 else v) for k, v in s.items()}
+    if n == 1:  # a single ion in a 17-sigma box
+        s = systems.lj_electrolyte(4000, seed=n + p)
+        s = {k: (v[:1] if isinstance(v, np.ndarray) and len(v) == 4000 else v)
+             for k, v in s.items()}
+        s["q"] = np.array([1.0])
         s["n"] = 1
     box = oracle.Box.make(s["lo"], s["hi"])
     rbox = rbx.Box.make(s["lo"], s["hi"])
@@ -125,8 +140,10 @@ def test_cells_and_full_list(cuda, rbx, oracle, n):
     hc = cos.cpu().numpy()
     assert np.all(np.diff(hc) >= 0)
     hs = cst.cpu().numpy()
+    key = _subcell_key(x, y, z, s["lo"], s["hi"], dims)
     for c in range(ncell):
-        assert np.all(np.diff(hp[hs[c]:hs[c + 1]]) > 0)  # stable inside a cell
+        seg = hp[hs[c]:hs[c + 1]]
+        assert np.all(np.diff(key[seg]) > 0)  # (Morton sub-cell, old index) ascending
     xs = [_t(cuda, a[hp]) for a in (x, y, z)]
     cap = 800
     cnt = cuda.zeros(n, dtype=cuda.int32, device="cuda")
