@@ -217,12 +217,15 @@ int rbx_engine::init() {
   pp.cubic = dbox.len[0] == dbox.len[1] && dbox.len[1] == dbox.len[2];
   if (pp.cubic) {
     const double L = dbox.len[0];
-    const double band = std::max(1e-5, 128.0 * (L / 4294967296.0) * (rcs + 1.0));
-    pp.sc_eps = make_screen(RBX_EPSILON, L, band);
-    pp.sc_core = make_screen(pp.core2_list, L, band);
-    pp.sc_rs = make_screen(pp.rs2, L, band);
-    pp.sc_force = make_screen(pp.force2_list, L, band);
-    pp.sc_rc = make_screen(pp.rc2, L, band);
+    // FP32 |d|^2 carries < 1e-6 relative rounding plus < 6 s |d| of quantisation
+    // error; the band is several times both
+    const double qerr = 64.0 * (L / 4294967296.0) * (rcs + 1.0);
+    auto band = [&](double C) { return 1e-4 + 8e-6 * C + qerr; };
+    pp.sc_eps = make_screen(RBX_EPSILON, L, std::min(band(RBX_EPSILON), 0.5 * RBX_EPSILON));
+    pp.sc_core = make_screen(pp.core2_list, L, band(pp.core2_list));
+    pp.sc_rs = make_screen(pp.rs2, L, band(pp.rs2));
+    pp.sc_force = make_screen(pp.force2_list, L, band(pp.force2_list));
+    pp.sc_rc = make_screen(pp.rc2, L, band(pp.rc2));
   }
   return RBX_OK;
 }

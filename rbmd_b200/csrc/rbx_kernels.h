@@ -67,10 +67,11 @@ int launch_ewald(const DBox& b, int n, const int kmax[3], double alpha, double q
 int rbe_axis_table(double L, double alpha, double* w, int max_entries, double* total);
 
 // ---- real space (rbx_pair.cu) ----
-// Integer screen of "r^2 < C" on fixed-point |d|^2: true at or below lo, false
-// at or above hi, undecided in between (the FP64 predicate decides).
+// Screen of "r^2 < C" on the fixed-point |d|^2 (FP32, units of s^2 with
+// s = L/2^32): decided below lo and at or above hi, undecided in between (the
+// FP64 predicate decides).
 struct IntScreen {
-  unsigned long long lo, hi;
+  float lo, hi;
 };
 // Build the screen for threshold C (r^2 units) on a cubic box of edge L.
 IntScreen make_screen(double C, double L, double band);

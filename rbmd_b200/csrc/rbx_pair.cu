@@ -99,21 +99,18 @@ __device__ __forceinline__ void write_block_partial(double (*s_acc)[3], double* 
 // Candidate classification shared by both forms.
 //
 // On a cubic box the pair vector in fixed point, d = u_j - u_i (wrapped int32),
-// is the exact minimum image, and s^2 * |d|^2 differs from the FP64 r^2 of the
-// reference predicate by far less than the guard band around each threshold.
-// Each predicate "r^2 < C" is decided in 64-bit integers when |d|^2 is outside
-// [lo, hi]; inside it, the reference's FP64 expression (CaculateDistance:
-// i minus j, min image, no FMA) decides.  The outcome is therefore identical
-// to the FP64 predicate on every pair, in both precision forms.
+// is the exact minimum image of the FP64 pair vector to within 3 units of
+// s = L/2^32 per coordinate.  |d|^2 is formed in FP32 (in units of s^2) and
+// each predicate "r^2 < C" is decided when |d|^2 lies outside a guard band
+// [lo, hi] around C/s^2 that exceeds every rounding and quantisation error;
+// inside the band the reference's FP64 expression (CaculateDistance: i minus
+// j, min image, no FMA) decides.  The outcome is therefore identical to the
+// FP64 predicate on every pair, in both precision forms.
 // ---------------------------------------------------------------------------
 struct Classified {
   bool core_active;    // core list and lj126_rs window (r^2 > EPS)
   bool shell_window;   // shell list and rcs window (r_core^2 < r^2 < cut_off^2)
 };
-
-__device__ __forceinline__ int screen_lt(unsigned long long d2i, const IntScreen& t) {
-  return d2i <= t.lo ? 1 : (d2i >= t.hi ? 0 : -1);
-}
 
 __device__ __forceinline__ Classified classify_exact(double d2, const PairParams& pp) {
   Classified c;
@@ -130,41 +127,63 @@ __device__ __forceinline__ double exact_d2(const PairParams& pp, const double* _
                     __ldg(y + j), __ldg(z + j));
 }
 
-__device__ __forceinline__ Classified classify(const PairParams& pp, const uint4& ai,
-                                               const uint4& aj, const double* __restrict__ x,
-                                               const double* __restrict__ y,
-                                               const double* __restrict__ z, int i, int j) {
-  if (pp.cubic) {
-    const int dx = (int)(aj.x - ai.x), dy = (int)(aj.y - ai.y), dz = (int)(aj.z - ai.z);
-    const unsigned long long d2i = (unsigned long long)((long long)dx * dx) +
-                                   (unsigned long long)((long long)dy * dy) +
-                                   (unsigned long long)((long long)dz * dz);
-    if (d2i >= pp.sc_force.hi) return Classified{false, false};  // beyond the shell
-    const int A = screen_lt(d2i, pp.sc_core), B = screen_lt(d2i, pp.sc_force);
-    const int E = screen_lt(d2i, pp.sc_eps), R = screen_lt(d2i, pp.sc_rs);
-    if ((A | B | E | R) >= 0) {
-      Classified c;
-      c.core_active = A && !E;
-      c.shell_window = !A && B && !R;
-      return c;
-    }
-  }
-  return classify_exact(exact_d2(pp, x, y, z, i, j), pp);
+// Screened classification; *unsure is set when a threshold band is hit.
+__device__ __forceinline__ Classified classify_screen(const PairParams& pp, float d2s,
+                                                      bool* unsure) {
+  const bool A = d2s < pp.sc_core.lo, nA = d2s >= pp.sc_core.hi;
+  const bool B = d2s < pp.sc_force.lo, nB = d2s >= pp.sc_force.hi;
+  const bool E = d2s > pp.sc_eps.hi, nE = d2s <= pp.sc_eps.lo;
+  const bool D = d2s > pp.sc_rs.hi, nD = d2s <= pp.sc_rs.lo;
+  // undecided predicates matter only where they can change the outcome
+  *unsure = (!A && !nA) || (nA && !B && !nB) || (A && !E && !nE) || (nA && B && !D && !nD);
+  Classified c;
+  c.core_active = A && E;
+  c.shell_window = nA && B && D;
+  return c;
 }
 
-template <typename T>
-struct PairQueue {
-  T dx[PAIR_WARPS][QCAP], dy[PAIR_WARPS][QCAP], dz[PAIR_WARPS][QCAP];
-  int j[PAIR_WARPS][QCAP];
+__device__ __forceinline__ float fixed_d2(const uint4& ai, const uint4& aj) {
+  const float dx = (float)(int)(aj.x - ai.x), dy = (float)(int)(aj.y - ai.y),
+              dz = (float)(int)(aj.z - ai.z);
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+// Per-warp queue of force-carrying pairs.  Mixed form: the FP32 pair vector
+// and q_j are captured at push time; plain FP64 form: only j is queued and the
+// drain gathers the FP64 position, charge and type of all 32 pairs at once.
+constexpr int RBL_UNROLL = 4;                    // 32-candidate chunks per batch
+constexpr int RBL_QCAP = 32 + 32 * RBL_UNROLL;   // queue stays below 32 between batches
+
+struct QueueMixed {
+  float4 v[PAIR_WARPS][RBL_QCAP];  // dx, dy, dz, q_j
+  int j[PAIR_WARPS][RBL_QCAP];
 };
+struct QueueF64 {
+  int j[PAIR_WARPS][RBL_QCAP];
+};
+
+// LJ 12-6 force/r in FP32 with one fast reciprocal (mixed form only).
+__device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
+  const float r2i = __fdividef(1.0f, d2);
+  const float sd6 = s6 * (r2i * r2i * r2i);
+  return -24.f * eps_ij * ((2.f * sd6 - 1.f) * sd6) * r2i;
+}
 
 // ---------------------------------------------------------------------------
 // Fused RBL filter + pair force.  MIXED = false: plain FP64 (pair vector and
 // force math in FP64 from the FP64 positions).  MIXED = true: FP32 force math
-// on the exact fixed-point pair vector.
+// on the exact fixed-point pair vector.  POW2: freq is a power of two, so the
+// batch test is a mask.
+//
+// The warp walks atom i's candidate row in batches of RBL_UNROLL x 32: index
+// loads and neighbour-record gathers of a batch are all issued before any is
+// consumed; classification and the shell hash are branch-free; pairs inside a
+// threshold guard band are settled once per batch with the FP64 predicate;
+// force-carrying pairs are appended to a per-warp queue and consumed 32 at a
+// time from its tail.
 // ---------------------------------------------------------------------------
-template <bool MIXED>
-__global__ void __launch_bounds__(PAIR_BLOCK)
+template <bool MIXED, bool POW2>
+__global__ void __launch_bounds__(PAIR_BLOCK, 3)
 k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
             const double* __restrict__ y, const double* __restrict__ z,
             const double* __restrict__ q, const int* __restrict__ type,
@@ -174,8 +193,9 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
             double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
             double* __restrict__ fpart) {
   using T = typename std::conditional<MIXED, float, double>::type;
+  using Queue = typename std::conditional<MIXED, QueueMixed, QueueF64>::type;
   __shared__ TypeTables tt;
-  __shared__ PairQueue<T> qu;
+  __shared__ Queue qu;
   __shared__ double s_acc[PAIR_WARPS][3];
   __shared__ float f_eps[MAX_TYPES_SMEM * MAX_TYPES_SMEM], f_s6[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
   load_type_tables(tt, pp);
@@ -188,6 +208,9 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = lanemask_lt();
+  const unsigned long long fmask = (unsigned long long)(pp.freq - 1);
+  const float alpha_f = (float)pp.alpha, sqa_f = (float)pp.sqrt_alpha, qqr2e_f = (float)pp.qqr2e;
+  const T freq_t = (T)pp.freq;
   double acc0 = 0, acc1 = 0, acc2 = 0;
   const int nt = pp.ntypes;
   for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += gridDim.x * PAIR_WARPS) {
@@ -200,88 +223,98 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
     const int* row = cand + (size_t)i * cap;
     int qn = 0;
     T fxa = 0, fya = 0, fza = 0;
-    for (int k0 = 0;;) {
-      const bool more = k0 < cnt;
-      if (more) {
-        const int k = k0 + lane;
-        bool push = false;
-        int code = 0, j = i;
-        uint4 aj = ai;
-        if (k < cnt) {
-          j = __ldg(row + k);
-          if (j != i) {
-            aj = __ldg(atoms + j);
-            const Classified c = classify(pp, ai, aj, x, y, z, i, j);
-            if (c.core_active) {
-              push = true;
-              code = j;
-            } else if (c.shell_window) {
-              push = rbl_selected(ea, __ldg(key_b + j), pp.div);  // shell batch hash
-              code = j | (int)0x80000000;
-            }
+
+    // force from queue slot `slot` (all 32 lanes take one pair each)
+    auto pair_force = [&](int slot) {
+      const int c = qu.j[warp][slot];
+      const int j = c & 0x7fffffff;
+      const int tj = __ldg(type + j);
+      if (MIXED) {
+        const float4 v = reinterpret_cast<const QueueMixed&>(qu).v[warp][slot];
+        const float d2 = fmaf(v.x, v.x, fmaf(v.y, v.y, v.z * v.z));
+        const float qq = (float)qi * v.w;
+        float f = lj_f32_fast(f_eps[ti * nt + tj], f_s6[ti * nt + tj], d2);
+        if (qq != 0.f) f += coul_f32(alpha_f, sqa_f, qqr2e_f, qq, d2);
+        if (c < 0) f *= (float)freq_t;
+        fxa += (T)(f * v.x);
+        fya += (T)(f * v.y);
+        fza += (T)(f * v.z);
+      } else {
+        // r_j - r_i, MinImageDistance (box.h:51-73)
+        const double ddx = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
+        const double ddy = min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
+        const double ddz = min_image1(__ldg(z + j) - zi, pp.box.len[2], pp.box.half[2]);
+        const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        const double qq = (double)qi * __ldg(q + j);
+        double f = lj_f64(tt.eps[ti * nt + tj], tt.s6[ti * nt + tj], d2);
+        if (qq != 0.0) f += coul_f64(pp.alpha, pp.sqrt_alpha, pp.qqr2e, qq, d2);
+        if (c < 0) f *= (double)freq_t;
+        fxa += (T)(f * ddx);
+        fya += (T)(f * ddy);
+        fza += (T)(f * ddz);
+      }
+    };
+
+    for (int k0 = 0; k0 < cnt; k0 += 32 * RBL_UNROLL) {
+      int jj[RBL_UNROLL];
+      uint4 aa[RBL_UNROLL];
+#pragma unroll
+      for (int u = 0; u < RBL_UNROLL; ++u) {
+        const int k = k0 + u * 32 + lane;
+        jj[u] = k < cnt ? __ldg(row + k) : i;
+      }
+#pragma unroll
+      for (int u = 0; u < RBL_UNROLL; ++u) aa[u] = __ldg(atoms + jj[u]);
+      unsigned core_bits = 0, shell_bits = 0, sel_bits = 0, unsure_bits = 0;
+#pragma unroll
+      for (int u = 0; u < RBL_UNROLL; ++u) {
+        const bool valid = jj[u] != i;
+        bool unsure = !pp.cubic;
+        Classified c{false, false};
+        if (pp.cubic) c = classify_screen(pp, fixed_d2(ai, aa[u]), &unsure);
+        // shell batch hash (RblShellSampleSelected)
+        const unsigned long long h = rbl_mix(ea ^ __ldg(key_b + jj[u]));
+        const bool sel = POW2 ? (h & fmask) == 0ULL : divisible(h, pp.div);
+        core_bits |= (unsigned)(valid && c.core_active) << u;
+        shell_bits |= (unsigned)(valid && c.shell_window) << u;
+        sel_bits |= (unsigned)sel << u;
+        unsure_bits |= (unsigned)(valid && unsure) << u;
+      }
+      if (__any_sync(0xffffffffu, unsure_bits != 0)) {  // rare: FP64 predicate decides
+#pragma unroll
+        for (int u = 0; u < RBL_UNROLL; ++u) {
+          if (unsure_bits & (1u << u)) {
+            const Classified c = classify_exact(exact_d2(pp, x, y, z, i, jj[u]), pp);
+            core_bits = (core_bits & ~(1u << u)) | ((unsigned)c.core_active << u);
+            shell_bits = (shell_bits & ~(1u << u)) | ((unsigned)c.shell_window << u);
           }
         }
+      }
+      const unsigned push_bits = core_bits | (shell_bits & sel_bits);
+#pragma unroll
+      for (int u = 0; u < RBL_UNROLL; ++u) {
+        const bool push = (push_bits >> u) & 1u;
         const unsigned m = __ballot_sync(0xffffffffu, push);
         if (push) {
           const int pos = qn + __popc(m & lt);
-          T dx, dy, dz;
-          if (MIXED) {  // exact wrapped fixed-point difference r_j - r_i
-            dx = (T)((float)(int)(aj.x - ai.x) * pp.sf[0]);
-            dy = (T)((float)(int)(aj.y - ai.y) * pp.sf[1]);
-            dz = (T)((float)(int)(aj.z - ai.z) * pp.sf[2]);
-          } else {  // r_j - r_i, MinImageDistance (box.h:51-73)
-            dx = (T)min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
-            dy = (T)min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
-            dz = (T)min_image1(__ldg(z + j) - zi, pp.box.len[2], pp.box.half[2]);
-          }
-          qu.dx[warp][pos] = dx;
-          qu.dy[warp][pos] = dy;
-          qu.dz[warp][pos] = dz;
-          qu.j[warp][pos] = code;
+          qu.j[warp][pos] = ((core_bits >> u) & 1u) ? jj[u] : (jj[u] | (int)0x80000000);
+          if (MIXED)  // exact wrapped fixed-point difference r_j - r_i
+            reinterpret_cast<QueueMixed&>(qu).v[warp][pos] =
+                make_float4((float)(int)(aa[u].x - ai.x) * pp.sf[0],
+                            (float)(int)(aa[u].y - ai.y) * pp.sf[1],
+                            (float)(int)(aa[u].z - ai.z) * pp.sf[2], __uint_as_float(aa[u].w));
         }
         qn += __popc(m);
-        k0 += 32;
-        __syncwarp();
       }
-      // drain full 32-pair batches, and the remainder after the last chunk
-      while (qn >= 32 || (!more && qn > 0)) {
-        if (lane < qn) {
-          const int c = qu.j[warp][lane];
-          const int j = c & 0x7fffffff;
-          const T ddx = qu.dx[warp][lane], ddy = qu.dy[warp][lane], ddz = qu.dz[warp][lane];
-          const int tj = __ldg(type + j);
-          T f;
-          if (MIXED) {
-            const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
-            const float qq = (float)qi * __uint_as_float(__ldg(&atoms[j].w));
-            f = lj_f32(f_eps[ti * nt + tj], f_s6[ti * nt + tj], d2);
-            if (qq != 0.f)
-              f += coul_f32((float)pp.alpha, (float)pp.sqrt_alpha, (float)pp.qqr2e, qq, d2);
-            if (c < 0) f *= (float)pp.freq;
-          } else {
-            const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-            const double qq = (double)qi * __ldg(q + j);
-            f = lj_f64(tt.eps[ti * nt + tj], tt.s6[ti * nt + tj], d2);
-            if (qq != 0.0) f += coul_f64(pp.alpha, pp.sqrt_alpha, pp.qqr2e, qq, d2);
-            if (c < 0) f *= (double)pp.freq;
-          }
-          fxa += f * ddx;
-          fya += f * ddy;
-          fza += f * ddz;
-        }
-        __syncwarp();
-        const int rem = qn > 32 ? qn - 32 : 0;
-        if (lane < rem) {
-          qu.dx[warp][lane] = qu.dx[warp][32 + lane];
-          qu.dy[warp][lane] = qu.dy[warp][32 + lane];
-          qu.dz[warp][lane] = qu.dz[warp][32 + lane];
-          qu.j[warp][lane] = qu.j[warp][32 + lane];
-        }
-        __syncwarp();
-        qn = rem;
+      __syncwarp();
+      while (qn >= 32) {  // full batches from the tail of the queue
+        qn -= 32;
+        pair_force(qn + lane);
       }
-      if (!more) break;
+      __syncwarp();
     }
+    if (lane < qn) pair_force(lane);
+    __syncwarp();
     const double gx = warp_sum((double)fxa), gy = warp_sum((double)fya),
                  gz = warp_sum((double)fza);
     if (lane == 0) {
@@ -317,7 +350,10 @@ k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
                    double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart,
                    double* __restrict__ epart) {
   __shared__ TypeTables tt;
-  __shared__ PairQueue<double> qu;
+  __shared__ struct {
+    double dx[PAIR_WARPS][QCAP], dy[PAIR_WARPS][QCAP], dz[PAIR_WARPS][QCAP];
+    int j[PAIR_WARPS][QCAP];
+  } qu;
   __shared__ double s_acc[PAIR_WARPS][3];
   __shared__ double s_e[PAIR_WARPS][8];
   load_type_tables(tt, pp);
@@ -346,12 +382,8 @@ k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
           if (j != i) {
             int in = -1;
             if (pp.cubic) {
-              const uint4 aj = __ldg(atoms + j);
-              const int dx = (int)(aj.x - ai.x), dy = (int)(aj.y - ai.y), dz = (int)(aj.z - ai.z);
-              const unsigned long long d2i = (unsigned long long)((long long)dx * dx) +
-                                             (unsigned long long)((long long)dy * dy) +
-                                             (unsigned long long)((long long)dz * dz);
-              in = screen_lt(d2i, pp.sc_rc);
+              const float d2s = fixed_d2(ai, __ldg(atoms + j));
+              in = d2s < pp.sc_rc.lo ? 1 : (d2s >= pp.sc_rc.hi ? 0 : -1);
             }
             if (in < 0) {
               const double ex = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
@@ -681,13 +713,11 @@ __global__ void k_sub_mean(int n, double* __restrict__ fx, double* __restrict__ 
 // Launchers
 // ---------------------------------------------------------------------------
 IntScreen make_screen(double C, double L, double band) {
-  // |d|^2 * s^2 < C  <=>  |d|^2 < C / s^2, s = L / 2^32; band in r^2 units
-  const long double scale = 18446744073709551616.0L / ((long double)L * (long double)L);
-  const long double K = (long double)C * scale, B = (long double)band * scale;
+  // |d|^2 s^2 < C  <=>  |d|^2 < C / s^2, s = L / 2^32; band in r^2 units
+  const double scale = 18446744073709551616.0 / (L * L);
   IntScreen t;
-  const long double lo = floorl(K - B), hi = ceill(K + B);
-  t.lo = lo <= 0.0L ? 0ULL : (unsigned long long)lo;
-  t.hi = hi >= 18446744073709551615.0L ? ~0ULL : (unsigned long long)hi;
+  t.lo = (float)((C - band) * scale);
+  t.hi = (float)((C + band) * scale);
   return t;
 }
 
@@ -705,14 +735,23 @@ int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms
                      const int* cand, int cap, double* fx, double* fy, double* fz, double* fpart,
                      int nblocks, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  if (mixed)
-    k_rbl_fused<true><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, key_a,
-                                                      key_b, epoch, cand_count, cand, cap, fx, fy,
-                                                      fz, fpart);
-  else
-    k_rbl_fused<false><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, key_a,
-                                                       key_b, epoch, cand_count, cand, cap, fx, fy,
-                                                       fz, fpart);
+  const bool pow2 = pp.freq >= 1 && (pp.freq & (pp.freq - 1)) == 0;
+#define RBX_LAUNCH_RBL(M, P2)                                                                  \
+  k_rbl_fused<M, P2><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, key_a,   \
+                                                     key_b, epoch, cand_count, cand, cap, fx, \
+                                                     fy, fz, fpart)
+  if (mixed) {
+    if (pow2)
+      RBX_LAUNCH_RBL(true, true);
+    else
+      RBX_LAUNCH_RBL(true, false);
+  } else {
+    if (pow2)
+      RBX_LAUNCH_RBL(false, true);
+    else
+      RBX_LAUNCH_RBL(false, false);
+  }
+#undef RBX_LAUNCH_RBL
   count_launch();
   return check_launch(mixed ? "rbl_fused_mixed" : "rbl_fused_f64");
 }
