@@ -89,6 +89,28 @@ int rbx_rbe_structure_factor(const rbx_box* box, int num_atoms, int p_number,
                              const double* pz, double* density_real,
                              double* density_imag, void* stream);
 
+/* rbx_rbe_structure_factor without any device allocation.  No counterpart in
+ * the reference: it exists for hosts that own all device memory themselves (a
+ * pre-sized arena, a job-enforced memory cap, or a step loop whose footprint
+ * must not change) and so cannot let a library call cudaMalloc or
+ * cudaMallocAsync.  The per-block partial sums live in a fixed array built into
+ * the library: RBX_NOALLOC_RHO_BLOCKS x RBX_NOALLOC_RHO_MAX_P doubles for Re and
+ * for Im (2 MiB), held on every GPU that loads the library until the process
+ * exits.  p_number above RBX_NOALLOC_RHO_MAX_P is rejected with RBX_ERR_INVALID.
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  All calls share the
+ * one array: calls whose work can overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller.  Results equal
+ * rbx_rbe_structure_factor's up to FP64 summation order. */
+#define RBX_NOALLOC_RHO_BLOCKS 256
+#define RBX_NOALLOC_RHO_MAX_P 512
+int rbx_rbe_structure_factor_noalloc(const rbx_box* box, int num_atoms, int p_number,
+                                     const double* charge, const double* p_sample_x,
+                                     const double* p_sample_y, const double* p_sample_z,
+                                     const double* px, const double* py,
+                                     const double* pz, double* density_real,
+                                     double* density_imag, void* stream);
+
 /* Per-atom RBE force.  Replaces ComputeRBEForceOp (kspace_calculator_op.h:123-135,
  * kernel kspace_calculator_op.hip.cu:678-738). */
 int rbx_rbe_force(const rbx_box* box, int num_atoms, int p_number, double alpha,

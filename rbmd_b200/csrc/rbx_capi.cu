@@ -4,6 +4,7 @@
 #include <stdio.h>
 
 #include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -509,3 +510,92 @@ int rbx_pair_force_verlet(const rbx_box* box, double cut_off, int num_atoms, dou
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// rbx_rbe_structure_factor_noalloc: the structure-factor pass for callers that
+// cannot let a library allocate device memory.  Its per-block partial sums
+// live in a fixed array compiled into the library instead of a temporary.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoallocBlocks = RBX_NOALLOC_RHO_BLOCKS;  // partial blocks per call
+constexpr int kNoallocMaxP = RBX_NOALLOC_RHO_MAX_P;     // largest p_number accepted
+
+// Re and Im partials, k-major: [2][kNoallocMaxP][kNoallocBlocks] doubles (2 MiB).
+// Every GPU that loads the library holds this array until the process exits.
+static __device__ __align__(256) double g_noalloc_rho_scratch[2 * kNoallocMaxP * kNoallocBlocks];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[256] = {};  // device address of the array, per device ordinal
+
+// Device address of the scratch array on the current device, looked up once per
+// device.  The array's name in host code is only a host-side handle; kernels
+// must be given this address.
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+    cudaGetLastError();
+    set_error("rbx_rbe_structure_factor_noalloc: no current CUDA device");
+    return RBX_ERR_DEVICE;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_rho_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      set_error("rbx_rbe_structure_factor_noalloc: cudaGetSymbolAddress failed on device %d: %s",
+                dev, cudaGetErrorString(e));
+      return RBX_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = (double*)p;
+  }
+  *out = g_noalloc_addr[dev];
+  return RBX_OK;
+}
+
+}  // namespace
+
+extern "C" int rbx_rbe_structure_factor_noalloc(const rbx_box* box, int num_atoms, int p_number,
+                                                const double* charge, const double* p_sample_x,
+                                                const double* p_sample_y,
+                                                const double* p_sample_z, const double* px,
+                                                const double* py, const double* pz,
+                                                double* density_real, double* density_imag,
+                                                void* stream) {
+  RBX_CHECK_BOX(box);
+  if (num_atoms < 0 || p_number < 0) {
+    set_error("rbx_rbe_structure_factor_noalloc: negative size");
+    return RBX_ERR_INVALID;
+  }
+  if (p_number > kNoallocMaxP) {
+    set_error("rbx_rbe_structure_factor_noalloc: p_number %d exceeds the built-in scratch limit "
+              "of %d k-vectors; use rbx_rbe_structure_factor",
+              p_number, kNoallocMaxP);
+    return RBX_ERR_INVALID;
+  }
+  if (p_number == 0) return RBX_OK;
+  RBX_TRY(require_device());
+  double* scratch = nullptr;
+  RBX_TRY(noalloc_scratch(&scratch));
+  cudaStream_t st = (cudaStream_t)stream;
+  const DBox b = make_dbox(*box);
+  int nb = rbe_partial_blocks(num_atoms);
+  if (nb > kNoallocBlocks) nb = kNoallocBlocks;
+  double* pr = scratch;
+  double* pi = scratch + (size_t)kNoallocMaxP * kNoallocBlocks;
+  // Every (k, block) slot the finalize reads is written below, so no clearing
+  // is needed; slots left from an earlier, larger call are never read.
+  if (num_atoms > 0) {
+    RBX_TRY(launch_rbe_rho_partial_f64(b, num_atoms, p_number, p_sample_x, p_sample_y, p_sample_z,
+                                       charge, px, py, pz, pr, pi, nb, st));
+  } else {
+    nb = 1;
+    if (cudaMemsetAsync(pr, 0, sizeof(double) * p_number, st) != cudaSuccess ||
+        cudaMemsetAsync(pi, 0, sizeof(double) * p_number, st) != cudaSuccess)
+      return check_launch("rbx_rbe_structure_factor_noalloc memset");
+  }
+  return launch_rbe_finalize(b, p_number, nb, pr, pi, p_sample_x, p_sample_y, p_sample_z, 1.0, 0.0,
+                             1.0, 0.0, 0.0, density_real, density_imag, nullptr, nullptr, nullptr,
+                             0, nullptr, 0, nullptr, st);
+}

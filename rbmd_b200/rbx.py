@@ -90,7 +90,7 @@ EXPORTS = [
     "rbx_engine_compute_forces", "rbx_engine_step", "rbx_engine_step_host",
     "rbx_engine_get_state", "rbx_engine_get_force_parts", "rbx_engine_get_rbl_pairs",
     "rbx_engine_get_stats", "rbx_engine_stream", "rbx_engine_phase_ms",
-    "rbx_engine_set_profiling",
+    "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc",
 ]
 
 
@@ -113,6 +113,7 @@ def lib():
     L.rbx_rbl_params.argtypes = [ip, B, dp, dp, ip, C.POINTER(C.c_int)]
     L.rbx_rbe_sample.argtypes = [B, dp, ip, C.c_uint64, C.c_int64, vp, vp, vp, vp]
     L.rbx_rbe_structure_factor.argtypes = [B, ip, ip] + [vp] * 9 + [vp]
+    L.rbx_rbe_structure_factor_noalloc.argtypes = [B, ip, ip] + [vp] * 9 + [vp]
     L.rbx_rbe_force.argtypes = [B, ip, ip, dp, dp, dp] + [vp] * 12 + [vp]
     L.rbx_rbe_energy_virial.argtypes = [B, ip, dp, dp, dp, dp, dp] + [vp] * 7 + [vp]
     L.rbx_ewald_force.argtypes = [B, ip, C.POINTER(C.c_int), dp, dp] + [vp] * 8 + [vp]
@@ -211,6 +212,14 @@ def rbe_structure_factor(box, q, mx, my, mz, x, y, z, re, im, stream=None):
     check(lib().rbx_rbe_structure_factor(C.byref(box), q.numel(), mx.numel(), _ptr(q), _ptr(mx),
                                          _ptr(my), _ptr(mz), _ptr(x), _ptr(y), _ptr(z), _ptr(re),
                                          _ptr(im), _stream(stream)), "rbx_rbe_structure_factor")
+
+
+def rbe_structure_factor_noalloc(box, q, mx, my, mz, x, y, z, re, im, stream=None):
+    """Structure factors without device allocation (built-in scratch; p <= 512)."""
+    check(lib().rbx_rbe_structure_factor_noalloc(C.byref(box), q.numel(), mx.numel(), _ptr(q),
+                                                 _ptr(mx), _ptr(my), _ptr(mz), _ptr(x), _ptr(y),
+                                                 _ptr(z), _ptr(re), _ptr(im), _stream(stream)),
+          "rbx_rbe_structure_factor_noalloc")
 
 
 def rbe_force(box, alpha, S, qqr2e, re, im, q, mx, my, mz, x, y, z, fx, fy, fz, stream=None):
