@@ -301,17 +301,19 @@ int rbx_engine_set_k_samples(rbx_engine* e, int p, const double* mx,
 int rbx_engine_compute_forces(rbx_engine* e, int epoch);
 /* nsteps velocity-Verlet steps, state resident on the device. */
 int rbx_engine_step(rbx_engine* e, int nsteps);
-/* One step end to end from host buffers: copies x, v in (pinned or pageable),
- * steps once and copies x, v, f out, in gid order of the host arrays given to
- * rbx_engine_set_state. */
+/* One step end to end from host buffers laid out [3][n] (x row, y row, z row),
+ * in the atom order given to rbx_engine_set_state: copies x, v in (pinned or
+ * pageable), steps once and copies x, v, f out. */
 int rbx_engine_step_host(rbx_engine* e, const double* x_in, const double* v_in,
                          double* x_out, double* v_out, double* f_out);
-/* Copy the state to host arrays in gid order (index gid-gid_min). Any pointer
- * may be NULL. f is the last total force (real space + k-space). */
+/* Copy the state to host arrays, in the atom order of the arrays given to
+ * rbx_engine_set_state. Any pointer may be NULL. f is the last total force
+ * (real space + k-space). */
 int rbx_engine_get_state(rbx_engine* e, double* px, double* py, double* pz,
                          double* vx, double* vy, double* vz, double* fx,
                          double* fy, double* fz);
-/* Last real-space (after mean removal for RBL) and k-space forces, gid order. */
+/* Last real-space (after mean removal for RBL) and k-space forces, [n][3] each,
+ * in the atom order given to rbx_engine_set_state. */
 int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace);
 /* Last RBL lists as (gid_i, gid_j) pairs; sizes in/out. */
 int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core,
