@@ -417,8 +417,14 @@ int rbx_full_list(const rbx_box* box, double neighbor_cutoff, int n, const doubl
     return RBX_ERR_INVALID;
   }
   RBX_TRY(require_device());
-  return launch_full_list(make_dbox(*box), dims, neighbor_cutoff, n, px, py, pz, cell_start, cap,
-                          count, nbrs, overflow, (cudaStream_t)stream);
+  if (n == 0) return RBX_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* scratch = nullptr;
+  RBX_TRY(async_alloc(&scratch, full_list_scratch_bytes(n, dims[0] * dims[1] * dims[2]), st));
+  const int rc = launch_full_list(make_dbox(*box), dims, neighbor_cutoff, n, px, py, pz,
+                                  cell_start, cap, count, nbrs, overflow, scratch, st);
+  cudaFreeAsync(scratch, st);
+  return rc;
 }
 
 int rbx_rbl_filter(double core_cutoff_2, double force_cutoff_2, int total_atom_num,

@@ -11,11 +11,12 @@
 //
 // The candidate list replaces Estimate/GenerateFullNeighborListOp
 // (src/neighbor_list/src/op/rocm/full_neighbor_list_op.hip.cu:177-288): one
-// CTA per cell stages the 27 stencil cells in shared memory as FP32
-// coordinates relative to the centre cell (periodic images pre-shifted), one
-// warp per centre atom screens them in FP32 and settles only the pairs inside
-// a guard band around the cutoff with the reference's FP64 predicate, so the
-// list is bit-identical (as a set) to the FP64 reference list.
+// warp per 32 centre atoms (one per lane) streams the chunks of the 27
+// stencil cells that survive a bounding-box cull through shared memory and
+// screens them in FP32; only pairs inside a guard band around the cutoff are
+// settled with the reference's FP64 predicate, so the list is bit-identical
+// (as a set) to the FP64 reference list.  Rows come out in stencil order,
+// then in cell order.
 #include <math.h>
 
 #include "rbx_common.cuh"
@@ -154,164 +155,193 @@ k_cell_segsort(int ncell, int n, const int* __restrict__ start, const unsigned* 
 }
 
 // ---------------------------------------------------------------------------
-// Candidate list: CTA per cell.  Stencil cells are staged in shared memory,
-// each padded to whole 32-atom chunks; every chunk gets a bounding box, and a
-// centre atom tests only the chunks whose box comes within the cutoff.
+// Candidate list.  Atoms of a cell are cut into 32-atom chunks; chunk k of
+// cell c sits at table index (cell_start[c] >> 5) + c + k, which is unique
+// and needs no scan (the indices of consecutive cells never overlap), and the
+// few indices between two cells are marked empty.  k_chunk_boxes writes each
+// chunk's bounding box, rounded outwards to FP32, and its cell.
+//
+// k_full_list runs one warp per chunk of centre atoms, one centre atom per
+// lane.  For each of the 27 stencil cells it culls the cell's chunks against
+// the group's box (directed rounding: a lower bound of the true box distance,
+// so no pair within the cutoff is ever culled), then streams each surviving
+// chunk through a 32-slot shared buffer as {v, |v|^2}, FP32 coordinates
+// relative to the centre cell's centre with the periodic image applied.
+// Lane u tests slot v as |v|^2 - 2 u.v < C - |u|^2: three FMAs per pair.
+// Pairs inside a guard band around the cutoff are settled with the
+// reference's FP64 predicate, so the list equals the FP64 reference list as a
+// set; rows come out in stencil order, then in cell order.
 // ---------------------------------------------------------------------------
-constexpr int NL_BLOCK = 256;
+constexpr int NL_BLOCK = 128;
 constexpr int NL_WARPS = NL_BLOCK / 32;
-constexpr int NL_STAGE = 2048;   // staged stencil slots per pass (multiple of 32)
-constexpr int NL_CHUNKS = NL_STAGE / 32;
-constexpr int NL_CENTER = 1024;  // centre-cell atoms tracked per CTA
 
-__global__ void __launch_bounds__(NL_BLOCK)
-k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float lo_band, float hi_band,
-            int n, const double* __restrict__ x, const double* __restrict__ y,
-            const double* __restrict__ z, const int* __restrict__ cell_start, int cap,
-            int* __restrict__ count, int* __restrict__ nbrs, int* __restrict__ overflow) {
-  __shared__ float sx[NL_STAGE], sy[NL_STAGE], sz[NL_STAGE];
-  __shared__ int sj[NL_STAGE];
-  __shared__ float bb[6][NL_CHUNKS];  // chunk boxes: min xyz, max xyz
-  __shared__ int s_cnt[NL_CENTER];
-  __shared__ int s_cbeg[27], s_ccnt[27];
-  __shared__ double s_shift[27][3];
+__device__ __forceinline__ int chunk_base(int c, int cs) { return (cs >> 5) + c; }
+
+int full_list_table_size(int n, int ncell) { return (n >> 5) + ncell; }
+
+__global__ void __launch_bounds__(128)
+k_chunk_boxes(const double* __restrict__ x, const double* __restrict__ y,
+              const double* __restrict__ z, const int* __restrict__ cell_start,
+              float4* __restrict__ box_lo, float4* __restrict__ box_hi, int* __restrict__ cell_of) {
   const int c = blockIdx.x;
-  const int cz = c / (dimx * dimy), cy = (c / dimx) % dimy, cx = c % dimx;
-  const double ex = b.len[0] / dimx, ey = b.len[1] / dimy, ez = b.len[2] / dimz;
-  const double ox = b.lo[0] + cx * ex, oy = b.lo[1] + cy * ey, oz = b.lo[2] + cz * ez;
   const int cs = cell_start[c], ce = cell_start[c + 1];
-  const int ncen = ce - cs;
-  if (ncen > NL_CENTER) {
-    if (threadIdx.x == 0) atomicOr(overflow, 2);
-    return;
+  const int nch = (ce - cs + 31) >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int base = chunk_base(c, cs);
+  for (int k = warp; k < nch; k += 4) {
+    const int a = cs + 32 * k + lane;
+    const bool ok = a < ce;
+    float lo[3], hi[3];
+    const double* p[3] = {x, y, z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double v = ok ? p[d][a] : 0.0;
+      lo[d] = ok ? __double2float_rd(v) : INFINITY;
+      hi[d] = ok ? __double2float_ru(v) : -INFINITY;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+        hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+      }
+    if (lane == 0) {
+      box_lo[base + k] = make_float4(lo[0], lo[1], lo[2], 0.f);
+      box_hi[base + k] = make_float4(hi[0], hi[1], hi[2], 0.f);
+      cell_of[base + k] = c;
+    }
   }
-  if (threadIdx.x < 27) {
+  const int next = chunk_base(c + 1, ce);  // first index of the next cell
+  for (int t = base + nch + threadIdx.x; t < next; t += blockDim.x) cell_of[t] = -1;
+}
+
+__global__ void __launch_bounds__(NL_BLOCK, 5)
+k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, float lo_band,
+            float hi_band, int nidx, const double* __restrict__ x, const double* __restrict__ y,
+            const double* __restrict__ z, const int* __restrict__ cell_start,
+            const float4* __restrict__ box_lo, const float4* __restrict__ box_hi,
+            const int* __restrict__ cell_of, int cap, int* __restrict__ count,
+            int* __restrict__ nbrs, int* __restrict__ overflow) {
+  __shared__ float4 buf[NL_WARPS][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int w = blockIdx.x * NL_WARPS + warp;
+  if (w >= nidx) return;
+  const int c = cell_of[w];
+  if (c < 0) return;  // an index between two cells
+  const int cs = cell_start[c], ce = cell_start[c + 1];
+  const int g = w - chunk_base(c, cs);
+  const int cz = c / (dimx * dimy), cy = (c / dimx) % dimy, cx = c % dimx;
+  const double ox = b.lo[0] + (cx + 0.5) * (b.len[0] / dimx);
+  const double oy = b.lo[1] + (cy + 0.5) * (b.len[1] / dimy);
+  const double oz = b.lo[2] + (cz + 0.5) * (b.len[2] / dimz);
+  const bool live = cs + g * 32 + lane < ce;
+  const int i = live ? cs + g * 32 + lane : cs + g * 32;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  const float ux = (float)(xi - ox), uy = (float)(yi - oy), uz = (float)(zi - oz);
+  const float uu = fmaf(ux, ux, fmaf(uy, uy, uz * uz));
+  const float ax = live ? -2.f * ux : 0.f, ay = live ? -2.f * uy : 0.f,
+              az = live ? -2.f * uz : 0.f;
+  const float lo_i = live ? lo_band - uu : -INFINITY;
+  const float hi_i = live ? hi_band - uu : -INFINITY;
+  // box of the group's centre atoms relative to the cell centre, rounded outwards
+  float glo[3], ghi[3];
+  {
+    const double p[3] = {xi, yi, zi}, o[3] = {ox, oy, oz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      glo[d] = live ? __double2float_rd(__dsub_rd(p[d], o[d])) : INFINITY;
+      ghi[d] = live ? __double2float_ru(__dsub_ru(p[d], o[d])) : -INFINITY;
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        glo[d] = fminf(glo[d], __shfl_xor_sync(0xffffffffu, glo[d], s));
+        ghi[d] = fmaxf(ghi[d], __shfl_xor_sync(0xffffffffu, ghi[d], s));
+      }
+  }
+  int cnt = 0;
+  int* row = nbrs + (size_t)i * cap;
+  for (int s = 0; s < 27; ++s) {
     // stencil order of ComputeFullNeighborStencilCellOnTheFly:
     // offsets (s%3-1, (s/3)%3-1, s/9-1)
-    const int s = threadIdx.x;
-    const int o[3] = {s % 3 - 1, (s / 3) % 3 - 1, s / 9 - 1};
-    const int cc[3] = {cx, cy, cz};
-    const int dims[3] = {dimx, dimy, dimz};
-    int nc[3];
-    for (int d = 0; d < 3; ++d) {
-      int v = cc[d] + o[d];
-      double sh = 0.0;
-      if (v < 0) {
-        v += dims[d];
-        sh = -b.len[d];
-      } else if (v >= dims[d]) {
-        v -= dims[d];
-        sh = b.len[d];
+    int nx = cx + s % 3 - 1, ny = cy + (s / 3) % 3 - 1, nz = cz + s / 9 - 1;
+    double shx = 0.0, shy = 0.0, shz = 0.0;
+    if (nx < 0) { nx += dimx; shx = -b.len[0]; } else if (nx >= dimx) { nx -= dimx; shx = b.len[0]; }
+    if (ny < 0) { ny += dimy; shy = -b.len[1]; } else if (ny >= dimy) { ny -= dimy; shy = b.len[1]; }
+    if (nz < 0) { nz += dimz; shz = -b.len[2]; } else if (nz >= dimz) { nz -= dimz; shz = b.len[2]; }
+    const int nc = (nz * dimy + ny) * dimx + nx;
+    const int ncs = cell_start[nc], nce = cell_start[nc + 1];
+    const int nch = (nce - ncs + 31) >> 5;
+    const int nb = chunk_base(nc, ncs);
+    const double dx = shx - ox, dy = shy - oy, dz = shz - oz;
+    const double dxl = __dsub_rd(shx, ox), dyl = __dsub_rd(shy, oy), dzl = __dsub_rd(shz, oz);
+    const double dxh = __dsub_ru(shx, ox), dyh = __dsub_ru(shy, oy), dzh = __dsub_ru(shz, oz);
+    for (int kb = 0; kb < nch; kb += 32) {
+      bool near = false;
+      if (kb + lane < nch) {  // lower bound of the box-box distance
+        const float4 bl = box_lo[nb + kb + lane], bh = box_hi[nb + kb + lane];
+        const float clx = __double2float_rd(__dadd_rd((double)bl.x, dxl));
+        const float cly = __double2float_rd(__dadd_rd((double)bl.y, dyl));
+        const float clz = __double2float_rd(__dadd_rd((double)bl.z, dzl));
+        const float chx = __double2float_ru(__dadd_ru((double)bh.x, dxh));
+        const float chy = __double2float_ru(__dadd_ru((double)bh.y, dyh));
+        const float chz = __double2float_ru(__dadd_ru((double)bh.z, dzh));
+        const float gx = fmaxf(0.f, fmaxf(__fsub_rd(clx, ghi[0]), __fsub_rd(glo[0], chx)));
+        const float gy = fmaxf(0.f, fmaxf(__fsub_rd(cly, ghi[1]), __fsub_rd(glo[1], chy)));
+        const float gz = fmaxf(0.f, fmaxf(__fsub_rd(clz, ghi[2]), __fsub_rd(glo[2], chz)));
+        const float d2 = __fadd_rd(__fadd_rd(__fmul_rd(gx, gx), __fmul_rd(gy, gy)), __fmul_rd(gz, gz));
+        near = d2 < cut2_up;
       }
-      nc[d] = v;
-      s_shift[s][d] = sh;
-    }
-    const int cell = (nc[2] * dimy + nc[1]) * dimx + nc[0];
-    s_cbeg[s] = cell_start[cell];
-    s_ccnt[s] = cell_start[cell + 1] - cell_start[cell];
-  }
-  for (int t = threadIdx.x; t < ncen; t += NL_BLOCK) s_cnt[t] = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned lt = (1u << lane) - 1u;
-  int s0 = 0;
-  while (s0 < 27) {
-    // greedy group of stencil cells whose padded sizes fit the stage
-    int s1 = s0, tot = 0;
-    while (s1 < 27 && tot + ((s_ccnt[s1] + 31) & ~31) <= NL_STAGE) {
-      tot += (s_ccnt[s1] + 31) & ~31;
-      ++s1;
-    }
-    if (s1 == s0) {  // a single cell larger than the stage
-      if (threadIdx.x == 0) atomicOr(overflow, 2);
-      return;
-    }
-    int off = 0;
-    for (int s = s0; s < s1; ++s) {
-      const int beg = s_cbeg[s], cnt = s_ccnt[s], pad = (cnt + 31) & ~31;
-      const double shx = s_shift[s][0] - ox, shy = s_shift[s][1] - oy, shz = s_shift[s][2] - oz;
-      for (int t = threadIdx.x; t < pad; t += NL_BLOCK) {
-        if (t < cnt) {
-          const int j = beg + t;
-          sx[off + t] = (float)(x[j] + shx);
-          sy[off + t] = (float)(y[j] + shy);
-          sz[off + t] = (float)(z[j] + shz);
-          sj[off + t] = j;
-        } else {  // padding slot: never within the cutoff
-          sx[off + t] = 1e30f;
-          sy[off + t] = 1e30f;
-          sz[off + t] = 1e30f;
-          sj[off + t] = -1;
+      unsigned m = __ballot_sync(0xffffffffu, near);
+      while (m) {
+        const int k = kb + __ffs(m) - 1;
+        m &= m - 1;
+        const int first = ncs + 32 * k;
+        float4 v = make_float4(0.f, 0.f, INFINITY, INFINITY);  // empty slot: never a hit
+        if (first + lane < nce) {
+          const int a = first + lane;
+          v.x = (float)(x[a] + dx);
+          v.y = (float)(y[a] + dy);
+          v.z = (float)(z[a] + dz);
+          v.w = fmaf(v.x, v.x, fmaf(v.y, v.y, v.z * v.z));
         }
-      }
-      off += pad;
-    }
-    __syncthreads();
-    const int nch = tot / 32;
-    for (int ch = warp; ch < nch; ch += NL_WARPS) {
-      const int t = ch * 32 + lane;
-      const bool real = sj[t] >= 0;
-      float lo[3] = {real ? sx[t] : 1e30f, real ? sy[t] : 1e30f, real ? sz[t] : 1e30f};
-      float hi[3] = {real ? sx[t] : -1e30f, real ? sy[t] : -1e30f, real ? sz[t] : -1e30f};
+        __syncwarp();  // the previous chunk's readers are done
+        buf[warp][lane] = v;
+        __syncwarp();
+        unsigned acc = 0, maybe = 0;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-          hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+        for (int t = 0; t < 32; ++t) {
+          const float4 q = buf[warp][t];  // broadcast
+          const float d = fmaf(ax, q.x, fmaf(ay, q.y, fmaf(az, q.z, q.w)));
+          acc |= d < lo_i ? 1u << t : 0u;
+          maybe |= d < hi_i ? 1u << t : 0u;
         }
-      if (lane < 3) {
-        bb[lane][ch] = lo[lane];
-        bb[3 + lane][ch] = hi[lane];
+        if (nc == c && k == g) {  // the centre atom itself
+          acc &= ~(1u << lane);
+          maybe &= ~(1u << lane);
+        }
+        unsigned unsure = maybe & ~acc;
+        if (__any_sync(0xffffffffu, unsure != 0)) {  // rare: the FP64 predicate decides
+          while (unsure) {
+            const int t = __ffs(unsure) - 1;
+            unsure &= unsure - 1;
+            const int j = first + t;
+            if (dist2_list(b, xi, yi, zi, x[j], y[j], z[j]) < cut2) acc |= 1u << t;
+          }
+        }
+        while (acc) {  // hits in cell order, each lane into its own row
+          const int t = __ffs(acc) - 1;
+          acc &= acc - 1;
+          if (cnt < cap) row[cnt] = first + t;
+          ++cnt;
+        }
       }
     }
-    __syncthreads();
-    for (int li = warp; li < ncen; li += NL_WARPS) {
-      const int i = cs + li;
-      const double xi = x[i], yi = y[i], zi = z[i];
-      const float fxi = (float)(xi - ox), fyi = (float)(yi - oy), fzi = (float)(zi - oz);
-      int cnt = s_cnt[li];
-      for (int cb = 0; cb < nch; cb += 32) {
-        const int ch = cb + lane;
-        bool near = false;
-        if (ch < nch) {
-          const float gx = fmaxf(0.f, fmaxf(bb[0][ch] - fxi, fxi - bb[3][ch]));
-          const float gy = fmaxf(0.f, fmaxf(bb[1][ch] - fyi, fyi - bb[4][ch]));
-          const float gz = fmaxf(0.f, fmaxf(bb[2][ch] - fzi, fzi - bb[5][ch]));
-          near = gx * gx + gy * gy + gz * gz < hi_band;
-        }
-        unsigned m = __ballot_sync(0xffffffffu, near);
-        while (m) {
-          const int chunk = cb + __ffs(m) - 1;
-          m &= m - 1;
-          const int t = chunk * 32 + lane;
-          const int j = sj[t];
-          bool in = false;
-          if (j >= 0 && j != i) {
-            const float dxf = sx[t] - fxi, dyf = sy[t] - fyi, dzf = sz[t] - fzi;
-            const float d2f = dxf * dxf + dyf * dyf + dzf * dzf;
-            if (d2f < lo_band)
-              in = true;
-            else if (d2f < hi_band)
-              in = dist2_list(b, xi, yi, zi, x[j], y[j], z[j]) < cut2;
-          }
-          const unsigned mm = __ballot_sync(0xffffffffu, in);
-          if (in) {
-            const int pos = cnt + __popc(mm & lt);
-            if (pos < cap) nbrs[(size_t)i * cap + pos] = j;
-          }
-          cnt += __popc(mm);
-        }
-      }
-      if (lane == 0) s_cnt[li] = cnt;
-      __syncwarp();
-    }
-    __syncthreads();
-    s0 = s1;
   }
-  for (int t = threadIdx.x; t < ncen; t += NL_BLOCK) {
-    const int cnt = s_cnt[t];
-    count[cs + t] = cnt;
+  if (live) {
+    count[i] = cnt;
     if (cnt > cap) atomicOr(overflow, 1);
   }
 }
@@ -473,18 +503,43 @@ int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, 
   return check_launch("cells_sort");
 }
 
+size_t full_list_scratch_bytes(int n, int ncell) {
+  const size_t t = (size_t)full_list_table_size(n, ncell);
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  return al(sizeof(float4) * t) * 2 + al(sizeof(int) * t);
+}
+
 int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
                      const double* y, const double* z, const int* cell_start, int cap,
-                     int* count, int* nbrs, int* overflow, cudaStream_t st) {
+                     int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st) {
   const int ncell = dims[0] * dims[1] * dims[2];
+  if (n <= 0) return RBX_OK;
   const double cut2 = cutoff * cutoff;
   double emax = 0.0;
   for (int d = 0; d < 3; ++d) emax = fmax(emax, b.len[d] / dims[d]);
-  // FP32 screening error is far below 1e-5 of (cutoff^2 + (2 edge)^2); guard band 1e-4 of it.
-  const double band = 1e-4 * (cut2 + 4.0 * emax * emax);
+  // FP32 screening error of |v|^2 - 2 u.v against C - |u|^2, with u (|u_d| <=
+  // e/2) and v (|v_d| <= 3e/2) rounded once to FP32 relative to the centre
+  // cell's centre: coordinate rounding moves |d|^2 by at most
+  // 4 sqrt(3) r e 2^-24, and the roundings of |v|^2, the three FMAs, |u|^2 and
+  // C - |u|^2 by at most (60 e^2 + 3 r^2) 2^-24 (e = largest cell edge,
+  // r = cutoff).  Pairs within twice that of the cutoff take the FP64 path.
+  const double err =
+      (4.0 * sqrt(3.0) * cutoff * emax + 60.0 * emax * emax + 3.0 * cut2) / 16777216.0;
+  const double band = 2.0 * err;
   const float lo_band = (float)(cut2 - band), hi_band = (float)(cut2 + band);
-  k_full_list<<<ncell, NL_BLOCK, 0, st>>>(b, dims[0], dims[1], dims[2], cut2, lo_band, hi_band, n,
-                                          x, y, z, cell_start, cap, count, nbrs, overflow);
+  float cut2_up = (float)cut2;  // rounded up
+  if ((double)cut2_up < cut2) cut2_up = nextafterf(cut2_up, INFINITY);
+  const int t = full_list_table_size(n, ncell);
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  char* p = (char*)scratch;
+  float4* box_lo = (float4*)p;
+  float4* box_hi = (float4*)(p + al(sizeof(float4) * t));
+  int* cell_of = (int*)(p + 2 * al(sizeof(float4) * t));
+  k_chunk_boxes<<<ncell, 128, 0, st>>>(x, y, z, cell_start, box_lo, box_hi, cell_of);
+  count_launch();
+  k_full_list<<<(t + NL_WARPS - 1) / NL_WARPS, NL_BLOCK, 0, st>>>(
+      b, dims[0], dims[1], dims[2], cut2, cut2_up, lo_band, hi_band, t, x, y, z, cell_start,
+      box_lo, box_hi, cell_of, cap, count, nbrs, overflow);
   count_launch();
   return check_launch("full_list");
 }

@@ -125,6 +125,7 @@ int rbx_engine::init() {
   ETRY(alloc(&atoms, N));
   ETRY(alloc(&cell_start, (size_t)ncell + 1));
   ETRY(alloc(&cell_scratch, cells_scratch_bytes(n, ncell)));
+  ETRY(alloc(&list_scratch, full_list_scratch_bytes(n, ncell)));
   ETRY(alloc(&dflags, 8));
   ETRY(alloc(&max_d2, 1));
   ETRY(alloc(&cand_total, 1));
@@ -297,16 +298,12 @@ int rbx_engine::rebuild() {
   for (int attempt = 0; attempt < 4; ++attempt) {
     ETRY(cuda_ok(cudaMemsetAsync(dflags + 1, 0, sizeof(int), st), "memset"));
     ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
-                          cand_count, cand, dflags + 1, st));
+                          cand_count, cand, dflags + 1, list_scratch, st));
     int h[2] = {0, 0};
     ETRY(cuda_ok(cudaMemcpyAsync(h, dflags, sizeof(int) * 2, cudaMemcpyDeviceToHost, st), "D2H"));
     ETRY(cuda_ok(cudaStreamSynchronize(st), "rebuild sync"));
     if (h[0]) {
       set_error("cell sort: a cell holds more than 2048 atoms");
-      return RBX_ERR_CAPACITY;
-    }
-    if (h[1] & 2) {
-      set_error("candidate list: a cell exceeds the staging capacity");
       return RBX_ERR_CAPACITY;
     }
     if (!(h[1] & 1)) {
@@ -351,7 +348,7 @@ int rbx_engine::real_space() {
   const bool mixed = prm.precision == RBX_MIXED;
   if (prm.neighbor_type == RBX_NEIGHBOR_RBL)
     return launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, cand_count,
-                            cand, cap, fpx, fpy, fpz, fpart, nfpart, st);
+                            cand, cap, fpx, fpy, fpz, fpart, nfpart, dflags + 3, st);
   return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, fpx, fpy,
                                  fpz, nullptr, epart, nfpart, st);
 }
@@ -417,11 +414,15 @@ int rbx_engine::compute_forces(int ep) {
   return RBX_OK;
 }
 
+// Device status words raised during the last steps: [2] k-sampler, [3] real-space kernel.
 int rbx_engine::check_sampler() {
-  if (P <= 0 || k_injected) return RBX_OK;
-  int h = 0;
-  ETRY(cuda_ok(cudaMemcpy(&h, dflags + 2, sizeof(int), cudaMemcpyDeviceToHost), "D2H"));
-  if (h) {
+  int h[2] = {0, 0};
+  ETRY(cuda_ok(cudaMemcpy(h, dflags + 2, sizeof(int) * 2, cudaMemcpyDeviceToHost), "D2H"));
+  if (h[1]) {
+    set_error("real-space kernel: a candidate-row copy did not complete (status %d)", h[1]);
+    return RBX_ERR_CUDA;
+  }
+  if (h[0] && P > 0 && !k_injected) {
     set_error("k-sampler: a sample needed more than 64 draws to avoid m = 0");
     return RBX_ERR_SAMPLER;
   }

@@ -41,7 +41,8 @@ struct rbx_engine {
 
   // cells and candidate list
   int *perm = nullptr, *cell_of_sorted = nullptr, *cell_start = nullptr;
-  void* cell_scratch = nullptr;
+  char* cell_scratch = nullptr;
+  char* list_scratch = nullptr;
   int cap = 0;
   int *cand_count = nullptr, *cand = nullptr;
 

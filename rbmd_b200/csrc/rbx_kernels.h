@@ -97,12 +97,13 @@ struct PairParams {
 // Fused RBL filter + pair force over a row-major candidate list.
 // fpart (nblocks x 3) receives per-block force sums for the mean removal.
 int rbl_fused_blocks(int n);
+// status (device int, may be null = no prefetch): bit 4 set if a row copy timed out.
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
                      const double* x, const double* y, const double* z, const double* q,
                      const int* type, const unsigned long long* key_a,
                      const unsigned long long* key_b, int epoch, const int* cand_count,
                      const int* cand, int cap, double* fx, double* fy, double* fz, double* fpart,
-                     int nblocks, cudaStream_t st);
+                     int nblocks, int* status, cudaStream_t st);
 // Verlet pair force over the candidate list, cut at cut_off (force predicate).
 int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, const double* x,
                             const double* y, const double* z, const double* q, const int* type,
@@ -146,9 +147,11 @@ int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, 
                       const double* z, int* perm, int* cell_of_sorted, int* cell_start,
                       void* scratch, int* status, cudaStream_t st);
 size_t cells_scratch_bytes(int n, int ncell);
+// Scratch of launch_full_list: per-chunk boxes and cells, full_list_scratch_bytes(n, ncell).
+size_t full_list_scratch_bytes(int n, int ncell);
 int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
                      const double* y, const double* z, const int* cell_start, int cap,
-                     int* count, int* nbrs, int* overflow, cudaStream_t st);
+                     int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st);
 int launch_gather_f64(int n, const int* perm, const double* src, double* dst, cudaStream_t st);
 int launch_gather_i32(int n, const int* perm, const int* src, int* dst, cudaStream_t st);
 int launch_gather_u64(int n, const int* perm, const unsigned long long* src,

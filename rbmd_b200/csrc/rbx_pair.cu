@@ -148,19 +148,69 @@ __device__ __forceinline__ float fixed_d2(const uint4& ai, const uint4& aj) {
   return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 
-// Per-warp queue of force-carrying pairs.  Mixed form: the FP32 pair vector
-// and q_j are captured at push time; plain FP64 form: only j is queued and the
-// drain gathers the FP64 position, charge and type of all 32 pairs at once.
+// ---------------------------------------------------------------------------
+// Bulk asynchronous global->shared copies (cp.async.bulk) tracked by an
+// mbarrier.  Used to prefetch the next atom's candidate row into shared memory
+// while the warp works on the current one.  Every wait is bounded.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_row_copy(int* dst, const int* src, unsigned bytes,
+                                              unsigned long long* bar) {
+  // order earlier generic-proxy reads of dst before the async-proxy write
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase `parity` of bar; false after a bounded number of tries.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  for (int it = 0; it < (1 << 22); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// Bytes of a candidate row copy: 16-byte multiple, at least 16, within the row.
+__device__ __forceinline__ unsigned row_bytes(int cnt, int cap) {
+  unsigned b = ((unsigned)cnt * 4u + 15u) & ~15u;
+  b = b < 16u ? 16u : b;
+  const unsigned capb = (unsigned)cap * 4u;
+  return b > capb ? capb : b;
+}
+
+// Per-warp queue of force-carrying pairs: only j (with the shell flag in the
+// sign bit) is queued; the drain gathers what the 32 pairs need at once (the
+// fixed-point record in the mixed form, FP64 position and charge in the plain
+// form), which keeps the queue small and the block's shared memory low.
 constexpr int RBL_UNROLL = 4;                    // 32-candidate chunks per batch
 constexpr int RBL_QCAP = 32 + 32 * RBL_UNROLL;   // queue stays below 32 between batches
 
-struct QueueMixed {
-  float4 v[PAIR_WARPS][RBL_QCAP];  // dx, dy, dz, q_j
-  int j[PAIR_WARPS][RBL_QCAP];
-};
 struct QueueF64 {
   int j[PAIR_WARPS][RBL_QCAP];
 };
+using QueueMixed = QueueF64;  // the drain re-reads the (L1-resident) fixed-point record
 
 // LJ 12-6 force/r in FP32 with one fast reciprocal (mixed form only).
 __device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
@@ -182,7 +232,7 @@ __device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
 // force-carrying pairs are appended to a per-warp queue and consumed 32 at a
 // time from its tail.
 // ---------------------------------------------------------------------------
-template <bool MIXED, bool POW2>
+template <bool MIXED, bool POW2, bool PREFETCH>
 __global__ void __launch_bounds__(PAIR_BLOCK, 3)
 k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
             const double* __restrict__ y, const double* __restrict__ z,
@@ -191,9 +241,11 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
             const unsigned long long* __restrict__ key_b, int epoch,
             const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
             double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-            double* __restrict__ fpart) {
+            double* __restrict__ fpart, int* __restrict__ status) {
   using T = typename std::conditional<MIXED, float, double>::type;
   using Queue = typename std::conditional<MIXED, QueueMixed, QueueF64>::type;
+  extern __shared__ __align__(128) int s_rows[];  // PREFETCH: [PAIR_WARPS][2][cap]
+  __shared__ __align__(8) unsigned long long s_bar[PAIR_WARPS][2];
   __shared__ TypeTables tt;
   __shared__ Queue qu;
   __shared__ double s_acc[PAIR_WARPS][3];
@@ -213,7 +265,25 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
   const T freq_t = (T)pp.freq;
   double acc0 = 0, acc1 = 0, acc2 = 0;
   const int nt = pp.ntypes;
-  for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += gridDim.x * PAIR_WARPS) {
+  const int wstride = gridDim.x * PAIR_WARPS;
+  const int i0 = blockIdx.x * PAIR_WARPS + warp;
+  int* rowbuf = s_rows + (size_t)warp * 2 * cap;
+  int cnt_next = 0;
+  if (PREFETCH) {
+    if (lane == 0) {
+      mbar_init(&s_bar[warp][0], 1);
+      mbar_init(&s_bar[warp][1], 1);
+      mbar_fence_init();
+    }
+    __syncwarp();
+    if (i0 < n) {
+      const int c0 = cand_count[i0];
+      if (lane == 0) bulk_row_copy(rowbuf, cand + (size_t)i0 * cap, row_bytes(c0, cap), &s_bar[warp][0]);
+      if (i0 + wstride < n) cnt_next = cand_count[i0 + wstride];
+    }
+  }
+  int t = 0;
+  for (int i = i0; i < n; i += wstride, ++t) {
     const uint4 ai = atoms[i];
     const double xi = x[i], yi = y[i], zi = z[i];
     const T qi = MIXED ? (T)__uint_as_float(ai.w) : (T)q[i];
@@ -221,6 +291,23 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
     const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
     const int cnt = cand_count[i];
     const int* row = cand + (size_t)i * cap;
+    if (PREFETCH) {
+      const int b = t & 1;
+      const int inext = i + wstride;
+      if (inext < n) {  // prefetch the next row into the other buffer
+        if (lane == 0)
+          bulk_row_copy(rowbuf + (size_t)(b ^ 1) * cap, cand + (size_t)inext * cap,
+                        row_bytes(cnt_next, cap), &s_bar[warp][b ^ 1]);
+        cnt_next = inext + wstride < n ? cand_count[inext + wstride] : 0;
+      }
+      if (!mbar_wait_bounded(&s_bar[warp][b], (unsigned)((t >> 1) & 1))) {
+        if (lane == 0) atomicOr(status, 4);  // a row copy never completed
+        if (inext < n)  // let the prefetch just issued land before leaving (bounded)
+          mbar_wait_bounded(&s_bar[warp][b ^ 1], (unsigned)(((t + 1) >> 1) & 1));
+        break;
+      }
+      row = rowbuf + (size_t)b * cap;
+    }
     int qn = 0;
     T fxa = 0, fya = 0, fza = 0;
 
@@ -230,7 +317,10 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
       const int j = c & 0x7fffffff;
       const int tj = __ldg(type + j);
       if (MIXED) {
-        const float4 v = reinterpret_cast<const QueueMixed&>(qu).v[warp][slot];
+        const uint4 aj = __ldg(atoms + j);  // exact wrapped fixed-point difference r_j - r_i
+        const float4 v = make_float4((float)(int)(aj.x - ai.x) * pp.sf[0],
+                                     (float)(int)(aj.y - ai.y) * pp.sf[1],
+                                     (float)(int)(aj.z - ai.z) * pp.sf[2], __uint_as_float(aj.w));
         const float d2 = fmaf(v.x, v.x, fmaf(v.y, v.y, v.z * v.z));
         const float qq = (float)qi * v.w;
         float f = lj_f32_fast(f_eps[ti * nt + tj], f_s6[ti * nt + tj], d2);
@@ -261,7 +351,7 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
 #pragma unroll
       for (int u = 0; u < RBL_UNROLL; ++u) {
         const int k = k0 + u * 32 + lane;
-        jj[u] = k < cnt ? __ldg(row + k) : i;
+        jj[u] = k < cnt ? row[k] : i;
       }
 #pragma unroll
       for (int u = 0; u < RBL_UNROLL; ++u) aa[u] = __ldg(atoms + jj[u]);
@@ -298,11 +388,6 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
         if (push) {
           const int pos = qn + __popc(m & lt);
           qu.j[warp][pos] = ((core_bits >> u) & 1u) ? jj[u] : (jj[u] | (int)0x80000000);
-          if (MIXED)  // exact wrapped fixed-point difference r_j - r_i
-            reinterpret_cast<QueueMixed&>(qu).v[warp][pos] =
-                make_float4((float)(int)(aa[u].x - ai.x) * pp.sf[0],
-                            (float)(int)(aa[u].y - ai.y) * pp.sf[1],
-                            (float)(int)(aa[u].z - ai.z) * pp.sf[2], __uint_as_float(aa[u].w));
         }
         qn += __popc(m);
       }
@@ -728,28 +813,46 @@ int rbl_fused_blocks(int n) {
   return b < 1 ? 1 : b;
 }
 
+int rbl_prefetch_smem(int cap) { return PAIR_WARPS * 2 * cap * (int)sizeof(int); }
+constexpr int kRblMaxDynSmem = 160 * 1024;  // prefetch buffers used up to this size
+
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
                      const double* x, const double* y, const double* z, const double* q,
                      const int* type, const unsigned long long* key_a,
                      const unsigned long long* key_b, int epoch, const int* cand_count,
                      const int* cand, int cap, double* fx, double* fy, double* fz, double* fpart,
-                     int nblocks, cudaStream_t st) {
+                     int nblocks, int* status, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
   const bool pow2 = pp.freq >= 1 && (pp.freq & (pp.freq - 1)) == 0;
-#define RBX_LAUNCH_RBL(M, P2)                                                                  \
-  k_rbl_fused<M, P2><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, key_a,   \
-                                                     key_b, epoch, cand_count, cand, cap, fx, \
-                                                     fy, fz, fpart)
+  // candidate rows prefetched into shared memory when both buffers fit
+  const int dyn = rbl_prefetch_smem(cap);
+  const bool prefetch = status != nullptr && dyn <= kRblMaxDynSmem;
+#define RBX_LAUNCH_RBL(M, P2, PF)                                                               \
+  do {                                                                                         \
+    auto kern = k_rbl_fused<M, P2, PF>;                                                        \
+    const int smem = PF ? dyn : 0;                                                             \
+    static bool attr_set = false; /* once per instantiation and process */                     \
+    if (PF && !attr_set) {                                                                     \
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kRblMaxDynSmem); \
+      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);         \
+      attr_set = true;                                                                         \
+    }                                                                                          \
+    kern<<<nblocks, PAIR_BLOCK, smem, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b,      \
+                                            epoch, cand_count, cand, cap, fx, fy, fz, fpart,   \
+                                            status);                                           \
+  } while (0)
   if (mixed) {
-    if (pow2)
-      RBX_LAUNCH_RBL(true, true);
-    else
-      RBX_LAUNCH_RBL(true, false);
+    if (pow2) {
+      if (prefetch) RBX_LAUNCH_RBL(true, true, true); else RBX_LAUNCH_RBL(true, true, false);
+    } else {
+      if (prefetch) RBX_LAUNCH_RBL(true, false, true); else RBX_LAUNCH_RBL(true, false, false);
+    }
   } else {
-    if (pow2)
-      RBX_LAUNCH_RBL(false, true);
-    else
-      RBX_LAUNCH_RBL(false, false);
+    if (pow2) {
+      if (prefetch) RBX_LAUNCH_RBL(false, true, true); else RBX_LAUNCH_RBL(false, true, false);
+    } else {
+      if (prefetch) RBX_LAUNCH_RBL(false, false, true); else RBX_LAUNCH_RBL(false, false, false);
+    }
   }
 #undef RBX_LAUNCH_RBL
   count_launch();
