@@ -48,26 +48,63 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    every 2 ms (read-only queries), else nvidia-smi every 200 ms."""
 
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index=0):
-        self.gpu = gpu_index
-        self.rows = []
+    def __init__(self, cuda_device=0):
+        self.dev = cuda_device
+        self.sm, self.sm_max, self.reasons = [], [], set()
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+
+    def _nvml_handle(self):
+        import pynvml as N
+        import torch
+
+        N.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.dev)
+        try:
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return N, N.nvmlDeviceGetHandleByPciBusId_v2(bus)
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.dev)
 
     def _run(self):
-        while not self._stop.is_set():
+        try:
+            N, h = self._nvml_handle()
+            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                self.sm.append(float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)))
+                self.sm_max.append(float(mx))
+                bits = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, attr in self.REASONS:
+                    if bits & getattr(N, attr):
+                        self.reasons.add(name)
+                self._stop.wait(0.002)
+            return
+        except Exception:
+            pass
+        while not self._stop.is_set():  # fallback: nvidia-smi
             try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}",
+                out = subprocess.run(["nvidia-smi", f"--id={self.dev}",
                                       f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits"],
                                      capture_output=True, text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
+                r = [c.strip() for c in out.split(",")]
+                if len(r) >= 9:
+                    self.sm.append(float(r[1]))
+                    self.sm_max.append(float(r[2]))
+                    for k, (name, _) in enumerate(self.REASONS):
+                        if r[5 + k].lower() == "active":
+                            self.reasons.add(name)
             except Exception:
                 pass
             self._stop.wait(0.2)
@@ -83,16 +120,10 @@ class ClockSampler:
             self._t.join(timeout=10)
 
     def summary(self):
-        if not self.rows:
+        if not self.sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4)
-                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+        return {"sm_mhz": float(np.median(self.sm)), "sm_max_mhz": max(self.sm_max),
+                "reasons": sorted(self.reasons), "samples": len(self.sm)}
 
 
 def _dist():
@@ -109,6 +140,25 @@ def _init_pg(ws, backend):
     if ws > 1 and not dist.is_initialized():
         dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
     return dist
+
+
+def max_over_ranks(value, ws, device):
+    """The largest of every rank's `value` (each rank passes its own), through
+    an all-reduce on `device` ("cuda" with NCCL, "cpu" with gloo)."""
+    if ws <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(ws, n, steps, ms):
+    """Whole-job atom-steps/s: every rank advances its own n-atom replica
+    `steps` times; `ms` is the slowest rank's device time."""
+    return ws * n * steps / (ms / 1e3)
 
 
 def cpu_baseline(n, p, steps, warmup):
@@ -178,7 +228,7 @@ def run_ours(args):
                "energy_kspace": abs(parts[1][3].e_kspace - parts[0][3].e_kspace) /
                abs(parts[0][3].e_kspace)}
 
-    def timed(precision, steps, warmup, profile=False):
+    def timed(precision, steps, warmup, profile=False, clk=None):
         e = rbx.Engine(s, precision=precision, seed=77 + rank, device=local)
         e.compute_forces(0)
         e.step(warmup)
@@ -190,17 +240,18 @@ def run_ours(args):
         if dist and ws > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        if clk:
+            clk.__enter__()
         l0 = rbx.launch_count()
         ev0.record(st)
         e.step(steps)
         ev1.record(st)
         torch.cuda.synchronize()
+        if clk:
+            clk.__exit__()
         launches = rbx.launch_count() - l0
         ms = ev0.elapsed_time(ev1)
-        if dist and ws > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, ws, "cuda")
         phases = e.phase_ms() if profile else None
         stats = e.stats()
         return e, ms, launches, phases, stats
@@ -209,37 +260,40 @@ def run_ours(args):
     e64, ms64, _, ph64, _ = timed(rbx.PLAIN_FP64, args.steps, args.warmup, profile=True)
     e64.close()
     # ---- mixed form (headline), clocks sampled during the timed region
-    with ClockSampler(local) as clk:
-        em, ms, launches, _, stats = timed(rbx.MIXED, args.steps, args.warmup)
+    clk = ClockSampler(local)
+    em, ms, launches, _, stats = timed(rbx.MIXED, args.steps, args.warmup, clk=clk)
     em.close()
     # per-phase device times of the mixed step (separate profiled run)
     em2, _, _, phm, stats2 = timed(rbx.MIXED, args.steps, args.warmup, profile=True)
     em2.close()
 
-    # ---- end to end through the host-buffer C-ABI call
+    # ---- end to end through the host-buffer C-ABI call: each step copies x, v
+    # in from pinned host memory and x, v, F back; buffers alternate so the
+    # outputs of one step are the inputs of the next without a host copy
     e2 = rbx.Engine(s, precision=rbx.MIXED, seed=5, device=local)
     e2.compute_forces(0)
-    xin = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
-    vin = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
-    xo = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
-    vo = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
+    bufs = [[torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+            for _ in range(2)]  # bufs[k] = [x, v] of parity k
     fo = torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy()
-    xin[:] = s["pos"].T
-    vin[:] = s["vel"].T
+    bufs[0][0][:] = s["pos"].T
+    bufs[0][1][:] = s["vel"].T
+    k = 0
     for _ in range(args.warmup):
-        e2.step_host(xin, vin, xo, vo, fo)
-        xin[:], vin[:] = xo, vo
+        e2.step_host(bufs[k][0], bufs[k][1], bufs[1 - k][0], bufs[1 - k][1], fo)
+        k = 1 - k
+    st2 = torch.cuda.ExternalStream(e2.stream)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
     if dist and ws > 1:
         dist.barrier()
-    t0 = time.perf_counter()
+    torch.cuda.synchronize()
+    ev0.record(st2)
     for _ in range(args.steps):
-        e2.step_host(xin, vin, xo, vo, fo)
-        xin[:], vin[:] = xo, vo
-    e2e_s = time.perf_counter() - t0
-    if dist and ws > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2.step_host(bufs[k][0], bufs[k][1], bufs[1 - k][0], bufs[1 - k][1], fo)
+        k = 1 - k
+    ev1.record(st2)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), ws, "cuda")
     e2.close()
 
     if rank != 0:
@@ -248,8 +302,8 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
 
-    value = ws * n * args.steps / (ms / 1e3)
-    v64 = ws * n * args.steps / (ms64 / 1e3)
+    value = job_throughput(ws, n, args.steps, ms)
+    v64 = job_throughput(ws, n, args.steps, ms64)
     peaks, peak_src = _peaks()
     # roofline of the fused RBL kernel (phase 2 of the profiled mixed step)
     cand_per_atom = stats2.candidates / n
@@ -279,7 +333,7 @@ def run_ours(args):
         "phase_ms_mixed": {"kick_drift": phm[0], "skin_rebuild": phm[1], "real_space": phm[2],
                            "kspace": phm[3]},
         "rebuilds_per_step": stats.rebuilds / max(1, stats.steps + 1),
-        "e2e": {"value": ws * n * args.steps / e2e_s, "unit": UNIT,
+        "e2e": {"value": job_throughput(ws, n, args.steps, e2e_ms), "unit": UNIT,
                 "h2d_bytes_per_step": 6 * 8 * n, "d2h_bytes_per_step": 9 * 8 * n},
         "gpu_launches": launches,
         "roofline": roof,

@@ -268,7 +268,7 @@ int rbx_rbe_structure_factor(const rbx_box* box, int num_atoms, int p_number,
   if (!rc)
     rc = launch_rbe_finalize(b, p_number, nb, pr, pi, p_sample_x, p_sample_y, p_sample_z, 1.0,
                              0.0, 1.0, 0.0, 0.0, density_real, density_imag, nullptr, nullptr,
-                             nullptr, 0, nullptr, 0, nullptr, st);
+                             nullptr, 0, nullptr, 0, nullptr, nullptr, st);
   cudaFreeAsync(pr, st);
   cudaFreeAsync(pi, st);
   return rc;
@@ -293,7 +293,7 @@ int rbx_rbe_force(const rbx_box* box, int num_atoms, int p_number, double alpha,
   RBX_TRY(async_alloc(&tab, (size_t)p_number, st));
   int rc = launch_rbe_finalize(b, p_number, 1, real_array, imag_array, p_sample_x, p_sample_y,
                                p_sample_z, alpha, rbe_sum_gauss, qqr2e, 0.0, 0.0, nullptr,
-                               nullptr, nullptr, nullptr, tab, 0, nullptr, 0, nullptr, st);
+                               nullptr, nullptr, nullptr, tab, 0, nullptr, 0, nullptr, nullptr, st);
   if (!rc) {
     RbeForceOut o;
     o.f_out_x = fx;
@@ -319,7 +319,8 @@ int rbx_rbe_energy_virial(const rbx_box* box, int p, double alpha, double rbe_su
   const DBox b = make_dbox(*box);
   return launch_rbe_finalize(b, p, 1, real_array, imag_array, p_sample_x, p_sample_y, p_sample_z,
                              alpha, rbe_sum_gauss, qqrd2e, qsqsum, qsum, nullptr, nullptr, energy,
-                             virial_tensor, nullptr, 0, nullptr, 0, nullptr, (cudaStream_t)stream);
+                             virial_tensor, nullptr, 0, nullptr, 0, nullptr, nullptr,
+                             (cudaStream_t)stream);
 }
 
 int rbx_ewald_force(const rbx_box* box, int num_atoms, const int kmax[3], double alpha,
@@ -603,5 +604,5 @@ extern "C" int rbx_rbe_structure_factor_noalloc(const rbx_box* box, int num_atom
   }
   return launch_rbe_finalize(b, p_number, nb, pr, pi, p_sample_x, p_sample_y, p_sample_z, 1.0, 0.0,
                              1.0, 0.0, 0.0, density_real, density_imag, nullptr, nullptr, nullptr,
-                             0, nullptr, 0, nullptr, st);
+                             0, nullptr, 0, nullptr, nullptr, st);
 }

@@ -53,6 +53,23 @@ __device__ __forceinline__ unsigned long long rbl_mix(unsigned long long v) {
   return v ^ (v >> 31);
 }
 
+// Batch test mix(key) % freq == 0 for freq in {1, 2, 4} (mask = freq - 1).
+// h = v ^ (v >> 31) for the last product v = w * C2, so h's two low bits need
+// only bits 0, 1, 31 and 32 of v, i.e. v mod 2^33: the 32x32->64 product of
+// the low halves of w and C2, with bit 32 flipped by the parity of
+// w_hi * C2_lo + w_lo * C2_hi (both halves of C2 are odd).
+__device__ __forceinline__ bool rbl_selected_low2(unsigned long long key, unsigned mask) {
+  unsigned long long v = key + 0x9e3779b97f4a7c15ULL;
+  v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+  const unsigned w_lo = lo ^ __funnelshift_r(lo, hi, 27);  // low half of v ^ (v >> 27)
+  const unsigned w_32 = (hi ^ (hi >> 27)) & 1u;             // its bit 32
+  const unsigned long long p = (unsigned long long)w_lo * 0x133111ebu;
+  const unsigned p_lo = (unsigned)p;
+  const unsigned v32 = ((unsigned)(p >> 32) ^ w_32 ^ w_lo) & 1u;
+  return ((p_lo ^ (p_lo >> 31) ^ (v32 << 1)) & mask) == 0u;
+}
+
 // Per-atom halves of the RBL pair key: A_i = mix(gid_i), B_j = mix(gid_j + C).
 __device__ __forceinline__ unsigned long long rbl_key_a(int gid) {
   return rbl_mix((unsigned long long)(long long)gid);

@@ -168,6 +168,7 @@ int rbx_engine::init() {
     ETRY(alloc(&rho_re, (size_t)P));
     ETRY(alloc(&rho_im, (size_t)P));
     ETRY(alloc(&tab, (size_t)P));
+    ETRY(alloc(&kterm, (size_t)8 * P));
     // Philox sampler tables
     std::vector<double> w;
     int off = 0;
@@ -208,6 +209,7 @@ int rbx_engine::init() {
   pp.sqrt_alpha = sqrt(prm.alpha);
   pp.qqr2e = prm.qqr2e;
   pp.freq = freq;
+  nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, freq, n, cap, nfpart);
   pp.div = div;
   pp.ntypes = prm.ntypes;
   pp.lj_eps = lj_eps;
@@ -322,6 +324,7 @@ int rbx_engine::rebuild() {
     release(cand);
     cap = ((int)(maxc * 1.2) + 31) / 32 * 32;
     ETRY(alloc(&cand, (size_t)n * cap));
+    nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart);
   }
   set_error("candidate list capacity did not converge");
   return RBX_ERR_CAPACITY;
@@ -348,7 +351,7 @@ int rbx_engine::real_space() {
   const bool mixed = prm.precision == RBX_MIXED;
   if (prm.neighbor_type == RBX_NEIGHBOR_RBL)
     return launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, cand_count,
-                            cand, cap, fpx, fpy, fpz, fpart, nfpart, dflags + 3, st);
+                            cand, cap, fpx, fpy, fpz, fpart, nrbl, dflags + 3, st);
   return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, fpx, fpy,
                                  fpz, nullptr, epart, nfpart, st);
 }
@@ -370,8 +373,8 @@ int rbx_engine::kspace_and_combine(bool kick) {
   }
   ETRY(launch_rbe_finalize(dbox, P, P > 0 ? nparts : 0, part_re, part_im, mx, my, mz, prm.alpha,
                            S, prm.qqr2e, qsq, qsum, P > 0 ? rho_re : nullptr, rho_im,
-                           P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr, rbl ? nfpart : 0,
-                           fpart, n, rbl ? mean : nullptr, st));
+                           P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr, rbl ? nrbl : 0,
+                           fpart, n, rbl ? mean : nullptr, kterm, st));
   RbeForceOut o;
   o.f_pair_x = fpx;
   o.f_pair_y = fpy;
@@ -432,7 +435,6 @@ int rbx_engine::check_sampler() {
 int rbx_engine::step(int nsteps) {
   cudaSetDevice(device);
   if (!have_forces) ETRY(compute_forces(epoch));
-  const bool mixed = prm.precision == RBX_MIXED;
   for (int s = 0; s < nsteps; ++s) {
     cudaEvent_t* e = nullptr;
     if (profiling) {

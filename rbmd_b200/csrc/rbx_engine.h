@@ -47,7 +47,8 @@ struct rbx_engine {
   int *cand_count = nullptr, *cand = nullptr;
 
   // reductions, flags
-  int nfpart = 0;
+  int nfpart = 0;  // capacity of fpart / epart (blocks)
+  int nrbl = 0;    // blocks of the fused RBL launch (depends on cap)
   double *fpart = nullptr, *epart = nullptr, *mean = nullptr;
   int* dflags = nullptr;  // [0] cell sort, [1] list overflow, [2] sampler
   unsigned long long* max_d2 = nullptr;
@@ -61,6 +62,7 @@ struct rbx_engine {
   int* mi = nullptr;
   double *part_re = nullptr, *part_im = nullptr, *rho_re = nullptr, *rho_im = nullptr;
   rbx::KTab* tab = nullptr;
+  double* kterm = nullptr;  // per-k energy/virial terms [P][8]
   double *ek = nullptr, *virk = nullptr;
   double* sample_tables = nullptr;
   int tcnt[3] = {0, 0, 0};

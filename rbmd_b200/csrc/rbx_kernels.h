@@ -47,7 +47,9 @@ int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
                         const double* mz, double alpha, double S, double qqr2e, double qsq,
                         double qsum, double* rho_re, double* rho_im, double* energy,
                         double* virial, KTab* tab, int mean_parts, const double* fpart,
-                        int n_atoms, double* mean_out, cudaStream_t st);
+                        int n_atoms, double* mean_out, double* kterm, cudaStream_t st);
+// kterm: scratch of 8 p doubles for the per-k energy/virial terms (parallel
+// finalize); when null and energy is requested, one block does the finalize.
 int launch_rbe_force_f64(int n, int p, const KTab* tab, const double* q, const double* x,
                          const double* y, const double* z, const RbeForceOut& out,
                          cudaStream_t st);
@@ -97,6 +99,9 @@ struct PairParams {
 // Fused RBL filter + pair force over a row-major candidate list.
 // fpart (nblocks x 3) receives per-block force sums for the mean removal.
 int rbl_fused_blocks(int n);
+// Grid of the fused RBL kernel for this form: one wave of resident blocks,
+// at most max_blocks (the capacity of the per-block partial buffer).
+int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks);
 // status (device int, may be null = no prefetch): bit 4 set if a row copy timed out.
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
                      const double* x, const double* y, const double* z, const double* q,

@@ -17,6 +17,8 @@
 // RBL mean-force removal.
 #include <math.h>
 
+#include <atomic>
+
 #include <type_traits>
 
 #include "rbx_common.cuh"
@@ -127,18 +129,22 @@ __device__ __forceinline__ double exact_d2(const PairParams& pp, const double* _
                     __ldg(y + j), __ldg(z + j));
 }
 
-// Screened classification; *unsure is set when a threshold band is hit.
+// Screened classification; *unsure is set when a threshold band is hit.  The
+// band around core2_list and the one around rs2 (which lies just above it)
+// are merged into one undecided interval, as are d2 values at or below the
+// EPS band: each undecided pair is settled by the FP64 predicate, so five
+// comparisons classify a pair.
 __device__ __forceinline__ Classified classify_screen(const PairParams& pp, float d2s,
                                                       bool* unsure) {
-  const bool A = d2s < pp.sc_core.lo, nA = d2s >= pp.sc_core.hi;
-  const bool B = d2s < pp.sc_force.lo, nB = d2s >= pp.sc_force.hi;
-  const bool E = d2s > pp.sc_eps.hi, nE = d2s <= pp.sc_eps.lo;
-  const bool D = d2s > pp.sc_rs.hi, nD = d2s <= pp.sc_rs.lo;
-  // undecided predicates matter only where they can change the outcome
-  *unsure = (!A && !nA) || (nA && !B && !nB) || (A && !E && !nE) || (nA && B && !D && !nD);
+  const bool A = d2s < pp.sc_core.lo;    // certainly d2 < core2_list
+  const bool B = d2s <= pp.sc_rs.hi;     // not certainly d2 > rs2
+  const bool C = d2s < pp.sc_force.lo;   // certainly d2 < force2_list
+  const bool D = d2s < pp.sc_force.hi;   // not certainly d2 >= force2_list
+  const bool E = d2s <= pp.sc_eps.hi;    // not certainly d2 > EPS
+  *unsure = (!A && B) || (!C && D) || E;
   Classified c;
-  c.core_active = A && E;
-  c.shell_window = nA && B && D;
+  c.core_active = A;
+  c.shell_window = !B && C;
   return c;
 }
 
@@ -222,8 +228,9 @@ __device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
 // ---------------------------------------------------------------------------
 // Fused RBL filter + pair force.  MIXED = false: plain FP64 (pair vector and
 // force math in FP64 from the FP64 positions).  MIXED = true: FP32 force math
-// on the exact fixed-point pair vector.  POW2: freq is a power of two, so the
-// batch test is a mask.
+// on the exact fixed-point pair vector.  SEL selects the batch test: 0 any
+// freq (divisibility by multiplication), 1 freq a power of two (mask), 2
+// freq <= 4 (two bits of a partial hash).
 //
 // The warp walks atom i's candidate row in batches of RBL_UNROLL x 32: index
 // loads and neighbour-record gathers of a batch are all issued before any is
@@ -232,7 +239,7 @@ __device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
 // force-carrying pairs are appended to a per-warp queue and consumed 32 at a
 // time from its tail.
 // ---------------------------------------------------------------------------
-template <bool MIXED, bool POW2, bool PREFETCH>
+template <bool MIXED, int SEL, bool PREFETCH>
 __global__ void __launch_bounds__(PAIR_BLOCK, 3)
 k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
             const double* __restrict__ y, const double* __restrict__ z,
@@ -363,8 +370,13 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
         Classified c{false, false};
         if (pp.cubic) c = classify_screen(pp, fixed_d2(ai, aa[u]), &unsure);
         // shell batch hash (RblShellSampleSelected)
-        const unsigned long long h = rbl_mix(ea ^ __ldg(key_b + jj[u]));
-        const bool sel = POW2 ? (h & fmask) == 0ULL : divisible(h, pp.div);
+        bool sel;
+        if (SEL == 2) {
+          sel = rbl_selected_low2(ea ^ __ldg(key_b + jj[u]), (unsigned)fmask);
+        } else {
+          const unsigned long long h = rbl_mix(ea ^ __ldg(key_b + jj[u]));
+          sel = SEL == 1 ? (h & fmask) == 0ULL : divisible(h, pp.div);
+        }
         core_bits |= (unsigned)(valid && c.core_active) << u;
         shell_bits |= (unsigned)(valid && c.shell_window) << u;
         sel_bits |= (unsigned)sel << u;
@@ -807,7 +819,8 @@ IntScreen make_screen(double C, double L, double band) {
 }
 
 int rbl_fused_blocks(int n) {
-  const int target = sm_count() * 8;  // 8 resident 256-thread blocks per SM
+  // capacity of the per-block partial buffers: enough for rbl_fused_grid
+  const int target = sm_count() * 32;
   int b = (n + PAIR_WARPS - 1) / PAIR_WARPS;
   if (b > target) b = target;
   return b < 1 ? 1 : b;
@@ -816,6 +829,63 @@ int rbl_fused_blocks(int n) {
 int rbl_prefetch_smem(int cap) { return PAIR_WARPS * 2 * cap * (int)sizeof(int); }
 constexpr int kRblMaxDynSmem = 160 * 1024;  // prefetch buffers used up to this size
 
+namespace {
+using RblKernel = void (*)(PairParams, int, const uint4*, const double*, const double*,
+                           const double*, const double*, const int*, const unsigned long long*,
+                           const unsigned long long*, int, const int*, const int*, int, double*,
+                           double*, double*, double*, int*);
+
+struct RblChoice {
+  RblKernel kern;
+  int smem;
+};
+
+// The instantiation a launch uses.  FP64 form: candidate rows prefetched into
+// shared memory when both buffers fit.  The mixed form runs faster at the
+// occupancy it keeps without them.
+RblChoice rbl_choose(bool mixed, int freq, int cap, bool with_status) {
+  const bool pow2 = freq >= 1 && (freq & (freq - 1)) == 0;
+  const int sel = pow2 ? (freq <= 4 ? 2 : 1) : 0;
+  const int dyn = rbl_prefetch_smem(cap);
+  const bool prefetch = !mixed && with_status && dyn <= kRblMaxDynSmem;
+  static RblKernel const table[2][3][2] = {
+      {{k_rbl_fused<false, 0, false>, k_rbl_fused<false, 0, true>},
+       {k_rbl_fused<false, 1, false>, k_rbl_fused<false, 1, true>},
+       {k_rbl_fused<false, 2, false>, k_rbl_fused<false, 2, true>}},
+      {{k_rbl_fused<true, 0, false>, nullptr},
+       {k_rbl_fused<true, 1, false>, nullptr},
+       {k_rbl_fused<true, 2, false>, nullptr}}};
+  RblChoice c{table[mixed][sel][prefetch], prefetch ? dyn : 0};
+  if (prefetch) {  // opt in to large dynamic shared memory, once per instantiation
+    static std::atomic<int> done[3] = {};
+    if (!done[sel].exchange(1)) {
+      cudaFuncSetAttribute(c.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kRblMaxDynSmem);
+      cudaFuncSetAttribute(c.kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
+  }
+  return c;
+}
+}  // namespace
+
+int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks) {
+  // kRblWaves waves of resident blocks: with several waves the block
+  // scheduler evens out the per-atom work (200k atoms, mixed form: 1 wave
+  // 0.59 ms, 3 waves 0.555 ms, 6-12 waves 0.54 ms, 48 waves 0.57 ms)
+  constexpr int kRblWaves = 8;
+  const RblChoice c = rbl_choose(mixed, freq, cap, true);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, c.kern, PAIR_BLOCK, c.smem) !=
+          cudaSuccess || occ < 1) {
+    cudaGetLastError();
+    occ = 1;
+  }
+  int b = kRblWaves * occ * sm_count();
+  const int need = (n + PAIR_WARPS - 1) / PAIR_WARPS;
+  if (b > need) b = need;
+  if (b > max_blocks) b = max_blocks;
+  return b < 1 ? 1 : b;
+}
+
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
                      const double* x, const double* y, const double* z, const double* q,
                      const int* type, const unsigned long long* key_a,
@@ -823,38 +893,9 @@ int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms
                      const int* cand, int cap, double* fx, double* fy, double* fz, double* fpart,
                      int nblocks, int* status, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  const bool pow2 = pp.freq >= 1 && (pp.freq & (pp.freq - 1)) == 0;
-  // candidate rows prefetched into shared memory when both buffers fit
-  const int dyn = rbl_prefetch_smem(cap);
-  const bool prefetch = status != nullptr && dyn <= kRblMaxDynSmem;
-#define RBX_LAUNCH_RBL(M, P2, PF)                                                               \
-  do {                                                                                         \
-    auto kern = k_rbl_fused<M, P2, PF>;                                                        \
-    const int smem = PF ? dyn : 0;                                                             \
-    static bool attr_set = false; /* once per instantiation and process */                     \
-    if (PF && !attr_set) {                                                                     \
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kRblMaxDynSmem); \
-      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);         \
-      attr_set = true;                                                                         \
-    }                                                                                          \
-    kern<<<nblocks, PAIR_BLOCK, smem, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b,      \
-                                            epoch, cand_count, cand, cap, fx, fy, fz, fpart,   \
-                                            status);                                           \
-  } while (0)
-  if (mixed) {
-    if (pow2) {
-      if (prefetch) RBX_LAUNCH_RBL(true, true, true); else RBX_LAUNCH_RBL(true, true, false);
-    } else {
-      if (prefetch) RBX_LAUNCH_RBL(true, false, true); else RBX_LAUNCH_RBL(true, false, false);
-    }
-  } else {
-    if (pow2) {
-      if (prefetch) RBX_LAUNCH_RBL(false, true, true); else RBX_LAUNCH_RBL(false, true, false);
-    } else {
-      if (prefetch) RBX_LAUNCH_RBL(false, false, true); else RBX_LAUNCH_RBL(false, false, false);
-    }
-  }
-#undef RBX_LAUNCH_RBL
+  const RblChoice c = rbl_choose(mixed, pp.freq, cap, status != nullptr);
+  c.kern<<<nblocks, PAIR_BLOCK, c.smem, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
+                                              cand_count, cand, cap, fx, fy, fz, fpart, status);
   count_launch();
   return check_launch(mixed ? "rbl_fused_mixed" : "rbl_fused_f64");
 }

@@ -270,6 +270,104 @@ k_rbe_finalize(int p, int nparts, const double* __restrict__ part_re,
   }
 }
 
+// Parallel finalize: block k < p reduces the partials of k-vector k (fixed
+// strided order, then a fixed tree) and writes rho(k), the force table entry
+// and its seven energy/virial terms to kterm[k][0..6]; blocks p..p+2 reduce
+// the per-block pair-force sums into the mean force.  k_rbe_energy_sum then
+// adds the per-k terms in increasing k (one warp, fixed order).
+constexpr int FK_BLOCK = 128;
+
+__global__ void __launch_bounds__(FK_BLOCK)
+k_rbe_finalize_k(int p, int nparts, const double* __restrict__ part_re,
+                 const double* __restrict__ part_im, const double* __restrict__ mx,
+                 const double* __restrict__ my, const double* __restrict__ mz, double Lx,
+                 double Ly, double Lz, double alpha, double S, double qqr2e,
+                 double* __restrict__ rho_re, double* __restrict__ rho_im,
+                 KTab* __restrict__ tab, double* __restrict__ kterm, int mean_parts,
+                 const double* __restrict__ fpart, double n_atoms, double* __restrict__ mean_out) {
+  __shared__ double sh[FK_BLOCK / 32];
+  const int blk = blockIdx.x;
+  if (blk >= p) {  // mean of the pair-force block sums, one component per block
+    const int d = blk - p;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < mean_parts; b += FK_BLOCK) s += fpart[(size_t)b * 3 + d];
+    s = block_sum_det<FK_BLOCK>(s, sh);
+    if (threadIdx.x == 0) mean_out[d] = s / n_atoms;
+    return;
+  }
+  const int k = blk;
+  double r = 0.0, im = 0.0;
+  const double* pr = part_re + (size_t)k * nparts;
+  const double* pi = part_im + (size_t)k * nparts;
+  for (int b = threadIdx.x; b < nparts; b += FK_BLOCK) {
+    r += pr[b];
+    im += pi[b];
+  }
+  r = block_sum_det<FK_BLOCK>(r, sh);
+  im = block_sum_det<FK_BLOCK>(im, sh);
+  if (threadIdx.x != 0) return;
+  if (rho_re) {
+    rho_re[k] = r;
+    rho_im[k] = im;
+  }
+  const double V = Lx * Ly * Lz;
+  const double kx = 2 * RBX_PI * mx[k] / Lx;
+  const double ky = 2 * RBX_PI * my[k] / Ly;
+  const double kz = 2 * RBX_PI * mz[k] / Lz;
+  const double k2 = kx * kx + ky * ky + kz * kz;
+  if (kterm) {
+    const double coef = (2 * RBX_PI * S) / (p * V);
+    const double base = coef * (r * r + im * im) / k2;
+    const double inner = (1.0 / (4 * alpha)) + (1.0 / k2);
+    double* t = kterm + (size_t)k * 8;
+    t[0] = base;
+    t[1] = base * (1.0 - 2 * kx * kx * inner);
+    t[2] = base * (1.0 - 2 * ky * ky * inner);
+    t[3] = base * (1.0 - 2 * kz * kz * inner);
+    t[4] = base * (-2 * kx * ky * inner);
+    t[5] = base * (-2 * kx * kz * inner);
+    t[6] = base * (-2 * ky * kz * inner);
+  }
+  if (tab) {
+    const double c = (-4 * RBX_PI * qqr2e * S / p) / (V * k2);
+    KTab t;
+    t.kx = kx;
+    t.ky = ky;
+    t.kz = kz;
+    t.a = c * r;
+    t.b = c * im;
+    t.m[0] = (int)mx[k];
+    t.m[1] = (int)my[k];
+    t.m[2] = (int)mz[k];
+    t.m[3] = 0;
+    tab[k] = t;
+  }
+}
+
+__global__ void __launch_bounds__(32)
+k_rbe_energy_sum(int p, const double* __restrict__ kterm, double alpha, double V, double qqr2e,
+                 double qsq, double qsum, double* __restrict__ energy,
+                 double* __restrict__ virial) {
+  const int lane = threadIdx.x;
+  double t[7] = {0, 0, 0, 0, 0, 0, 0};
+  // each lane adds its k in increasing order; the seven loads of a k are independent
+  for (int k = lane; k < p; k += 32) {
+    const double* r = kterm + (size_t)k * 8;
+#pragma unroll
+    for (int c = 0; c < 7; ++c) t[c] += r[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 7; ++c)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t[c] += __shfl_down_sync(0xffffffffu, t[c], o);
+  if (lane == 0) {
+    const double MY_PIS = 1.77245385090551602729, MY_PI2 = 1.57079632679489661923;
+    const double etot = t[0] - (sqrt(alpha) * qsq / MY_PIS + MY_PI2 * qsum * qsum / (alpha * V));
+    *energy = etot * qqr2e;
+    for (int c = 0; c < 6; ++c) virial[c] = t[1 + c] * qqr2e;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Force scatter.  Thread per atom; the k table is staged in shared memory.
 // Epilogue variants: plain store of F_k, or the fused combine
@@ -432,16 +530,28 @@ __device__ __forceinline__ int table_pick(const double* cdf, int cnt, double tot
   return (idx & 1) ? (idx + 1) / 2 : -(idx / 2);
 }
 
-__global__ void k_rbe_sample(int p, const double* __restrict__ tables, int c0, int c1, int c2,
-                             double t0, double t1, double t2, uint32_t key0, uint32_t key1,
-                             uint64_t step, double* __restrict__ mx, double* __restrict__ my,
-                             double* __restrict__ mz, int* __restrict__ mi,
-                             int* __restrict__ status) {
+constexpr int kSampleSmemTables = 6144;  // staged table entries (48 KB)
+constexpr int SAMPLE_BLOCK = 128;
+
+__global__ void __launch_bounds__(SAMPLE_BLOCK)
+k_rbe_sample(int p, const double* __restrict__ tables, int c0, int c1, int c2, double t0,
+             double t1, double t2, uint32_t key0, uint32_t key1, uint64_t step,
+             double* __restrict__ mx, double* __restrict__ my, double* __restrict__ mz,
+             int* __restrict__ mi, int* __restrict__ status) {
+  // the three cumulative tables are staged in shared memory when they fit
+  // (dynamic size (c0 + c1 + c2) doubles), so the binary searches run there
+  extern __shared__ double s_tab[];
+  const int tot = c0 + c1 + c2;
+  const bool staged = tot <= kSampleSmemTables;
+  if (staged) {
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) s_tab[t] = tables[t];
+    __syncthreads();
+  }
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= p) return;
-  const double* w0 = tables;
-  const double* w1 = tables + c0;
-  const double* w2 = tables + c0 + c1;
+  const double* w0 = staged ? s_tab : tables;
+  const double* w1 = w0 + c0;
+  const double* w2 = w0 + c0 + c1;
   for (int a = 0; a < 64; ++a) {
     uint32_t c[4] = {(uint32_t)s, (uint32_t)(2 * a), (uint32_t)step, (uint32_t)(step >> 32)};
     philox4x32_10(c, key0, key1);
@@ -593,13 +703,31 @@ int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
                         const double* mz, double alpha, double S, double qqr2e, double qsq,
                         double qsum, double* rho_re, double* rho_im, double* energy,
                         double* virial, KTab* tab, int mean_parts, const double* fpart,
-                        int n_atoms, double* mean_out, cudaStream_t st) {
-  k_rbe_finalize<<<1, FIN_WIDE, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
-                                          b.len[1], b.len[2], alpha, S, qqr2e, qsq, qsum, rho_re,
-                                          rho_im, energy, virial, tab, mean_parts, fpart,
-                                          (double)n_atoms, mean_out);
-  count_launch();
-  return check_launch("rbe_finalize");
+                        int n_atoms, double* mean_out, double* kterm, cudaStream_t st) {
+  if (energy && !kterm) {  // no per-k scratch: one block does it all
+    k_rbe_finalize<<<1, FIN_WIDE, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
+                                            b.len[1], b.len[2], alpha, S, qqr2e, qsq, qsum,
+                                            rho_re, rho_im, energy, virial, tab, mean_parts, fpart,
+                                            (double)n_atoms, mean_out);
+    count_launch();
+    return check_launch("rbe_finalize");
+  }
+  const int grid = p + (mean_out ? 3 : 0);
+  if (grid > 0) {
+    k_rbe_finalize_k<<<grid, FK_BLOCK, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
+                                                b.len[1], b.len[2], alpha, S, qqr2e, rho_re,
+                                                rho_im, tab, energy ? kterm : nullptr, mean_parts,
+                                                fpart, (double)n_atoms, mean_out);
+    count_launch();
+    const int rc = check_launch("rbe_finalize_k");
+    if (rc) return rc;
+  }
+  if (energy) {
+    k_rbe_energy_sum<<<1, 32, 0, st>>>(p, kterm, alpha, b.len[0] * b.len[1] * b.len[2], qqr2e, qsq,
+                                      qsum, energy, virial);
+    count_launch();
+  }
+  return check_launch("rbe_energy_sum");
 }
 
 static ForceEpilogue make_ep(const RbeForceOut& o) {
@@ -646,9 +774,11 @@ int launch_rbe_sample(int p, const double* tables, const int cnt[3], const doubl
                       uint64_t seed, int64_t step, double* mx, double* my, double* mz, int* mi,
                       int* status, cudaStream_t st) {
   if (p <= 0) return RBX_OK;
-  k_rbe_sample<<<(p + 31) / 32, 32, 0, st>>>(p, tables, cnt[0], cnt[1], cnt[2], tot[0], tot[1],
-                                                tot[2], (uint32_t)seed, (uint32_t)(seed >> 32),
-                                                (uint64_t)step, mx, my, mz, mi, status);
+  const int entries = cnt[0] + cnt[1] + cnt[2];
+  const size_t smem = entries <= kSampleSmemTables ? sizeof(double) * entries : 0;
+  k_rbe_sample<<<(p + SAMPLE_BLOCK - 1) / SAMPLE_BLOCK, SAMPLE_BLOCK, smem, st>>>(
+      p, tables, cnt[0], cnt[1], cnt[2], tot[0], tot[1], tot[2], (uint32_t)seed,
+      (uint32_t)(seed >> 32), (uint64_t)step, mx, my, mz, mi, status);
   count_launch();
   return check_launch("rbe_sample");
 }
