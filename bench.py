@@ -37,6 +37,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "RBE+LJ atom-steps/s @200k atoms: mixed vs FP64 plain at <=1e-5 rel force err"
 UNIT = "atom-steps/s"
+# DRAM bytes (read + written) per atom of one mixed k_rbl_fused launch, from an ncu
+# capture of the same workload at N = 100,000 (209.2 MB per launch).  The candidate
+# rows are streamed once per launch, so the traffic scales with N.
+RBL_TRAFFIC_BYTES_PER_ATOM = 2092.0
 
 
 def _peaks():
@@ -312,7 +316,9 @@ def run_ours(args):
     achieved = alg_bytes / t_pair / 1e9
     roof = {"kernel": "k_rbl_fused_mixed", "bound": "hbm", "achieved": achieved,
             "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-            "peak_source": peak_src, "traffic": None,
+            "peak_source": peak_src, "traffic": RBL_TRAFFIC_BYTES_PER_ATOM * n,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at N=100000, "
+                              "scaled by N",
             "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": phm[2]}
     base = cpu_baseline(n, p, 2, 1) if not args.no_cpu_baseline else None
     line = {
