@@ -328,6 +328,14 @@ int rbx_engine_phase_ms(rbx_engine* e, float out[4]);
 /* Enable/disable CUDA events around the phases (off by default); resets the
  * accumulated phase times. */
 int rbx_engine_set_profiling(rbx_engine* e, int on);
+/* Run rbx_engine_step as a CUDA graph per MD step (on, the default) or as
+ * individual launches with the host deciding each rebuild (off).  The graph
+ * holds kick, drift, the skin check, the neighbour rebuild under a conditional
+ * node, the forces and the second kick, with no host synchronisation inside a
+ * call of rbx_engine_step; both give identical results.  Profiled steps always
+ * run as individual launches.  No counterpart in the reference (its
+ * NVEensemble::Solve launches and synchronises step by step). */
+int rbx_engine_set_step_graph(rbx_engine* e, int on);
 
 #ifdef __cplusplus
 }

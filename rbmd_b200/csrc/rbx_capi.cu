@@ -223,8 +223,8 @@ int rbx_rbe_sample(const rbx_box* box, double alpha, int p, uint64_t seed, int64
   RBX_TRY(async_alloc(&dstatus, 1, st));
   cudaMemcpyAsync(dtab, w, sizeof(double) * off, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(dstatus, 0, sizeof(int), st);
-  int rc = launch_rbe_sample(p, dtab, cnt, tot, seed, step, p_sample_x, p_sample_y, p_sample_z,
-                             nullptr, dstatus, st);
+  int rc = launch_rbe_sample(p, dtab, cnt, tot, seed, step, nullptr, p_sample_x, p_sample_y,
+                             p_sample_z, nullptr, dstatus, st);
   int hstatus = 0;
   if (!rc) {
     cudaMemcpyAsync(&hstatus, dstatus, sizeof(int), cudaMemcpyDeviceToHost, st);

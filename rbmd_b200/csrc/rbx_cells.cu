@@ -349,6 +349,41 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
 // ---------------------------------------------------------------------------
 // Gathers / scatters and integration.
 // ---------------------------------------------------------------------------
+__global__ void k_fill_i32(int n, int* __restrict__ p, int v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// One pass over a set of per-atom arrays: dst[a][i] = src[a][perm[i]] (perm
+// null: a plain copy).  The set's pointers are kernel parameters, so one
+// launch moves every array of the rebuild.
+__global__ void k_move_set(int n, const int* __restrict__ perm, ArraySet s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = perm ? perm[i] : i;
+#pragma unroll
+  for (int a = 0; a < ArraySet::kMaxF64; ++a)
+    if (a < s.nf64) s.dst_f64[a][i] = s.src_f64[a][p];
+#pragma unroll
+  for (int a = 0; a < ArraySet::kMaxI32; ++a)
+    if (a < s.ni32) s.dst_i32[a][i] = s.src_i32[a][p];
+#pragma unroll
+  for (int a = 0; a < ArraySet::kMaxU64; ++a)
+    if (a < s.nu64) s.dst_u64[a][i] = s.src_u64[a][p];
+}
+
+// Per-step decision inside the step graph: advance the device epoch and take
+// the rebuild branch when some atom moved more than skin / 2 since the last
+// rebuild (max_d2 holds the bits of a non-negative double).
+__global__ void k_step_decide(const unsigned long long* __restrict__ max_d2, double thr2,
+                              int* __restrict__ epoch, cudaGraphConditionalHandle rebuild) {
+  *epoch += 1;
+  cudaGraphSetConditional(rebuild, __longlong_as_double((long long)*max_d2) > thr2 ? 1u : 0u);
+}
+
+__global__ void k_zero_u64(unsigned long long* __restrict__ p) { *p = 0ULL; }
+
+__global__ void k_add_i32(int* __restrict__ p, int v) { *p += v; }
+
 template <typename T>
 __global__ void k_gather(int n, const int* __restrict__ perm, const T* __restrict__ src,
                          T* __restrict__ dst) {
@@ -483,10 +518,8 @@ int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, 
   unsigned* sub = (unsigned*)p;
   p += al(sizeof(int) * (size_t)n);
   unsigned* tmp = (unsigned*)p;
-  if (cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)ncell, st) != cudaSuccess) {
-    set_error("cudaMemsetAsync failed in cells_sort");
-    return RBX_ERR_CUDA;
-  }
+  k_fill_i32<<<grid_for(ncell, 256, sm_count() * 4), 256, 0, st>>>(ncell, counts, 0);
+  count_launch();
   if (n > 0) {
     k_cell_assign<<<(n + 255) / 256, 256, 0, st>>>(b, dims[0], dims[1], dims[2], n, x, y, z, cell,
                                                    sub, counts);
@@ -542,6 +575,39 @@ int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, con
       box_lo, box_hi, cell_of, cap, count, nbrs, overflow);
   count_launch();
   return check_launch("full_list");
+}
+
+int launch_move_set(int n, const int* perm, const ArraySet& set, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_move_set<<<(n + 255) / 256, 256, 0, st>>>(n, perm, set);
+  count_launch();
+  return check_launch("move_set");
+}
+
+int launch_fill_i32(int n, int* p, int v, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_fill_i32<<<grid_for(n, 256, sm_count() * 4), 256, 0, st>>>(n, p, v);
+  count_launch();
+  return check_launch("fill_i32");
+}
+
+int launch_zero_u64(unsigned long long* p, cudaStream_t st) {
+  k_zero_u64<<<1, 1, 0, st>>>(p);
+  count_launch();
+  return check_launch("zero_u64");
+}
+
+int launch_add_i32(int* p, int v, cudaStream_t st) {
+  k_add_i32<<<1, 1, 0, st>>>(p, v);
+  count_launch();
+  return check_launch("add_i32");
+}
+
+int launch_step_decide(const unsigned long long* max_d2, double thr2, int* epoch,
+                       cudaGraphConditionalHandle rebuild, cudaStream_t st) {
+  k_step_decide<<<1, 1, 0, st>>>(max_d2, thr2, epoch, rebuild);
+  count_launch();
+  return check_launch("step_decide");
 }
 
 int launch_gather_f64(int n, const int* perm, const double* src, double* dst, cudaStream_t st) {

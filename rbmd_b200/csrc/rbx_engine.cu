@@ -60,7 +60,17 @@ rbx_engine::~rbx_engine() {
   for (int i = 0; i < 8; ++i)
     if (ev[i]) cudaEventDestroy(ev[i]);
   for (cudaEvent_t e : pev) cudaEventDestroy(e);
+  release_graph();
+  if (st_body) cudaStreamDestroy(st_body);
   if (st) cudaStreamDestroy(st);
+}
+
+void rbx_engine::release_graph() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (graph) cudaGraphDestroy(graph);
+  graph_exec = nullptr;
+  graph = nullptr;
+  graph_dirty = true;
 }
 
 template <typename T>
@@ -83,6 +93,7 @@ int rbx_engine::init() {
   ETRY(cuda_ok(cudaSetDevice(device), "cudaSetDevice"));
   ETRY(require_device());
   ETRY(cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate"));
+  ETRY(cuda_ok(cudaStreamCreateWithFlags(&st_body, cudaStreamNonBlocking), "cudaStreamCreate"));
   dbox = make_dbox(box);
   const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
   if (!(prm.cut_off > 0.0) || prm.skin < 0.0 || (rbl && !(prm.r_core > 0.0)) ||
@@ -117,6 +128,12 @@ int rbx_engine::init() {
                       &fpx, &fpy, &fpz, &fkx, &fky, &fkz, &tmpd};
   for (double** p : dptrs) ETRY(alloc(p, N));
   ETRY(alloc(&stage, 9 * N));  // host transfer staging (x,v in; x,v,f out)
+  for (double*& p : shd) ETRY(alloc(&p, N));
+  for (int*& p : shi) ETRY(alloc(&p, N));
+  for (unsigned long long*& p : shu) ETRY(alloc(&p, N));
+  for (double*& p : snapd) ETRY(alloc(&p, N));
+  for (int*& p : snapi) ETRY(alloc(&p, N));
+  for (unsigned long long*& p : snapu) ETRY(alloc(&p, N));
   int** iptrs[] = {&type, &gid, &orig, &tmpi, &perm, &cell_of_sorted, &cand_count};
   for (int** p : iptrs) ETRY(alloc(p, N));
   ETRY(alloc(&key_a, N));
@@ -127,6 +144,7 @@ int rbx_engine::init() {
   ETRY(alloc(&cell_scratch, cells_scratch_bytes(n, ncell)));
   ETRY(alloc(&list_scratch, full_list_scratch_bytes(n, ncell)));
   ETRY(alloc(&dflags, 8));
+  ETRY(cuda_ok(cudaMemsetAsync(dflags, 0, sizeof(int) * 8, st), "memset"));
   ETRY(alloc(&max_d2, 1));
   ETRY(alloc(&cand_total, 1));
   nfpart = rbl_fused_blocks(n);
@@ -268,39 +286,94 @@ int rbx_engine::set_state(const int* hgid, const int* htype, const double* hq, c
   have_cache = false;
   have_forces = false;
   epoch = 0;
+  graph_dirty = true;
   return RBX_OK;
 }
 
-// Rebuild: cell sort, permute every per-atom array, candidate list.
-int rbx_engine::rebuild() {
-  int* status = dflags;
-  ETRY(cuda_ok(cudaMemsetAsync(dflags, 0, sizeof(int) * 8, st), "memset"));
-  ETRY(cuda_ok(cudaMemsetAsync(cand_total, 0, sizeof(long long), st), "memset"));
+// The per-atom arrays a rebuild permutes, moved into their shadows
+// (to_shadow, through perm) or copied back (with x0 = x for the skin check).
+ArraySet rbx_engine::permute_set(bool to_shadow) const {
+  ArraySet a{};
+  double* const pd[13] = {x, y, z, vx, vy, vz, fx, fy, fz, q, fpx, fpy, fpz};
+  int* const pi[3] = {type, gid, orig};
+  unsigned long long* const pu[2] = {key_a, key_b};
+  for (int k = 0; k < 13; ++k) {
+    a.src_f64[k] = to_shadow ? pd[k] : shd[k];
+    a.dst_f64[k] = to_shadow ? shd[k] : pd[k];
+  }
+  a.nf64 = 13;
+  if (!to_shadow) {  // positions at the rebuild, for the skin check
+    double* const p0[3] = {x0, y0, z0};
+    for (int k = 0; k < 3; ++k) {
+      a.src_f64[13 + k] = shd[k];
+      a.dst_f64[13 + k] = p0[k];
+    }
+    a.nf64 = 16;
+  }
+  for (int k = 0; k < 3; ++k) {
+    a.src_i32[k] = to_shadow ? pi[k] : shi[k];
+    a.dst_i32[k] = to_shadow ? shi[k] : pi[k];
+  }
+  a.ni32 = 3;
+  for (int k = 0; k < 2; ++k) {
+    a.src_u64[k] = to_shadow ? pu[k] : shu[k];
+    a.dst_u64[k] = to_shadow ? shu[k] : pu[k];
+  }
+  a.nu64 = 2;
+  return a;
+}
+
+// The integration state and the arrays a rebuild permutes, copied to the
+// saved set (save) or back from it.
+ArraySet rbx_engine::state_set(bool save) const {
+  ArraySet a{};
+  double* const pd[10] = {x, y, z, vx, vy, vz, fx, fy, fz, q};
+  int* const pi[3] = {type, gid, orig};
+  unsigned long long* const pu[2] = {key_a, key_b};
+  for (int k = 0; k < 10; ++k) {
+    a.src_f64[k] = save ? pd[k] : snapd[k];
+    a.dst_f64[k] = save ? snapd[k] : pd[k];
+  }
+  for (int k = 0; k < 3; ++k) {
+    a.src_i32[k] = save ? pi[k] : snapi[k];
+    a.dst_i32[k] = save ? snapi[k] : pi[k];
+  }
+  for (int k = 0; k < 2; ++k) {
+    a.src_u64[k] = save ? pu[k] : snapu[k];
+    a.dst_u64[k] = save ? snapu[k] : pu[k];
+  }
+  a.nf64 = 10;
+  a.ni32 = 3;
+  a.nu64 = 2;
+  return a;
+}
+
+// The device work of a rebuild on stream s: cell sort, permutation of every
+// per-atom array (addresses unchanged), fixed-point records, candidate list.
+// in_graph: also the candidate total and the device rebuild counter, with no
+// host decision (the host checks the flags after the graph has run).
+int rbx_engine::rebuild_launches(cudaStream_t s, bool in_graph) {
+  ETRY(launch_fill_i32(2, dflags, 0, s));  // cell-sort status, list overflow
   ETRY(launch_cells_sort(dbox, dims, n, x, y, z, perm, cell_of_sorted, cell_start, cell_scratch,
-                         status, st));
-  double** darr[] = {&x, &y, &z, &vx, &vy, &vz, &fx, &fy, &fz, &q, &fpx, &fpy, &fpz};
-  for (double** a : darr) {
-    ETRY(launch_gather_f64(n, perm, *a, tmpd, st));
-    std::swap(*a, tmpd);
+                         dflags, s));
+  ETRY(launch_move_set(n, perm, permute_set(true), s));
+  ETRY(launch_move_set(n, nullptr, permute_set(false), s));
+  ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, s));
+  ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
+                        cand_count, cand, dflags + 1, list_scratch, s));
+  if (in_graph) {
+    ETRY(launch_zero_u64((unsigned long long*)cand_total, s));
+    ETRY(launch_sum_i32(n, cand_count, cand_total, s));
+    ETRY(launch_add_i32(dflags + 5, 1, s));
   }
-  int** iarr[] = {&type, &gid, &orig};
-  for (int** a : iarr) {
-    ETRY(launch_gather_i32(n, perm, *a, tmpi, st));
-    std::swap(*a, tmpi);
-  }
-  unsigned long long** uarr[] = {&key_a, &key_b};
-  for (unsigned long long** a : uarr) {
-    ETRY(launch_gather_u64(n, perm, *a, tmpu, st));
-    std::swap(*a, tmpu);
-  }
-  ETRY(cuda_ok(cudaMemcpyAsync(x0, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
-  ETRY(cuda_ok(cudaMemcpyAsync(y0, y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
-  ETRY(cuda_ok(cudaMemcpyAsync(z0, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "D2D"));
-  ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
+  return RBX_OK;
+}
+
+// Rebuild: cell sort, permute every per-atom array, candidate list; the row
+// capacity grows (and the list is built again) until no row overflows.
+int rbx_engine::rebuild() {
+  ETRY(rebuild_launches(st, false));
   for (int attempt = 0; attempt < 4; ++attempt) {
-    ETRY(cuda_ok(cudaMemsetAsync(dflags + 1, 0, sizeof(int), st), "memset"));
-    ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
-                          cand_count, cand, dflags + 1, list_scratch, st));
     int h[2] = {0, 0};
     ETRY(cuda_ok(cudaMemcpyAsync(h, dflags, sizeof(int) * 2, cudaMemcpyDeviceToHost, st), "D2H"));
     ETRY(cuda_ok(cudaStreamSynchronize(st), "rebuild sync"));
@@ -311,9 +384,10 @@ int rbx_engine::rebuild() {
     if (!(h[1] & 1)) {
       have_cache = true;
       ++rebuilds;
+      ETRY(launch_zero_u64((unsigned long long*)cand_total, st));
       return launch_sum_i32(n, cand_count, cand_total, st);
     }
-    // grow the row capacity and rebuild the list
+    // grow the row capacity and build the list again
     int maxc = 0;
     {
       std::vector<int> hc(n);
@@ -325,6 +399,10 @@ int rbx_engine::rebuild() {
     cap = ((int)(maxc * 1.2) + 31) / 32 * 32;
     ETRY(alloc(&cand, (size_t)n * cap));
     nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart);
+    graph_dirty = true;  // the list moved
+    ETRY(launch_fill_i32(1, dflags + 1, 0, st));
+    ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
+                          cand_count, cand, dflags + 1, list_scratch, st));
   }
   set_error("candidate list capacity did not converge");
   return RBX_ERR_CAPACITY;
@@ -347,23 +425,23 @@ int rbx_engine::check_rebuild(bool disp_from_drift) {
   return RBX_OK;
 }
 
-int rbx_engine::real_space() {
+int rbx_engine::real_space(const int* epoch_dev) {
   const bool mixed = prm.precision == RBX_MIXED;
   if (prm.neighbor_type == RBX_NEIGHBOR_RBL)
-    return launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, cand_count,
-                            cand, cap, fpx, fpy, fpz, fpart, nrbl, dflags + 3, st);
+    return launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, epoch_dev,
+                            cand_count, cand, cap, fpx, fpy, fpz, fpart, nrbl, dflags + 3, st);
   return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, fpx, fpy,
                                  fpz, nullptr, epart, nfpart, st);
 }
 
-int rbx_engine::kspace_and_combine(bool kick) {
+int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
   const bool mixed = prm.precision == RBX_MIXED;
   const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
   if (P > 0) {
     if (!k_injected) {
       ETRY(cuda_ok(cudaMemsetAsync(dflags + 2, 0, sizeof(int), st), "memset"));
-      ETRY(launch_rbe_sample(P, sample_tables, tcnt, ttot, prm.random_seed, epoch, mx, my, mz,
-                             mixed ? mi : nullptr, dflags + 2, st));
+      ETRY(launch_rbe_sample(P, sample_tables, tcnt, ttot, prm.random_seed, epoch, epoch_dev, mx,
+                             my, mz, mixed ? mi : nullptr, dflags + 2, st));
     }
     if (mixed)
       ETRY(launch_rbe_rho_partial_mixed(n, P, mi, atoms, part_re, part_im, nparts, st));
@@ -435,6 +513,14 @@ int rbx_engine::check_sampler() {
 int rbx_engine::step(int nsteps) {
   cudaSetDevice(device);
   if (!have_forces) ETRY(compute_forces(epoch));
+  if (nsteps <= 0) return RBX_OK;
+  // profiled steps time their phases with events between launches: no graph
+  if (use_graph && !profiling && have_cache && prm.skin > 0.0) return step_graph(nsteps);
+  return step_plain(nsteps);
+}
+
+// One velocity-Verlet step after another, the host deciding each rebuild.
+int rbx_engine::step_plain(int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
     cudaEvent_t* e = nullptr;
     if (profiling) {
@@ -466,6 +552,103 @@ int rbx_engine::step(int nsteps) {
   if (profiling) ETRY(flush_profile());
   ETRY(check_sampler());
   return RBX_OK;
+}
+
+// Capture one MD step as a CUDA graph: kick, drift, the rebuild decision (a
+// one-thread kernel that advances the device epoch and sets the condition),
+// an IF node whose body is the rebuild, then the real-space force, k-space and
+// the second half kick.  Nothing in it waits for the host.
+int rbx_engine::capture_step_graph() {
+  release_graph();
+  ETRY(cuda_ok(cudaGraphCreate(&graph, 0), "cudaGraphCreate"));
+  cudaGraphConditionalHandle cond;
+  ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault),
+               "cudaGraphConditionalHandleCreate"));
+  const unsigned long long l0 = rbx_launch_count();
+  ETRY(cuda_ok(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal),
+               "cudaStreamBeginCaptureToGraph"));
+  int rc = RBX_OK;
+  auto capture = [&]() -> int {
+    const double thr = prm.skin * 0.5;
+    ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
+    ETRY(launch_zero_u64(max_d2, st));
+    ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q, st));
+    ETRY(launch_step_decide(max_d2, thr * thr, dflags + 4, cond, st));
+    // the conditional node after everything captured so far
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    ETRY(cuda_ok(cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &ndeps),
+                 "cudaStreamGetCaptureInfo"));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    ETRY(cuda_ok(cudaGraphAddNode(&node, capg, deps, ndeps, &np), "cudaGraphAddNode"));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    ETRY(cuda_ok(cudaStreamUpdateCaptureDependencies(st, &node, 1,
+                                                     cudaStreamSetCaptureDependencies),
+                 "cudaStreamUpdateCaptureDependencies"));
+    const unsigned long long b0 = rbx_launch_count();
+    ETRY(cuda_ok(cudaStreamBeginCaptureToGraph(st_body, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal),
+                 "cudaStreamBeginCaptureToGraph"));
+    const int brc = rebuild_launches(st_body, true);
+    cudaGraph_t body_out = body;
+    const cudaError_t be = cudaStreamEndCapture(st_body, &body_out);
+    ETRY(brc);
+    ETRY(cuda_ok(be, "cudaStreamEndCapture (rebuild body)"));
+    graph_rebuild_launches = rbx_launch_count() - b0;
+    ETRY(real_space(dflags + 4));
+    ETRY(kspace_and_combine(true, dflags + 4));
+    return RBX_OK;
+  };
+  rc = capture();
+  cudaGraph_t g = graph;
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (rc) {
+    release_graph();
+    return rc;
+  }
+  ETRY(cuda_ok(e, "cudaStreamEndCapture"));
+  graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
+  ETRY(cuda_ok(cudaGraphInstantiate(&graph_exec, graph, 0), "cudaGraphInstantiate"));
+  graph_dirty = false;
+  return RBX_OK;
+}
+
+// nsteps launches of the step graph with one host synchronisation at the
+// end.  The state is saved first: if a rebuild inside the graph ran out of
+// row capacity (or a cell overflowed the sort), the saved state comes back
+// and the same steps run again with the host deciding each rebuild (which
+// grows the capacity).
+int rbx_engine::step_graph(int nsteps) {
+  if (graph_dirty || !graph_exec) ETRY(capture_step_graph());
+  const ArraySet save = state_set(true), restore = state_set(false);
+  ETRY(launch_move_set(n, nullptr, save, st));
+  const int dev_init[2] = {epoch, 0};  // [4] epoch, [5] rebuilds in the graph
+  ETRY(cuda_ok(cudaMemcpyAsync(dflags + 4, dev_init, sizeof(int) * 2, cudaMemcpyHostToDevice, st),
+               "H2D"));
+  for (int k = 0; k < nsteps; ++k)
+    ETRY(cuda_ok(cudaGraphLaunch(graph_exec, st), "cudaGraphLaunch"));
+  int h[6];
+  ETRY(cuda_ok(cudaMemcpyAsync(h, dflags, sizeof(int) * 6, cudaMemcpyDeviceToHost, st), "D2H"));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "step graph sync"));
+  if (h[0] || (h[1] & 1)) {  // a rebuild inside the graph overflowed: replay on the host path
+    ETRY(launch_move_set(n, nullptr, restore, st));
+    have_cache = false;
+    return step_plain(nsteps);
+  }
+  count_launch((int)(graph_step_launches * nsteps + graph_rebuild_launches * h[5]));
+  epoch += nsteps;
+  steps += nsteps;
+  force_calls += nsteps;
+  rebuilds += h[5];
+  return check_sampler();
 }
 
 // Fold the recorded per-step phase events into the running totals.
@@ -623,6 +806,7 @@ int rbx_engine::get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs
 
 int rbx_engine::set_k_samples(int p, const double* hmx, const double* hmy, const double* hmz) {
   cudaSetDevice(device);
+  graph_dirty = true;
   if (!hmx) {
     k_injected = false;
     return RBX_OK;
@@ -755,6 +939,12 @@ void* rbx_engine_stream(rbx_engine* e) { return e ? (void*)e->st : nullptr; }
 int rbx_engine_phase_ms(rbx_engine* e, float out[4]) {
   if (!e || !out) return RBX_ERR_INVALID;
   return e->phase_ms(out);
+}
+
+int rbx_engine_set_step_graph(rbx_engine* e, int on) {
+  if (!e) return RBX_ERR_INVALID;
+  e->use_graph = on != 0;
+  return RBX_OK;
 }
 
 int rbx_engine_set_profiling(rbx_engine* e, int on) {

@@ -50,7 +50,9 @@ struct rbx_engine {
   int nfpart = 0;  // capacity of fpart / epart (blocks)
   int nrbl = 0;    // blocks of the fused RBL launch (depends on cap)
   double *fpart = nullptr, *epart = nullptr, *mean = nullptr;
-  int* dflags = nullptr;  // [0] cell sort, [1] list overflow, [2] sampler
+  // [0] cell sort, [1] list overflow, [2] sampler, [3] real-space kernel,
+  // [4] device epoch (step graphs), [5] rebuilds inside step graphs
+  int* dflags = nullptr;
   unsigned long long* max_d2 = nullptr;
   double* inv_mass = nullptr;
   double *lj_eps = nullptr, *lj_s6 = nullptr;
@@ -67,6 +69,25 @@ struct rbx_engine {
   double* sample_tables = nullptr;
   int tcnt[3] = {0, 0, 0};
   double ttot[3] = {0, 0, 0};
+
+  // arrays a rebuild permutes move through shadow copies and back, so every
+  // device array keeps its address (a captured step graph stays valid)
+  double* shd[13] = {};
+  int* shi[3] = {};
+  unsigned long long* shu[2] = {};
+  // state saved before a run of graph steps (restored if a rebuild inside
+  // the graph ran out of capacity): x y z vx vy vz fx fy fz q, type gid orig, keys
+  double* snapd[10] = {};
+  int* snapi[3] = {};
+  unsigned long long* snapu[2] = {};
+
+  // CUDA graph of one MD step, the rebuild under a conditional (IF) node
+  bool use_graph = true;
+  bool graph_dirty = true;   // addresses, capacity or modes changed: capture again
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaStream_t st_body = nullptr;  // captures the rebuild body
+  unsigned long long graph_step_launches = 0, graph_rebuild_launches = 0;
 
   // bookkeeping
   bool have_cache = false, have_forces = false, k_injected = false, keep_parts = false;
@@ -89,9 +110,16 @@ struct rbx_engine {
                 const double* vz);
   int set_k_samples(int p, const double* mx, const double* my, const double* mz);
   int rebuild();
+  int rebuild_launches(cudaStream_t s, bool in_graph);  // the device work of a rebuild
+  rbx::ArraySet permute_set(bool to_shadow) const;
+  rbx::ArraySet state_set(bool save) const;
+  int capture_step_graph();
+  int step_graph(int nsteps);
+  int step_plain(int nsteps);
+  void release_graph();
   int check_rebuild(bool disp_from_drift);
-  int real_space();
-  int kspace_and_combine(bool kick);
+  int real_space(const int* epoch_dev = nullptr);
+  int kspace_and_combine(bool kick, const int* epoch_dev = nullptr);
   int compute_forces(int epoch);
   int check_sampler();
   int step(int nsteps);

@@ -55,9 +55,10 @@ int launch_rbe_force_f64(int n, int p, const KTab* tab, const double* q, const d
                          cudaStream_t st);
 int launch_rbe_force_mixed(int n, int p, const KTab* tab, const uint4* atoms,
                            const RbeForceOut& out, cudaStream_t st);
+// step_dev (may be null): read the step from device memory (step graphs).
 int launch_rbe_sample(int p, const double* tables, const int cnt[3], const double tot[3],
-                      uint64_t seed, int64_t step, double* mx, double* my, double* mz, int* mi,
-                      int* status, cudaStream_t st);
+                      uint64_t seed, int64_t step, const int* step_dev, double* mx, double* my,
+                      double* mz, int* mi, int* status, cudaStream_t st);
 int launch_m_to_int(int p, const double* mx, const double* my, const double* mz, int* mi,
                     cudaStream_t st);
 int launch_ewald(const DBox& b, int n, const int kmax[3], double alpha, double qqr2e,
@@ -106,9 +107,9 @@ int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks);
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
                      const double* x, const double* y, const double* z, const double* q,
                      const int* type, const unsigned long long* key_a,
-                     const unsigned long long* key_b, int epoch, const int* cand_count,
-                     const int* cand, int cap, double* fx, double* fy, double* fz, double* fpart,
-                     int nblocks, int* status, cudaStream_t st);
+                     const unsigned long long* key_b, int epoch, const int* epoch_dev,
+                     const int* cand_count, const int* cand, int cap, double* fx, double* fy,
+                     double* fz, double* fpart, int nblocks, int* status, cudaStream_t st);
 // Verlet pair force over the candidate list, cut at cut_off (force predicate).
 int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, const double* x,
                             const double* y, const double* z, const double* q, const int* type,
@@ -157,6 +158,25 @@ size_t full_list_scratch_bytes(int n, int ncell);
 int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
                      const double* y, const double* z, const int* cell_start, int cap,
                      int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st);
+// A set of per-atom arrays moved together: dst[a][i] = src[a][perm[i]].
+struct ArraySet {
+  static constexpr int kMaxF64 = 16, kMaxI32 = 4, kMaxU64 = 2;
+  const double* src_f64[kMaxF64];
+  double* dst_f64[kMaxF64];
+  const int* src_i32[kMaxI32];
+  int* dst_i32[kMaxI32];
+  const unsigned long long* src_u64[kMaxU64];
+  unsigned long long* dst_u64[kMaxU64];
+  int nf64, ni32, nu64;
+};
+// perm may be null (plain copy).
+int launch_move_set(int n, const int* perm, const ArraySet& set, cudaStream_t st);
+int launch_fill_i32(int n, int* p, int v, cudaStream_t st);
+int launch_zero_u64(unsigned long long* p, cudaStream_t st);
+int launch_add_i32(int* p, int v, cudaStream_t st);
+// Step-graph decision: ++*epoch; rebuild branch iff max displacement^2 > thr2.
+int launch_step_decide(const unsigned long long* max_d2, double thr2, int* epoch,
+                       cudaGraphConditionalHandle rebuild, cudaStream_t st);
 int launch_gather_f64(int n, const int* perm, const double* src, double* dst, cudaStream_t st);
 int launch_gather_i32(int n, const int* perm, const int* src, int* dst, cudaStream_t st);
 int launch_gather_u64(int n, const int* perm, const unsigned long long* src,

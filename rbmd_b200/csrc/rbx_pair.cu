@@ -245,11 +245,13 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
             const double* __restrict__ y, const double* __restrict__ z,
             const double* __restrict__ q, const int* __restrict__ type,
             const unsigned long long* __restrict__ key_a,
-            const unsigned long long* __restrict__ key_b, int epoch,
-            const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
-            double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-            double* __restrict__ fpart, int* __restrict__ status) {
+            const unsigned long long* __restrict__ key_b, int epoch_arg,
+            const int* __restrict__ epoch_dev, const int* __restrict__ cand_count,
+            const int* __restrict__ cand, int cap, double* __restrict__ fx,
+            double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart,
+            int* __restrict__ status) {
   using T = typename std::conditional<MIXED, float, double>::type;
+  const int epoch = epoch_dev ? *epoch_dev : epoch_arg;  // device copy inside a step graph
   using Queue = typename std::conditional<MIXED, QueueMixed, QueueF64>::type;
   extern __shared__ __align__(128) int s_rows[];  // PREFETCH: [PAIR_WARPS][2][cap]
   __shared__ __align__(8) unsigned long long s_bar[PAIR_WARPS][2];
@@ -298,6 +300,11 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
     const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
     const int cnt = cand_count[i];
     const int* row = cand + (size_t)i * cap;
+    if (!PREFETCH) {  // pull the next atom's row toward L2 while this one is processed
+      const int inext = i + wstride;
+      if (inext < n && lane * 32 < cap)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(cand + (size_t)inext * cap + lane * 32));
+    }
     if (PREFETCH) {
       const int b = t & 1;
       const int inext = i + wstride;
@@ -832,8 +839,8 @@ constexpr int kRblMaxDynSmem = 160 * 1024;  // prefetch buffers used up to this 
 namespace {
 using RblKernel = void (*)(PairParams, int, const uint4*, const double*, const double*,
                            const double*, const double*, const int*, const unsigned long long*,
-                           const unsigned long long*, int, const int*, const int*, int, double*,
-                           double*, double*, double*, int*);
+                           const unsigned long long*, int, const int*, const int*, const int*, int,
+                           double*, double*, double*, double*, int*);
 
 struct RblChoice {
   RblKernel kern;
@@ -889,13 +896,14 @@ int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks) {
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
                      const double* x, const double* y, const double* z, const double* q,
                      const int* type, const unsigned long long* key_a,
-                     const unsigned long long* key_b, int epoch, const int* cand_count,
-                     const int* cand, int cap, double* fx, double* fy, double* fz, double* fpart,
-                     int nblocks, int* status, cudaStream_t st) {
+                     const unsigned long long* key_b, int epoch, const int* epoch_dev,
+                     const int* cand_count, const int* cand, int cap, double* fx, double* fy,
+                     double* fz, double* fpart, int nblocks, int* status, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
   const RblChoice c = rbl_choose(mixed, pp.freq, cap, status != nullptr);
   c.kern<<<nblocks, PAIR_BLOCK, c.smem, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
-                                              cand_count, cand, cap, fx, fy, fz, fpart, status);
+                                              epoch_dev, cand_count, cand, cap, fx, fy, fz, fpart,
+                                              status);
   count_launch();
   return check_launch(mixed ? "rbl_fused_mixed" : "rbl_fused_f64");
 }

@@ -535,9 +535,9 @@ constexpr int SAMPLE_BLOCK = 128;
 
 __global__ void __launch_bounds__(SAMPLE_BLOCK)
 k_rbe_sample(int p, const double* __restrict__ tables, int c0, int c1, int c2, double t0,
-             double t1, double t2, uint32_t key0, uint32_t key1, uint64_t step,
-             double* __restrict__ mx, double* __restrict__ my, double* __restrict__ mz,
-             int* __restrict__ mi, int* __restrict__ status) {
+             double t1, double t2, uint32_t key0, uint32_t key1, uint64_t step_arg,
+             const int* __restrict__ step_dev, double* __restrict__ mx, double* __restrict__ my,
+             double* __restrict__ mz, int* __restrict__ mi, int* __restrict__ status) {
   // the three cumulative tables are staged in shared memory when they fit
   // (dynamic size (c0 + c1 + c2) doubles), so the binary searches run there
   extern __shared__ double s_tab[];
@@ -549,6 +549,8 @@ k_rbe_sample(int p, const double* __restrict__ tables, int c0, int c1, int c2, d
   }
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= p) return;
+  // the MD step: a device copy inside a step graph
+  const uint64_t step = step_dev ? (uint64_t)(int64_t)*step_dev : step_arg;
   const double* w0 = staged ? s_tab : tables;
   const double* w1 = w0 + c0;
   const double* w2 = w0 + c0 + c1;
@@ -771,14 +773,14 @@ int launch_rbe_force_mixed(int n, int p, const KTab* tab, const uint4* atoms,
 }
 
 int launch_rbe_sample(int p, const double* tables, const int cnt[3], const double tot[3],
-                      uint64_t seed, int64_t step, double* mx, double* my, double* mz, int* mi,
-                      int* status, cudaStream_t st) {
+                      uint64_t seed, int64_t step, const int* step_dev, double* mx, double* my,
+                      double* mz, int* mi, int* status, cudaStream_t st) {
   if (p <= 0) return RBX_OK;
   const int entries = cnt[0] + cnt[1] + cnt[2];
   const size_t smem = entries <= kSampleSmemTables ? sizeof(double) * entries : 0;
   k_rbe_sample<<<(p + SAMPLE_BLOCK - 1) / SAMPLE_BLOCK, SAMPLE_BLOCK, smem, st>>>(
       p, tables, cnt[0], cnt[1], cnt[2], tot[0], tot[1], tot[2], (uint32_t)seed,
-      (uint32_t)(seed >> 32), (uint64_t)step, mx, my, mz, mi, status);
+      (uint32_t)(seed >> 32), (uint64_t)step, step_dev, mx, my, mz, mi, status);
   count_launch();
   return check_launch("rbe_sample");
 }

@@ -90,7 +90,7 @@ EXPORTS = [
     "rbx_engine_compute_forces", "rbx_engine_step", "rbx_engine_step_host",
     "rbx_engine_get_state", "rbx_engine_get_force_parts", "rbx_engine_get_rbl_pairs",
     "rbx_engine_get_stats", "rbx_engine_stream", "rbx_engine_phase_ms",
-    "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc",
+    "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc", "rbx_engine_set_step_graph",
 ]
 
 
@@ -144,6 +144,7 @@ def lib():
     L.rbx_engine_stream.argtypes = [vp]
     L.rbx_engine_phase_ms.argtypes = [vp, C.POINTER(C.c_float)]
     L.rbx_engine_set_profiling.argtypes = [vp, ip]
+    L.rbx_engine_set_step_graph.argtypes = [vp, ip]
     _lib = L
     return L
 
@@ -395,6 +396,9 @@ class Engine:
     @property
     def stream(self) -> int:
         return int(lib().rbx_engine_stream(self._h) or 0)
+
+    def set_step_graph(self, on=True):
+        check(lib().rbx_engine_set_step_graph(self._h, int(on)), "set_step_graph")
 
     def set_profiling(self, on=True):
         check(lib().rbx_engine_set_profiling(self._h, int(on)), "set_profiling")
