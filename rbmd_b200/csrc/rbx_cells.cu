@@ -123,8 +123,13 @@ k_cell_segsort(int ncell, int n, const int* __restrict__ start, const unsigned* 
   __shared__ unsigned s[SEG_MAX];
   const int c = blockIdx.x;
   const int a = start[c], cnt = start[c + 1] - a;
-  if (cnt > SEG_MAX) {
+  const unsigned mask = n < (1 << SUB_SHIFT) ? (1u << SUB_SHIFT) - 1u : 0xffffffffu;
+  if (cnt > SEG_MAX) {  // reported; the cell keeps a valid, unsorted permutation
     if (threadIdx.x == 0) atomicOr(status, 2);
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      perm[a + t] = (int)(tmp[a + t] & mask);
+      cell_of_sorted[a + t] = c;
+    }
     return;
   }
   int p2 = 1;
@@ -147,7 +152,6 @@ k_cell_segsort(int ncell, int n, const int* __restrict__ start, const unsigned* 
       __syncthreads();
     }
   }
-  const unsigned mask = n < (1 << SUB_SHIFT) ? (1u << SUB_SHIFT) - 1u : 0xffffffffu;
   for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
     perm[a + t] = (int)(s[t] & mask);
     cell_of_sorted[a + t] = c;

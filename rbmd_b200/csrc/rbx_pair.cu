@@ -286,9 +286,9 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
     }
     __syncwarp();
     if (i0 < n) {
-      const int c0 = cand_count[i0];
+      const int c0 = min(cand_count[i0], cap);
       if (lane == 0) bulk_row_copy(rowbuf, cand + (size_t)i0 * cap, row_bytes(c0, cap), &s_bar[warp][0]);
-      if (i0 + wstride < n) cnt_next = cand_count[i0 + wstride];
+      if (i0 + wstride < n) cnt_next = min(cand_count[i0 + wstride], cap);
     }
   }
   int t = 0;
@@ -298,7 +298,9 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
     const T qi = MIXED ? (T)__uint_as_float(ai.w) : (T)q[i];
     const int ti = type[i];
     const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
-    const int cnt = cand_count[i];
+    // a row never holds more than cap entries; a larger count marks an
+    // overflowed list (a rebuild inside a step graph), which the host replays
+    const int cnt = min(cand_count[i], cap);
     const int* row = cand + (size_t)i * cap;
     if (!PREFETCH) {  // pull the next atom's row toward L2 while this one is processed
       const int inext = i + wstride;
@@ -312,7 +314,7 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
         if (lane == 0)
           bulk_row_copy(rowbuf + (size_t)(b ^ 1) * cap, cand + (size_t)inext * cap,
                         row_bytes(cnt_next, cap), &s_bar[warp][b ^ 1]);
-        cnt_next = inext + wstride < n ? cand_count[inext + wstride] : 0;
+        cnt_next = inext + wstride < n ? min(cand_count[inext + wstride], cap) : 0;
       }
       if (!mbar_wait_bounded(&s_bar[warp][b], (unsigned)((t >> 1) & 1))) {
         if (lane == 0) atomicOr(status, 4);  // a row copy never completed
@@ -470,7 +472,7 @@ k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
     const uint4 ai = atoms[i];
     const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
     const int ti = type[i];
-    const int cnt = cand_count[i];
+    const int cnt = min(cand_count[i], cap);
     const int* row = cand + (size_t)i * cap;
     int qn = 0;
     double fxa = 0, fya = 0, fza = 0;
@@ -605,7 +607,8 @@ __global__ void k_rbl_lists(PairParams pp, int n, const uint4* __restrict__ atom
   if (i >= n) return;
   const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
   int nc = 0, ns = 0;
-  for (int t = 0; t < cand_count[i]; ++t) {
+  const int cnt = min(cand_count[i], cap);
+  for (int t = 0; t < cnt; ++t) {
     const int j = cand[(size_t)i * cap + t];
     if (j == i) continue;
     const double d2 = exact_d2(pp, x, y, z, i, j);

@@ -376,6 +376,36 @@ def test_step_graph_matches_individual_launches(cuda, rbx, prec):
     assert sa.rebuilds == sb.rebuilds and sa.rebuilds >= 2
 
 
+def test_step_graph_recovers_from_list_overflow(cuda, rbx):
+    """A rebuild inside the step graph that overflows the candidate rows
+    (here: the host hands in a configuration compressed to 0.7 of the box,
+    three times denser) is detected after the graph has run; the saved state
+    comes back and the step is replayed launch by launch, growing the rows.
+    The result equals the engine that never used the graph."""
+    s = systems.lj_electrolyte(4000, seed=5)
+    lo, hi = np.asarray(s["lo"]), np.asarray(s["hi"])
+    c = 0.5 * (lo + hi)
+    x = np.ascontiguousarray(s["pos"].T)
+    v = np.ascontiguousarray(s["vel"].T)
+    xc = np.ascontiguousarray((c + 0.7 * (s["pos"] - c)).T)
+    out = []
+    for graph in (True, False):
+        e = rbx.Engine(s, precision=rbx.PLAIN_FP64, seed=3)
+        e.set_step_graph(graph)
+        e.compute_forces(0)
+        cap0 = e.stats().candidate_capacity
+        xo, vo, fo = np.zeros((3, s["n"])), np.zeros((3, s["n"])), np.zeros((3, s["n"]))
+        e.step_host(x, v, xo, vo, fo)
+        e.step_host(xc, v, xo, vo, fo)
+        st = e.stats()
+        assert st.candidate_capacity > cap0  # the rows grew
+        out.append((xo.copy(), vo.copy(), fo.copy()))
+        e.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+    assert np.isfinite(out[0][2]).all()
+
+
 def test_engine_step_host_roundtrip(cuda, rbx, sys4k):
     s = sys4k
     e1 = rbx.Engine(s, precision=rbx.MIXED, seed=1)
