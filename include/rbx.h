@@ -162,6 +162,18 @@ int rbx_cells_sort(const rbx_box* box, double neighbor_cutoff, int n,
                    int* perm, int* cell_of_sorted, int* cell_start,
                    void* scratch, void* stream);
 
+/* Skin test of a cached list: *reuse = 1 when every atom moved at most
+ * skin / 2 (minimum image) since the positions cached at the last build,
+ * else 0; *max_disp_sq (may be null) receives the largest squared
+ * displacement.  The displacement test of
+ * BaseNeighborListBuilder::ShouldReuseNeighborList
+ * (base_neighbor_list_builder.cpp:219-319); the cache-validity bookkeeping
+ * (atom count, order, box) stays with the caller.  Synchronises the stream. */
+int rbx_nlist_should_reuse(const rbx_box* box, int n, const double* px, const double* py,
+                           const double* pz, const double* cached_px, const double* cached_py,
+                           const double* cached_pz, double skin, int* reuse,
+                           double* max_disp_sq, void* stream);
+
 /* Full (i->j and j->i) list of sorted atoms within neighbor_cutoff, j != i,
  * row-major with a fixed row capacity: nbrs[i*cap + t], count[i] = true count.
  * *overflow (device int) is set to 1 when some count exceeds cap.  Replaces

@@ -4,6 +4,7 @@
 #include <stdio.h>
 
 #include <atomic>
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -406,6 +407,35 @@ int rbx_cells_sort(const rbx_box* box, double neighbor_cutoff, int n, const doub
     return RBX_ERR_CAPACITY;
   }
   return rc;
+}
+
+int rbx_nlist_should_reuse(const rbx_box* box, int n, const double* px, const double* py,
+                           const double* pz, const double* cached_px, const double* cached_py,
+                           const double* cached_pz, double skin, int* reuse,
+                           double* max_disp_sq, void* stream) {
+  if (!box || n < 0 || !reuse || !(skin >= 0.0)) {
+    set_error("rbx_nlist_should_reuse: invalid box/n/skin/reuse");
+    return RBX_ERR_INVALID;
+  }
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long* d = nullptr;
+  RBX_TRY(async_alloc(&d, 1, st));
+  cudaMemsetAsync(d, 0, sizeof(unsigned long long), st);
+  int rc = launch_max_disp(make_dbox(*box), n, px, py, pz, cached_px, cached_py, cached_pz, d, st);
+  unsigned long long bits = 0;
+  if (!rc) {
+    cudaMemcpyAsync(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = check_launch("should_reuse sync");
+  }
+  cudaFreeAsync(d, st);
+  if (rc) return rc;
+  double d2;
+  memcpy(&d2, &bits, sizeof(d2));
+  const double thr = 0.5 * skin;
+  *reuse = d2 <= thr * thr ? 1 : 0;
+  if (max_disp_sq) *max_disp_sq = d2;
+  return RBX_OK;
 }
 
 int rbx_full_list(const rbx_box* box, double neighbor_cutoff, int n, const double* px,

@@ -91,6 +91,7 @@ EXPORTS = [
     "rbx_engine_get_state", "rbx_engine_get_force_parts", "rbx_engine_get_rbl_pairs",
     "rbx_engine_get_stats", "rbx_engine_stream", "rbx_engine_phase_ms",
     "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc", "rbx_engine_set_step_graph",
+    "rbx_nlist_should_reuse",
 ]
 
 
@@ -145,6 +146,8 @@ def lib():
     L.rbx_engine_phase_ms.argtypes = [vp, C.POINTER(C.c_float)]
     L.rbx_engine_set_profiling.argtypes = [vp, ip]
     L.rbx_engine_set_step_graph.argtypes = [vp, ip]
+    L.rbx_nlist_should_reuse.argtypes = [B, ip] + [vp] * 6 + [dp, C.POINTER(C.c_int),
+                                                             C.POINTER(C.c_double), vp]
     _lib = L
     return L
 
@@ -253,6 +256,15 @@ def cells_sort(box, cutoff, x, y, z, perm, cell_of_sorted, cell_start, scratch, 
 
 def cells_scratch_bytes(n, ncell) -> int:
     return int(lib().rbx_cells_scratch_bytes(n, ncell))
+
+
+def nlist_should_reuse(box, x, y, z, x0, y0, z0, skin, stream=None):
+    """(reuse, max squared displacement) of a list cached at x0, y0, z0."""
+    reuse, d2 = C.c_int(0), C.c_double(0.0)
+    check(lib().rbx_nlist_should_reuse(C.byref(box), x.numel(), _ptr(x), _ptr(y), _ptr(z),
+                                       _ptr(x0), _ptr(y0), _ptr(z0), skin, C.byref(reuse),
+                                       C.byref(d2), _stream(stream)), "rbx_nlist_should_reuse")
+    return bool(reuse.value), d2.value
 
 
 def full_list(box, cutoff, x, y, z, cell_start, cap, count, nbrs, overflow, stream=None):

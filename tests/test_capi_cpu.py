@@ -50,6 +50,10 @@ def test_compute_without_gpu_fails(rbx):
     rc = rbx.lib().rbx_rbe_sample(C.byref(b), 0.16, 4, 1, 0, None, None, None, None)
     assert rc == 5  # RBX_ERR_DEVICE: no CPU fallback
     assert "no CPU fallback" in rbx.last_error() or "device" in rbx.last_error()
+    reuse, d2 = C.c_int(7), C.c_double(0.0)
+    rc = rbx.lib().rbx_nlist_should_reuse(C.byref(b), 10, *([None] * 6), 0.3, C.byref(reuse),
+                                          C.byref(d2), None)
+    assert rc == 5 and reuse.value == 7
 
 
 JSON_OK = """{

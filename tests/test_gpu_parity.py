@@ -161,6 +161,30 @@ def test_cells_and_full_list(cuda, rbx, oracle, n):
         assert set(gn[i, :gc[i]].tolist()) == set(orows[i, :ocnt[i]].tolist())
 
 
+def test_nlist_should_reuse_matches_oracle(cuda, rbx, oracle, sys4k):
+    """Skin test of a cached list (ShouldReuseNeighborList): the largest
+    minimum-image displacement, and reuse iff it is at most skin / 2."""
+    import torch
+
+    s = sys4k
+    box = oracle.Box.make(s["lo"], s["hi"])
+    rbox = rbx.Box.make(s["lo"], s["hi"])
+    L = np.asarray(s["hi"]) - np.asarray(s["lo"])
+    rng = np.random.default_rng(3)
+    p0 = s["pos"]
+    for scale, wrap in ((0.05, False), (0.2, True)):
+        p1 = p0 + rng.uniform(-scale, scale, p0.shape)
+        if wrap:  # moved across the periodic boundary: the minimum image applies
+            p1 = np.asarray(s["lo"]) + np.mod(p1 - np.asarray(s["lo"]), L)
+        cols = [np.ascontiguousarray(a[:, d]) for a in (p1, p0) for d in range(3)]
+        want = oracle.max_disp2(box, *cols)
+        dev = [torch.tensor(c, device="cuda") for c in cols]
+        for skin in (0.3, 2.0 * np.sqrt(want) * 0.999):
+            reuse, d2 = rbx.nlist_should_reuse(rbox, *dev, skin)
+            assert abs(d2 - want) <= 1e-12 * want
+            assert reuse == (want <= (0.5 * skin) ** 2)  # thresholds far from the rounding
+
+
 def test_full_list_overflow_flag(cuda, rbx, sys4k):
     s = sys4k
     n = s["n"]
