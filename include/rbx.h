@@ -349,6 +349,21 @@ int rbx_engine_set_profiling(rbx_engine* e, int on);
  * NVEensemble::Solve launches and synchronises step by step). */
 int rbx_engine_set_step_graph(rbx_engine* e, int on);
 
+/* ---- Batches of replicas ------------------------------------------------
+ * Independent engines on one device advanced together: each rbx_batch_step
+ * MD step is one CUDA graph launch in which every replica's step is a
+ * parallel branch (kick, drift, its own rebuild decision and conditional
+ * rebuild, forces, second kick).  The engines stay owned by the caller and
+ * must outlive the batch; each must have skin > 0 and profiling off.  Results
+ * equal stepping each engine alone.  No counterpart in the reference (one
+ * system per process). */
+typedef struct rbx_batch rbx_batch;
+rbx_batch* rbx_batch_create(rbx_engine* const* engines, int count);
+void rbx_batch_destroy(rbx_batch* b);
+int rbx_batch_step(rbx_batch* b, int nsteps);
+/* The stream the batch graph runs on (cudaStream_t). */
+void* rbx_batch_stream(rbx_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -216,7 +216,9 @@ int rbx_engine::init() {
   const double expect = (double)n / V * 4.0 / 3.0 * M_PI * rcs * rcs * rcs;
   cap = ((int)(1.3 * expect + 64) + 31) / 32 * 32;
   ETRY(alloc(&cand, N * (size_t)cap));
-  ETRY(cuda_ok(cudaHostAlloc((void**)&h_pinned, 64, cudaHostAllocDefault), "cudaHostAlloc"));
+  ETRY(cuda_ok(cudaHostAlloc((void**)&h_pinned, 128, cudaHostAllocDefault), "cudaHostAlloc"));
+  run_init = (int*)(h_pinned + 2);   // 2 ints
+  run_flags = (int*)(h_pinned + 4);  // 6 ints
   for (int i = 0; i < 8; ++i) ETRY(cuda_ok(cudaEventCreate(&ev[i]), "cudaEventCreate"));
   pp.box = dbox;
   pp.rs2 = prm.r_core * prm.r_core;
@@ -287,6 +289,7 @@ int rbx_engine::set_state(const int* hgid, const int* htype, const double* hq, c
   have_forces = false;
   epoch = 0;
   graph_dirty = true;
+  ++graph_version;
   return RBX_OK;
 }
 
@@ -400,6 +403,7 @@ int rbx_engine::rebuild() {
     ETRY(alloc(&cand, (size_t)n * cap));
     nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart);
     graph_dirty = true;  // the list moved
+    ++graph_version;
     ETRY(launch_fill_i32(1, dflags + 1, 0, st));
     ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
                           cand_count, cand, dflags + 1, list_scratch, st));
@@ -561,53 +565,10 @@ int rbx_engine::step_plain(int nsteps) {
 int rbx_engine::capture_step_graph() {
   release_graph();
   ETRY(cuda_ok(cudaGraphCreate(&graph, 0), "cudaGraphCreate"));
-  cudaGraphConditionalHandle cond;
-  ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault),
-               "cudaGraphConditionalHandleCreate"));
-  const unsigned long long l0 = rbx_launch_count();
   ETRY(cuda_ok(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0,
                                              cudaStreamCaptureModeThreadLocal),
                "cudaStreamBeginCaptureToGraph"));
-  int rc = RBX_OK;
-  auto capture = [&]() -> int {
-    const double thr = prm.skin * 0.5;
-    ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
-    ETRY(launch_zero_u64(max_d2, st));
-    ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q, st));
-    ETRY(launch_step_decide(max_d2, thr * thr, dflags + 4, cond, st));
-    // the conditional node after everything captured so far
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t capg = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    ETRY(cuda_ok(cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &ndeps),
-                 "cudaStreamGetCaptureInfo"));
-    cudaGraphNodeParams np{};
-    np.type = cudaGraphNodeTypeConditional;
-    np.conditional.handle = cond;
-    np.conditional.type = cudaGraphCondTypeIf;
-    np.conditional.size = 1;
-    cudaGraphNode_t node;
-    ETRY(cuda_ok(cudaGraphAddNode(&node, capg, deps, ndeps, &np), "cudaGraphAddNode"));
-    cudaGraph_t body = np.conditional.phGraph_out[0];
-    ETRY(cuda_ok(cudaStreamUpdateCaptureDependencies(st, &node, 1,
-                                                     cudaStreamSetCaptureDependencies),
-                 "cudaStreamUpdateCaptureDependencies"));
-    const unsigned long long b0 = rbx_launch_count();
-    ETRY(cuda_ok(cudaStreamBeginCaptureToGraph(st_body, body, nullptr, nullptr, 0,
-                                               cudaStreamCaptureModeThreadLocal),
-                 "cudaStreamBeginCaptureToGraph"));
-    const int brc = rebuild_launches(st_body, true);
-    cudaGraph_t body_out = body;
-    const cudaError_t be = cudaStreamEndCapture(st_body, &body_out);
-    ETRY(brc);
-    ETRY(cuda_ok(be, "cudaStreamEndCapture (rebuild body)"));
-    graph_rebuild_launches = rbx_launch_count() - b0;
-    ETRY(real_space(dflags + 4));
-    ETRY(kspace_and_combine(true, dflags + 4));
-    return RBX_OK;
-  };
-  rc = capture();
+  const int rc = capture_step_into(graph);
   cudaGraph_t g = graph;
   const cudaError_t e = cudaStreamEndCapture(st, &g);
   if (rc) {
@@ -615,31 +576,74 @@ int rbx_engine::capture_step_graph() {
     return rc;
   }
   ETRY(cuda_ok(e, "cudaStreamEndCapture"));
-  graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
   ETRY(cuda_ok(cudaGraphInstantiate(&graph_exec, graph, 0), "cudaGraphInstantiate"));
   graph_dirty = false;
   return RBX_OK;
 }
 
-// nsteps launches of the step graph with one host synchronisation at the
-// end.  The state is saved first: if a rebuild inside the graph ran out of
-// row capacity (or a cell overflowed the sort), the saved state comes back
-// and the same steps run again with the host deciding each rebuild (which
-// grows the capacity).
-int rbx_engine::step_graph(int nsteps) {
-  if (graph_dirty || !graph_exec) ETRY(capture_step_graph());
-  const ArraySet save = state_set(true), restore = state_set(false);
-  ETRY(launch_move_set(n, nullptr, save, st));
-  const int dev_init[2] = {epoch, 0};  // [4] epoch, [5] rebuilds in the graph
-  ETRY(cuda_ok(cudaMemcpyAsync(dflags + 4, dev_init, sizeof(int) * 2, cudaMemcpyHostToDevice, st),
-               "H2D"));
-  for (int k = 0; k < nsteps; ++k)
-    ETRY(cuda_ok(cudaGraphLaunch(graph_exec, st), "cudaGraphLaunch"));
-  int h[6];
-  ETRY(cuda_ok(cudaMemcpyAsync(h, dflags, sizeof(int) * 6, cudaMemcpyDeviceToHost, st), "D2H"));
-  ETRY(cuda_ok(cudaStreamSynchronize(st), "step graph sync"));
-  if (h[0] || (h[1] & 1)) {  // a rebuild inside the graph overflowed: replay on the host path
-    ETRY(launch_move_set(n, nullptr, restore, st));
+// Record one MD step on st, which must be capturing into g (its own graph or
+// a batch graph): the conditional handle is created on g, the IF node goes
+// after what st has captured so far, its body is captured on st_body.
+int rbx_engine::capture_step_into(cudaGraph_t g) {
+  cudaGraphConditionalHandle cond;
+  ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault),
+               "cudaGraphConditionalHandleCreate"));
+  const unsigned long long l0 = rbx_launch_count();
+  const double thr = prm.skin * 0.5;
+  ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
+  ETRY(launch_zero_u64(max_d2, st));
+  ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q, st));
+  ETRY(launch_step_decide(max_d2, thr * thr, dflags + 4, cond, st));
+  // the conditional node after everything captured so far on st
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t capg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  ETRY(cuda_ok(cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &ndeps),
+               "cudaStreamGetCaptureInfo"));
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = cond;
+  np.conditional.type = cudaGraphCondTypeIf;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  ETRY(cuda_ok(cudaGraphAddNode(&node, capg, deps, ndeps, &np), "cudaGraphAddNode"));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  ETRY(cuda_ok(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
+               "cudaStreamUpdateCaptureDependencies"));
+  const unsigned long long b0 = rbx_launch_count();
+  ETRY(cuda_ok(cudaStreamBeginCaptureToGraph(st_body, body, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal),
+               "cudaStreamBeginCaptureToGraph"));
+  const int brc = rebuild_launches(st_body, true);
+  cudaGraph_t body_out = body;
+  const cudaError_t be = cudaStreamEndCapture(st_body, &body_out);
+  ETRY(brc);
+  ETRY(cuda_ok(be, "cudaStreamEndCapture (rebuild body)"));
+  graph_rebuild_launches = rbx_launch_count() - b0;
+  ETRY(real_space(dflags + 4));
+  ETRY(kspace_and_combine(true, dflags + 4));
+  graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
+  return RBX_OK;
+}
+
+// Before a run of graph steps: save the state, seed the device epoch and the
+// in-graph rebuild counter (all on stream s).
+int rbx_engine::graph_run_begin(cudaStream_t s) {
+  ETRY(launch_move_set(n, nullptr, state_set(true), s));
+  run_init[0] = epoch;  // [4] epoch, [5] rebuilds inside the graph
+  run_init[1] = 0;
+  return cuda_ok(cudaMemcpyAsync(dflags + 4, run_init, sizeof(int) * 2, cudaMemcpyHostToDevice, s),
+                 "H2D");
+}
+
+// After the graph steps (flags copied to run_flags and the stream synchronised):
+// account for the steps, or restore the saved state and replay them launch by
+// launch when a rebuild inside the graph overflowed.
+int rbx_engine::graph_run_end(int nsteps) {
+  const int* h = run_flags;
+  if (h[0] || (h[1] & 1)) {
+    ETRY(launch_move_set(n, nullptr, state_set(false), st));
     have_cache = false;
     return step_plain(nsteps);
   }
@@ -649,6 +653,22 @@ int rbx_engine::step_graph(int nsteps) {
   force_calls += nsteps;
   rebuilds += h[5];
   return check_sampler();
+}
+
+// nsteps launches of the step graph with one host synchronisation at the
+// end.  The state is saved first: if a rebuild inside the graph ran out of
+// row capacity (or a cell overflowed the sort), the saved state comes back
+// and the same steps run again with the host deciding each rebuild (which
+// grows the capacity).
+int rbx_engine::step_graph(int nsteps) {
+  if (graph_dirty || !graph_exec) ETRY(capture_step_graph());
+  ETRY(graph_run_begin(st));
+  for (int k = 0; k < nsteps; ++k)
+    ETRY(cuda_ok(cudaGraphLaunch(graph_exec, st), "cudaGraphLaunch"));
+  ETRY(cuda_ok(cudaMemcpyAsync(run_flags, dflags, sizeof(int) * 6, cudaMemcpyDeviceToHost, st),
+               "D2H"));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "step graph sync"));
+  return graph_run_end(nsteps);
 }
 
 // Fold the recorded per-step phase events into the running totals.
@@ -807,6 +827,7 @@ int rbx_engine::get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs
 int rbx_engine::set_k_samples(int p, const double* hmx, const double* hmy, const double* hmz) {
   cudaSetDevice(device);
   graph_dirty = true;
+  ++graph_version;
   if (!hmx) {
     k_injected = false;
     return RBX_OK;

@@ -84,10 +84,13 @@ struct rbx_engine {
   // CUDA graph of one MD step, the rebuild under a conditional (IF) node
   bool use_graph = true;
   bool graph_dirty = true;   // addresses, capacity or modes changed: capture again
+  unsigned graph_version = 0;  // bumped on each such change (batch graphs compare it)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t st_body = nullptr;  // captures the rebuild body
   unsigned long long graph_step_launches = 0, graph_rebuild_launches = 0;
+  int* run_init = nullptr;   // pinned: device epoch / counter seeds of a graph run
+  int* run_flags = nullptr;  // pinned: dflags[0..5] after a graph run
 
   // bookkeeping
   bool have_cache = false, have_forces = false, k_injected = false, keep_parts = false;
@@ -114,6 +117,9 @@ struct rbx_engine {
   rbx::ArraySet permute_set(bool to_shadow) const;
   rbx::ArraySet state_set(bool save) const;
   int capture_step_graph();
+  int capture_step_into(cudaGraph_t g);
+  int graph_run_begin(cudaStream_t s);
+  int graph_run_end(int nsteps);
   int step_graph(int nsteps);
   int step_plain(int nsteps);
   void release_graph();

@@ -91,7 +91,8 @@ EXPORTS = [
     "rbx_engine_get_state", "rbx_engine_get_force_parts", "rbx_engine_get_rbl_pairs",
     "rbx_engine_get_stats", "rbx_engine_stream", "rbx_engine_phase_ms",
     "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc", "rbx_engine_set_step_graph",
-    "rbx_nlist_should_reuse",
+    "rbx_nlist_should_reuse", "rbx_batch_create", "rbx_batch_destroy", "rbx_batch_step",
+    "rbx_batch_stream",
 ]
 
 
@@ -146,6 +147,12 @@ def lib():
     L.rbx_engine_phase_ms.argtypes = [vp, C.POINTER(C.c_float)]
     L.rbx_engine_set_profiling.argtypes = [vp, ip]
     L.rbx_engine_set_step_graph.argtypes = [vp, ip]
+    L.rbx_batch_create.restype = vp
+    L.rbx_batch_create.argtypes = [C.POINTER(vp), ip]
+    L.rbx_batch_destroy.argtypes = [vp]
+    L.rbx_batch_step.argtypes = [vp, ip]
+    L.rbx_batch_stream.restype = vp
+    L.rbx_batch_stream.argtypes = [vp]
     L.rbx_nlist_should_reuse.argtypes = [B, ip] + [vp] * 6 + [dp, C.POINTER(C.c_int),
                                                              C.POINTER(C.c_double), vp]
     _lib = L
@@ -423,6 +430,36 @@ class Engine:
     def close(self):
         if getattr(self, "_h", None):
             lib().rbx_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Replicas advanced by one CUDA graph launch per MD step (rbx_batch_*).
+    Keeps references to its engines, which must stay open."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e._h.value for e in self.engines])
+        self._h = lib().rbx_batch_create(arr, len(self.engines))
+        if not self._h:
+            raise RbxError(f"rbx_batch_create failed: {last_error()}")
+
+    def step(self, nsteps=1):
+        check(lib().rbx_batch_step(self._h, nsteps), "rbx_batch_step")
+
+    @property
+    def stream(self) -> int:
+        return lib().rbx_batch_stream(self._h) or 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rbx_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

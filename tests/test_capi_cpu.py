@@ -41,6 +41,11 @@ def test_host_helpers(rbx, oracle):
         rbx.cell_grid(rbx.Box.make([0, 0, 0], [10.0] * 3), 5.3)  # fewer than 3 cells
 
 
+def test_batch_create_rejects_empty(rbx):
+    assert not rbx.lib().rbx_batch_create(None, 0)
+    assert "no engines" in rbx.last_error()
+
+
 def test_compute_without_gpu_fails(rbx):
     import torch
 

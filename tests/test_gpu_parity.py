@@ -430,6 +430,32 @@ def test_step_graph_recovers_from_list_overflow(cuda, rbx):
     assert np.isfinite(out[0][2]).all()
 
 
+def test_batch_matches_single_engines(cuda, rbx):
+    """Replicas of different sizes and forms advanced by one graph launch per
+    step (rbx_batch) end bit-identical to the same engines stepped alone."""
+    specs = [(4000, 11, rbx.MIXED), (5200, 12, rbx.PLAIN_FP64), (6500, 13, rbx.MIXED)]
+    systems_ = [systems.lj_electrolyte(n, seed=sd) for n, sd, _ in specs]
+    batched = [rbx.Engine(s, precision=p, seed=21) for s, (_, _, p) in zip(systems_, specs)]
+    single = [rbx.Engine(s, precision=p, seed=21) for s, (_, _, p) in zip(systems_, specs)]
+    for e in batched + single:
+        e.compute_forces(0)
+    b = rbx.Batch(batched)
+    b.step(12)
+    b.step(18)
+    for e in single:
+        e.step(12)
+        e.step(18)
+    for e1, e2 in zip(batched, single):
+        a, c = e1.get_state(), e2.get_state()
+        for key in ("pos", "vel", "force"):
+            assert np.array_equal(a[key], c[key]), key
+        s1, s2 = e1.stats(), e2.stats()
+        assert s1.steps == s2.steps == 30 and s1.rebuilds == s2.rebuilds
+    b.close()
+    for e in batched + single:
+        e.close()
+
+
 def test_engine_step_host_roundtrip(cuda, rbx, sys4k):
     s = sys4k
     e1 = rbx.Engine(s, precision=rbx.MIXED, seed=1)
