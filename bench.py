@@ -358,6 +358,91 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    """Batched replicas (the cfg-4 recipe): R independent LJ electrolytes with
+    log-uniform atom counts, mixed form, all advanced by one CUDA graph launch
+    per step (rbx_batch), against the same replicas stepped one engine at a
+    time: plain FP64 launch by launch (the one-replica-per-launch baseline)
+    and mixed with each engine's own step graph."""
+    import torch
+
+    from rbmd_b200 import rbx, systems
+
+    rng = np.random.default_rng(args.batch_seed)
+    sizes = np.exp(rng.uniform(np.log(args.batch_nmin), np.log(args.batch_nmax),
+                               args.replicas)).astype(int)
+    syss = [systems.lj_electrolyte(int(n), seed=1000 + r, kspace_p=args.p)
+            for r, n in enumerate(sizes)]
+    total = int(sizes.sum())
+
+    def make(precision, graph):
+        es = []
+        for r, s in enumerate(syss):
+            e = rbx.Engine(s, precision=precision, seed=77 + r)
+            e.set_step_graph(graph)
+            e.compute_forces(0)
+            es.append(e)
+        return es
+
+    def close(es):
+        for e in es:
+            e.close()
+
+    # batched, mixed: device time on the batch stream
+    es = make(rbx.MIXED, True)
+    b = rbx.Batch(es)
+    b.step(args.warmup)
+    st = torch.cuda.ExternalStream(b.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(st)
+    b.step(args.steps)
+    ev1.record(st)
+    torch.cuda.synchronize()
+    ms_batch = ev0.elapsed_time(ev1)
+    b.close()
+    close(es)
+
+    def one_at_a_time(precision, graph, steps):
+        es = make(precision, graph)
+        for e in es:
+            e.step(max(1, args.warmup // 2))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for e in es:
+                e.step(1)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        close(es)
+        return dt
+
+    base_steps = max(1, args.steps // 4)
+    t64 = one_at_a_time(rbx.PLAIN_FP64, False, base_steps)
+    tmix = one_at_a_time(rbx.MIXED, True, base_steps)
+    value = total * args.steps / (ms_batch / 1e3)
+    line = {
+        "metric": "batched replicas: aggregate atom-steps/s, mixed, one graph launch per step",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_batch / args.steps, "higher_is_better": True, "scaling": "weak",
+        "dtype": "mixed(u32 fixed-point, f32 SFU, f64 reductions/integrator)",
+        "data": "synthetic",
+        "config": {"workload": f"{args.replicas} LJ electrolytes rho*=0.8 10% ions, N log-uniform "
+                               f"[{args.batch_nmin}, {args.batch_nmax}] (seed {args.batch_seed}), "
+                               f"RBL + RBE(P={args.p}), NVE dt=0.005",
+                   "total_atoms": total, "replicas": args.replicas},
+        "one_replica_per_launch_fp64": {"value": total * base_steps / t64, "steps": base_steps,
+                                        "timing": "host wall clock around launch-by-launch steps"},
+        "one_engine_at_a_time_mixed_graph": {"value": total * base_steps / tmix,
+                                             "steps": base_steps,
+                                             "timing": "host wall clock, one graph launch per "
+                                                       "engine and step"},
+        "batched_over_fp64_baseline": value / (total * base_steps / t64),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -367,11 +452,19 @@ def main():
     ap.add_argument("--n", type=int, default=200000)
     ap.add_argument("--p", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched", action="store_true",
+                    help="batched-replica measurement instead of the headline line")
+    ap.add_argument("--replicas", type=int, default=256)
+    ap.add_argument("--batch-nmin", type=int, default=4000)
+    ap.add_argument("--batch-nmax", type=int, default=20000)
+    ap.add_argument("--batch-seed", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.batched:
+        return run_batched(args)
     return run_ours(args)
 
 
