@@ -349,6 +349,18 @@ int rbx_engine_set_profiling(rbx_engine* e, int on);
  * NVEensemble::Solve launches and synchronises step by step). */
 int rbx_engine_set_step_graph(rbx_engine* e, int on);
 
+/* Adjoint of the last force evaluation (rbx_engine_compute_forces or the last
+ * step), for force-field fitting: given g = dL/dF ([n][3], host atom order)
+ * it returns dL/d(eps_t) and dL/d(sigma_t) per type ([ntypes]; mixing
+ * eps_ij = sqrt(eps_i eps_j), sigma_ij = (sigma_i + sigma_j)/2), dL/dq_i
+ * ([n], host order), dL/dalpha ([1]) and dL/dr_i ([n][3], host order, the
+ * Hessian-vector product), with the same RBL lists, batch selection and
+ * k-samples held fixed.  Computed in FP64 in both forms (the mixed form's
+ * rho(k) is recomputed in FP64); any output may be null.  RBL engines only.
+ * No counterpart in the reference (RBMD has no adjoint). */
+int rbx_engine_force_vjp(rbx_engine* e, const double* g, double* d_eps, double* d_sigma,
+                         double* d_charge, double* d_alpha, double* d_pos);
+
 /* ---- Batches of replicas ------------------------------------------------
  * Independent engines on one device advanced together: each rbx_batch_step
  * MD step is one CUDA graph launch in which every replica's step is a

@@ -122,6 +122,24 @@ double gauss_sum(const rbx_box& b, double alpha) {
   return h[0] * h[1] * h[2] - 1.0;
 }
 
+// dS/dalpha of gauss_sum: H_d = sqrt(alpha L^2 / pi) sum_m e^{-alpha L^2 m^2}.
+double gauss_sum_dalpha(const rbx_box& b, double alpha) {
+  double h[3], dh[3];
+  for (int d = 0; d < 3; ++d) {
+    const double L = b.hi[d] - b.lo[d];
+    double w = 0.0, w2 = 0.0;
+    for (int m = -10; m <= 10; ++m) {
+      const double e = exp(-alpha * L * L * (double)(m * m));
+      w += e;
+      w2 += L * L * (double)(m * m) * e;
+    }
+    const double pre = sqrt(alpha * L * L / M_PI);
+    h[d] = pre * w;
+    dh[d] = pre * w / (2.0 * alpha) - pre * w2;
+  }
+  return dh[0] * h[1] * h[2] + h[0] * dh[1] * h[2] + h[0] * h[1] * dh[2];
+}
+
 int rbl_freq(int n_global, const rbx_box& b, double r_core, double cut_off, int sample_num) {
   const double V = (b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]) * (b.hi[2] - b.lo[2]);
   const double rho = (double)n_global / V;

@@ -27,6 +27,7 @@
 namespace rbx {
 int require_device();
 double gauss_sum(const rbx_box& b, double alpha);
+double gauss_sum_dalpha(const rbx_box& b, double alpha);
 int rbl_freq(int n_global, const rbx_box& b, double r_core, double cut_off, int sample_num);
 }  // namespace rbx
 
@@ -846,6 +847,98 @@ int rbx_engine::set_k_samples(int p, const double* hmx, const double* hmy, const
   return RBX_OK;
 }
 
+// Adjoint of the last force evaluation: upstream g = dL/dF ([n][3], host
+// order) -> dL/d(eps_t, sigma_t) per type, dL/dq_i, dL/dalpha, dL/dr_i
+// (host order).  Uses the lists, batch selection (epoch) and k-samples of that
+// evaluation; nothing may have moved since.
+int rbx_engine::force_vjp(const double* g, double* d_eps, double* d_sigma, double* d_q_out,
+                          double* d_alpha, double* d_r_out) {
+  cudaSetDevice(device);
+  if (prm.neighbor_type != RBX_NEIGHBOR_RBL || !have_forces || !have_cache) {
+    set_error("force_vjp: needs an RBL engine whose forces were computed at the current state");
+    return RBX_ERR_INVALID;
+  }
+  const size_t N = (size_t)n;
+  const int nt = prm.ntypes, npar = 2 * nt + 1;
+  const int nb_pair = adj_pair_blocks(n), nb_k = adj_k_blocks(n);
+  if (!adj_buf) {
+    // g (3n), d_r (3n), d_q (n), type tables (2 nt), pair partials, k partials
+    adj_len = 7 * N + 2 * (size_t)nt + (size_t)nb_pair * npar + (size_t)nb_k;
+    ETRY(alloc(&adj_buf, adj_len));
+  }
+  double* gx = adj_buf;
+  double* gy = gx + N;
+  double* gz = gy + N;
+  double* rx = gz + N;
+  double* ry = rx + N;
+  double* rz = ry + N;
+  double* dq = rz + N;
+  double* sig_t = dq + N;
+  double* eps_t = sig_t + nt;
+  double* ppart = eps_t + nt;
+  double* kpart = ppart + (size_t)nb_pair * npar;
+  double mean_g[3] = {0, 0, 0};
+  for (size_t i = 0; i < N; ++i)
+    for (int d = 0; d < 3; ++d) mean_g[d] += g[3 * i + d];
+  for (int d = 0; d < 3; ++d) mean_g[d] /= (double)n;
+  ETRY(cuda_ok(cudaMemcpyAsync(stage, g, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st),
+               "H2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(sig_t, sigma.data(), sizeof(double) * nt, cudaMemcpyHostToDevice,
+                               st),
+               "H2D"));
+  ETRY(cuda_ok(cudaMemcpyAsync(eps_t, eps.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, st),
+               "H2D"));
+  ETRY(launch_gather_vec3(n, orig, stage, gx, gy, gz, st));
+  ETRY(launch_adj_pair(pp, n, x, y, z, q, type, sig_t, eps_t, key_a, key_b, epoch, cand_count,
+                       cand, cap, gx, gy, gz, mean_g, rx, ry, rz, dq, ppart, nb_pair, st));
+  if (P > 0) {
+    if (prm.precision == RBX_MIXED) {  // the k table from an FP64 rho(k) of the same samples
+      ETRY(launch_rbe_rho_partial_f64(dbox, n, P, mx, my, mz, q, x, y, z, part_re, part_im,
+                                      nparts, st));
+      ETRY(launch_rbe_finalize(dbox, P, nparts, part_re, part_im, mx, my, mz, prm.alpha, S,
+                               prm.qqr2e, qsq, qsum, rho_re, rho_im, nullptr, nullptr, tab, 0,
+                               nullptr, n, nullptr, nullptr, st));
+    }
+    const double V = dbox.len[0] * dbox.len[1] * dbox.len[2];
+    const double cscale = -4.0 * M_PI * prm.qqr2e * S / ((double)P * V);
+    ETRY(launch_adj_kspace(n, P, cscale, tab, q, x, y, z, gx, gy, gz, part_re, part_im, nparts,
+                           kterm, rx, ry, rz, dq, kpart, st));
+  }
+  std::vector<double> hp((size_t)nb_pair * npar), hk(P > 0 ? nb_k : 0);
+  ETRY(cuda_ok(cudaMemcpyAsync(hp.data(), ppart, sizeof(double) * hp.size(),
+                               cudaMemcpyDeviceToHost, st),
+               "D2H"));
+  if (P > 0)
+    ETRY(cuda_ok(cudaMemcpyAsync(hk.data(), kpart, sizeof(double) * hk.size(),
+                                 cudaMemcpyDeviceToHost, st),
+                 "D2H"));
+  // per-atom outputs back in host order: [n][3] positions, [n] charges
+  double* const src[4] = {rx, ry, rz, dq};
+  for (int a = 0; a < 4; ++a) ETRY(launch_scatter_f64(n, orig, src[a], stage + (size_t)a * N, st));
+  std::vector<double> h(4 * N);
+  ETRY(cuda_ok(cudaMemcpyAsync(h.data(), stage, sizeof(double) * 4 * N, cudaMemcpyDeviceToHost,
+                               st),
+               "D2H"));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "force_vjp sync"));
+  std::vector<double> par(npar, 0.0);
+  for (int b = 0; b < nb_pair; ++b)  // fixed order
+    for (int t = 0; t < npar; ++t) par[t] += hp[(size_t)b * npar + t];
+  double gk = 0.0;
+  for (double v : hk) gk += v;
+  if (d_eps)
+    for (int t = 0; t < nt; ++t) d_eps[t] = par[t];
+  if (d_sigma)
+    for (int t = 0; t < nt; ++t) d_sigma[t] = par[nt + t];
+  if (d_alpha)  // k-space: the force scales with S(alpha) for fixed k-samples
+    *d_alpha = par[2 * nt] + (P > 0 ? gauss_sum_dalpha(box, prm.alpha) / S * gk : 0.0);
+  if (d_q_out)
+    for (size_t i = 0; i < N; ++i) d_q_out[i] = h[3 * N + i];
+  if (d_r_out)
+    for (size_t i = 0; i < N; ++i)
+      for (int d = 0; d < 3; ++d) d_r_out[3 * i + d] = h[(size_t)d * N + i];
+  return RBX_OK;
+}
+
 int rbx_engine::get_stats(rbx_stats* s) {
   cudaSetDevice(device);
   memset(s, 0, sizeof(*s));
@@ -960,6 +1053,15 @@ void* rbx_engine_stream(rbx_engine* e) { return e ? (void*)e->st : nullptr; }
 int rbx_engine_phase_ms(rbx_engine* e, float out[4]) {
   if (!e || !out) return RBX_ERR_INVALID;
   return e->phase_ms(out);
+}
+
+int rbx_engine_force_vjp(rbx_engine* e, const double* g, double* d_eps, double* d_sigma,
+                         double* d_charge, double* d_alpha, double* d_pos) {
+  if (!e || !g) {
+    set_error("rbx_engine_force_vjp: null engine or upstream gradient");
+    return RBX_ERR_INVALID;
+  }
+  return e->force_vjp(g, d_eps, d_sigma, d_charge, d_alpha, d_pos);
 }
 
 int rbx_engine_set_step_graph(rbx_engine* e, int on) {

@@ -92,6 +92,10 @@ struct rbx_engine {
   int* run_init = nullptr;   // pinned: device epoch / counter seeds of a graph run
   int* run_flags = nullptr;  // pinned: dflags[0..5] after a graph run
 
+  // adjoint scratch (allocated on first use)
+  double* adj_buf = nullptr;
+  size_t adj_len = 0;
+
   // bookkeeping
   bool have_cache = false, have_forces = false, k_injected = false, keep_parts = false;
   bool profiling = false;
@@ -135,6 +139,8 @@ struct rbx_engine {
   int get_force_parts(double* f_pair, double* f_kspace);
   int get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs, int64_t* n_shell);
   int get_stats(rbx_stats* s);
+  int force_vjp(const double* g, double* d_eps, double* d_sigma, double* d_q, double* d_alpha,
+                double* d_r);
   int phase_ms(float out[4]);
   int flush_profile();
 

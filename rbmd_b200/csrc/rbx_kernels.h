@@ -158,6 +158,28 @@ size_t full_list_scratch_bytes(int n, int ncell);
 int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
                      const double* y, const double* z, const int* cell_start, int cap,
                      int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st);
+// Force adjoint (rbx_adjoint.cu).  Pair part: per-atom dL/dr, dL/dq and
+// per-block partials [nblocks][2 ntypes + 1] (d_eps, d_sigma, d_alpha).
+int adj_pair_blocks(int n);
+int launch_adj_pair(const PairParams& pp, int n, const double* x, const double* y,
+                    const double* z, const double* q, const int* type, const double* sigma_t,
+                    const double* eps_t, const unsigned long long* key_a,
+                    const unsigned long long* key_b, int epoch, const int* cand_count,
+                    const int* cand, int cap, const double* gx, const double* gy,
+                    const double* gz, const double mean_g[3], double* d_rx, double* d_ry,
+                    double* d_rz, double* d_q, double* part, int nblocks, cudaStream_t st);
+// k-space part, added to d_r and d_q; part_gk[adj_k_blocks(n)] = block sums of g . K.
+// cscale = -4 pi qqr2e S / (P V); ab: 2p scratch; part_a/b: p * nparts scratch.
+int adj_k_blocks(int n);
+int launch_adj_kspace(int n, int p, double cscale, const KTab* tab, const double* q,
+                      const double* x, const double* y, const double* z, const double* gx,
+                      const double* gy, const double* gz, double* part_a, double* part_b,
+                      int nparts, double* ab, double* d_rx, double* d_ry, double* d_rz,
+                      double* d_q, double* part_gk, cudaStream_t st);
+// [n][3] interleaved host-order rows -> three cell-order arrays (orig[i] = host index).
+int launch_gather_vec3(int n, const int* orig, const double* src, double* x, double* y, double* z,
+                       cudaStream_t st);
+
 // A set of per-atom arrays moved together: dst[a][i] = src[a][perm[i]].
 struct ArraySet {
   static constexpr int kMaxF64 = 16, kMaxI32 = 4, kMaxU64 = 2;

@@ -23,6 +23,7 @@
 
 #include "rbx_common.cuh"
 #include "rbx_kernels.h"
+#include "rbx_pair_device.cuh"
 
 namespace rbx {
 
@@ -37,12 +38,6 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 
 // LJ 12-6 force/r (lj126_rs, src/force/src/lj_op/rocm/lj_op.hip.cu:40-54) in FP64.
 __device__ __forceinline__ double lj_f64(double eps_ij, double s6, double d2) {
@@ -109,26 +104,6 @@ __device__ __forceinline__ void write_block_partial(double (*s_acc)[3], double* 
 // j, min image, no FMA) decides.  The outcome is therefore identical to the
 // FP64 predicate on every pair, in both precision forms.
 // ---------------------------------------------------------------------------
-struct Classified {
-  bool core_active;    // core list and lj126_rs window (r^2 > EPS)
-  bool shell_window;   // shell list and rcs window (r_core^2 < r^2 < cut_off^2)
-};
-
-__device__ __forceinline__ Classified classify_exact(double d2, const PairParams& pp) {
-  Classified c;
-  const bool A = d2 < pp.core2_list;
-  c.core_active = A && d2 > RBX_EPSILON;  // d2 < rs2 holds: core2_list < rs2
-  c.shell_window = !A && d2 < pp.force2_list && d2 > pp.rs2;  // force2_list < rc2
-  return c;
-}
-
-__device__ __forceinline__ double exact_d2(const PairParams& pp, const double* __restrict__ x,
-                                           const double* __restrict__ y,
-                                           const double* __restrict__ z, int i, int j) {
-  return dist2_list(pp.box, __ldg(x + i), __ldg(y + i), __ldg(z + i), __ldg(x + j),
-                    __ldg(y + j), __ldg(z + j));
-}
-
 // Screened classification; *unsure is set when a threshold band is hit.  The
 // band around core2_list and the one around rs2 (which lies just above it)
 // are merged into one undecided interval, as are d2 values at or below the

@@ -92,7 +92,7 @@ EXPORTS = [
     "rbx_engine_get_stats", "rbx_engine_stream", "rbx_engine_phase_ms",
     "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc", "rbx_engine_set_step_graph",
     "rbx_nlist_should_reuse", "rbx_batch_create", "rbx_batch_destroy", "rbx_batch_step",
-    "rbx_batch_stream",
+    "rbx_batch_stream", "rbx_engine_force_vjp",
 ]
 
 
@@ -147,6 +147,7 @@ def lib():
     L.rbx_engine_phase_ms.argtypes = [vp, C.POINTER(C.c_float)]
     L.rbx_engine_set_profiling.argtypes = [vp, ip]
     L.rbx_engine_set_step_graph.argtypes = [vp, ip]
+    L.rbx_engine_force_vjp.argtypes = [vp] + [vp] * 6
     L.rbx_batch_create.restype = vp
     L.rbx_batch_create.argtypes = [C.POINTER(vp), ip]
     L.rbx_batch_destroy.argtypes = [vp]
@@ -415,6 +416,19 @@ class Engine:
     @property
     def stream(self) -> int:
         return int(lib().rbx_engine_stream(self._h) or 0)
+
+    def force_vjp(self, g):
+        """dL/d(eps, sigma per type; q per atom; alpha; positions) for g = dL/dF [n, 3]."""
+        g = np.ascontiguousarray(g, dtype=np.float64).reshape(self.n, 3)
+        nt = len(self._sigma)
+        out = {"eps": np.zeros(nt), "sigma": np.zeros(nt), "charge": np.zeros(self.n),
+               "alpha": np.zeros(1), "pos": np.zeros((self.n, 3))}
+        check(lib().rbx_engine_force_vjp(self._h, _np_ptr(g), _np_ptr(out["eps"]),
+                                         _np_ptr(out["sigma"]), _np_ptr(out["charge"]),
+                                         _np_ptr(out["alpha"]), _np_ptr(out["pos"])),
+              "rbx_engine_force_vjp")
+        out["alpha"] = float(out["alpha"][0])
+        return out
 
     def set_step_graph(self, on=True):
         check(lib().rbx_engine_set_step_graph(self._h, int(on)), "set_step_graph")

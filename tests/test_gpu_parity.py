@@ -499,3 +499,48 @@ def test_engine_energy_conservation_short(cuda, rbx):
     assert np.isfinite(out["pos"]).all() and np.isfinite(out["vel"]).all()
     T = (out["vel"] ** 2).sum() / (3 * s["n"])
     assert 0.5 < T < 3.0
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_force_vjp_matches_oracle_adjoint(cuda, rbx, oracle, prec):
+    """The engine's adjoint (rbx_engine_force_vjp) against the FP64 adjoint
+    reference, itself pinned to central differences of the oracle's force:
+    parameter gradients per type, dL/dq per atom and dL/dr (Hessian-vector
+    product), with the same lists, batch and k-samples."""
+    from oracle import adjoint as A
+
+    s = systems.lj_electrolyte(4000, seed=41)
+    p = s["params"]
+    ep = 7
+    box = oracle.Box.make(s["lo"], s["hi"])
+    L = np.asarray(s["hi"]) - np.asarray(s["lo"])
+    m = oracle.rbe_sample_philox(box, p["alpha"], p["kspace_p"], 3, ep)
+    e = rbx.Engine(s, precision=prec)
+    e.set_k_samples(*m)
+    e.compute_forces(epoch=ep)
+    g = np.random.default_rng(5).normal(size=(s["n"], 3))
+    got = e.force_vjp(g)
+    e.close()
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    perm, cell, cs, ce = oracle.cells_sort(box, 5.3, x, y, z)
+    pos = s["pos"][perm]
+    cnt, rows = oracle.full_list(box, 5.3, *(np.ascontiguousarray(pos[:, d]) for d in range(3)),
+                                 cell, cs, ce)
+    freq, _, _ = oracle.rbl_params(s["n"], box, p["r_core"], p["cut_off"],
+                                   p["neighbor_sample_num"])
+    cc, core, sc, shell = oracle.rbl_filter(box, p["r_core"], p["cut_off"], freq, ep, s["gid"][perm],
+                                            *(np.ascontiguousarray(pos[:, d]) for d in range(3)),
+                                            cnt, rows)
+    lists = A.rbl_pairs(cc, core, sc, shell, freq)
+    d_eps, d_sig, d_q, d_alpha, d_r = A.force_vjp(
+        pos, L, s["type"][perm], np.asarray(s["sigma"], float), np.asarray(s["eps"], float),
+        s["q"][perm], p["alpha"], p["qqr2e"], p["r_core"], p["cut_off"], freq, lists, m, g[perm])
+    want_q = np.zeros(s["n"])
+    want_q[perm] = d_q
+    want_r = np.zeros((s["n"], 3))
+    want_r[perm] = d_r
+    assert np.allclose(got["eps"], d_eps, rtol=1e-9, atol=1e-9 * np.abs(d_eps).max())
+    assert np.allclose(got["sigma"], d_sig, rtol=1e-9, atol=1e-9 * np.abs(d_sig).max())
+    assert abs(got["alpha"] - d_alpha) < 1e-9 * abs(d_alpha)
+    assert systems.rel_rms(got["charge"][:, None], want_q[:, None]) < 1e-9
+    assert systems.rel_rms(got["pos"], want_r) < 1e-9
