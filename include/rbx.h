@@ -349,6 +349,15 @@ int rbx_engine_set_profiling(rbx_engine* e, int on);
  * NVEensemble::Solve launches and synchronises step by step). */
 int rbx_engine_set_step_graph(rbx_engine* e, int on);
 
+/* Force-field parameters of a live engine (for fitting): per-type LJ sigma
+ * and eps ([ntypes]), per-atom charges ([n], host atom order), the RBE/Ewald
+ * alpha (JSON alpha = g_ewald^2).  Forces must be computed again afterwards.
+ * RBMD reads these once at Init (LJCutCoulKspace::Init, KSpaceCalculator::Init);
+ * no counterpart for changing them later. */
+int rbx_engine_set_lj_params(rbx_engine* e, const double* sigma, const double* eps);
+int rbx_engine_set_charges(rbx_engine* e, const double* charge);
+int rbx_engine_set_alpha(rbx_engine* e, double alpha);
+
 /* Adjoint of the last force evaluation (rbx_engine_compute_forces or the last
  * step), for force-field fitting: given g = dL/dF ([n][3], host atom order)
  * it returns dL/d(eps_t) and dL/d(sigma_t) per type ([ntypes]; mixing

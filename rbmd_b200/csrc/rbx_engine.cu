@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <string>
 #include <unordered_map>
+#include <cmath>
 #include <vector>
 
 #include "rbx.h"
@@ -158,24 +159,7 @@ int rbx_engine::init() {
   ETRY(alloc(&lj_eps, (size_t)prm.ntypes * prm.ntypes));
   ETRY(alloc(&lj_s6, (size_t)prm.ntypes * prm.ntypes));
   // LJ mixing of ComputeLJCutCoulRBLForce (lj_cut_coul_kspace_op.hip.cu:582-600):
-  // eps_ij = sqrt(eps_i eps_j), sigma_ij = (sigma_i + sigma_j)/2, sigma_ij^6.
-  {
-    const int nt = prm.ntypes;
-    std::vector<double> he(nt * nt), hs(nt * nt), im(nt);
-    for (int a = 0; a < nt; ++a) {
-      im[a] = 1.0 / mass[a];
-      for (int b = 0; b < nt; ++b) {
-        he[a * nt + b] = sqrt(eps[a] * eps[b]);
-        hs[a * nt + b] = pow((sigma[a] + sigma[b]) / 2, 6.0);
-      }
-    }
-    ETRY(cuda_ok(cudaMemcpy(inv_mass, im.data(), sizeof(double) * nt, cudaMemcpyHostToDevice),
-                 "H2D"));
-    ETRY(cuda_ok(cudaMemcpy(lj_eps, he.data(), sizeof(double) * nt * nt, cudaMemcpyHostToDevice),
-                 "H2D"));
-    ETRY(cuda_ok(cudaMemcpy(lj_s6, hs.data(), sizeof(double) * nt * nt, cudaMemcpyHostToDevice),
-                 "H2D"));
-  }
+  ETRY(upload_type_tables());
   if (P > 0) {
     nparts = rbe_partial_blocks(n);
     ETRY(alloc(&mx, (size_t)P));
@@ -188,22 +172,7 @@ int rbx_engine::init() {
     ETRY(alloc(&rho_im, (size_t)P));
     ETRY(alloc(&tab, (size_t)P));
     ETRY(alloc(&kterm, (size_t)8 * P));
-    // Philox sampler tables
-    std::vector<double> w;
-    int off = 0;
-    for (int d = 0; d < 3; ++d) {
-      std::vector<double> t(8192);
-      tcnt[d] = rbe_axis_table(dbox.len[d], prm.alpha, t.data(), 8192, &ttot[d]);
-      if (tcnt[d] < 0) {
-        set_error("k-sampler table too large for this box/alpha");
-        return RBX_ERR_SAMPLER;
-      }
-      w.insert(w.end(), t.begin(), t.begin() + tcnt[d]);
-      off += tcnt[d];
-    }
-    ETRY(alloc(&sample_tables, (size_t)off));
-    ETRY(cuda_ok(cudaMemcpy(sample_tables, w.data(), sizeof(double) * off, cudaMemcpyHostToDevice),
-                 "H2D"));
+    ETRY(build_sampler_tables());
   } else {
     ETRY(alloc(&tab, 1));
     ETRY(alloc(&mx, 1));
@@ -939,6 +908,102 @@ int rbx_engine::force_vjp(const double* g, double* d_eps, double* d_sigma, doubl
   return RBX_OK;
 }
 
+// Per-type-pair LJ tables, eps_ij = sqrt(eps_i eps_j), sigma_ij^6 with
+// sigma_ij = (sigma_i + sigma_j)/2, and the inverse masses.
+int rbx_engine::upload_type_tables() {
+  const int nt = prm.ntypes;
+  std::vector<double> he(nt * nt), hs(nt * nt), im(nt);
+  for (int a = 0; a < nt; ++a) {
+    im[a] = 1.0 / mass[a];
+    for (int b = 0; b < nt; ++b) {
+      he[a * nt + b] = sqrt(eps[a] * eps[b]);
+      hs[a * nt + b] = pow((sigma[a] + sigma[b]) / 2, 6.0);
+    }
+  }
+  ETRY(cuda_ok(cudaMemcpy(inv_mass, im.data(), sizeof(double) * nt, cudaMemcpyHostToDevice),
+               "H2D"));
+  ETRY(cuda_ok(cudaMemcpy(lj_eps, he.data(), sizeof(double) * nt * nt, cudaMemcpyHostToDevice),
+               "H2D"));
+  return cuda_ok(cudaMemcpy(lj_s6, hs.data(), sizeof(double) * nt * nt, cudaMemcpyHostToDevice),
+                 "H2D");
+}
+
+// Cumulative per-axis k-sampling tables for the current alpha.
+int rbx_engine::build_sampler_tables() {
+  std::vector<double> w;
+  int off = 0;
+  for (int d = 0; d < 3; ++d) {
+    std::vector<double> t(8192);
+    tcnt[d] = rbe_axis_table(dbox.len[d], prm.alpha, t.data(), 8192, &ttot[d]);
+    if (tcnt[d] < 0) {
+      set_error("k-sampler table too large for this box/alpha");
+      return RBX_ERR_SAMPLER;
+    }
+    w.insert(w.end(), t.begin(), t.begin() + tcnt[d]);
+    off += tcnt[d];
+  }
+  release(sample_tables);
+  ETRY(alloc(&sample_tables, (size_t)off));
+  return cuda_ok(cudaMemcpy(sample_tables, w.data(), sizeof(double) * off, cudaMemcpyHostToDevice),
+                 "H2D");
+}
+
+// Force-field parameters (host atom order for charges).  Forces must be
+// computed again; a captured step graph is captured again where it holds them.
+int rbx_engine::set_lj_params(const double* hsigma, const double* heps) {
+  cudaSetDevice(device);
+  for (int t = 0; t < prm.ntypes; ++t)
+    if (!(hsigma[t] > 0.0) || !(heps[t] >= 0.0)) {
+      set_error("type %d: sigma must be > 0 and eps >= 0", t);
+      return RBX_ERR_INVALID;
+    }
+  sigma.assign(hsigma, hsigma + prm.ntypes);
+  eps.assign(heps, heps + prm.ntypes);
+  have_forces = false;
+  return upload_type_tables();
+}
+
+int rbx_engine::set_charges(const double* hq) {
+  cudaSetDevice(device);
+  qsq = 0;
+  qsum = 0;
+  for (int i = 0; i < n; ++i) {
+    if (!std::isfinite(hq[i])) {
+      set_error("atom %d has a non-finite charge", i);
+      return RBX_ERR_INVALID;
+    }
+    qsq += hq[i] * hq[i];
+    qsum += hq[i];
+  }
+  ETRY(cuda_ok(cudaMemcpyAsync(stage, hq, sizeof(double) * n, cudaMemcpyHostToDevice, st), "H2D"));
+  ETRY(launch_gather_f64(n, orig, stage, q, st));
+  ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "set_charges sync"));
+  have_forces = false;
+  graph_dirty = true;  // the energy terms carry the charge sums
+  ++graph_version;
+  return RBX_OK;
+}
+
+int rbx_engine::set_alpha(double a) {
+  cudaSetDevice(device);
+  if (!(a > 0.0)) {
+    set_error("alpha must be > 0");
+    return RBX_ERR_INVALID;
+  }
+  prm.alpha = a;
+  pp.alpha = a;
+  pp.sqrt_alpha = sqrt(a);
+  if (P > 0) {
+    S = gauss_sum(box, a);
+    ETRY(build_sampler_tables());
+  }
+  have_forces = false;
+  graph_dirty = true;
+  ++graph_version;
+  return RBX_OK;
+}
+
 int rbx_engine::get_stats(rbx_stats* s) {
   cudaSetDevice(device);
   memset(s, 0, sizeof(*s));
@@ -1062,6 +1127,27 @@ int rbx_engine_force_vjp(rbx_engine* e, const double* g, double* d_eps, double* 
     return RBX_ERR_INVALID;
   }
   return e->force_vjp(g, d_eps, d_sigma, d_charge, d_alpha, d_pos);
+}
+
+int rbx_engine_set_lj_params(rbx_engine* e, const double* sigma, const double* eps) {
+  if (!e || !sigma || !eps) {
+    set_error("rbx_engine_set_lj_params: null argument");
+    return RBX_ERR_INVALID;
+  }
+  return e->set_lj_params(sigma, eps);
+}
+
+int rbx_engine_set_charges(rbx_engine* e, const double* charge) {
+  if (!e || !charge) {
+    set_error("rbx_engine_set_charges: null argument");
+    return RBX_ERR_INVALID;
+  }
+  return e->set_charges(charge);
+}
+
+int rbx_engine_set_alpha(rbx_engine* e, double alpha) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->set_alpha(alpha);
 }
 
 int rbx_engine_set_step_graph(rbx_engine* e, int on) {

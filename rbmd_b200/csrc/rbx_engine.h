@@ -139,6 +139,11 @@ struct rbx_engine {
   int get_force_parts(double* f_pair, double* f_kspace);
   int get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs, int64_t* n_shell);
   int get_stats(rbx_stats* s);
+  int upload_type_tables();
+  int build_sampler_tables();
+  int set_lj_params(const double* sigma, const double* eps);
+  int set_charges(const double* q);
+  int set_alpha(double alpha);
   int force_vjp(const double* g, double* d_eps, double* d_sigma, double* d_q, double* d_alpha,
                 double* d_r);
   int phase_ms(float out[4]);

@@ -92,7 +92,8 @@ EXPORTS = [
     "rbx_engine_get_stats", "rbx_engine_stream", "rbx_engine_phase_ms",
     "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc", "rbx_engine_set_step_graph",
     "rbx_nlist_should_reuse", "rbx_batch_create", "rbx_batch_destroy", "rbx_batch_step",
-    "rbx_batch_stream", "rbx_engine_force_vjp",
+    "rbx_batch_stream", "rbx_engine_force_vjp", "rbx_engine_set_lj_params",
+    "rbx_engine_set_charges", "rbx_engine_set_alpha",
 ]
 
 
@@ -148,6 +149,9 @@ def lib():
     L.rbx_engine_set_profiling.argtypes = [vp, ip]
     L.rbx_engine_set_step_graph.argtypes = [vp, ip]
     L.rbx_engine_force_vjp.argtypes = [vp] + [vp] * 6
+    L.rbx_engine_set_lj_params.argtypes = [vp, vp, vp]
+    L.rbx_engine_set_charges.argtypes = [vp, vp]
+    L.rbx_engine_set_alpha.argtypes = [vp, dp]
     L.rbx_batch_create.restype = vp
     L.rbx_batch_create.argtypes = [C.POINTER(vp), ip]
     L.rbx_batch_destroy.argtypes = [vp]
@@ -363,8 +367,19 @@ class Engine:
                [np.ascontiguousarray(vel[:, d]) for d in range(3)]
         gid = np.ascontiguousarray(sys["gid"], dtype=np.int32)
         typ = np.ascontiguousarray(sys["type"], dtype=np.int32)
+        self._gid, self._typ, self._q = gid, typ, q
         check(L.rbx_engine_set_state(self._h, _np_ptr(gid), _np_ptr(typ), _np_ptr(q),
                                      *[_np_ptr(c) for c in cols]), "rbx_engine_set_state")
+
+    def set_positions(self, pos, vel=None):
+        """New positions (host order, [n, 3]); velocities kept unless given."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(self.n, 3)
+        vel = self.get_state()["vel"] if vel is None else np.asarray(vel, dtype=np.float64)
+        cols = [np.ascontiguousarray(pos[:, d]) for d in range(3)] + \
+               [np.ascontiguousarray(vel[:, d]) for d in range(3)]
+        check(lib().rbx_engine_set_state(self._h, _np_ptr(self._gid), _np_ptr(self._typ),
+                                         _np_ptr(self._q), *[_np_ptr(c) for c in cols]),
+              "rbx_engine_set_state")
 
     def set_k_samples(self, mx, my, mz):
         if mx is None:
@@ -416,6 +431,20 @@ class Engine:
     @property
     def stream(self) -> int:
         return int(lib().rbx_engine_stream(self._h) or 0)
+
+    def set_lj_params(self, sigma, eps):
+        self._sigma = np.ascontiguousarray(sigma, dtype=np.float64)
+        self._eps = np.ascontiguousarray(eps, dtype=np.float64)
+        check(lib().rbx_engine_set_lj_params(self._h, _np_ptr(self._sigma), _np_ptr(self._eps)),
+              "rbx_engine_set_lj_params")
+
+    def set_charges(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        check(lib().rbx_engine_set_charges(self._h, _np_ptr(q)), "rbx_engine_set_charges")
+        self._q = q
+
+    def set_alpha(self, alpha):
+        check(lib().rbx_engine_set_alpha(self._h, float(alpha)), "rbx_engine_set_alpha")
 
     def force_vjp(self, g):
         """dL/d(eps, sigma per type; q per atom; alpha; positions) for g = dL/dF [n, 3]."""

@@ -544,3 +544,85 @@ def test_force_vjp_matches_oracle_adjoint(cuda, rbx, oracle, prec):
     assert abs(got["alpha"] - d_alpha) < 1e-9 * abs(d_alpha)
     assert systems.rel_rms(got["charge"][:, None], want_q[:, None]) < 1e-9
     assert systems.rel_rms(got["pos"], want_r) < 1e-9
+
+
+def test_force_vjp_against_engine_finite_differences(cuda, rbx):
+    """Central differences of the engine's own FP64 force, through the
+    parameter setters, against rbx_engine_force_vjp."""
+    s = systems.lj_electrolyte(4000, seed=43)
+    p = s["params"]
+    from oracle import oracle as O
+
+    m = O.rbe_sample_philox(O.Box.make(s["lo"], s["hi"]), p["alpha"], p["kspace_p"], 2, 4)
+    e = rbx.Engine(s, precision=rbx.PLAIN_FP64)
+    e.set_k_samples(*m)
+    e.compute_forces(4)
+    g = np.random.default_rng(8).normal(size=(s["n"], 3))
+    got = e.force_vjp(g)
+    sig0, eps0 = np.asarray(s["sigma"], float), np.asarray(s["eps"], float)
+    Q = np.array([0.0, 1.0, -1.0])
+
+    def L():
+        e.compute_forces(4)
+        return float((g * e.get_state()["force"]).sum())
+
+    def fd(setter, base, step):
+        """Central difference along `step` (scalar, or an array with one nonzero entry)."""
+        h = float(np.max(np.abs(step)))
+        setter(base + step)
+        up = L()
+        setter(base - step)
+        dn = L()
+        setter(base)
+        return (up - dn) / (2 * h)
+
+    def close(a, b, rel=1e-5):
+        assert abs(a - b) <= rel * max(abs(a), abs(b)) + 1e-8, (a, b)
+
+    for t in range(3):
+        unit = np.eye(3)[t]
+        close(got["eps"][t], fd(lambda v: e.set_lj_params(sig0, v), eps0, 1e-6 * eps0[t] * unit))
+        close(got["sigma"][t], fd(lambda v: e.set_lj_params(v, eps0), sig0, 1e-6 * sig0[t] * unit))
+        close(got["charge"][s["type"] == t].sum(),
+              fd(lambda v: e.set_charges(v[s["type"]]), Q, 1e-6 * unit))
+    close(got["alpha"], fd(e.set_alpha, p["alpha"], 1e-6 * p["alpha"]))
+    pos0 = s["pos"].copy()
+    for a in (0, 1234):
+        for d in range(3):
+            dp = np.zeros_like(pos0)
+            dp[a, d] = 1e-6
+            close(got["pos"][a, d], fd(e.set_positions, pos0, dp), rel=1e-4)
+    e.close()
+
+
+def test_autograd_function_gradients(cuda, rbx):
+    """torch.autograd through RBLRBEForce gives the adjoint's gradients."""
+    import torch
+
+    from rbmd_b200.autograd import force
+
+    s = systems.lj_electrolyte(4000, seed=44)
+    p = s["params"]
+    from oracle import oracle as O
+
+    m = O.rbe_sample_philox(O.Box.make(s["lo"], s["hi"]), p["alpha"], p["kspace_p"], 6, 1)
+    e = rbx.Engine(s, precision=rbx.MIXED)
+    e.set_k_samples(*m)
+    t64 = torch.float64
+    eps = torch.tensor(s["eps"], dtype=t64, requires_grad=True)
+    sig = torch.tensor(s["sigma"], dtype=t64, requires_grad=True)
+    Q = torch.tensor([0.0, 1.0, -1.0], dtype=t64, requires_grad=True)
+    alpha = torch.tensor(p["alpha"], dtype=t64, requires_grad=True)
+    pos = torch.tensor(s["pos"], dtype=t64, requires_grad=True)
+    typ = torch.as_tensor(s["type"], dtype=torch.long)
+    f_ref = force(e, eps.detach() * 1.05, sig.detach() * 0.97, Q.detach()[typ] * 1.02,
+                  alpha.detach(), pos.detach(), 1).detach()
+    f = force(e, eps, sig, Q[typ], alpha, pos, 1)
+    loss = ((f - f_ref) ** 2).mean()
+    loss.backward()
+    g = (2.0 * (f - f_ref) / f.numel()).detach().numpy()
+    direct = e.force_vjp(g)  # same state as the forward above
+    assert np.allclose(eps.grad.numpy(), direct["eps"], rtol=1e-12)
+    assert np.allclose(pos.grad.numpy(), direct["pos"], rtol=1e-12, atol=1e-15)
+    assert np.isfinite(Q.grad.numpy()).all() and alpha.grad is not None
+    e.close()
