@@ -370,6 +370,45 @@ int rbx_engine_set_alpha(rbx_engine* e, double alpha);
 int rbx_engine_force_vjp(rbx_engine* e, const double* g, double* d_eps, double* d_sigma,
                          double* d_charge, double* d_alpha, double* d_pos);
 
+/* ---- LAMMPS data files --------------------------------------------------
+ * The reader of RBMD's read_data (LammpsFullReader,
+ * src/reader/src/format/lammps/lammps_full_reader.cpp): header counts and
+ * orthogonal box, Masses, Pair Coeffs (eps sigma per type), Atoms in the
+ * atomic / charge / full style with optional image flags, Velocities, Bonds,
+ * Angles, Dihedrals, Impropers.  Ids, types and molecules are returned 0-based
+ * as RBMD stores them (its atom id is the RBL batch-hash id); atoms stay in
+ * file order.  atom_style may be null (taken from the "Atoms # <style>"
+ * comment); replicate (may be null) tiles the box like
+ * init_configuration.read_data.replicate. */
+typedef struct rbx_lammps_data rbx_lammps_data;
+typedef struct rbx_lammps_info {
+  int64_t n_atoms, n_bonds, n_angles, n_dihedrals, n_impropers;
+  int n_atom_types, n_bond_types, n_angle_types, n_dihedral_types, n_improper_types;
+  int atom_style; /* 0 atomic, 1 charge, 2 full */
+  int has_masses, has_pair_coeffs, has_velocities, has_images;
+  rbx_box box;
+} rbx_lammps_info;
+rbx_lammps_data* rbx_lammps_read(const char* path, const char* atom_style, const int* replicate);
+void rbx_lammps_free(rbx_lammps_data* d);
+int rbx_lammps_get_info(const rbx_lammps_data* d, rbx_lammps_info* out);
+/* Per-atom arrays of n_atoms entries (image: [n][3]); any may be null. */
+int rbx_lammps_get_atoms(const rbx_lammps_data* d, int64_t* id, int* type, int* molecule,
+                         double* charge, double* x, double* y, double* z, double* vx,
+                         double* vy, double* vz, int* image);
+/* Per-type mass, Pair Coeffs eps and sigma ([n_atom_types]); any may be null. */
+int rbx_lammps_get_types(const rbx_lammps_data* d, double* mass, double* eps, double* sigma);
+/* kind 2 bonds, 3 angles, 4 dihedrals, 5 impropers: types [count] and 0-based
+ * atom ids [count][kind == 2 ? 2 : kind == 3 ? 3 : 4]. */
+int rbx_lammps_get_topology(const rbx_lammps_data* d, int kind, int* type, int64_t* atoms);
+/* Writes an atom_style charge data file with ids id[i] + 1 and types
+ * type[i] + 1 (so a reader that makes them 0-based sees id[i], type[i]);
+ * velocities may be null. */
+int rbx_lammps_write_charge(const char* path, const rbx_box* box, int n, int ntypes,
+                            const double* mass, const double* eps, const double* sigma,
+                            const int64_t* id, const int* type, const double* charge,
+                            const double* x, const double* y, const double* z, const double* vx,
+                            const double* vy, const double* vz);
+
 /* ---- Batches of replicas ------------------------------------------------
  * Independent engines on one device advanced together: each rbx_batch_step
  * MD step is one CUDA graph launch in which every replica's step is a

@@ -93,8 +93,19 @@ EXPORTS = [
     "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc", "rbx_engine_set_step_graph",
     "rbx_nlist_should_reuse", "rbx_batch_create", "rbx_batch_destroy", "rbx_batch_step",
     "rbx_batch_stream", "rbx_engine_force_vjp", "rbx_engine_set_lj_params",
-    "rbx_engine_set_charges", "rbx_engine_set_alpha",
+    "rbx_engine_set_charges", "rbx_engine_set_alpha", "rbx_lammps_read", "rbx_lammps_free",
+    "rbx_lammps_get_info", "rbx_lammps_get_atoms", "rbx_lammps_get_types",
+    "rbx_lammps_get_topology", "rbx_lammps_write_charge",
 ]
+
+
+class LammpsInfo(C.Structure):
+    _fields_ = [("n_atoms", C.c_int64), ("n_bonds", C.c_int64), ("n_angles", C.c_int64),
+                ("n_dihedrals", C.c_int64), ("n_impropers", C.c_int64),
+                ("n_atom_types", C.c_int), ("n_bond_types", C.c_int), ("n_angle_types", C.c_int),
+                ("n_dihedral_types", C.c_int), ("n_improper_types", C.c_int),
+                ("atom_style", C.c_int), ("has_masses", C.c_int), ("has_pair_coeffs", C.c_int),
+                ("has_velocities", C.c_int), ("has_images", C.c_int), ("box", Box)]
 
 
 def lib():
@@ -152,6 +163,14 @@ def lib():
     L.rbx_engine_set_lj_params.argtypes = [vp, vp, vp]
     L.rbx_engine_set_charges.argtypes = [vp, vp]
     L.rbx_engine_set_alpha.argtypes = [vp, dp]
+    L.rbx_lammps_read.restype = vp
+    L.rbx_lammps_read.argtypes = [C.c_char_p, C.c_char_p, vp]
+    L.rbx_lammps_free.argtypes = [vp]
+    L.rbx_lammps_get_info.argtypes = [vp, C.POINTER(LammpsInfo)]
+    L.rbx_lammps_get_atoms.argtypes = [vp] + [vp] * 11
+    L.rbx_lammps_get_types.argtypes = [vp, vp, vp, vp]
+    L.rbx_lammps_get_topology.argtypes = [vp, ip, vp, vp]
+    L.rbx_lammps_write_charge.argtypes = [C.c_char_p, B, ip, ip] + [vp] * 12
     L.rbx_batch_create.restype = vp
     L.rbx_batch_create.argtypes = [C.POINTER(vp), ip]
     L.rbx_batch_destroy.argtypes = [vp]
@@ -510,3 +529,62 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# LAMMPS data files
+# ---------------------------------------------------------------------------
+def read_lammps(path, atom_style=None, replicate=None) -> dict:
+    """rbx_lammps_read: the data file as 0-based arrays (file order)."""
+    L = lib()
+    rep = (C.c_int * 3)(*replicate) if replicate is not None else None
+    h = L.rbx_lammps_read(str(path).encode(), atom_style.encode() if atom_style else None, rep)
+    if not h:
+        raise RbxError(f"rbx_lammps_read failed: {last_error()}")
+    try:
+        info = LammpsInfo()
+        check(L.rbx_lammps_get_info(h, C.byref(info)), "rbx_lammps_get_info")
+        n, nt = info.n_atoms, info.n_atom_types
+        out = {"n": n, "ntypes": nt, "atom_style": ["atomic", "charge", "full"][info.atom_style],
+               "lo": [info.box.lo[d] for d in range(3)], "hi": [info.box.hi[d] for d in range(3)],
+               "has_velocities": bool(info.has_velocities), "has_images": bool(info.has_images),
+               "id": np.zeros(n, np.int64), "type": np.zeros(n, np.int32),
+               "molecule": np.zeros(n, np.int32), "q": np.zeros(n), "pos": None, "vel": None,
+               "image": np.zeros((n, 3), np.int32), "mass": np.zeros(nt), "eps": np.zeros(nt),
+               "sigma": np.zeros(nt)}
+        cols = [np.zeros(n) for _ in range(6)]
+        check(L.rbx_lammps_get_atoms(h, _np_ptr(out["id"]), _np_ptr(out["type"]),
+                                     _np_ptr(out["molecule"]), _np_ptr(out["q"]),
+                                     *[_np_ptr(c) for c in cols], _np_ptr(out["image"])),
+              "rbx_lammps_get_atoms")
+        out["pos"] = np.stack(cols[:3], 1)
+        out["vel"] = np.stack(cols[3:], 1)
+        check(L.rbx_lammps_get_types(h, _np_ptr(out["mass"]), _np_ptr(out["eps"]),
+                                     _np_ptr(out["sigma"])), "rbx_lammps_get_types")
+        for kind, name, cnt, width in ((2, "bonds", info.n_bonds, 2), (3, "angles", info.n_angles, 3),
+                                       (4, "dihedrals", info.n_dihedrals, 4),
+                                       (5, "impropers", info.n_impropers, 4)):
+            t = np.zeros(cnt, np.int32)
+            a = np.zeros((cnt, width), np.int64)
+            check(L.rbx_lammps_get_topology(h, kind, _np_ptr(t), _np_ptr(a)), name)
+            out[name] = (t, a)
+        return out
+    finally:
+        L.rbx_lammps_free(h)
+
+
+def write_lammps_charge(path, sys: dict):
+    """rbx_lammps_write_charge of a system dict (ids written as gid + 1)."""
+    n = int(sys["n"])
+    box = Box.make(sys["lo"], sys["hi"])
+    nt = len(sys["sigma"])
+    pos = np.ascontiguousarray(sys["pos"], np.float64)
+    vel = np.ascontiguousarray(sys["vel"], np.float64)
+    a = [np.ascontiguousarray(sys["mass"], np.float64), np.ascontiguousarray(sys["eps"], np.float64),
+         np.ascontiguousarray(sys["sigma"], np.float64),
+         np.ascontiguousarray(sys["gid"], np.int64), np.ascontiguousarray(sys["type"], np.int32),
+         np.ascontiguousarray(sys["q"], np.float64)] + \
+        [np.ascontiguousarray(pos[:, d]) for d in range(3)] + \
+        [np.ascontiguousarray(vel[:, d]) for d in range(3)]
+    check(lib().rbx_lammps_write_charge(str(path).encode(), C.byref(box), n, nt,
+                                        *[_np_ptr(v) for v in a]), "rbx_lammps_write_charge")
