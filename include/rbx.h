@@ -269,6 +269,8 @@ typedef struct {
   const double* sigma;      /* host, ntypes */
   const double* eps;        /* host, ntypes */
   const double* mass;       /* host, ntypes */
+  double fmt2v;             /* force/mass*time -> velocity of the unit style
+                               (UnitFactor::_fmt2v; 0 is read as 1, LJ units) */
 } rbx_params;
 
 /* Engine statistics (host copy). */
@@ -298,6 +300,23 @@ rbx_engine* rbx_engine_create_json(const char* json_text, const rbx_box* box,
                                    const double* eps, const double* mass,
                                    const double* charges, int precision, int device);
 void rbx_engine_destroy(rbx_engine* e);
+/* Build and load an engine from RBMD's input files the way MDApplication
+ * starts (md_application.cpp:175-195, LammpsFullReader::Load,
+ * lammps_full_reader.cpp:455-632): the JSON config at json_path ('//' and
+ * block comments allowed) names init_configuration.read_data.file (resolved
+ * next to the config, else from the working directory), atom_style, unit,
+ * replicate and velocity_type GAUSS (execution.temperature[0], velocity_seed);
+ * Masses and Pair Coeffs (eps, sigma per type) come from the data file; the
+ * plugin parameters as rbx_engine_create_json.  Atoms keep file order (host
+ * order), gid = file id - 1, positions wrapped into the box with the wraps
+ * added to the file's image flags.  Returns NULL on error. */
+rbx_engine* rbx_engine_create_from_files(const char* json_path, int precision, int device);
+/* Size, types and box of an engine; per-atom gid / type / charge in host
+ * order and per-type sigma / eps / mass.  Any pointer may be NULL. */
+int rbx_engine_get_system(rbx_engine* e, int* num_atoms, int* ntypes, rbx_box* box);
+int rbx_engine_get_atoms(rbx_engine* e, int* gid, int* type, double* charge);
+int rbx_engine_get_type_params(rbx_engine* e, double* sigma, double* eps, double* mass);
+
 
 /* Host arrays in any atom order; the engine keeps its own (cell-sorted) order. */
 int rbx_engine_set_state(rbx_engine* e, const int* gid, const int* type,
@@ -324,6 +343,20 @@ int rbx_engine_step_host(rbx_engine* e, const double* x_in, const double* v_in,
 int rbx_engine_get_state(rbx_engine* e, double* px, double* py, double* pz,
                          double* vx, double* vy, double* vz, double* fx,
                          double* fy, double* fz);
+/* Periodic image counters, [n][3] ints in the atom order given to
+ * rbx_engine_set_state: how many times each atom has wrapped through each face
+ * (+1 leaving through hi).  rbx_engine_set_state zeroes them; the drift of
+ * every step counts the wraps (UpdatePositionFlagOp, default_position_controller.cpp:111-121
+ * and update_position_op.hip.cu:22, replaces; unwrapped x = x + image * L as
+ * UnwarpPositionOp). */
+int rbx_engine_set_images(rbx_engine* e, const int* image);
+int rbx_engine_get_images(rbx_engine* e, int* image);
+/* Append (append != 0) or write one frame in RBMD's trajectory format
+ * (TrajectoryOutput::Execute, src/output/src/TrajectoryOutput.cpp:467-500):
+ * "ITEM: TIMESTEP", "ITEM: NUMBER OF ATOMS", "ITEM: BOX BOUNDS pp pp pp" with
+ * lo hi per axis, then "ITEM: ATOMS id type q x y z xu yu zu vx vy vz" sorted
+ * by id, ids and types 1-based, reals in shortest round-trip form. */
+int rbx_engine_write_trajectory(rbx_engine* e, const char* path, int64_t timestep, int append);
 /* Last real-space (after mean removal for RBL) and k-space forces, [n][3] each,
  * in the atom order given to rbx_engine_set_state. */
 int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace);
@@ -390,6 +423,14 @@ typedef struct rbx_lammps_info {
 } rbx_lammps_info;
 rbx_lammps_data* rbx_lammps_read(const char* path, const char* atom_style, const int* replicate);
 void rbx_lammps_free(rbx_lammps_data* d);
+/* velocity_type GAUSS on a data set read by rbx_lammps_read
+ * (LammpsFullReader::ApplyGaussianVelocitiesIfRequested,
+ * lammps_full_reader.cpp:710-864): per atom a std::mt19937_64 seeded from
+ * (seed, file id), three std::normal_distribution<double> draws / sqrt(mass),
+ * centre-of-mass velocity removed, scaled to temperature with 3N - 3 degrees
+ * of freedom (kb, mvv2e of unit "LJ" / "REAL" / "METAL").  Needs Masses. */
+int rbx_lammps_gauss_velocities(rbx_lammps_data* h, double temperature, const char* unit,
+                                int seed);
 int rbx_lammps_get_info(const rbx_lammps_data* d, rbx_lammps_info* out);
 /* Per-atom arrays of n_atoms entries (image: [n][3]); any may be null. */
 int rbx_lammps_get_atoms(const rbx_lammps_data* d, int64_t* id, int* type, int* molecule,

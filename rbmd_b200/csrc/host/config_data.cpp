@@ -16,8 +16,21 @@ struct Parser {
     throw std::runtime_error(std::string("JSON parse error at offset ") + std::to_string(i) +
                              ": " + what);
   }
+  // Whitespace and comments: "// ..." to the end of the line, "/* ... */".
   void Ws() {
-    while (i < s.size() && (s[i] == ' ' || s[i] == '\t' || s[i] == '\n' || s[i] == '\r')) ++i;
+    for (;;) {
+      while (i < s.size() && (s[i] == ' ' || s[i] == '\t' || s[i] == '\n' || s[i] == '\r')) ++i;
+      if (i + 1 >= s.size() || s[i] != '/') return;
+      if (s[i + 1] == '/') {
+        while (i < s.size() && s[i] != '\n') ++i;
+      } else if (s[i + 1] == '*') {
+        const size_t end = s.find("*/", i + 2);
+        if (end == std::string::npos) Fail("unterminated comment");
+        i = end + 2;
+      } else {
+        return;
+      }
+    }
   }
   bool Eat(char c) {
     Ws();
@@ -124,6 +137,7 @@ struct Parser {
 
 JsonValue ParseJson(const std::string& text) {
   Parser p(text);
+  if (text.compare(0, 3, "\xEF\xBB\xBF") == 0) p.i = 3;  // UTF-8 byte-order mark
   JsonValue v = p.Value();
   p.Ws();
   if (p.i != text.size()) p.Fail("trailing characters");

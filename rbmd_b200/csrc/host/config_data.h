@@ -19,7 +19,10 @@ struct JsonValue {
   std::map<std::string, JsonValue> obj;
 };
 
-// Parses RFC 8259 JSON (no comments). Throws std::runtime_error on bad input.
+// Parses RFC 8259 JSON plus // and /* */ comments and a leading UTF-8
+// byte-order mark, as ConfigData::ParseJsonFile reads the reference's config
+// files (nlohmann::ordered_json::parse with ignore_comments, config_data.h:239-256).
+// Throws std::runtime_error on bad input.
 JsonValue ParseJson(const std::string& text);
 
 class ConfigData {

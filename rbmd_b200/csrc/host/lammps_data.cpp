@@ -8,7 +8,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <random>
 #include <unordered_map>
+
+#include "units.h"
 
 namespace rbx_host {
 namespace {
@@ -357,6 +360,65 @@ std::string LammpsData::replicate(int nx, int ny, int nz) {
   return "";
 }
 
+namespace {
+// Seed of one atom's generator: the seed and atom id combined and passed
+// through the SplitMix64 finaliser (MixVelocitySeed, lammps_full_reader.cpp:134-143).
+uint64_t velocity_seed(uint64_t seed, uint64_t atom_id) {
+  uint64_t v = seed + 0x9e3779b97f4a7c15ULL + (atom_id << 6) + (atom_id >> 2);
+  v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  v = (v ^ (v >> 27)) * 0x94d049bb133111ebULL;
+  return v ^ (v >> 31);
+}
+}  // namespace
+
+std::string LammpsData::gauss_velocities(double temperature, const std::string& unit, int seed) {
+  if (!std::isfinite(temperature) || temperature <= 0)
+    return "velocity_type GAUSS requires execution.temperature[0] > 0";
+  if (seed <= 0) return "velocity_type GAUSS requires a positive seed";
+  UnitFactors u;
+  try {
+    u = UnitsOf(unit);
+  } catch (const std::exception& ex) {
+    return ex.what();
+  }
+  const size_t n = id.size();
+  if (n == 0) return "";
+  std::vector<double> m(n);
+  for (size_t i = 0; i < n; ++i) {
+    const double mi = has_masses ? mass[type[i]] : 0.0;
+    if (!std::isfinite(mi) || mi <= 0)
+      return "velocity_type GAUSS requires positive mass for every atom type";
+    m[i] = mi;
+  }
+  double mtot = 0, p[3] = {0, 0, 0};
+  std::vector<double>* v[3] = {&vx, &vy, &vz};
+  for (size_t i = 0; i < n; ++i) {
+    std::mt19937_64 rng(velocity_seed((uint64_t)seed, (uint64_t)(id[i] + 1)));
+    std::normal_distribution<double> normal(0.0, 1.0);
+    const double f = 1.0 / std::sqrt(m[i]);
+    for (int d = 0; d < 3; ++d) {
+      (*v[d])[i] = normal(rng) * f;
+      p[d] += m[i] * (*v[d])[i];
+    }
+    mtot += m[i];
+  }
+  double twice_ke = 0;
+  for (size_t i = 0; i < n; ++i) {
+    for (int d = 0; d < 3; ++d) (*v[d])[i] -= p[d] / mtot;
+    twice_ke += m[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]);
+  }
+  twice_ke *= u.mvv2e;
+  if (!(twice_ke > 0) || !std::isfinite(twice_ke))
+    return "velocity_type GAUSS failed to create finite kinetic energy";
+  const long long dof = 3LL * (long long)n - 3;
+  if (dof <= 0) return "velocity_type GAUSS computed non-positive temperature DOF";
+  const double scale = std::sqrt(temperature * (double)dof * u.kb / twice_ke);
+  for (size_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) (*v[d])[i] *= scale;
+  has_velocities = true;
+  return "";
+}
+
 std::string write_lammps_charge(const std::string& path, const double lo[3], const double hi[3],
                                 int n, int ntypes, const double* mass, const double* eps,
                                 const double* sigma, const int64_t* id, const int* type,
@@ -421,6 +483,20 @@ rbx_lammps_data* rbx_lammps_read(const char* path, const char* atom_style,
 }
 
 void rbx_lammps_free(rbx_lammps_data* h) { delete h; }
+
+int rbx_lammps_gauss_velocities(rbx_lammps_data* h, double temperature, const char* unit,
+                                int seed) {
+  if (!h || !unit) {
+    rbx::set_error("rbx_lammps_gauss_velocities: null argument");
+    return RBX_ERR_INVALID;
+  }
+  const std::string err = h->d.gauss_velocities(temperature, unit, seed);
+  if (!err.empty()) {
+    rbx::set_error("%s", err.c_str());
+    return RBX_ERR_INVALID;
+  }
+  return RBX_OK;
+}
 
 int rbx_lammps_get_info(const rbx_lammps_data* h, rbx_lammps_info* out) {
   if (!h || !out) return RBX_ERR_INVALID;

@@ -38,6 +38,12 @@ struct LammpsData {
   // ids id + r (max id + 1) and molecules + r (max molecule + 1); positions are
   // unwrapped by their image flags, shifted and wrapped into the new box.
   std::string replicate(int nx, int ny, int nz);
+  // velocity_type GAUSS (LammpsFullReader::ApplyGaussianVelocitiesIfRequested,
+  // :710-864): per atom an std::mt19937_64 seeded by a SplitMix64-style mix of
+  // (seed, file id) draws three std::normal_distribution<double> values scaled
+  // by 1/sqrt(mass); the centre-of-mass velocity is removed and all velocities
+  // scaled to temperature with 3N - 3 degrees of freedom.  Needs Masses.
+  std::string gauss_velocities(double temperature, const std::string& unit, int seed);
 };
 
 // Writes an atom_style charge data file (Masses, Pair Coeffs, Atoms,

@@ -1,19 +1,15 @@
 // lj_cut_coul_kspace.cpp -- see lj_cut_coul_kspace.h.
 #include "lj_cut_coul_kspace.h"
+#include "units.h"
 
 #include <cmath>
 #include <stdexcept>
 
 namespace rbx_host {
 
-// UnitFactor<...>::_qqr2e (src/common/unit_factor.h): LJ 1, REAL 332.06371,
+// UnitFactor<...>::_qqr2e (src/common/unit_factor.cpp): LJ 1, REAL 332.06371,
 // METAL 14.399645.
-double QqrdFromUnit(const std::string& unit) {
-  if (unit == "LJ") return 1.0;
-  if (unit == "REAL") return 332.06371;
-  if (unit == "METAL") return 14.399645;
-  throw std::runtime_error("unsupported init_configuration.read_data.unit: " + unit);
-}
+double QqrdFromUnit(const std::string& unit) { return UnitsOf(unit).qqr2e; }
 
 // SetAlphaFromManual (kspace_calculator.cpp:105-118): JSON alpha is g_ewald^2.
 void KSpaceCalculator::SetAlphaFromManual(double alpha) {
@@ -142,10 +138,10 @@ void LJCutCoulKspace::Init() {
           : std::string("LJ/CUT/COUL/LONG");
   if (ff != "LJ/CUT/COUL/LONG")
     throw std::runtime_error("force_field.type " + ff + " is not LJ/CUT/COUL/LONG");
-  const double qqr2e = QqrdFromUnit(
-      _cfg.PathExists({"init_configuration", "read_data", "unit"})
-          ? _cfg.Get<std::string>("unit", "init_configuration", "read_data")
-          : std::string("LJ"));
+  const std::string unit = _cfg.PathExists({"init_configuration", "read_data", "unit"})
+                               ? _cfg.Get<std::string>("unit", "init_configuration", "read_data")
+                               : std::string("LJ");
+  const double qqr2e = QqrdFromUnit(unit);
   const double cut_off = _cfg.Get<double>("cut_off", "hyper_parameters", "neighbor");
   _neighbor_type = _cfg.Get<std::string>("type", "hyper_parameters", "neighbor");
   rbx_params p{};
@@ -184,6 +180,7 @@ void LJCutCoulKspace::Init() {
                       ? (uint64_t)_cfg.Get<long long>("random_seed", "hyper_parameters", "coulomb")
                       : 0x5EEDULL;
   p.qqr2e = qqr2e;
+  p.fmt2v = UnitsOf(unit).fmt2v;
   p.dt = _cfg.PathExists({"execution", "timestep"}) ? _cfg.Get<double>("timestep", "execution")
                                                      : 0.001;
   p.precision = _precision;

@@ -437,14 +437,23 @@ __global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double
                         const double* __restrict__ vy, const double* __restrict__ vz,
                         const double* __restrict__ x0, const double* __restrict__ y0,
                         const double* __restrict__ z0, unsigned long long* __restrict__ max_d2,
-                        uint4* __restrict__ atoms, const double* __restrict__ q) {
+                        uint4* __restrict__ atoms, const double* __restrict__ q,
+                        ImageRefs img) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0.0;
   if (i < n) {
     double p[3] = {x[i] + vx[i] * dt, y[i] + vy[i] * dt, z[i] + vz[i] * dt};
-    for (int d = 0; d < 3; ++d) {
-      if (p[d] >= b.lo[d] + b.len[d]) p[d] -= b.len[d];
-      if (p[d] < b.lo[d]) p[d] += b.len[d];
+    for (int d = 0; d < 3; ++d) {  // periodic wrap, counted in the image flags
+      int w = 0;
+      if (p[d] >= b.lo[d] + b.len[d]) {
+        p[d] -= b.len[d];
+        w = 1;
+      }
+      if (p[d] < b.lo[d]) {
+        p[d] += b.len[d];
+        w = -1;
+      }
+      if (w && img.c[d]) img.c[d][i] += w;
     }
     x[i] = p[0];
     y[i] = p[1];
@@ -639,6 +648,12 @@ int launch_scatter_f64(int n, const int* idx, const double* src, double* dst, cu
   count_launch();
   return check_launch("scatter_f64");
 }
+int launch_scatter_i32(int n, const int* idx, const int* src, int* dst, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_scatter<int><<<(n + 255) / 256, 256, 0, st>>>(n, idx, src, dst);
+  count_launch();
+  return check_launch("scatter_i32");
+}
 
 int launch_kick(int n, const double* fx, const double* fy, const double* fz, const int* type,
                 const double* inv_mass, double half_dt, double* vx, double* vy, double* vz,
@@ -652,10 +667,10 @@ int launch_kick(int n, const double* fx, const double* fy, const double* fz, con
 int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* z,
                  const double* vx, const double* vy, const double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
-                 uint4* atoms, const double* q, cudaStream_t st) {
+                 uint4* atoms, const double* q, ImageRefs img, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
   k_drift<<<(n + 255) / 256, 256, 0, st>>>(b, n, dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2_bits,
-                                           atoms, q);
+                                           atoms, q, img);
   count_launch();
   return check_launch("drift");
 }

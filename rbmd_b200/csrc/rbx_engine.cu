@@ -18,6 +18,7 @@
 #include <string>
 #include <unordered_map>
 #include <cmath>
+#include <charconv>
 #include <vector>
 
 #include "rbx.h"
@@ -132,6 +133,7 @@ int rbx_engine::init() {
   ETRY(alloc(&stage, 9 * N));  // host transfer staging (x,v in; x,v,f out)
   for (double*& p : shd) ETRY(alloc(&p, N));
   for (int*& p : shi) ETRY(alloc(&p, N));
+  for (int*& p : img) ETRY(alloc(&p, N));
   for (unsigned long long*& p : shu) ETRY(alloc(&p, N));
   for (double*& p : snapd) ETRY(alloc(&p, N));
   for (int*& p : snapi) ETRY(alloc(&p, N));
@@ -254,6 +256,11 @@ int rbx_engine::set_state(const int* hgid, const int* htype, const double* hq, c
   ETRY(cuda_ok(cudaMemsetAsync(fy, 0, sizeof(double) * N, st), "memset"));
   ETRY(cuda_ok(cudaMemsetAsync(fz, 0, sizeof(double) * N, st), "memset"));
   ETRY(launch_rbl_keys(n, gid, key_a, key_b, st));
+  for (int d = 0; d < 3; ++d)
+    ETRY(cuda_ok(cudaMemsetAsync(img[d], 0, sizeof(int) * N, st), "memset"));
+  h_gid.assign(hgid, hgid + n);
+  h_type.assign(htype, htype + n);
+  h_q.assign(hq, hq + n);
   ETRY(cuda_ok(cudaStreamSynchronize(st), "set_state sync"));
   have_cache = false;
   have_forces = false;
@@ -268,7 +275,7 @@ int rbx_engine::set_state(const int* hgid, const int* htype, const double* hq, c
 ArraySet rbx_engine::permute_set(bool to_shadow) const {
   ArraySet a{};
   double* const pd[13] = {x, y, z, vx, vy, vz, fx, fy, fz, q, fpx, fpy, fpz};
-  int* const pi[3] = {type, gid, orig};
+  int* const pi[6] = {type, gid, orig, img[0], img[1], img[2]};
   unsigned long long* const pu[2] = {key_a, key_b};
   for (int k = 0; k < 13; ++k) {
     a.src_f64[k] = to_shadow ? pd[k] : shd[k];
@@ -283,11 +290,11 @@ ArraySet rbx_engine::permute_set(bool to_shadow) const {
     }
     a.nf64 = 16;
   }
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < 6; ++k) {
     a.src_i32[k] = to_shadow ? pi[k] : shi[k];
     a.dst_i32[k] = to_shadow ? shi[k] : pi[k];
   }
-  a.ni32 = 3;
+  a.ni32 = 6;
   for (int k = 0; k < 2; ++k) {
     a.src_u64[k] = to_shadow ? pu[k] : shu[k];
     a.dst_u64[k] = to_shadow ? shu[k] : pu[k];
@@ -301,13 +308,13 @@ ArraySet rbx_engine::permute_set(bool to_shadow) const {
 ArraySet rbx_engine::state_set(bool save) const {
   ArraySet a{};
   double* const pd[10] = {x, y, z, vx, vy, vz, fx, fy, fz, q};
-  int* const pi[3] = {type, gid, orig};
+  int* const pi[6] = {type, gid, orig, img[0], img[1], img[2]};
   unsigned long long* const pu[2] = {key_a, key_b};
   for (int k = 0; k < 10; ++k) {
     a.src_f64[k] = save ? pd[k] : snapd[k];
     a.dst_f64[k] = save ? snapd[k] : pd[k];
   }
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < 6; ++k) {
     a.src_i32[k] = save ? pi[k] : snapi[k];
     a.dst_i32[k] = save ? snapi[k] : pi[k];
   }
@@ -316,7 +323,7 @@ ArraySet rbx_engine::state_set(bool save) const {
     a.dst_u64[k] = save ? snapu[k] : pu[k];
   }
   a.nf64 = 10;
-  a.ni32 = 3;
+  a.ni32 = 6;
   a.nu64 = 2;
   return a;
 }
@@ -510,7 +517,8 @@ int rbx_engine::step_plain(int nsteps) {
     }
     ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
     ETRY(cuda_ok(cudaMemsetAsync(max_d2, 0, sizeof(unsigned long long), st), "memset"));
-    ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q, st));
+    ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
+                     ImageRefs{{img[0], img[1], img[2]}}, st));
     if (e) cudaEventRecord(e[1], st);
     ++epoch;
     ETRY(check_rebuild(true));
@@ -562,7 +570,8 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
   const double thr = prm.skin * 0.5;
   ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
   ETRY(launch_zero_u64(max_d2, st));
-  ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q, st));
+  ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
+                     ImageRefs{{img[0], img[1], img[2]}}, st));
   ETRY(launch_step_decide(max_d2, thr * thr, dflags + 4, cond, st));
   // the conditional node after everything captured so far on st
   cudaStreamCaptureStatus cs;
@@ -909,12 +918,14 @@ int rbx_engine::force_vjp(const double* g, double* d_eps, double* d_sigma, doubl
 }
 
 // Per-type-pair LJ tables, eps_ij = sqrt(eps_i eps_j), sigma_ij^6 with
-// sigma_ij = (sigma_i + sigma_j)/2, and the inverse masses.
+// sigma_ij = (sigma_i + sigma_j)/2, and fmt2v / mass for the kick (the unit's
+// force-to-velocity factor folded in, as UpdateVelocityOp multiplies by it).
 int rbx_engine::upload_type_tables() {
   const int nt = prm.ntypes;
+  const double fmt2v = prm.fmt2v > 0 ? prm.fmt2v : 1.0;
   std::vector<double> he(nt * nt), hs(nt * nt), im(nt);
   for (int a = 0; a < nt; ++a) {
-    im[a] = 1.0 / mass[a];
+    im[a] = fmt2v == 1.0 ? 1.0 / mass[a] : fmt2v / mass[a];
     for (int b = 0; b < nt; ++b) {
       he[a * nt + b] = sqrt(eps[a] * eps[b]);
       hs[a * nt + b] = pow((sigma[a] + sigma[b]) / 2, 6.0);
@@ -977,6 +988,7 @@ int rbx_engine::set_charges(const double* hq) {
   }
   ETRY(cuda_ok(cudaMemcpyAsync(stage, hq, sizeof(double) * n, cudaMemcpyHostToDevice, st), "H2D"));
   ETRY(launch_gather_f64(n, orig, stage, q, st));
+  h_q.assign(hq, hq + n);
   ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
   ETRY(cuda_ok(cudaStreamSynchronize(st), "set_charges sync"));
   have_forces = false;
@@ -1001,6 +1013,107 @@ int rbx_engine::set_alpha(double a) {
   have_forces = false;
   graph_dirty = true;
   ++graph_version;
+  return RBX_OK;
+}
+
+// Periodic image counters, [n][3] in host order.
+int rbx_engine::set_images(const int* himg) {
+  cudaSetDevice(device);
+  const size_t N = (size_t)n;
+  std::vector<int> cols(3 * N);
+  for (size_t i = 0; i < N; ++i)
+    for (int d = 0; d < 3; ++d) cols[d * N + i] = himg[3 * i + d];
+  int* s32 = reinterpret_cast<int*>(stage);
+  ETRY(cuda_ok(cudaMemcpyAsync(s32, cols.data(), sizeof(int) * 3 * N, cudaMemcpyHostToDevice, st),
+               "H2D"));
+  for (int d = 0; d < 3; ++d) ETRY(launch_gather_i32(n, orig, s32 + d * N, img[d], st));
+  return cuda_ok(cudaStreamSynchronize(st), "set_images sync");
+}
+
+int rbx_engine::get_images(int* himg) {
+  cudaSetDevice(device);
+  const size_t N = (size_t)n;
+  std::vector<int> h(3 * N);
+  for (int d = 0; d < 3; ++d) {
+    ETRY(launch_scatter_i32(n, orig, img[d], reinterpret_cast<int*>(stage) + d * N, st));
+  }
+  ETRY(cuda_ok(cudaMemcpyAsync(h.data(), stage, sizeof(int) * 3 * N, cudaMemcpyDeviceToHost, st),
+               "D2H"));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "get_images sync"));
+  for (size_t i = 0; i < N; ++i)
+    for (int d = 0; d < 3; ++d) himg[3 * i + d] = h[d * N + i];
+  return RBX_OK;
+}
+
+namespace {
+// Shortest decimal that reads back as the same double (the "{}" format of the
+// reference's trajectory writer).
+void put_real(std::string& out, double v) {
+  char b[32];
+  const auto r = std::to_chars(b, b + sizeof b, v);
+  out.append(b, r.ptr);
+}
+}  // namespace
+
+// One frame in the reference's trajectory format (TrajectoryOutput::Execute,
+// src/output/src/TrajectoryOutput.cpp:467-500): LAMMPS custom dump with
+// id type q x y z xu yu zu vx vy vz, atoms by id, ids and types 1-based,
+// xu = x + image * L.
+int rbx_engine::write_trajectory(const char* path, int64_t timestep, bool append) {
+  cudaSetDevice(device);
+  const size_t N = (size_t)n;
+  std::vector<double> h(6 * N);
+  double* c[6];
+  for (int a = 0; a < 6; ++a) c[a] = h.data() + a * N;
+  ETRY(get_state(c[0], c[1], c[2], c[3], c[4], c[5], nullptr, nullptr, nullptr));
+  std::vector<int> im(3 * N);
+  ETRY(get_images(im.data()));
+  std::vector<size_t> order(N);
+  for (size_t i = 0; i < N; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return h_gid[a] < h_gid[b]; });
+  FILE* fp = fopen(path, append ? "a" : "w");
+  if (!fp) {
+    set_error("cannot write %s", path);
+    return RBX_ERR_INVALID;
+  }
+  std::string s;
+  s.reserve(N * 200 + 256);
+  s += "ITEM: TIMESTEP\n" + std::to_string(timestep) + "\nITEM: NUMBER OF ATOMS\n" +
+       std::to_string(n) + "\nITEM: BOX BOUNDS pp pp pp\n";
+  for (int d = 0; d < 3; ++d) {
+    put_real(s, box.lo[d]);
+    s += ' ';
+    put_real(s, box.hi[d]);
+    s += '\n';
+  }
+  s += "ITEM: ATOMS id type q x y z xu yu zu vx vy vz\n";
+  const double L[3] = {dbox.len[0], dbox.len[1], dbox.len[2]};
+  for (size_t k = 0; k < N; ++k) {
+    const size_t i = order[k];
+    s += std::to_string((long long)h_gid[i] + 1);
+    s += ' ';
+    s += std::to_string(h_type[i] + 1);
+    s += ' ';
+    put_real(s, h_q[i]);
+    for (int d = 0; d < 3; ++d) {
+      s += ' ';
+      put_real(s, c[d][i]);
+    }
+    for (int d = 0; d < 3; ++d) {
+      s += ' ';
+      put_real(s, c[d][i] + im[3 * i + d] * L[d]);
+    }
+    for (int d = 0; d < 3; ++d) {
+      s += ' ';
+      put_real(s, c[3 + d][i]);
+    }
+    s += '\n';
+  }
+  const bool ok = fwrite(s.data(), 1, s.size(), fp) == s.size();
+  if (fclose(fp) != 0 || !ok) {
+    set_error("write error on %s", path);
+    return RBX_ERR_INVALID;
+  }
   return RBX_OK;
 }
 
@@ -1148,6 +1261,49 @@ int rbx_engine_set_charges(rbx_engine* e, const double* charge) {
 int rbx_engine_set_alpha(rbx_engine* e, double alpha) {
   if (!e) return RBX_ERR_INVALID;
   return e->set_alpha(alpha);
+}
+
+int rbx_engine_get_system(rbx_engine* e, int* num_atoms, int* ntypes, rbx_box* box) {
+  if (!e) return RBX_ERR_INVALID;
+  if (num_atoms) *num_atoms = e->n;
+  if (ntypes) *ntypes = e->prm.ntypes;
+  if (box) *box = e->box;
+  return RBX_OK;
+}
+
+int rbx_engine_get_atoms(rbx_engine* e, int* gid, int* type, double* charge) {
+  if (!e) return RBX_ERR_INVALID;
+  if (e->h_gid.size() != (size_t)e->n) {
+    set_error("rbx_engine_get_atoms: no state set");
+    return RBX_ERR_INVALID;
+  }
+  if (gid) std::copy(e->h_gid.begin(), e->h_gid.end(), gid);
+  if (type) std::copy(e->h_type.begin(), e->h_type.end(), type);
+  if (charge) std::copy(e->h_q.begin(), e->h_q.end(), charge);
+  return RBX_OK;
+}
+
+int rbx_engine_get_type_params(rbx_engine* e, double* sigma, double* eps, double* mass) {
+  if (!e) return RBX_ERR_INVALID;
+  if (sigma) std::copy(e->sigma.begin(), e->sigma.end(), sigma);
+  if (eps) std::copy(e->eps.begin(), e->eps.end(), eps);
+  if (mass) std::copy(e->mass.begin(), e->mass.end(), mass);
+  return RBX_OK;
+}
+
+int rbx_engine_set_images(rbx_engine* e, const int* image) {
+  if (!e || !image) return RBX_ERR_INVALID;
+  return e->set_images(image);
+}
+
+int rbx_engine_get_images(rbx_engine* e, int* image) {
+  if (!e || !image) return RBX_ERR_INVALID;
+  return e->get_images(image);
+}
+
+int rbx_engine_write_trajectory(rbx_engine* e, const char* path, int64_t timestep, int append) {
+  if (!e || !path) return RBX_ERR_INVALID;
+  return e->write_trajectory(path, timestep, append != 0);
 }
 
 int rbx_engine_set_step_graph(rbx_engine* e, int on) {

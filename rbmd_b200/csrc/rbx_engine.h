@@ -33,6 +33,10 @@ struct rbx_engine {
   double *q = nullptr, *x0 = nullptr, *y0 = nullptr, *z0 = nullptr;
   int *type = nullptr, *gid = nullptr, *orig = nullptr;
   unsigned long long *key_a = nullptr, *key_b = nullptr;
+  int* img[3] = {};  // periodic image counters per atom (x, y, z)
+  // host-order copies of what set_state received (trajectory output)
+  std::vector<int> h_gid, h_type;
+  std::vector<double> h_q;
   uint4* atoms = nullptr;  // mixed form: {ux, uy, uz, q_f32}
   double* tmpd = nullptr;
   int* tmpi = nullptr;
@@ -73,12 +77,13 @@ struct rbx_engine {
   // arrays a rebuild permutes move through shadow copies and back, so every
   // device array keeps its address (a captured step graph stays valid)
   double* shd[13] = {};
-  int* shi[3] = {};
+  int* shi[6] = {};
   unsigned long long* shu[2] = {};
   // state saved before a run of graph steps (restored if a rebuild inside
-  // the graph ran out of capacity): x y z vx vy vz fx fy fz q, type gid orig, keys
+  // the graph ran out of capacity): x y z vx vy vz fx fy fz q, type gid orig,
+  // images, keys
   double* snapd[10] = {};
-  int* snapi[3] = {};
+  int* snapi[6] = {};
   unsigned long long* snapu[2] = {};
 
   // CUDA graph of one MD step, the rebuild under a conditional (IF) node
@@ -139,6 +144,9 @@ struct rbx_engine {
   int get_force_parts(double* f_pair, double* f_kspace);
   int get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs, int64_t* n_shell);
   int get_stats(rbx_stats* s);
+  int set_images(const int* image);
+  int get_images(int* image);
+  int write_trajectory(const char* path, int64_t timestep, bool append);
   int upload_type_tables();
   int build_sampler_tables();
   int set_lj_params(const double* sigma, const double* eps);

@@ -182,7 +182,7 @@ int launch_gather_vec3(int n, const int* orig, const double* src, double* x, dou
 
 // A set of per-atom arrays moved together: dst[a][i] = src[a][perm[i]].
 struct ArraySet {
-  static constexpr int kMaxF64 = 16, kMaxI32 = 4, kMaxU64 = 2;
+  static constexpr int kMaxF64 = 16, kMaxI32 = 8, kMaxU64 = 2;
   const double* src_f64[kMaxF64];
   double* dst_f64[kMaxF64];
   const int* src_i32[kMaxI32];
@@ -204,14 +204,19 @@ int launch_gather_i32(int n, const int* perm, const int* src, int* dst, cudaStre
 int launch_gather_u64(int n, const int* perm, const unsigned long long* src,
                       unsigned long long* dst, cudaStream_t st);
 int launch_scatter_f64(int n, const int* idx, const double* src, double* dst, cudaStream_t st);
+int launch_scatter_i32(int n, const int* idx, const int* src, int* dst, cudaStream_t st);
 int launch_kick(int n, const double* fx, const double* fy, const double* fz, const int* type,
                 const double* inv_mass, double half_dt, double* vx, double* vy, double* vz,
                 cudaStream_t st);
 // Drift + periodic wrap + max displacement since the last build (+ fixed point).
+// Per-atom periodic image counters (may be null: not tracked).
+struct ImageRefs {
+  int* c[3];
+};
 int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* z,
                  const double* vx, const double* vy, const double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
-                 uint4* atoms, const double* q, cudaStream_t st);
+                 uint4* atoms, const double* q, ImageRefs img, cudaStream_t st);
 int launch_to_fixed(const DBox& b, int n, const double* x, const double* y, const double* z,
                     const double* q, uint4* atoms, cudaStream_t st);
 int launch_max_disp(const DBox& b, int n, const double* x, const double* y, const double* z,

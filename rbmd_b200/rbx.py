@@ -62,6 +62,7 @@ class Params(C.Structure):
         ("sigma", C.POINTER(C.c_double)),
         ("eps", C.POINTER(C.c_double)),
         ("mass", C.POINTER(C.c_double)),
+        ("fmt2v", C.c_double),
     ]
 
 
@@ -95,7 +96,10 @@ EXPORTS = [
     "rbx_batch_stream", "rbx_engine_force_vjp", "rbx_engine_set_lj_params",
     "rbx_engine_set_charges", "rbx_engine_set_alpha", "rbx_lammps_read", "rbx_lammps_free",
     "rbx_lammps_get_info", "rbx_lammps_get_atoms", "rbx_lammps_get_types",
-    "rbx_lammps_get_topology", "rbx_lammps_write_charge",
+    "rbx_lammps_get_topology", "rbx_lammps_write_charge", "rbx_engine_set_images",
+    "rbx_engine_get_images", "rbx_engine_write_trajectory", "rbx_engine_create_from_files",
+    "rbx_engine_get_system", "rbx_engine_get_atoms", "rbx_engine_get_type_params",
+    "rbx_lammps_gauss_velocities",
 ]
 
 
@@ -163,6 +167,15 @@ def lib():
     L.rbx_engine_set_lj_params.argtypes = [vp, vp, vp]
     L.rbx_engine_set_charges.argtypes = [vp, vp]
     L.rbx_engine_set_alpha.argtypes = [vp, dp]
+    L.rbx_engine_set_images.argtypes = [vp, vp]
+    L.rbx_engine_get_images.argtypes = [vp, vp]
+    L.rbx_engine_write_trajectory.argtypes = [vp, C.c_char_p, C.c_int64, ip]
+    L.rbx_engine_create_from_files.restype = vp
+    L.rbx_engine_create_from_files.argtypes = [C.c_char_p, ip, ip]
+    L.rbx_engine_get_system.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), B]
+    L.rbx_engine_get_atoms.argtypes = [vp, vp, vp, vp]
+    L.rbx_engine_get_type_params.argtypes = [vp, vp, vp, vp]
+    L.rbx_lammps_gauss_velocities.argtypes = [vp, dp, C.c_char_p, ip]
     L.rbx_lammps_read.restype = vp
     L.rbx_lammps_read.argtypes = [C.c_char_p, C.c_char_p, vp]
     L.rbx_lammps_free.argtypes = [vp]
@@ -390,6 +403,43 @@ class Engine:
         check(L.rbx_engine_set_state(self._h, _np_ptr(gid), _np_ptr(typ), _np_ptr(q),
                                      *[_np_ptr(c) for c in cols]), "rbx_engine_set_state")
 
+    @classmethod
+    def from_files(cls, json_path, *, precision=PLAIN_FP64, device=0):
+        """rbx_engine_create_from_files: RBMD's JSON config and the LAMMPS data
+        file it names (replicate, GAUSS velocities, image flags), host order =
+        file order."""
+        L = lib()
+        h = L.rbx_engine_create_from_files(os.fsencode(json_path), precision, device)
+        if not h:
+            raise RbxError(f"rbx_engine_create_from_files failed: {last_error()}")
+        self = cls.__new__(cls)
+        self._h = C.c_void_p(h)
+        n, nt = C.c_int(0), C.c_int(0)
+        self.box = Box()
+        check(L.rbx_engine_get_system(self._h, C.byref(n), C.byref(nt), C.byref(self.box)),
+              "rbx_engine_get_system")
+        self.n = n.value
+        self._sigma, self._eps, self._mass = (np.zeros(nt.value) for _ in range(3))
+        check(L.rbx_engine_get_type_params(self._h, _np_ptr(self._sigma), _np_ptr(self._eps),
+                                           _np_ptr(self._mass)), "rbx_engine_get_type_params")
+        self._gid, self._typ = np.zeros(self.n, np.int32), np.zeros(self.n, np.int32)
+        self._q = np.zeros(self.n)
+        check(L.rbx_engine_get_atoms(self._h, _np_ptr(self._gid), _np_ptr(self._typ),
+                                     _np_ptr(self._q)), "rbx_engine_get_atoms")
+        return self
+
+    @property
+    def gid(self):
+        return self._gid
+
+    @property
+    def types(self):
+        return self._typ
+
+    @property
+    def charges(self):
+        return self._q
+
     def set_positions(self, pos, vel=None):
         """New positions (host order, [n, 3]); velocities kept unless given."""
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(self.n, 3)
@@ -465,6 +515,22 @@ class Engine:
     def set_alpha(self, alpha):
         check(lib().rbx_engine_set_alpha(self._h, float(alpha)), "rbx_engine_set_alpha")
 
+    def images(self):
+        """Periodic image counters [n, 3] (int32), host atom order."""
+        out = np.zeros((self.n, 3), np.int32)
+        check(lib().rbx_engine_get_images(self._h, _np_ptr(out)), "rbx_engine_get_images")
+        return out
+
+    def set_images(self, image):
+        image = np.ascontiguousarray(image, dtype=np.int32).reshape(self.n, 3)
+        check(lib().rbx_engine_set_images(self._h, _np_ptr(image)), "rbx_engine_set_images")
+
+    def write_trajectory(self, path, timestep, append=True):
+        """One frame of RBMD's rbmd.trj format (LAMMPS custom dump with xu yu zu)."""
+        check(lib().rbx_engine_write_trajectory(self._h, os.fsencode(path), int(timestep),
+                                                int(bool(append))),
+              "rbx_engine_write_trajectory")
+
     def force_vjp(self, g):
         """dL/d(eps, sigma per type; q per atom; alpha; positions) for g = dL/dF [n, 3]."""
         g = np.ascontiguousarray(g, dtype=np.float64).reshape(self.n, 3)
@@ -534,14 +600,18 @@ class Batch:
 # ---------------------------------------------------------------------------
 # LAMMPS data files
 # ---------------------------------------------------------------------------
-def read_lammps(path, atom_style=None, replicate=None) -> dict:
-    """rbx_lammps_read: the data file as 0-based arrays (file order)."""
+def read_lammps(path, atom_style=None, replicate=None, gauss=None) -> dict:
+    """rbx_lammps_read: the data file as 0-based arrays (file order).
+    gauss=(temperature, unit, seed) draws velocity_type GAUSS velocities."""
     L = lib()
     rep = (C.c_int * 3)(*replicate) if replicate is not None else None
     h = L.rbx_lammps_read(str(path).encode(), atom_style.encode() if atom_style else None, rep)
     if not h:
         raise RbxError(f"rbx_lammps_read failed: {last_error()}")
     try:
+        if gauss is not None:
+            check(L.rbx_lammps_gauss_velocities(h, float(gauss[0]), gauss[1].encode(),
+                                                int(gauss[2])), "rbx_lammps_gauss_velocities")
         info = LammpsInfo()
         check(L.rbx_lammps_get_info(h, C.byref(info)), "rbx_lammps_get_info")
         n, nt = info.n_atoms, info.n_atom_types

@@ -96,3 +96,65 @@ def test_json_config_errors(rbx, mutate, needle):
                                          s["q"].ctypes.data, 0, 0)
     assert not h
     assert needle in rbx.last_error()
+
+
+def test_json_comments_and_bom(rbx):
+    """Config files as RBMD ships them ('//' and block comments, a UTF-8
+    byte-order mark) parse; the first error is then the missing key."""
+    from rbmd_b200 import systems
+
+    text = "﻿// comment line\n" + JSON_OK.replace(
+        '"energy_rbl_flag": "no"', '/* block */ "x": 1 // line\n')
+    s = systems.lj_electrolyte(4000)
+    box = rbx.Box.make(s["lo"], s["hi"])
+    sig = np.ones(3)
+    h = rbx.lib().rbx_engine_create_json(text.encode(), C.byref(box), 4000, 3, sig.ctypes.data,
+                                         sig.ctypes.data, sig.ctypes.data, s["q"].ctypes.data,
+                                         0, 0)
+    assert not h
+    assert "energy_rbl_flag" in rbx.last_error()
+
+
+FILES_JSON = """{
+  "init_configuration": {"read_data": {"file": "sys.data", "unit": "LJ",
+      "atom_style": "charge", "velocity_type": "GAUSS", "replicate": [1, 1, 1]}},
+  "hyper_parameters": {
+    "force_field": {"type": "LJ/CUT/COUL/LONG"},
+    "neighbor": {"type": "RBL", "cut_off": 5, "r_core": 2.5, "skin": 0.3,
+                 "neighbor_sample_num": 100, "energy_rbl_flag": "no"},
+    "coulomb": {"type": "RBE", "coulomb_sample_num": 100, "alpha": 0.16,
+                "energy_rbe_flag": "no"}},
+  "execution": {"timestep": 0.005, "temperature": [1.0, 1.0, 1]}
+}"""
+
+
+@pytest.mark.parametrize("mutate, data, needle", [
+    (lambda s: s.replace('"sys.data"', '"missing.data"'), None, "missing.data"),
+    (lambda s: s.replace('"atom_style": "charge", ', ""), None, "atom_style"),
+    (lambda s: s.replace("[1, 1, 1]", "[1, 0, 1]"), None, "must be positive"),
+    (lambda s: s.replace("[1, 1, 1]", "[1, 1]"), None, "exactly 3 integers"),
+    (lambda s: s.replace('"GAUSS"', '"UNIFORM"'), "novel", "Unsupported velocity_type"),
+    (lambda s: s.replace("[1.0, 1.0, 1]", "[0.0, 1.0, 1]"), "novel",
+     "temperature[0] > 0"),
+    (lambda s: s, "nopair", "Pair Coeffs"),
+])
+def test_engine_from_files_errors(rbx, tmp_path, mutate, data, needle):
+    """rbx_engine_create_from_files reports config and data-file errors as the
+    reader does, before any device work."""
+    from rbmd_b200 import systems
+
+    s = systems.lj_electrolyte(2000, seed=1)
+    rbx.write_lammps_charge(tmp_path / "sys.data", s)
+    text = (tmp_path / "sys.data").read_text()
+    if data in ("novel", "nopair"):  # drop the Velocities (so GAUSS runs) or Pair Coeffs
+        head, _, _ = text.partition("\nVelocities")
+        text = head + "\n"
+        if data == "nopair":
+            a, _, rest = text.partition("\nPair Coeffs")
+            text = a + "\n" + rest[rest.index("\nAtoms"):]
+        (tmp_path / "sys.data").write_text(text)
+    cfg = tmp_path / "rbmd.json"
+    cfg.write_text(mutate(FILES_JSON))
+    h = rbx.lib().rbx_engine_create_from_files(str(cfg).encode(), 0, 0)
+    assert not h
+    assert needle in rbx.last_error(), rbx.last_error()

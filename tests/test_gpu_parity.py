@@ -626,3 +626,133 @@ def test_autograd_function_gradients(cuda, rbx):
     assert np.allclose(pos.grad.numpy(), direct["pos"], rtol=1e-12, atol=1e-15)
     assert np.isfinite(Q.grad.numpy()).all() and alpha.grad is not None
     e.close()
+
+
+def _read_frames(path):
+    """Parse frames of the rbmd.trj format written by rbx_engine_write_trajectory."""
+    lines = open(path).read().splitlines()
+    frames, i = [], 0
+    while i < len(lines):
+        assert lines[i] == "ITEM: TIMESTEP"
+        ts = int(lines[i + 1])
+        assert lines[i + 2] == "ITEM: NUMBER OF ATOMS"
+        n = int(lines[i + 3])
+        assert lines[i + 4] == "ITEM: BOX BOUNDS pp pp pp"
+        bounds = np.array([[float(v) for v in lines[i + 5 + d].split()] for d in range(3)])
+        assert lines[i + 8] == "ITEM: ATOMS id type q x y z xu yu zu vx vy vz"
+        rows = [r.split() for r in lines[i + 9:i + 9 + n]]
+        frames.append({"timestep": ts, "bounds": bounds,
+                       "id": np.array([int(r[0]) for r in rows]),
+                       "type": np.array([int(r[1]) for r in rows]),
+                       "data": np.array([[float(v) for v in r[2:]] for r in rows])})
+        i += 9 + n
+    return frames
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_trajectory_frames_and_images(cuda, rbx, tmp_path, graph):
+    """Image counters follow every wrap of the drift through rebuild
+    permutations (graph and launch-by-launch steps alike), and the trajectory
+    writer puts out RBMD's frame layout: ids and types 1-based in id order,
+    positions and velocities that read back as the engine's doubles, and
+    unwrapped xu = x + image * L that moves continuously across the faces."""
+    s = systems.lj_electrolyte(4000, seed=41)
+    perm = np.random.default_rng(2).permutation(s["n"])  # host order != id order
+    s2 = dict(s)
+    for key in ("pos", "vel", "type", "q", "gid"):
+        s2[key] = np.ascontiguousarray(s[key][perm])
+    e = rbx.Engine(s2, precision=rbx.MIXED, seed=5)
+    e.set_step_graph(graph)
+    e.compute_forces(0)
+    L = np.asarray(s["hi"]) - np.asarray(s["lo"])
+    path = tmp_path / "rbmd.trj"
+    e.write_trajectory(path, 0, append=False)
+    states, images = [e.get_state()], [e.images()]
+    for t in (1, 2):
+        e.step(60)
+        e.write_trajectory(path, 60 * t)
+        states.append(e.get_state())
+        images.append(e.images())
+    assert e.stats().rebuilds >= 2
+    assert not images[0].any() and np.abs(images[-1]).sum() > 50
+    frames = _read_frames(path)
+    assert [f["timestep"] for f in frames] == [0, 60, 120]
+    order = np.argsort(s2["gid"])
+    for f, st, im in zip(frames, states, images):
+        assert np.array_equal(f["bounds"], np.stack([s["lo"], s["hi"]], 1))
+        assert np.array_equal(f["id"], np.arange(1, s["n"] + 1))
+        assert np.array_equal(f["type"], s2["type"][order] + 1)
+        d = f["data"]
+        assert np.array_equal(d[:, 0], s2["q"][order])
+        assert np.array_equal(d[:, 1:4], st["pos"][order])
+        assert np.array_equal(d[:, 7:10], st["vel"][order])
+        assert np.array_equal(d[:, 4:7], st["pos"][order] + im[order] * L)
+    for a, b in zip(frames[:-1], frames[1:]):
+        jump = np.abs(b["data"][:, 4:7] - a["data"][:, 4:7]).max()
+        assert jump < 2.0  # unwrapped paths are continuous
+        assert np.abs(b["data"][:, 1:4] - a["data"][:, 1:4]).max() > 0.5 * L.min()  # wraps happened
+    e.close()
+
+
+FILES_JSON = """{
+  "init_configuration": {"read_data": {"file": "sys.data", "unit": "LJ",
+      "atom_style": "charge", "velocity_type": "GAUSS", "velocity_seed": 77, "replicate": REP}},
+  // RBMD's config files carry comments
+  "hyper_parameters": {
+    "force_field": {"type": "LJ/CUT/COUL/LONG"},
+    "neighbor": {"type": "RBL", "cut_off": 5.0, "r_core": 2.5, "skin": 0.3,
+                 "neighbor_sample_num": 100, "energy_rbl_flag": "no"},
+    "coulomb": {"type": "RBE", "coulomb_sample_num": 100, "alpha": 0.16,
+                "energy_rbe_flag": "no", "random_seed": 9}},
+  "execution": {"timestep": 0.005, "temperature": [1.2, 1.2, 1]}
+}"""
+
+
+@pytest.mark.parametrize("rep, velocities", [((1, 1, 1), True), ((2, 1, 1), False)])
+def test_engine_from_files_matches_arrays(cuda, rbx, tmp_path, rep, velocities):
+    """rbx_engine_create_from_files on a data file + JSON config equals the
+    engine built from the same arrays (rbx_engine_create_json): forces and a
+    40-step trajectory bit for bit.  Atoms written outside the box come in
+    wrapped, with the wrap in their image flags; without a Velocities section
+    the GAUSS velocities are those of the reader."""
+    s = systems.lj_electrolyte(4000, seed=23)
+    L = np.asarray(s["hi"]) - np.asarray(s["lo"])
+    moved = np.arange(0, s["n"], 397) if rep == (1, 1, 1) else np.arange(0)
+    out_of_box = dict(s, pos=s["pos"].copy())
+    out_of_box["pos"][moved, 0] += L[0]  # one box length out
+    data = tmp_path / "sys.data"
+    rbx.write_lammps_charge(data, out_of_box)
+    if not velocities:
+        data.write_text(data.read_text().partition("\nVelocities")[0] + "\n")
+    cfg = tmp_path / "rbmd.json"
+    text = FILES_JSON.replace("REP", str(list(rep)))
+    cfg.write_text(text)
+    a = rbx.Engine.from_files(cfg, precision=rbx.MIXED)
+    ref = rbx.read_lammps(data, replicate=rep, gauss=None if velocities else (1.2, "LJ", 77))
+    assert a.n == ref["n"] == s["n"] * np.prod(rep)
+    assert np.array_equal(a.gid, ref["id"]) and np.array_equal(a.types, ref["type"])
+    im = a.images()
+    pos = ref["pos"].copy()
+    Lr = np.asarray(ref["hi"]) - np.asarray(ref["lo"])
+    if rep == (1, 1, 1):
+        assert np.array_equal(np.nonzero(im[:, 0])[0], moved) and (im[moved, 0] == 1).all()
+        pos[moved, 0] -= L[0]
+    else:
+        assert np.array_equal(im, ref["image"])
+    sysd = {"n": ref["n"], "lo": ref["lo"], "hi": ref["hi"], "sigma": ref["sigma"],
+            "eps": ref["eps"], "mass": ref["mass"], "q": ref["q"], "pos": pos, "vel": ref["vel"],
+            "gid": ref["id"].astype(np.int32), "type": ref["type"]}
+    b = rbx.Engine(sysd, precision=rbx.MIXED, json_text=text.replace("// RBMD's config files "
+                                                                      "carry comments", ""))
+    b.set_images(im)
+    sa, sb = a.get_state(), b.get_state()
+    assert np.array_equal(sa["pos"], sb["pos"]) and np.array_equal(sa["vel"], sb["vel"])
+    for e in (a, b):
+        e.compute_forces(0)
+        e.step(40)
+    sa, sb = a.get_state(), b.get_state()
+    for key in ("pos", "vel", "force"):
+        assert np.array_equal(sa[key], sb[key]), key
+    assert np.abs(sa["pos"] + a.images() * Lr - (sb["pos"] + b.images() * Lr)).max() == 0
+    a.close()
+    b.close()

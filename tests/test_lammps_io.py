@@ -141,3 +141,127 @@ def test_reader_errors(rbx, tmp_path, text, needle):
     path.write_text(text)
     with pytest.raises(rbx.RbxError, match=needle):
         rbx.read_lammps(path)
+
+
+class _MT19937_64:
+    """std::mt19937_64 as the C++ standard defines it ([rand.predef]: w=64,
+    n=312, m=156, r=31, a=0xB5026F5AA96619E9, tempering u=29 d=0x5555...,
+    s=17 b=0x71D67FFFEDA60000, t=37 c=0xFFF7EEE000000000, l=43,
+    f=6364136223846793005)."""
+    M = (1 << 64) - 1
+
+    def __init__(self, seed):
+        mt = [seed & self.M]
+        for i in range(1, 312):
+            mt.append((6364136223846793005 * (mt[-1] ^ (mt[-1] >> 62)) + i) & self.M)
+        self.mt, self.i = mt, 312
+
+    def __call__(self):
+        mt = self.mt
+        if self.i >= 312:
+            for k in range(312):
+                x = (mt[k] & ~0x7FFFFFFF & self.M) | (mt[(k + 1) % 312] & 0x7FFFFFFF)
+                mt[k] = mt[(k + 156) % 312] ^ (x >> 1) ^ (0xB5026F5AA96619E9 if x & 1 else 0)
+            self.i = 0
+        x = mt[self.i]
+        self.i += 1
+        x ^= (x >> 29) & 0x5555555555555555
+        x ^= (x << 17) & 0x71D67FFFEDA60000
+        x ^= (x << 37) & 0xFFF7EEE000000000
+        x &= self.M
+        return x ^ (x >> 43)
+
+
+def _normal_triplet(seed):
+    """Three std::normal_distribution<double>(0, 1) draws from one fresh
+    distribution on std::mt19937_64(seed): libstdc++'s Marsaglia polar method
+    (two values per accepted pair, the second kept for the next call) over
+    generate_canonical<double, 53>, i.e. double(g()) / 2^64."""
+    import math
+
+    g = _MT19937_64(seed)
+
+    def uniform():
+        u = float(g()) / 2.0 ** 64
+        return u if u < 1.0 else math.nextafter(1.0, 0.0)
+
+    out, saved = [], None
+    while len(out) < 3:
+        if saved is not None:
+            out.append(saved)
+            saved = None
+            continue
+        while True:
+            x = 2.0 * uniform() - 1.0
+            y = 2.0 * uniform() - 1.0
+            r2 = x * x + y * y
+            if not (r2 > 1.0 or r2 == 0.0):
+                break
+        mult = math.sqrt(-2 * math.log(r2) / r2)
+        saved = x * mult
+        out.append(y * mult)
+    return out
+
+
+def _gauss_reference(ids, types, mass, temperature, kb, mvv2e, seed):
+    """velocity_type GAUSS restated (LammpsFullReader::ApplyGaussianVelocitiesIfRequested,
+    lammps_full_reader.cpp:710-864 with MixVelocitySeed :134-143)."""
+    M = (1 << 64) - 1
+    v = np.zeros((len(ids), 3))
+    m = np.asarray(mass, float)[types]
+    for i, a in enumerate(ids):
+        aid = int(a) + 1
+        z = (seed + 0x9E3779B97F4A7C15 + (aid << 6) + (aid >> 2)) & M
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        z ^= z >> 31
+        f = 1.0 / np.sqrt(m[i])
+        v[i] = [r * f for r in _normal_triplet(z)]
+    p = [0.0, 0.0, 0.0]
+    mt = 0.0
+    for i in range(len(ids)):  # sequential sums in atom order, as the reader
+        for d in range(3):
+            p[d] += m[i] * v[i, d]
+        mt += m[i]
+    ke = 0.0
+    for i in range(len(ids)):
+        for d in range(3):
+            v[i, d] -= p[d] / mt
+        ke += m[i] * (v[i, 0] * v[i, 0] + v[i, 1] * v[i, 1] + v[i, 2] * v[i, 2])
+    ke *= mvv2e
+    scale = np.sqrt(temperature * (3 * len(ids) - 3) * kb / ke)
+    return v * scale
+
+
+@pytest.mark.parametrize("unit, kb, mvv2e", [
+    ("LJ", 1.0, 1.0),
+    ("REAL", 1.9872067 * 10.0 ** -3.0, 1.0 / (4.186 * 10.0 ** -4.0)),
+])
+def test_gauss_velocities_match_restatement(rbx, tmp_path, unit, kb, mvv2e):
+    """GAUSS velocities equal a from-the-standard restatement of the
+    reader's generator bit for bit; total momentum ~0 and the kinetic
+    temperature is the target."""
+    s = systems.lj_electrolyte(2000, seed=8)
+    path = tmp_path / "sys.data"
+    rbx.write_lammps_charge(path, s)
+    T, seed = (1.5, 4242) if unit == "LJ" else (298.0, 12345)
+    got = rbx.read_lammps(path, replicate=(1, 1, 2), gauss=(T, unit, seed))
+    want = _gauss_reference(got["id"], got["type"], got["mass"], T, kb, mvv2e, seed)
+    assert np.array_equal(got["vel"], want)
+    m = got["mass"][got["type"]]
+    assert np.abs((m[:, None] * got["vel"]).sum(0)).max() < 1e-10 * m.sum()
+    temp = mvv2e * (m[:, None] * got["vel"] ** 2).sum() / ((3 * got["n"] - 3) * kb)
+    assert abs(temp - T) < 1e-12 * T
+
+
+@pytest.mark.parametrize("args, needle", [
+    ((0.0, "LJ", 1), "temperature[0] > 0"),
+    ((1.0, "LJ", 0), "positive seed"),
+    ((1.0, "SI", 1), "unsupported"),
+])
+def test_gauss_velocities_errors(rbx, tmp_path, args, needle):
+    s = systems.lj_electrolyte(2000, seed=8)
+    path = tmp_path / "sys.data"
+    rbx.write_lammps_charge(path, s)
+    with pytest.raises(rbx.RbxError, match=needle.replace("[", r"\[").replace("]", r"\]")):
+        rbx.read_lammps(path, gauss=args)
