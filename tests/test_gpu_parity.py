@@ -680,7 +680,7 @@ def test_trajectory_frames_and_images(cuda, rbx, tmp_path, graph):
     order = np.argsort(s2["gid"])
     for f, st, im in zip(frames, states, images):
         assert np.array_equal(f["bounds"], np.stack([s["lo"], s["hi"]], 1))
-        assert np.array_equal(f["id"], np.arange(1, s["n"] + 1))
+        assert np.array_equal(f["id"], np.sort(s2["gid"]) + 1)  # internal ids + 1
         assert np.array_equal(f["type"], s2["type"][order] + 1)
         d = f["data"]
         assert np.array_equal(d[:, 0], s2["q"][order])
