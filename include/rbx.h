@@ -343,6 +343,21 @@ int rbx_engine_step_host(rbx_engine* e, const double* x_in, const double* v_in,
 int rbx_engine_get_state(rbx_engine* e, double* px, double* py, double* pz,
                          double* vx, double* vy, double* vz, double* fx,
                          double* fy, double* fz);
+/* NVT: Nose-Hoover chain thermostat of RBMD's NVT ensemble with
+ * temp_ctrl_type NOSE_HOOVER (NVTensemble::Solve, nvt_ensemble.cpp:128-160;
+ * NoseHooverController, nose_hoover_controller.cpp): chain length 3, one
+ * sub-cycle, temperature ramped t_start -> t_stop over num_steps, damping
+ * t_damp (execution.temperature = [t_start, t_stop, t_damp]); kb and mvv2e of
+ * the unit style; tdof <= 0 means 3N - 3.  Each step scales the velocities
+ * before the first half kick and after the second, as InitialIntegrate /
+ * FinalIntegrate do, all on the device (inside the step graph).  Call after
+ * rbx_engine_set_state: the chain starts from the current temperature.
+ * t_damp <= 0 switches the thermostat off (NVE). */
+int rbx_engine_set_nose_hoover(rbx_engine* e, double t_start, double t_stop, double t_damp,
+                               int64_t num_steps, double kb, double mvv2e, double tdof);
+/* Current thermostat state: temperature (after the last step's scaling),
+ * eta[3], eta_dot[3]; any pointer may be NULL. */
+int rbx_engine_get_thermostat(rbx_engine* e, double* temperature, double* eta, double* eta_dot);
 /* Periodic image counters, [n][3] ints in the atom order given to
  * rbx_engine_set_state: how many times each atom has wrapped through each face
  * (+1 leaving through hi).  rbx_engine_set_state zeroes them; the drift of

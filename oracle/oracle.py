@@ -108,6 +108,10 @@ def lib():
             "orc_engine_get": (C.c_int, [C.c_void_p, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                          _dp, _dp]),
             "orc_engine_rebuilds": (C.c_int, [C.c_void_p]),
+            "orc_engine_set_nose_hoover": (C.c_int, [C.c_void_p, C.c_double, C.c_double,
+                                                     C.c_double, C.c_longlong, C.c_double,
+                                                     C.c_double, C.c_double]),
+            "orc_engine_get_thermostat": (None, [C.c_void_p, _dp, _dp, _dp]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -353,6 +357,17 @@ class Engine:
     @property
     def rebuilds(self):
         return lib().orc_engine_rebuilds(self._h)
+
+    def set_nose_hoover(self, t_start, t_stop, t_damp, num_steps=0, kb=1.0, mvv2e=1.0, tdof=0.0):
+        """NVT Nose-Hoover chain (NVTensemble::Solve with NOSE_HOOVER)."""
+        lib().orc_engine_set_nose_hoover(self._h, t_start, t_stop, t_damp, num_steps, kb, mvv2e,
+                                         tdof)
+
+    def thermostat(self):
+        t = np.zeros(1)
+        eta, eta_dot = np.zeros(3), np.zeros(3)
+        lib().orc_engine_get_thermostat(self._h, t, eta, eta_dot)
+        return {"temperature": t[0], "eta": eta, "eta_dot": eta_dot}
 
     def __del__(self):
         try:

@@ -859,6 +859,11 @@ struct orc_engine {
   double *q, *x, *y, *z, *vx, *vy, *vz, *fx, *fy, *fz, *x0, *y0, *z0, *tmp;
   double *kfx, *kfy, *kfz, *mx, *my, *mz, *re, *im;
   int ncell;
+  /* Nose-Hoover chain (NVT) */
+  int nh_on;
+  long long nh_num_steps;
+  double nh_t_start, nh_t_stop, nh_t_freq, nh_kb, nh_mvv2e, nh_tdof;
+  double eta[3], eta_dot[4], eta_dotdot[3], eta_mass[3], temperature, t_target, ke_target;
 };
 
 orc_engine* orc_engine_create(int n, const orc_box* box, int ntypes,
@@ -1049,16 +1054,123 @@ static void engine_drift(orc_engine* e) {
   }
 }
 
+/* ---- Nose-Hoover chain thermostat -------------------------------------- */
+/* NoseHooverController (src/simulate_pipeline/src/controller/pressure_controller/
+ * nose_hoover_controller.cpp): chain of 3, one sub-cycle, no drag.
+ * Temperature: ComputeTemperature (update_temperature_op.hip.cu:7-29) and
+ * SampleCurrentTemperatureState (:256-287), summed here in atom order. */
+static double nh_temperature(const orc_engine* e) {
+  double s = 0;
+  for (int i = 0; i < e->n; ++i)
+    s += e->nh_mvv2e * e->mass[e->type[i]] *
+         (e->vx[i] * e->vx[i] + e->vy[i] * e->vy[i] + e->vz[i] * e->vz[i]);
+  return 0.5 * s / (e->nh_tdof * e->nh_kb / 2.0);
+}
+
+/* ComputeTempTarget (:473-497). */
+static void nh_temp_target(orc_engine* e, long long step) {
+  double t = e->nh_t_start;
+  if (e->nh_t_stop != e->nh_t_start) {
+    double delta = (double)step;
+    if (delta != 0.0) delta = delta / (double)e->nh_num_steps;
+    t = e->nh_t_start + delta * (e->nh_t_stop - e->nh_t_start);
+  }
+  e->t_target = t;
+  e->ke_target = e->nh_tdof * e->nh_kb * t;
+}
+
+/* NHCTempIntegrate (:732-840) with the velocity rescale it contains. */
+static void nh_chain(orc_engine* e) {
+  const double dt8 = 0.125 * e->dt, dt4 = 0.25 * e->dt, dthalf = 0.5 * e->dt;
+  const double tf2 = e->nh_t_freq * e->nh_t_freq;
+  double ke = e->nh_tdof * e->nh_kb * e->temperature;
+  e->eta_mass[0] = e->nh_tdof * e->nh_kb * e->t_target / tf2;
+  for (int c = 1; c < 3; ++c) e->eta_mass[c] = e->nh_kb * e->t_target / tf2;
+  e->eta_dotdot[0] = e->eta_mass[0] > 0.0 ? (ke - e->ke_target) / e->eta_mass[0] : 0.0;
+  for (int c = 2; c > 0; --c) {
+    const double x = exp(-dt8 * e->eta_dot[c + 1]);
+    e->eta_dot[c] = (e->eta_dot[c] * x + e->eta_dotdot[c] * dt4) * x;
+  }
+  const double x1 = exp(-dt8 * e->eta_dot[1]);
+  e->eta_dot[0] = (e->eta_dot[0] * x1 + e->eta_dotdot[0] * dt4) * x1;
+  const double f = exp(-dthalf * e->eta_dot[0]);
+  for (int i = 0; i < e->n; ++i) {
+    e->vx[i] *= f;
+    e->vy[i] *= f;
+    e->vz[i] *= f;
+  }
+  e->temperature = e->temperature * f * f;
+  ke = e->nh_tdof * e->nh_kb * e->temperature;
+  e->eta_dotdot[0] = e->eta_mass[0] > 0.0 ? (ke - e->ke_target) / e->eta_mass[0] : 0.0;
+  for (int c = 0; c < 3; ++c) e->eta[c] += dthalf * e->eta_dot[c];
+  e->eta_dot[0] = (e->eta_dot[0] * x1 + e->eta_dotdot[0] * dt4) * x1;
+  for (int c = 1; c < 3; ++c) {
+    const double x = exp(-dt8 * e->eta_dot[c + 1]);
+    e->eta_dot[c] *= x;
+    e->eta_dotdot[c] = (e->eta_mass[c - 1] * e->eta_dot[c - 1] * e->eta_dot[c - 1] -
+                        e->nh_kb * e->t_target) / e->eta_mass[c];
+    e->eta_dot[c] = (e->eta_dot[c] + e->eta_dotdot[c] * dt4) * x;
+  }
+}
+
+/* Init + SetUp (:89-250, :415-471); t_damp <= 0 switches it off. */
+int orc_engine_set_nose_hoover(orc_engine* e, double t_start, double t_stop, double t_damp,
+                               long long num_steps, double kb, double mvv2e, double tdof) {
+  if (!(t_damp > 0)) {
+    e->nh_on = 0;
+    return 0;
+  }
+  e->nh_on = 1;
+  e->nh_t_start = t_start;
+  e->nh_t_stop = t_stop;
+  e->nh_t_freq = 1.0 / t_damp;
+  e->nh_num_steps = num_steps;
+  e->nh_kb = kb;
+  e->nh_mvv2e = mvv2e;
+  e->nh_tdof = tdof > 0 ? tdof : 3.0 * e->n - 3.0;
+  for (int c = 0; c < 3; ++c) e->eta[c] = e->eta_dot[c] = e->eta_dotdot[c] = 0.0;
+  e->eta_dot[3] = 0.0;
+  e->temperature = nh_temperature(e);
+  nh_temp_target(e, 0);
+  const double tf2 = e->nh_t_freq * e->nh_t_freq;
+  e->eta_mass[0] = e->nh_tdof * kb * e->t_target / tf2;
+  for (int c = 1; c < 3; ++c) e->eta_mass[c] = kb * e->t_target / tf2;
+  for (int c = 1; c < 3; ++c)
+    e->eta_dotdot[c] = (e->eta_mass[c - 1] * e->eta_dot[c - 1] * e->eta_dot[c - 1] -
+                        kb * e->t_target) / e->eta_mass[c];
+  return 0;
+}
+
+void orc_engine_get_thermostat(const orc_engine* e, double* temperature, double* eta,
+                               double* eta_dot) {
+  if (temperature) *temperature = e->temperature;
+  for (int c = 0; c < 3; ++c) {
+    if (eta) eta[c] = e->eta[c];
+    if (eta_dot) eta_dot[c] = e->eta_dot[c];
+  }
+}
+
+/* NVEensemble::Solve, or NVTensemble::Solve with NOSE_HOOVER (nvt_ensemble.cpp:128-160):
+ * InitialIntegrate = target + chain + kick + drift; force; FinalIntegrate =
+ * kick + temperature + chain. */
 int orc_engine_step(orc_engine* e, int nsteps) {
   if (!e->have_cache) {
     if (orc_engine_compute_forces(e, e->epoch) != 0) return -1;
   }
   for (int s = 0; s < nsteps; ++s) {
+    if (e->nh_on) {
+      nh_temp_target(e, (long long)e->epoch + 1);
+      nh_chain(e);
+    }
     engine_kick(e);
     engine_drift(e);
     e->epoch++;
     if (orc_engine_compute_forces(e, e->epoch) != 0) return -1;
     engine_kick(e);
+    if (e->nh_on) {
+      e->temperature = nh_temperature(e);
+      nh_chain(e);
+    }
   }
   return 0;
 }

@@ -15,6 +15,7 @@
 #include "lammps_data.h"
 #include "lj_cut_coul_kspace.h"
 #include "rbx.h"
+#include "units.h"
 
 namespace rbx {
 void set_error(const char* fmt, ...);
@@ -142,13 +143,41 @@ rbx_engine* create_from_files(const std::string& json_path, int precision, int d
   for (auto& v : vel)
     if (v.size() != (size_t)n) v.assign(n, 0.0);
 
+  // execution.ensemble: NVE, or NVT with the Nose-Hoover chain
+  // (NVTensemble, nvt_ensemble.cpp; NoseHooverController::Init reads
+  // execution.temperature = [start, stop, damp] and num_steps for a ramp).
+  const std::string ensemble = cfg.PathExists({"execution", "ensemble"})
+                                   ? upper(cfg.Get<std::string>("ensemble", "execution"))
+                                   : std::string("NVE");
+  std::vector<double> nh;
+  long long num_steps = 0;
+  if (ensemble == "NVT") {
+    const std::string tc = cfg.PathExists({"execution", "temp_ctrl_type"})
+                               ? upper(cfg.Get<std::string>("temp_ctrl_type", "execution"))
+                               : std::string("NOSE_HOOVER");
+    if (tc != "NOSE_HOOVER")
+      throw std::runtime_error("execution.temp_ctrl_type " + tc +
+                               " is not provided by this engine (NOSE_HOOVER)");
+    nh = cfg.GetArray<double>("temperature", "execution");
+    if (nh.size() < 3)
+      throw std::runtime_error("execution.temperature must be [t_start, t_stop, t_damp]");
+    if (cfg.PathExists({"execution", "num_steps"}))
+      num_steps = cfg.Get<long long>("num_steps", "execution");
+  } else if (ensemble != "NVE") {
+    throw std::runtime_error("execution.ensemble " + ensemble +
+                             " is not provided by this engine (NVE, NVT)");
+  }
+
   LJCutCoulKspace plugin(text, box, n, nt, d.pair_sigma.data(), d.pair_eps.data(), d.mass.data(),
                          q.data(), precision, device);
   plugin.Init();
   rbx_engine* e = plugin.Release();
+  const UnitFactors u = UnitsOf(unit);
   if (rbx_engine_set_state(e, gid.data(), type.data(), q.data(), pos[0].data(), pos[1].data(),
                            pos[2].data(), vel[0].data(), vel[1].data(), vel[2].data()) != RBX_OK ||
-      rbx_engine_set_images(e, image.data()) != RBX_OK) {
+      rbx_engine_set_images(e, image.data()) != RBX_OK ||
+      (!nh.empty() && rbx_engine_set_nose_hoover(e, nh[0], nh[1], nh[2], num_steps, u.kb,
+                                                 u.mvv2e, 0.0) != RBX_OK)) {
     const std::string msg = rbx_last_error();
     rbx_engine_destroy(e);
     throw std::runtime_error(msg);

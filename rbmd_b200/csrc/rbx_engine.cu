@@ -158,6 +158,11 @@ int rbx_engine::init() {
   ETRY(alloc(&ek, 1));
   ETRY(alloc(&virk, 6));
   ETRY(alloc(&inv_mass, (size_t)prm.ntypes));
+  ETRY(alloc(&mass_d, (size_t)prm.ntypes));
+  ETRY(alloc(&nh_state, (size_t)NH_SLOTS));
+  ETRY(alloc(&nh_snap, (size_t)NH_SLOTS));
+  ETRY(alloc(&ke_part, (size_t)KE_PARTS));
+  ETRY(cuda_ok(cudaMemsetAsync(nh_state, 0, sizeof(double) * NH_SLOTS, st), "memset"));
   ETRY(alloc(&lj_eps, (size_t)prm.ntypes * prm.ntypes));
   ETRY(alloc(&lj_s6, (size_t)prm.ntypes * prm.ntypes));
   // LJ mixing of ComputeLJCutCoulRBLForce (lj_cut_coul_kspace_op.hip.cu:582-600):
@@ -515,6 +520,7 @@ int rbx_engine::step_plain(int nsteps) {
       pev_used += 5;
       cudaEventRecord(e[0], st);
     }
+    if (nh_on) ETRY(nh_initial(nullptr, epoch + 1, st));
     ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
     ETRY(cuda_ok(cudaMemsetAsync(max_d2, 0, sizeof(unsigned long long), st), "memset"));
     ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
@@ -526,6 +532,7 @@ int rbx_engine::step_plain(int nsteps) {
     ETRY(real_space());
     if (e) cudaEventRecord(e[3], st);
     ETRY(kspace_and_combine(true));
+    if (nh_on) ETRY(nh_final(st));
     if (e) cudaEventRecord(e[4], st);
     ++steps;
     ++force_calls;
@@ -568,6 +575,7 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
                "cudaGraphConditionalHandleCreate"));
   const unsigned long long l0 = rbx_launch_count();
   const double thr = prm.skin * 0.5;
+  if (nh_on) ETRY(nh_initial(dflags + 4, 1, st));  // the device epoch is still the last step's
   ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
   ETRY(launch_zero_u64(max_d2, st));
   ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
@@ -602,6 +610,7 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
   graph_rebuild_launches = rbx_launch_count() - b0;
   ETRY(real_space(dflags + 4));
   ETRY(kspace_and_combine(true, dflags + 4));
+  if (nh_on) ETRY(nh_final(st));
   graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
   return RBX_OK;
 }
@@ -610,6 +619,10 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
 // in-graph rebuild counter (all on stream s).
 int rbx_engine::graph_run_begin(cudaStream_t s) {
   ETRY(launch_move_set(n, nullptr, state_set(true), s));
+  if (nh_on)
+    ETRY(cuda_ok(cudaMemcpyAsync(nh_snap, nh_state, sizeof(double) * NH_SLOTS,
+                                 cudaMemcpyDeviceToDevice, s),
+                 "D2D"));
   run_init[0] = epoch;  // [4] epoch, [5] rebuilds inside the graph
   run_init[1] = 0;
   return cuda_ok(cudaMemcpyAsync(dflags + 4, run_init, sizeof(int) * 2, cudaMemcpyHostToDevice, s),
@@ -623,6 +636,10 @@ int rbx_engine::graph_run_end(int nsteps) {
   const int* h = run_flags;
   if (h[0] || (h[1] & 1)) {
     ETRY(launch_move_set(n, nullptr, state_set(false), st));
+    if (nh_on)
+      ETRY(cuda_ok(cudaMemcpyAsync(nh_state, nh_snap, sizeof(double) * NH_SLOTS,
+                                   cudaMemcpyDeviceToDevice, st),
+                   "D2D"));
     have_cache = false;
     return step_plain(nsteps);
   }
@@ -933,6 +950,8 @@ int rbx_engine::upload_type_tables() {
   }
   ETRY(cuda_ok(cudaMemcpy(inv_mass, im.data(), sizeof(double) * nt, cudaMemcpyHostToDevice),
                "H2D"));
+  ETRY(cuda_ok(cudaMemcpy(mass_d, mass.data(), sizeof(double) * nt, cudaMemcpyHostToDevice),
+               "H2D"));
   ETRY(cuda_ok(cudaMemcpy(lj_eps, he.data(), sizeof(double) * nt * nt, cudaMemcpyHostToDevice),
                "H2D"));
   return cuda_ok(cudaMemcpy(lj_s6, hs.data(), sizeof(double) * nt * nt, cudaMemcpyHostToDevice),
@@ -1013,6 +1032,68 @@ int rbx_engine::set_alpha(double a) {
   have_forces = false;
   graph_dirty = true;
   ++graph_version;
+  return RBX_OK;
+}
+
+// Nose-Hoover chain thermostat (NoseHooverController, nose_hoover_controller.cpp):
+// t_damp <= 0 switches it off; tdof <= 0 means 3N - 3 (Computedof :1013-1025).
+// SetUp (:415-471) runs here on the current velocities.
+int rbx_engine::set_nose_hoover(double t_start, double t_stop, double t_damp, long long num_steps,
+                                double kb, double mvv2e, double tdof) {
+  cudaSetDevice(device);
+  graph_dirty = true;
+  if (!(t_damp > 0)) {
+    nh_on = false;
+    return RBX_OK;
+  }
+  if (!(t_start > 0) || !(t_stop > 0) || !(kb > 0) || !(mvv2e > 0)) {
+    set_error("Nose-Hoover: temperatures, kB and mvv2e must be > 0");
+    return RBX_ERR_INVALID;
+  }
+  if (t_stop != t_start && num_steps <= 0) {
+    set_error("Nose-Hoover: a temperature ramp needs num_steps > 0");
+    return RBX_ERR_INVALID;
+  }
+  nhp.t_start = t_start;
+  nhp.t_stop = t_stop;
+  nhp.t_freq = 1.0 / t_damp;
+  nhp.dt = prm.dt;
+  nhp.kb = kb;
+  nhp.mvv2e = mvv2e;
+  nhp.tdof = tdof > 0 ? tdof : 3.0 * n - 3.0;
+  nhp.num_steps = num_steps;
+  nh_on = true;
+  ETRY(cuda_ok(cudaMemsetAsync(nh_state, 0, sizeof(double) * NH_SLOTS, st), "memset"));
+  ETRY(launch_ke_partials(n, type, mass_d, vx, vy, vz, nhp.mvv2e, ke_part, st));
+  ETRY(launch_nh_chain(nhp, nh_state, ke_part, nullptr, 0, 0, st));
+  return cuda_ok(cudaStreamSynchronize(st), "set_nose_hoover sync");
+}
+
+// InitialIntegrate's thermostat half (nose_hoover_controller.cpp:633-646):
+// target at the step being taken, chain half step, velocities scaled.
+int rbx_engine::nh_initial(const int* step_dev, long long step_add, cudaStream_t s) {
+  ETRY(launch_nh_chain(nhp, nh_state, ke_part, step_dev, step_add, 1, s));
+  return launch_scale_v(n, nh_state, vx, vy, vz, s);
+}
+
+// FinalIntegratePostShake (:689-711): temperature of the new velocities,
+// chain half step, velocities scaled.
+int rbx_engine::nh_final(cudaStream_t s) {
+  ETRY(launch_ke_partials(n, type, mass_d, vx, vy, vz, nhp.mvv2e, ke_part, s));
+  ETRY(launch_nh_chain(nhp, nh_state, ke_part, nullptr, 0, 2, s));
+  return launch_scale_v(n, nh_state, vx, vy, vz, s);
+}
+
+int rbx_engine::get_thermostat(double* temperature, double* eta, double* eta_dot) {
+  cudaSetDevice(device);
+  double h[NH_SLOTS];
+  ETRY(cuda_ok(cudaMemcpyAsync(h, nh_state, sizeof(h), cudaMemcpyDeviceToHost, st), "D2H"));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "sync"));
+  if (temperature) *temperature = h[NH_TEMP];
+  for (int c = 0; c < NH_CHAIN; ++c) {
+    if (eta) eta[c] = h[NH_ETA + c];
+    if (eta_dot) eta_dot[c] = h[NH_ETA_DOT + c];
+  }
   return RBX_OK;
 }
 
@@ -1289,6 +1370,17 @@ int rbx_engine_get_type_params(rbx_engine* e, double* sigma, double* eps, double
   if (eps) std::copy(e->eps.begin(), e->eps.end(), eps);
   if (mass) std::copy(e->mass.begin(), e->mass.end(), mass);
   return RBX_OK;
+}
+
+int rbx_engine_set_nose_hoover(rbx_engine* e, double t_start, double t_stop, double t_damp,
+                               int64_t num_steps, double kb, double mvv2e, double tdof) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->set_nose_hoover(t_start, t_stop, t_damp, (long long)num_steps, kb, mvv2e, tdof);
+}
+
+int rbx_engine_get_thermostat(rbx_engine* e, double* temperature, double* eta, double* eta_dot) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->get_thermostat(temperature, eta, eta_dot);
 }
 
 int rbx_engine_set_images(rbx_engine* e, const int* image) {

@@ -59,6 +59,14 @@ struct rbx_engine {
   int* dflags = nullptr;
   unsigned long long* max_d2 = nullptr;
   double* inv_mass = nullptr;
+  double* mass_d = nullptr;  // per type, for the kinetic energy
+  // Nose-Hoover chain thermostat (NVT): device state, its snapshot for graph
+  // replays, and the kinetic-energy partial sums
+  bool nh_on = false;
+  rbx::NHParams nhp{};
+  double* nh_state = nullptr;
+  double* nh_snap = nullptr;
+  double* ke_part = nullptr;
   double *lj_eps = nullptr, *lj_s6 = nullptr;
   unsigned long long* h_pinned = nullptr;
 
@@ -145,6 +153,11 @@ struct rbx_engine {
   int get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs, int64_t* n_shell);
   int get_stats(rbx_stats* s);
   int set_images(const int* image);
+  int set_nose_hoover(double t_start, double t_stop, double t_damp, long long num_steps,
+                      double kb, double mvv2e, double tdof);
+  int get_thermostat(double* temperature, double* eta, double* eta_dot);
+  int nh_initial(const int* step_dev, long long step_add, cudaStream_t s);
+  int nh_final(cudaStream_t s);
   int get_images(int* image);
   int write_trajectory(const char* path, int64_t timestep, bool append);
   int upload_type_tables();

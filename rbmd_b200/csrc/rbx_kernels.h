@@ -180,6 +180,30 @@ int launch_adj_kspace(int n, int p, double cscale, const KTab* tab, const double
 int launch_gather_vec3(int n, const int* orig, const double* src, double* x, double* y, double* z,
                        cudaStream_t st);
 
+// Nose-Hoover chain (rbx_thermo.cu): parameters and the device state layout.
+constexpr int NH_CHAIN = 3;
+enum NHSlot {
+  NH_ETA = 0,                            // [NH_CHAIN]
+  NH_ETA_DOT = NH_ETA + NH_CHAIN,        // [NH_CHAIN + 1], last entry 0
+  NH_ETA_DOTDOT = NH_ETA_DOT + NH_CHAIN + 1,
+  NH_ETA_MASS = NH_ETA_DOTDOT + NH_CHAIN,
+  NH_TEMP = NH_ETA_MASS + NH_CHAIN,      // current temperature
+  NH_T_TARGET, NH_KE_TARGET, NH_FACTOR,  // target, tdof kB T_target, last scale
+  NH_SLOTS
+};
+struct NHParams {
+  double t_start, t_stop, t_freq, dt, kb, mvv2e, tdof;
+  long long num_steps;
+};
+constexpr int KE_PARTS = 296;  // fixed reduction grid (2 x 148 SMs)
+int launch_ke_partials(int n, const int* type, const double* mass, const double* vx,
+                       const double* vy, const double* vz, double mvv2e, double* part,
+                       cudaStream_t st);
+int launch_nh_chain(const NHParams& p, double* state, const double* part, const int* step_dev,
+                    long long step_add, int mode, cudaStream_t st);
+int launch_scale_v(int n, const double* state, double* vx, double* vy, double* vz,
+                   cudaStream_t st);
+
 // A set of per-atom arrays moved together: dst[a][i] = src[a][perm[i]].
 struct ArraySet {
   static constexpr int kMaxF64 = 16, kMaxI32 = 8, kMaxU64 = 2;

@@ -99,7 +99,7 @@ EXPORTS = [
     "rbx_lammps_get_topology", "rbx_lammps_write_charge", "rbx_engine_set_images",
     "rbx_engine_get_images", "rbx_engine_write_trajectory", "rbx_engine_create_from_files",
     "rbx_engine_get_system", "rbx_engine_get_atoms", "rbx_engine_get_type_params",
-    "rbx_lammps_gauss_velocities",
+    "rbx_lammps_gauss_velocities", "rbx_engine_set_nose_hoover", "rbx_engine_get_thermostat",
 ]
 
 
@@ -176,6 +176,8 @@ def lib():
     L.rbx_engine_get_atoms.argtypes = [vp, vp, vp, vp]
     L.rbx_engine_get_type_params.argtypes = [vp, vp, vp, vp]
     L.rbx_lammps_gauss_velocities.argtypes = [vp, dp, C.c_char_p, ip]
+    L.rbx_engine_set_nose_hoover.argtypes = [vp, dp, dp, dp, C.c_int64, dp, dp, dp]
+    L.rbx_engine_get_thermostat.argtypes = [vp, vp, vp, vp]
     L.rbx_lammps_read.restype = vp
     L.rbx_lammps_read.argtypes = [C.c_char_p, C.c_char_p, vp]
     L.rbx_lammps_free.argtypes = [vp]
@@ -514,6 +516,19 @@ class Engine:
 
     def set_alpha(self, alpha):
         check(lib().rbx_engine_set_alpha(self._h, float(alpha)), "rbx_engine_set_alpha")
+
+    def set_nose_hoover(self, t_start, t_stop, t_damp, num_steps=0, kb=1.0, mvv2e=1.0,
+                        tdof=0.0):
+        """NVT with RBMD's Nose-Hoover chain; t_damp <= 0 goes back to NVE."""
+        check(lib().rbx_engine_set_nose_hoover(self._h, t_start, t_stop, t_damp, int(num_steps),
+                                               kb, mvv2e, tdof), "rbx_engine_set_nose_hoover")
+
+    def thermostat(self):
+        t = np.zeros(1)
+        eta, eta_dot = np.zeros(3), np.zeros(3)
+        check(lib().rbx_engine_get_thermostat(self._h, _np_ptr(t), _np_ptr(eta),
+                                              _np_ptr(eta_dot)), "rbx_engine_get_thermostat")
+        return {"temperature": t[0], "eta": eta, "eta_dot": eta_dot}
 
     def images(self):
         """Periodic image counters [n, 3] (int32), host atom order."""

@@ -158,3 +158,18 @@ def test_engine_from_files_errors(rbx, tmp_path, mutate, data, needle):
     h = rbx.lib().rbx_engine_create_from_files(str(cfg).encode(), 0, 0)
     assert not h
     assert needle in rbx.last_error(), rbx.last_error()
+
+
+@pytest.mark.parametrize("execution, needle", [
+    ('"ensemble": "NPT", ', "ensemble NPT"),
+    ('"ensemble": "NVT", "temp_ctrl_type": "BERENDSEN", ', "BERENDSEN"),
+])
+def test_engine_from_files_ensemble_errors(rbx, tmp_path, execution, needle):
+    from rbmd_b200 import systems
+
+    s = systems.lj_electrolyte(2000, seed=1)
+    rbx.write_lammps_charge(tmp_path / "sys.data", s)
+    cfg = tmp_path / "rbmd.json"
+    cfg.write_text(FILES_JSON.replace('"execution": {', '"execution": {' + execution))
+    assert not rbx.lib().rbx_engine_create_from_files(str(cfg).encode(), 0, 0)
+    assert needle in rbx.last_error(), rbx.last_error()

@@ -378,26 +378,57 @@ def test_engine_philox_matches_oracle_engine(cuda, rbx, oracle, sys4k):
     assert st.steps == 3 and st.selection_frequency == 4
 
 
-@pytest.mark.parametrize("prec", [0, 1])
-def test_step_graph_matches_individual_launches(cuda, rbx, prec):
-    """The CUDA-graph step (rebuild under a conditional node, device epoch)
-    runs the same kernels on the same data as the step the host drives launch
-    by launch: the trajectories are bit-identical, rebuilds included."""
+@pytest.mark.parametrize("prec, nvt", [(0, False), (1, False), (1, True)])
+def test_step_graph_matches_individual_launches(cuda, rbx, prec, nvt):
+    """The CUDA-graph step (rebuild under a conditional node, device epoch,
+    the Nose-Hoover chain on the device) runs the same kernels on the same
+    data as the step the host drives launch by launch: the trajectories are
+    bit-identical, rebuilds and thermostat included."""
     s = systems.lj_electrolyte(4000, seed=31)
     runs = []
     for graph in (True, False):
         e = rbx.Engine(s, precision=prec, seed=9)
         e.set_step_graph(graph)
         e.compute_forces(0)
+        if nvt:
+            e.set_nose_hoover(1.0, 1.6, 0.1, num_steps=40)
         e.step(15)
         e.step(25)
-        runs.append((e.get_state(), e.stats()))
+        runs.append((e.get_state(), e.stats(), e.thermostat()))
         e.close()
-    (a, sa), (b, sb) = runs
+    (a, sa, ta), (b, sb, tb) = runs
     for key in ("pos", "vel", "force"):
         assert np.array_equal(a[key], b[key]), key
+    if nvt:
+        assert ta["temperature"] == tb["temperature"]
+        assert np.array_equal(ta["eta_dot"], tb["eta_dot"])
     assert sa.steps == sb.steps == 40
     assert sa.rebuilds == sb.rebuilds and sa.rebuilds >= 2
+
+
+@pytest.mark.parametrize("ramp", [False, True])
+def test_nose_hoover_matches_oracle(cuda, rbx, oracle, sys4k, ramp):
+    """NVT steps (Nose-Hoover chain of NVTensemble::Solve) agree with the
+    oracle's NVT step to FP64 round-off: positions, velocities and the chain."""
+    s = sys4k
+    t_stop = 1.8 if ramp else 1.3
+    e = rbx.Engine(s, precision=rbx.PLAIN_FP64, seed=4242)
+    ref = oracle.Engine(s, seed=4242)
+    for x in (e, ref):
+        x.compute_forces(0)
+        x.set_nose_hoover(1.3, t_stop, 0.05, num_steps=20)
+    for k in range(4):
+        e.step(5)
+        ref.step(5)
+        a, b = e.get_state(), ref.get()
+        order = np.argsort(b["gid"])
+        assert np.abs(a["pos"] - b["pos"][order]).max() < 1e-9, k
+        assert systems.rel_rms(a["vel"], b["vel"][order]) < 1e-9, k
+        ta, tb = e.thermostat(), ref.thermostat()
+        assert abs(ta["temperature"] - tb["temperature"]) < 1e-9 * tb["temperature"]
+        assert np.allclose(ta["eta_dot"], tb["eta_dot"], rtol=1e-7, atol=1e-12)
+        assert np.allclose(ta["eta"], tb["eta"], rtol=1e-7, atol=1e-12)
+    e.close()
 
 
 def test_step_graph_recovers_from_list_overflow(cuda, rbx):
@@ -726,6 +757,9 @@ def test_engine_from_files_matches_arrays(cuda, rbx, tmp_path, rep, velocities):
         data.write_text(data.read_text().partition("\nVelocities")[0] + "\n")
     cfg = tmp_path / "rbmd.json"
     text = FILES_JSON.replace("REP", str(list(rep)))
+    if not velocities:  # and NVT with the Nose-Hoover chain
+        text = text.replace('"execution": {', '"execution": {"ensemble": "NVT", '
+                            '"temp_ctrl_type": "NOSE_HOOVER", ')
     cfg.write_text(text)
     a = rbx.Engine.from_files(cfg, precision=rbx.MIXED)
     ref = rbx.read_lammps(data, replicate=rep, gauss=None if velocities else (1.2, "LJ", 77))
@@ -745,6 +779,8 @@ def test_engine_from_files_matches_arrays(cuda, rbx, tmp_path, rep, velocities):
     b = rbx.Engine(sysd, precision=rbx.MIXED, json_text=text.replace("// RBMD's config files "
                                                                       "carry comments", ""))
     b.set_images(im)
+    if not velocities:
+        b.set_nose_hoover(1.2, 1.2, 1.0)
     sa, sb = a.get_state(), b.get_state()
     assert np.array_equal(sa["pos"], sb["pos"]) and np.array_equal(sa["vel"], sb["vel"])
     for e in (a, b):
@@ -754,5 +790,8 @@ def test_engine_from_files_matches_arrays(cuda, rbx, tmp_path, rep, velocities):
     for key in ("pos", "vel", "force"):
         assert np.array_equal(sa[key], sb[key]), key
     assert np.abs(sa["pos"] + a.images() * Lr - (sb["pos"] + b.images() * Lr)).max() == 0
+    if not velocities:
+        assert a.thermostat()["temperature"] == b.thermostat()["temperature"]
+        assert a.thermostat()["eta_dot"][0] != 0
     a.close()
     b.close()
