@@ -358,6 +358,21 @@ int rbx_engine_set_nose_hoover(rbx_engine* e, double t_start, double t_stop, dou
 /* Current thermostat state: temperature (after the last step's scaling),
  * eta[3], eta_dot[3]; any pointer may be NULL. */
 int rbx_engine_get_thermostat(rbx_engine* e, double* temperature, double* eta, double* eta_dot);
+/* SHAKE / RATTLE of rigid three-atom clusters (RBMD's ShakeA / ShakeB,
+ * shake_controller_op.hip.cu:19-660, serial path shake_controller.cpp:2130-2220):
+ * clusters [nclusters][3] are atom indices in the order given to
+ * rbx_engine_set_state with the centre atom second (the angle's atoms, H O H
+ * for water); distances held at bond (0-1, 1-2) and
+ * sqrt(2 bond^2 (1 - cos angle_deg)) (0-2); RBMD hard-codes bond 1.0 and
+ * 109.47 degrees.  Position constraints after the drift, velocity constraints
+ * after the second half kick, on the device inside the step.  With the
+ * Nose-Hoover thermostat pass tdof = 3N - 3 - N as RBMD's Computedof does.
+ * nclusters = 0 switches it off. */
+int rbx_engine_set_shake(rbx_engine* e, int nclusters, const int* clusters, double bond,
+                         double angle_deg);
+/* Clusters in use and the number of cluster solves that did not converge
+ * (5000 iterations, 1e-5 on the multipliers) or had a near-singular matrix. */
+int rbx_engine_get_shake(rbx_engine* e, int* nclusters, int* failures);
 /* Periodic image counters, [n][3] ints in the atom order given to
  * rbx_engine_set_state: how many times each atom has wrapped through each face
  * (+1 leaving through hi).  rbx_engine_set_state zeroes them; the drift of

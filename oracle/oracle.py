@@ -112,6 +112,10 @@ def lib():
                                                      C.c_double, C.c_longlong, C.c_double,
                                                      C.c_double, C.c_double]),
             "orc_engine_get_thermostat": (None, [C.c_void_p, _dp, _dp, _dp]),
+            "orc_engine_set_fmt2v": (None, [C.c_void_p, C.c_double]),
+            "orc_engine_set_shake": (C.c_int, [C.c_void_p, C.c_int, _ip, C.c_double,
+                                               C.c_double]),
+            "orc_engine_shake_failures": (C.c_int, [C.c_void_p]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -334,6 +338,8 @@ class Engine:
                                       p["qqr2e"], p["dt"], seed, int(use_rbl))
         if not self._h:
             raise RuntimeError("orc_engine_create failed")
+        L.orc_engine_set_fmt2v(self._h, float(p.get("fmt2v", 1.0)))
+        self._gid = np.asarray(sys["gid"], dtype=np.int32)
         L.orc_engine_set_state(self._h, _i(sys["gid"]), _i(sys["type"]), _d(sys["q"]),
                                *[_d(sys["pos"][:, d]) for d in range(3)],
                                *[_d(sys["vel"][:, d]) for d in range(3)])
@@ -362,6 +368,15 @@ class Engine:
         """NVT Nose-Hoover chain (NVTensemble::Solve with NOSE_HOOVER)."""
         lib().orc_engine_set_nose_hoover(self._h, t_start, t_stop, t_damp, num_steps, kb, mvv2e,
                                          tdof)
+
+    def set_shake(self, clusters, bond, angle_deg):
+        """SHAKE / RATTLE clusters given as host atom indices [nc, 3], centre second."""
+        gids = np.ascontiguousarray(self._gid[np.asarray(clusters)], dtype=np.int32)
+        lib().orc_engine_set_shake(self._h, len(gids), _i(gids.ravel()), bond, angle_deg)
+
+    @property
+    def shake_failures(self):
+        return lib().orc_engine_shake_failures(self._h)
 
     def thermostat(self):
         t = np.zeros(1)

@@ -864,6 +864,14 @@ struct orc_engine {
   long long nh_num_steps;
   double nh_t_start, nh_t_stop, nh_t_freq, nh_kb, nh_mvv2e, nh_tdof;
   double eta[3], eta_dot[4], eta_dotdot[3], eta_mass[3], temperature, t_target, ke_target;
+  /* unit style: force/mass*time -> velocity */
+  double fmt2v;
+  /* SHAKE clusters by gid (centre second) */
+  int shake_nc, max_gid;
+  int *shake_gid, *where;
+  double shake_b1sq, shake_b2sq, shake_b12sq;
+  double *xs, *ys, *zs;
+  int shake_failures;
 };
 
 orc_engine* orc_engine_create(int n, const orc_box* box, int ntypes,
@@ -892,6 +900,7 @@ orc_engine* orc_engine_create(int n, const orc_box* box, int ntypes,
   e->dt = dt;
   e->seed = seed;
   e->use_rbl = use_rbl;
+  e->fmt2v = 1.0;
   e->freq = orc_rbl_params(n, box, r_core, cut_off, neighbor_sample_num, NULL, NULL);
   e->S = orc_rbe_gauss_sum(box, alpha);
   int dims[3];
@@ -920,6 +929,11 @@ void orc_engine_destroy(orc_engine* e) {
                   e->vz, e->fx, e->fy, e->fz, e->x0, e->y0, e->z0, e->tmp, e->kfx, e->kfy,
                   e->kfz, e->mx, e->my, e->mz, e->re, e->im, e->cand, e->core, e->shell};
   for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
+  free(e->shake_gid);
+  free(e->where);
+  free(e->xs);
+  free(e->ys);
+  free(e->zs);
   free(e);
 }
 
@@ -1034,9 +1048,213 @@ static void engine_kick(orc_engine* e) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < e->n; ++i) {
     const double m = e->mass[e->type[i]];
-    e->vx[i] += 0.5 * e->fx[i] / m * e->dt;
-    e->vy[i] += 0.5 * e->fy[i] / m * e->dt;
-    e->vz[i] += 0.5 * e->fz[i] / m * e->dt;
+    e->vx[i] += 0.5 * e->fx[i] / m * e->dt * e->fmt2v;
+    e->vy[i] += 0.5 * e->fy[i] / m * e->dt * e->fmt2v;
+    e->vz[i] += 0.5 * e->fz[i] / m * e->dt * e->fmt2v;
+  }
+}
+
+void orc_engine_set_fmt2v(orc_engine* e, double fmt2v) { e->fmt2v = fmt2v; }
+
+/* ---- SHAKE / RATTLE of rigid 3-atom clusters ---------------------------- */
+/* ShakeA / ShakeB of RBMD (shake_controller_op.hip.cu:19-389, 391-660),
+ * restated: MinImageDistanceVec (box.h:115-131) = a - b with
+ * d -= L rint(d / L). */
+static void shk_sub(const orc_box* b, const double* a, const double* c, double* o) {
+  for (int k = 0; k < 3; ++k) {
+    const double L = box_len(b, k);
+    o[k] = a[k] - c[k];
+    o[k] -= L * rint(o[k] * (1.0 / L));
+  }
+}
+static double shk_dot(const double* a, const double* b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+static double shk_inv3(const double a[3][3], double ai[3][3]) {
+  const double d = a[0][0] * a[1][1] * a[2][2] + a[0][1] * a[1][2] * a[2][0] +
+                   a[0][2] * a[1][0] * a[2][1] - a[0][0] * a[1][2] * a[2][1] -
+                   a[0][1] * a[1][0] * a[2][2] - a[0][2] * a[1][1] * a[2][0];
+  const double r = 1 / d;
+  ai[0][0] = r * (a[1][1] * a[2][2] - a[1][2] * a[2][1]);
+  ai[0][1] = -r * (a[0][1] * a[2][2] - a[0][2] * a[2][1]);
+  ai[0][2] = r * (a[0][1] * a[1][2] - a[0][2] * a[1][1]);
+  ai[1][0] = -r * (a[1][0] * a[2][2] - a[1][2] * a[2][0]);
+  ai[1][1] = r * (a[0][0] * a[2][2] - a[0][2] * a[2][0]);
+  ai[1][2] = -r * (a[0][0] * a[1][2] - a[0][2] * a[1][0]);
+  ai[2][0] = r * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+  ai[2][1] = -r * (a[0][0] * a[2][1] - a[0][1] * a[2][0]);
+  ai[2][2] = r * (a[0][0] * a[1][1] - a[0][1] * a[1][0]);
+  return d;
+}
+
+int orc_engine_set_shake(orc_engine* e, int nc, const int* cluster_gids, double bond,
+                         double angle_deg) {
+  free(e->shake_gid);
+  free(e->where);
+  e->shake_gid = NULL;
+  e->where = NULL;
+  e->shake_nc = 0;
+  if (nc <= 0 || !(bond > 0)) return 0;
+  int mg = 0;
+  for (int i = 0; i < e->n; ++i) mg = e->gid[i] > mg ? e->gid[i] : mg;
+  e->max_gid = mg;
+  e->shake_gid = (int*)malloc(sizeof(int) * 3 * (size_t)nc);
+  memcpy(e->shake_gid, cluster_gids, sizeof(int) * 3 * (size_t)nc);
+  e->where = (int*)malloc(sizeof(int) * ((size_t)mg + 1));
+  if (!e->xs) {
+    e->xs = (double*)malloc(sizeof(double) * (size_t)e->n);
+    e->ys = (double*)malloc(sizeof(double) * (size_t)e->n);
+    e->zs = (double*)malloc(sizeof(double) * (size_t)e->n);
+  }
+  const double a = angle_deg / 180.0 * M_PI;
+  e->shake_b1sq = e->shake_b2sq = bond * bond;
+  const double b12 = sqrt(bond * bond + bond * bond - 2.0 * bond * bond * cos(a));
+  e->shake_b12sq = b12 * b12;
+  e->shake_nc = nc;
+  e->shake_failures = 0;
+  return 0;
+}
+
+int orc_engine_shake_failures(const orc_engine* e) { return e->shake_failures; }
+
+static void shk_index(orc_engine* e) {
+  for (int i = 0; i < e->n; ++i) e->where[e->gid[i]] = i;
+}
+
+static void shake_a(orc_engine* e) {
+  shk_index(e);
+  for (int c = 0; c < e->shake_nc; ++c) {
+    int id[3];
+    double po[3][3], pu[3][3], im[3];
+    for (int k = 0; k < 3; ++k) {
+      id[k] = e->where[e->shake_gid[3 * c + k]];
+      po[k][0] = e->xs[id[k]];
+      po[k][1] = e->ys[id[k]];
+      po[k][2] = e->zs[id[k]];
+      pu[k][0] = e->x[id[k]];
+      pu[k][1] = e->y[id[k]];
+      pu[k][2] = e->z[id[k]];
+      im[k] = 1 / e->mass[e->type[id[k]]];
+    }
+    double r01[3], r12[3], r20[3], s10[3], s21[3], s02[3];
+    shk_sub(&e->box, po[1], po[0], r01);
+    shk_sub(&e->box, po[2], po[1], r12);
+    shk_sub(&e->box, po[0], po[2], r20);
+    shk_sub(&e->box, pu[0], pu[1], s10);
+    shk_sub(&e->box, pu[1], pu[2], s21);
+    shk_sub(&e->box, pu[2], pu[0], s02);
+    const double r01sq = shk_dot(r01, r01), r02sq = shk_dot(r20, r20), r12sq = shk_dot(r12, r12);
+    const double s01sq = shk_dot(s10, s10), s02sq = shk_dot(s02, s02), s12sq = shk_dot(s21, s21);
+    double A[3][3], Ai[3][3];
+    A[0][0] = 2 * (im[0] + im[1]) * shk_dot(s10, r01);
+    A[0][1] = -2 * im[1] * shk_dot(s10, r12);
+    A[0][2] = -2 * im[0] * shk_dot(s10, r20);
+    A[1][0] = -2 * im[1] * shk_dot(s21, r01);
+    A[1][1] = 2 * (im[1] + im[2]) * shk_dot(s21, r12);
+    A[1][2] = -2 * im[2] * shk_dot(s21, r20);
+    A[2][0] = -2 * im[0] * shk_dot(s02, r01);
+    A[2][1] = -2 * im[2] * shk_dot(s02, r12);
+    A[2][2] = 2 * (im[0] + im[2]) * shk_dot(s02, r20);
+    const double det = shk_inv3(A, Ai);
+    const double r0120 = shk_dot(r01, r20), r0112 = shk_dot(r01, r12), r2012 = shk_dot(r20, r12);
+    /* coefficients of l01^2, l20^2, l12^2, l01 l20, l01 l12, l20 l12 */
+    const double Q[3][6] = {
+        {(im[0] + im[1]) * (im[0] + im[1]) * r01sq, im[0] * im[0] * r02sq, im[1] * im[1] * r12sq,
+         -2 * (im[0] + im[1]) * im[0] * r0120, -2 * (im[0] + im[1]) * im[1] * r0112,
+         2 * im[0] * im[1] * r2012},
+        {im[1] * im[1] * r01sq, im[2] * im[2] * r02sq, (im[1] + im[2]) * (im[1] + im[2]) * r12sq,
+         2 * im[1] * im[2] * r0120, -2 * (im[1] + im[2]) * im[1] * r0112,
+         -2 * (im[1] + im[2]) * im[2] * r2012},
+        {im[0] * im[0] * r01sq, (im[0] + im[2]) * (im[0] + im[2]) * r02sq, im[2] * im[2] * r12sq,
+         -2 * (im[0] + im[2]) * im[0] * r0120, 2 * im[0] * im[2] * r0112,
+         -2 * (im[0] + im[2]) * im[2] * r2012}};
+    const double rhs0[3] = {e->shake_b1sq - s01sq, e->shake_b2sq - s12sq,
+                            e->shake_b12sq - s02sq};
+    double l01 = 0, l20 = 0, l12 = 0;
+    int done = 0, overflow = 0, it = 0;
+    while (!done && it < 5000) {
+      const double t[6] = {l01 * l01, l20 * l20, l12 * l12, l01 * l20, l01 * l12, l20 * l12};
+      double bq[3];
+      for (int r = 0; r < 3; ++r) {
+        double quad = Q[r][0] * t[0];
+        for (int m = 1; m < 6; ++m) quad += Q[r][m] * t[m];
+        bq[r] = rhs0[r] - quad;
+      }
+      const double n01 = Ai[0][0] * bq[0] + Ai[0][1] * bq[1] + Ai[0][2] * bq[2];
+      const double n12 = Ai[1][0] * bq[0] + Ai[1][1] * bq[1] + Ai[1][2] * bq[2];
+      const double n20 = Ai[2][0] * bq[0] + Ai[2][1] * bq[1] + Ai[2][2] * bq[2];
+      done = fabs(n01 - l01) <= 1e-5 && fabs(n20 - l20) <= 1e-5 && fabs(n12 - l12) <= 1e-5;
+      l01 = n01;
+      l20 = n20;
+      l12 = n12;
+      if (isnan(l01) || isnan(l20) || isnan(l12) || fabs(l01) > 1e20 || fabs(l20) > 1e20 ||
+          fabs(l12) > 1e20)
+        done = overflow = 1;
+      ++it;
+    }
+    if (!done || overflow || fabs(det) < 1e-4) e->shake_failures++;
+    double* pos[3] = {e->x, e->y, e->z};
+    double* vel[3] = {e->vx, e->vy, e->vz};
+    for (int k = 0; k < 3; ++k) {
+      const double d[3] = {l01 * r01[k] * im[0] - l20 * r20[k] * im[0],
+                           l12 * r12[k] * im[1] - l01 * r01[k] * im[1],
+                           l20 * r20[k] * im[2] - l12 * r12[k] * im[2]};
+      const double L = box_len(&e->box, k);
+      for (int a2 = 0; a2 < 3; ++a2) {
+        vel[k][id[a2]] += d[a2] / e->dt;
+        double p = pu[a2][k] + d[a2];
+        if (p >= e->box.hi[k]) p -= L;
+        if (p < e->box.lo[k]) p += L;
+        pos[k][id[a2]] = p;
+      }
+    }
+  }
+}
+
+static void shake_b(orc_engine* e) {
+  shk_index(e);
+  for (int c = 0; c < e->shake_nc; ++c) {
+    int id[3];
+    double p[3][3], v[3][3], im[3];
+    for (int k = 0; k < 3; ++k) {
+      id[k] = e->where[e->shake_gid[3 * c + k]];
+      p[k][0] = e->x[id[k]];
+      p[k][1] = e->y[id[k]];
+      p[k][2] = e->z[id[k]];
+      v[k][0] = e->vx[id[k]];
+      v[k][1] = e->vy[id[k]];
+      v[k][2] = e->vz[id[k]];
+      im[k] = 1 / e->mass[e->type[id[k]]];
+    }
+    double r01[3], r12[3], r20[3], sv10[3], sv21[3], sv02[3];
+    shk_sub(&e->box, p[1], p[0], r01);
+    shk_sub(&e->box, p[2], p[1], r12);
+    shk_sub(&e->box, p[0], p[2], r20);
+    for (int k = 0; k < 3; ++k) {
+      sv10[k] = v[0][k] - v[1][k];
+      sv21[k] = v[1][k] - v[2][k];
+      sv02[k] = v[2][k] - v[0][k];
+    }
+    double A[3][3], Ai[3][3];
+    A[0][0] = (im[1] + im[0]) * shk_dot(r01, r01);
+    A[0][1] = -im[1] * shk_dot(r01, r12);
+    A[0][2] = -im[0] * shk_dot(r01, r20);
+    A[1][0] = A[0][1];
+    A[1][1] = (im[1] + im[2]) * shk_dot(r12, r12);
+    A[1][2] = -im[2] * shk_dot(r20, r12);
+    A[2][0] = A[0][2];
+    A[2][1] = A[1][2];
+    A[2][2] = (im[0] + im[2]) * shk_dot(r20, r20);
+    const double c3[3] = {-shk_dot(sv10, r01), -shk_dot(sv21, r12), -shk_dot(sv02, r20)};
+    if (fabs(shk_inv3(A, Ai)) < 1e-4) e->shake_failures++;
+    double l[3];
+    for (int r = 0; r < 3; ++r) l[r] = Ai[r][0] * c3[0] + Ai[r][1] * c3[1] + Ai[r][2] * c3[2];
+    double* vel[3] = {e->vx, e->vy, e->vz};
+    for (int k = 0; k < 3; ++k) {
+      vel[k][id[0]] = v[0][k] + (l[0] * r01[k] * im[0] - l[2] * r20[k] * im[0]);
+      vel[k][id[1]] = v[1][k] + (l[1] * r12[k] * im[1] - l[0] * r01[k] * im[1]);
+      vel[k][id[2]] = v[2][k] + (l[2] * r20[k] * im[2] - l[1] * r12[k] * im[2]);
+    }
   }
 }
 static void engine_drift(orc_engine* e) {
@@ -1163,10 +1381,17 @@ int orc_engine_step(orc_engine* e, int nsteps) {
       nh_chain(e);
     }
     engine_kick(e);
+    if (e->shake_nc) {
+      memcpy(e->xs, e->x, sizeof(double) * (size_t)e->n);
+      memcpy(e->ys, e->y, sizeof(double) * (size_t)e->n);
+      memcpy(e->zs, e->z, sizeof(double) * (size_t)e->n);
+    }
     engine_drift(e);
+    if (e->shake_nc) shake_a(e);
     e->epoch++;
     if (orc_engine_compute_forces(e, e->epoch) != 0) return -1;
     engine_kick(e);
+    if (e->shake_nc) shake_b(e);
     if (e->nh_on) {
       e->temperature = nh_temperature(e);
       nh_chain(e);

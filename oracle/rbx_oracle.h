@@ -126,6 +126,17 @@ int orc_engine_get(orc_engine* e, int* gid, double* x, double* y, double* z,
                    double* vx, double* vy, double* vz, double* fx, double* fy,
                    double* fz);
 int orc_engine_rebuilds(const orc_engine* e);
+/* NVT with the Nose-Hoover chain (t_damp <= 0: off; tdof <= 0: 3N - 3). */
+int orc_engine_set_nose_hoover(orc_engine* e, double t_start, double t_stop, double t_damp,
+                               long long num_steps, double kb, double mvv2e, double tdof);
+void orc_engine_get_thermostat(const orc_engine* e, double* temperature, double* eta,
+                               double* eta_dot);
+/* Unit style's force/mass*time -> velocity factor (1 for LJ). */
+void orc_engine_set_fmt2v(orc_engine* e, double fmt2v);
+/* SHAKE / RATTLE clusters given by gid, centre second (nc = 0: off). */
+int orc_engine_set_shake(orc_engine* e, int nc, const int* cluster_gids, double bond,
+                         double angle_deg);
+int orc_engine_shake_failures(const orc_engine* e);
 int orc_num_threads(void);
 
 #ifdef __cplusplus

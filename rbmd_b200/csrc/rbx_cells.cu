@@ -415,20 +415,6 @@ __global__ void k_kick(int n, const double* __restrict__ fx, const double* __res
   vz[i] += fz[i] * s;
 }
 
-__device__ __forceinline__ unsigned to_fixed(double v, double lo, double scale) {
-  return (unsigned)(unsigned long long)__double2ll_rd((v - lo) * scale);
-}
-
-__device__ __forceinline__ void warp_max_atomic(double d2, unsigned long long* out) {
-  unsigned long long bits = (unsigned long long)__double_as_longlong(d2);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long t = __shfl_xor_sync(0xffffffffu, bits, o);
-    bits = t > bits ? t : bits;
-  }
-  if ((threadIdx.x & 31) == 0) atomicMax(out, bits);
-}
-
 // UpdatePositionFlag + ApplyPBC (update_position_op.hip.cu:22-46, box.h:133-169),
 // fused with the skin check DisplacementSq (base_neighbor_list_builder.cpp:102-116)
 // and, for the mixed form, the fixed-point record {ux, uy, uz, q_f32}.
@@ -438,10 +424,15 @@ __global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double
                         const double* __restrict__ x0, const double* __restrict__ y0,
                         const double* __restrict__ z0, unsigned long long* __restrict__ max_d2,
                         uint4* __restrict__ atoms, const double* __restrict__ q,
-                        ImageRefs img) {
+                        ImageRefs img, Pos3 old) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0.0;
   if (i < n) {
+    if (old.x) {  // positions before the drift, for SHAKE
+      old.x[i] = x[i];
+      old.y[i] = y[i];
+      old.z[i] = z[i];
+    }
     double p[3] = {x[i] + vx[i] * dt, y[i] + vy[i] * dt, z[i] + vz[i] * dt};
     for (int d = 0; d < 3; ++d) {  // periodic wrap, counted in the image flags
       int w = 0;
@@ -667,10 +658,10 @@ int launch_kick(int n, const double* fx, const double* fy, const double* fz, con
 int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* z,
                  const double* vx, const double* vy, const double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
-                 uint4* atoms, const double* q, ImageRefs img, cudaStream_t st) {
+                 uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
   k_drift<<<(n + 255) / 256, 256, 0, st>>>(b, n, dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2_bits,
-                                           atoms, q, img);
+                                           atoms, q, img, old);
   count_launch();
   return check_launch("drift");
 }

@@ -33,6 +33,23 @@ __device__ __forceinline__ double min_image1(double d, double len, double half) 
   return d;
 }
 
+// Fixed-point coordinate of the mixed form: floor((v - lo) * 2^32 / L).
+__device__ __forceinline__ unsigned to_fixed(double v, double lo, double scale) {
+  return (unsigned)(unsigned long long)__double2ll_rd((v - lo) * scale);
+}
+
+// Warp maximum of a non-negative double, then one atomicMax on its bits.
+// Every lane of the warp must call it.
+__device__ __forceinline__ void warp_max_atomic(double d2, unsigned long long* out) {
+  unsigned long long bits = (unsigned long long)__double_as_longlong(d2);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(0xffffffffu, bits, o);
+    bits = t > bits ? t : bits;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, bits);
+}
+
 // CaculateDistance (src/neighbor_list/src/op/full_neighbor_list_op.h:98-106):
 // i minus j, min image, squares summed left to right with no fused
 // multiply-add, so list membership rounds like the reference.

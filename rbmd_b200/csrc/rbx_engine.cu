@@ -524,7 +524,9 @@ int rbx_engine::step_plain(int nsteps) {
     ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
     ETRY(cuda_ok(cudaMemsetAsync(max_d2, 0, sizeof(unsigned long long), st), "memset"));
     ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
-                     ImageRefs{{img[0], img[1], img[2]}}, st));
+                     ImageRefs{{img[0], img[1], img[2]}}, Pos3{shake_nc ? xs : nullptr, ys, zs},
+                     st));
+    if (shake_nc) ETRY(shake_a(st));
     if (e) cudaEventRecord(e[1], st);
     ++epoch;
     ETRY(check_rebuild(true));
@@ -532,6 +534,7 @@ int rbx_engine::step_plain(int nsteps) {
     ETRY(real_space());
     if (e) cudaEventRecord(e[3], st);
     ETRY(kspace_and_combine(true));
+    if (shake_nc) ETRY(shake_b(st));
     if (nh_on) ETRY(nh_final(st));
     if (e) cudaEventRecord(e[4], st);
     ++steps;
@@ -579,7 +582,9 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
   ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
   ETRY(launch_zero_u64(max_d2, st));
   ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
-                     ImageRefs{{img[0], img[1], img[2]}}, st));
+                     ImageRefs{{img[0], img[1], img[2]}}, Pos3{shake_nc ? xs : nullptr, ys, zs},
+                     st));
+  if (shake_nc) ETRY(shake_a(st));
   ETRY(launch_step_decide(max_d2, thr * thr, dflags + 4, cond, st));
   // the conditional node after everything captured so far on st
   cudaStreamCaptureStatus cs;
@@ -610,6 +615,7 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
   graph_rebuild_launches = rbx_launch_count() - b0;
   ETRY(real_space(dflags + 4));
   ETRY(kspace_and_combine(true, dflags + 4));
+  if (shake_nc) ETRY(shake_b(st));
   if (nh_on) ETRY(nh_final(st));
   graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
   return RBX_OK;
@@ -1097,6 +1103,69 @@ int rbx_engine::get_thermostat(double* temperature, double* eta, double* eta_dot
   return RBX_OK;
 }
 
+// SHAKE / RATTLE clusters (ShakeController serial path): clusters[3c..3c+2]
+// are host atom indices with the centre second; bond <= 0 or no clusters
+// switches it off.  The geometry of all clusters is bond, bond and
+// sqrt(2 bond^2 (1 - cos angle)) as the reference's ShakeA hard-codes it.
+int rbx_engine::set_shake(int nclusters, const int* clusters, double bond, double angle_deg) {
+  cudaSetDevice(device);
+  graph_dirty = true;
+  if (nclusters <= 0 || !(bond > 0)) {
+    shake_nc = 0;
+    return RBX_OK;
+  }
+  std::vector<int> seen(n, 0);
+  for (int c = 0; c < 3 * nclusters; ++c) {
+    const int h = clusters[c];
+    if (h < 0 || h >= n) {
+      set_error("SHAKE cluster %d names atom %d outside [0, %d)", c / 3, h, n);
+      return RBX_ERR_INVALID;
+    }
+    if (seen[h]++) {
+      set_error("atom %d is in more than one SHAKE cluster", h);
+      return RBX_ERR_INVALID;
+    }
+  }
+  if (nclusters > shake_cap) {
+    ETRY(alloc(&shake_cl, (size_t)3 * nclusters));
+    shake_cap = nclusters;
+  }
+  if (!where) {
+    ETRY(alloc(&where, (size_t)n));
+    ETRY(alloc(&xs, (size_t)n));
+    ETRY(alloc(&ys, (size_t)n));
+    ETRY(alloc(&zs, (size_t)n));
+  }
+  ETRY(cuda_ok(cudaMemcpyAsync(shake_cl, clusters, sizeof(int) * 3 * nclusters,
+                               cudaMemcpyHostToDevice, st),
+               "H2D"));
+  const double ang = angle_deg / 180.0 * M_PI;
+  shp.dt = prm.dt;
+  shp.b1sq = bond * bond;
+  shp.b2sq = bond * bond;
+  const double b12 = sqrt(bond * bond + bond * bond - 2.0 * bond * bond * cos(ang));
+  shp.b12sq = b12 * b12;
+  shp.tol = 1e-5;
+  shp.max_iter = 5000;
+  shake_nc = nclusters;
+  ETRY(cuda_ok(cudaMemsetAsync(dflags + 6, 0, sizeof(int), st), "memset"));
+  return cuda_ok(cudaStreamSynchronize(st), "set_shake sync");
+}
+
+int rbx_engine::shake_a(cudaStream_t s) {
+  ETRY(launch_inverse_perm(n, orig, where, s));
+  return launch_shake_a(dbox, shp, shake_nc, shake_cl, where, type, mass_d, Pos3{xs, ys, zs},
+                        Pos3{x, y, z}, Pos3{vx, vy, vz}, ImageRefs{{img[0], img[1], img[2]}}, x0,
+                        y0, z0, max_d2, prm.precision == RBX_MIXED ? atoms : nullptr, q,
+                        dflags + 6, s);
+}
+
+int rbx_engine::shake_b(cudaStream_t s) {
+  ETRY(launch_inverse_perm(n, orig, where, s));
+  return launch_shake_b(dbox, shake_nc, shake_cl, where, type, mass_d, Pos3{x, y, z},
+                        Pos3{vx, vy, vz}, dflags + 6, s);
+}
+
 // Periodic image counters, [n][3] in host order.
 int rbx_engine::set_images(const int* himg) {
   cudaSetDevice(device);
@@ -1381,6 +1450,25 @@ int rbx_engine_set_nose_hoover(rbx_engine* e, double t_start, double t_stop, dou
 int rbx_engine_get_thermostat(rbx_engine* e, double* temperature, double* eta, double* eta_dot) {
   if (!e) return RBX_ERR_INVALID;
   return e->get_thermostat(temperature, eta, eta_dot);
+}
+
+int rbx_engine_set_shake(rbx_engine* e, int nclusters, const int* clusters, double bond,
+                         double angle_deg) {
+  if (!e || (nclusters > 0 && !clusters)) return RBX_ERR_INVALID;
+  return e->set_shake(nclusters, clusters, bond, angle_deg);
+}
+
+int rbx_engine_get_shake(rbx_engine* e, int* nclusters, int* failures) {
+  if (!e) return RBX_ERR_INVALID;
+  cudaSetDevice(e->device);
+  int f = 0;
+  if (cudaMemcpy(&f, e->dflags + 6, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    set_error("rbx_engine_get_shake: device read failed");
+    return RBX_ERR_DEVICE;
+  }
+  if (nclusters) *nclusters = e->shake_nc;
+  if (failures) *failures = f;
+  return RBX_OK;
 }
 
 int rbx_engine_set_images(rbx_engine* e, const int* image) {

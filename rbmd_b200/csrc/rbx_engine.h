@@ -55,11 +55,12 @@ struct rbx_engine {
   int nrbl = 0;    // blocks of the fused RBL launch (depends on cap)
   double *fpart = nullptr, *epart = nullptr, *mean = nullptr;
   // [0] cell sort, [1] list overflow, [2] sampler, [3] real-space kernel,
-  // [4] device epoch (step graphs), [5] rebuilds inside step graphs
+  // [4] device epoch (step graphs), [5] rebuilds inside step graphs,
+  // [6] SHAKE solves that failed
   int* dflags = nullptr;
   unsigned long long* max_d2 = nullptr;
   double* inv_mass = nullptr;
-  double* mass_d = nullptr;  // per type, for the kinetic energy
+  double* mass_d = nullptr;  // per type, for the kinetic energy and SHAKE
   // Nose-Hoover chain thermostat (NVT): device state, its snapshot for graph
   // replays, and the kinetic-energy partial sums
   bool nh_on = false;
@@ -67,6 +68,18 @@ struct rbx_engine {
   double* nh_state = nullptr;
   double* nh_snap = nullptr;
   double* ke_part = nullptr;
+  // SHAKE / RATTLE clusters (host indices, centre second), the host index ->
+  // cell slot map, positions before the drift, failure counter (dflags[6])
+  int shake_nc = 0, shake_cap = 0;
+  rbx::ShakeParams shp{};
+  int* shake_cl = nullptr;
+  int* where = nullptr;
+  double* xs = nullptr;
+  double* ys = nullptr;
+  double* zs = nullptr;
+  int shake_a(cudaStream_t s);
+  int shake_b(cudaStream_t s);
+  int set_shake(int nclusters, const int* clusters, double bond, double angle_deg);
   double *lj_eps = nullptr, *lj_s6 = nullptr;
   unsigned long long* h_pinned = nullptr;
 

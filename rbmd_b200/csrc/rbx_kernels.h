@@ -234,13 +234,32 @@ int launch_kick(int n, const double* fx, const double* fy, const double* fz, con
                 cudaStream_t st);
 // Drift + periodic wrap + max displacement since the last build (+ fixed point).
 // Per-atom periodic image counters (may be null: not tracked).
+// Three coordinate arrays (any may be null as a whole: x == nullptr).
+struct Pos3 {
+  double* x;
+  double* y;
+  double* z;
+};
 struct ImageRefs {
   int* c[3];
 };
 int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* z,
                  const double* vx, const double* vy, const double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
-                 uint4* atoms, const double* q, ImageRefs img, cudaStream_t st);
+                 uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st);
+// SHAKE / RATTLE of rigid three-atom clusters (rbx_shake.cu).
+struct ShakeParams {
+  double dt, b1sq, b2sq, b12sq, tol;
+  int max_iter;
+};
+int launch_inverse_perm(int n, const int* orig, int* where, cudaStream_t st);
+int launch_shake_a(const DBox& b, const ShakeParams& sp, int nc, const int* cl, const int* where,
+                   const int* type, const double* mass, Pos3 old, Pos3 pos, Pos3 vel,
+                   ImageRefs img, const double* x0, const double* y0, const double* z0,
+                   unsigned long long* max_d2, uint4* atoms, const double* q, int* status,
+                   cudaStream_t st);
+int launch_shake_b(const DBox& b, int nc, const int* cl, const int* where, const int* type,
+                   const double* mass, Pos3 pos, Pos3 vel, int* status, cudaStream_t st);
 int launch_to_fixed(const DBox& b, int n, const double* x, const double* y, const double* z,
                     const double* q, uint4* atoms, cudaStream_t st);
 int launch_max_disp(const DBox& b, int n, const double* x, const double* y, const double* z,

@@ -100,6 +100,7 @@ EXPORTS = [
     "rbx_engine_get_images", "rbx_engine_write_trajectory", "rbx_engine_create_from_files",
     "rbx_engine_get_system", "rbx_engine_get_atoms", "rbx_engine_get_type_params",
     "rbx_lammps_gauss_velocities", "rbx_engine_set_nose_hoover", "rbx_engine_get_thermostat",
+    "rbx_engine_set_shake", "rbx_engine_get_shake",
 ]
 
 
@@ -178,6 +179,8 @@ def lib():
     L.rbx_lammps_gauss_velocities.argtypes = [vp, dp, C.c_char_p, ip]
     L.rbx_engine_set_nose_hoover.argtypes = [vp, dp, dp, dp, C.c_int64, dp, dp, dp]
     L.rbx_engine_get_thermostat.argtypes = [vp, vp, vp, vp]
+    L.rbx_engine_set_shake.argtypes = [vp, ip, vp, dp, dp]
+    L.rbx_engine_get_shake.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.rbx_lammps_read.restype = vp
     L.rbx_lammps_read.argtypes = [C.c_char_p, C.c_char_p, vp]
     L.rbx_lammps_free.argtypes = [vp]
@@ -391,6 +394,7 @@ class Engine:
             prm.sigma = self._sigma.ctypes.data_as(C.POINTER(C.c_double))
             prm.eps = self._eps.ctypes.data_as(C.POINTER(C.c_double))
             prm.mass = self._mass.ctypes.data_as(C.POINTER(C.c_double))
+            prm.fmt2v = float(p.get("fmt2v", 0.0))
             h = L.rbx_engine_create(C.byref(prm), C.byref(self.box), self.n, device)
         if not h:
             raise RbxError(f"rbx_engine_create failed: {last_error()}")
@@ -522,6 +526,18 @@ class Engine:
         """NVT with RBMD's Nose-Hoover chain; t_damp <= 0 goes back to NVE."""
         check(lib().rbx_engine_set_nose_hoover(self._h, t_start, t_stop, t_damp, int(num_steps),
                                                kb, mvv2e, tdof), "rbx_engine_set_nose_hoover")
+
+    def set_shake(self, clusters, bond=1.0, angle=109.47):
+        """SHAKE / RATTLE clusters [nc, 3] of host atom indices, centre second."""
+        cl = np.ascontiguousarray(clusters, dtype=np.int32).reshape(-1, 3)
+        self._shake = cl
+        check(lib().rbx_engine_set_shake(self._h, len(cl), _np_ptr(cl), float(bond), float(angle)),
+              "rbx_engine_set_shake")
+
+    def shake_status(self):
+        nc, bad = C.c_int(0), C.c_int(0)
+        check(lib().rbx_engine_get_shake(self._h, C.byref(nc), C.byref(bad)), "rbx_engine_get_shake")
+        return nc.value, bad.value
 
     def thermostat(self):
         t = np.zeros(1)

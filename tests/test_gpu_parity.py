@@ -795,3 +795,87 @@ def test_engine_from_files_matches_arrays(cuda, rbx, tmp_path, rep, velocities):
         assert a.thermostat()["eta_dot"][0] != 0
     a.close()
     b.close()
+
+
+def _water_geometry(s, pos, vel):
+    """Largest bond / H-H distance error and largest bond-direction relative
+    velocity (the RATTLE condition) over all molecules."""
+    L = np.asarray(s["hi"]) - np.asarray(s["lo"])
+    cl = s["clusters"]
+
+    def vec(a, b):
+        d = pos[a] - pos[b]
+        return d - L * np.rint(d / L)
+    r01, r12, r02 = vec(cl[:, 1], cl[:, 0]), vec(cl[:, 2], cl[:, 1]), vec(cl[:, 2], cl[:, 0])
+    hh = 2 * np.sin(np.radians(systems.WATER_ANGLE) / 2)
+    err = max(np.abs(np.linalg.norm(r01, axis=1) - 1).max(),
+              np.abs(np.linalg.norm(r12, axis=1) - 1).max(),
+              np.abs(np.linalg.norm(r02, axis=1) - hh).max())
+    rv = max(np.abs(((vel[cl[:, 1]] - vel[cl[:, 0]]) * r01).sum(1)).max(),
+             np.abs(((vel[cl[:, 2]] - vel[cl[:, 1]]) * r12).sum(1)).max())
+    return err, rv
+
+
+@pytest.fixture(scope="module")
+def water3k():
+    return systems.water(3000, seed=11)
+
+
+def _water_nvt(e, s):
+    p = s["params"]
+    e.set_shake(s["clusters"], systems.WATER_BOND, systems.WATER_ANGLE)
+    e.compute_forces(0)
+    e.set_nose_hoover(298.0, 298.0, 100.0, kb=p["kb"], mvv2e=p["mvv2e"],
+                      tdof=3 * s["n"] - 3 - s["n"])
+
+
+def test_shake_water_matches_oracle(cuda, rbx, oracle, water3k):
+    """Rigid water (9,000 atoms, REAL units) under SHAKE / RATTLE and the
+    Nose-Hoover chain: the engine's steps agree with the oracle's, the bonds
+    hold to the solver's tolerance and the bond-direction velocities vanish."""
+    s = water3k
+    e = rbx.Engine(s, precision=rbx.PLAIN_FP64, seed=77)
+    ref = oracle.Engine(s, seed=77)
+    ref.set_shake(s["clusters"], systems.WATER_BOND, systems.WATER_ANGLE)
+    ref.compute_forces(0)
+    p = s["params"]
+    ref.set_nose_hoover(298.0, 298.0, 100.0, kb=p["kb"], mvv2e=p["mvv2e"],
+                        tdof=3 * s["n"] - 3 - s["n"])
+    _water_nvt(e, s)
+    for k in range(3):
+        e.step(4)
+        ref.step(4)
+        a, b = e.get_state(), ref.get()
+        order = np.argsort(b["gid"])
+        assert np.abs(a["pos"] - b["pos"][order]).max() < 1e-8, k
+        assert systems.rel_rms(a["vel"], b["vel"][order]) < 1e-8, k
+        assert systems.rel_rms(a["force"], b["force"][order]) < 1e-8, k
+        err, rv = _water_geometry(s, a["pos"], a["vel"])
+        assert err < 1e-4 and rv < 1e-9, (err, rv)
+        ta, tb = e.thermostat(), ref.thermostat()
+        assert abs(ta["temperature"] - tb["temperature"]) < 1e-8 * tb["temperature"]
+    assert e.shake_status() == (3000, 0) and ref.shake_failures == 0
+    e.close()
+
+
+def test_shake_water_graph_and_mixed(cuda, rbx, water3k):
+    """The step graph with SHAKE and the thermostat equals the launch-by-launch
+    step bit for bit (mixed form, rebuilds included), and holds the geometry."""
+    s = water3k
+    runs = []
+    for graph in (True, False):
+        e = rbx.Engine(s, precision=rbx.MIXED, seed=77)
+        e.set_step_graph(graph)
+        _water_nvt(e, s)
+        e.step(10)
+        e.step(15)
+        runs.append((e.get_state(), e.stats(), e.images()))
+        assert e.shake_status()[1] == 0
+        e.close()
+    (a, sa, ia), (b, sb, ib) = runs
+    for key in ("pos", "vel", "force"):
+        assert np.array_equal(a[key], b[key]), key
+    assert np.array_equal(ia, ib)
+    assert sa.rebuilds == sb.rebuilds and sa.rebuilds >= 1
+    err, rv = _water_geometry(s, a["pos"], a["vel"])
+    assert err < 1e-4 and rv < 1e-9, (err, rv)
