@@ -1156,8 +1156,7 @@ int rbx_engine::shake_a(cudaStream_t s) {
   ETRY(launch_inverse_perm(n, orig, where, s));
   return launch_shake_a(dbox, shp, shake_nc, shake_cl, where, type, mass_d, Pos3{xs, ys, zs},
                         Pos3{x, y, z}, Pos3{vx, vy, vz}, ImageRefs{{img[0], img[1], img[2]}}, x0,
-                        y0, z0, max_d2, prm.precision == RBX_MIXED ? atoms : nullptr, q,
-                        dflags + 6, s);
+                        y0, z0, max_d2, atoms, q, dflags + 6, s);
 }
 
 int rbx_engine::shake_b(cudaStream_t s) {

@@ -11,6 +11,8 @@
 // velocities; ShakeB, after the second half kick, removes the velocity
 // components along the bonds of the new positions (a 3 x 3 linear solve).
 // One thread per cluster; clusters are disjoint, so no atomics on atoms.
+// ShakeA also refreshes the moved atoms' fixed-point records, which the list
+// screens of both precision forms read, and their skin-check displacement.
 // The reference recomputes the unconstrained update from copies of x and v
 // taken before the drift and the kick and copies its result over every atom;
 // here the unconstrained positions and half-step velocities are the ones the
