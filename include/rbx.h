@@ -358,6 +358,26 @@ int rbx_engine_set_nose_hoover(rbx_engine* e, double t_start, double t_stop, dou
 /* Current thermostat state: temperature (after the last step's scaling),
  * eta[3], eta_dot[3]; any pointer may be NULL. */
 int rbx_engine_get_thermostat(rbx_engine* e, double* temperature, double* eta, double* eta_dot);
+/* CVFF special bonds on the RBL pair force (ComputeSpecialLJCutCoulRBLForce,
+ * src/force/src/cvff_op/rocm/cvff_op.hip.cu:401-533): row h of special
+ * ([n][maxspecial], atom indices in the order given to rbx_engine_set_state)
+ * lists atom h's 1-2, then 1-3, then 1-4 partners, nspecial[h] ([n][3]) the
+ * cumulative counts; a listed pair's LJ is scaled by its weight w and its
+ * Coulomb loses (1 - w) times the bare Coulomb, so w = 0 excludes it from
+ * real space and cancels its k-space part.  Weights of
+ * hyper_parameters.extend.special_bonds.  maxspecial = 0 switches it off.
+ * The bonded CVFF terms (bond, angle, dihedral, improper) are not computed. */
+int rbx_engine_set_special(rbx_engine* e, int maxspecial, const int* nspecial,
+                           const int* special, double w12, double w13, double w14);
+/* Special rows from the topology as LammpsFullReader builds them
+ * (lammps_full_reader.cpp:2101-2230): bonds [nbonds][2] give 1-2 pairs,
+ * angles [nangles][3] their end atoms (1-3), dihedrals [ndihedrals][4] their
+ * end atoms (1-4), 0-based atom indices; a repeated pair keeps its first
+ * band.  Writes *maxspecial; fills nspecial [n][3] and special
+ * [n][*maxspecial] when both are non-NULL (call once for the size). */
+int rbx_special_build(int n, int nbonds, const int64_t* bonds, int nangles,
+                      const int64_t* angles, int ndihedrals, const int64_t* dihedrals,
+                      int* maxspecial, int* nspecial, int* special);
 /* SHAKE / RATTLE of rigid three-atom clusters (RBMD's ShakeA / ShakeB,
  * shake_controller_op.hip.cu:19-660, serial path shake_controller.cpp:2130-2220):
  * clusters [nclusters][3] are atom indices in the order given to

@@ -7,6 +7,7 @@ package.  Each wrapper names the RBMD 2.0 source it restates.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -91,6 +92,11 @@ def lib():
                                           _dp, _dp, C.c_int, _ip, _ip, _ip, _ip, _dp, _dp,
                                           _dp]),
             "orc_fix_rbl": (None, [C.c_int, _dp, _dp, _dp, _dp]),
+            "orc_pair_force_rbl_special": (None, [C.c_int, B, C.c_double, C.c_double, C.c_int,
+                                                  C.c_double, C.c_double, _ip, C.c_int, _dp, _dp,
+                                                  _ip, _dp, _dp, _dp, _dp, C.c_int, _ip, _ip,
+                                                  _ip, _ip, _ip, _ip, C.c_int, C.c_double,
+                                                  C.c_double, C.c_double, _dp, _dp, _dp]),
             "orc_pair_force_verlet": (None, [C.c_int, B, C.c_double, C.c_double, C.c_double,
                                              _ip, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int, _ip,
                                              _ip, _dp, _dp, _dp, _dp,
@@ -294,6 +300,34 @@ def pair_force_rbl(box, r_core, cut_off, freq, alpha, qqr2e, typ, sigma, eps, q,
     lib().orc_pair_force_rbl(n, C.byref(box), r_core, cut_off, freq, alpha, qqr2e, _i(typ),
                              _d(sigma), _d(eps), _d(q), _d(x), _d(y), _d(z), cap,
                              _i(core_count), _i(core), _i(shell_count), _i(shell), *f)
+    return np.stack(f, axis=1)
+
+
+def pair_force_rbl_special(box, r_core, cut_off, freq, alpha, qqr2e, typ, sigma, eps, gid, q,
+                           x, y, z, core_count, core, shell_count, shell, nspecial, special,
+                           weights):
+    """ComputeSpecialLJCutCoulRBLForce (cvff_op.hip.cu:401-533), no mean removal.
+    nspecial [n, 3] / special [n, maxs] are indexed like the atoms and hold
+    partner gids."""
+    n, cap = core.shape
+    nt = len(sigma)
+    sig = np.asarray(sigma, float)
+    ep = np.asarray(eps, float)
+    lj12 = np.zeros(nt * nt)
+    lj6 = np.zeros(nt * nt)
+    for a in range(nt):  # CVFF::Init (cvff.cpp:855-870)
+        for b in range(nt):
+            e_ab = math.sqrt(ep[a] * ep[b])
+            s_ab = (sig[a] + sig[b]) * 0.5
+            s6 = (s_ab * s_ab) ** 3
+            lj12[a * nt + b] = 48.0 * e_ab * s6 * s6
+            lj6[a * nt + b] = 24.0 * e_ab * s6
+    sp = np.ascontiguousarray(special, dtype=np.int32)
+    f = [np.zeros(n) for _ in range(3)]
+    lib().orc_pair_force_rbl_special(n, C.byref(box), r_core, cut_off, freq, alpha, qqr2e,
+                                     _i(typ), nt, _d(lj12), _d(lj6), _i(gid), _d(q), _d(x), _d(y),
+                                     _d(z), cap, _i(core_count), _i(core), _i(shell_count),
+                                     _i(shell), _i(nspecial), _i(sp), sp.shape[1], *weights, *f)
     return np.stack(f, axis=1)
 
 

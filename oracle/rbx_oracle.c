@@ -730,6 +730,84 @@ void orc_pair_force_rbl(int n, const orc_box* box, double r_core, double cut_off
   }
 }
 
+/* ComputeSpecialLJCutCoulRBLForce (src/force/src/cvff_op/rocm/cvff_op.hip.cu:401-533),
+ * CVFF's RBL pair force: LJ from the type-pair tables 48 eps sigma^12 and
+ * 24 eps sigma^6 (CVFF::Init, cvff.cpp:855-870; LJForceFromTypePair :387-398),
+ * both multiplied by the special-bond weight of the pair, and the erfc
+ * Coulomb minus (1 - weight) times the bare Coulomb -qqr2e qi qj / r^3 (not
+ * multiplied by pice_num in the shell).  The weight of partner gid g in row i
+ * (LookupSpecialWeight :79-110): w12 / w13 / w14 by its position against the
+ * cumulative counts nspecial[i][0..2] (clamped as LoadSpecialCounts :51-77),
+ * 1 when g is absent. */
+static double special_weight(const int* ns, const int* row, int maxs, int g, double w12,
+                             double w13, double w14) {
+  int n12 = ns[0] < 0 ? 0 : ns[0], n13 = ns[1] < 0 ? 0 : ns[1], n14 = ns[2] < 0 ? 0 : ns[2];
+  if (n12 > n13) n13 = n12;
+  if (n13 > n14) n14 = n13;
+  if (n14 > maxs) n14 = maxs;
+  if (n13 > n14) n13 = n14;
+  if (n12 > n13) n12 = n13;
+  for (int k = 0; k < n14; ++k)
+    if (row[k] == g) return k < n12 ? w12 : (k < n13 ? w13 : w14);
+  return 1.0;
+}
+
+void orc_pair_force_rbl_special(int n, const orc_box* box, double r_core, double cut_off,
+                                int freq, double alpha, double qqr2e, const int* type,
+                                int ntypes, const double* lj12, const double* lj6,
+                                const int* gid, const double* q, const double* x,
+                                const double* y, const double* z, int cap,
+                                const int* core_count, const int* core, const int* shell_count,
+                                const int* shell, const int* nspecial, const int* special,
+                                int maxs, double w12, double w13, double w14, double* fx,
+                                double* fy, double* fz) {
+  const double rs2 = r_core * r_core, rc2 = cut_off * cut_off;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < n; ++i) {
+    const int ti = type[i];
+    const double qi = q[i];
+    double f3[3] = {0, 0, 0};
+    for (int pass = 0; pass < 2; ++pass) {
+      const int cnt = pass == 0 ? core_count[i] : shell_count[i];
+      const int* lst = pass == 0 ? core : shell;
+      const double lo = pass == 0 ? ORC_EPSILON : rs2, hi = pass == 0 ? rs2 : rc2;
+      const double mult = pass == 0 ? 1.0 : (double)freq;
+      for (int t = 0; t < cnt; ++t) {
+        const int j = lst[(size_t)i * cap + t];
+        if (j == i) continue;
+        const int pair = ti * ntypes + type[j];
+        double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+        min_image_while(box, &dx, &dy, &dz);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        double flj = 0.0;
+        if (d2 > lo && d2 < hi) {
+          const double r2inv = 1.0 / d2, r6inv = r2inv * r2inv * r2inv;
+          flj = -mult * r2inv * r6inv * (lj12[pair] * r6inv - lj6[pair]);
+        }
+        const double w = special ? special_weight(nspecial + 3 * (size_t)i,
+                                                  special + (size_t)i * maxs, maxs, gid[j],
+                                                  w12, w13, w14)
+                                 : 1.0;
+        double fc = 0.0, bare = 0.0;
+        if (d2 < hi && d2 > lo) {
+          const double dis = sqrt(d2);
+          const double g = (1.0 - erf(sqrt(alpha) * dis)) / d2 +
+                           2 * sqrt(alpha) * exp(-alpha * d2) / (sqrt(M_PI) * dis);
+          bare = -qqr2e * qi * q[j] / pow(dis, 3.0);
+          fc = -mult * qqr2e * qi * q[j] * g / dis;
+        }
+        const double f = w * flj + (fc - (1 - w) * bare);
+        f3[0] += f * dx;
+        f3[1] += f * dy;
+        f3[2] += f * dz;
+      }
+    }
+    fx[i] = f3[0];
+    fy[i] = f3[1];
+    fz[i] = f3[2];
+  }
+}
+
 /* LJCutCoulKspace::ComputeLJRBL mean-force removal (lj_cut_coul_kspace.cpp:537-563)
  * + FixRBLForce (src/force/src/force_op/rocm/force_op.hip.cu:9-45). */
 void orc_fix_rbl(int n, double* fx, double* fy, double* fz, double mean_out[3]) {

@@ -95,6 +95,17 @@ void orc_pair_force_rbl(int n, const orc_box* box, double r_core, double cut_off
                         int cap, const int* core_count, const int* core,
                         const int* shell_count, const int* shell, double* fx,
                         double* fy, double* fz);
+/* CVFF RBL pair force with special-bond weights (specials indexed by atom
+ * index i, partners as gids; special may be NULL). */
+void orc_pair_force_rbl_special(int n, const orc_box* box, double r_core, double cut_off,
+                                int freq, double alpha, double qqr2e, const int* type,
+                                int ntypes, const double* lj12, const double* lj6,
+                                const int* gid, const double* q, const double* x,
+                                const double* y, const double* z, int cap,
+                                const int* core_count, const int* core, const int* shell_count,
+                                const int* shell, const int* nspecial, const int* special,
+                                int maxs, double w12, double w13, double w14, double* fx,
+                                double* fy, double* fz);
 void orc_fix_rbl(int n, double* fx, double* fy, double* fz, double mean_out[3]);
 void orc_pair_force_verlet(int n, const orc_box* box, double cut_off,
                            double alpha, double qqr2e, const int* type,

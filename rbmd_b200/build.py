@@ -18,9 +18,10 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librbx.so")
 
 CU_SOURCES = ["rbx_capi.cu", "rbx_rbe.cu", "rbx_pair.cu", "rbx_cells.cu", "rbx_engine.cu",
-              "rbx_batch.cu", "rbx_adjoint.cu", "rbx_thermo.cu", "rbx_shake.cu"]
+              "rbx_batch.cu", "rbx_adjoint.cu", "rbx_thermo.cu", "rbx_shake.cu",
+              "rbx_special.cu"]
 CXX_SOURCES = ["host/config_data.cpp", "host/lj_cut_coul_kspace.cpp", "host/lammps_data.cpp",
-               "host/md_files.cpp"]
+               "host/md_files.cpp", "host/special_bonds.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -152,7 +152,7 @@ int rbx_engine::init() {
   ETRY(alloc(&max_d2, 1));
   ETRY(alloc(&cand_total, 1));
   nfpart = rbl_fused_blocks(n);
-  ETRY(alloc(&fpart, (size_t)nfpart * 3));
+  ETRY(alloc(&fpart, (size_t)(nfpart + SPEC_PARTS) * 3));
   ETRY(alloc(&epart, (size_t)nfpart * 8));
   ETRY(alloc(&mean, 3));
   ETRY(alloc(&ek, 1));
@@ -413,9 +413,15 @@ int rbx_engine::check_rebuild(bool disp_from_drift) {
 
 int rbx_engine::real_space(const int* epoch_dev) {
   const bool mixed = prm.precision == RBX_MIXED;
-  if (prm.neighbor_type == RBX_NEIGHBOR_RBL)
-    return launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, epoch_dev,
-                            cand_count, cand, cap, fpx, fpy, fpz, fpart, nrbl, dflags + 3, st);
+  if (prm.neighbor_type == RBX_NEIGHBOR_RBL) {
+    ETRY(launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, epoch_dev,
+                          cand_count, cand, cap, fpx, fpy, fpz, fpart, nrbl, dflags + 3, st));
+    if (!spec_natoms) return RBX_OK;
+    ETRY(launch_inverse_perm(n, orig, where, st));
+    return launch_special_rbl(pp, spec_natoms, spec_atoms, spec_cnt, spec_part, spec_max,
+                              spec_w[0], spec_w[1], spec_w[2], where, x, y, z, q, type, key_a,
+                              key_b, epoch, epoch_dev, fpx, fpy, fpz, fpart + (size_t)nrbl * 3, st);
+  }
   return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, fpx, fpy,
                                  fpz, nullptr, epart, nfpart, st);
 }
@@ -437,7 +443,8 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
   }
   ETRY(launch_rbe_finalize(dbox, P, P > 0 ? nparts : 0, part_re, part_im, mx, my, mz, prm.alpha,
                            S, prm.qqr2e, qsq, qsum, P > 0 ? rho_re : nullptr, rho_im,
-                           P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr, rbl ? nrbl : 0,
+                           P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr,
+                           rbl ? nrbl + (spec_natoms ? SPEC_PARTS : 0) : 0,
                            fpart, n, rbl ? mean : nullptr, kterm, st));
   RbeForceOut o;
   o.f_pair_x = fpx;
@@ -1152,6 +1159,58 @@ int rbx_engine::set_shake(int nclusters, const int* clusters, double bond, doubl
   return cuda_ok(cudaStreamSynchronize(st), "set_shake sync");
 }
 
+// CVFF special bonds (LammpsFullReader's special rows, cvff_op.hip.cu
+// LookupSpecialWeight): row h lists partner atoms in host order, 1-2 first,
+// nspecial[h] the cumulative counts; maxspecial = 0 switches it off.
+int rbx_engine::set_special(int maxspecial, const int* nspecial, const int* special, double w12,
+                            double w13, double w14) {
+  cudaSetDevice(device);
+  graph_dirty = true;
+  spec_natoms = 0;
+  if (maxspecial <= 0) return RBX_OK;
+  if (prm.neighbor_type != RBX_NEIGHBOR_RBL) {
+    set_error("special bonds are applied on the RBL pair force only");
+    return RBX_ERR_INVALID;
+  }
+  std::vector<int> list;
+  for (int h = 0; h < n; ++h) {
+    const int c = std::min(std::max(nspecial[3 * h + 2], 0), maxspecial);
+    bool any = false;
+    for (int k = 0; k < c; ++k) {
+      const int p = special[(size_t)h * maxspecial + k];
+      if (p < 0 || p >= n) {
+        set_error("special partner %d of atom %d outside [0, %d)", p, h, n);
+        return RBX_ERR_INVALID;
+      }
+      any = true;
+    }
+    if (any) list.push_back(h);
+  }
+  if (maxspecial > spec_cap) {
+    ETRY(alloc(&spec_part, (size_t)n * maxspecial));
+    spec_cap = maxspecial;
+  }
+  spec_max = maxspecial;
+  if (!spec_cnt) {
+    ETRY(alloc(&spec_cnt, (size_t)3 * n));
+    ETRY(alloc(&spec_atoms, (size_t)n));
+  }
+  if (!where) ETRY(alloc(&where, (size_t)n));
+  ETRY(cuda_ok(cudaMemcpy(spec_cnt, nspecial, sizeof(int) * 3 * n, cudaMemcpyHostToDevice), "H2D"));
+  ETRY(cuda_ok(cudaMemcpy(spec_part, special, sizeof(int) * (size_t)n * maxspecial,
+                          cudaMemcpyHostToDevice),
+               "H2D"));
+  if (!list.empty())
+    ETRY(cuda_ok(cudaMemcpy(spec_atoms, list.data(), sizeof(int) * list.size(),
+                            cudaMemcpyHostToDevice),
+                 "H2D"));
+  spec_w[0] = w12;
+  spec_w[1] = w13;
+  spec_w[2] = w14;
+  spec_natoms = (int)list.size();
+  return RBX_OK;
+}
+
 int rbx_engine::shake_a(cudaStream_t s) {
   ETRY(launch_inverse_perm(n, orig, where, s));
   return launch_shake_a(dbox, shp, shake_nc, shake_cl, where, type, mass_d, Pos3{xs, ys, zs},
@@ -1449,6 +1508,12 @@ int rbx_engine_set_nose_hoover(rbx_engine* e, double t_start, double t_stop, dou
 int rbx_engine_get_thermostat(rbx_engine* e, double* temperature, double* eta, double* eta_dot) {
   if (!e) return RBX_ERR_INVALID;
   return e->get_thermostat(temperature, eta, eta_dot);
+}
+
+int rbx_engine_set_special(rbx_engine* e, int maxspecial, const int* nspecial,
+                           const int* special, double w12, double w13, double w14) {
+  if (!e || (maxspecial > 0 && (!nspecial || !special))) return RBX_ERR_INVALID;
+  return e->set_special(maxspecial, nspecial, special, w12, w13, w14);
 }
 
 int rbx_engine_set_shake(rbx_engine* e, int nclusters, const int* clusters, double bond,

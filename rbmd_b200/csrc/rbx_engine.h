@@ -80,6 +80,15 @@ struct rbx_engine {
   int shake_a(cudaStream_t s);
   int shake_b(cudaStream_t s);
   int set_shake(int nclusters, const int* clusters, double bond, double angle_deg);
+  // CVFF special bonds (host order): cumulative 1-2/1-3/1-4 counts [n][3],
+  // partner host indices [n][spec_max], the atoms that have any, weights
+  int spec_max = 0, spec_cap = 0, spec_natoms = 0;
+  int* spec_cnt = nullptr;
+  int* spec_part = nullptr;
+  int* spec_atoms = nullptr;
+  double spec_w[3] = {1, 1, 1};
+  int set_special(int maxspecial, const int* nspecial, const int* special, double w12,
+                  double w13, double w14);
   double *lj_eps = nullptr, *lj_s6 = nullptr;
   unsigned long long* h_pinned = nullptr;
 

@@ -247,6 +247,15 @@ int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* 
                  const double* vx, const double* vy, const double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
                  uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st);
+// CVFF special-bond correction of the RBL pair force (rbx_special.cu): its
+// SPEC_PARTS per-block force sums follow the fused kernel's in fpart.
+constexpr int SPEC_PARTS = 148;
+int launch_special_rbl(const PairParams& pp, int natoms, const int* atoms_h, const int* cnt,
+                       const int* part, int maxs, double w12, double w13, double w14,
+                       const int* where, const double* x, const double* y, const double* z,
+                       const double* q, const int* type, const unsigned long long* key_a,
+                       const unsigned long long* key_b, int epoch, const int* epoch_dev,
+                       double* fx, double* fy, double* fz, double* fpart, cudaStream_t st);
 // SHAKE / RATTLE of rigid three-atom clusters (rbx_shake.cu).
 struct ShakeParams {
   double dt, b1sq, b2sq, b12sq, tol;

@@ -100,7 +100,7 @@ EXPORTS = [
     "rbx_engine_get_images", "rbx_engine_write_trajectory", "rbx_engine_create_from_files",
     "rbx_engine_get_system", "rbx_engine_get_atoms", "rbx_engine_get_type_params",
     "rbx_lammps_gauss_velocities", "rbx_engine_set_nose_hoover", "rbx_engine_get_thermostat",
-    "rbx_engine_set_shake", "rbx_engine_get_shake",
+    "rbx_engine_set_shake", "rbx_engine_get_shake", "rbx_engine_set_special", "rbx_special_build",
 ]
 
 
@@ -181,6 +181,8 @@ def lib():
     L.rbx_engine_get_thermostat.argtypes = [vp, vp, vp, vp]
     L.rbx_engine_set_shake.argtypes = [vp, ip, vp, dp, dp]
     L.rbx_engine_get_shake.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.rbx_engine_set_special.argtypes = [vp, ip, vp, vp, dp, dp, dp]
+    L.rbx_special_build.argtypes = [ip, ip, vp, ip, vp, ip, vp, C.POINTER(C.c_int), vp, vp]
     L.rbx_lammps_read.restype = vp
     L.rbx_lammps_read.argtypes = [C.c_char_p, C.c_char_p, vp]
     L.rbx_lammps_free.argtypes = [vp]
@@ -534,6 +536,15 @@ class Engine:
         check(lib().rbx_engine_set_shake(self._h, len(cl), _np_ptr(cl), float(bond), float(angle)),
               "rbx_engine_set_shake")
 
+    def set_special(self, nspecial, special, weights=(0.0, 0.0, 0.0)):
+        """CVFF special-bond rows (rbx_special_build's output) and weights
+        (hyper_parameters.extend.special_bonds)."""
+        ns = np.ascontiguousarray(nspecial, dtype=np.int32).reshape(self.n, 3)
+        sp = np.ascontiguousarray(special, dtype=np.int32).reshape(self.n, -1)
+        self._special = (ns, sp)
+        check(lib().rbx_engine_set_special(self._h, sp.shape[1], _np_ptr(ns), _np_ptr(sp),
+                                           *[float(w) for w in weights]), "rbx_engine_set_special")
+
     def shake_status(self):
         nc, bad = C.c_int(0), C.c_int(0)
         check(lib().rbx_engine_get_shake(self._h, C.byref(nc), C.byref(bad)), "rbx_engine_get_shake")
@@ -689,3 +700,20 @@ def write_lammps_charge(path, sys: dict):
         [np.ascontiguousarray(vel[:, d]) for d in range(3)]
     check(lib().rbx_lammps_write_charge(str(path).encode(), C.byref(box), n, nt,
                                         *[_np_ptr(v) for v in a]), "rbx_lammps_write_charge")
+
+
+def special_build(n, bonds=None, angles=None, dihedrals=None):
+    """rbx_special_build: (nspecial [n, 3], special [n, maxspecial]) from
+    0-based bonds [nb, 2], angles [na, 3], dihedrals [nd, 4]."""
+    L = lib()
+    arrs = [np.ascontiguousarray(np.zeros((0, k)) if a is None else a, dtype=np.int64).reshape(-1, k)
+            for a, k in ((bonds, 2), (angles, 3), (dihedrals, 4))]
+    ms = C.c_int(0)
+    args = [int(n)]
+    for a in arrs:
+        args += [len(a), _np_ptr(a)]
+    check(L.rbx_special_build(*args, C.byref(ms), None, None), "rbx_special_build")
+    ns = np.zeros((n, 3), np.int32)
+    sp = np.zeros((n, max(ms.value, 1)), np.int32)
+    check(L.rbx_special_build(*args, C.byref(ms), _np_ptr(ns), _np_ptr(sp)), "rbx_special_build")
+    return ns, sp[:, :ms.value]

@@ -879,3 +879,87 @@ def test_shake_water_graph_and_mixed(cuda, rbx, water3k):
     assert sa.rebuilds == sb.rebuilds and sa.rebuilds >= 1
     err, rv = _water_geometry(s, a["pos"], a["vel"])
     assert err < 1e-4 and rv < 1e-9, (err, rv)
+
+
+def _oracle_special_pair_force(oracle, s, nspecial, special, weights, epoch):
+    """The oracle's CVFF RBL pair force (mean removed) in host order."""
+    p = s["params"]
+    box = oracle.Box.make(s["lo"], s["hi"])
+    cols = [np.ascontiguousarray(s["pos"][:, d]) for d in range(3)]
+    perm, cell, cs, ce = oracle.cells_sort(box, p["cut_off"] + p["skin"], *cols)
+    pos = s["pos"][perm]
+    xyz = [np.ascontiguousarray(pos[:, d]) for d in range(3)]
+    gid = np.ascontiguousarray(s["gid"][perm], dtype=np.int32)
+    cnt, rows = oracle.full_list(box, p["cut_off"] + p["skin"], *xyz, cell, cs, ce)
+    freq, _, _ = oracle.rbl_params(s["n"], box, p["r_core"], p["cut_off"], p["neighbor_sample_num"])
+    cc, core, sc, shell = oracle.rbl_filter(box, p["r_core"], p["cut_off"], freq, epoch, gid, *xyz,
+                                            cnt, rows)
+    sp_gid = np.asarray(s["gid"])[special[perm]]  # partners as gids, rows in oracle order
+    f = oracle.pair_force_rbl_special(box, p["r_core"], p["cut_off"], freq, p["alpha"], p["qqr2e"],
+                                      s["type"][perm].astype(np.int32), s["sigma"], s["eps"], gid,
+                                      s["q"][perm], *xyz, cc, core, sc, shell,
+                                      np.ascontiguousarray(nspecial[perm]), sp_gid, weights)
+    f, _ = oracle.fix_rbl(f)
+    out = np.empty_like(f)
+    out[perm] = f
+    return out
+
+
+def _random_specials(s, rng, per_atom=3):
+    """Symmetric special rows of random neighbour pairs within cut_off (core
+    and shell), bands 1-2 / 1-3 / 1-4 drawn at random."""
+    n, L = s["n"], np.asarray(s["hi"]) - np.asarray(s["lo"])
+    pos = s["pos"]
+    bonds, angles, dih = [], [], []
+    for i in rng.choice(n, size=n // 8, replace=False):
+        d = pos - pos[i]
+        d -= L * np.rint(d / L)
+        r = np.linalg.norm(d, axis=1)
+        near = np.nonzero((r > 0) & (r < s["params"]["cut_off"]))[0]
+        for j in rng.choice(near, size=per_atom, replace=False):
+            band = rng.integers(3)
+            if band == 0:
+                bonds.append((i, j))
+            elif band == 1:
+                angles.append((i, -1, j))
+            else:
+                dih.append((i, -1, -1, j))
+    return bonds, angles, dih
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_special_bonds_lj_electrolyte(cuda, rbx, oracle, prec):
+    """CVFF special-bond weights on the RBL pair force (core and sampled shell
+    pairs, weights 0 / 0.5 / 0.8) against the oracle's restatement of
+    ComputeSpecialLJCutCoulRBLForce + mean removal."""
+    s = systems.lj_electrolyte(4000, seed=19)
+    rng = np.random.default_rng(5)
+    bonds, angles, dih = _random_specials(s, rng)
+    ns, sp = rbx.special_build(s["n"], bonds, angles, dih)
+    w = (0.0, 0.5, 0.8)
+    e = rbx.Engine(s, precision=prec, seed=3)
+    e.set_special(ns, sp, w)
+    for epoch in (0, 3):
+        e.compute_forces(epoch)
+        fp, _ = e.force_parts()
+        want = _oracle_special_pair_force(oracle, s, ns, sp, w, epoch)
+        plain = _oracle_special_pair_force(oracle, s, ns, sp, (1.0, 1.0, 1.0), epoch)
+        assert systems.rel_rms(want, plain) > 1e-3  # the weights matter
+        assert systems.rel_rms(fp, want) < (1e-10 if prec == 0 else 1e-5), epoch
+    e.close()
+
+
+def test_special_bonds_water(cuda, rbx, oracle, water3k):
+    """Water with special_bonds [0, 0, 0] (the reference's water config): the
+    intramolecular O-H and H-H pairs leave real space and their k-space part
+    is cancelled; pair force against the oracle."""
+    s = water3k
+    ns, sp = rbx.special_build(s["n"], s["bonds"], s["angles"])
+    assert (ns[0::3] == [2, 2, 2]).all() and (ns[1::3] == [1, 2, 2]).all()
+    e = rbx.Engine(s, precision=rbx.PLAIN_FP64, seed=3)
+    e.set_special(ns, sp, (0.0, 0.0, 0.0))
+    e.compute_forces(2)
+    fp, _ = e.force_parts()
+    want = _oracle_special_pair_force(oracle, s, ns, sp, (0.0, 0.0, 0.0), 2)
+    assert systems.rel_rms(fp, want) < 1e-10
+    e.close()

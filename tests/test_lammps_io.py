@@ -265,3 +265,42 @@ def test_gauss_velocities_errors(rbx, tmp_path, args, needle):
     rbx.write_lammps_charge(path, s)
     with pytest.raises(rbx.RbxError, match=needle.replace("[", r"\[").replace("]", r"\]")):
         rbx.read_lammps(path, gauss=args)
+
+
+def _special_reference(n, bonds, angles, dihedrals):
+    """LammpsFullReader's special rows restated (lammps_full_reader.cpp:2101-2230)."""
+    rows = [[] for _ in range(n)]
+    seen = set()
+    for band, items, a, b in ((0, bonds, 0, 1), (1, angles, 0, 2), (2, dihedrals, 0, 3)):
+        for t in items:
+            i, j = int(t[a]), int(t[b])
+            if i < 0 or j < 0 or i == j or (min(i, j), max(i, j)) in seen:
+                continue
+            seen.add((min(i, j), max(i, j)))
+            rows[i].append((j, band))
+            rows[j].append((i, band))
+    return rows
+
+
+def test_special_build_matches_reader_rule(rbx):
+    rng = np.random.default_rng(3)
+    n = 300
+    bonds = rng.integers(0, n, size=(400, 2))
+    angles = rng.integers(0, n, size=(300, 3))
+    dih = rng.integers(0, n, size=(200, 4))
+    ns, sp = rbx.special_build(n, bonds, angles, dih)
+    rows = _special_reference(n, bonds, angles, dih)
+    assert sp.shape[1] == max(len(r) for r in rows)
+    for i, r in enumerate(rows):
+        assert list(sp[i, :len(r)]) == [j for j, _ in r]
+        c = [sum(1 for _, b in r if b == k) for k in range(3)]
+        assert list(ns[i]) == [c[0], c[0] + c[1], c[0] + c[1] + c[2]]
+
+
+def test_special_build_water(rbx):
+    s = systems.water(50, seed=2)
+    ns, sp = rbx.special_build(s["n"], s["bonds"], s["angles"])
+    o = np.arange(50) * 3
+    assert (sp[o] == np.stack([o + 1, o + 2], 1)).all()
+    assert (sp[o + 1] == np.stack([o, o + 2], 1)).all()
+    assert (ns[o + 1] == [1, 2, 2]).all()
