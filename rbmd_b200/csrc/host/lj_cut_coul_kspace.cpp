@@ -136,8 +136,11 @@ void LJCutCoulKspace::Init() {
       _cfg.PathExists({"hyper_parameters", "force_field", "type"})
           ? _cfg.Get<std::string>("type", "hyper_parameters", "force_field")
           : std::string("LJ/CUT/COUL/LONG");
-  if (ff != "LJ/CUT/COUL/LONG")
-    throw std::runtime_error("force_field.type " + ff + " is not LJ/CUT/COUL/LONG");
+  // CVFF (src/force/src/cvff.cpp) runs the same RBL / RBE force with
+  // special-bond weights on the pair term; its bonded terms are not part of
+  // this engine (rigid water under SHAKE does not feel them).
+  if (ff != "LJ/CUT/COUL/LONG" && ff != "CVFF")
+    throw std::runtime_error("force_field.type " + ff + " is not LJ/CUT/COUL/LONG or CVFF");
   const std::string unit = _cfg.PathExists({"init_configuration", "read_data", "unit"})
                                ? _cfg.Get<std::string>("unit", "init_configuration", "read_data")
                                : std::string("LJ");

@@ -9,12 +9,14 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "config_data.h"
 #include "lammps_data.h"
 #include "lj_cut_coul_kspace.h"
 #include "rbx.h"
+#include "special_bonds.h"
 #include "units.h"
 
 namespace rbx {
@@ -22,6 +24,7 @@ void set_error(const char* fmt, ...);
 }
 
 namespace rbx_host {
+
 namespace {
 
 std::string read_text(const std::string& path) {
@@ -168,6 +171,52 @@ rbx_engine* create_from_files(const std::string& json_path, int precision, int d
                              " is not provided by this engine (NVE, NVT)");
   }
 
+  // hyper_parameters.extend: fix_shake (every angle a rigid cluster, the
+  // reference's serial ShakeA) and special_bonds (CVFF; read_special_bond_weights,
+  // cvff.cpp:309-330, default 1 1 1)
+  const bool shake = cfg.PathExists({"hyper_parameters", "extend", "fix_shake"}) &&
+                     cfg.Get<bool>("fix_shake", "hyper_parameters", "extend");
+  const std::string ff = cfg.PathExists({"hyper_parameters", "force_field", "type"})
+                             ? cfg.Get<std::string>("type", "hyper_parameters", "force_field")
+                             : std::string("LJ/CUT/COUL/LONG");
+  double w[3] = {1.0, 1.0, 1.0};
+  if (ff == "CVFF" && cfg.PathExists({"hyper_parameters", "extend", "special_bonds"})) {
+    const auto v = cfg.GetArray<double>("special_bonds", "hyper_parameters", "extend");
+    for (size_t k = 0; k < v.size() && k < 3; ++k) w[k] = v[k];
+  }
+  // topology by host index (file order) instead of atom id
+  std::unordered_map<int64_t, int> host_of_id;
+  for (int i = 0; i < n; ++i) host_of_id[d.id[i]] = i;
+  auto to_host = [&](const std::vector<int64_t>& ids) {
+    std::vector<int64_t> h(ids.size());
+    for (size_t k = 0; k < ids.size(); ++k) {
+      const auto it = host_of_id.find(ids[k]);
+      if (it == host_of_id.end())
+        throw std::runtime_error("topology names atom id " + std::to_string(ids[k] + 1) +
+                                 " that is not in Atoms");
+      h[k] = it->second;
+    }
+    return h;
+  };
+  std::vector<int> clusters;
+  if (shake) {
+    for (int64_t h : to_host(d.angle_atoms)) clusters.push_back((int)h);
+    if (clusters.empty()) throw std::runtime_error("fix_shake needs Angles (rigid clusters)");
+  }
+  std::vector<int> nspecial, special;
+  int maxspecial = 0;
+  if (ff == "CVFF" && (w[0] != 1.0 || w[1] != 1.0 || w[2] != 1.0)) {
+    const auto hb = to_host(d.bond_atoms), ha = to_host(d.angle_atoms),
+               hd = to_host(d.dihedral_atoms);
+    const auto rows = build_special(n, (int)d.bond_type.size(), hb.data(),
+                                    (int)d.angle_type.size(), ha.data(),
+                                    (int)d.dihedral_type.size(), hd.data());
+    maxspecial = rows.maxspecial;
+    nspecial.resize(3 * (size_t)n);
+    special.resize((size_t)n * std::max(maxspecial, 1));
+    fill_special(rows, nspecial.data(), special.data());
+  }
+
   LJCutCoulKspace plugin(text, box, n, nt, d.pair_sigma.data(), d.pair_eps.data(), d.mass.data(),
                          q.data(), precision, device);
   plugin.Init();
@@ -176,8 +225,13 @@ rbx_engine* create_from_files(const std::string& json_path, int precision, int d
   if (rbx_engine_set_state(e, gid.data(), type.data(), q.data(), pos[0].data(), pos[1].data(),
                            pos[2].data(), vel[0].data(), vel[1].data(), vel[2].data()) != RBX_OK ||
       rbx_engine_set_images(e, image.data()) != RBX_OK ||
-      (!nh.empty() && rbx_engine_set_nose_hoover(e, nh[0], nh[1], nh[2], num_steps, u.kb,
-                                                 u.mvv2e, 0.0) != RBX_OK)) {
+      (shake && rbx_engine_set_shake(e, (int)clusters.size() / 3, clusters.data(), 1.0,
+                                     109.47) != RBX_OK) ||
+      (maxspecial > 0 && rbx_engine_set_special(e, maxspecial, nspecial.data(), special.data(),
+                                                w[0], w[1], w[2]) != RBX_OK) ||
+      (!nh.empty() &&
+       rbx_engine_set_nose_hoover(e, nh[0], nh[1], nh[2], num_steps, u.kb, u.mvv2e,
+                                  shake ? 3.0 * n - 3.0 - n : 0.0) != RBX_OK)) {
     const std::string msg = rbx_last_error();
     rbx_engine_destroy(e);
     throw std::runtime_error(msg);

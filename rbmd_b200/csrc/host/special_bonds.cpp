@@ -10,18 +10,13 @@
 #include <vector>
 
 #include "rbx.h"
+#include "special_bonds.h"
 
 namespace rbx {
 void set_error(const char* fmt, ...);
 }
 
 namespace rbx_host {
-
-struct SpecialRows {
-  int maxspecial = 0;
-  std::vector<std::vector<int>> part;
-  std::vector<std::vector<int>> band;
-};
 
 SpecialRows build_special(int n, int nb, const int64_t* bonds, int na, const int64_t* angles,
                           int nd, const int64_t* dihedrals) {

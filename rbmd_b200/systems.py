@@ -103,9 +103,10 @@ WATER_PARAMS = {
     "kspace_p": 300,
     "qqr2e": 332.06371,      # REAL
     "dt": 2.0,               # fs
-    "fmt2v": 4.186e-4,       # UnitFactor<REAL>::_fmt2v
-    "kb": 1.9872067e-3,
-    "mvv2e": 1.0 / 4.186e-4,
+    # UnitFactor<REAL> (src/common/unit_factor.cpp:37-42), the same expressions
+    "fmt2v": 4.186 * 10.0 ** -4.0,
+    "kb": 1.9872067 * 10.0 ** -3.0,
+    "mvv2e": 1.0 / (4.186 * 10.0 ** -4.0),
 }
 WATER_BOND, WATER_ANGLE = 1.0, 109.47
 

@@ -963,3 +963,73 @@ def test_special_bonds_water(cuda, rbx, oracle, water3k):
     want = _oracle_special_pair_force(oracle, s, ns, sp, (0.0, 0.0, 0.0), 2)
     assert systems.rel_rms(fp, want) < 1e-10
     e.close()
+
+
+def _write_water_full(path, s):
+    """A LAMMPS data file (atom_style full) of a systems.water dict."""
+    n, nm = s["n"], s["n"] // 3
+    lines = ["water", "", f"{n} atoms", f"{len(s['bonds'])} bonds", f"{len(s['angles'])} angles",
+             "2 atom types", "1 bond types", "1 angle types", ""]
+    for d, ax in enumerate("xyz"):
+        lines.append(f"{s['lo'][d]!r} {s['hi'][d]!r} {ax}lo {ax}hi")
+    lines += ["", "Masses", ""] + [f"{t + 1} {m!r}" for t, m in enumerate(s["mass"])]
+    lines += ["", "Pair Coeffs", ""] + [f"{t + 1} {e!r} {g!r}"
+                                        for t, (e, g) in enumerate(zip(s["eps"], s["sigma"]))]
+    lines += ["", "Bond Coeffs", "", "1 450.0 1.0", "", "Angle Coeffs", "", "1 55.0 109.47"]
+    lines += ["", "Atoms # full", ""]
+    for i in range(n):
+        x, y, z = (repr(float(v)) for v in s["pos"][i])
+        lines.append(f"{s['gid'][i] + 1} {i // 3 + 1} {s['type'][i] + 1} {s['q'][i]!r} {x} {y} {z}")
+    lines += ["", "Velocities", ""]
+    for i in range(n):
+        lines.append(f"{s['gid'][i] + 1} " + " ".join(repr(float(v)) for v in s["vel"][i]))
+    lines += ["", "Bonds", ""] + [f"{k + 1} 1 {a + 1} {b + 1}" for k, (a, b) in enumerate(s["bonds"])]
+    lines += ["", "Angles", ""] + [f"{k + 1} 1 {a + 1} {b + 1} {c + 1}"
+                                   for k, (a, b, c) in enumerate(s["angles"])]
+    path.write_text("\n".join(lines) + "\n")
+
+
+WATER_JSON = """{
+  "init_configuration": {"read_data": {"file": "water.data", "unit": "REAL",
+                                       "atom_style": "full", "velocity_type": "NONE"}},
+  "hyper_parameters": {
+    "force_field": {"type": "CVFF", "mixing_rule": "arithmetic"},
+    "neighbor": {"type": "RBL", "cut_off": 10, "r_core": 6.5, "neighbor_sample_num": 100,
+                 "energy_rbl_flag": "no", "skin": 2},
+    "coulomb": {"type": "RBE", "alpha": 0.09, "coulomb_sample_num": 300,
+                "energy_rbe_flag": "no", "random_seed": 21},
+    "extend": {"fix_shake": true, "special_bonds": [0, 0, 0]}},
+  "execution": {"ensemble": "NVT", "temperature": [298, 298, 100],
+                "temp_ctrl_type": "NOSE_HOOVER", "timestep": 2.0, "num_steps": 1000}
+}"""
+
+
+def test_water_config_from_files(cuda, rbx, tmp_path, water3k):
+    """RBMD's water workload from its own kind of input (CVFF, RBL + RBE,
+    fix_shake, special_bonds [0 0 0], NVT Nose-Hoover, REAL units, a full-style
+    data file): the engine built from the files steps exactly like the one
+    assembled from arrays with set_shake / set_special / set_nose_hoover."""
+    s = water3k
+    _write_water_full(tmp_path / "water.data", s)
+    (tmp_path / "rbmd.json").write_text(WATER_JSON)
+    a = rbx.Engine.from_files(tmp_path / "rbmd.json", precision=rbx.MIXED)
+    assert a.shake_status() == (3000, 0)
+    b = rbx.Engine(s, precision=rbx.MIXED, seed=21)
+    b.set_shake(s["clusters"][:, [0, 1, 2]], 1.0, 109.47)
+    ns, sp = rbx.special_build(s["n"], s["bonds"], s["angles"])
+    b.set_special(ns, sp, (0.0, 0.0, 0.0))
+    b.compute_forces(0)
+    p = s["params"]
+    b.set_nose_hoover(298.0, 298.0, 100.0, num_steps=1000, kb=p["kb"], mvv2e=p["mvv2e"],
+                      tdof=2.0 * s["n"] - 3)
+    a.compute_forces(0)
+    for e in (a, b):
+        e.step(12)
+    sa, sb = a.get_state(), b.get_state()
+    for key in ("pos", "vel", "force"):
+        assert np.array_equal(sa[key], sb[key]), key
+    assert a.thermostat()["temperature"] == b.thermostat()["temperature"]
+    err, rv = _water_geometry(s, sa["pos"], sa["vel"])
+    assert err < 1e-4 and rv < 1e-9
+    a.close()
+    b.close()
