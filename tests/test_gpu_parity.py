@@ -971,15 +971,16 @@ def _write_water_full(path, s):
     lines = ["water", "", f"{n} atoms", f"{len(s['bonds'])} bonds", f"{len(s['angles'])} angles",
              "2 atom types", "1 bond types", "1 angle types", ""]
     for d, ax in enumerate("xyz"):
-        lines.append(f"{s['lo'][d]!r} {s['hi'][d]!r} {ax}lo {ax}hi")
-    lines += ["", "Masses", ""] + [f"{t + 1} {m!r}" for t, m in enumerate(s["mass"])]
-    lines += ["", "Pair Coeffs", ""] + [f"{t + 1} {e!r} {g!r}"
+        lines.append(f"{float(s['lo'][d])!r} {float(s['hi'][d])!r} {ax}lo {ax}hi")
+    lines += ["", "Masses", ""] + [f"{t + 1} {float(m)!r}" for t, m in enumerate(s["mass"])]
+    lines += ["", "Pair Coeffs", ""] + [f"{t + 1} {float(e)!r} {float(g)!r}"
                                         for t, (e, g) in enumerate(zip(s["eps"], s["sigma"]))]
     lines += ["", "Bond Coeffs", "", "1 450.0 1.0", "", "Angle Coeffs", "", "1 55.0 109.47"]
     lines += ["", "Atoms # full", ""]
     for i in range(n):
         x, y, z = (repr(float(v)) for v in s["pos"][i])
-        lines.append(f"{s['gid'][i] + 1} {i // 3 + 1} {s['type'][i] + 1} {s['q'][i]!r} {x} {y} {z}")
+        lines.append(f"{s['gid'][i] + 1} {i // 3 + 1} {s['type'][i] + 1} {float(s['q'][i])!r} "
+                     f"{x} {y} {z}")
     lines += ["", "Velocities", ""]
     for i in range(n):
         lines.append(f"{s['gid'][i] + 1} " + " ".join(repr(float(v)) for v in s["vel"][i]))
