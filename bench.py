@@ -443,6 +443,107 @@ def run_batched(args):
     return 0
 
 
+def run_water(args):
+    """Rigid water (the reference's water workload: CVFF with special_bonds
+    [0 0 0], RBL + RBE, SHAKE / RATTLE, Nose-Hoover NVT at 298 K, REAL units,
+    dt = 2 fs): 24,327 molecules / 72,981 atoms in a 90 A box.  The lattice
+    start is first equilibrated (untimed, mixed form, thermostat 100 fs) so
+    the timed steps see liquid at ~300 K with its normal rebuild rate; both
+    forms then start from that state.  Reports device time per step of each
+    form, the mixed form's force error against plain FP64 on the same state
+    and k-samples, and the constraint residuals after the run."""
+    import torch
+
+    from rbmd_b200 import rbx, systems
+
+    s = systems.water(args.water_mol, seed=7, kspace_p=args.water_p)
+    p = s["params"]
+    L = np.asarray(s["hi"]) - np.asarray(s["lo"])
+    ns, sp = rbx.special_build(s["n"], s["bonds"], s["angles"])
+    tdof = 2.0 * s["n"] - 3  # 3N - 3 - N with SHAKE (Computedof)
+
+    def make(sysd, precision, seed=77):
+        e = rbx.Engine(sysd, precision=precision, seed=seed)
+        e.set_shake(s["clusters"], systems.WATER_BOND, systems.WATER_ANGLE)
+        e.set_special(ns, sp, (0.0, 0.0, 0.0))
+        return e
+
+    # untimed equilibration from the lattice
+    e = make(s, rbx.MIXED, seed=5)
+    e.compute_forces(0)
+    e.set_nose_hoover(298.0, 298.0, 100.0, kb=p["kb"], mvv2e=p["mvv2e"], tdof=tdof)
+    e.step(args.water_equil)
+    st0 = e.get_state()
+    t_equil = e.thermostat()["temperature"]
+    e.close()
+    s_eq = dict(s, pos=st0["pos"], vel=st0["vel"])
+
+    # force accuracy of the mixed form, same state and k-samples
+    from oracle import oracle as O
+
+    m = O.rbe_sample_philox(O.Box.make(s["lo"], s["hi"]), p["alpha"], args.water_p, 5, 0)
+    forces = {}
+    for prec in (rbx.PLAIN_FP64, rbx.MIXED):
+        e = make(s_eq, prec)
+        e.set_k_samples(*m)
+        e.compute_forces(0)
+        forces[prec] = e.force_parts()
+        e.close()
+    err = {"force": systems.rel_rms(sum(forces[1]), sum(forces[0])),
+           "pair": systems.rel_rms(forces[1][0], forces[0][0]),
+           "kspace": systems.rel_rms(forces[1][1], forces[0][1])}
+
+    out = {}
+    for name, prec in (("mixed", rbx.MIXED), ("fp64_plain", rbx.PLAIN_FP64)):
+        e = make(s_eq, prec)
+        e.compute_forces(0)
+        e.set_nose_hoover(298.0, 298.0, 100.0, kb=p["kb"], mvv2e=p["mvv2e"], tdof=tdof)
+        e.step(args.warmup)
+        r0 = e.stats().rebuilds
+        st = torch.cuda.ExternalStream(e.stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(st)
+        e.step(args.steps)
+        ev1.record(st)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        rebuilds = e.stats().rebuilds - r0
+        e.set_profiling(True)
+        e.step(args.steps)
+        ph = e.phase_ms()
+        stt = e.get_state()
+        cl = s["clusters"]
+        d = stt["pos"][cl[:, 1]] - stt["pos"][cl[:, 0]]
+        d -= L * np.rint(d / L)
+        out[name] = {"value": s["n"] * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                     "phase_ms": {"kick_drift_shake": ph[0], "skin_check_rebuild": ph[1],
+                                  "real_space_special": ph[2],
+                                  "kspace_kick_rattle_thermostat": ph[3]},
+                     "rebuilds_in_timed_steps": rebuilds, "shake_failures": e.shake_status()[1],
+                     "bond_error_max": float(np.abs(np.linalg.norm(d, axis=1) - 1.0).max()),
+                     "temperature_end": e.thermostat()["temperature"]}
+        e.close()
+    line = {
+        "metric": "rigid water (CVFF special bonds, RBL + RBE, SHAKE, NVT): atom-steps/s",
+        "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": out["mixed"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak",
+        "dtype": "mixed(u32 fixed-point, f32 SFU, f64 reductions/integrator)",
+        "data": "synthetic",
+        "config": {"workload": f"{args.water_mol} rigid 3-site waters ({s['n']} atoms), L = "
+                               f"{float(L[0]):.2f} A, REAL, cut_off 10 r_core 6.5 skin 2, "
+                               f"RBE alpha 0.09 P={args.water_p}, special_bonds [0 0 0], SHAKE "
+                               f"(1.0 A, 109.47 deg), Nose-Hoover 298 K / 100 fs, dt = 2 fs",
+                   "equilibration_steps": args.water_equil, "temperature_after_equil": t_equil},
+        "mixed": out["mixed"], "fp64_plain": out["fp64_plain"],
+        "mixed_over_fp64": out["mixed"]["value"] / out["fp64_plain"]["value"],
+        "mixed_rel_force_err": err,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_gradient(args):
     """Force-field fitting gradient (the gradient recipe): N atoms, three types,
     16 frames every 50 steps of an MD run at theta*, a fixed k-sample per frame;
@@ -561,6 +662,11 @@ def main():
     ap.add_argument("--gradient", action="store_true",
                     help="force-field gradient measurement instead of the headline line")
     ap.add_argument("--grad-n", type=int, default=20000)
+    ap.add_argument("--water", action="store_true",
+                    help="rigid-water (CVFF, SHAKE, NVT) measurement instead of the headline line")
+    ap.add_argument("--water-mol", type=int, default=24327)
+    ap.add_argument("--water-p", type=int, default=200)
+    ap.add_argument("--water-equil", type=int, default=1500)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -570,6 +676,8 @@ def main():
         return run_batched(args)
     if args.gradient:
         return run_gradient(args)
+    if args.water:
+        return run_water(args)
     return run_ours(args)
 
 
