@@ -112,11 +112,13 @@ WATER_BOND, WATER_ANGLE = 1.0, 109.47
 
 
 def water(n_mol: int, seed: int = 7, density: float = 0.0334, temperature: float = 298.0,
-          jitter: float = 0.3, **overrides) -> dict:
+          jitter: float = 0.15, **overrides) -> dict:
     """n_mol rigid waters (3 n_mol atoms: O, H, H per molecule, types 0 = O,
     1 = H) in a cubic box at `density` molecules / A^3, centres on a jittered
-    simple-cubic lattice, random orientations, Maxwell-Boltzmann velocities
-    of the rigid bodies' atoms at `temperature` K with zero net momentum.
+    simple-cubic lattice, random orientations redrawn for any molecule with an
+    atom closer than 1.7 A to another molecule's atom (hydrogens carry no LJ
+    core, so such a contact would collapse), Maxwell-Boltzmann velocities of
+    the rigid bodies' atoms at `temperature` K with zero net momentum.
     Returns the lj_electrolyte-style dict plus 'clusters' (H, O, H atom
     indices per molecule), 'bonds' and 'angles' (0-based atom indices)."""
     rng = np.random.default_rng(seed)
@@ -128,24 +130,40 @@ def water(n_mol: int, seed: int = 7, density: float = 0.0334, temperature: float
     sites = rng.choice(side ** 3, size=n_mol, replace=False)
     cen = (np.stack([sites % side, (sites // side) % side, sites // (side * side)], 1) + 0.5)
     cen = cen * spacing + rng.uniform(-jitter, jitter, size=(n_mol, 3))
-    # random orthonormal frames from normalised Gaussian quaternions
-    qv = rng.normal(size=(n_mol, 4))
-    qv /= np.linalg.norm(qv, axis=1, keepdims=True)
-    w, a, b, c = qv.T
-    R = np.stack([np.stack([1 - 2 * (b * b + c * c), 2 * (a * b - c * w), 2 * (a * c + b * w)], 1),
-                  np.stack([2 * (a * b + c * w), 1 - 2 * (a * a + c * c), 2 * (b * c - a * w)], 1),
-                  np.stack([2 * (a * c - b * w), 2 * (b * c + a * w), 1 - 2 * (a * a + b * b)], 1)],
-                 1)
     half = math.radians(WATER_ANGLE) / 2
     h1 = WATER_BOND * np.array([math.sin(half), math.cos(half), 0.0])
     h2 = WATER_BOND * np.array([-math.sin(half), math.cos(half), 0.0])
     n = 3 * n_mol
+
+    def frames(m):
+        # random orthonormal frames from normalised Gaussian quaternions
+        qv = rng.normal(size=(m, 4))
+        qv /= np.linalg.norm(qv, axis=1, keepdims=True)
+        w, a, b, c = qv.T
+        return np.stack(
+            [np.stack([1 - 2 * (b * b + c * c), 2 * (a * b - c * w), 2 * (a * c + b * w)], 1),
+             np.stack([2 * (a * b + c * w), 1 - 2 * (a * a + c * c), 2 * (b * c - a * w)], 1),
+             np.stack([2 * (a * c - b * w), 2 * (b * c + a * w), 1 - 2 * (a * a + b * b)], 1)], 1)
+
+    R = frames(n_mol)
     pos = np.empty((n, 3))
-    pos[0::3] = cen
-    pos[1::3] = cen + np.einsum("mij,j->mi", R, h1)
-    pos[2::3] = cen + np.einsum("mij,j->mi", R, h2)
-    pos = np.mod(pos, L)
-    pos[pos >= L] -= L
+    mol = np.repeat(np.arange(n_mol), 3)
+    for _ in range(200):
+        pos[0::3] = cen
+        pos[1::3] = cen + np.einsum("mij,j->mi", R, h1)
+        pos[2::3] = cen + np.einsum("mij,j->mi", R, h2)
+        pos = np.mod(pos, L)
+        pos[pos >= L] -= L
+        from scipy.spatial import cKDTree
+
+        pairs = cKDTree(pos, boxsize=L).query_pairs(1.7, output_type="ndarray")
+        pairs = pairs[mol[pairs[:, 0]] != mol[pairs[:, 1]]]
+        if len(pairs) == 0:
+            break
+        bad = np.unique(mol[pairs.ravel()])
+        R[bad] = frames(len(bad))
+    else:
+        raise RuntimeError("water: could not place the molecules without close contacts")
     typ = np.tile(np.array([0, 1, 1], dtype=np.int32), n_mol)
     mass = np.array([15.9994, 1.008])
     p = dict(WATER_PARAMS)
