@@ -444,10 +444,12 @@ def run_batched(args):
 
 
 def run_water(args):
-    """Rigid water (the reference's water workload: CVFF with special_bonds
-    [0 0 0], RBL + RBE, SHAKE / RATTLE, Nose-Hoover NVT at 298 K, REAL units,
-    dt = 2 fs): 24,327 molecules / 72,981 atoms in a 90 A box.  The lattice
-    start is first equilibrated (untimed, mixed form, thermostat 100 fs) so
+    """Rigid water with the settings of the reference's water workload
+    (benchmark/systems/water.json: CVFF with special_bonds [0 0 0], RBL
+    cut_off 10 r_core 6.5 skin 2, RBE P = 300, SHAKE, Nose-Hoover NVT at
+    298 K with 10 fs damping, dt = 0.5 fs, REAL units): 24,327 molecules /
+    72,981 atoms in a 90 A box.  The lattice start is first equilibrated
+    (untimed, mixed form, same settings) so
     the timed steps see liquid at ~300 K with its normal rebuild rate; both
     forms then start from that state.  Reports device time per step of each
     form, the mixed form's force error against plain FP64 on the same state
@@ -456,9 +458,10 @@ def run_water(args):
 
     from rbmd_b200 import rbx, systems
 
-    s = systems.water(args.water_mol, seed=7, kspace_p=args.water_p)
+    s = systems.water(args.water_mol, seed=7, kspace_p=args.water_p, dt=args.water_dt)
     p = s["params"]
     L = np.asarray(s["hi"]) - np.asarray(s["lo"])
+    damp = args.water_damp
     ns, sp = rbx.special_build(s["n"], s["bonds"], s["angles"])
     tdof = 2.0 * s["n"] - 3  # 3N - 3 - N with SHAKE (Computedof)
 
@@ -471,7 +474,7 @@ def run_water(args):
     # untimed equilibration from the lattice
     e = make(s, rbx.MIXED, seed=5)
     e.compute_forces(0)
-    e.set_nose_hoover(298.0, 298.0, 100.0, kb=p["kb"], mvv2e=p["mvv2e"], tdof=tdof)
+    e.set_nose_hoover(298.0, 298.0, damp, kb=p["kb"], mvv2e=p["mvv2e"], tdof=tdof)
     e.step(args.water_equil)
     st0 = e.get_state()
     t_equil = e.thermostat()["temperature"]
@@ -497,7 +500,7 @@ def run_water(args):
     for name, prec in (("mixed", rbx.MIXED), ("fp64_plain", rbx.PLAIN_FP64)):
         e = make(s_eq, prec)
         e.compute_forces(0)
-        e.set_nose_hoover(298.0, 298.0, 100.0, kb=p["kb"], mvv2e=p["mvv2e"], tdof=tdof)
+        e.set_nose_hoover(298.0, 298.0, damp, kb=p["kb"], mvv2e=p["mvv2e"], tdof=tdof)
         e.step(args.warmup)
         r0 = e.stats().rebuilds
         st = torch.cuda.ExternalStream(e.stream)
@@ -534,7 +537,8 @@ def run_water(args):
         "config": {"workload": f"{args.water_mol} rigid 3-site waters ({s['n']} atoms), L = "
                                f"{float(L[0]):.2f} A, REAL, cut_off 10 r_core 6.5 skin 2, "
                                f"RBE alpha 0.09 P={args.water_p}, special_bonds [0 0 0], SHAKE "
-                               f"(1.0 A, 109.47 deg), Nose-Hoover 298 K / 100 fs, dt = 2 fs",
+                               f"(1.0 A, 109.47 deg), Nose-Hoover 298 K / {damp} fs, "
+                               f"dt = {args.water_dt} fs",
                    "equilibration_steps": args.water_equil, "temperature_after_equil": t_equil},
         "mixed": out["mixed"], "fp64_plain": out["fp64_plain"],
         "mixed_over_fp64": out["mixed"]["value"] / out["fp64_plain"]["value"],
@@ -665,8 +669,10 @@ def main():
     ap.add_argument("--water", action="store_true",
                     help="rigid-water (CVFF, SHAKE, NVT) measurement instead of the headline line")
     ap.add_argument("--water-mol", type=int, default=24327)
-    ap.add_argument("--water-p", type=int, default=200)
-    ap.add_argument("--water-equil", type=int, default=1500)
+    ap.add_argument("--water-p", type=int, default=300)
+    ap.add_argument("--water-dt", type=float, default=0.5)
+    ap.add_argument("--water-damp", type=float, default=10.0)
+    ap.add_argument("--water-equil", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
