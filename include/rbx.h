@@ -142,6 +142,61 @@ int rbx_ewald_force(const rbx_box* box, int num_atoms, const int kmax[3],
                     double* fx, double* fy, double* fz, double* energy,
                     void* stream);
 
+/* RBSOG (random-batch sum of Gaussians) k-space, coulomb.type "RBSOG"
+ * (KSpaceCalculator::Init RBSOG branch, kspace_calculator.cpp:253-330;
+ * RBSOGInit / RBSOGSetup :988-1140; ComputeRBSOG :1331-1543).
+ * Parameters of hyper_parameters.coulomb.rbsog_level (0..4) at this cut_off
+ * and box: Gaussian base b, width sigma = sigma_at_rc10 cut_off / 10, count
+ * mmax, w0, the sampling normalisation S (and S_npt) as RBSOGSetup computes
+ * them, the self-energy coefficient (E_self = -self_coeff sum q^2 qqr2e) and
+ * the VERLET-SOG Taylor coefficients (LJCoulSOGInit,
+ * lj_cut_coul_kspace.cpp:651-711).  Host only. */
+typedef struct {
+  int level, mmax;
+  double b, sigma, w0, S, S_npt, self_coeff;
+  double taylor[6];
+  int n_direct;             /* |m|^2 <= 1 vectors summed directly (6) */
+  double S_full;            /* the sampled density's full normalisation,
+                               sum of G^(m)|k|^2 over |m|^2 > 1.  RBSOGSetup's S
+                               keeps only the l = 0 Gaussian's high-k sum (its
+                               loop's stop value is not reset between
+                               Gaussians), so S / S_full < 1 (0.44 - 0.89 by
+                               level) scales the reference's sampled far field */
+} rbx_rbsog_info;
+/* coef [mmax], direct_m [n_direct][3], direct_fb [n_direct] may be NULL. */
+int rbx_rbsog_params(int level, double cut_off, const rbx_box* box, rbx_rbsog_info* out,
+                     double* coef, int* direct_m, double* direct_fb);
+/* p integer k-samples (device arrays, values integral) from p(m) ~ G^(m)|k|^2
+ * on |m|^2 > 1, the density RBSOGSampleKSpace's Metropolis chain targets
+ * (kspace_calculator.cpp:1142-1240), drawn exactly and independently on the
+ * device (Philox4x32-10, counter = sample, attempt, step; key = seed). */
+int rbx_rbsog_sample(const rbx_box* box, int level, double cut_off, int p, uint64_t seed,
+                     int64_t step, double* mx, double* my, double* mz, void* stream);
+/* RBSOG k-space force of the p samples plus the six |m| = 1 vectors
+ * (ComputeRBSOGSampleForceOp + ComputeRBSOGDirectForceOp + their energies
+ * and the self energy, kspace_calculator.cpp:1380-1535, NVT/NVE factors
+ * fac = 1).  S = 0 uses RBSOGSetup's S (the reference's forces), S < 0
+ * the full normalisation S_full (an unbiased far field), S > 0 that value;
+ * qsqsum = sum q^2.  Device arrays;
+ * energy (host, may be NULL).  The virial is not computed. */
+int rbx_rbsog_force(const rbx_box* box, int level, double cut_off, double qqr2e, double S,
+                    double qsqsum, int num_atoms, int p, const double* charge, const double* mx,
+                    const double* my, const double* mz, const double* px, const double* py,
+                    const double* pz, double* fx, double* fy, double* fz, double* energy,
+                    void* stream);
+/* VERLET-SOG pair force over a full candidate list (LJCutCoulForceUserOp:
+ * ComputeLJCutCoulForceUserKernel with lj126 and CoulCutForceUser,
+ * lj_cut_coul_kspace_op.hip.cu:196-254, 357-470): LJ 12-6 plus the
+ * short-range SOG Coulomb inside cut_off.  sigma / eps per type (host);
+ * energy (host, may be NULL) receives {E_LJ, E_coul}, half-counted.  The
+ * per-atom virial is not computed. */
+int rbx_pair_force_verlet_sog(const rbx_box* box, int level, double cut_off, double qqr2e,
+                              int num_atoms, int ntypes, const double* sigma, const double* eps,
+                              const int* type, const double* charge, const double* px,
+                              const double* py, const double* pz, int cap, const int* cand_count,
+                              const int* cand, double* fx, double* fy, double* fz,
+                              double* energy, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Neighbor-list ops (device pointers)                                       */
 /* ------------------------------------------------------------------------ */

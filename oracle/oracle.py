@@ -74,6 +74,20 @@ def lib():
             "orc_rbe_sample_philox": (C.c_int, [C.c_int, B, C.c_double, C.c_uint64,
                                                 C.c_int64, _dp, _dp, _dp]),
             "orc_rbe_sample_mh": (None, [C.c_int, B, C.c_double, C.c_uint64, _dp, _dp, _dp]),
+            "orc_rbsog_params": (C.c_int, [C.c_int, C.c_double, B, _dp, _dp, _ip, _dp]),
+            "orc_rbsog_sample_philox": (C.c_int, [C.c_int, C.c_double, B, C.c_int, C.c_uint64,
+                                                  C.c_int64, _dp, _dp, _dp]),
+            "orc_rbsog_sample_mh": (C.c_int, [C.c_int, C.c_double, B, C.c_int, C.c_uint64,
+                                              _dp, _dp, _dp]),
+            "orc_rbsog_force": (C.c_int, [C.c_int, C.c_double, B, C.c_double, C.c_double,
+                                          C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                          _dp, _dp, _dp, C.POINTER(C.c_double)]),
+            "orc_rbsog_far_exact": (C.c_int, [C.c_int, C.c_double, B, C.c_double, C.c_int, _dp,
+                                              _dp, _dp, _dp, C.c_int, _dp, _dp, _dp,
+                                              C.POINTER(C.c_double)]),
+            "orc_pair_force_verlet_sog": (None, [C.c_int, C.c_double, B, C.c_double, C.c_int,
+                                                 _ip, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int,
+                                                 _ip, _ip, _dp, _dp, _dp, _dp]),
             "orc_dist2": (C.c_double, [B] + [C.c_double] * 6),
             "orc_cell_grid": (C.c_int, [B, C.c_double, _ip]),
             "orc_cells_sort": (C.c_int, [C.c_int, B, C.c_double, _dp, _dp, _dp, _ip, _ip,
@@ -223,6 +237,66 @@ def rbe_sample_mh(box, alpha, p, seed):
     m = [np.zeros(p) for _ in range(3)]
     lib().orc_rbe_sample_mh(p, C.byref(box), alpha, seed, *m)
     return m
+
+
+# --- RBSOG ---------------------------------------------------------------------
+def rbsog_params(level, cut_off, box):
+    """RBSOGInit / RBSOGSetup / LJCoulSOGInit parameters (kspace_calculator.cpp:988-1140)."""
+    sc = np.zeros(13)
+    coef = np.zeros(128)
+    dm = np.zeros(18, dtype=np.int32)
+    dfb = np.zeros(6)
+    if lib().orc_rbsog_params(level, cut_off, C.byref(box), sc, coef, dm, dfb) != 0:
+        raise ValueError("rbsog_level outside [0, 4]")
+    mmax = int(sc[0])
+    return {"mmax": mmax, "b": sc[1], "sigma": sc[2], "w0": sc[3], "S": sc[4], "S_npt": sc[5],
+            "self_coeff": sc[6], "taylor": sc[7:13].copy(), "coef": coef[:mmax].copy(),
+            "direct_m": dm.reshape(6, 3), "direct_fb": dfb}
+
+
+def rbsog_sample_philox(level, cut_off, box, p, seed, step):
+    m = [np.zeros(p) for _ in range(3)]
+    if lib().orc_rbsog_sample_philox(level, cut_off, C.byref(box), p, seed, step, *m) != 0:
+        raise RuntimeError("RBSOG philox sampler failed")
+    return m
+
+
+def rbsog_sample_mh(level, cut_off, box, p, seed):
+    """RBSOGSampleKSpace's Metropolis chain (kspace_calculator.cpp:1142-1240)."""
+    m = [np.zeros(p) for _ in range(3)]
+    lib().orc_rbsog_sample_mh(level, cut_off, C.byref(box), p, seed, *m)
+    return m
+
+
+def rbsog_force(level, cut_off, box, qqr2e, q, m, x, y, z, S=0.0):
+    """ComputeRBSOG's k-space force and energy for the samples m (+ the 6 direct vectors)."""
+    n, p = len(q), len(m[0])
+    f = [np.zeros(n) for _ in range(3)]
+    e = C.c_double()
+    lib().orc_rbsog_force(level, cut_off, C.byref(box), qqr2e, S, n, p, _d(q), *[_d(v) for v in m],
+                          _d(x), _d(y), _d(z), *f, C.byref(e))
+    return np.stack(f, axis=1), e.value
+
+
+def rbsog_far_exact(level, cut_off, box, qqr2e, q, x, y, z, mcut):
+    """Exact far field over |m_d| <= mcut, |m|^2 > 1; returns (F, S_full)."""
+    n = len(q)
+    f = [np.zeros(n) for _ in range(3)]
+    sf = C.c_double()
+    lib().orc_rbsog_far_exact(level, cut_off, C.byref(box), qqr2e, n, _d(q), _d(x), _d(y), _d(z),
+                              mcut, *f, C.byref(sf))
+    return np.stack(f, axis=1), sf.value
+
+
+def pair_force_verlet_sog(level, cut_off, box, qqr2e, typ, sigma, eps, q, x, y, z, count, rows):
+    """LJCutCoulForceUserOp (lj_cut_coul_kspace_op.hip.cu:196-254, 357-470)."""
+    n, cap = rows.shape
+    f = [np.zeros(n) for _ in range(3)]
+    en = np.zeros(2)
+    lib().orc_pair_force_verlet_sog(level, cut_off, C.byref(box), qqr2e, n, _i(typ), _d(sigma),
+                                    _d(eps), _d(q), _d(x), _d(y), _d(z), cap, _i(count), _i(rows),
+                                    *f, en)
+    return np.stack(f, axis=1), en
 
 
 # --- lists -------------------------------------------------------------------

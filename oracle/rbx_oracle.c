@@ -1496,3 +1496,476 @@ int orc_engine_get(orc_engine* e, int* gid, double* x, double* y, double* z,
 }
 
 int orc_engine_rebuilds(const orc_engine* e) { return e->rebuilds; }
+
+/* ========================================================================== */
+/* RBSOG k-space and VERLET-SOG real space                                    */
+/* ========================================================================== */
+/* rbsog_level presets (src/force/include/rbsog_level_preset.h:14-38). */
+static const double kSogB[5] = {2.0, 1.62976708826776469, 1.48783512395703226,
+                                1.32070036405934420, 1.21812525709410644};
+static const double kSogSig[5] = {5.027010924194599, 3.633717409009413, 2.662784519725113,
+                                  2.277149356440992, 1.774456369233284};
+static const int kSogM[5] = {6, 16, 30, 64, 102};
+
+typedef struct {
+  int mmax;
+  double b, sigma, w0, S, S_npt, self_coeff, taylor[6];
+  double coef[128], coef_npt[128];
+  int dm[18];
+  double dfb[6];
+} orc_sog;
+
+static double sog_g1(double r) { return exp(-r * r / 2.0) / sqrt(2 * M_PI); }
+
+/* G^(m) = sum_l coef_l exp(-(b^2)^l sigma^2 k^2 / 2) (KSpaceCalculator::Gaussian,
+ * kspace_calculator.cpp:1559-1573) */
+static double sog_ghat(const orc_sog* s, const double* coef, double k2) {
+  double sum = 0.0;
+  for (int l = 0; l < s->mmax; ++l)
+    sum += coef[l] * exp(-(pow(s->b * s->b, l + 0.0) * s->sigma * s->sigma) * k2 / 2.0);
+  return sum;
+}
+
+/* RBSOGInit + RBSOGSetup (:988-1140), Compute_W01 (RBEPSample.h:19-34),
+ * direct vectors and self term of ComputeRBSOG (:1423-1535), LJCoulSOGInit
+ * (lj_cut_coul_kspace.cpp:651-711).  S keeps the reference's l = 0-only
+ * high-k sum (its stop value is never reset between Gaussians). */
+static int sog_setup(int level, double cut_off, const orc_box* box, orc_sog* s) {
+  if (level < 0 || level > 4) return -1;
+  memset(s, 0, sizeof(*s));
+  s->b = kSogB[level];
+  s->sigma = kSogSig[level] * cut_off / 10.0;
+  s->mmax = kSogM[level];
+  const double L[3] = {box_len(box, 0), box_len(box, 1), box_len(box, 2)};
+  const double b = s->b, logb = log(b), r0 = cut_off / s->sigma;
+  double acc = 0.0;
+  for (int i = 1; i < 200; ++i) acc += pow(b, -i + 0.0) * sog_g1(pow(b, -i + 0.0) * r0);
+  s->w0 = (1.0 / sog_g1(r0)) * ((1.0 / (2 * logb * r0)) - acc);
+  const double sig2 = s->sigma * s->sigma, sig4 = sig2 * sig2;
+  s->coef[0] = 4 * M_PI * logb * s->w0 * sig2;
+  s->coef_npt[0] = 8 * M_PI * logb * s->w0 * sig4;
+  for (int l = 1; l < s->mmax; ++l) {
+    s->coef[l] = s->coef[l - 1] * (b * b);
+    s->coef_npt[l] = s->coef_npt[l - 1] * (b * b * b * b);
+  }
+  double low = 0.0, low_npt = 0.0;
+  const int ijk[4][3] = {{0, 0, 0}, {0, 0, 1}, {0, 1, 0}, {1, 0, 0}};
+  for (int t = 0; t < 4; ++t) {
+    double K[3], k2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      K[d] = (2 * M_PI / L[d]) * (ijk[t][d] + 0.00);
+      k2 += pow((ijk[t][d] + 0.00) * 2 * M_PI / L[d], 2);
+    }
+    const double K2 = K[0] * K[0] + K[1] * K[1] + K[2] * K[2];
+    low += 2 * sog_ghat(s, s->coef, k2) * K2;
+    low_npt += 2 * sog_ghat(s, s->coef_npt, k2) * (K2 * K2);
+  }
+  const double prd = fmax(L[0], fmax(L[1], L[2]));
+  double sum = 0.0, sum_npt = 0.0, bound = 1.0, sl = sqrt(2.0) * s->sigma;
+  for (int l = 0; l < s->mmax; ++l) {
+    if (l > 0) sl *= b;
+    double H[3] = {0, 0, 0}, Y[3] = {0, 0, 0}, Z[3] = {0, 0, 0};
+    for (int j = 1; bound > 1e-12; ++j) {
+      for (int d = 0; d < 3; ++d) {
+        const double kd = M_PI * j / L[d];
+        const double e = exp(-(kd * sl * kd * sl));
+        H[d] += 2 * e;
+        Y[d] += 2 * e * (4 * kd * kd);
+        Z[d] += 2 * e * (16 * kd * kd * kd * kd);
+      }
+      const double km = M_PI * j / prd, km2 = km * km;
+      bound = exp(4 * l * logb - km2 * (sl * sl)) * (km2 * km2) * sig4;
+    }
+    for (int d = 0; d < 3; ++d) H[d] += 1;
+    sum += s->coef[l] * (Y[0] * H[1] * H[2] + H[0] * Y[1] * H[2] + H[0] * H[1] * Y[2]);
+    sum_npt += s->coef_npt[l] * (Z[0] * H[1] * H[2] + H[0] * Z[1] * H[2] + H[0] * H[1] * Z[2] +
+                                 2 * Y[0] * Y[1] * H[2] + 2 * Y[0] * H[1] * Y[2] +
+                                 2 * H[0] * Y[1] * Y[2]);
+  }
+  s->S = sum - low;
+  s->S_npt = sum_npt - low_npt;
+  int nd = 0;
+  for (int i = -1; i <= 1; ++i)
+    for (int j = -1; j <= 1; ++j)
+      for (int k = -1; k <= 1; ++k) {
+        if ((i == 0 && j == 0 && k == 0) || i * i + j * j + k * k > 1) continue;
+        const double Kx = (2 * M_PI / L[0]) * (i + 0.00), Ky = (2 * M_PI / L[1]) * (j + 0.00),
+                     Kz = (2 * M_PI / L[2]) * (k + 0.00);
+        s->dm[3 * nd] = i;
+        s->dm[3 * nd + 1] = j;
+        s->dm[3 * nd + 2] = k;
+        s->dfb[nd++] = sog_ghat(s, s->coef, Kx * Kx + Ky * Ky + Kz * Kz);
+      }
+  s->self_coeff = (logb / (sqrt(2 * M_PI) * s->sigma)) *
+                  (s->w0 + (1 - pow(b, -s->mmax + 0.0)) / (b - 1));
+  const double ct = logb / (sig2 * sqrt(2 * M_PI * sig2));
+  const double fact[6] = {1, 1, 2, 6, 24, 120};
+  for (int i = 0; i < 6; ++i) {
+    double ss = 0.0;
+    for (int j = 0; j < s->mmax; ++j) {
+      const double bl = pow(b, j + 0.0);
+      const double w = j == 0 ? s->w0 : (1.0 / bl) * (1.0 / bl) * (1.0 / bl);
+      ss += w * (1.0 / fact[i]) * pow(1.0 / (2.0 * sig2 * bl * bl), i + 0.0);
+    }
+    s->taylor[i] = pow(-1.0, i + 1.0) * 2.0 * ct * ss;
+  }
+  return 0;
+}
+
+int orc_rbsog_params(int level, double cut_off, const orc_box* box, double* scal,
+                     double* coef, int* dm, double* dfb) {
+  orc_sog s;
+  if (sog_setup(level, cut_off, box, &s)) return -1;
+  /* scal: mmax, b, sigma, w0, S, S_npt, self_coeff, taylor[6] */
+  const double v[13] = {(double)s.mmax, s.b, s.sigma, s.w0, s.S, s.S_npt, s.self_coeff,
+                        s.taylor[0], s.taylor[1], s.taylor[2], s.taylor[3], s.taylor[4],
+                        s.taylor[5]};
+  memcpy(scal, v, sizeof v);
+  if (coef) memcpy(coef, s.coef, sizeof(double) * (size_t)s.mmax);
+  if (dm) memcpy(dm, s.dm, sizeof s.dm);
+  if (dfb) memcpy(dfb, s.dfb, sizeof s.dfb);
+  return 0;
+}
+
+/* Exact sampler of p(m) ~ G^(m)|k|^2 on |m|^2 > 1: a mixture over (l, axis d)
+ * of separable densities k_d^2 g_l(m_d) prod_(d' != d) g_l(m_d'); one Philox
+ * draw per component pick and axis, tables over m = 0, +1, -1, +2, ... */
+typedef struct {
+  int mmax, ncomp;
+  double* comp;   /* cumulative [3 mmax] */
+  double* tab;    /* concatenated cumulative tables */
+  int off[6 * 128], cnt[6 * 128];
+  double tot[6 * 128];
+} sog_tables;
+
+static int sog_tables_build(const orc_sog* s, const orc_box* box, sog_tables* t) {
+  const double L[3] = {box_len(box, 0), box_len(box, 1), box_len(box, 2)};
+  size_t total = 0;
+  int M[128][3];
+  for (int l = 0; l < s->mmax; ++l)
+    for (int d = 0; d < 3; ++d) {
+      const double kd = 2 * M_PI / L[d];
+      const double a = pow(s->b * s->b, l + 0.0) * (s->sigma * s->sigma) * kd * kd / 2.0;
+      M[l][d] = (int)ceil(sqrt(50.0 / a)) + 1;
+      if (M[l][d] > (1 << 14)) return -1;
+      total += 2 * (size_t)(2 * M[l][d] + 1);
+    }
+  t->mmax = s->mmax;
+  t->ncomp = 3 * s->mmax;
+  t->tab = (double*)malloc(sizeof(double) * total);
+  t->comp = (double*)malloc(sizeof(double) * (size_t)t->ncomp);
+  size_t pos = 0;
+  for (int l = 0; l < s->mmax; ++l)
+    for (int d = 0; d < 3; ++d) {
+      const double kd = 2 * M_PI / L[d];
+      const double a = pow(s->b * s->b, l + 0.0) * (s->sigma * s->sigma) * kd * kd / 2.0;
+      for (int kind = 0; kind < 2; ++kind) {
+        const int ti = (l * 3 + d) * 2 + kind;
+        t->off[ti] = (int)pos;
+        double acc = 0.0;
+        for (int e = 0; e <= 2 * M[l][d]; ++e) {
+          const int m = e == 0 ? 0 : ((e & 1) ? (e + 1) / 2 : -(e / 2));
+          const double k = kd * m;
+          acc += exp(-a * (double)m * (double)m) * (kind ? k * k : 1.0);
+          t->tab[pos++] = acc;
+        }
+        t->cnt[ti] = 2 * M[l][d] + 1;
+        t->tot[ti] = acc;
+      }
+    }
+  double acc = 0.0;
+  for (int l = 0; l < s->mmax; ++l)
+    for (int d = 0; d < 3; ++d) {
+      double w = s->coef[l];
+      for (int a2 = 0; a2 < 3; ++a2) w *= t->tot[(l * 3 + a2) * 2 + (a2 == d ? 1 : 0)];
+      acc += w;
+      t->comp[l * 3 + d] = acc;
+    }
+  return 0;
+}
+
+static int sog_first_above(const double* cdf, int cnt, double target) {
+  for (int i = 0; i < cnt; ++i)
+    if (target < cdf[i]) return i;
+  return cnt - 1;
+}
+
+static double sog_u53(uint32_t hi, uint32_t lo) {
+  return (double)(((((uint64_t)hi) << 32) | lo) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+int orc_rbsog_sample_philox(int level, double cut_off, const orc_box* box, int p, uint64_t seed,
+                            int64_t step, double* mx, double* my, double* mz) {
+  orc_sog s;
+  sog_tables t;
+  if (sog_setup(level, cut_off, box, &s) || sog_tables_build(&s, box, &t)) return -1;
+  int rc = 0;
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int i = 0; i < p && !rc; ++i) {
+    int done = 0;
+    for (int a = 0; a < 64 && !done; ++a) {
+      const uint32_t c0[4] = {(uint32_t)i, (uint32_t)(2 * a), (uint32_t)step,
+                              (uint32_t)((uint64_t)step >> 32)};
+      const uint32_t d0[4] = {(uint32_t)i, (uint32_t)(2 * a + 1), (uint32_t)step,
+                              (uint32_t)((uint64_t)step >> 32)};
+      uint32_t c[4], d[4];
+      orc_philox4x32_10(c0, key, c);
+      orc_philox4x32_10(d0, key, d);
+      const int comp = sog_first_above(t.comp, t.ncomp, sog_u53(c[0], c[1]) * t.comp[t.ncomp - 1]);
+      const int l = comp / 3, dd = comp - 3 * l;
+      const double u[3] = {sog_u53(c[2], c[3]), sog_u53(d[0], d[1]), sog_u53(d[2], d[3])};
+      int m[3];
+      for (int ax = 0; ax < 3; ++ax) {
+        const int ti = (l * 3 + ax) * 2 + (ax == dd ? 1 : 0);
+        const int e = sog_first_above(t.tab + t.off[ti], t.cnt[ti], u[ax] * t.tot[ti]);
+        m[ax] = e == 0 ? 0 : ((e & 1) ? (e + 1) / 2 : -(e / 2));
+      }
+      if (m[0] * m[0] + m[1] * m[1] + m[2] * m[2] > 1) {
+        mx[i] = m[0];
+        my[i] = m[1];
+        mz[i] = m[2];
+        done = 1;
+      }
+    }
+    if (!done) rc = -2;
+  }
+  free(t.tab);
+  free(t.comp);
+  return rc;
+}
+
+/* RBSOGSampleKSpace's Metropolis chain (kspace_calculator.cpp:1142-1240):
+ * proposals round(N(0, L / (2 pi sigma))) per axis, acceptance
+ * min(1, p(new) q(old) / (p(old) q(new))) with p = G^(m)|k|^2 and q the
+ * discretised-Gaussian mass MH_D_Modify (:1669-1677); |m|^2 <= 1 redrawn; the
+ * odd entries of a chain of 2P are the samples.  Seeded SplitMix64 uniforms
+ * stand in for the reference's unseeded std::random_device stream. */
+static double sog_q(int m, double f) {
+  return m == 0 ? erf(0.5 * f) : 0.5 * (erf((abs(m) + 0.5) * f) - erf((abs(m) - 0.5) * f));
+}
+
+int orc_rbsog_sample_mh(int level, double cut_off, const orc_box* box, int p, uint64_t seed,
+                        double* mx, double* my, double* mz) {
+  orc_sog s;
+  if (sog_setup(level, cut_off, box, &s)) return -1;
+  const double L[3] = {box_len(box, 0), box_len(box, 1), box_len(box, 2)};
+  orc_rng r = {seed};
+  double fac[3], mhd[3];
+  for (int d = 0; d < 3; ++d) {
+    fac[d] = L[d] / (2 * M_PI * s.sigma);
+    mhd[d] = sqrt(2 * s.sigma * s.sigma * M_PI * M_PI) / L[d];
+  }
+  const int n = 2 * p;
+  int* cx = (int*)malloc(sizeof(int) * 3 * (size_t)n);
+#define PDENS(m)                                                                                \
+  (sog_ghat(&s, s.coef,                                                                         \
+            pow((m)[0] * 2 * M_PI / L[0], 2) + pow((m)[1] * 2 * M_PI / L[1], 2) +                \
+                pow((m)[2] * 2 * M_PI / L[2], 2)) *                                              \
+   (pow((m)[0] * 2 * M_PI / L[0], 2) + pow((m)[1] * 2 * M_PI / L[1], 2) +                       \
+    pow((m)[2] * 2 * M_PI / L[2], 2)))
+  do {
+    for (int d = 0; d < 3; ++d) cx[d] = (int)round(mh_gauss(&r, fac[d]));
+  } while (cx[0] == 0 && cx[1] == 0 && cx[2] == 0);
+  for (int i = 0; i < n - 1; ++i) {
+    int mo[3], mn[3];
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = (int)round(mh_gauss(&r, fac[d]));
+      mo[d] = cx[3 * i + d];
+    }
+    const double pu = PDENS(mn) * sog_q(mo[0], mhd[0]) * sog_q(mo[1], mhd[1]) * sog_q(mo[2], mhd[2]);
+    const double pd = PDENS(mo) * sog_q(mn[0], mhd[0]) * sog_q(mn[1], mhd[1]) * sog_q(mn[2], mhd[2]);
+    const double acc = pu / pd > 1.0 ? 1.0 : pu / pd;
+    const int* pick = rng_uniform(&r) < acc ? mn : mo;
+    for (int d = 0; d < 3; ++d) cx[3 * (i + 1) + d] = pick[d];
+    const int* q = cx + 3 * (i + 1);
+    if (q[0] * q[0] + q[1] * q[1] + q[2] * q[2] <= 1) i = i - 1;
+  }
+#undef PDENS
+  for (int i = 0; i < p; ++i) {
+    mx[i] = cx[3 * (2 * i + 1)];
+    my[i] = cx[3 * (2 * i + 1) + 1];
+    mz[i] = cx[3 * (2 * i + 1) + 2];
+  }
+  free(cx);
+  return 0;
+}
+
+/* ComputeRBSOG's force and energy for given samples: the sampled vectors
+ * (c_k = -(S/P) qqr2e / (V k^2)) and the six direct ones (c_k = -qqr2e G^/V),
+ * rho by ComputePnumberChargeStructureFactorSOG, energies of
+ * ComputeRBSOGSample/DirectEnergyKernel and the self term (:1525-1535).
+ * S <= 0: RBSOGSetup's S. */
+int orc_rbsog_force(int level, double cut_off, const orc_box* box, double qqr2e, double S, int n,
+                    int p, const double* q, const double* mx, const double* my,
+                    const double* mz, const double* x, const double* y, const double* z,
+                    double* fx, double* fy, double* fz, double* energy) {
+  orc_sog s;
+  if (sog_setup(level, cut_off, box, &s)) return -1;
+  const double L[3] = {box_len(box, 0), box_len(box, 1), box_len(box, 2)};
+  const double V = L[0] * L[1] * L[2], Su = S > 0 ? S : s.S;
+  const int pt = p + 6;
+  double* K = (double*)malloc(sizeof(double) * 3 * (size_t)pt);
+  double* c = (double*)malloc(sizeof(double) * (size_t)pt);
+  double* re = (double*)calloc((size_t)pt, sizeof(double));
+  double* im = (double*)calloc((size_t)pt, sizeof(double));
+  double e = 0.0;
+  for (int k = 0; k < pt; ++k) {
+    const double m[3] = {k < p ? mx[k] : s.dm[3 * (k - p)], k < p ? my[k] : s.dm[3 * (k - p) + 1],
+                         k < p ? mz[k] : s.dm[3 * (k - p) + 2]};
+    for (int d = 0; d < 3; ++d) K[3 * k + d] = 2 * M_PI * m[d] / L[d];
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < pt; ++k) {
+    double r = 0.0, ii = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double ph = K[3 * k] * x[i] + K[3 * k + 1] * y[i] + K[3 * k + 2] * z[i];
+      r += q[i] * cos(ph);
+      ii += q[i] * sin(ph);
+    }
+    re[k] = r;
+    im[k] = ii;
+  }
+  for (int k = 0; k < pt; ++k) {
+    const double k2 = K[3 * k] * K[3 * k] + K[3 * k + 1] * K[3 * k + 1] + K[3 * k + 2] * K[3 * k + 2];
+    const double r2 = re[k] * re[k] + im[k] * im[k];
+    if (k < p) {
+      c[k] = -(Su / p) * qqr2e / V / k2;
+      e += (Su / (2.0 * p * V)) * qqr2e * r2 / k2;
+    } else {
+      c[k] = -qqr2e / V * s.dfb[k - p];
+      e += qqr2e / (2.0 * V) * s.dfb[k - p] * r2;
+    }
+  }
+  double qsq = 0.0;
+  for (int i = 0; i < n; ++i) qsq += q[i] * q[i];
+  e += -s.self_coeff * qsq * qqr2e;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double f[3] = {0, 0, 0};
+    for (int k = 0; k < pt; ++k) {
+      const double ph = K[3 * k] * x[i] + K[3 * k + 1] * y[i] + K[3 * k + 2] * z[i];
+      const double t = (cos(ph) * im[k] - sin(ph) * re[k]) * c[k];
+      for (int d = 0; d < 3; ++d) f[d] += q[i] * t * K[3 * k + d];
+    }
+    fx[i] = f[0];
+    fy[i] = f[1];
+    fz[i] = f[2];
+  }
+  if (energy) *energy = e;
+  free(K);
+  free(c);
+  free(re);
+  free(im);
+  return 0;
+}
+
+/* The far field the sampled sum estimates, summed exactly: all m with
+ * |m_d| <= mcut and |m|^2 > 1, weight G^(m) (the sampled estimator's
+ * expectation is S / S_full times this, S_full = sum G^(m) |k|^2 over the
+ * same m, written to *S_full). */
+int orc_rbsog_far_exact(int level, double cut_off, const orc_box* box, double qqr2e, int n,
+                        const double* q, const double* x, const double* y, const double* z,
+                        int mcut, double* fx, double* fy, double* fz, double* S_full) {
+  orc_sog s;
+  if (sog_setup(level, cut_off, box, &s)) return -1;
+  const double L[3] = {box_len(box, 0), box_len(box, 1), box_len(box, 2)};
+  const double V = L[0] * L[1] * L[2];
+  const int side = 2 * mcut + 1;
+  const int nk = side * side * side;
+  double* K = (double*)malloc(sizeof(double) * 4 * (size_t)nk);
+  int cntk = 0;
+  double Sf = 0.0;
+  for (int a = -mcut; a <= mcut; ++a)
+    for (int b = -mcut; b <= mcut; ++b)
+      for (int c = -mcut; c <= mcut; ++c) {
+        if (a * a + b * b + c * c <= 1) continue;
+        double* k = K + 4 * (size_t)cntk++;
+        k[0] = 2 * M_PI * a / L[0];
+        k[1] = 2 * M_PI * b / L[1];
+        k[2] = 2 * M_PI * c / L[2];
+        const double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+        k[3] = sog_ghat(&s, s.coef, k2);
+        Sf += k[3] * k2;
+      }
+  double* re = (double*)calloc((size_t)cntk, sizeof(double));
+  double* im = (double*)calloc((size_t)cntk, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < cntk; ++k) {
+    double r = 0.0, ii = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double ph = K[4 * k] * x[i] + K[4 * k + 1] * y[i] + K[4 * k + 2] * z[i];
+      r += q[i] * cos(ph);
+      ii += q[i] * sin(ph);
+    }
+    re[k] = r;
+    im[k] = ii;
+  }
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double f[3] = {0, 0, 0};
+    for (int k = 0; k < cntk; ++k) {
+      const double ph = K[4 * k] * x[i] + K[4 * k + 1] * y[i] + K[4 * k + 2] * z[i];
+      const double t = (cos(ph) * im[k] - sin(ph) * re[k]) * (-qqr2e / V * K[4 * k + 3]);
+      for (int d = 0; d < 3; ++d) f[d] += q[i] * t * K[4 * k + d];
+    }
+    fx[i] = f[0];
+    fy[i] = f[1];
+    fz[i] = f[2];
+  }
+  if (S_full) *S_full = Sf;
+  free(K);
+  free(re);
+  free(im);
+  return 0;
+}
+
+/* VERLET-SOG pair force (ComputeLJCutCoulForceUserKernel with lj126 and
+ * CoulCutForceUser, lj_cut_coul_kspace_op.hip.cu:196-254, 357-470, lj_op.hip.cu:18-37). */
+void orc_pair_force_verlet_sog(int level, double cut_off, const orc_box* box, double qqr2e,
+                               int n, const int* type, const double* sigma, const double* eps,
+                               const double* q, const double* x, const double* y,
+                               const double* z, int cap, const int* count, const int* cand,
+                               double* fx, double* fy, double* fz, double* energy) {
+  orc_sog s;
+  if (sog_setup(level, cut_off, box, &s)) return;
+  const double cut2 = cut_off * cut_off;
+  double elj = 0.0, ecl = 0.0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : elj, ecl)
+  for (int i = 0; i < n; ++i) {
+    double f[3] = {0, 0, 0};
+    for (int t = 0; t < count[i]; ++t) {
+      const int j = cand[(size_t)i * cap + t];
+      double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+      min_image_while(box, &dx, &dy, &dz);
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (!(d2 < cut2)) continue;
+      const double eij = sqrt(eps[type[i]] * eps[type[j]]);
+      const double sij = (sigma[type[i]] + sigma[type[j]]) / 2;
+      const double s6 = pow(sij, 6.0), d6 = pow(d2, 3.0), sd6 = s6 / d6;
+      const double flj = -24 * eij * ((2 * sd6 - 1) * sd6) / d2;
+      const double r2inv = 1.0 / d2, rinv = sqrt(r2inv), r3inv = rinv * r2inv;
+      const double pre = qqr2e * q[i] * q[j];
+      const double poly = s.taylor[0] + s.taylor[1] * d2 + s.taylor[2] * pow(d2, 2.0) +
+                          s.taylor[3] * pow(d2, 3.0) + s.taylor[4] * pow(d2, 4.0) +
+                          s.taylor[5] * pow(d2, 5.0);
+      const double fp = flj + (-pre * (r3inv + poly));
+      f[0] += dx * fp;
+      f[1] += dy * fp;
+      f[2] += dz * fp;
+      elj += 0.5 * (4 * eij * (s6 / d6 - 1) * sd6);
+      const double norm = 2.0 * log(s.b) / sqrt(2.0 * M_PI * s.sigma * s.sigma);
+      double sume = norm * s.w0 * exp(-d2 / (2.0 * s.sigma * s.sigma));
+      for (int l = 1; l < s.mmax; ++l)
+        sume += norm * (1.0 / pow(s.b, l + 0.00)) *
+                exp(-d2 / (2 * s.sigma * s.sigma * pow(s.b, l + 0.00) * pow(s.b, l + 0.00)));
+      ecl += 0.5 * pre * (rinv - sume);
+    }
+    fx[i] = f[0];
+    fy[i] = f[1];
+    fz[i] = f[2];
+  }
+  if (energy) {
+    energy[0] = elj;
+    energy[1] = ecl;
+  }
+}

@@ -19,9 +19,10 @@ LIB = os.path.join(HERE, "librbx.so")
 
 CU_SOURCES = ["rbx_capi.cu", "rbx_rbe.cu", "rbx_pair.cu", "rbx_cells.cu", "rbx_engine.cu",
               "rbx_batch.cu", "rbx_adjoint.cu", "rbx_thermo.cu", "rbx_shake.cu",
-              "rbx_special.cu"]
+              "rbx_special.cu", "rbx_rbsog.cu"]
 CXX_SOURCES = ["host/config_data.cpp", "host/lj_cut_coul_kspace.cpp", "host/lammps_data.cpp",
-               "host/md_files.cpp", "host/special_bonds.cpp"]
+               "host/md_files.cpp", "host/special_bonds.cpp",
+               "host/rbsog.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

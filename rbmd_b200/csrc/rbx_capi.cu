@@ -654,3 +654,239 @@ extern "C" int rbx_rbe_structure_factor_noalloc(const rbx_box* box, int num_atom
                              1.0, 0.0, 0.0, density_real, density_imag, nullptr, nullptr, nullptr,
                              0, nullptr, 0, nullptr, nullptr, st);
 }
+
+// ---------------------------------------------------------------------------
+// RBSOG k-space and VERLET-SOG real space (op level)
+// ---------------------------------------------------------------------------
+#include <stdexcept>
+
+#include "host/rbsog.h"
+
+namespace {
+
+int cuda_ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return RBX_OK;
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  return RBX_ERR_DEVICE;
+}
+
+int rbsog_setup_checked(int level, double cut_off, const rbx_box* box,
+                        rbx_host::RbsogSetup* out) {
+  try {
+    *out = rbx_host::rbsog_setup(level, cut_off, *box);
+  } catch (const std::exception& ex) {
+    set_error("%s", ex.what());
+    return RBX_ERR_INVALID;
+  }
+  return RBX_OK;
+}
+
+}  // namespace
+
+int rbx_rbsog_params(int level, double cut_off, const rbx_box* box, rbx_rbsog_info* out,
+                     double* coef, int* direct_m, double* direct_fb) {
+  RBX_CHECK_BOX(box);
+  if (!out) {
+    set_error("rbx_rbsog_params: null output");
+    return RBX_ERR_INVALID;
+  }
+  rbx_host::RbsogSetup s;
+  RBX_TRY(rbsog_setup_checked(level, cut_off, box, &s));
+  out->level = s.level;
+  out->mmax = s.mmax;
+  out->b = s.b;
+  out->sigma = s.sigma;
+  out->w0 = s.w0;
+  out->S = s.S;
+  out->S_npt = s.S_npt;
+  out->self_coeff = s.self_coeff;
+  for (int i = 0; i < 6; ++i) out->taylor[i] = s.taylor[i];
+  out->n_direct = (int)s.direct_fb.size();
+  out->S_full = s.S_full;
+  if (coef) std::copy(s.coef.begin(), s.coef.end(), coef);
+  if (direct_m) std::copy(s.direct_m.begin(), s.direct_m.end(), direct_m);
+  if (direct_fb) std::copy(s.direct_fb.begin(), s.direct_fb.end(), direct_fb);
+  return RBX_OK;
+}
+
+int rbx_rbsog_sample(const rbx_box* box, int level, double cut_off, int p, uint64_t seed,
+                     int64_t step, double* mx, double* my, double* mz, void* stream) {
+  RBX_CHECK_BOX(box);
+  if (p <= 0 || !mx || !my || !mz) {
+    set_error("rbx_rbsog_sample: need p > 0 and output arrays");
+    return RBX_ERR_INVALID;
+  }
+  rbx_host::RbsogSetup s;
+  RBX_TRY(rbsog_setup_checked(level, cut_off, box, &s));
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  double *cdf = nullptr, *tables = nullptr, *tot = nullptr;
+  int *off = nullptr, *cnt = nullptr, *status = nullptr;
+  int rc = async_alloc(&cdf, s.comp_cdf.size(), st);
+  if (!rc) rc = async_alloc(&tables, s.tables.size(), st);
+  if (!rc) rc = async_alloc(&tot, s.tab_tot.size(), st);
+  if (!rc) rc = async_alloc(&off, s.tab_off.size(), st);
+  if (!rc) rc = async_alloc(&cnt, s.tab_cnt.size(), st);
+  if (!rc) rc = async_alloc(&status, 1, st);
+  if (!rc) {
+    cudaMemcpyAsync(cdf, s.comp_cdf.data(), sizeof(double) * s.comp_cdf.size(),
+                    cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(tables, s.tables.data(), sizeof(double) * s.tables.size(),
+                    cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(tot, s.tab_tot.data(), sizeof(double) * s.tab_tot.size(),
+                    cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(off, s.tab_off.data(), sizeof(int) * s.tab_off.size(),
+                    cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(cnt, s.tab_cnt.data(), sizeof(int) * s.tab_cnt.size(),
+                    cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(status, 0, sizeof(int), st);
+    RbsogTables t{cdf, (int)s.comp_cdf.size(), s.comp_cdf.back(), tables, off, cnt, tot};
+    rc = launch_rbsog_sample(p, t, seed, (uint64_t)step, nullptr, mx, my, mz, nullptr, status, st);
+  }
+  int hs = 0;
+  if (!rc) {
+    cudaMemcpyAsync(&hs, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    rc = cuda_ok(cudaStreamSynchronize(st), "rbx_rbsog_sample");
+  }
+  for (void* ptr : {(void*)cdf, (void*)tables, (void*)tot, (void*)off, (void*)cnt, (void*)status})
+    if (ptr) cudaFreeAsync(ptr, st);
+  if (!rc && hs) {
+    set_error("rbx_rbsog_sample: a sample found no |m|^2 > 1 draw in 64 tries");
+    return RBX_ERR_SAMPLER;
+  }
+  return rc;
+}
+
+int rbx_rbsog_force(const rbx_box* box, int level, double cut_off, double qqr2e, double S,
+                    double qsqsum, int num_atoms, int p, const double* charge, const double* mx,
+                    const double* my, const double* mz, const double* px, const double* py,
+                    const double* pz, double* fx, double* fy, double* fz, double* energy,
+                    void* stream) {
+  RBX_CHECK_BOX(box);
+  if (num_atoms < 0 || p <= 0 || !mx || !my || !mz || !fx || !fy || !fz) {
+    set_error("rbx_rbsog_force: need num_atoms >= 0, p > 0 and the arrays");
+    return RBX_ERR_INVALID;
+  }
+  rbx_host::RbsogSetup s;
+  RBX_TRY(rbsog_setup_checked(level, cut_off, box, &s));
+  if (num_atoms == 0) return RBX_OK;
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  const DBox b = make_dbox(*box);
+  const double V = b.len[0] * b.len[1] * b.len[2];
+  const double Suse = S > 0 ? S : (S < 0 ? s.S_full : s.S);
+  const int nd = (int)s.direct_fb.size(), pt = p + nd;
+  std::vector<double4> w(pt);
+  std::vector<double> dm(3 * (size_t)nd);
+  for (int k = 0; k < p; ++k) w[k] = make_double4(-Suse * qqr2e / p, 0.0, Suse * qqr2e / (2.0 * p * V), 0.0);
+  for (int k = 0; k < nd; ++k) {
+    w[p + k] = make_double4(0.0, -qqr2e * s.direct_fb[k], 0.0, qqr2e * s.direct_fb[k] / (2.0 * V));
+    for (int d = 0; d < 3; ++d) dm[3 * k + d] = s.direct_m[3 * k + d];
+  }
+  const int nparts = rbe_partial_blocks(num_atoms);
+  double *m3 = nullptr, *pre = nullptr, *pim = nullptr, *kterm = nullptr, *en = nullptr;
+  double4* wd = nullptr;
+  KTab* tab = nullptr;
+  int rc = async_alloc(&m3, 3 * (size_t)pt, st);
+  if (!rc) rc = async_alloc(&wd, (size_t)pt, st);
+  if (!rc) rc = async_alloc(&pre, (size_t)pt * nparts, st);
+  if (!rc) rc = async_alloc(&pim, (size_t)pt * nparts, st);
+  if (!rc) rc = async_alloc(&tab, (size_t)pt, st);
+  if (!rc) rc = async_alloc(&kterm, (size_t)pt, st);
+  if (!rc) rc = async_alloc(&en, 1, st);
+  if (!rc) {
+    double* mxs[3] = {m3, m3 + pt, m3 + 2 * pt};
+    const double* src[3] = {mx, my, mz};
+    for (int d = 0; d < 3; ++d) {
+      cudaMemcpyAsync(mxs[d], src[d], sizeof(double) * p, cudaMemcpyDeviceToDevice, st);
+      std::vector<double> col(nd);
+      for (int k = 0; k < nd; ++k) col[k] = dm[3 * k + d];
+      cudaMemcpyAsync(mxs[d] + p, col.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, st);
+      cudaStreamSynchronize(st);  // col is a host temporary
+    }
+    cudaMemcpyAsync(wd, w.data(), sizeof(double4) * pt, cudaMemcpyHostToDevice, st);
+    rc = launch_rbe_rho_partial_f64(b, num_atoms, pt, mxs[0], mxs[1], mxs[2], charge, px, py, pz,
+                                    pre, pim, nparts, st);
+    if (!rc)
+      rc = launch_rbsog_finalize(b, pt, nparts, pre, pim, mxs[0], mxs[1], mxs[2], wd, nullptr,
+                                 nullptr, tab, kterm, -s.self_coeff * qsqsum * qqr2e,
+                                 energy ? en : nullptr, 0, nullptr, 0, nullptr, st);
+    if (!rc) {
+      RbeForceOut o;
+      o.f_out_x = fx;
+      o.f_out_y = fy;
+      o.f_out_z = fz;
+      rc = launch_rbe_force_f64(num_atoms, pt, tab, charge, px, py, pz, o, st);
+    }
+    if (!rc && energy) {
+      cudaMemcpyAsync(energy, en, sizeof(double), cudaMemcpyDeviceToHost, st);
+      rc = cuda_ok(cudaStreamSynchronize(st), "rbx_rbsog_force");
+    }
+  }
+  for (void* ptr : {(void*)m3, (void*)wd, (void*)pre, (void*)pim, (void*)tab, (void*)kterm,
+                    (void*)en})
+    if (ptr) cudaFreeAsync(ptr, st);
+  return rc;
+}
+
+int rbx_pair_force_verlet_sog(const rbx_box* box, int level, double cut_off, double qqr2e,
+                              int num_atoms, int ntypes, const double* sigma, const double* eps,
+                              const int* type, const double* charge, const double* px,
+                              const double* py, const double* pz, int cap, const int* cand_count,
+                              const int* cand, double* fx, double* fy, double* fz,
+                              double* energy, void* stream) {
+  RBX_CHECK_BOX(box);
+  if (num_atoms < 0 || ntypes <= 0 || !sigma || !eps || cap < 0) {
+    set_error("rbx_pair_force_verlet_sog: invalid arguments");
+    return RBX_ERR_INVALID;
+  }
+  rbx_host::RbsogSetup s;
+  RBX_TRY(rbsog_setup_checked(level, cut_off, box, &s));
+  if (num_atoms == 0) return RBX_OK;
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<double> he((size_t)ntypes * ntypes), hs((size_t)ntypes * ntypes);
+  for (int a = 0; a < ntypes; ++a)
+    for (int c = 0; c < ntypes; ++c) {
+      he[a * ntypes + c] = sqrt(eps[a] * eps[c]);
+      hs[a * ntypes + c] = pow((sigma[a] + sigma[c]) / 2, 6.0);
+    }
+  SogPairParams sp{};
+  sp.box = make_dbox(*box);
+  sp.cut_off = cut_off;
+  sp.qqr2e = qqr2e;
+  sp.ntypes = ntypes;
+  for (int i = 0; i < 6; ++i) sp.taylor[i] = s.taylor[i];
+  sp.sigma = s.sigma;
+  sp.b = s.b;
+  sp.w0 = s.w0;
+  sp.norm = 2.0 * log(s.b) / sqrt(2.0 * RBX_PI * s.sigma * s.sigma);
+  sp.mmax = s.mmax;
+  double *tabs = nullptr, *epart = nullptr;
+  const int nb = verlet_sog_blocks(num_atoms);
+  int rc = async_alloc(&tabs, 2 * he.size(), st);
+  if (!rc && energy) rc = async_alloc(&epart, 2 * (size_t)nb, st);
+  if (!rc) {
+    cudaMemcpyAsync(tabs, he.data(), sizeof(double) * he.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(tabs + he.size(), hs.data(), sizeof(double) * hs.size(),
+                    cudaMemcpyHostToDevice, st);
+    sp.lj_eps = tabs;
+    sp.lj_s6 = tabs + he.size();
+    rc = launch_verlet_sog(sp, num_atoms, px, py, pz, charge, type, cand_count, cand, cap, fx, fy,
+                           fz, epart, st);
+  }
+  if (!rc) rc = cuda_ok(cudaStreamSynchronize(st), "rbx_pair_force_verlet_sog");
+  if (!rc && energy) {
+    std::vector<double> h(2 * (size_t)nb);
+    rc = cuda_ok(cudaMemcpy(h.data(), epart, sizeof(double) * h.size(), cudaMemcpyDeviceToHost),
+                 "D2H");
+    energy[0] = energy[1] = 0.0;
+    for (int k = 0; k < nb; ++k) {
+      energy[0] += h[2 * k];
+      energy[1] += h[2 * k + 1];
+    }
+  }
+  for (void* ptr : {(void*)tabs, (void*)epart})
+    if (ptr) cudaFreeAsync(ptr, st);
+  return rc;
+}

@@ -180,6 +180,44 @@ int launch_adj_kspace(int n, int p, double cscale, const KTab* tab, const double
 int launch_gather_vec3(int n, const int* orig, const double* src, double* x, double* y, double* z,
                        cudaStream_t st);
 
+// RBSOG k-space and VERLET-SOG real space (rbx_rbsog.cu).
+struct RbsogTables {         // device views of the mixture sampler's tables
+  const double* comp_cdf;    // [ncomp = 3 mmax] cumulative component weights
+  int ncomp;
+  double comp_tot;
+  const double* tables;      // concatenated cumulative per-axis tables
+  const int* off;            // [mmax][3][2] offsets, counts and totals
+  const int* cnt;
+  const double* tot;
+};
+struct SogPairParams {
+  DBox box;
+  double cut_off, qqr2e;
+  int ntypes;
+  const double* lj_eps;      // ntypes^2
+  const double* lj_s6;
+  double taylor[6];          // short-range force polynomial in r^2
+  double sigma, b, w0, norm; // energy: norm w_l exp(-r^2 / (2 sigma^2 b^(2l)))
+  int mmax;
+};
+int launch_rbsog_sample(int p, const RbsogTables& t, uint64_t seed, uint64_t step,
+                        const int* step_dev, double* mx, double* my, double* mz, int* mi,
+                        int* status, cudaStream_t st);
+// w[k] = {wa, wb, ea, eb}: c_k = (wa / k^2 + wb) / V, e_k = (ea / k^2 + eb) |rho|^2.
+// energy (may be null) needs kterm [p]; E = sum_k e_k + self_energy.
+int launch_rbsog_finalize(const DBox& b, int p, int nparts, const double* part_re,
+                          const double* part_im, const double* mx, const double* my,
+                          const double* mz, const double4* w, double* rho_re, double* rho_im,
+                          KTab* tab, double* kterm, double self_energy, double* energy,
+                          int mean_parts, const double* fpart, int n_atoms, double* mean_out,
+                          cudaStream_t st);
+int verlet_sog_blocks(int n);
+// epart (may be null) receives [blocks][2] = {E_LJ, E_coul} per-block sums.
+int launch_verlet_sog(const SogPairParams& sp, int n, const double* x, const double* y,
+                      const double* z, const double* q, const int* type, const int* cand_count,
+                      const int* cand, int cap, double* fx, double* fy, double* fz, double* epart,
+                      cudaStream_t st);
+
 // Nose-Hoover chain (rbx_thermo.cu): parameters and the device state layout.
 constexpr int NH_CHAIN = 3;
 enum NHSlot {

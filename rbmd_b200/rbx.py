@@ -101,7 +101,15 @@ EXPORTS = [
     "rbx_engine_get_system", "rbx_engine_get_atoms", "rbx_engine_get_type_params",
     "rbx_lammps_gauss_velocities", "rbx_engine_set_nose_hoover", "rbx_engine_get_thermostat",
     "rbx_engine_set_shake", "rbx_engine_get_shake", "rbx_engine_set_special", "rbx_special_build",
+    "rbx_rbsog_params", "rbx_rbsog_sample", "rbx_rbsog_force", "rbx_pair_force_verlet_sog",
 ]
+
+
+class RbsogInfo(C.Structure):
+    _fields_ = [("level", C.c_int), ("mmax", C.c_int), ("b", C.c_double), ("sigma", C.c_double),
+                ("w0", C.c_double), ("S", C.c_double), ("S_npt", C.c_double),
+                ("self_coeff", C.c_double), ("taylor", C.c_double * 6), ("n_direct", C.c_int),
+                ("S_full", C.c_double)]
 
 
 class LammpsInfo(C.Structure):
@@ -183,6 +191,12 @@ def lib():
     L.rbx_engine_get_shake.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.rbx_engine_set_special.argtypes = [vp, ip, vp, vp, dp, dp, dp]
     L.rbx_special_build.argtypes = [ip, ip, vp, ip, vp, ip, vp, C.POINTER(C.c_int), vp, vp]
+    L.rbx_rbsog_params.argtypes = [ip, dp, B, C.POINTER(RbsogInfo), vp, vp, vp]
+    L.rbx_rbsog_sample.argtypes = [B, ip, dp, ip, C.c_uint64, C.c_int64, vp, vp, vp, vp]
+    L.rbx_rbsog_force.argtypes = [B, ip, dp, dp, dp, dp, ip, ip] + [vp] * 11 + [
+        C.POINTER(C.c_double), vp]
+    L.rbx_pair_force_verlet_sog.argtypes = [B, ip, dp, dp, ip, ip, vp, vp] + [vp] * 5 + [
+        ip, vp, vp, vp, vp, vp, vp, vp]
     L.rbx_lammps_read.restype = vp
     L.rbx_lammps_read.argtypes = [C.c_char_p, C.c_char_p, vp]
     L.rbx_lammps_free.argtypes = [vp]
@@ -717,3 +731,47 @@ def special_build(n, bonds=None, angles=None, dihedrals=None):
     sp = np.zeros((n, max(ms.value, 1)), np.int32)
     check(L.rbx_special_build(*args, C.byref(ms), _np_ptr(ns), _np_ptr(sp)), "rbx_special_build")
     return ns, sp[:, :ms.value]
+
+
+def rbsog_params(level, cut_off, box):
+    """rbx_rbsog_params: the RBSOG set-up of a level at this cut_off and box (host)."""
+    info = RbsogInfo()
+    coef = np.zeros(128)
+    dm = np.zeros(18, np.int32)
+    dfb = np.zeros(6)
+    check(lib().rbx_rbsog_params(level, cut_off, C.byref(box), C.byref(info), _np_ptr(coef),
+                                 _np_ptr(dm), _np_ptr(dfb)), "rbx_rbsog_params")
+    return {"mmax": info.mmax, "b": info.b, "sigma": info.sigma, "w0": info.w0, "S": info.S,
+            "S_npt": info.S_npt, "self_coeff": info.self_coeff, "S_full": info.S_full,
+            "taylor": np.array(info.taylor[:]), "coef": coef[:info.mmax].copy(),
+            "direct_m": dm.reshape(6, 3), "direct_fb": dfb}
+
+
+def rbsog_sample(box, level, cut_off, p, seed, step, mx, my, mz, stream=None):
+    check(lib().rbx_rbsog_sample(C.byref(box), level, cut_off, p, seed, step, _ptr(mx), _ptr(my),
+                                 _ptr(mz), _stream(stream)), "rbx_rbsog_sample")
+
+
+def rbsog_force(box, level, cut_off, qqr2e, S, qsqsum, q, mx, my, mz, x, y, z, fx, fy, fz,
+                stream=None):
+    """RBSOG k-space force (sampled + direct); returns the energy."""
+    e = C.c_double()
+    check(lib().rbx_rbsog_force(C.byref(box), level, cut_off, qqr2e, S, qsqsum, q.numel(),
+                                mx.numel(), _ptr(q), _ptr(mx), _ptr(my), _ptr(mz), _ptr(x),
+                                _ptr(y), _ptr(z), _ptr(fx), _ptr(fy), _ptr(fz), C.byref(e),
+                                _stream(stream)), "rbx_rbsog_force")
+    return e.value
+
+
+def pair_force_verlet_sog(box, level, cut_off, qqr2e, sigma, eps, typ, q, x, y, z, count, rows,
+                          fx, fy, fz, stream=None):
+    """VERLET-SOG pair force over row-major candidate rows [n, cap]; returns (E_LJ, E_coul)."""
+    sg = np.ascontiguousarray(sigma, np.float64)
+    ep = np.ascontiguousarray(eps, np.float64)
+    en = np.zeros(2)
+    check(lib().rbx_pair_force_verlet_sog(C.byref(box), level, cut_off, qqr2e, q.numel(), len(sg),
+                                          _np_ptr(sg), _np_ptr(ep), _ptr(typ), _ptr(q), _ptr(x),
+                                          _ptr(y), _ptr(z), rows.shape[1], _ptr(count), _ptr(rows),
+                                          _ptr(fx), _ptr(fy), _ptr(fz), _np_ptr(en),
+                                          _stream(stream)), "rbx_pair_force_verlet_sog")
+    return en
