@@ -193,7 +193,7 @@ def lib():
     L.rbx_special_build.argtypes = [ip, ip, vp, ip, vp, ip, vp, C.POINTER(C.c_int), vp, vp]
     L.rbx_rbsog_params.argtypes = [ip, dp, B, C.POINTER(RbsogInfo), vp, vp, vp]
     L.rbx_rbsog_sample.argtypes = [B, ip, dp, ip, C.c_uint64, C.c_int64, vp, vp, vp, vp]
-    L.rbx_rbsog_force.argtypes = [B, ip, dp, dp, dp, dp, ip, ip] + [vp] * 11 + [
+    L.rbx_rbsog_force.argtypes = [B, ip, dp, dp, dp, dp, ip, ip] + [vp] * 10 + [
         C.POINTER(C.c_double), vp]
     L.rbx_pair_force_verlet_sog.argtypes = [B, ip, dp, dp, ip, ip, vp, vp] + [vp] * 5 + [
         ip, vp, vp, vp, vp, vp, vp, vp]
