@@ -303,8 +303,20 @@ int rbx_pair_force_verlet(const rbx_box* box, double cut_off, int num_atoms,
 typedef struct rbx_engine rbx_engine;
 
 typedef enum { RBX_PLAIN_FP64 = 0, RBX_MIXED = 1 } rbx_precision;
-typedef enum { RBX_NEIGHBOR_VERLET = 0, RBX_NEIGHBOR_RBL = 1 } rbx_neighbor_type;
-typedef enum { RBX_COULOMB_NONE = 0, RBX_COULOMB_RBE = 1, RBX_COULOMB_EWALD = 2 } rbx_coulomb_type;
+/* neighbor.type: "Verlet-List", "RBL", "VERLET-SOG" (Verlet list with the
+ * short-range SOG Coulomb of RBSOG in place of erfc) */
+typedef enum {
+  RBX_NEIGHBOR_VERLET = 0,
+  RBX_NEIGHBOR_RBL = 1,
+  RBX_NEIGHBOR_VERLET_SOG = 2
+} rbx_neighbor_type;
+/* coulomb.type: RBE, EWALD (op level only), RBSOG */
+typedef enum {
+  RBX_COULOMB_NONE = 0,
+  RBX_COULOMB_RBE = 1,
+  RBX_COULOMB_EWALD = 2,
+  RBX_COULOMB_RBSOG = 3
+} rbx_coulomb_type;
 
 typedef struct {
   int neighbor_type;        /* hyper_parameters.neighbor.type */
@@ -326,6 +338,11 @@ typedef struct {
   const double* mass;       /* host, ntypes */
   double fmt2v;             /* force/mass*time -> velocity of the unit style
                                (UnitFactor::_fmt2v; 0 is read as 1, LJ units) */
+  int rbsog_level;          /* hyper_parameters.coulomb.rbsog_level (RBSOG,
+                               VERLET-SOG) */
+  double rbsog_S;           /* RBSOG sampling normalisation: 0 = RBSOGSetup's S
+                               (the reference's forces), < 0 = the full S_full
+                               (see rbx_rbsog_info), > 0 = this value */
 } rbx_params;
 
 /* Engine statistics (host copy). */

@@ -110,7 +110,29 @@ void KSpaceCalculator::Init(const ConfigData& cfg, double qqr2e, double cut_off,
     derive_alpha();
     set_kmax();
   } else if (_coulomb_type == "RBSOG") {
-    throw std::runtime_error("coulomb.type RBSOG is not provided by this engine (RBE, EWALD)");
+    // KSpaceCalculator::Init RBSOG branch (kspace_calculator.cpp:253-330)
+    if (!cfg.PathExists({"hyper_parameters", "coulomb", "rbsog_level"}))
+      throw std::runtime_error("RBSOG requires hyper_parameters.coulomb.rbsog_level.");
+    for (const char* legacy : {"accuracy", "rbsog_b", "rbsog_sigma", "rbsog_Mmax", "rbsog_Kcut"})
+      if (cfg.PathExists({"hyper_parameters", "coulomb", legacy}))
+        throw std::runtime_error(std::string("Legacy RBSOG config key '") + legacy +
+                                 "' is not supported. Use hyper_parameters.coulomb.rbsog_level "
+                                 "instead.");
+    _rbsog_level = cfg.Get<int>("rbsog_level", "hyper_parameters", "coulomb");
+    if (_rbsog_level < 0 || _rbsog_level > 4)
+      throw std::runtime_error("RBSOG rbsog_level must be in [0, 4]. Current value: " +
+                               std::to_string(_rbsog_level));
+    _rbe_p = cfg.Get<int>("coulomb_sample_num", "hyper_parameters", "coulomb");
+    if (cfg.PathExists({"hyper_parameters", "coulomb", "alpha"})) {
+      SetAlphaFromManual(cfg.Get<double>("alpha", "hyper_parameters", "coulomb"));
+    } else {
+      static const double kTargetAccuracy[5] = {2.289e-3, 1.158e-4, 1.142e-5, 5.583e-8,
+                                                3.389e-11};
+      if (charges.empty())
+        throw std::runtime_error("alpha derivation from accuracy needs the atom charges");
+      DeriveAlphaFromAccuracy(kTargetAccuracy[_rbsog_level], qqr2e, cut_off, box, num_atoms);
+    }
+    _rbe_p = ((_rbe_p + 15) / 16) * 16;
   } else {
     throw std::runtime_error("Unsupported coulomb type: " + _coulomb_type);
   }
@@ -164,14 +186,25 @@ void LJCutCoulKspace::Init() {
       throw std::runtime_error("Error neighbor_sample_num must be large than 0.");
   } else if (_neighbor_type == "Verlet-List" || _neighbor_type == "VERLET") {
     p.neighbor_type = RBX_NEIGHBOR_VERLET;
+  } else if (_neighbor_type == "VERLET-SOG") {
+    // LJCutCoulKspace::LJCoulSOGInit (lj_cut_coul_kspace.cpp:651-667) reads the level
+    p.neighbor_type = RBX_NEIGHBOR_VERLET_SOG;
+    p.rbsog_level = _cfg.Get<int>("rbsog_level", "hyper_parameters", "coulomb");
+    if (p.rbsog_level < 0 || p.rbsog_level > 4)
+      throw std::runtime_error("RBSOG rbsog_level must be in [0, 4]. Current value: " +
+                               std::to_string(p.rbsog_level));
   } else {
     throw std::runtime_error("neighbor.type " + _neighbor_type +
-                             " is not provided by this engine (RBL, Verlet-List)");
+                             " is not provided by this engine (RBL, Verlet-List, VERLET-SOG)");
   }
   _kspace.Init(_cfg, qqr2e, cut_off, _box, _n, _charges);
   if (_kspace.type() == "RBE") {
     p.coulomb_type = RBX_COULOMB_RBE;
     p.coulomb_sample_num = _kspace.sample_num();
+  } else if (_kspace.type() == "RBSOG") {
+    p.coulomb_type = RBX_COULOMB_RBSOG;
+    p.coulomb_sample_num = _kspace.sample_num();
+    p.rbsog_level = _kspace.rbsog_level();
   } else if (_kspace.type() == "EWALD") {
     throw std::runtime_error("coulomb.type EWALD runs through rbx_ewald_force, not the engine");
   } else {

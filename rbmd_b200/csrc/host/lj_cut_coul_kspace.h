@@ -28,6 +28,7 @@ class KSpaceCalculator {
   const int* kmax() const { return _kmax; }
   bool manual_alpha() const { return _manual_alpha; }
   std::string energy_rbe_flag() const { return _energy_rbe_flag; }
+  int rbsog_level() const { return _rbsog_level; }
 
  private:
   void SetAlphaFromManual(double alpha);
@@ -41,6 +42,7 @@ class KSpaceCalculator {
   double _alpha = 0.0, _g_ewald = 0.0, _accuracy = 0.0, _q2 = 0.0;
   bool _manual_alpha = false;
   int _rbe_p = 0;
+  int _rbsog_level = 0;
   int _kmax[3] = {0, 0, 0};
 };
 

@@ -15,6 +15,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <stdexcept>
 #include <string>
 #include <unordered_map>
 #include <cmath>
@@ -25,6 +26,7 @@
 #include "rbx_common.cuh"
 #include "rbx_engine.h"
 #include "rbx_kernels.h"
+#include "host/rbsog.h"
 
 namespace rbx {
 int require_device();
@@ -109,6 +111,20 @@ int rbx_engine::init() {
     set_error("RBE needs coulomb_sample_num > 0 and alpha > 0");
     return RBX_ERR_CONFIG;
   }
+  if (prm.coulomb_type == RBX_COULOMB_RBSOG && prm.coulomb_sample_num <= 0) {
+    set_error("RBSOG needs coulomb_sample_num > 0");
+    return RBX_ERR_CONFIG;
+  }
+  if (prm.coulomb_type != RBX_COULOMB_NONE && prm.coulomb_type != RBX_COULOMB_RBE &&
+      prm.coulomb_type != RBX_COULOMB_RBSOG) {
+    set_error("the engine runs coulomb types NONE, RBE and RBSOG");
+    return RBX_ERR_CONFIG;
+  }
+  if (prm.neighbor_type != RBX_NEIGHBOR_VERLET && prm.neighbor_type != RBX_NEIGHBOR_RBL &&
+      prm.neighbor_type != RBX_NEIGHBOR_VERLET_SOG) {
+    set_error("neighbor type must be Verlet-List, RBL or VERLET-SOG");
+    return RBX_ERR_CONFIG;
+  }
   if (prm.ntypes <= 0 || prm.ntypes > 16) {
     set_error("ntypes must be in [1, 16]");
     return RBX_ERR_CONFIG;
@@ -123,8 +139,11 @@ int rbx_engine::init() {
   ncell = dims[0] * dims[1] * dims[2];
   freq = rbl ? rbl_freq(n, box, prm.r_core, prm.cut_off, prm.neighbor_sample_num) : 1;
   div = make_divtest(freq);
-  P = prm.coulomb_type == RBX_COULOMB_RBE ? prm.coulomb_sample_num : 0;
-  S = P > 0 ? gauss_sum(box, prm.alpha) : 0.0;
+  sog = prm.coulomb_type == RBX_COULOMB_RBSOG;
+  sog_pair = prm.neighbor_type == RBX_NEIGHBOR_VERLET_SOG;
+  P = (prm.coulomb_type == RBX_COULOMB_RBE || sog) ? prm.coulomb_sample_num : 0;
+  Pk = sog ? P + 6 : P;
+  S = (P > 0 && !sog) ? gauss_sum(box, prm.alpha) : 0.0;
 
   const size_t N = (size_t)n;
   double** dptrs[] = {&x, &y, &z, &vx, &vy, &vz, &fx, &fy, &fz, &q, &x0, &y0, &z0,
@@ -169,23 +188,24 @@ int rbx_engine::init() {
   ETRY(upload_type_tables());
   if (P > 0) {
     nparts = rbe_partial_blocks(n);
-    ETRY(alloc(&mx, (size_t)P));
-    ETRY(alloc(&my, (size_t)P));
-    ETRY(alloc(&mz, (size_t)P));
-    ETRY(alloc(&mi, (size_t)3 * P));
-    ETRY(alloc(&part_re, (size_t)nparts * P));
-    ETRY(alloc(&part_im, (size_t)nparts * P));
-    ETRY(alloc(&rho_re, (size_t)P));
-    ETRY(alloc(&rho_im, (size_t)P));
-    ETRY(alloc(&tab, (size_t)P));
-    ETRY(alloc(&kterm, (size_t)8 * P));
-    ETRY(build_sampler_tables());
+    ETRY(alloc(&mx, (size_t)Pk));
+    ETRY(alloc(&my, (size_t)Pk));
+    ETRY(alloc(&mz, (size_t)Pk));
+    ETRY(alloc(&mi, (size_t)3 * Pk));
+    ETRY(alloc(&part_re, (size_t)nparts * Pk));
+    ETRY(alloc(&part_im, (size_t)nparts * Pk));
+    ETRY(alloc(&rho_re, (size_t)Pk));
+    ETRY(alloc(&rho_im, (size_t)Pk));
+    ETRY(alloc(&tab, (size_t)Pk));
+    ETRY(alloc(&kterm, (size_t)8 * Pk));
+    if (!sog) ETRY(build_sampler_tables());
   } else {
     ETRY(alloc(&tab, 1));
     ETRY(alloc(&mx, 1));
     ETRY(alloc(&my, 1));
     ETRY(alloc(&mz, 1));
   }
+  if (sog || sog_pair) ETRY(init_rbsog());
   // candidate capacity from the number density, with headroom (a row that
   // overflows triggers a regrow and rebuild)
   const double V = dbox.len[0] * dbox.len[1] * dbox.len[2];
@@ -422,6 +442,9 @@ int rbx_engine::real_space(const int* epoch_dev) {
                               spec_w[0], spec_w[1], spec_w[2], where, x, y, z, q, type, key_a,
                               key_b, epoch, epoch_dev, fpx, fpy, fpz, fpart + (size_t)nrbl * 3, st);
   }
+  if (sog_pair)
+    return launch_verlet_sog(sogp, n, x, y, z, q, type, cand_count, cand, cap, fpx, fpy, fpz,
+                             nullptr, st);
   return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, fpx, fpy,
                                  fpz, nullptr, epart, nfpart, st);
 }
@@ -432,20 +455,29 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
   if (P > 0) {
     if (!k_injected) {
       ETRY(cuda_ok(cudaMemsetAsync(dflags + 2, 0, sizeof(int), st), "memset"));
-      ETRY(launch_rbe_sample(P, sample_tables, tcnt, ttot, prm.random_seed, epoch, epoch_dev, mx,
-                             my, mz, mixed ? mi : nullptr, dflags + 2, st));
+      if (sog)
+        ETRY(launch_rbsog_sample(P, sog_tables, prm.random_seed, (uint64_t)(int64_t)epoch,
+                                 epoch_dev, mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
+      else
+        ETRY(launch_rbe_sample(P, sample_tables, tcnt, ttot, prm.random_seed, epoch, epoch_dev,
+                               mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
     }
     if (mixed)
-      ETRY(launch_rbe_rho_partial_mixed(n, P, mi, atoms, part_re, part_im, nparts, st));
+      ETRY(launch_rbe_rho_partial_mixed(n, Pk, mi, atoms, part_re, part_im, nparts, st));
     else
-      ETRY(launch_rbe_rho_partial_f64(dbox, n, P, mx, my, mz, q, x, y, z, part_re, part_im, nparts,
-                                      st));
+      ETRY(launch_rbe_rho_partial_f64(dbox, n, Pk, mx, my, mz, q, x, y, z, part_re, part_im,
+                                      nparts, st));
   }
-  ETRY(launch_rbe_finalize(dbox, P, P > 0 ? nparts : 0, part_re, part_im, mx, my, mz, prm.alpha,
-                           S, prm.qqr2e, qsq, qsum, P > 0 ? rho_re : nullptr, rho_im,
-                           P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr,
-                           rbl ? nrbl + (spec_natoms ? SPEC_PARTS : 0) : 0,
-                           fpart, n, rbl ? mean : nullptr, kterm, st));
+  const int mean_parts = rbl ? nrbl + (spec_natoms ? SPEC_PARTS : 0) : 0;
+  if (sog)
+    ETRY(launch_rbsog_finalize(dbox, Pk, nparts, part_re, part_im, mx, my, mz, sog_w, rho_re,
+                               rho_im, tab, kterm, -sog_self * qsq * prm.qqr2e, ek, mean_parts,
+                               fpart, n, rbl ? mean : nullptr, st));
+  else
+    ETRY(launch_rbe_finalize(dbox, P, P > 0 ? nparts : 0, part_re, part_im, mx, my, mz,
+                             prm.alpha, S, prm.qqr2e, qsq, qsum, P > 0 ? rho_re : nullptr,
+                             rho_im, P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr,
+                             mean_parts, fpart, n, rbl ? mean : nullptr, kterm, st));
   RbeForceOut o;
   o.f_pair_x = fpx;
   o.f_pair_y = fpy;
@@ -468,9 +500,73 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
     o.half_dt = 0.5 * prm.dt;
   }
   if (mixed)
-    ETRY(launch_rbe_force_mixed(n, P, tab, atoms, o, st));
+    ETRY(launch_rbe_force_mixed(n, Pk, tab, atoms, o, st));
   else
-    ETRY(launch_rbe_force_f64(n, P, tab, q, x, y, z, o, st));
+    ETRY(launch_rbe_force_f64(n, Pk, tab, q, x, y, z, o, st));
+  return RBX_OK;
+}
+
+// RBSOG k-space (per-k weights, the |m| = 1 vectors after the P samples, the
+// mixture sampler's tables) and the VERLET-SOG pair parameters; see rbx_rbsog.cu.
+int rbx_engine::init_rbsog() {
+  rbx_host::RbsogSetup s;
+  try {
+    s = rbx_host::rbsog_setup(prm.rbsog_level, prm.cut_off, box);
+  } catch (const std::exception& ex) {
+    set_error("%s", ex.what());
+    return RBX_ERR_CONFIG;
+  }
+  if (sog_pair) {
+    sogp.box = dbox;
+    sogp.cut_off = prm.cut_off;
+    sogp.qqr2e = prm.qqr2e;
+    sogp.ntypes = prm.ntypes;
+    sogp.lj_eps = lj_eps;
+    sogp.lj_s6 = lj_s6;
+    for (int i = 0; i < 6; ++i) sogp.taylor[i] = s.taylor[i];
+    sogp.sigma = s.sigma;
+    sogp.b = s.b;
+    sogp.w0 = s.w0;
+    sogp.norm = 2.0 * log(s.b) / sqrt(2.0 * M_PI * s.sigma * s.sigma);
+    sogp.mmax = s.mmax;
+  }
+  if (!sog) return RBX_OK;
+  S = prm.rbsog_S > 0 ? prm.rbsog_S : (prm.rbsog_S < 0 ? s.S_full : s.S);
+  sog_self = s.self_coeff;
+  const double V = dbox.len[0] * dbox.len[1] * dbox.len[2], qe = prm.qqr2e;
+  std::vector<double4> w(Pk);
+  for (int k = 0; k < P; ++k) w[k] = make_double4(-S * qe / P, 0.0, S * qe / (2.0 * P * V), 0.0);
+  std::vector<double> dm[3];
+  std::vector<int> dmi;
+  for (int k = 0; k < 6; ++k) {
+    w[P + k] = make_double4(0.0, -qe * s.direct_fb[k], 0.0, qe * s.direct_fb[k] / (2.0 * V));
+    for (int d = 0; d < 3; ++d) {
+      dm[d].push_back(s.direct_m[3 * k + d]);
+      dmi.push_back(s.direct_m[3 * k + d]);
+    }
+  }
+  ETRY(alloc(&sog_w, (size_t)Pk));
+  ETRY(alloc(&sog_cdf, s.comp_cdf.size()));
+  ETRY(alloc(&sog_tab, s.tables.size()));
+  ETRY(alloc(&sog_tot, s.tab_tot.size()));
+  ETRY(alloc(&sog_off, s.tab_off.size()));
+  ETRY(alloc(&sog_cnt, s.tab_cnt.size()));
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return cuda_ok(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "H2D");
+  };
+  ETRY(up(sog_w, w.data(), sizeof(double4) * Pk));
+  ETRY(up(sog_cdf, s.comp_cdf.data(), sizeof(double) * s.comp_cdf.size()));
+  ETRY(up(sog_tab, s.tables.data(), sizeof(double) * s.tables.size()));
+  ETRY(up(sog_tot, s.tab_tot.data(), sizeof(double) * s.tab_tot.size()));
+  ETRY(up(sog_off, s.tab_off.data(), sizeof(int) * s.tab_off.size()));
+  ETRY(up(sog_cnt, s.tab_cnt.data(), sizeof(int) * s.tab_cnt.size()));
+  ETRY(up(mx + P, dm[0].data(), sizeof(double) * 6));
+  ETRY(up(my + P, dm[1].data(), sizeof(double) * 6));
+  ETRY(up(mz + P, dm[2].data(), sizeof(double) * 6));
+  ETRY(up(mi + 3 * P, dmi.data(), sizeof(int) * 18));
+  ETRY(cuda_ok(cudaMemset(virk, 0, sizeof(double) * 6), "memset"));
+  sog_tables = RbsogTables{sog_cdf, (int)s.comp_cdf.size(), s.comp_cdf.back(), sog_tab, sog_off,
+                           sog_cnt, sog_tot};
   return RBX_OK;
 }
 
@@ -862,8 +958,9 @@ int rbx_engine::set_k_samples(int p, const double* hmx, const double* hmy, const
 int rbx_engine::force_vjp(const double* g, double* d_eps, double* d_sigma, double* d_q_out,
                           double* d_alpha, double* d_r_out) {
   cudaSetDevice(device);
-  if (prm.neighbor_type != RBX_NEIGHBOR_RBL || !have_forces || !have_cache) {
-    set_error("force_vjp: needs an RBL engine whose forces were computed at the current state");
+  if (prm.neighbor_type != RBX_NEIGHBOR_RBL || sog || !have_forces || !have_cache) {
+    set_error("force_vjp: needs an RBL + RBE engine whose forces were computed at the current "
+              "state");
     return RBX_ERR_INVALID;
   }
   const size_t N = (size_t)n;
@@ -1038,7 +1135,7 @@ int rbx_engine::set_alpha(double a) {
   prm.alpha = a;
   pp.alpha = a;
   pp.sqrt_alpha = sqrt(a);
-  if (P > 0) {
+  if (P > 0 && !sog) {
     S = gauss_sum(box, a);
     ETRY(build_sampler_tables());
   }

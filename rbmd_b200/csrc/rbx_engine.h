@@ -21,6 +21,17 @@ struct rbx_engine {
   int freq = 1;
   rbx::DivTest div{};
   int P = 0;
+  // RBSOG: Pk = P + 6 k entries (samples, then the |m| = 1 vectors), per-k
+  // weights, the mixture sampler's tables; VERLET-SOG pair parameters
+  bool sog = false, sog_pair = false;
+  int Pk = 0;
+  double sog_self = 0.0;  // self_coeff (E_self = -self_coeff qsq qqr2e)
+  double4* sog_w = nullptr;
+  double *sog_cdf = nullptr, *sog_tab = nullptr, *sog_tot = nullptr;
+  int *sog_off = nullptr, *sog_cnt = nullptr;
+  rbx::RbsogTables sog_tables{};
+  rbx::SogPairParams sogp{};
+  int init_rbsog();
   double S = 0.0, qsq = 0.0, qsum = 0.0;
   rbx::PairParams pp{};
 

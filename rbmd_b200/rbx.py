@@ -22,9 +22,11 @@ PLAIN_FP64 = 0
 MIXED = 1
 NEIGHBOR_VERLET = 0
 NEIGHBOR_RBL = 1
+NEIGHBOR_VERLET_SOG = 2
 COULOMB_NONE = 0
 COULOMB_RBE = 1
 COULOMB_EWALD = 2
+COULOMB_RBSOG = 3
 
 
 class RbxError(RuntimeError):
@@ -63,6 +65,8 @@ class Params(C.Structure):
         ("eps", C.POINTER(C.c_double)),
         ("mass", C.POINTER(C.c_double)),
         ("fmt2v", C.c_double),
+        ("rbsog_level", C.c_int),
+        ("rbsog_S", C.c_double),
     ]
 
 
@@ -394,12 +398,16 @@ class Engine:
         else:
             p = sys["params"]
             prm = Params()
-            prm.neighbor_type = NEIGHBOR_RBL if neighbor == "RBL" else NEIGHBOR_VERLET
+            prm.neighbor_type = {"RBL": NEIGHBOR_RBL, "VERLET": NEIGHBOR_VERLET,
+                                 "VERLET-SOG": NEIGHBOR_VERLET_SOG}[neighbor]
             prm.cut_off = p["cut_off"]
             prm.r_core = p["r_core"]
             prm.skin = p["skin"]
             prm.neighbor_sample_num = p["neighbor_sample_num"]
-            prm.coulomb_type = {"RBE": COULOMB_RBE, "NONE": COULOMB_NONE}[coulomb]
+            prm.coulomb_type = {"RBE": COULOMB_RBE, "NONE": COULOMB_NONE,
+                                "RBSOG": COULOMB_RBSOG}[coulomb]
+            prm.rbsog_level = int(p.get("rbsog_level", 2))
+            prm.rbsog_S = float(p.get("rbsog_S", 0.0))
             prm.alpha = p["alpha"]
             prm.coulomb_sample_num = p["kspace_p"]
             prm.random_seed = seed

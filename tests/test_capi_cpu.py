@@ -82,6 +82,12 @@ JSON_OK = """{
     (lambda s: s.replace('"neighbor_sample_num": 100', '"neighbor_sample_num": 0'),
      "neighbor_sample_num"),
     (lambda s: s[:-3], "JSON parse error"),
+    (lambda s: s.replace('"type": "RBE"', '"type": "RBSOG"'), "RBSOG requires hyper_parameters"),
+    (lambda s: s.replace('"type": "RBE"', '"type": "RBSOG", "rbsog_level": 2, "accuracy": 1e-4'),
+     "Legacy RBSOG config key 'accuracy'"),
+    (lambda s: s.replace('"type": "RBE"', '"type": "RBSOG", "rbsog_level": 7'),
+     "rbsog_level must be in [0, 4]"),
+    (lambda s: s.replace('"type": "RBL"', '"type": "VERLET-SOG"'), "rbsog_level"),
 ])
 def test_json_config_errors(rbx, mutate, needle):
     """Missing or bad keys fail the way LJCutCoulKspace::Init /

@@ -69,3 +69,85 @@ def test_verlet_sog_pair_force_matches_oracle(cuda, rbx, oracle, sys4k):
     got = np.stack([a.cpu().numpy() for a in F], 1)
     assert systems.rel_rms(got, want) < 1e-10
     assert np.allclose(en, ew, rtol=1e-10)
+
+
+def _sog_system(n=4000, seed=29, level=2):
+    s = systems.lj_electrolyte(n, seed=seed, rbsog_level=level, kspace_p=112)
+    return s
+
+
+def _oracle_sog_total(oracle, s, m, level):
+    """VERLET-SOG pair force + RBSOG k-space force of the oracle (host order)."""
+    p = s["params"]
+    box = oracle.Box.make(s["lo"], s["hi"])
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    perm, cell, cs, ce = oracle.cells_sort(box, p["cut_off"] + p["skin"], x, y, z)
+    cnt, rows = oracle.full_list(box, p["cut_off"] + p["skin"], x[perm], y[perm], z[perm], cell,
+                                 cs, ce)
+    fp, _ = oracle.pair_force_verlet_sog(level, p["cut_off"], box, p["qqr2e"],
+                                         s["type"][perm].astype(np.int32), s["sigma"], s["eps"],
+                                         s["q"][perm], x[perm], y[perm], z[perm], cnt, rows)
+    pair = np.empty_like(fp)
+    pair[perm] = fp
+    fk, ek = oracle.rbsog_force(level, p["cut_off"], box, p["qqr2e"], s["q"], m, x, y, z)
+    return pair, fk, ek
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_engine_rbsog_verlet_sog_forces(cuda, rbx, oracle, prec):
+    """The engine with neighbor VERLET-SOG and coulomb RBSOG: pair part,
+    k-space part and energy against the oracle on injected samples; then with
+    its own device sampler at step 3 against the oracle's Philox sampler."""
+    s = _sog_system()
+    p = s["params"]
+    box = oracle.Box.make(s["lo"], s["hi"])
+    m = oracle.rbsog_sample_philox(2, p["cut_off"], box, 112, 5, 0)
+    pair, fk, ek = _oracle_sog_total(oracle, s, m, 2)
+    e = rbx.Engine(s, precision=prec, neighbor="VERLET-SOG", coulomb="RBSOG", seed=31)
+    e.set_k_samples(*m)
+    e.compute_forces(0)
+    fp, fkk = e.force_parts()
+    tol = 1e-10 if prec == 0 else 1e-5
+    assert systems.rel_rms(fp, pair) < tol
+    assert systems.rel_rms(fkk, fk) < (1e-10 if prec == 0 else 2e-5)
+    assert abs(e.stats().e_kspace - ek) < (1e-10 if prec == 0 else 1e-6) * abs(ek)
+    e.set_k_samples(None, None, None)
+    e.compute_forces(3)
+    m3 = oracle.rbsog_sample_philox(2, p["cut_off"], box, 112, 31, 3)
+    _, fk3, _ = _oracle_sog_total(oracle, s, m3, 2)
+    assert systems.rel_rms(e.force_parts()[1], fk3) < (1e-10 if prec == 0 else 2e-5)
+    e.close()
+
+
+def test_engine_rbl_with_rbsog_kspace(cuda, rbx, oracle):
+    """RBL real space with RBSOG k-space (a combination the reference's
+    configuration allows): the k-space part against the oracle."""
+    s = _sog_system(seed=31)
+    p = s["params"]
+    box = oracle.Box.make(s["lo"], s["hi"])
+    m = oracle.rbsog_sample_philox(2, p["cut_off"], box, 112, 5, 0)
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    fk, ek = oracle.rbsog_force(2, p["cut_off"], box, p["qqr2e"], s["q"], m, x, y, z)
+    e = rbx.Engine(s, precision=rbx.PLAIN_FP64, coulomb="RBSOG", seed=31)
+    e.set_k_samples(*m)
+    e.compute_forces(0)
+    assert systems.rel_rms(e.force_parts()[1], fk) < 1e-10
+    e.close()
+
+
+def test_engine_rbsog_graph_matches_launches(cuda, rbx):
+    s = _sog_system(seed=37)
+    runs = []
+    for graph in (True, False):
+        e = rbx.Engine(s, precision=rbx.MIXED, neighbor="VERLET-SOG", coulomb="RBSOG", seed=9)
+        e.set_step_graph(graph)
+        e.compute_forces(0)
+        e.step(12)
+        e.step(13)
+        runs.append((e.get_state(), e.stats()))
+        e.close()
+    (a, sa), (b, sb) = runs
+    for key in ("pos", "vel", "force"):
+        assert np.array_equal(a[key], b[key]), key
+    assert sa.rebuilds == sb.rebuilds
+    assert sa.e_kspace == sb.e_kspace
