@@ -548,6 +548,68 @@ def run_water(args):
     return 0
 
 
+def run_rbsog(args):
+    """RBSOG: the 200k-atom LJ electrolyte with neighbor VERLET-SOG and coulomb
+    RBSOG (rbsog_level 2, P = 112: 100 rounded up to 16 as the reference
+    does), and RBL real space with RBSOG k-space; mixed and plain FP64, NVE,
+    device time per step; the mixed form's force error against plain FP64 on
+    the same state and k-samples."""
+    import torch
+
+    from oracle import oracle as O
+    from rbmd_b200 import rbx, systems
+
+    n, level, P = args.n, args.rbsog_level, 112
+    s = systems.lj_electrolyte(n, seed=2024, kspace_p=P, rbsog_level=level)
+    box = O.Box.make(s["lo"], s["hi"])
+    m = O.rbsog_sample_philox(level, s["params"]["cut_off"], box, P, 5, 0)
+    out = {}
+    for nb in ("VERLET-SOG", "RBL"):
+        forces = {}
+        for prec in (rbx.PLAIN_FP64, rbx.MIXED):
+            e = rbx.Engine(s, precision=prec, neighbor=nb, coulomb="RBSOG", seed=7)
+            e.set_k_samples(*m)
+            e.compute_forces(0)
+            forces[prec] = e.force_parts()
+            e.close()
+        err = systems.rel_rms(sum(forces[1]), sum(forces[0]))
+        for name, prec in (("mixed", rbx.MIXED), ("fp64_plain", rbx.PLAIN_FP64)):
+            e = rbx.Engine(s, precision=prec, neighbor=nb, coulomb="RBSOG", seed=77)
+            e.compute_forces(0)
+            e.step(args.warmup)
+            st = torch.cuda.ExternalStream(e.stream)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev0.record(st)
+            e.step(args.steps)
+            ev1.record(st)
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1)
+            e.set_profiling(True)
+            e.step(args.steps)
+            ph = e.phase_ms()
+            out[f"{nb}+RBSOG {name}"] = {
+                "value": n * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                "phase_ms": {"kick_drift": ph[0], "skin_rebuild": ph[1], "real_space": ph[2],
+                             "kspace": ph[3]}}
+            e.close()
+        out[f"{nb}+RBSOG mixed_rel_force_err"] = err
+    line = {
+        "metric": "RBSOG (VERLET-SOG / RBL real space): atom-steps/s @200k atoms",
+        "value": out["VERLET-SOG+RBSOG mixed"]["value"], "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": out["VERLET-SOG+RBSOG mixed"]["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "dtype": "mixed(u32 fixed-point, f32 SFU, f64 reductions/integrator)",
+        "data": "synthetic",
+        "config": {"workload": f"lj_electrolyte N={n} rho*=0.8 10% ions, cut_off 5 skin 0.3, "
+                               f"RBSOG rbsog_level {level} P={P} (+6 direct vectors), "
+                               f"NVE dt=0.005"},
+        "runs": out,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_gradient(args):
     """Force-field fitting gradient (the gradient recipe): N atoms, three types,
     16 frames every 50 steps of an MD run at theta*, a fixed k-sample per frame;
@@ -666,6 +728,9 @@ def main():
     ap.add_argument("--gradient", action="store_true",
                     help="force-field gradient measurement instead of the headline line")
     ap.add_argument("--grad-n", type=int, default=20000)
+    ap.add_argument("--rbsog", action="store_true",
+                    help="RBSOG (VERLET-SOG and RBL real space) measurement")
+    ap.add_argument("--rbsog-level", type=int, default=2)
     ap.add_argument("--water", action="store_true",
                     help="rigid-water (CVFF, SHAKE, NVT) measurement instead of the headline line")
     ap.add_argument("--water-mol", type=int, default=24327)
@@ -684,6 +749,8 @@ def main():
         return run_gradient(args)
     if args.water:
         return run_water(args)
+    if args.rbsog:
+        return run_rbsog(args)
     return run_ours(args)
 
 
