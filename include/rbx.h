@@ -415,6 +415,24 @@ int rbx_engine_step_host(rbx_engine* e, const double* x_in, const double* v_in,
 int rbx_engine_get_state(rbx_engine* e, double* px, double* py, double* pz,
                          double* vx, double* vy, double* vz, double* fx,
                          double* fy, double* fz);
+/* Autotuner (no counterpart in the reference): times the engine's kernels on
+ * its current state for each candidate launch shape -- rho(k): k-vectors per
+ * thread 1/2/4/8 (32 per warp each) x atom blocks (1, 2, 4, 8 per SM); force
+ * scatter: 128/256/512 atoms per block; RBL kernel: 2/4/8/16 waves of
+ * resident blocks -- keeps the fastest, and caches the choice per size bin
+ * (atom count and k count on a half-octave grid, precision, neighbor and
+ * coulomb type), so engines of the same bin reuse it without timing
+ * (force = 0).  The choice of atom blocks and waves changes the order of the
+ * fixed-order sums (results stay deterministic for a given choice).  Forces
+ * are recomputed with the chosen shapes. */
+typedef struct {
+  int rho_kpt, rho_blocks, force_block, rbl_waves;
+  int cache_hit;            /* 1: taken from the cache, nothing timed */
+  float rho_ms, force_ms, rbl_ms;      /* best times per launch */
+  float rho_ms_default, force_ms_default, rbl_ms_default;  /* built-in shapes */
+} rbx_tuning;
+int rbx_engine_autotune(rbx_engine* e, int force, rbx_tuning* out);
+
 /* NVT: Nose-Hoover chain thermostat of RBMD's NVT ensemble with
  * temp_ctrl_type NOSE_HOOVER (NVTensemble::Solve, nvt_ensemble.cpp:128-160;
  * NoseHooverController, nose_hoover_controller.cpp): chain length 3, one
@@ -582,6 +600,9 @@ int rbx_lammps_write_charge(const char* path, const rbx_box* box, int n, int nty
  * system per process). */
 typedef struct rbx_batch rbx_batch;
 rbx_batch* rbx_batch_create(rbx_engine* const* engines, int count);
+/* Autotune every engine of a batch (rbx_engine_autotune without forcing:
+ * replicas of one size bin share one timing); before the first rbx_batch_step. */
+int rbx_batch_autotune(rbx_batch* b);
 void rbx_batch_destroy(rbx_batch* b);
 int rbx_batch_step(rbx_batch* b, int nsteps);
 /* The stream the batch graph runs on (cudaStream_t). */

@@ -119,6 +119,18 @@ void rbx_batch_destroy(rbx_batch* b) { delete b; }
 
 void* rbx_batch_stream(rbx_batch* b) { return b ? (void*)b->st : nullptr; }
 
+int rbx_batch_autotune(rbx_batch* b) {
+  if (!b) {
+    set_error("rbx_batch_autotune: null batch");
+    return RBX_ERR_INVALID;
+  }
+  for (rbx_engine* e : b->eng) {
+    const int rc = e->autotune(false, nullptr);
+    if (rc) return rc;
+  }
+  return RBX_OK;
+}
+
 int rbx_batch_step(rbx_batch* b, int nsteps) {
   if (!b || nsteps < 0) {
     set_error("rbx_batch_step: invalid batch or step count");

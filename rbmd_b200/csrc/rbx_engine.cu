@@ -20,6 +20,9 @@
 #include <unordered_map>
 #include <cmath>
 #include <charconv>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "rbx.h"
@@ -188,12 +191,13 @@ int rbx_engine::init() {
   ETRY(upload_type_tables());
   if (P > 0) {
     nparts = rbe_partial_blocks(n);
+    nparts_cap = std::max(nparts, 8 * sm_count());
     ETRY(alloc(&mx, (size_t)Pk));
     ETRY(alloc(&my, (size_t)Pk));
     ETRY(alloc(&mz, (size_t)Pk));
     ETRY(alloc(&mi, (size_t)3 * Pk));
-    ETRY(alloc(&part_re, (size_t)nparts * Pk));
-    ETRY(alloc(&part_im, (size_t)nparts * Pk));
+    ETRY(alloc(&part_re, (size_t)nparts_cap * Pk));
+    ETRY(alloc(&part_im, (size_t)nparts_cap * Pk));
     ETRY(alloc(&rho_re, (size_t)Pk));
     ETRY(alloc(&rho_im, (size_t)Pk));
     ETRY(alloc(&tab, (size_t)Pk));
@@ -226,7 +230,7 @@ int rbx_engine::init() {
   pp.sqrt_alpha = sqrt(prm.alpha);
   pp.qqr2e = prm.qqr2e;
   pp.freq = freq;
-  nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, freq, n, cap, nfpart);
+  nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, freq, n, cap, nfpart, tun.rbl_waves);
   pp.div = div;
   pp.ntypes = prm.ntypes;
   pp.lj_eps = lj_eps;
@@ -403,7 +407,7 @@ int rbx_engine::rebuild() {
     release(cand);
     cap = ((int)(maxc * 1.2) + 31) / 32 * 32;
     ETRY(alloc(&cand, (size_t)n * cap));
-    nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart);
+    nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart, tun.rbl_waves);
     graph_dirty = true;  // the list moved
     ++graph_version;
     ETRY(launch_fill_i32(1, dflags + 1, 0, st));
@@ -463,10 +467,11 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
                                mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
     }
     if (mixed)
-      ETRY(launch_rbe_rho_partial_mixed(n, Pk, mi, atoms, part_re, part_im, nparts, st));
+      ETRY(launch_rbe_rho_partial_mixed(n, Pk, mi, atoms, part_re, part_im, nparts, st,
+                                        tun.rho_kpt));
     else
       ETRY(launch_rbe_rho_partial_f64(dbox, n, Pk, mx, my, mz, q, x, y, z, part_re, part_im,
-                                      nparts, st));
+                                      nparts, st, tun.rho_kpt));
   }
   const int mean_parts = rbl ? nrbl + (spec_natoms ? SPEC_PARTS : 0) : 0;
   if (sog)
@@ -500,9 +505,169 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
     o.half_dt = 0.5 * prm.dt;
   }
   if (mixed)
-    ETRY(launch_rbe_force_mixed(n, Pk, tab, atoms, o, st));
+    ETRY(launch_rbe_force_mixed(n, Pk, tab, atoms, o, st, tun.frc_block));
   else
-    ETRY(launch_rbe_force_f64(n, Pk, tab, q, x, y, z, o, st));
+    ETRY(launch_rbe_force_f64(n, Pk, tab, q, x, y, z, o, st, tun.frc_block));
+  return RBX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: candidate launch shapes timed on the current state with CUDA
+// events on the engine's stream; the choice is cached per size bin.
+// ---------------------------------------------------------------------------
+namespace {
+struct TuneKey {
+  int nbin, kbin, precision, neighbor, coulomb, sms;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(nbin, kbin, precision, neighbor, coulomb, sms) <
+           std::tie(o.nbin, o.kbin, o.precision, o.neighbor, o.coulomb, o.sms);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, rbx_engine::Tuning> g_tune_cache;
+
+int half_octave(int v) { return v > 0 ? (int)std::lround(2.0 * std::log2((double)v)) : -1; }
+}  // namespace
+
+int rbx_engine::apply_tuning(const Tuning& t) {
+  tun = t;
+  if (P > 0) nparts = t.rho_parts > 0 ? std::min(t.rho_parts, nparts_cap) : rbe_partial_blocks(n);
+  if (prm.neighbor_type == RBX_NEIGHBOR_RBL)
+    nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart, tun.rbl_waves);
+  graph_dirty = true;
+  ++graph_version;
+  return RBX_OK;
+}
+
+int rbx_engine::autotune(bool force, rbx_tuning* out) {
+  cudaSetDevice(device);
+  const TuneKey key{half_octave(n), half_octave(Pk), prm.precision, prm.neighbor_type,
+                    prm.coulomb_type, sm_count()};
+  rbx_tuning info{};
+  if (!force) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      ETRY(apply_tuning(it->second));
+      info.cache_hit = 1;
+    }
+  }
+  if (!info.cache_hit) {
+    if (!have_cache) ETRY(compute_forces(epoch));
+    const bool mixed = prm.precision == RBX_MIXED;
+    cudaEvent_t e0, e1;
+    ETRY(cuda_ok(cudaEventCreate(&e0), "cudaEventCreate"));
+    ETRY(cuda_ok(cudaEventCreate(&e1), "cudaEventCreate"));
+    constexpr int kReps = 5;
+    // mean device time per launch of fn (2 untimed launches first)
+    auto time_it = [&](auto&& fn, float* ms) -> int {
+      for (int r = 0; r < 2; ++r) ETRY(fn());
+      ETRY(cuda_ok(cudaEventRecord(e0, st), "cudaEventRecord"));
+      for (int r = 0; r < kReps; ++r) ETRY(fn());
+      ETRY(cuda_ok(cudaEventRecord(e1, st), "cudaEventRecord"));
+      ETRY(cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize"));
+      float t = 0.f;
+      ETRY(cuda_ok(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime"));
+      *ms = t / kReps;
+      return RBX_OK;
+    };
+    Tuning best = tun;
+    int rc = RBX_OK;
+    if (P > 0) {
+      // rho(k): k-vectors per thread x atom blocks
+      float best_ms = 1e30f;
+      const int sm = sm_count();
+      for (int mult : {1, 2, 4, 8}) {
+        int parts = std::min(std::min(mult * sm, nparts_cap), std::max(1, (n + 31) / 32));
+        for (int kpt : {1, 2, 4, 8}) {
+          float ms = 0.f;
+          rc = time_it(
+              [&]() {
+                return mixed ? launch_rbe_rho_partial_mixed(n, Pk, mi, atoms, part_re, part_im,
+                                                            parts, st, kpt)
+                             : launch_rbe_rho_partial_f64(dbox, n, Pk, mx, my, mz, q, x, y, z,
+                                                          part_re, part_im, parts, st, kpt);
+              },
+              &ms);
+          if (rc) break;
+          if (kpt == 4 && parts == rbe_partial_blocks(n)) info.rho_ms_default = ms;
+          if (ms < best_ms) {
+            best_ms = ms;
+            best.rho_kpt = kpt;
+            best.rho_parts = parts;
+          }
+        }
+        if (rc) break;
+      }
+      info.rho_ms = best_ms;
+      if (!info.rho_ms_default) info.rho_ms_default = best_ms;
+      // force scatter (the table of the last evaluation; output to the k-space scratch)
+      RbeForceOut o;
+      o.f_out_x = fkx;
+      o.f_out_y = fky;
+      o.f_out_z = fkz;
+      best_ms = 1e30f;
+      for (int blk : {128, 256, 512}) {
+        if (rc) break;
+        float ms = 0.f;
+        rc = time_it(
+            [&]() {
+              return mixed ? launch_rbe_force_mixed(n, Pk, tab, atoms, o, st, blk)
+                           : launch_rbe_force_f64(n, Pk, tab, q, x, y, z, o, st, blk);
+            },
+            &ms);
+        if (blk == 256) info.force_ms_default = ms;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best.frc_block = blk;
+        }
+      }
+      info.force_ms = best_ms;
+    }
+    if (!rc && prm.neighbor_type == RBX_NEIGHBOR_RBL) {
+      float best_ms = 1e30f;
+      for (int waves : {2, 4, 8, 16}) {
+        const int nb = rbl_fused_grid(mixed, pp.freq, n, cap, nfpart, waves);
+        float ms = 0.f;
+        rc = time_it(
+            [&]() {
+              return launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
+                                      nullptr, cand_count, cand, cap, fpx, fpy, fpz, fpart, nb,
+                                      dflags + 3, st);
+            },
+            &ms);
+        if (rc) break;
+        if (waves == 8) info.rbl_ms_default = ms;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best.rbl_waves = waves;
+        }
+      }
+      info.rbl_ms = best_ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ETRY(rc);
+    ETRY(apply_tuning(best));
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune_cache[key] = best;
+    }
+    ETRY(compute_forces(epoch));  // forces of the current state with the chosen shapes
+  }
+  if (out) {
+    out->rho_kpt = tun.rho_kpt;
+    out->rho_blocks = nparts;
+    out->force_block = tun.frc_block;
+    out->rbl_waves = tun.rbl_waves;
+    out->cache_hit = info.cache_hit;
+    out->rho_ms = info.rho_ms;
+    out->force_ms = info.force_ms;
+    out->rbl_ms = info.rbl_ms;
+    out->rho_ms_default = info.rho_ms_default;
+    out->force_ms_default = info.force_ms_default;
+    out->rbl_ms_default = info.rbl_ms_default;
+  }
   return RBX_OK;
 }
 
@@ -1630,6 +1795,11 @@ int rbx_engine_get_shake(rbx_engine* e, int* nclusters, int* failures) {
   if (nclusters) *nclusters = e->shake_nc;
   if (failures) *failures = f;
   return RBX_OK;
+}
+
+int rbx_engine_autotune(rbx_engine* e, int force, rbx_tuning* out) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->autotune(force != 0, out);
 }
 
 int rbx_engine_set_images(rbx_engine* e, const int* image) {

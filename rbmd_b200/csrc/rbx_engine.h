@@ -91,6 +91,16 @@ struct rbx_engine {
   int shake_a(cudaStream_t s);
   int shake_b(cudaStream_t s);
   int set_shake(int nclusters, const int* clusters, double bond, double angle_deg);
+  // launch shapes picked by the autotuner: k-vectors per thread and atom
+  // blocks of rho(k), atoms per block of the force scatter, waves of the RBL
+  // kernel (defaults = the built-in heuristics)
+  struct Tuning {
+    int rho_kpt = 4, rho_parts = 0, frc_block = 256, rbl_waves = 8;
+  };
+  Tuning tun;
+  int nparts_cap = 0;
+  int autotune(bool force, rbx_tuning* out);
+  int apply_tuning(const Tuning& t);
   // CVFF special bonds (host order): cumulative 1-2/1-3/1-4 counts [n][3],
   // partner host indices [n][spec_max], the atoms that have any, weights
   int spec_max = 0, spec_cap = 0, spec_natoms = 0;

@@ -39,9 +39,10 @@ int rbe_partial_blocks(int n);
 int launch_rbe_rho_partial_f64(const DBox& b, int n, int p, const double* mx, const double* my,
                                const double* mz, const double* q, const double* x,
                                const double* y, const double* z, double* part_re,
-                               double* part_im, int nblocks, cudaStream_t st);
+                               double* part_im, int nblocks, cudaStream_t st, int kpt = 4);
 int launch_rbe_rho_partial_mixed(int n, int p, const int* mi, const uint4* atoms,
-                                 double* part_re, double* part_im, int nblocks, cudaStream_t st);
+                                 double* part_re, double* part_im, int nblocks, cudaStream_t st,
+                                 int kpt = 4);
 int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
                         const double* part_im, const double* mx, const double* my,
                         const double* mz, double alpha, double S, double qqr2e, double qsq,
@@ -52,9 +53,9 @@ int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
 // finalize); when null and energy is requested, one block does the finalize.
 int launch_rbe_force_f64(int n, int p, const KTab* tab, const double* q, const double* x,
                          const double* y, const double* z, const RbeForceOut& out,
-                         cudaStream_t st);
+                         cudaStream_t st, int block = 256);
 int launch_rbe_force_mixed(int n, int p, const KTab* tab, const uint4* atoms,
-                           const RbeForceOut& out, cudaStream_t st);
+                           const RbeForceOut& out, cudaStream_t st, int block = 256);
 // step_dev (may be null): read the step from device memory (step graphs).
 int launch_rbe_sample(int p, const double* tables, const int cnt[3], const double tot[3],
                       uint64_t seed, int64_t step, const int* step_dev, double* mx, double* my,
@@ -102,7 +103,7 @@ struct PairParams {
 int rbl_fused_blocks(int n);
 // Grid of the fused RBL kernel for this form: one wave of resident blocks,
 // at most max_blocks (the capacity of the per-block partial buffer).
-int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks);
+int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int waves = 8);
 // status (device int, may be null = no prefetch): bit 4 set if a row copy timed out.
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
                      const double* x, const double* y, const double* z, const double* q,

@@ -852,11 +852,11 @@ RblChoice rbl_choose(bool mixed, int freq, int cap, bool with_status) {
 }
 }  // namespace
 
-int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks) {
-  // kRblWaves waves of resident blocks: with several waves the block
+int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int waves) {
+  // waves of resident blocks (default 8): with several waves the block
   // scheduler evens out the per-atom work (200k atoms, mixed form: 1 wave
   // 0.59 ms, 3 waves 0.555 ms, 6-12 waves 0.54 ms, 48 waves 0.57 ms)
-  constexpr int kRblWaves = 8;
+  const int kRblWaves = waves > 0 ? waves : 8;
   const RblChoice c = rbl_choose(mixed, freq, cap, true);
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, c.kern, PAIR_BLOCK, c.smem) !=

@@ -30,6 +30,7 @@ constexpr int RBE_WARPS = RBE_BLOCK / 32;
 constexpr int RBE_KPT = 4;
 constexpr int RBE_KGROUP = 32 * RBE_KPT;  // k-slots per warp
 
+template <int KPT>
 __global__ void __launch_bounds__(RBE_BLOCK)
 k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kzs,
                       const double* __restrict__ mx, const double* __restrict__ my,
@@ -37,13 +38,13 @@ k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kz
                       const double* __restrict__ x, const double* __restrict__ y,
                       const double* __restrict__ z, double* __restrict__ part_re,
                       double* __restrict__ part_im) {
-  __shared__ double s_re[RBE_WARPS][RBE_KGROUP];
-  __shared__ double s_im[RBE_WARPS][RBE_KGROUP];
+  __shared__ double s_re[RBE_WARPS][(32 * KPT)];
+  __shared__ double s_im[RBE_WARPS][(32 * KPT)];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int kbase = blockIdx.y * RBE_KGROUP;
-  double kx[RBE_KPT], ky[RBE_KPT], kz[RBE_KPT], sr[RBE_KPT], si[RBE_KPT];
+  const int kbase = blockIdx.y * (32 * KPT);
+  double kx[KPT], ky[KPT], kz[KPT], sr[KPT], si[KPT];
 #pragma unroll
-  for (int t = 0; t < RBE_KPT; ++t) {
+  for (int t = 0; t < KPT; ++t) {
     const int k = kbase + lane + 32 * t;
     const bool ok = k < p;
     // k = 2 pi m / L, evaluated as (2 pi * m) / L like the reference.
@@ -60,7 +61,7 @@ k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kz
   for (int j = w0; j < w1; ++j) {
     const double xj = __ldg(x + j), yj = __ldg(y + j), zj = __ldg(z + j), qj = __ldg(q + j);
 #pragma unroll
-    for (int t = 0; t < RBE_KPT; ++t) {
+    for (int t = 0; t < KPT; ++t) {
       const double dot = kx[t] * xj + ky[t] * yj + kz[t] * zj;
       double s, c;
       sincos(dot, &s, &c);
@@ -69,12 +70,12 @@ k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kz
     }
   }
 #pragma unroll
-  for (int t = 0; t < RBE_KPT; ++t) {
+  for (int t = 0; t < KPT; ++t) {
     s_re[warp][lane + 32 * t] = sr[t];
     s_im[warp][lane + 32 * t] = si[t];
   }
   __syncthreads();
-  for (int s = threadIdx.x; s < RBE_KGROUP; s += RBE_BLOCK) {
+  for (int s = threadIdx.x; s < (32 * KPT); s += RBE_BLOCK) {
     const int k = kbase + s;
     if (k >= p) continue;
     double r = 0.0, im = 0.0;
@@ -100,18 +101,19 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
 // (hi, lo) pair.
 constexpr int RBE_TILE = 32;
 
+template <int KPT>
 __global__ void __launch_bounds__(RBE_BLOCK)
 k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
                         const uint4* __restrict__ atoms, double* __restrict__ part_re,
                         double* __restrict__ part_im) {
-  __shared__ double s_re[RBE_WARPS][RBE_KGROUP];
-  __shared__ double s_im[RBE_WARPS][RBE_KGROUP];
+  __shared__ double s_re[RBE_WARPS][(32 * KPT)];
+  __shared__ double s_im[RBE_WARPS][(32 * KPT)];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int kbase = blockIdx.y * RBE_KGROUP;
-  int m0[RBE_KPT], m1[RBE_KPT], m2[RBE_KPT];
-  float hr[RBE_KPT], lr[RBE_KPT], hi[RBE_KPT], li[RBE_KPT];
+  const int kbase = blockIdx.y * (32 * KPT);
+  int m0[KPT], m1[KPT], m2[KPT];
+  float hr[KPT], lr[KPT], hi[KPT], li[KPT];
 #pragma unroll
-  for (int t = 0; t < RBE_KPT; ++t) {
+  for (int t = 0; t < KPT; ++t) {
     const int k = kbase + lane + 32 * t;
     const bool ok = k < p;
     m0[t] = ok ? mi[3 * k] : 0;
@@ -126,14 +128,14 @@ k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
   const int w0 = a0 + warp * sub, w1 = min(a1, w0 + sub);
   for (int jt = w0; jt < w1; jt += RBE_TILE) {
     const int je = min(w1, jt + RBE_TILE);
-    float tr[RBE_KPT], ti[RBE_KPT];
+    float tr[KPT], ti[KPT];
 #pragma unroll
-    for (int t = 0; t < RBE_KPT; ++t) tr[t] = ti[t] = 0.f;
+    for (int t = 0; t < KPT; ++t) tr[t] = ti[t] = 0.f;
     for (int j = jt; j < je; ++j) {
       const uint4 a = __ldg(atoms + j);
       const float qj = __uint_as_float(a.w);
 #pragma unroll
-      for (int t = 0; t < RBE_KPT; ++t) {
+      for (int t = 0; t < KPT; ++t) {
         const unsigned ph = (unsigned)m0[t] * a.x + (unsigned)m1[t] * a.y + (unsigned)m2[t] * a.z;
         float s, c;
         __sincosf((float)(int)ph * ang, &s, &c);
@@ -142,7 +144,7 @@ k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
       }
     }
 #pragma unroll
-    for (int t = 0; t < RBE_KPT; ++t) {
+    for (int t = 0; t < KPT; ++t) {
       float s, e;
       two_sum(hr[t], tr[t], s, e);
       hr[t] = s;
@@ -153,12 +155,12 @@ k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
     }
   }
 #pragma unroll
-  for (int t = 0; t < RBE_KPT; ++t) {
+  for (int t = 0; t < KPT; ++t) {
     s_re[warp][lane + 32 * t] = (double)hr[t] + (double)lr[t];
     s_im[warp][lane + 32 * t] = (double)hi[t] + (double)li[t];
   }
   __syncthreads();
-  for (int s = threadIdx.x; s < RBE_KGROUP; s += RBE_BLOCK) {
+  for (int s = threadIdx.x; s < (32 * KPT); s += RBE_BLOCK) {
     const int k = kbase + s;
     if (k >= p) continue;
     double r = 0.0, im = 0.0;
@@ -424,19 +426,20 @@ __device__ __forceinline__ void force_epilogue(const ForceEpilogue& ep, int i, d
   }
 }
 
-__global__ void __launch_bounds__(FRC_BLOCK)
+template <int FB>
+__global__ void __launch_bounds__(FB)
 k_rbe_force_f64(int n, int p, const KTab* __restrict__ tab, const double* __restrict__ q,
                 const double* __restrict__ x, const double* __restrict__ y,
                 const double* __restrict__ z, ForceEpilogue ep) {
   __shared__ KTab s_tab[FRC_TABLE];
-  const int i = blockIdx.x * FRC_BLOCK + threadIdx.x;
+  const int i = blockIdx.x * FB + threadIdx.x;
   const bool live = i < n;
   const double xi = live ? x[i] : 0.0, yi = live ? y[i] : 0.0, zi = live ? z[i] : 0.0;
   double fx = 0, fy = 0, fz = 0;
   for (int k0 = 0; k0 < p; k0 += FRC_TABLE) {
     const int kn = min(FRC_TABLE, p - k0);
     __syncthreads();
-    for (int s = threadIdx.x; s < kn; s += FRC_BLOCK) s_tab[s] = tab[k0 + s];
+    for (int s = threadIdx.x; s < kn; s += FB) s_tab[s] = tab[k0 + s];
     __syncthreads();
     if (live) {
       for (int s = 0; s < kn; ++s) {
@@ -463,11 +466,12 @@ struct KTabF {
   float a, b, kx, ky, kz;
 };
 
-__global__ void __launch_bounds__(FRC_BLOCK)
+template <int FB>
+__global__ void __launch_bounds__(FB)
 k_rbe_force_mixed(int n, int p, const KTab* __restrict__ tab, const uint4* __restrict__ atoms,
                   ForceEpilogue ep) {
   __shared__ KTabF s_tab[FRC_TABLE];
-  const int i = blockIdx.x * FRC_BLOCK + threadIdx.x;
+  const int i = blockIdx.x * FB + threadIdx.x;
   const bool live = i < n;
   const uint4 a = live ? atoms[i] : make_uint4(0, 0, 0, 0);
   const float ang = (float)(2.0 * RBX_PI / 4294967296.0);
@@ -475,7 +479,7 @@ k_rbe_force_mixed(int n, int p, const KTab* __restrict__ tab, const uint4* __res
   for (int k0 = 0; k0 < p; k0 += FRC_TABLE) {
     const int kn = min(FRC_TABLE, p - k0);
     __syncthreads();
-    for (int s = threadIdx.x; s < kn; s += FRC_BLOCK) {
+    for (int s = threadIdx.x; s < kn; s += FB) {
       const KTab t = tab[k0 + s];
       KTabF f;
       f.m0 = t.m[0];
@@ -677,25 +681,45 @@ int rbe_partial_blocks(int n) {
   return blocks < 1 ? 1 : blocks;
 }
 
+// kpt: k-vectors per thread (1, 2, 4 or 8; 32 kpt per block); the partial
+// sums do not depend on it.
 int launch_rbe_rho_partial_f64(const DBox& b, int n, int p, const double* mx, const double* my,
                                const double* mz, const double* q, const double* x,
                                const double* y, const double* z, double* part_re,
-                               double* part_im, int nblocks, cudaStream_t st) {
+                               double* part_im, int nblocks, cudaStream_t st, int kpt) {
   if (n <= 0 || p <= 0) return RBX_OK;
   const int chunk = (n + nblocks - 1) / nblocks;
-  dim3 grid(nblocks, (p + RBE_KGROUP - 1) / RBE_KGROUP);
-  k_rbe_rho_partial_f64<<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, b.len[0], b.len[1], b.len[2],
-                                                    mx, my, mz, q, x, y, z, part_re, part_im);
+  dim3 grid(nblocks, (p + 32 * kpt - 1) / (32 * kpt));
+#define RHO_F64(K)                                                                             \
+  k_rbe_rho_partial_f64<K><<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, b.len[0], b.len[1],       \
+                                                       b.len[2], mx, my, mz, q, x, y, z,       \
+                                                       part_re, part_im)
+  switch (kpt) {
+    case 1: RHO_F64(1); break;
+    case 2: RHO_F64(2); break;
+    case 8: RHO_F64(8); break;
+    default: RHO_F64(4); break;
+  }
+#undef RHO_F64
   count_launch();
   return check_launch("rbe_rho_partial_f64");
 }
 
 int launch_rbe_rho_partial_mixed(int n, int p, const int* mi, const uint4* atoms,
-                                 double* part_re, double* part_im, int nblocks, cudaStream_t st) {
+                                 double* part_re, double* part_im, int nblocks, cudaStream_t st,
+                                 int kpt) {
   if (n <= 0 || p <= 0) return RBX_OK;
   const int chunk = (n + nblocks - 1) / nblocks;
-  dim3 grid(nblocks, (p + RBE_KGROUP - 1) / RBE_KGROUP);
-  k_rbe_rho_partial_mixed<<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, mi, atoms, part_re, part_im);
+  dim3 grid(nblocks, (p + 32 * kpt - 1) / (32 * kpt));
+#define RHO_MIX(K) \
+  k_rbe_rho_partial_mixed<K><<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, mi, atoms, part_re, part_im)
+  switch (kpt) {
+    case 1: RHO_MIX(1); break;
+    case 2: RHO_MIX(2); break;
+    case 8: RHO_MIX(8); break;
+    default: RHO_MIX(4); break;
+  }
+#undef RHO_MIX
   count_launch();
   return check_launch("rbe_rho_partial_mixed");
 }
@@ -753,21 +777,32 @@ static ForceEpilogue make_ep(const RbeForceOut& o) {
   return ep;
 }
 
+// block: atoms per block (128, 256 or 512); the forces do not depend on it.
 int launch_rbe_force_f64(int n, int p, const KTab* tab, const double* q, const double* x,
                          const double* y, const double* z, const RbeForceOut& out,
-                         cudaStream_t st) {
+                         cudaStream_t st, int block) {
   if (n <= 0) return RBX_OK;
-  k_rbe_force_f64<<<(n + FRC_BLOCK - 1) / FRC_BLOCK, FRC_BLOCK, 0, st>>>(n, p, tab, q, x, y, z,
-                                                                         make_ep(out));
+  const ForceEpilogue ep = make_ep(out);
+  if (block == 128)
+    k_rbe_force_f64<128><<<(n + 127) / 128, 128, 0, st>>>(n, p, tab, q, x, y, z, ep);
+  else if (block == 512)
+    k_rbe_force_f64<512><<<(n + 511) / 512, 512, 0, st>>>(n, p, tab, q, x, y, z, ep);
+  else
+    k_rbe_force_f64<256><<<(n + 255) / 256, 256, 0, st>>>(n, p, tab, q, x, y, z, ep);
   count_launch();
   return check_launch("rbe_force_f64");
 }
 
 int launch_rbe_force_mixed(int n, int p, const KTab* tab, const uint4* atoms,
-                           const RbeForceOut& out, cudaStream_t st) {
+                           const RbeForceOut& out, cudaStream_t st, int block) {
   if (n <= 0) return RBX_OK;
-  k_rbe_force_mixed<<<(n + FRC_BLOCK - 1) / FRC_BLOCK, FRC_BLOCK, 0, st>>>(n, p, tab, atoms,
-                                                                           make_ep(out));
+  const ForceEpilogue ep = make_ep(out);
+  if (block == 128)
+    k_rbe_force_mixed<128><<<(n + 127) / 128, 128, 0, st>>>(n, p, tab, atoms, ep);
+  else if (block == 512)
+    k_rbe_force_mixed<512><<<(n + 511) / 512, 512, 0, st>>>(n, p, tab, atoms, ep);
+  else
+    k_rbe_force_mixed<256><<<(n + 255) / 256, 256, 0, st>>>(n, p, tab, atoms, ep);
   count_launch();
   return check_launch("rbe_force_mixed");
 }

@@ -106,6 +106,7 @@ EXPORTS = [
     "rbx_lammps_gauss_velocities", "rbx_engine_set_nose_hoover", "rbx_engine_get_thermostat",
     "rbx_engine_set_shake", "rbx_engine_get_shake", "rbx_engine_set_special", "rbx_special_build",
     "rbx_rbsog_params", "rbx_rbsog_sample", "rbx_rbsog_force", "rbx_pair_force_verlet_sog",
+    "rbx_engine_autotune", "rbx_batch_autotune",
 ]
 
 
@@ -114,6 +115,13 @@ class RbsogInfo(C.Structure):
                 ("w0", C.c_double), ("S", C.c_double), ("S_npt", C.c_double),
                 ("self_coeff", C.c_double), ("taylor", C.c_double * 6), ("n_direct", C.c_int),
                 ("S_full", C.c_double)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("rho_kpt", C.c_int), ("rho_blocks", C.c_int), ("force_block", C.c_int),
+                ("rbl_waves", C.c_int), ("cache_hit", C.c_int), ("rho_ms", C.c_float),
+                ("force_ms", C.c_float), ("rbl_ms", C.c_float), ("rho_ms_default", C.c_float),
+                ("force_ms_default", C.c_float), ("rbl_ms_default", C.c_float)]
 
 
 class LammpsInfo(C.Structure):
@@ -196,6 +204,8 @@ def lib():
     L.rbx_engine_set_special.argtypes = [vp, ip, vp, vp, dp, dp, dp]
     L.rbx_special_build.argtypes = [ip, ip, vp, ip, vp, ip, vp, C.POINTER(C.c_int), vp, vp]
     L.rbx_rbsog_params.argtypes = [ip, dp, B, C.POINTER(RbsogInfo), vp, vp, vp]
+    L.rbx_engine_autotune.argtypes = [vp, ip, C.POINTER(Tuning)]
+    L.rbx_batch_autotune.argtypes = [vp]
     L.rbx_rbsog_sample.argtypes = [B, ip, dp, ip, C.c_uint64, C.c_int64, vp, vp, vp, vp]
     L.rbx_rbsog_force.argtypes = [B, ip, dp, dp, dp, dp, ip, ip] + [vp] * 10 + [
         C.POINTER(C.c_double), vp]
@@ -545,6 +555,13 @@ class Engine:
     def set_alpha(self, alpha):
         check(lib().rbx_engine_set_alpha(self._h, float(alpha)), "rbx_engine_set_alpha")
 
+    def autotune(self, force=False):
+        """rbx_engine_autotune: launch shapes timed on the current state (cached per size bin)."""
+        t = Tuning()
+        check(lib().rbx_engine_autotune(self._h, int(bool(force)), C.byref(t)),
+              "rbx_engine_autotune")
+        return {f: getattr(t, f) for f, _ in Tuning._fields_}
+
     def set_nose_hoover(self, t_start, t_stop, t_damp, num_steps=0, kb=1.0, mvv2e=1.0,
                         tdof=0.0):
         """NVT with RBMD's Nose-Hoover chain; t_damp <= 0 goes back to NVE."""
@@ -641,6 +658,10 @@ class Batch:
         self._h = lib().rbx_batch_create(arr, len(self.engines))
         if not self._h:
             raise RbxError(f"rbx_batch_create failed: {last_error()}")
+
+    def autotune(self):
+        """rbx_batch_autotune: tune each replica (one timing per size bin)."""
+        check(lib().rbx_batch_autotune(self._h), "rbx_batch_autotune")
 
     def step(self, nsteps=1):
         check(lib().rbx_batch_step(self._h, nsteps), "rbx_batch_step")

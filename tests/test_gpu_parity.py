@@ -1034,3 +1034,43 @@ def test_water_config_from_files(cuda, rbx, tmp_path, water3k):
     assert err < 1e-4 and rv < 1e-9
     a.close()
     b.close()
+
+
+def test_autotune_keeps_parity_and_caches(cuda, rbx, oracle, sys4k):
+    """The autotuner picks valid launch shapes, the forces with them still
+    match the oracle, a second engine of the same size bin takes the cached
+    choice without timing, and the tuned step graph equals the tuned
+    launch-by-launch step bit for bit."""
+    s = sys4k
+    box = oracle.Box.make(s["lo"], s["hi"])
+    m = oracle.rbe_sample_philox(box, 0.16, 100, 7, 0)
+    import __graft_entry__ as ge
+
+    want = ge._oracle_forces(s, m)
+    e = rbx.Engine(s, precision=rbx.MIXED, seed=4)
+    e.set_k_samples(*m)
+    e.compute_forces(0)
+    t = e.autotune(force=True)
+    assert t["cache_hit"] == 0 and t["rho_kpt"] in (1, 2, 4, 8)
+    assert t["force_block"] in (128, 256, 512) and t["rbl_waves"] in (2, 4, 8, 16)
+    assert t["rho_blocks"] >= 1 and t["rho_ms"] <= t["rho_ms_default"] + 1e-6
+    assert systems.rel_rms(e.get_state()["force"], want) < 1e-5
+    e2 = rbx.Engine(s, precision=rbx.MIXED, seed=4)
+    e2.compute_forces(0)
+    t2 = e2.autotune()
+    assert t2["cache_hit"] == 1
+    for k in ("rho_kpt", "rho_blocks", "force_block", "rbl_waves"):
+        assert t2[k] == t[k], k
+    runs = []
+    for graph in (True, False):
+        x = rbx.Engine(s, precision=rbx.MIXED, seed=9)
+        x.set_step_graph(graph)
+        x.compute_forces(0)
+        x.autotune()
+        x.step(10)
+        runs.append(x.get_state())
+        x.close()
+    for key in ("pos", "vel", "force"):
+        assert np.array_equal(runs[0][key], runs[1][key]), key
+    e.close()
+    e2.close()
