@@ -558,7 +558,8 @@ int rbx_engine::autotune(bool force, rbx_tuning* out) {
     cudaEvent_t e0, e1;
     ETRY(cuda_ok(cudaEventCreate(&e0), "cudaEventCreate"));
     ETRY(cuda_ok(cudaEventCreate(&e1), "cudaEventCreate"));
-    constexpr int kReps = 5;
+    constexpr int kReps = 10;
+    constexpr float kMargin = 0.97f;  // a candidate must beat the default by 3 %
     // mean device time per launch of fn (2 untimed launches first)
     auto time_it = [&](auto&& fn, float* ms) -> int {
       for (int r = 0; r < 2; ++r) ETRY(fn());
@@ -573,12 +574,32 @@ int rbx_engine::autotune(bool force, rbx_tuning* out) {
     };
     Tuning best = tun;
     int rc = RBX_OK;
+    // the fastest candidate, unless the built-in shape is within the margin
+    struct Cand {
+      int a, b;
+      float ms;
+    };
+    auto pick = [&](const std::vector<Cand>& c, int def_a, int def_b, float* def_ms) {
+      Cand best_c = c.front();
+      *def_ms = 0.f;
+      for (const Cand& k : c) {
+        if (k.ms < best_c.ms) best_c = k;
+        if (k.a == def_a && k.b == def_b) *def_ms = k.ms;
+      }
+      if (*def_ms > 0.f && !(best_c.ms < kMargin * *def_ms)) return Cand{def_a, def_b, *def_ms};
+      return best_c;
+    };
     if (P > 0) {
       // rho(k): k-vectors per thread x atom blocks
-      float best_ms = 1e30f;
-      const int sm = sm_count();
+      std::vector<Cand> c;
+      const int sm = sm_count(), def_parts = rbe_partial_blocks(n);
+      std::vector<int> parts_list = {def_parts};
       for (int mult : {1, 2, 4, 8}) {
-        int parts = std::min(std::min(mult * sm, nparts_cap), std::max(1, (n + 31) / 32));
+        const int parts = std::min(std::min(mult * sm, nparts_cap), std::max(1, (n + 31) / 32));
+        if (std::find(parts_list.begin(), parts_list.end(), parts) == parts_list.end())
+          parts_list.push_back(parts);
+      }
+      for (int parts : parts_list)
         for (int kpt : {1, 2, 4, 8}) {
           float ms = 0.f;
           rc = time_it(
@@ -590,23 +611,20 @@ int rbx_engine::autotune(bool force, rbx_tuning* out) {
               },
               &ms);
           if (rc) break;
-          if (kpt == 4 && parts == rbe_partial_blocks(n)) info.rho_ms_default = ms;
-          if (ms < best_ms) {
-            best_ms = ms;
-            best.rho_kpt = kpt;
-            best.rho_parts = parts;
-          }
+          c.push_back({kpt, parts, ms});
         }
-        if (rc) break;
+      if (!rc) {
+        const Cand r = pick(c, 4, def_parts, &info.rho_ms_default);
+        best.rho_kpt = r.a;
+        best.rho_parts = r.b;
+        info.rho_ms = r.ms;
       }
-      info.rho_ms = best_ms;
-      if (!info.rho_ms_default) info.rho_ms_default = best_ms;
       // force scatter (the table of the last evaluation; output to the k-space scratch)
       RbeForceOut o;
       o.f_out_x = fkx;
       o.f_out_y = fky;
       o.f_out_z = fkz;
-      best_ms = 1e30f;
+      c.clear();
       for (int blk : {128, 256, 512}) {
         if (rc) break;
         float ms = 0.f;
@@ -616,16 +634,16 @@ int rbx_engine::autotune(bool force, rbx_tuning* out) {
                            : launch_rbe_force_f64(n, Pk, tab, q, x, y, z, o, st, blk);
             },
             &ms);
-        if (blk == 256) info.force_ms_default = ms;
-        if (ms < best_ms) {
-          best_ms = ms;
-          best.frc_block = blk;
-        }
+        c.push_back({blk, 0, ms});
       }
-      info.force_ms = best_ms;
+      if (!rc) {
+        const Cand r = pick(c, 256, 0, &info.force_ms_default);
+        best.frc_block = r.a;
+        info.force_ms = r.ms;
+      }
     }
     if (!rc && prm.neighbor_type == RBX_NEIGHBOR_RBL) {
-      float best_ms = 1e30f;
+      std::vector<Cand> c;
       for (int waves : {2, 4, 8, 16}) {
         const int nb = rbl_fused_grid(mixed, pp.freq, n, cap, nfpart, waves);
         float ms = 0.f;
@@ -637,13 +655,13 @@ int rbx_engine::autotune(bool force, rbx_tuning* out) {
             },
             &ms);
         if (rc) break;
-        if (waves == 8) info.rbl_ms_default = ms;
-        if (ms < best_ms) {
-          best_ms = ms;
-          best.rbl_waves = waves;
-        }
+        c.push_back({waves, 0, ms});
       }
-      info.rbl_ms = best_ms;
+      if (!rc) {
+        const Cand r = pick(c, 8, 0, &info.rbl_ms_default);
+        best.rbl_waves = r.a;
+        info.rbl_ms = r.ms;
+      }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -1054,6 +1054,7 @@ def test_autotune_keeps_parity_and_caches(cuda, rbx, oracle, sys4k):
     assert t["cache_hit"] == 0 and t["rho_kpt"] in (1, 2, 4, 8)
     assert t["force_block"] in (128, 256, 512) and t["rbl_waves"] in (2, 4, 8, 16)
     assert t["rho_blocks"] >= 1 and t["rho_ms"] <= t["rho_ms_default"] + 1e-6
+    assert t["rbl_ms"] <= t["rbl_ms_default"] + 1e-6
     assert systems.rel_rms(e.get_state()["force"], want) < 1e-5
     e2 = rbx.Engine(s, precision=rbx.MIXED, seed=4)
     e2.compute_forces(0)
