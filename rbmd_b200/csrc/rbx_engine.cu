@@ -446,9 +446,13 @@ int rbx_engine::real_space(const int* epoch_dev) {
                               spec_w[0], spec_w[1], spec_w[2], where, x, y, z, q, type, key_a,
                               key_b, epoch, epoch_dev, fpx, fpy, fpz, fpart + (size_t)nrbl * 3, st);
   }
-  if (sog_pair)
+  if (sog_pair) {
+    if (mixed)
+      return launch_verlet_sog_mixed(sogp, pp.sf, n, atoms, type, cand_count, cand, cap, fpx, fpy,
+                                     fpz, st);
     return launch_verlet_sog(sogp, n, x, y, z, q, type, cand_count, cand, cap, fpx, fpy, fpz,
                              nullptr, st);
+  }
   return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, fpx, fpy,
                                  fpz, nullptr, epart, nfpart, st);
 }

@@ -214,6 +214,10 @@ int launch_rbsog_finalize(const DBox& b, int p, int nparts, const double* part_r
                           cudaStream_t st);
 int verlet_sog_blocks(int n);
 // epart (may be null) receives [blocks][2] = {E_LJ, E_coul} per-block sums.
+// Mixed form: fixed-point records, FP32 pair terms, no energies.
+int launch_verlet_sog_mixed(const SogPairParams& sp, const float sf[3], int n, const uint4* atoms,
+                            const int* type, const int* cand_count, const int* cand, int cap,
+                            double* fx, double* fy, double* fz, cudaStream_t st);
 int launch_verlet_sog(const SogPairParams& sp, int n, const double* x, const double* y,
                       const double* z, const double* q, const int* type, const int* cand_count,
                       const int* cand, int cap, double* fx, double* fy, double* fz, double* epart,

@@ -233,6 +233,59 @@ k_verlet_sog(SogPairParams sp, int n, const double* __restrict__ x, const double
     }
   }
 }
+// Mixed form of the VERLET-SOG force: the pair vector is the exact wrapped
+// difference of the fixed-point records scaled by L / 2^32 per axis, the LJ
+// and short-range SOG terms are FP32 (cut decided on the FP32 r^2), each lane
+// sums its pairs in FP32 and the warp reduces in FP64.
+__global__ void __launch_bounds__(SOG_PAIR_BLOCK)
+k_verlet_sog_mixed(SogPairParams sp, float sfx, float sfy, float sfz, int n,
+                   const uint4* __restrict__ atoms, const int* __restrict__ type,
+                   const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
+                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+  __shared__ float s_eps[256], s_s6[256];
+  const int nt2 = sp.ntypes * sp.ntypes;
+  for (int t = threadIdx.x; t < nt2; t += SOG_PAIR_BLOCK) {
+    s_eps[t] = (float)sp.lj_eps[t];
+    s_s6[t] = (float)sp.lj_s6[t];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int i = blockIdx.x * (SOG_PAIR_BLOCK / 32) + wib;
+  if (i >= n) return;
+  const uint4 ai = atoms[i];
+  const int ti = type[i];
+  const float qi = __uint_as_float(ai.w);
+  const float cut2 = (float)(sp.cut_off * sp.cut_off);
+  const float qe = (float)sp.qqr2e;
+  float c[6];
+  for (int k = 0; k < 6; ++k) c[k] = (float)sp.taylor[k];
+  const int cnt = min(cand_count[i], cap);
+  float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+  for (int t = lane; t < cnt; t += 32) {
+    const int j = cand[(size_t)i * cap + t];
+    const uint4 aj = __ldg(atoms + j);
+    const float dx = (float)(int)(aj.x - ai.x) * sfx, dy = (float)(int)(aj.y - ai.y) * sfy,
+                dz = (float)(int)(aj.z - ai.z) * sfz;
+    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    if (!(d2 < cut2)) continue;
+    const int pt = ti * sp.ntypes + __ldg(type + j);
+    const float r2inv = 1.0f / d2;
+    const float sd6 = s_s6[pt] * (r2inv * r2inv * r2inv);
+    const float flj = -24.f * s_eps[pt] * ((2.f * sd6 - 1.f) * sd6) * r2inv;
+    const float rinv = rsqrtf(d2);
+    const float poly = c[0] + d2 * (c[1] + d2 * (c[2] + d2 * (c[3] + d2 * (c[4] + d2 * c[5]))));
+    const float f = flj - qe * qi * __uint_as_float(aj.w) * (rinv * r2inv + poly);
+    f0 = fmaf(f, dx, f0);
+    f1 = fmaf(f, dy, f1);
+    f2 = fmaf(f, dz, f2);
+  }
+  const double g0 = warp_sum((double)f0), g1 = warp_sum((double)f1), g2 = warp_sum((double)f2);
+  if (lane == 0) {
+    fx[i] = g0;
+    fy[i] = g1;
+    fz[i] = g2;
+  }
+}
 }  // namespace
 
 int launch_rbsog_sample(int p, const RbsogTables& t, uint64_t seed, uint64_t step,
@@ -286,4 +339,20 @@ int launch_verlet_sog(const SogPairParams& sp, int n, const double* x, const dou
   return check_launch("verlet_sog");
 }
 
+}  // namespace rbx
+
+namespace rbx {
+int launch_verlet_sog_mixed(const SogPairParams& sp, const float sf[3], int n, const uint4* atoms,
+                            const int* type, const int* cand_count, const int* cand, int cap,
+                            double* fx, double* fy, double* fz, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  if (sp.ntypes * sp.ntypes > 256) {
+    set_error("VERLET-SOG mixed form: at most 16 atom types");
+    return RBX_ERR_INVALID;
+  }
+  k_verlet_sog_mixed<<<verlet_sog_blocks(n), SOG_PAIR_BLOCK, 0, st>>>(
+      sp, sf[0], sf[1], sf[2], n, atoms, type, cand_count, cand, cap, fx, fy, fz);
+  count_launch();
+  return check_launch("verlet_sog_mixed");
+}
 }  // namespace rbx
