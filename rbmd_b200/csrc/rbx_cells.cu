@@ -581,6 +581,29 @@ int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, con
   return check_launch("full_list");
 }
 
+// dst[a][idx[i]] = src[a][i] for every array of the set (one launch).
+__global__ void k_scatter_set(int n, const int* __restrict__ idx, ArraySet s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = idx[i];
+#pragma unroll
+  for (int a = 0; a < ArraySet::kMaxF64; ++a)
+    if (a < s.nf64) s.dst_f64[a][p] = s.src_f64[a][i];
+#pragma unroll
+  for (int a = 0; a < ArraySet::kMaxI32; ++a)
+    if (a < s.ni32) s.dst_i32[a][p] = s.src_i32[a][i];
+#pragma unroll
+  for (int a = 0; a < ArraySet::kMaxU64; ++a)
+    if (a < s.nu64) s.dst_u64[a][p] = s.src_u64[a][i];
+}
+
+int launch_scatter_set(int n, const int* idx, const ArraySet& set, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_scatter_set<<<(n + 255) / 256, 256, 0, st>>>(n, idx, set);
+  count_launch();
+  return check_launch("scatter_set");
+}
+
 int launch_move_set(int n, const int* perm, const ArraySet& set, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
   k_move_set<<<(n + 255) / 256, 256, 0, st>>>(n, perm, set);

@@ -1016,19 +1016,50 @@ int rbx_engine::step_host(const double* xin, const double* vin, double* xout, do
   ETRY(cuda_ok(cudaMemcpyAsync(stage + 3 * N, vin, sizeof(double) * 3 * N, cudaMemcpyHostToDevice,
                                st),
                "H2D"));
+  ArraySet in{};
   double* dst[] = {x, y, z, vx, vy, vz};
-  for (int a = 0; a < 6; ++a) ETRY(launch_gather_f64(n, orig, stage + a * N, dst[a], st));
-  ETRY(step(1));
-  const double* src[] = {x, y, z, vx, vy, vz, fx, fy, fz};
-  for (int a = 0; a < 9; ++a) ETRY(launch_scatter_f64(n, orig, src[a], stage + a * N, st));
-  ETRY(cuda_ok(cudaMemcpyAsync(xout, stage, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st),
-               "D2H"));
-  ETRY(cuda_ok(cudaMemcpyAsync(vout, stage + 3 * N, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost,
-                               st),
-               "D2H"));
-  ETRY(cuda_ok(cudaMemcpyAsync(fout, stage + 6 * N, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost,
-                               st),
-               "D2H"));
+  for (int a = 0; a < 6; ++a) {
+    in.src_f64[a] = stage + a * N;
+    in.dst_f64[a] = dst[a];
+  }
+  in.nf64 = 6;
+  ETRY(launch_move_set(n, orig, in, st));  // host order -> cell order
+  // outputs: cell order -> host order, then three copies out, all queued on st
+  auto queue_out = [&]() -> int {
+    ArraySet out{};
+    const double* src[] = {x, y, z, vx, vy, vz, fx, fy, fz};
+    for (int a = 0; a < 9; ++a) {
+      out.src_f64[a] = src[a];
+      out.dst_f64[a] = stage + a * N;
+    }
+    out.nf64 = 9;
+    ETRY(launch_scatter_set(n, orig, out, st));
+    ETRY(cuda_ok(cudaMemcpyAsync(xout, stage, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st),
+                 "D2H"));
+    ETRY(cuda_ok(cudaMemcpyAsync(vout, stage + 3 * N, sizeof(double) * 3 * N,
+                                 cudaMemcpyDeviceToHost, st),
+                 "D2H"));
+    return cuda_ok(cudaMemcpyAsync(fout, stage + 6 * N, sizeof(double) * 3 * N,
+                                   cudaMemcpyDeviceToHost, st),
+                   "D2H");
+  };
+  if (!have_forces) ETRY(compute_forces(epoch));
+  if (use_graph && !profiling && have_cache && prm.skin > 0.0) {
+    // the graph step and the copies out behind it, one host synchronisation
+    if (graph_dirty || !graph_exec) ETRY(capture_step_graph());
+    ETRY(graph_run_begin(st));
+    ETRY(cuda_ok(cudaGraphLaunch(graph_exec, st), "cudaGraphLaunch"));
+    ETRY(cuda_ok(cudaMemcpyAsync(run_flags, dflags, sizeof(int) * 6, cudaMemcpyDeviceToHost, st),
+                 "D2H"));
+    ETRY(queue_out());
+    ETRY(cuda_ok(cudaStreamSynchronize(st), "step_host sync"));
+    const bool replay = run_flags[0] || (run_flags[1] & 1);
+    ETRY(graph_run_end(1));  // on overflow: state restored, the step replayed
+    if (!replay) return RBX_OK;
+  } else {
+    ETRY(step(1));
+  }
+  ETRY(queue_out());
   return cuda_ok(cudaStreamSynchronize(st), "step_host sync");
 }
 

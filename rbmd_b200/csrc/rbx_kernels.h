@@ -260,6 +260,8 @@ struct ArraySet {
 };
 // perm may be null (plain copy).
 int launch_move_set(int n, const int* perm, const ArraySet& set, cudaStream_t st);
+// dst[a][idx[i]] = src[a][i] (host order <- cell order).
+int launch_scatter_set(int n, const int* idx, const ArraySet& set, cudaStream_t st);
 int launch_fill_i32(int n, int* p, int v, cudaStream_t st);
 int launch_zero_u64(unsigned long long* p, cudaStream_t st);
 int launch_add_i32(int* p, int v, cudaStream_t st);
