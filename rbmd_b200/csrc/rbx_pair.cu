@@ -215,7 +215,7 @@ __device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
 // time from its tail.
 // ---------------------------------------------------------------------------
 template <bool MIXED, int SEL, bool PREFETCH>
-__global__ void __launch_bounds__(PAIR_BLOCK, 3)
+__global__ void __launch_bounds__(PAIR_BLOCK, MIXED ? 4 : 3)  // no spills in either form
 k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
             const double* __restrict__ y, const double* __restrict__ z,
             const double* __restrict__ q, const int* __restrict__ type,

@@ -357,6 +357,38 @@ def test_engine_rbl_pairs_bit_exact(cuda, rbx, oracle, sys4k, prec):
         e.close()
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_engine_rbl_pairs_between_rebuilds(cuda, rbx, oracle, prec):
+    """The engine keeps its candidate rows between skin rebuilds.  After
+    dynamics that moved the atoms up to skin / 2 from the list build, the core
+    and shell pairs of each epoch equal the oracle's lists built from the
+    current positions."""
+    s = systems.lj_electrolyte(4000, seed=31, temperature=3.0)
+    e = rbx.Engine(s, precision=prec, seed=5)
+    e.compute_forces(epoch=0)
+    checked = 0
+    for k in range(8):
+        e.step(6)
+        st = e.get_state()
+        s2 = dict(s, pos=st["pos"])
+        epoch = 1000 + k
+        e.compute_forces(epoch=epoch)  # keeps the rows unless the skin test fails
+        *_, gid, cnt, rows, cc, core, sc, shell = _ref_lists(oracle, s2, epoch, 4)
+        gc, gs = e.rbl_pairs()
+        want_c = {(int(gid[i]), int(gid[j])) for i in range(s["n"]) for j in core[i, :cc[i]]}
+        want_s = {(int(gid[i]), int(gid[j])) for i in range(s["n"]) for j in shell[i, :sc[i]]}
+        got_c = set(map(tuple, gc.tolist()))
+        got_s = set(map(tuple, gs.tolist()))
+        if prec == 0:
+            assert got_c == want_c and got_s == want_s, k
+        else:
+            assert len(got_c ^ want_c) <= 2 and len(got_s ^ want_s) <= 2, k
+        checked += 1
+    stats = e.stats()
+    assert checked == 8 and 1 <= stats.rebuilds < stats.force_calls
+    e.close()
+
+
 def test_engine_philox_matches_oracle_engine(cuda, rbx, oracle, sys4k):
     """Full velocity-Verlet steps with on-device Philox k-samples and RBL
     batches: the first steps agree with the oracle's step to FP64 round-off."""
