@@ -21,14 +21,13 @@ namespace rbx {
 
 // ---------------------------------------------------------------------------
 // rho(k) partial sums: block (bx, by) covers atom chunk bx and k-group by.
-// A thread owns RBE_KPT k-vectors {kg*128 + lane + 32*t}; warps of the block
-// take disjoint atom sub-ranges; the block combines its warps in fixed order
-// and writes one partial per k.  No atomics: the result is deterministic.
+// A thread owns KPT k-vectors {kg*32*KPT + lane + 32*t} (KPT a template
+// parameter, default 4); warps of the block take disjoint atom sub-ranges; the
+// block combines its warps in fixed order and writes one partial per k.  No
+// atomics: the result is deterministic.
 // ---------------------------------------------------------------------------
 constexpr int RBE_BLOCK = 256;
 constexpr int RBE_WARPS = RBE_BLOCK / 32;
-constexpr int RBE_KPT = 4;
-constexpr int RBE_KGROUP = 32 * RBE_KPT;  // k-slots per warp
 
 template <int KPT>
 __global__ void __launch_bounds__(RBE_BLOCK)
@@ -375,7 +374,6 @@ k_rbe_energy_sum(int p, const double* __restrict__ kterm, double alpha, double V
 // Epilogue variants: plain store of F_k, or the fused combine
 // F = F_pair - mean + F_k with the second velocity-Verlet half kick.
 // ---------------------------------------------------------------------------
-constexpr int FRC_BLOCK = 256;
 constexpr int FRC_TABLE = 512;  // k entries staged per pass
 
 struct ForceEpilogue {
