@@ -171,7 +171,7 @@ int rbx_batch_step(rbx_batch* b, int nsteps) {
   }
   int rc = rbx_batch::ok(cudaStreamSynchronize(b->st), "batch sync");
   for (rbx_engine* e : b->eng)
-    if (!rc) rc = e->graph_run_end(nsteps);
+    if (!rc) rc = e->graph_run_end(nsteps, e->graph_step_launches);
   return rc;
 }
 

@@ -69,8 +69,21 @@ rbx_engine::~rbx_engine() {
     if (ev[i]) cudaEventDestroy(ev[i]);
   for (cudaEvent_t e : pev) cudaEventDestroy(e);
   release_graph();
+  release_host_graphs();
+  if (ev_side) cudaEventDestroy(ev_side);
+  if (st_side) cudaStreamDestroy(st_side);
   if (st_body) cudaStreamDestroy(st_body);
   if (st) cudaStreamDestroy(st);
+}
+
+void rbx_engine::release_host_graphs() {
+  for (int k = 0; k < 2; ++k) {
+    if (hexec[k]) cudaGraphExecDestroy(hexec[k]);
+    if (hgraph[k]) cudaGraphDestroy(hgraph[k]);
+    hexec[k] = nullptr;
+    hgraph[k] = nullptr;
+  }
+  host_graph_dirty = true;
 }
 
 void rbx_engine::release_graph() {
@@ -102,6 +115,8 @@ int rbx_engine::init() {
   ETRY(require_device());
   ETRY(cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate"));
   ETRY(cuda_ok(cudaStreamCreateWithFlags(&st_body, cudaStreamNonBlocking), "cudaStreamCreate"));
+  ETRY(cuda_ok(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking), "cudaStreamCreate"));
+  ETRY(cuda_ok(cudaEventCreateWithFlags(&ev_side, cudaEventDisableTiming), "cudaEventCreate"));
   dbox = make_dbox(box);
   const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
   if (!(prm.cut_off > 0.0) || prm.skin < 0.0 || (rbl && !(prm.r_core > 0.0)) ||
@@ -294,7 +309,7 @@ int rbx_engine::set_state(const int* hgid, const int* htype, const double* hq, c
   have_cache = false;
   have_forces = false;
   epoch = 0;
-  graph_dirty = true;
+  graph_dirty = host_graph_dirty = true;
   ++graph_version;
   return RBX_OK;
 }
@@ -408,7 +423,7 @@ int rbx_engine::rebuild() {
     cap = ((int)(maxc * 1.2) + 31) / 32 * 32;
     ETRY(alloc(&cand, (size_t)n * cap));
     nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart, tun.rbl_waves);
-    graph_dirty = true;  // the list moved
+    graph_dirty = host_graph_dirty = true;  // the list moved
     ++graph_version;
     ETRY(launch_fill_i32(1, dflags + 1, 0, st));
     ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
@@ -538,7 +553,7 @@ int rbx_engine::apply_tuning(const Tuning& t) {
   if (P > 0) nparts = t.rho_parts > 0 ? std::min(t.rho_parts, nparts_cap) : rbe_partial_blocks(n);
   if (prm.neighbor_type == RBX_NEIGHBOR_RBL)
     nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart, tun.rbl_waves);
-  graph_dirty = true;
+  graph_dirty = host_graph_dirty = true;
   ++graph_version;
   return RBX_OK;
 }
@@ -863,11 +878,15 @@ int rbx_engine::capture_step_graph() {
 // a batch graph): the conditional handle is created on g, the IF node goes
 // after what st has captured so far, its body is captured on st_body.
 int rbx_engine::capture_step_into(cudaGraph_t g) {
-  cudaGraphConditionalHandle cond;
-  ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault),
-               "cudaGraphConditionalHandleCreate"));
   const unsigned long long l0 = rbx_launch_count();
-  const double thr = prm.skin * 0.5;
+  ETRY(capture_step_head());
+  ETRY(capture_step_tail(g));
+  graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
+  return RBX_OK;
+}
+
+// First part of a step: half kick, drift with the skin check (+ SHAKE).
+int rbx_engine::capture_step_head() {
   if (nh_on) ETRY(nh_initial(dflags + 4, 1, st));  // the device epoch is still the last step's
   ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
   ETRY(launch_zero_u64(max_d2, st));
@@ -875,6 +894,16 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
                      ImageRefs{{img[0], img[1], img[2]}}, Pos3{shake_nc ? xs : nullptr, ys, zs},
                      st));
   if (shake_nc) ETRY(shake_a(st));
+  return RBX_OK;
+}
+
+// Rest of a step, captured on st into g: rebuild decision and the rebuild
+// under an IF node, forces, second half kick (+ RATTLE, thermostat).
+int rbx_engine::capture_step_tail(cudaGraph_t g) {
+  cudaGraphConditionalHandle cond;
+  ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault),
+               "cudaGraphConditionalHandleCreate"));
+  const double thr = prm.skin * 0.5;
   ETRY(launch_step_decide(max_d2, thr * thr, dflags + 4, cond, st));
   // the conditional node after everything captured so far on st
   cudaStreamCaptureStatus cs;
@@ -907,7 +936,45 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
   ETRY(kspace_and_combine(true, dflags + 4));
   if (shake_nc) ETRY(shake_b(st));
   if (nh_on) ETRY(nh_final(st));
-  graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
+  return RBX_OK;
+}
+
+// The two graphs of a host-buffer step (see hgraph).
+int rbx_engine::capture_host_graphs() {
+  release_host_graphs();
+  const unsigned long long l0 = rbx_launch_count();
+  for (int k = 0; k < 2; ++k) {
+    ETRY(cuda_ok(cudaGraphCreate(&hgraph[k], 0), "cudaGraphCreate"));
+    ETRY(cuda_ok(cudaStreamBeginCaptureToGraph(st, hgraph[k], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal),
+                 "cudaStreamBeginCaptureToGraph"));
+    int rc;
+    if (k == 0) {
+      rc = capture_step_head();
+      if (!rc) {  // positions, cell order -> host order, into stage[0, 3n)
+        ArraySet out{};
+        const double* src[] = {x, y, z};
+        for (int a = 0; a < 3; ++a) {
+          out.src_f64[a] = src[a];
+          out.dst_f64[a] = stage + (size_t)a * n;
+        }
+        out.nf64 = 3;
+        rc = launch_scatter_set(n, orig, out, st);
+      }
+    } else {
+      rc = capture_step_tail(hgraph[k]);
+    }
+    cudaGraph_t gk = hgraph[k];
+    const cudaError_t e = cudaStreamEndCapture(st, &gk);
+    if (rc) {
+      release_host_graphs();
+      return rc;
+    }
+    ETRY(cuda_ok(e, "cudaStreamEndCapture"));
+    ETRY(cuda_ok(cudaGraphInstantiate(&hexec[k], hgraph[k], 0), "cudaGraphInstantiate"));
+  }
+  host_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
+  host_graph_dirty = false;
   return RBX_OK;
 }
 
@@ -928,7 +995,7 @@ int rbx_engine::graph_run_begin(cudaStream_t s) {
 // After the graph steps (flags copied to run_flags and the stream synchronised):
 // account for the steps, or restore the saved state and replay them launch by
 // launch when a rebuild inside the graph overflowed.
-int rbx_engine::graph_run_end(int nsteps) {
+int rbx_engine::graph_run_end(int nsteps, unsigned long long step_launches) {
   const int* h = run_flags;
   if (h[0] || (h[1] & 1)) {
     ETRY(launch_move_set(n, nullptr, state_set(false), st));
@@ -939,7 +1006,7 @@ int rbx_engine::graph_run_end(int nsteps) {
     have_cache = false;
     return step_plain(nsteps);
   }
-  count_launch((int)(graph_step_launches * nsteps + graph_rebuild_launches * h[5]));
+  count_launch((int)(step_launches * nsteps + graph_rebuild_launches * h[5]));
   epoch += nsteps;
   steps += nsteps;
   force_calls += nsteps;
@@ -960,7 +1027,7 @@ int rbx_engine::step_graph(int nsteps) {
   ETRY(cuda_ok(cudaMemcpyAsync(run_flags, dflags, sizeof(int) * 6, cudaMemcpyDeviceToHost, st),
                "D2H"));
   ETRY(cuda_ok(cudaStreamSynchronize(st), "step graph sync"));
-  return graph_run_end(nsteps);
+  return graph_run_end(nsteps, graph_step_launches);
 }
 
 // Fold the recorded per-step phase events into the running totals.
@@ -1024,42 +1091,49 @@ int rbx_engine::step_host(const double* xin, const double* vin, double* xout, do
   }
   in.nf64 = 6;
   ETRY(launch_move_set(n, orig, in, st));  // host order -> cell order
-  // outputs: cell order -> host order, then three copies out, all queued on st
-  auto queue_out = [&]() -> int {
+  // outputs from array `first` on (x y z vx vy vz fx fy fz): cell order ->
+  // host order into stage, then the copies out, all queued on st
+  double* const outs[3] = {xout, vout, fout};
+  auto queue_out = [&](int first) -> int {
     ArraySet out{};
     const double* src[] = {x, y, z, vx, vy, vz, fx, fy, fz};
-    for (int a = 0; a < 9; ++a) {
-      out.src_f64[a] = src[a];
-      out.dst_f64[a] = stage + a * N;
+    for (int a = first; a < 9; ++a) {
+      out.src_f64[a - first] = src[a];
+      out.dst_f64[a - first] = stage + a * N;
     }
-    out.nf64 = 9;
+    out.nf64 = 9 - first;
     ETRY(launch_scatter_set(n, orig, out, st));
-    ETRY(cuda_ok(cudaMemcpyAsync(xout, stage, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st),
-                 "D2H"));
-    ETRY(cuda_ok(cudaMemcpyAsync(vout, stage + 3 * N, sizeof(double) * 3 * N,
-                                 cudaMemcpyDeviceToHost, st),
-                 "D2H"));
-    return cuda_ok(cudaMemcpyAsync(fout, stage + 6 * N, sizeof(double) * 3 * N,
+    for (int b = first / 3; b < 3; ++b)
+      ETRY(cuda_ok(cudaMemcpyAsync(outs[b], stage + 3 * b * N, sizeof(double) * 3 * N,
                                    cudaMemcpyDeviceToHost, st),
-                   "D2H");
+                   "D2H"));
+    return RBX_OK;
   };
   if (!have_forces) ETRY(compute_forces(epoch));
   if (use_graph && !profiling && have_cache && prm.skin > 0.0) {
-    // the graph step and the copies out behind it, one host synchronisation
-    if (graph_dirty || !graph_exec) ETRY(capture_step_graph());
+    // two graph launches; the positions go out on st_side while the second
+    // computes the forces; one host synchronisation
+    if (host_graph_dirty || !hexec[0] || !hexec[1]) ETRY(capture_host_graphs());
     ETRY(graph_run_begin(st));
-    ETRY(cuda_ok(cudaGraphLaunch(graph_exec, st), "cudaGraphLaunch"));
+    ETRY(cuda_ok(cudaGraphLaunch(hexec[0], st), "cudaGraphLaunch"));
+    ETRY(cuda_ok(cudaEventRecord(ev_side, st), "cudaEventRecord"));
+    ETRY(cuda_ok(cudaStreamWaitEvent(st_side, ev_side, 0), "cudaStreamWaitEvent"));
+    ETRY(cuda_ok(cudaMemcpyAsync(xout, stage, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost,
+                                 st_side),
+                 "D2H"));
+    ETRY(cuda_ok(cudaGraphLaunch(hexec[1], st), "cudaGraphLaunch"));
     ETRY(cuda_ok(cudaMemcpyAsync(run_flags, dflags, sizeof(int) * 6, cudaMemcpyDeviceToHost, st),
                  "D2H"));
-    ETRY(queue_out());
+    ETRY(queue_out(3));
+    ETRY(cuda_ok(cudaStreamSynchronize(st_side), "step_host sync"));
     ETRY(cuda_ok(cudaStreamSynchronize(st), "step_host sync"));
     const bool replay = run_flags[0] || (run_flags[1] & 1);
-    ETRY(graph_run_end(1));  // on overflow: state restored, the step replayed
+    ETRY(graph_run_end(1, host_step_launches));  // on overflow: state restored, step replayed
     if (!replay) return RBX_OK;
   } else {
     ETRY(step(1));
   }
-  ETRY(queue_out());
+  ETRY(queue_out(0));
   return cuda_ok(cudaStreamSynchronize(st), "step_host sync");
 }
 
@@ -1149,7 +1223,7 @@ int rbx_engine::get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs
 
 int rbx_engine::set_k_samples(int p, const double* hmx, const double* hmy, const double* hmz) {
   cudaSetDevice(device);
-  graph_dirty = true;
+  graph_dirty = host_graph_dirty = true;
   ++graph_version;
   if (!hmx) {
     k_injected = false;
@@ -1339,7 +1413,7 @@ int rbx_engine::set_charges(const double* hq) {
   ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
   ETRY(cuda_ok(cudaStreamSynchronize(st), "set_charges sync"));
   have_forces = false;
-  graph_dirty = true;  // the energy terms carry the charge sums
+  graph_dirty = host_graph_dirty = true;  // the energy terms carry the charge sums
   ++graph_version;
   return RBX_OK;
 }
@@ -1358,7 +1432,7 @@ int rbx_engine::set_alpha(double a) {
     ETRY(build_sampler_tables());
   }
   have_forces = false;
-  graph_dirty = true;
+  graph_dirty = host_graph_dirty = true;
   ++graph_version;
   return RBX_OK;
 }
@@ -1369,7 +1443,7 @@ int rbx_engine::set_alpha(double a) {
 int rbx_engine::set_nose_hoover(double t_start, double t_stop, double t_damp, long long num_steps,
                                 double kb, double mvv2e, double tdof) {
   cudaSetDevice(device);
-  graph_dirty = true;
+  graph_dirty = host_graph_dirty = true;
   if (!(t_damp > 0)) {
     nh_on = false;
     return RBX_OK;
@@ -1431,7 +1505,7 @@ int rbx_engine::get_thermostat(double* temperature, double* eta, double* eta_dot
 // sqrt(2 bond^2 (1 - cos angle)) as the reference's ShakeA hard-codes it.
 int rbx_engine::set_shake(int nclusters, const int* clusters, double bond, double angle_deg) {
   cudaSetDevice(device);
-  graph_dirty = true;
+  graph_dirty = host_graph_dirty = true;
   if (nclusters <= 0 || !(bond > 0)) {
     shake_nc = 0;
     return RBX_OK;
@@ -1480,7 +1554,7 @@ int rbx_engine::set_shake(int nclusters, const int* clusters, double bond, doubl
 int rbx_engine::set_special(int maxspecial, const int* nspecial, const int* special, double w12,
                             double w13, double w14) {
   cudaSetDevice(device);
-  graph_dirty = true;
+  graph_dirty = host_graph_dirty = true;
   spec_natoms = 0;
   if (maxspecial <= 0) return RBX_OK;
   if (prm.neighbor_type != RBX_NEIGHBOR_RBL) {

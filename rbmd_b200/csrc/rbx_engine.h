@@ -145,6 +145,15 @@ struct rbx_engine {
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t st_body = nullptr;  // captures the rebuild body
   unsigned long long graph_step_launches = 0, graph_rebuild_launches = 0;
+  // the same step as two graphs for rbx_engine_step_host: [0] up to the drift
+  // (+ SHAKE) and the positions in host order, [1] the rest; the copy of the
+  // positions to the host runs on st_side while [1] computes the forces
+  bool host_graph_dirty = true;
+  cudaGraph_t hgraph[2] = {nullptr, nullptr};
+  cudaGraphExec_t hexec[2] = {nullptr, nullptr};
+  cudaStream_t st_side = nullptr;
+  cudaEvent_t ev_side = nullptr;
+  unsigned long long host_step_launches = 0;
   int* run_init = nullptr;   // pinned: device epoch / counter seeds of a graph run
   int* run_flags = nullptr;  // pinned: dflags[0..5] after a graph run
 
@@ -178,8 +187,12 @@ struct rbx_engine {
   rbx::ArraySet state_set(bool save) const;
   int capture_step_graph();
   int capture_step_into(cudaGraph_t g);
+  int capture_step_head();               // kick, drift (+ SHAKE) on st
+  int capture_step_tail(cudaGraph_t g);  // decide, rebuild (IF node), forces, ... on st
+  int capture_host_graphs();
+  void release_host_graphs();
   int graph_run_begin(cudaStream_t s);
-  int graph_run_end(int nsteps);
+  int graph_run_end(int nsteps, unsigned long long step_launches);
   int step_graph(int nsteps);
   int step_plain(int nsteps);
   void release_graph();

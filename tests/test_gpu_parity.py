@@ -913,6 +913,36 @@ def test_shake_water_graph_and_mixed(cuda, rbx, water3k):
     assert err < 1e-4 and rv < 1e-9, (err, rv)
 
 
+def test_step_host_water_shake_nvt(cuda, rbx, water3k):
+    """Host-buffer steps (positions copied out while the forces are computed)
+    with SHAKE and the thermostat equal device-resident steps bit for bit,
+    over enough steps for rebuilds."""
+    s = water3k
+    n = s["n"]
+    e1 = rbx.Engine(s, precision=rbx.MIXED, seed=77)
+    e2 = rbx.Engine(s, precision=rbx.MIXED, seed=77)
+    for e in (e1, e2):
+        _water_nvt(e, s)
+    st0 = e1.get_state()
+    x = np.ascontiguousarray(st0["pos"].T)
+    v = np.ascontiguousarray(st0["vel"].T)
+    xo, vo, fo = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
+    for _ in range(25):
+        e1.step_host(x, v, xo, vo, fo)
+        x, v = xo.copy(), vo.copy()
+        e2.step(1)
+    b = e2.get_state()
+    assert np.array_equal(b["pos"], xo.T)
+    assert np.array_equal(b["vel"], vo.T)
+    assert np.array_equal(b["force"], fo.T)
+    s1, s2 = e1.stats(), e2.stats()
+    assert s1.steps == s2.steps == 25 and s1.rebuilds == s2.rebuilds >= 1
+    assert e1.thermostat()["temperature"] == e2.thermostat()["temperature"]
+    assert e1.shake_status() == e2.shake_status()
+    e1.close()
+    e2.close()
+
+
 def _oracle_special_pair_force(oracle, s, nspecial, special, weights, epoch):
     """The oracle's CVFF RBL pair force (mean removed) in host order."""
     p = s["params"]
