@@ -406,7 +406,8 @@ int rbx_engine_compute_forces(rbx_engine* e, int epoch);
 int rbx_engine_step(rbx_engine* e, int nsteps);
 /* One step end to end from host buffers laid out [3][n] (x row, y row, z row),
  * in the atom order given to rbx_engine_set_state: copies x, v in (pinned or
- * pageable), steps once and copies x, v, f out. */
+ * pageable), steps once and copies x, v, f out; the copy of x out overlaps the
+ * force computation.  Returns when the outputs are on the host. */
 int rbx_engine_step_host(rbx_engine* e, const double* x_in, const double* v_in,
                          double* x_out, double* v_out, double* f_out);
 /* Copy the state to host arrays, in the atom order of the arrays given to
