@@ -296,6 +296,7 @@ int rbx_engine::set_state(const int* hgid, const int* htype, const double* hq, c
   ETRY(cuda_ok(cudaMemcpyAsync(gid, hgid, sizeof(int) * N, cudaMemcpyHostToDevice, st), "H2D"));
   ETRY(cuda_ok(cudaMemcpyAsync(orig, horig.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st),
                "H2D"));
+  if (where) ETRY(launch_inverse_perm(n, orig, where, st));
   ETRY(cuda_ok(cudaMemsetAsync(fx, 0, sizeof(double) * N, st), "memset"));
   ETRY(cuda_ok(cudaMemsetAsync(fy, 0, sizeof(double) * N, st), "memset"));
   ETRY(cuda_ok(cudaMemsetAsync(fz, 0, sizeof(double) * N, st), "memset"));
@@ -382,6 +383,7 @@ int rbx_engine::rebuild_launches(cudaStream_t s, bool in_graph) {
                          dflags, s));
   ETRY(launch_move_set(n, perm, permute_set(true), s));
   ETRY(launch_move_set(n, nullptr, permute_set(false), s));
+  if (where) ETRY(launch_inverse_perm(n, orig, where, s));  // SHAKE / special rows
   ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, s));
   ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
                         cand_count, cand, dflags + 1, list_scratch, s));
@@ -456,7 +458,6 @@ int rbx_engine::real_space(const int* epoch_dev) {
     ETRY(launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, epoch_dev,
                           cand_count, cand, cap, fpx, fpy, fpz, fpart, nrbl, dflags + 3, st));
     if (!spec_natoms) return RBX_OK;
-    ETRY(launch_inverse_perm(n, orig, where, st));
     return launch_special_rbl(pp, spec_natoms, spec_atoms, spec_cnt, spec_part, spec_max,
                               spec_w[0], spec_w[1], spec_w[2], where, x, y, z, q, type, key_a,
                               key_b, epoch, epoch_dev, fpx, fpy, fpz, fpart + (size_t)nrbl * 3, st);
@@ -999,6 +1000,7 @@ int rbx_engine::graph_run_end(int nsteps, unsigned long long step_launches) {
   const int* h = run_flags;
   if (h[0] || (h[1] & 1)) {
     ETRY(launch_move_set(n, nullptr, state_set(false), st));
+    if (where) ETRY(launch_inverse_perm(n, orig, where, st));
     if (nh_on)
       ETRY(cuda_ok(cudaMemcpyAsync(nh_state, nh_snap, sizeof(double) * NH_SLOTS,
                                    cudaMemcpyDeviceToDevice, st),
@@ -1444,6 +1446,7 @@ int rbx_engine::set_nose_hoover(double t_start, double t_stop, double t_damp, lo
                                 double kb, double mvv2e, double tdof) {
   cudaSetDevice(device);
   graph_dirty = host_graph_dirty = true;
+  ++graph_version;  // batch graphs holding this engine are captured again
   if (!(t_damp > 0)) {
     nh_on = false;
     return RBX_OK;
@@ -1506,6 +1509,7 @@ int rbx_engine::get_thermostat(double* temperature, double* eta, double* eta_dot
 int rbx_engine::set_shake(int nclusters, const int* clusters, double bond, double angle_deg) {
   cudaSetDevice(device);
   graph_dirty = host_graph_dirty = true;
+  ++graph_version;  // batch graphs holding this engine are captured again
   if (nclusters <= 0 || !(bond > 0)) {
     shake_nc = 0;
     return RBX_OK;
@@ -1531,6 +1535,7 @@ int rbx_engine::set_shake(int nclusters, const int* clusters, double bond, doubl
     ETRY(alloc(&xs, (size_t)n));
     ETRY(alloc(&ys, (size_t)n));
     ETRY(alloc(&zs, (size_t)n));
+    ETRY(launch_inverse_perm(n, orig, where, st));
   }
   ETRY(cuda_ok(cudaMemcpyAsync(shake_cl, clusters, sizeof(int) * 3 * nclusters,
                                cudaMemcpyHostToDevice, st),
@@ -1555,6 +1560,7 @@ int rbx_engine::set_special(int maxspecial, const int* nspecial, const int* spec
                             double w13, double w14) {
   cudaSetDevice(device);
   graph_dirty = host_graph_dirty = true;
+  ++graph_version;  // batch graphs holding this engine are captured again
   spec_natoms = 0;
   if (maxspecial <= 0) return RBX_OK;
   if (prm.neighbor_type != RBX_NEIGHBOR_RBL) {
@@ -1584,7 +1590,10 @@ int rbx_engine::set_special(int maxspecial, const int* nspecial, const int* spec
     ETRY(alloc(&spec_cnt, (size_t)3 * n));
     ETRY(alloc(&spec_atoms, (size_t)n));
   }
-  if (!where) ETRY(alloc(&where, (size_t)n));
+  if (!where) {
+    ETRY(alloc(&where, (size_t)n));
+    ETRY(launch_inverse_perm(n, orig, where, st));
+  }
   ETRY(cuda_ok(cudaMemcpy(spec_cnt, nspecial, sizeof(int) * 3 * n, cudaMemcpyHostToDevice), "H2D"));
   ETRY(cuda_ok(cudaMemcpy(spec_part, special, sizeof(int) * (size_t)n * maxspecial,
                           cudaMemcpyHostToDevice),
@@ -1601,14 +1610,12 @@ int rbx_engine::set_special(int maxspecial, const int* nspecial, const int* spec
 }
 
 int rbx_engine::shake_a(cudaStream_t s) {
-  ETRY(launch_inverse_perm(n, orig, where, s));
   return launch_shake_a(dbox, shp, shake_nc, shake_cl, where, type, mass_d, Pos3{xs, ys, zs},
                         Pos3{x, y, z}, Pos3{vx, vy, vz}, ImageRefs{{img[0], img[1], img[2]}}, x0,
                         y0, z0, max_d2, atoms, q, dflags + 6, s);
 }
 
 int rbx_engine::shake_b(cudaStream_t s) {
-  ETRY(launch_inverse_perm(n, orig, where, s));
   return launch_shake_b(dbox, shake_nc, shake_cl, where, type, mass_d, Pos3{x, y, z},
                         Pos3{vx, vy, vz}, dflags + 6, s);
 }

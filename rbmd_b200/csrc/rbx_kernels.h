@@ -294,7 +294,7 @@ int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* 
                  uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st);
 // CVFF special-bond correction of the RBL pair force (rbx_special.cu): its
 // SPEC_PARTS per-block force sums follow the fused kernel's in fpart.
-constexpr int SPEC_PARTS = 148;
+constexpr int SPEC_PARTS = 1184;  // 8 blocks per SM of 148: about one atom per thread
 int launch_special_rbl(const PairParams& pp, int natoms, const int* atoms_h, const int* cnt,
                        const int* part, int maxs, double w12, double w13, double w14,
                        const int* where, const double* x, const double* y, const double* z,

@@ -519,6 +519,33 @@ def test_batch_matches_single_engines(cuda, rbx):
         e.close()
 
 
+def test_batch_follows_thermostat_set_after_capture(cuda, rbx):
+    """A batch graph captured before a replica was given a thermostat is
+    captured again: the replica then steps NVT, bit-identical to the same
+    engine stepped alone."""
+    s = systems.lj_electrolyte(4000, seed=41)
+    a = rbx.Engine(s, precision=rbx.MIXED, seed=3)
+    b = rbx.Engine(s, precision=rbx.MIXED, seed=3)
+    for e in (a, b):
+        e.compute_forces(0)
+    batch = rbx.Batch([a])
+    batch.step(5)
+    b.step(5)
+    for e in (a, b):
+        e.set_nose_hoover(1.0, 1.6, 0.05, num_steps=30)
+    batch.step(12)
+    b.step(12)
+    sa, sb = a.get_state(), b.get_state()
+    for key in ("pos", "vel", "force"):
+        assert np.array_equal(sa[key], sb[key]), key
+    ta, tb = a.thermostat(), b.thermostat()
+    assert ta["temperature"] == tb["temperature"]
+    assert np.array_equal(ta["eta"], tb["eta"]) and np.any(ta["eta"] != 0)
+    batch.close()
+    a.close()
+    b.close()
+
+
 def test_engine_step_host_roundtrip(cuda, rbx, sys4k):
     s = sys4k
     e1 = rbx.Engine(s, precision=rbx.MIXED, seed=1)
