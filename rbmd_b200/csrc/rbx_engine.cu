@@ -1117,16 +1117,23 @@ int rbx_engine::step_host(const double* xin, const double* vin, double* xout, do
     // computes the forces; one host synchronisation
     if (host_graph_dirty || !hexec[0] || !hexec[1]) ETRY(capture_host_graphs());
     ETRY(graph_run_begin(st));
-    ETRY(cuda_ok(cudaGraphLaunch(hexec[0], st), "cudaGraphLaunch"));
-    ETRY(cuda_ok(cudaEventRecord(ev_side, st), "cudaEventRecord"));
-    ETRY(cuda_ok(cudaStreamWaitEvent(st_side, ev_side, 0), "cudaStreamWaitEvent"));
-    ETRY(cuda_ok(cudaMemcpyAsync(xout, stage, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost,
-                                 st_side),
-                 "D2H"));
-    ETRY(cuda_ok(cudaGraphLaunch(hexec[1], st), "cudaGraphLaunch"));
-    ETRY(cuda_ok(cudaMemcpyAsync(run_flags, dflags, sizeof(int) * 6, cudaMemcpyDeviceToHost, st),
-                 "D2H"));
-    ETRY(queue_out(3));
+    int rc = cuda_ok(cudaGraphLaunch(hexec[0], st), "cudaGraphLaunch");
+    if (!rc) rc = cuda_ok(cudaEventRecord(ev_side, st), "cudaEventRecord");
+    if (!rc) rc = cuda_ok(cudaStreamWaitEvent(st_side, ev_side, 0), "cudaStreamWaitEvent");
+    if (!rc)
+      rc = cuda_ok(cudaMemcpyAsync(xout, stage, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost,
+                                   st_side),
+                   "D2H");
+    if (!rc) rc = cuda_ok(cudaGraphLaunch(hexec[1], st), "cudaGraphLaunch");
+    if (!rc)
+      rc = cuda_ok(cudaMemcpyAsync(run_flags, dflags, sizeof(int) * 6, cudaMemcpyDeviceToHost, st),
+                   "D2H");
+    if (!rc) rc = queue_out(3);
+    if (rc) {  // no copy into the caller's buffers may be left in flight
+      cudaStreamSynchronize(st_side);
+      cudaStreamSynchronize(st);
+      return rc;
+    }
     ETRY(cuda_ok(cudaStreamSynchronize(st_side), "step_host sync"));
     ETRY(cuda_ok(cudaStreamSynchronize(st), "step_host sync"));
     const bool replay = run_flags[0] || (run_flags[1] & 1);
@@ -1135,7 +1142,11 @@ int rbx_engine::step_host(const double* xin, const double* vin, double* xout, do
   } else {
     ETRY(step(1));
   }
-  ETRY(queue_out(0));
+  const int rc = queue_out(0);
+  if (rc) {
+    cudaStreamSynchronize(st);
+    return rc;
+  }
   return cuda_ok(cudaStreamSynchronize(st), "step_host sync");
 }
 
