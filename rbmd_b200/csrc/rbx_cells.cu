@@ -44,18 +44,58 @@ __device__ __forceinline__ unsigned morton2(unsigned a, unsigned b, unsigned c) 
 
 constexpr int SUB_SHIFT = 26;  // key = sub-cell code << 26 | old index (n < 2^26)
 
-__global__ void k_cell_assign(DBox b, int dx, int dy, int dz, int n, const double* __restrict__ x,
-                              const double* __restrict__ y, const double* __restrict__ z,
-                              int* __restrict__ cell, unsigned* __restrict__ sub,
-                              int* __restrict__ counts) {
+// Cell edge and its reciprocal per dimension, formed on the host as LinkedCell
+// does (edge = box length / cells, reciprocal = 1 / edge).
+struct CellGeom {
+  double edge[3], inv[3];
+};
+
+// AssignAtomsToCell (linked_cell_op.hip.cu:57-138, no halo): floor((p - lo) *
+// 1/edge) clamped, then, for a point outside that cell's bounds
+// [lo + c edge, lo + (c + 1) edge) (products and sums rounded separately), a
+// move of one cell per dimension that is kept only if the point lies inside
+// the corrected cell.
+__device__ __forceinline__ void assign_cell(const DBox& b, const CellGeom& g, const int dims[3],
+                                            const double p[3], int c[3]) {
+  bool inside = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    c[d] = cell_coord(p[d], b.lo[d], g.inv[d], dims[d]);
+    const double cmin = __dadd_rn(__dmul_rn((double)c[d], g.edge[d]), b.lo[d]);
+    const double cmax = __dadd_rn(__dmul_rn((double)(c[d] + 1), g.edge[d]), b.lo[d]);
+    inside = inside && cmin <= p[d] && p[d] < cmax;
+  }
+  if (inside) return;
+  int cc[3];
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double cmin = __dadd_rn(__dmul_rn((double)c[d], g.edge[d]), b.lo[d]);
+    const double cmax = __dadd_rn(__dmul_rn((double)(c[d] + 1), g.edge[d]), b.lo[d]);
+    cc[d] = c[d] + (p[d] < cmin ? -1 : (p[d] >= cmax ? 1 : 0));
+    cc[d] = cc[d] < 0 ? 0 : (cc[d] > dims[d] - 1 ? dims[d] - 1 : cc[d]);
+    const double nmin = __dadd_rn(__dmul_rn((double)cc[d], g.edge[d]), b.lo[d]);
+    const double nmax = __dadd_rn(__dmul_rn((double)(cc[d] + 1), g.edge[d]), b.lo[d]);
+    ok = ok && nmin <= p[d] && p[d] < nmax;
+  }
+  if (ok)
+    for (int d = 0; d < 3; ++d) c[d] = cc[d];
+}
+
+__global__ void k_cell_assign(DBox b, CellGeom g, int dx, int dy, int dz, int n,
+                              const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, int* __restrict__ cell,
+                              unsigned* __restrict__ sub, int* __restrict__ counts) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double fx = (x[i] - b.lo[0]) * (dx / b.len[0]);
   const double fy = (y[i] - b.lo[1]) * (dy / b.len[1]);
   const double fz = (z[i] - b.lo[2]) * (dz / b.len[2]);
-  const int cx = cell_coord(x[i], b.lo[0], dx / b.len[0], dx);
-  const int cy = cell_coord(y[i], b.lo[1], dy / b.len[1], dy);
-  const int cz = cell_coord(z[i], b.lo[2], dz / b.len[2], dz);
+  const int dims[3] = {dx, dy, dz};
+  const double p[3] = {x[i], y[i], z[i]};
+  int cc[3];
+  assign_cell(b, g, dims, p, cc);
+  const int cx = cc[0], cy = cc[1], cz = cc[2];
   const int c = (cz * dy + cy) * dx + cx;
   cell[i] = c;
   auto sub4 = [](double f, int c0) {
@@ -525,8 +565,13 @@ int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, 
   k_fill_i32<<<grid_for(ncell, 256, sm_count() * 4), 256, 0, st>>>(ncell, counts, 0);
   count_launch();
   if (n > 0) {
-    k_cell_assign<<<(n + 255) / 256, 256, 0, st>>>(b, dims[0], dims[1], dims[2], n, x, y, z, cell,
-                                                   sub, counts);
+    CellGeom g;
+    for (int d = 0; d < 3; ++d) {
+      g.edge[d] = b.len[d] / dims[d];
+      g.inv[d] = 1.0 / g.edge[d];
+    }
+    k_cell_assign<<<(n + 255) / 256, 256, 0, st>>>(b, g, dims[0], dims[1], dims[2], n, x, y, z,
+                                                   cell, sub, counts);
     count_launch();
   }
   k_cell_scan<<<1, 1024, 0, st>>>(ncell, counts, cell_start, fill);

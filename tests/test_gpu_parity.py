@@ -161,6 +161,102 @@ def test_cells_and_full_list(cuda, rbx, oracle, n):
         assert set(gn[i, :gc[i]].tolist()) == set(orows[i, :ocnt[i]].tolist())
 
 
+def test_ops_without_atoms(cuda, rbx):
+    """Zero atoms: structure factors are zero, the force, cell sort and list
+    ops succeed and write nothing."""
+    box = rbx.Box.make([0.0, 0.0, 0.0], [20.0, 21.0, 22.0])
+    e = cuda.zeros(0, dtype=cuda.float64, device="cuda")
+    m = [cuda.tensor([1.0, -2.0, 0.0], dtype=cuda.float64, device="cuda") for _ in range(3)]
+    re = cuda.full((3,), 7.0, dtype=cuda.float64, device="cuda")
+    im = cuda.full((3,), 7.0, dtype=cuda.float64, device="cuda")
+    rbx.rbe_structure_factor(box, e, *m, e, e, e, re, im)
+    rbx.rbe_force(box, 0.16, 1.0, 1.0, re, im, e, *m, e, e, e, e, e, e)
+    dims = rbx.cell_grid(box, 5.3)
+    ncell = int(np.prod(dims))
+    ei = cuda.zeros(0, dtype=cuda.int32, device="cuda")
+    cst = cuda.full((ncell + 1,), -1, dtype=cuda.int32, device="cuda")
+    scratch = cuda.zeros(max(rbx.cells_scratch_bytes(0, ncell), 1), dtype=cuda.uint8,
+                         device="cuda")
+    rbx.cells_sort(box, 5.3, e, e, e, ei, ei, cst, scratch)
+    ovf = cuda.zeros(1, dtype=cuda.int32, device="cuda")
+    rbx.full_list(box, 5.3, e, e, e, cst, 64, ei, ei, ovf)
+    cuda.cuda.synchronize()
+    assert np.all(re.cpu().numpy() == 0.0) and np.all(im.cpu().numpy() == 0.0)
+    assert np.all(cst.cpu().numpy() == 0) and ovf.item() == 0
+
+
+def test_cells_sort_reports_overfull_cell(cuda, rbx):
+    """More atoms in one cell than the in-cell sort holds (2048): the op
+    returns the capacity error and still leaves a valid permutation."""
+    n = 2100
+    rng = np.random.default_rng(3)
+    pos = rng.uniform(1.0, 4.0, size=(n, 3))  # all inside cell (0, 0, 0)
+    box = rbx.Box.make([0.0, 0.0, 0.0], [18.0, 18.0, 18.0])
+    X = [_t(cuda, pos[:, d]) for d in range(3)]
+    dims = rbx.cell_grid(box, 5.3)
+    ncell = int(np.prod(dims))
+    perm = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    cos = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    cst = cuda.zeros(ncell + 1, dtype=cuda.int32, device="cuda")
+    scratch = cuda.zeros(rbx.cells_scratch_bytes(n, ncell), dtype=cuda.uint8, device="cuda")
+    with pytest.raises(rbx.RbxError, match="2048"):
+        rbx.cells_sort(box, 5.3, *X, perm, cos, cst, scratch)
+    cuda.cuda.synchronize()
+    assert sorted(perm.cpu().numpy().tolist()) == list(range(n))
+    hs = cst.cpu().numpy()
+    assert hs[0] == 0 and hs[1] == n and hs[-1] == n
+
+
+def test_full_list_atoms_on_faces(cuda, rbx, oracle):
+    """Atoms exactly on the box's lower faces, one ulp below its upper faces
+    and on interior cell faces: cell sort and candidate list equal the
+    oracle's as sets."""
+    s = systems.lj_electrolyte(4000, seed=17)
+    lo, hi = np.asarray(s["lo"], float), np.asarray(s["hi"], float)
+    rc = 5.3
+    dims = np.asarray(rbx.cell_grid(rbx.Box.make(lo, hi), rc))
+    edge = (hi - lo) / dims
+    pos = s["pos"].copy()
+    rng = np.random.default_rng(5)
+    idx = rng.choice(s["n"], size=300, replace=False)
+    for k, a in enumerate(idx):
+        d = k % 3
+        if k % 3 == 0:
+            pos[a, d] = lo[d]
+        elif k % 3 == 1:
+            pos[a, d] = np.nextafter(hi[d], -np.inf)
+        else:
+            pos[a, d] = lo[d] + edge[d] * (1 + k % (dims[d] - 1))
+    s2 = dict(s, pos=pos)
+    x, y, z = (np.ascontiguousarray(pos[:, d]) for d in range(3))
+    rbox = rbx.Box.make(lo, hi)
+    n = s["n"]
+    ncell = int(np.prod(dims))
+    X = [_t(cuda, a) for a in (x, y, z)]
+    perm = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    cos = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    cst = cuda.zeros(ncell + 1, dtype=cuda.int32, device="cuda")
+    scratch = cuda.zeros(rbx.cells_scratch_bytes(n, ncell), dtype=cuda.uint8, device="cuda")
+    rbx.cells_sort(rbox, rc, *X, perm, cos, cst, scratch)
+    hp = perm.cpu().numpy()
+    xs = [_t(cuda, a[hp]) for a in (x, y, z)]
+    cap = 800
+    cnt = cuda.zeros(n, dtype=cuda.int32, device="cuda")
+    nb = cuda.full((n, cap), -1, dtype=cuda.int32, device="cuda")
+    ovf = cuda.zeros(1, dtype=cuda.int32, device="cuda")
+    rbx.full_list(rbox, rc, *xs, cst, cap, cnt, nb, ovf)
+    cuda.cuda.synchronize()
+    box, operm, ocell, ocs, oce, oxs, oys, ozs = _sorted(oracle, s2, rc)
+    assert np.array_equal(np.sort(hp), np.arange(n))
+    assert np.array_equal(cos.cpu().numpy(), ocell)  # same cell for every sorted slot
+    ocnt, orows = oracle.full_list(box, rc, oxs, oys, ozs, ocell, ocs, oce)
+    gcnt, grows = cnt.cpu().numpy(), nb.cpu().numpy()
+    # compare by original atom index (the in-cell orders may differ)
+    want = {int(operm[i]): set(operm[orows[i, :ocnt[i]]].tolist()) for i in range(n)}
+    got = {int(hp[i]): set(hp[grows[i, :gcnt[i]]].tolist()) for i in range(n)}
+    assert got == want
+
+
 def test_nlist_should_reuse_matches_oracle(cuda, rbx, oracle, sys4k):
     """Skin test of a cached list (ShouldReuseNeighborList): the largest
     minimum-image displacement, and reuse iff it is at most skin / 2."""
