@@ -453,6 +453,59 @@ def test_engine_rbl_pairs_bit_exact(cuda, rbx, oracle, sys4k, prec):
         e.close()
 
 
+def _orthorhombic(n, seed, scale=(1.15, 0.92, 1.0)):
+    """An LJ electrolyte whose box and positions are stretched per axis."""
+    s = systems.lj_electrolyte(n, seed=seed)
+    lo = np.asarray(s["lo"], float)
+    sc = np.asarray(scale, float)
+    hi = lo + (np.asarray(s["hi"], float) - lo) * sc
+    pos = lo + (s["pos"] - lo) * sc
+    return dict(s, lo=lo, hi=hi, pos=pos)
+
+
+def test_engine_orthorhombic_box(cuda, rbx, oracle):
+    """A box with three different edge lengths (the mixed form's fixed-point
+    screen is for cubic boxes; here every candidate takes the FP64
+    predicate): forces in both forms against the oracle, RBL pairs as exact
+    sets, and velocity-Verlet steps against the oracle's engine."""
+    import __graft_entry__ as ge
+
+    s = _orthorhombic(8000, seed=61)
+    box = oracle.Box.make(s["lo"], s["hi"])
+    m = oracle.rbe_sample_philox(box, 0.16, 100, 7, 0)
+    want = ge._oracle_forces(s, m)
+    for prec, tol in ((rbx.PLAIN_FP64, 1e-9), (rbx.MIXED, 1e-5)):
+        e = rbx.Engine(s, precision=prec)
+        e.set_k_samples(*m)
+        e.compute_forces(epoch=0)
+        assert systems.rel_rms(e.get_state()["force"], want) < tol, prec
+        freq = e.stats().selection_frequency
+        p = s["params"]
+        _, perm, cell, cs, ce, xs, ys, zs = _sorted(oracle, s, p["cut_off"] + p["skin"])
+        cnt, rows = oracle.full_list(box, p["cut_off"] + p["skin"], xs, ys, zs, cell, cs, ce)
+        gid = s["gid"][perm]
+        cc, core, sc, shell = oracle.rbl_filter(box, p["r_core"], p["cut_off"], freq, 0, gid, xs,
+                                                ys, zs, cnt, rows)
+        gc, gs = e.rbl_pairs()
+        want_c = {(int(gid[i]), int(gid[j])) for i in range(s["n"]) for j in core[i, :cc[i]]}
+        want_s = {(int(gid[i]), int(gid[j])) for i in range(s["n"]) for j in shell[i, :sc[i]]}
+        got_c, got_s = set(map(tuple, gc.tolist())), set(map(tuple, gs.tolist()))
+        assert got_c == want_c and got_s == want_s, prec
+        e.close()
+    e = rbx.Engine(s, precision=rbx.PLAIN_FP64, seed=4242)
+    ref = oracle.Engine(s, seed=4242)
+    ref.compute_forces(0)
+    e.compute_forces(0)
+    for k in range(3):
+        e.step(1)
+        ref.step(1)
+        a, b = e.get_state(), ref.get()
+        order = np.argsort(b["gid"])
+        assert systems.rel_rms(a["force"], b["force"][order]) < 1e-8, k
+        assert np.abs(a["pos"] - b["pos"][order]).max() < 1e-10, k
+    e.close()
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_engine_rbl_pairs_between_rebuilds(cuda, rbx, oracle, prec):
     """The engine keeps its candidate rows between skin rebuilds.  After
