@@ -251,12 +251,15 @@ int rbx_engine::init() {
   pp.lj_eps = lj_eps;
   pp.lj_s6 = lj_s6;
   for (int d = 0; d < 3; ++d) pp.sf[d] = (float)(dbox.len[d] / 4294967296.0);
-  // fixed-point screens (cubic boxes): the guard band covers the fixed-point
-  // quantisation (< 3 units of L/2^32 per coordinate) with a wide margin
+  // fixed-point screens: the guard band covers the fixed-point quantisation
+  // (< 3 units of L_d/2^32 per coordinate, at most 3 units of L_max/2^32 once
+  // weighted by L_d/L_max) with a wide margin
   pp.cubic = dbox.len[0] == dbox.len[1] && dbox.len[1] == dbox.len[2];
-  if (pp.cubic) {
-    const double L = dbox.len[0];
-    // FP32 |d|^2 carries < 1e-6 relative rounding plus < 6 s |d| of quantisation
+  {
+    const double L = std::max(dbox.len[0], std::max(dbox.len[1], dbox.len[2]));
+    for (int d = 0; d < 3; ++d) pp.sw[d] = (float)(dbox.len[d] / L);
+    // FP32 |d|^2 carries < 1e-6 relative rounding (the weights add two
+    // roundings per coordinate, < 2e-7 more) plus < 6 s |d| of quantisation
     // error; the band is several times both
     const double qerr = 64.0 * (L / 4294967296.0) * (rcs + 1.0);
     auto band = [&](double C) { return 1e-4 + 8e-6 * C + qerr; };

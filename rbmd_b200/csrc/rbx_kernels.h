@@ -72,12 +72,12 @@ int rbe_axis_table(double L, double alpha, double* w, int max_entries, double* t
 
 // ---- real space (rbx_pair.cu) ----
 // Screen of "r^2 < C" on the fixed-point |d|^2 (FP32, units of s^2 with
-// s = L/2^32): decided below lo and at or above hi, undecided in between (the
-// FP64 predicate decides).
+// s = L/2^32, L the longest box edge): decided below lo and at or above hi,
+// undecided in between (the FP64 predicate decides).
 struct IntScreen {
   float lo, hi;
 };
-// Build the screen for threshold C (r^2 units) on a cubic box of edge L.
+// Build the screen for threshold C (r^2 units) with L the longest box edge.
 IntScreen make_screen(double C, double L, double band);
 
 struct PairParams {
@@ -91,8 +91,11 @@ struct PairParams {
   int ntypes;
   const double* lj_eps;       // ntypes^2 eps_ij
   const double* lj_s6;        // ntypes^2 sigma_ij^6
-  // fixed-point screen (cubic box): |u_j - u_i|^2 against integer thresholds
+  // fixed-point screen: |u_j - u_i|^2 in units of (L_max / 2^32)^2 against
+  // FP32 thresholds; on a box with unequal edges each difference is first
+  // weighted by L_d / L_max (cubic: no weights)
   int cubic;
+  float sw[3];                // L_d / L_max in FP32
   float sf[3];                // L_d / 2^32 in FP32 (mixed pair vector)
   IntScreen sc_eps, sc_core, sc_rs, sc_force, sc_rc;
 };

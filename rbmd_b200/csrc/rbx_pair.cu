@@ -95,14 +95,16 @@ __device__ __forceinline__ void write_block_partial(double (*s_acc)[3], double* 
 // ---------------------------------------------------------------------------
 // Candidate classification shared by both forms.
 //
-// On a cubic box the pair vector in fixed point, d = u_j - u_i (wrapped int32),
-// is the exact minimum image of the FP64 pair vector to within 3 units of
-// s = L/2^32 per coordinate.  |d|^2 is formed in FP32 (in units of s^2) and
-// each predicate "r^2 < C" is decided when |d|^2 lies outside a guard band
-// [lo, hi] around C/s^2 that exceeds every rounding and quantisation error;
-// inside the band the reference's FP64 expression (CaculateDistance: i minus
-// j, min image, no FMA) decides.  The outcome is therefore identical to the
-// FP64 predicate on every pair, in both precision forms.
+// The pair vector in fixed point, d = u_j - u_i (wrapped int32), is the exact
+// minimum image of the FP64 pair vector to within 3 units of s_d = L_d/2^32
+// per coordinate.  |d|^2 is formed in FP32 in units of s^2, s = L_max/2^32
+// (on a box with unequal edges each coordinate is first weighted by
+// L_d/L_max, which keeps its error below 3 units of s), and each predicate
+// "r^2 < C" is decided when |d|^2 lies outside a guard band [lo, hi] around
+// C/s^2 that exceeds every rounding and quantisation error; inside the band
+// the reference's FP64 expression (CaculateDistance: i minus j, min image, no
+// FMA) decides.  The outcome is therefore identical to the FP64 predicate on
+// every pair, in both precision forms.
 // ---------------------------------------------------------------------------
 // Screened classification; *unsure is set when a threshold band is hit.  The
 // band around core2_list and the one around rs2 (which lies just above it)
@@ -126,6 +128,14 @@ __device__ __forceinline__ Classified classify_screen(const PairParams& pp, floa
 __device__ __forceinline__ float fixed_d2(const uint4& ai, const uint4& aj) {
   const float dx = (float)(int)(aj.x - ai.x), dy = (float)(int)(aj.y - ai.y),
               dz = (float)(int)(aj.z - ai.z);
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+// The same in units of the longest edge's fixed-point step on a box with
+// unequal edges (each difference weighted by L_d / L_max).
+__device__ __forceinline__ float fixed_d2_weighted(const PairParams& pp, const uint4& ai,
+                                                   const uint4& aj) {
+  const float dx = (float)(int)(aj.x - ai.x) * pp.sw[0], dy = (float)(int)(aj.y - ai.y) * pp.sw[1],
+              dz = (float)(int)(aj.z - ai.z) * pp.sw[2];
   return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 
@@ -214,7 +224,7 @@ __device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
 // force-carrying pairs are appended to a per-warp queue and consumed 32 at a
 // time from its tail.
 // ---------------------------------------------------------------------------
-template <bool MIXED, int SEL, bool PREFETCH>
+template <bool MIXED, int SEL, bool PREFETCH, bool CUBIC>
 __global__ void __launch_bounds__(PAIR_BLOCK, MIXED ? 4 : 3)  // no spills in either form
 k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
             const double* __restrict__ y, const double* __restrict__ z,
@@ -350,9 +360,9 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
 #pragma unroll
       for (int u = 0; u < RBL_UNROLL; ++u) {
         const bool valid = jj[u] != i;
-        bool unsure = !pp.cubic;
-        Classified c{false, false};
-        if (pp.cubic) c = classify_screen(pp, fixed_d2(ai, aa[u]), &unsure);
+        bool unsure;
+        const Classified c = classify_screen(
+            pp, CUBIC ? fixed_d2(ai, aa[u]) : fixed_d2_weighted(pp, ai, aa[u]), &unsure);
         // shell batch hash (RblShellSampleSelected)
         bool sel;
         if (SEL == 2) {
@@ -461,11 +471,9 @@ k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
         if (k < cnt) {
           j = __ldg(row + k);
           if (j != i) {
-            int in = -1;
-            if (pp.cubic) {
-              const float d2s = fixed_d2(ai, __ldg(atoms + j));
-              in = d2s < pp.sc_rc.lo ? 1 : (d2s >= pp.sc_rc.hi ? 0 : -1);
-            }
+            const uint4 aj = __ldg(atoms + j);
+            const float d2s = pp.cubic ? fixed_d2(ai, aj) : fixed_d2_weighted(pp, ai, aj);
+            int in = d2s < pp.sc_rc.lo ? 1 : (d2s >= pp.sc_rc.hi ? 0 : -1);
             if (in < 0) {
               const double ex = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
               const double ey = min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
@@ -827,23 +835,30 @@ struct RblChoice {
 
 // The instantiation a launch uses.  FP64 form: candidate rows prefetched into
 // shared memory when both buffers fit.  The mixed form runs faster at the
-// occupancy it keeps without them.
-RblChoice rbl_choose(bool mixed, int freq, int cap, bool with_status) {
+// occupancy it keeps without them.  Cubic boxes take the unweighted distance
+// screen.
+RblChoice rbl_choose(bool mixed, int freq, int cap, bool with_status, bool cubic) {
   const bool pow2 = freq >= 1 && (freq & (freq - 1)) == 0;
   const int sel = pow2 ? (freq <= 4 ? 2 : 1) : 0;
   const int dyn = rbl_prefetch_smem(cap);
   const bool prefetch = !mixed && with_status && dyn <= kRblMaxDynSmem;
-  static RblKernel const table[2][3][2] = {
-      {{k_rbl_fused<false, 0, false>, k_rbl_fused<false, 0, true>},
-       {k_rbl_fused<false, 1, false>, k_rbl_fused<false, 1, true>},
-       {k_rbl_fused<false, 2, false>, k_rbl_fused<false, 2, true>}},
-      {{k_rbl_fused<true, 0, false>, nullptr},
-       {k_rbl_fused<true, 1, false>, nullptr},
-       {k_rbl_fused<true, 2, false>, nullptr}}};
-  RblChoice c{table[mixed][sel][prefetch], prefetch ? dyn : 0};
+  static RblKernel const table[2][3][2][2] = {
+      {{{k_rbl_fused<false, 0, false, false>, k_rbl_fused<false, 0, false, true>},
+        {k_rbl_fused<false, 0, true, false>, k_rbl_fused<false, 0, true, true>}},
+       {{k_rbl_fused<false, 1, false, false>, k_rbl_fused<false, 1, false, true>},
+        {k_rbl_fused<false, 1, true, false>, k_rbl_fused<false, 1, true, true>}},
+       {{k_rbl_fused<false, 2, false, false>, k_rbl_fused<false, 2, false, true>},
+        {k_rbl_fused<false, 2, true, false>, k_rbl_fused<false, 2, true, true>}}},
+      {{{k_rbl_fused<true, 0, false, false>, k_rbl_fused<true, 0, false, true>},
+        {nullptr, nullptr}},
+       {{k_rbl_fused<true, 1, false, false>, k_rbl_fused<true, 1, false, true>},
+        {nullptr, nullptr}},
+       {{k_rbl_fused<true, 2, false, false>, k_rbl_fused<true, 2, false, true>},
+        {nullptr, nullptr}}}};
+  RblChoice c{table[mixed][sel][prefetch][cubic], prefetch ? dyn : 0};
   if (prefetch) {  // opt in to large dynamic shared memory, once per instantiation
-    static std::atomic<int> done[3] = {};
-    if (!done[sel].exchange(1)) {
+    static std::atomic<int> done[3][2] = {};
+    if (!done[sel][cubic].exchange(1)) {
       cudaFuncSetAttribute(c.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kRblMaxDynSmem);
       cudaFuncSetAttribute(c.kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     }
@@ -857,7 +872,7 @@ int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int wav
   // scheduler evens out the per-atom work (200k atoms, mixed form: 1 wave
   // 0.59 ms, 3 waves 0.555 ms, 6-12 waves 0.54 ms, 48 waves 0.57 ms)
   const int kRblWaves = waves > 0 ? waves : 8;
-  const RblChoice c = rbl_choose(mixed, freq, cap, true);
+  const RblChoice c = rbl_choose(mixed, freq, cap, true, true);  // occupancy of the cubic form
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, c.kern, PAIR_BLOCK, c.smem) !=
           cudaSuccess || occ < 1) {
@@ -878,7 +893,7 @@ int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms
                      const int* cand_count, const int* cand, int cap, double* fx, double* fy,
                      double* fz, double* fpart, int nblocks, int* status, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  const RblChoice c = rbl_choose(mixed, pp.freq, cap, status != nullptr);
+  const RblChoice c = rbl_choose(mixed, pp.freq, cap, status != nullptr, pp.cubic != 0);
   c.kern<<<nblocks, PAIR_BLOCK, c.smem, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
                                               epoch_dev, cand_count, cand, cap, fx, fy, fz, fpart,
                                               status);

@@ -463,14 +463,15 @@ def _orthorhombic(n, seed, scale=(1.15, 0.92, 1.0)):
     return dict(s, lo=lo, hi=hi, pos=pos)
 
 
-def test_engine_orthorhombic_box(cuda, rbx, oracle):
-    """A box with three different edge lengths (the mixed form's fixed-point
-    screen is for cubic boxes; here every candidate takes the FP64
-    predicate): forces in both forms against the oracle, RBL pairs as exact
-    sets, and velocity-Verlet steps against the oracle's engine."""
+@pytest.mark.parametrize("scale", [(1.15, 0.92, 1.0), (1.6, 0.8, 1.05)])
+def test_engine_orthorhombic_box(cuda, rbx, oracle, scale):
+    """A box with three different edge lengths (the fixed-point distance
+    screen weights each axis by L_d / L_max): forces in both forms against
+    the oracle, RBL pairs as exact sets in both forms, and velocity-Verlet
+    steps against the oracle's engine."""
     import __graft_entry__ as ge
 
-    s = _orthorhombic(8000, seed=61)
+    s = _orthorhombic(8000, seed=61, scale=scale)
     box = oracle.Box.make(s["lo"], s["hi"])
     m = oracle.rbe_sample_philox(box, 0.16, 100, 7, 0)
     want = ge._oracle_forces(s, m)
