@@ -432,6 +432,7 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
 // {evdwl, ecoul, vxx, vyy, vzz, vxy, vxz, vyz} (ComputeVirial, lj_op.hip.cu:76-88).
 // The cutoff test uses the integer screen with the FP64 fallback.
 // ---------------------------------------------------------------------------
+template <bool CUBIC>
 __global__ void __launch_bounds__(PAIR_BLOCK)
 k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
                    const double* __restrict__ x, const double* __restrict__ y,
@@ -472,7 +473,7 @@ k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
           j = __ldg(row + k);
           if (j != i) {
             const uint4 aj = __ldg(atoms + j);
-            const float d2s = pp.cubic ? fixed_d2(ai, aj) : fixed_d2_weighted(pp, ai, aj);
+            const float d2s = CUBIC ? fixed_d2(ai, aj) : fixed_d2_weighted(pp, ai, aj);
             int in = d2s < pp.sc_rc.lo ? 1 : (d2s >= pp.sc_rc.hi ? 0 : -1);
             if (in < 0) {
               const double ex = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
@@ -907,8 +908,14 @@ int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, con
                             double* fy, double* fz, double* fpart, double* epart, int nblocks,
                             cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  k_verlet_fused_f64<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, cand_count,
-                                                     cand, cap, fx, fy, fz, fpart, epart);
+  if (pp.cubic)
+    k_verlet_fused_f64<true><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type,
+                                                             cand_count, cand, cap, fx, fy, fz,
+                                                             fpart, epart);
+  else
+    k_verlet_fused_f64<false><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type,
+                                                              cand_count, cand, cap, fx, fy, fz,
+                                                              fpart, epart);
   count_launch();
   return check_launch("verlet_fused_f64");
 }

@@ -507,6 +507,46 @@ def test_engine_orthorhombic_box(cuda, rbx, oracle, scale):
     e.close()
 
 
+@pytest.mark.parametrize("scale", [(1.0, 1.0, 1.0), (1.15, 0.92, 1.0)])
+def test_engine_verlet_list(cuda, rbx, oracle, scale):
+    """The engine with a plain Verlet list (LJ + erfc-Coulomb to cut_off over
+    the candidate rows, no random batch): its pair force against the oracle's
+    ComputeLJCutCoulForce restatement on a cubic and an orthorhombic box, and
+    its graph step against launch-by-launch steps bit for bit."""
+    s = _orthorhombic(8000, seed=71, scale=scale)
+    p = s["params"]
+    box = oracle.Box.make(s["lo"], s["hi"])
+    rcs = p["cut_off"] + p["skin"]
+    _, perm, cell, cs, ce, xs, ys, zs = _sorted(oracle, s, rcs)
+    cnt, rows = oracle.full_list(box, rcs, xs, ys, zs, cell, cs, ce)
+    f, _, _, _ = oracle.pair_force_verlet(box, p["cut_off"], p["alpha"], p["qqr2e"],
+                                          s["type"][perm], s["sigma"], s["eps"], s["q"][perm], xs,
+                                          ys, zs, cnt, rows)
+    want = np.empty_like(f)
+    want[perm] = f
+    m = oracle.rbe_sample_philox(box, p["alpha"], 100, 7, 0)
+    for prec in (rbx.PLAIN_FP64, rbx.MIXED):
+        e = rbx.Engine(s, precision=prec, neighbor="VERLET")
+        e.set_k_samples(*m)
+        e.compute_forces(epoch=0)
+        fp, _ = e.force_parts()
+        assert systems.rel_rms(fp, want) < 1e-10, prec  # real space is FP64 in both forms
+        e.close()
+    runs = []
+    for graph in (True, False):
+        e = rbx.Engine(s, precision=rbx.MIXED, neighbor="VERLET", seed=13)
+        e.set_step_graph(graph)
+        e.compute_forces(0)
+        e.step(8)
+        e.step(12)
+        runs.append((e.get_state(), e.stats()))
+        e.close()
+    (a, sa), (b, sb) = runs
+    for key in ("pos", "vel", "force"):
+        assert np.array_equal(a[key], b[key]), key
+    assert sa.rebuilds == sb.rebuilds
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_engine_rbl_pairs_between_rebuilds(cuda, rbx, oracle, prec):
     """The engine keeps its candidate rows between skin rebuilds.  After
