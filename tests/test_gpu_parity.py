@@ -432,6 +432,30 @@ def test_engine_forces_fp64_and_mixed(cuda, rbx, oracle, n):
         e.close()
 
 
+def test_engine_kspace_energy_and_virial(cuda, rbx, oracle, sys20k):
+    """The RBE energy and virial the engine reports with each force
+    evaluation (KSpaceCalculator's energy and ComputeRBEForceVirial) against
+    the oracle on the same configuration and k-samples."""
+    s = sys20k
+    p = s["params"]
+    box = oracle.Box.make(s["lo"], s["hi"])
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    m = oracle.rbe_sample_philox(box, p["alpha"], 100, 5, 0)
+    S = oracle.rbe_gauss_sum(box, p["alpha"])
+    re, im = oracle.rbe_structure_factor(box, s["q"], x, y, z, *m)
+    ek, vir = oracle.rbe_energy_virial(box, p["alpha"], S, p["qqr2e"], float((s["q"] ** 2).sum()),
+                                       float(s["q"].sum()), re, im, *m)
+    for prec, tol in ((rbx.PLAIN_FP64, 1e-10), (rbx.MIXED, 1e-6)):
+        e = rbx.Engine(s, precision=prec)
+        e.set_k_samples(*m)
+        e.compute_forces(epoch=0)
+        st = e.stats()
+        assert abs(st.e_kspace - ek) < tol * abs(ek), prec
+        assert np.allclose(np.asarray(st.virial_kspace[:]), vir, rtol=tol,
+                           atol=tol * np.abs(vir).max()), prec
+        e.close()
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_engine_rbl_pairs_bit_exact(cuda, rbx, oracle, sys4k, prec):
     s = sys4k
