@@ -501,6 +501,16 @@ int rbx_engine_write_trajectory(rbx_engine* e, const char* path, int64_t timeste
 /* Last real-space (after mean removal for RBL) and k-space forces, [n][3] each,
  * in the atom order given to rbx_engine_set_state. */
 int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace);
+/* LJ and Coulomb (erfc) pair energies and the pair virial (xx, yy, zz, xy,
+ * xz, yz) of the current positions over every pair within cut_off, each pair
+ * counted from both sides: LJCutCoulKspace::ComputeLJCoulEnergy with
+ * LJCutCoulEnergyOp (src/force/src/lj_cut_coul_kspace.cpp:821-865,
+ * lj_cut_coul_kspace_op.hip.cu:475-568), which RBMD runs after the RBL force
+ * when neighbor.energy_rbl_flag is "yes" and inside the force op for a Verlet
+ * list.  FP64 in both precision forms.  Totals: RBMD divides them by the atom
+ * count in LJ units.  Any pointer may be NULL.  RBL and Verlet-list engines
+ * (VERLET-SOG reports its energies through rbx_pair_force_verlet_sog). */
+int rbx_engine_pair_energy(rbx_engine* e, double* e_vdwl, double* e_coul, double* virial);
 /* Last RBL lists as (gid_i, gid_j) pairs; sizes in/out. */
 int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core,
                              int* shell_pairs, int64_t* n_shell);

@@ -167,6 +167,7 @@ void LJCutCoulKspace::Init() {
                                ? _cfg.Get<std::string>("unit", "init_configuration", "read_data")
                                : std::string("LJ");
   const double qqr2e = QqrdFromUnit(unit);
+  _lj_units = unit == "LJ";
   const double cut_off = _cfg.Get<double>("cut_off", "hyper_parameters", "neighbor");
   _neighbor_type = _cfg.Get<std::string>("type", "hyper_parameters", "neighbor");
   rbx_params p{};
@@ -234,11 +235,25 @@ void LJCutCoulKspace::Execute() {
   EvaluatePotentialEnergy();
 }
 
-// EvaluatePotentialEnergy: energies per atom in LJ units
-// (lj_cut_coul_kspace.cpp:627-632, kspace_calculator.cpp:374-385).
+// EvaluatePotentialEnergy (lj_cut_coul_kspace.cpp:867-878): k-space energy
+// (KSpaceCalculator::EvaluatePotentialEnergy, kspace_calculator.cpp:375-385),
+// pair energies where RBMD computes them (ComputeLJVerlet every step,
+// ComputeLJCoulEnergy after the RBL force when energy_rbl_flag is "yes",
+// :570-572, :821-865), each divided by the atom count in LJ units.
 void LJCutCoulKspace::EvaluatePotentialEnergy() {
+  const double per = _lj_units ? 1.0 / (double)_n : 1.0;
   rbx_stats s;
-  if (rbx_engine_get_stats(_engine, &s) == RBX_OK) _e_kspace = s.e_kspace;
+  if (rbx_engine_get_stats(_engine, &s) != RBX_OK) throw std::runtime_error(rbx_last_error());
+  _e_kspace = s.e_kspace * per;
+  const bool verlet = _neighbor_type == "Verlet-List" || _neighbor_type == "VERLET";
+  if (verlet || (_neighbor_type == "RBL" && _energy_rbl_flag == "yes")) {
+    double ev = 0.0, ec = 0.0;
+    if (rbx_engine_pair_energy(_engine, &ev, &ec, nullptr) != RBX_OK)
+      throw std::runtime_error(rbx_last_error());
+    _e_vdwl = ev * per;
+    _e_coul = ec * per;
+  }
+  _e_pe = _e_vdwl + _e_coul + _e_kspace;
 }
 
 }  // namespace rbx_host

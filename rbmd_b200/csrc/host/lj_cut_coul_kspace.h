@@ -66,7 +66,12 @@ class LJCutCoulKspace : public Force {
     return e;
   }
   int epoch = 0;
+  // energies of the last evaluation, per atom in LJ units (totals otherwise);
+  // the pair energies only for a Verlet list or RBL with energy_rbl_flag "yes"
   double e_kspace() const { return _e_kspace; }
+  double e_vdwl() const { return _e_vdwl; }
+  double e_coul() const { return _e_coul; }
+  double e_pe() const { return _e_pe; }
 
  private:
   ConfigData _cfg;
@@ -76,7 +81,8 @@ class LJCutCoulKspace : public Force {
   std::string _neighbor_type, _energy_rbl_flag = "yes";
   KSpaceCalculator _kspace;
   rbx_engine* _engine = nullptr;
-  double _e_kspace = 0.0;
+  bool _lj_units = true;
+  double _e_kspace = 0.0, _e_vdwl = 0.0, _e_coul = 0.0, _e_pe = 0.0;
 };
 
 }  // namespace rbx_host

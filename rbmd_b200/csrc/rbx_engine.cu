@@ -1176,6 +1176,35 @@ int rbx_engine::get_force_parts(double* f_pair, double* f_kspace) {
   return RBX_OK;
 }
 
+// LJ and erfc-Coulomb energies and the virial over every pair within cut_off
+// of the current positions: the Verlet kernel over the candidate rows (their
+// forces go to scratch), per-block partials summed here in block order.
+int rbx_engine::pair_energy(double* e_vdwl, double* e_coul, double* virial) {
+  cudaSetDevice(device);
+  if (prm.neighbor_type == RBX_NEIGHBOR_VERLET_SOG) {
+    set_error("pair energy: the VERLET-SOG energies come from rbx_pair_force_verlet_sog");
+    return RBX_ERR_INVALID;
+  }
+  ETRY(check_rebuild(false));  // rows that hold every pair within cut_off
+  ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
+  const size_t N = (size_t)n;
+  ETRY(launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, stage,
+                               stage + N, stage + 2 * N, nullptr, epart, nfpart, st));
+  std::vector<double> h((size_t)nfpart * 8);
+  ETRY(cuda_ok(cudaMemcpyAsync(h.data(), epart, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                               st),
+               "D2H"));
+  ETRY(cuda_ok(cudaStreamSynchronize(st), "pair energy sync"));
+  double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < nfpart; ++b)
+    for (int k = 0; k < 8; ++k) t[k] += h[(size_t)b * 8 + k];
+  if (e_vdwl) *e_vdwl = t[0];
+  if (e_coul) *e_coul = t[1];
+  if (virial)
+    for (int k = 0; k < 6; ++k) virial[k] = t[2 + k];
+  return RBX_OK;
+}
+
 int rbx_engine::get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs,
                               int64_t* n_shell) {
   cudaSetDevice(device);
@@ -1831,6 +1860,11 @@ int rbx_engine_get_state(rbx_engine* e, double* px, double* py, double* pz, doub
 int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace) {
   if (!e) return RBX_ERR_INVALID;
   return e->get_force_parts(f_pair, f_kspace);
+}
+
+int rbx_engine_pair_energy(rbx_engine* e, double* e_vdwl, double* e_coul, double* virial) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->pair_energy(e_vdwl, e_coul, virial);
 }
 
 int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core, int* shell_pairs,

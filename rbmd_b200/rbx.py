@@ -94,6 +94,7 @@ EXPORTS = [
     "rbx_engine_destroy", "rbx_engine_set_state", "rbx_engine_set_k_samples",
     "rbx_engine_compute_forces", "rbx_engine_step", "rbx_engine_step_host",
     "rbx_engine_get_state", "rbx_engine_get_force_parts", "rbx_engine_get_rbl_pairs",
+    "rbx_engine_pair_energy",
     "rbx_engine_get_stats", "rbx_engine_stream", "rbx_engine_phase_ms",
     "rbx_engine_set_profiling", "rbx_rbe_structure_factor_noalloc", "rbx_engine_set_step_graph",
     "rbx_nlist_should_reuse", "rbx_batch_create", "rbx_batch_destroy", "rbx_batch_step",
@@ -176,6 +177,7 @@ def lib():
     L.rbx_engine_step_host.argtypes = [vp] * 6
     L.rbx_engine_get_state.argtypes = [vp] * 10
     L.rbx_engine_get_force_parts.argtypes = [vp, vp, vp]
+    L.rbx_engine_pair_energy.argtypes = [vp, vp, vp, vp]
     L.rbx_engine_get_rbl_pairs.argtypes = [vp, vp, C.POINTER(C.c_int64), vp,
                                            C.POINTER(C.c_int64)]
     L.rbx_engine_get_stats.argtypes = [vp, C.POINTER(Stats)]
@@ -521,6 +523,14 @@ class Engine:
         fk = np.zeros((self.n, 3))
         check(lib().rbx_engine_get_force_parts(self._h, _np_ptr(fp), _np_ptr(fk)), "force_parts")
         return fp, fk
+
+    def pair_energy(self):
+        """(E_LJ, E_coul, virial[6]) over every pair within cut_off, totals."""
+        ev, ec = np.zeros(1), np.zeros(1)
+        vir = np.zeros(6)
+        check(lib().rbx_engine_pair_energy(self._h, _np_ptr(ev), _np_ptr(ec), _np_ptr(vir)),
+              "rbx_engine_pair_energy")
+        return ev[0], ec[0], vir
 
     def rbl_pairs(self):
         nc, ns = C.c_int64(0), C.c_int64(0)

@@ -456,6 +456,39 @@ def test_engine_kspace_energy_and_virial(cuda, rbx, oracle, sys20k):
         e.close()
 
 
+def test_engine_pair_energy(cuda, rbx, oracle):
+    """Pair energies and virial over every pair within cut_off
+    (rbx_engine_pair_energy, what RBMD computes with energy_rbl_flag "yes")
+    against the oracle's LJCutCoulForce energies, for RBL engines in both
+    forms and a Verlet-list engine, at the start and after steps that moved
+    the atoms without a rebuild in between."""
+    s = systems.lj_electrolyte(8000, seed=81)
+    p = s["params"]
+    rcs = p["cut_off"] + p["skin"]
+
+    def want(pos):
+        s2 = dict(s, pos=pos)
+        box, perm, cell, cs, ce, xs, ys, zs = _sorted(oracle, s2, rcs)
+        cnt, rows = oracle.full_list(box, rcs, xs, ys, zs, cell, cs, ce)
+        _, vir, el, ec = oracle.pair_force_verlet(box, p["cut_off"], p["alpha"], p["qqr2e"],
+                                                  s["type"][perm], s["sigma"], s["eps"],
+                                                  s["q"][perm], xs, ys, zs, cnt, rows)
+        return el, ec, np.asarray(vir)
+
+    for neighbor, prec in (("RBL", rbx.PLAIN_FP64), ("RBL", rbx.MIXED), ("VERLET", rbx.MIXED)):
+        e = rbx.Engine(s, precision=prec, neighbor=neighbor, seed=3)
+        e.compute_forces(0)
+        for k in range(2):
+            if k:
+                e.step(3)
+            el, ec, vir = want(e.get_state()["pos"])
+            gl, gc, gv = e.pair_energy()
+            assert abs(gl - el) < 1e-10 * abs(el), (neighbor, prec, k)
+            assert abs(gc - ec) < 1e-10 * abs(ec), (neighbor, prec, k)
+            assert np.allclose(gv, vir, rtol=1e-10, atol=1e-10 * np.abs(vir).max()), (neighbor, k)
+        e.close()
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_engine_rbl_pairs_bit_exact(cuda, rbx, oracle, sys4k, prec):
     s = sys4k
