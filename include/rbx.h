@@ -97,8 +97,11 @@ int rbx_rbe_structure_factor(const rbx_box* box, int num_atoms, int p_number,
  * the library: RBX_NOALLOC_RHO_BLOCKS x RBX_NOALLOC_RHO_MAX_P doubles for Re and
  * for Im (2 MiB), held on every GPU that loads the library until the process
  * exits.  p_number above RBX_NOALLOC_RHO_MAX_P is rejected with RBX_ERR_INVALID.
- * The first call on a device looks up the array's device address (once per
- * device); make that first call before any stream capture.  All calls share the
+ * Each call outside a stream capture looks up the array's device address on
+ * the current device (no allocation), so a device reset is picked up by the
+ * next such call; a call inside a capture reuses the address of the last call
+ * outside one, so make one call on the device before any stream capture (and
+ * again after a device reset).  All calls share the
  * one array: calls whose work can overlap on the GPU (other streams, other
  * host threads) race and must be serialised by the caller.  Results equal
  * rbx_rbe_structure_factor's up to FP64 summation order. */

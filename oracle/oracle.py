@@ -499,3 +499,68 @@ class Engine:
                 self._h = None
         except Exception:
             pass
+
+
+# --- one force evaluation of the RBL + RBE path --------------------------------
+def pair_keys(pairs):
+    """Sorted int64 keys gid_i * 2^32 + gid_j of an [m, 2] array of gid pairs."""
+    a = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+    return np.sort((a[:, 0] << 32) | (a[:, 1] & 0xFFFFFFFF))
+
+
+def _pair_keys(gid, count, rows):
+    n, cap = rows.shape
+    mask = np.arange(cap)[None, :] < count[:, None]
+    gi = np.broadcast_to(np.asarray(gid, dtype=np.int64)[:, None], rows.shape)[mask]
+    gj = np.asarray(gid, dtype=np.int64)[rows[mask]]
+    return np.sort((gi << 32) | (gj & 0xFFFFFFFF))
+
+
+def rbl_rbe_evaluation(sys, m, epoch=0, pair_energy=True):
+    """One LJCutCoulKspace::Execute of the RBL + RBE path on a system dict
+    (rbmd_b200.systems layout) with injected k-samples m = (mx, my, mz):
+    cell sort, candidate list at cut_off + skin, RBL filter with the batch
+    hash of `epoch`, RBL pair force with mean removal, RBE structure factor,
+    force, energy and virial (lj_cut_coul_kspace.cpp:464-573,
+    kspace_calculator.cpp:532-669).  Optionally the pair energies and virial
+    over every pair within cut_off (LJCutCoulEnergyOp).  Arrays are returned
+    in the order of the input atoms; the core and shell pairs as sorted keys
+    (pair_keys)."""
+    p = sys["params"]
+    box = Box.make(sys["lo"], sys["hi"])
+    n = int(sys["n"])
+    rcs = p["cut_off"] + p["skin"]
+    x, y, z = (np.ascontiguousarray(sys["pos"][:, d]) for d in range(3))
+    perm, cell, cs, ce = cells_sort(box, rcs, x, y, z)
+    xs, ys, zs = x[perm], y[perm], z[perm]
+    cnt, rows = full_list(box, rcs, xs, ys, zs, cell, cs, ce)
+    freq, _, _ = rbl_params(n, box, p["r_core"], p["cut_off"], p["neighbor_sample_num"])
+    gid = np.asarray(sys["gid"])[perm]
+    typ = np.asarray(sys["type"])[perm]
+    q = np.asarray(sys["q"])[perm]
+    cc, core, sc, shell = rbl_filter(box, p["r_core"], p["cut_off"], freq, epoch, gid, xs, ys, zs,
+                                     cnt, rows)
+    fp = pair_force_rbl(box, p["r_core"], p["cut_off"], freq, p["alpha"], p["qqr2e"], typ,
+                        sys["sigma"], sys["eps"], q, xs, ys, zs, cc, core, sc, shell)
+    fp, _ = fix_rbl(fp)
+    S = rbe_gauss_sum(box, p["alpha"])
+    re, im = rbe_structure_factor(box, q, xs, ys, zs, *m)
+    fk = rbe_force(box, S, p["qqr2e"], re, im, q, *m, xs, ys, zs)
+    ek, vk = rbe_energy_virial(box, p["alpha"], S, p["qqr2e"], float((q ** 2).sum()),
+                               float(q.sum()), re, im, *m)
+    # the sampled sum before the self term is subtracted: the scale of the
+    # k-space energy's rounding error (the two nearly cancel)
+    V = float(np.prod(np.asarray(sys["hi"], float) - np.asarray(sys["lo"], float)))
+    e_self = p["qqr2e"] * (np.sqrt(p["alpha"]) * float((q ** 2).sum()) / np.sqrt(np.pi)
+                           + 0.5 * np.pi * float(q.sum()) ** 2 / (p["alpha"] * V))
+    out = {"freq": freq, "f_pair": np.zeros((n, 3)), "f_kspace": np.zeros((n, 3)),
+           "e_kspace": ek, "e_kspace_scale": abs(ek + e_self), "virial_kspace": np.asarray(vk),
+           "core_keys": _pair_keys(gid, cc, core), "shell_keys": _pair_keys(gid, sc, shell)}
+    out["f_pair"][perm] = fp
+    out["f_kspace"][perm] = fk
+    out["force"] = out["f_pair"] + out["f_kspace"]
+    if pair_energy:
+        _, vir, el, ec = pair_force_verlet(box, p["cut_off"], p["alpha"], p["qqr2e"], typ,
+                                           sys["sigma"], sys["eps"], q, xs, ys, zs, cnt, rows)
+        out.update(e_vdwl=el, e_coul=ec, virial_pair=np.asarray(vir))
+    return out

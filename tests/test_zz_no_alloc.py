@@ -49,3 +49,26 @@ def test_noalloc_rejects_oversize(cuda, rbx, oracle):
     out = [torch.zeros(513, dtype=torch.float64, device="cuda") for _ in range(2)]
     with pytest.raises(rbx.RbxError, match="exceeds the built-in scratch limit"):
         rbx.rbe_structure_factor_noalloc(box, *t, *out)
+
+
+def test_noalloc_largest_size_then_no_atoms(cuda, rbx, oracle):
+    """p_number = 512, the largest size the built-in scratch holds, against the
+    allocating entry; then a call with no atoms after it, whose structure
+    factors must be exactly zero whatever the previous call left behind."""
+    torch = cuda
+    s, t = _inputs(torch, oracle, 20000, 512, 5)
+    box = rbx.Box.make(s["lo"], s["hi"])
+    ref = [torch.zeros(512, dtype=torch.float64, device="cuda") for _ in range(2)]
+    got = [torch.zeros(512, dtype=torch.float64, device="cuda") for _ in range(2)]
+    rbx.rbe_structure_factor(box, *t, *ref)
+    rbx.rbe_structure_factor_noalloc(box, *t, *got)
+    torch.cuda.synchronize()
+    scale = np.sqrt((ref[0].cpu().numpy() ** 2 + ref[1].cpu().numpy() ** 2).mean())
+    for a, b in zip(got, ref):
+        assert np.abs(a.cpu().numpy() - b.cpu().numpy()).max() < 1e-11 * scale * np.sqrt(20000)
+    empty = [a[:0] for a in t[4:]]
+    out = [torch.full((512,), 7.0, dtype=torch.float64, device="cuda") for _ in range(2)]
+    rbx.rbe_structure_factor_noalloc(box, t[0][:0], *t[1:4], *empty, *out)
+    torch.cuda.synchronize()
+    for a in out:
+        assert np.array_equal(a.cpu().numpy(), np.zeros(512))
