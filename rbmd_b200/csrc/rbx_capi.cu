@@ -581,20 +581,35 @@ constexpr int kNoallocMaxP = RBX_NOALLOC_RHO_MAX_P;     // largest p_number acce
 static __device__ __align__(256) double g_noalloc_rho_scratch[2 * kNoallocMaxP * kNoallocBlocks];
 
 std::mutex g_noalloc_mu;
-double* g_noalloc_addr[256] = {};  // device address of the array, per device ordinal
+double* g_noalloc_addr[256] = {};  // last looked-up device address, per device ordinal
 
-// Device address of the scratch array on the current device, looked up once per
-// device.  The array's name in host code is only a host-side handle; kernels
-// must be given this address.
-int noalloc_scratch(double** out) {
+// Device address of the scratch array on the current device.  The array's name
+// in host code is only a host-side handle; kernels must be given this address.
+// Outside a stream capture the address is looked up on every call (the lookup
+// allocates nothing), so a context torn down and created again, e.g. after
+// cudaDeviceReset, is picked up; inside a capture, where the lookup may not be
+// issued, the address of the last call outside a capture on this device is used.
+int noalloc_scratch(cudaStream_t st, double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
     cudaGetLastError();
     set_error("rbx_rbe_structure_factor_noalloc: no current CUDA device");
     return RBX_ERR_DEVICE;
   }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = cudaStreamCaptureStatusNone;
+  }
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  if (cap != cudaStreamCaptureStatusNone) {
+    if (!g_noalloc_addr[dev]) {
+      set_error("rbx_rbe_structure_factor_noalloc: the first call on device %d must come before "
+                "any stream capture",
+                dev);
+      return RBX_ERR_INVALID;
+    }
+  } else {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_rho_scratch);
     if (e != cudaSuccess || !p) {
@@ -631,9 +646,9 @@ extern "C" int rbx_rbe_structure_factor_noalloc(const rbx_box* box, int num_atom
   }
   if (p_number == 0) return RBX_OK;
   RBX_TRY(require_device());
-  double* scratch = nullptr;
-  RBX_TRY(noalloc_scratch(&scratch));
   cudaStream_t st = (cudaStream_t)stream;
+  double* scratch = nullptr;
+  RBX_TRY(noalloc_scratch(st, &scratch));
   const DBox b = make_dbox(*box);
   int nb = rbe_partial_blocks(num_atoms);
   if (nb > kNoallocBlocks) nb = kNoallocBlocks;
