@@ -66,8 +66,7 @@ k_adj_pair(PairParams pp, int n, const double* __restrict__ x, const double* __r
            const double* __restrict__ z, const double* __restrict__ q,
            const int* __restrict__ type, const double* __restrict__ sigma_t,
            const double* __restrict__ eps_t, const unsigned long long* __restrict__ key_a,
-           const unsigned long long* __restrict__ key_b, int epoch,
-           const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
+           const unsigned long long* __restrict__ key_b, int epoch, Rows rows,
            const double* __restrict__ gx, const double* __restrict__ gy,
            const double* __restrict__ gz, double mgx, double mgy, double mgz,
            double* __restrict__ d_rx, double* __restrict__ d_ry, double* __restrict__ d_rz,
@@ -88,9 +87,11 @@ k_adj_pair(PairParams pp, int n, const double* __restrict__ x, const double* __r
     const unsigned long long ea_m = key_a[m] ^ (unsigned long long)(long long)epoch;
     const unsigned long long kb_m = key_b[m];
     double rx = 0.0, ry = 0.0, rz = 0.0, dq = 0.0;
-    const int cnt = min(cand_count[m], cap);
-    for (int k = lane; k < cnt; k += 32) {
-      const int j = cand[(size_t)m * cap + k];
+    int nf, nb;
+    row_extent(rows, m, nf, nb);
+    const int* row = rows.idx + (size_t)m * rows.cap;
+    for (int k = lane; k < nf + nb; k += 32) {
+      const int j = row_at(row, rows.cap, nf, nb, k);
       if (j == m) continue;
       const Classified c = classify_exact(exact_d2(pp, x, y, z, m, j), pp);
       if (!c.core_active && !c.shell_window) continue;
@@ -268,8 +269,8 @@ int adj_pair_blocks(int n) {
 int launch_adj_pair(const PairParams& pp, int n, const double* x, const double* y,
                     const double* z, const double* q, const int* type, const double* sigma_t,
                     const double* eps_t, const unsigned long long* key_a,
-                    const unsigned long long* key_b, int epoch, const int* cand_count,
-                    const int* cand, int cap, const double* gx, const double* gy,
+                    const unsigned long long* key_b, int epoch, const Rows& rows,
+                    const double* gx, const double* gy,
                     const double* gz, const double mean_g[3], double* d_rx, double* d_ry,
                     double* d_rz, double* d_q, double* part, int nblocks, cudaStream_t st) {
   if (pp.ntypes > ADJ_MAX_TYPES) {
@@ -277,7 +278,7 @@ int launch_adj_pair(const PairParams& pp, int n, const double* x, const double* 
     return RBX_ERR_INVALID;
   }
   k_adj_pair<<<nblocks, ADJ_BLOCK, 0, st>>>(pp, n, x, y, z, q, type, sigma_t, eps_t, key_a, key_b,
-                                            epoch, cand_count, cand, cap, gx, gy, gz, mean_g[0],
+                                            epoch, rows, gx, gy, gz, mean_g[0],
                                             mean_g[1], mean_g[2], d_rx, d_ry, d_rz, d_q, part);
   count_launch();
   return check_launch("adj_pair");

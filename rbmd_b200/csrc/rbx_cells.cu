@@ -215,6 +215,14 @@ k_cell_segsort(int ncell, int n, const int* __restrict__ start, const unsigned* 
 // Pairs inside a guard band around the cutoff are settled with the
 // reference's FP64 predicate, so the list equals the FP64 reference list as a
 // set; rows come out in stencil order, then in cell order.
+//
+// Split rows (RBL engines): a pair whose build distance is certainly at least
+// r_near = r_core + skin cannot come within r_core before the next rebuild (no
+// atom moves more than skin/2 before one), so the fused RBL kernel tests it
+// with its batch hash first.  Such far pairs are written from the end of the
+// row backwards; every other candidate from the front.  count[i] is the
+// number of candidates (above cap: overflow), far[i] the number written to
+// the back; the front holds min(count, cap) - far[i] entries, all written.
 // ---------------------------------------------------------------------------
 constexpr int NL_BLOCK = 128;
 constexpr int NL_WARPS = NL_BLOCK / 32;
@@ -266,7 +274,8 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
             const double* __restrict__ z, const int* __restrict__ cell_start,
             const float4* __restrict__ box_lo, const float4* __restrict__ box_hi,
             const int* __restrict__ cell_of, int cap, int* __restrict__ count,
-            int* __restrict__ nbrs, int* __restrict__ overflow) {
+            int* __restrict__ nbrs, int* __restrict__ overflow, float near2,
+            int* __restrict__ far) {
   __shared__ float4 buf[NL_WARPS][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int w = blockIdx.x * NL_WARPS + warp;
@@ -288,6 +297,8 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
               az = live ? -2.f * uz : 0.f;
   const float lo_i = live ? lo_band - uu : -INFINITY;
   const float hi_i = live ? hi_band - uu : -INFINITY;
+  const bool split = far != nullptr;
+  const float near_i = near2 - uu;  // far pairs: d above this
   // box of the group's centre atoms relative to the cell centre, rounded outwards
   float glo[3], ghi[3];
   {
@@ -305,7 +316,7 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
         ghi[d] = fmaxf(ghi[d], __shfl_xor_sync(0xffffffffu, ghi[d], s));
       }
   }
-  int cnt = 0;
+  int cnt = 0, nback = 0;  // candidates found, entries written to the back
   int* row = nbrs + (size_t)i * cap;
   for (int s = 0; s < 27; ++s) {
     // stencil order of ComputeFullNeighborStencilCellOnTheFly:
@@ -378,7 +389,18 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
         while (acc) {  // hits in cell order, each lane into its own row
           const int t = __ffs(acc) - 1;
           acc &= acc - 1;
-          if (cnt < cap) row[cnt] = first + t;
+          bool to_back = false;
+          if (split) {  // build distance d + |u|^2 certainly at least r_near
+            const float4 q = buf[warp][t];
+            const float d = fmaf(ax, q.x, fmaf(ay, q.y, fmaf(az, q.z, q.w)));
+            to_back = d > near_i;
+          }
+          if (cnt < cap) {
+            if (to_back)
+              row[cap - 1 - nback++] = first + t;
+            else
+              row[cnt - nback] = first + t;
+          }
           ++cnt;
         }
       }
@@ -386,6 +408,7 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
   }
   if (live) {
     count[i] = cnt;
+    if (split) far[i] = nback;
     if (cnt > cap) atomicOr(overflow, 1);
   }
 }
@@ -593,7 +616,8 @@ size_t full_list_scratch_bytes(int n, int ncell) {
 
 int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
                      const double* y, const double* z, const int* cell_start, int cap,
-                     int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st) {
+                     int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st,
+                     const FarSplit* split) {
   const int ncell = dims[0] * dims[1] * dims[2];
   if (n <= 0) return RBX_OK;
   const double cut2 = cutoff * cutoff;
@@ -619,9 +643,11 @@ int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, con
   int* cell_of = (int*)(p + 2 * al(sizeof(float4) * t));
   k_chunk_boxes<<<ncell, 128, 0, st>>>(x, y, z, cell_start, box_lo, box_hi, cell_of);
   count_launch();
+  // far threshold in r^2, raised by the FP32 error of the test value
+  const float near2 = split ? (float)(split->r_near * split->r_near + band) : INFINITY;
   k_full_list<<<(t + NL_WARPS - 1) / NL_WARPS, NL_BLOCK, 0, st>>>(
       b, dims[0], dims[1], dims[2], cut2, cut2_up, lo_band, hi_band, t, x, y, z, cell_start,
-      box_lo, box_hi, cell_of, cap, count, nbrs, overflow);
+      box_lo, box_hi, cell_of, cap, count, nbrs, overflow, near2, split ? split->far : nullptr);
   count_launch();
   return check_launch("full_list");
 }

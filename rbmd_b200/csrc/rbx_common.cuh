@@ -63,35 +63,47 @@ __device__ __forceinline__ double dist2_list(const DBox& b, double xi, double yi
 }
 
 // MixRblSampleKey (rbl_full_neighbor_list_op.hip.cu:6-11).
-__device__ __forceinline__ unsigned long long rbl_mix(unsigned long long v) {
+__host__ __device__ __forceinline__ unsigned long long rbl_mix(unsigned long long v) {
   v += 0x9e3779b97f4a7c15ULL;
   v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ULL;
   v = (v ^ (v >> 27)) * 0x94d049bb133111ebULL;
   return v ^ (v >> 31);
 }
 
+// Low word of the 64-bit value (hi, lo) shifted right by s (0 < s < 32).
+__host__ __device__ __forceinline__ unsigned funnel_r(unsigned lo, unsigned hi, unsigned s) {
+#ifdef __CUDA_ARCH__
+  return __funnelshift_r(lo, hi, s);
+#else
+  return (unsigned)((((unsigned long long)hi << 32) | lo) >> s);
+#endif
+}
+
 // Batch test mix(key) % freq == 0 for freq in {1, 2, 4} (mask = freq - 1).
-// h = v ^ (v >> 31) for the last product v = w * C2, so h's two low bits need
-// only bits 0, 1, 31 and 32 of v, i.e. v mod 2^33: the 32x32->64 product of
-// the low halves of w and C2, with bit 32 flipped by the parity of
-// w_hi * C2_lo + w_lo * C2_hi (both halves of C2 are odd).
-__device__ __forceinline__ bool rbl_selected_low2(unsigned long long key, unsigned mask) {
+// With w = v ^ (v >> 27) after the second round and u = w * C2, the test reads
+// bits 0 and 1 of h = u ^ (u >> 31): h_0 = u_0 ^ u_31 and h_1 = u_1 ^ u_32.
+// u mod 2^33 needs only the 32x32->64 product p of the low halves of w and C2
+// and the parity of w_hi * C2_lo + w_lo * C2_hi, which is w_32 ^ w_0 because
+// both halves of C2 are odd: u_32 = p_32 ^ w_32 ^ w_0.  The funnel shift of p
+// by 31 lines p_31 and p_32 up with bits 0 and 1.
+__host__ __device__ __forceinline__ bool rbl_selected_low2(unsigned long long key,
+                                                           unsigned mask) {
   unsigned long long v = key + 0x9e3779b97f4a7c15ULL;
   v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ULL;
   const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
-  const unsigned w_lo = lo ^ __funnelshift_r(lo, hi, 27);  // low half of v ^ (v >> 27)
-  const unsigned w_32 = (hi ^ (hi >> 27)) & 1u;             // its bit 32
+  const unsigned w_lo = lo ^ funnel_r(lo, hi, 27);  // low half of w
+  const unsigned t = hi ^ (hi >> 27) ^ w_lo;        // bit 0: w_32 ^ w_0
   const unsigned long long p = (unsigned long long)w_lo * 0x133111ebu;
   const unsigned p_lo = (unsigned)p;
-  const unsigned v32 = ((unsigned)(p >> 32) ^ w_32 ^ w_lo) & 1u;
-  return ((p_lo ^ (p_lo >> 31) ^ (v32 << 1)) & mask) == 0u;
+  const unsigned f = funnel_r(p_lo, (unsigned)(p >> 32), 31);  // bit 0: p_31, bit 1: p_32
+  return ((p_lo ^ f ^ (t << 1)) & mask) == 0u;
 }
 
 // Per-atom halves of the RBL pair key: A_i = mix(gid_i), B_j = mix(gid_j + C).
-__device__ __forceinline__ unsigned long long rbl_key_a(int gid) {
+__host__ __device__ __forceinline__ unsigned long long rbl_key_a(int gid) {
   return rbl_mix((unsigned long long)(long long)gid);
 }
-__device__ __forceinline__ unsigned long long rbl_key_b(int gid) {
+__host__ __device__ __forceinline__ unsigned long long rbl_key_b(int gid) {
   return rbl_mix((unsigned long long)(long long)gid + 0xd1b54a32d192ed03ULL);
 }
 
@@ -129,7 +141,7 @@ inline DivTest make_divtest(int d) {
   return t;
 }
 
-__device__ __forceinline__ bool divisible(unsigned long long x, const DivTest& t) {
+__host__ __device__ __forceinline__ bool divisible(unsigned long long x, const DivTest& t) {
   if (t.trivial) return true;
   unsigned long long y = x * t.inv;
   if (t.shift) y = (y >> t.shift) | (y << (64 - t.shift));

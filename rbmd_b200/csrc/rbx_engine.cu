@@ -177,6 +177,7 @@ int rbx_engine::init() {
   for (unsigned long long*& p : snapu) ETRY(alloc(&p, N));
   int** iptrs[] = {&type, &gid, &orig, &tmpi, &perm, &cell_of_sorted, &cand_count};
   for (int** p : iptrs) ETRY(alloc(p, N));
+  if (prm.neighbor_type == RBX_NEIGHBOR_RBL) ETRY(alloc(&cand_far, N));
   ETRY(alloc(&key_a, N));
   ETRY(alloc(&key_b, N));
   ETRY(alloc(&tmpu, N));
@@ -389,7 +390,7 @@ int rbx_engine::rebuild_launches(cudaStream_t s, bool in_graph) {
   if (where) ETRY(launch_inverse_perm(n, orig, where, s));  // SHAKE / special rows
   ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, s));
   ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
-                        cand_count, cand, dflags + 1, list_scratch, s));
+                        cand_count, cand, dflags + 1, list_scratch, s, far_split()));
   if (in_graph) {
     ETRY(launch_zero_u64((unsigned long long*)cand_total, s));
     ETRY(launch_sum_i32(n, cand_count, cand_total, s));
@@ -432,7 +433,7 @@ int rbx_engine::rebuild() {
     ++graph_version;
     ETRY(launch_fill_i32(1, dflags + 1, 0, st));
     ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
-                          cand_count, cand, dflags + 1, list_scratch, st));
+                          cand_count, cand, dflags + 1, list_scratch, st, far_split()));
   }
   set_error("candidate list capacity did not converge");
   return RBX_ERR_CAPACITY;
@@ -459,7 +460,7 @@ int rbx_engine::real_space(const int* epoch_dev) {
   const bool mixed = prm.precision == RBX_MIXED;
   if (prm.neighbor_type == RBX_NEIGHBOR_RBL) {
     ETRY(launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch, epoch_dev,
-                          cand_count, cand, cap, fpx, fpy, fpz, fpart, nrbl, dflags + 3, st));
+                          rows(), fpx, fpy, fpz, fpart, nrbl, st));
     if (!spec_natoms) return RBX_OK;
     return launch_special_rbl(pp, spec_natoms, spec_atoms, spec_cnt, spec_part, spec_max,
                               spec_w[0], spec_w[1], spec_w[2], where, x, y, z, q, type, key_a,
@@ -472,8 +473,8 @@ int rbx_engine::real_space(const int* epoch_dev) {
     return launch_verlet_sog(sogp, n, x, y, z, q, type, cand_count, cand, cap, fpx, fpy, fpz,
                              nullptr, st);
   }
-  return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, fpx, fpy,
-                                 fpz, nullptr, epart, nfpart, st);
+  return launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, rows(), fpx, fpy,
+                                 fpz, nullptr, epart, verlet_blocks(), st);
 }
 
 int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
@@ -673,8 +674,7 @@ int rbx_engine::autotune(bool force, rbx_tuning* out) {
         rc = time_it(
             [&]() {
               return launch_rbl_fused(mixed, pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
-                                      nullptr, cand_count, cand, cap, fpx, fpy, fpz, fpart, nb,
-                                      dflags + 3, st);
+                                      nullptr, rows(), fpx, fpy, fpz, fpart, nb, st);
             },
             &ms);
         if (rc) break;
@@ -1188,15 +1188,16 @@ int rbx_engine::pair_energy(double* e_vdwl, double* e_coul, double* virial) {
   ETRY(check_rebuild(false));  // rows that hold every pair within cut_off
   ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
   const size_t N = (size_t)n;
-  ETRY(launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, cand_count, cand, cap, stage,
-                               stage + N, stage + 2 * N, nullptr, epart, nfpart, st));
-  std::vector<double> h((size_t)nfpart * 8);
+  const int nvb = verlet_blocks();
+  ETRY(launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, rows(), stage,
+                               stage + N, stage + 2 * N, nullptr, epart, nvb, st));
+  std::vector<double> h((size_t)nvb * 8);
   ETRY(cuda_ok(cudaMemcpyAsync(h.data(), epart, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
                                st),
                "D2H"));
   ETRY(cuda_ok(cudaStreamSynchronize(st), "pair energy sync"));
   double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < nfpart; ++b)
+  for (int b = 0; b < nvb; ++b)
     for (int k = 0; k < 8; ++k) t[k] += h[(size_t)b * 8 + k];
   if (e_vdwl) *e_vdwl = t[0];
   if (e_coul) *e_coul = t[1];
@@ -1220,7 +1221,7 @@ int rbx_engine::get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs
   ETRY(dalloc(&shell, N * cap));
   int rc = launch_to_fixed(dbox, n, x, y, z, q, atoms, st);
   if (!rc)
-    rc = launch_rbl_lists(pp, n, atoms, x, y, z, key_a, key_b, epoch, cand_count, cand, cap, cc,
+    rc = launch_rbl_lists(pp, n, atoms, x, y, z, key_a, key_b, epoch, rows(), cc,
                           core, sc, shell, st);
   std::vector<int> hcc(N), hsc(N), hcore(N * cap), hshell(N * cap), hgid(N);
   if (!rc) {
@@ -1331,8 +1332,8 @@ int rbx_engine::force_vjp(const double* g, double* d_eps, double* d_sigma, doubl
   ETRY(cuda_ok(cudaMemcpyAsync(eps_t, eps.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, st),
                "H2D"));
   ETRY(launch_gather_vec3(n, orig, stage, gx, gy, gz, st));
-  ETRY(launch_adj_pair(pp, n, x, y, z, q, type, sig_t, eps_t, key_a, key_b, epoch, cand_count,
-                       cand, cap, gx, gy, gz, mean_g, rx, ry, rz, dq, ppart, nb_pair, st));
+  ETRY(launch_adj_pair(pp, n, x, y, z, q, type, sig_t, eps_t, key_a, key_b, epoch, rows(), gx,
+                       gy, gz, mean_g, rx, ry, rz, dq, ppart, nb_pair, st));
   if (P > 0) {
     if (prm.precision == RBX_MIXED) {  // the k table from an FP64 rho(k) of the same samples
       ETRY(launch_rbe_rho_partial_f64(dbox, n, P, mx, my, mz, q, x, y, z, part_re, part_im,

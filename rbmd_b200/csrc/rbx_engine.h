@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "rbx.h"
@@ -60,6 +61,25 @@ struct rbx_engine {
   char* list_scratch = nullptr;
   int cap = 0;
   int *cand_count = nullptr, *cand = nullptr;
+  int* cand_far = nullptr;  // RBL engines: far-segment size of each candidate row
+  rbx::Rows rows() const {
+    rbx::Rows r;
+    r.count = cand_count;
+    r.far = cand_far;
+    r.idx = cand;
+    r.cap = cap;
+    return r;
+  }
+  // RBL engines split the candidate rows at r_core + skin (near / far segments)
+  const rbx::FarSplit* far_split() {
+    if (!cand_far) return nullptr;
+    split.r_near = prm.r_core + prm.skin;
+    split.far = cand_far;
+    return &split;
+  }
+  rbx::FarSplit split{};
+  // blocks of the Verlet pair kernel (its energy partials live in epart)
+  int verlet_blocks() const { return std::min(nfpart, rbx::sm_count() * 32); }
 
   // reductions, flags
   int nfpart = 0;  // capacity of fpart / epart (blocks)

@@ -70,6 +70,27 @@ int launch_ewald(const DBox& b, int n, const int kmax[3], double alpha, double q
 // Host-side sampler tables (order m = 0, +1, -1, ...), identical to the oracle's.
 int rbe_axis_table(double L, double alpha, double* w, int max_entries, double* total);
 
+// Candidate rows of the list builder: row i (idx + i * cap) holds
+// c = min(count[i], cap) entries, nf = c - nb in the near segment [0, nf) and
+// nb = far[i] (0 when far is null) in the far segment [cap - nb, cap);
+// count[i] > cap marks an overflowed build.
+struct Rows {
+  const int* count = nullptr;
+  const int* far = nullptr;
+  const int* idx = nullptr;
+  int cap = 0;
+};
+
+__device__ __forceinline__ void row_extent(const Rows& r, int i, int& nf, int& nb) {
+  const int c = min(r.count[i], r.cap);
+  nb = r.far ? min(r.far[i], c) : 0;
+  nf = c - nb;
+}
+// Entry k (0 <= k < nf + nb) of a row: the near segment, then the far one.
+__device__ __forceinline__ int row_at(const int* row, int cap, int nf, int nb, int k) {
+  return __ldg(row + (k < nf ? k : k + (cap - nf - nb)));
+}
+
 // ---- real space (rbx_pair.cu) ----
 // Screen of "r^2 < C" on the fixed-point |d|^2 (FP32, units of s^2 with
 // s = L/2^32, L the longest box edge): decided below lo and at or above hi,
@@ -107,25 +128,26 @@ int rbl_fused_blocks(int n);
 // Grid of the fused RBL kernel for this form: one wave of resident blocks,
 // at most max_blocks (the capacity of the per-block partial buffer).
 int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int waves = 8);
-// status (device int, may be null = no prefetch): bit 4 set if a row copy timed out.
+// Rows may be split (near / far segments, the far pairs certainly outside
+// r_core until the next rebuild) or not (far null: every pair classified).
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
                      const double* x, const double* y, const double* z, const double* q,
                      const int* type, const unsigned long long* key_a,
                      const unsigned long long* key_b, int epoch, const int* epoch_dev,
-                     const int* cand_count, const int* cand, int cap, double* fx, double* fy,
-                     double* fz, double* fpart, int nblocks, int* status, cudaStream_t st);
+                     const Rows& rows, double* fx, double* fy, double* fz, double* fpart,
+                     int nblocks, cudaStream_t st);
 // Verlet pair force over the candidate list, cut at cut_off (force predicate).
 int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, const double* x,
                             const double* y, const double* z, const double* q, const int* type,
-                            const int* cand_count, const int* cand, int cap, double* fx,
+                            const Rows& rows, double* fx,
                             double* fy, double* fz, double* fpart, double* epart, int nblocks,
                             cudaStream_t st);
 // Emit RBL lists (parity checks / export): core and shell rows (cap stride).
 int launch_rbl_lists(const PairParams& pp, int n, const uint4* atoms, const double* x,
                      const double* y, const double* z, const unsigned long long* key_a,
-                     const unsigned long long* key_b, int epoch, const int* cand_count,
-                     const int* cand, int cap, int* core_count, int* core, int* shell_count,
-                     int* shell, cudaStream_t st);
+                     const unsigned long long* key_b, int epoch, const Rows& rows,
+                     int* core_count, int* core, int* shell_count, int* shell,
+                     cudaStream_t st);
 int launch_rbl_keys(int n, const int* gid, unsigned long long* key_a, unsigned long long* key_b,
                     cudaStream_t st);
 // Drop-in ops with the reference layouts.
@@ -159,17 +181,26 @@ int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, 
 size_t cells_scratch_bytes(int n, int ncell);
 // Scratch of launch_full_list: per-chunk boxes and cells, full_list_scratch_bytes(n, ncell).
 size_t full_list_scratch_bytes(int n, int ncell);
+// Split of the candidate rows for RBL engines: candidates whose build distance
+// is certainly at least r_near go to the far segment at the back of the row,
+// far[i] of them (see Rows); the others, and any within the FP32 error of
+// r_near, to the near segment.
+struct FarSplit {
+  double r_near;
+  int* far;
+};
 int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
                      const double* y, const double* z, const int* cell_start, int cap,
-                     int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st);
+                     int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st,
+                     const FarSplit* split = nullptr);
 // Force adjoint (rbx_adjoint.cu).  Pair part: per-atom dL/dr, dL/dq and
 // per-block partials [nblocks][2 ntypes + 1] (d_eps, d_sigma, d_alpha).
 int adj_pair_blocks(int n);
 int launch_adj_pair(const PairParams& pp, int n, const double* x, const double* y,
                     const double* z, const double* q, const int* type, const double* sigma_t,
                     const double* eps_t, const unsigned long long* key_a,
-                    const unsigned long long* key_b, int epoch, const int* cand_count,
-                    const int* cand, int cap, const double* gx, const double* gy,
+                    const unsigned long long* key_b, int epoch, const Rows& rows,
+                    const double* gx, const double* gy,
                     const double* gz, const double mean_g[3], double* d_rx, double* d_ry,
                     double* d_rz, double* d_q, double* part, int nblocks, cudaStream_t st);
 // k-space part, added to d_r and d_q; part_gk[adj_k_blocks(n)] = block sums of g . K.

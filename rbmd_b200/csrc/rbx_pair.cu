@@ -140,68 +140,36 @@ __device__ __forceinline__ float fixed_d2_weighted(const PairParams& pp, const u
 }
 
 // ---------------------------------------------------------------------------
-// Bulk asynchronous global->shared copies (cp.async.bulk) tracked by an
-// mbarrier.  Used to prefetch the next atom's candidate row into shared memory
-// while the warp works on the current one.  Every wait is bounded.
+// Fused RBL filter + pair force over split candidate rows.
+//
+// The list builder writes each candidate row in two segments (see Rows): the
+// near segment holds every pair whose build distance is below
+// r_core + skin, the far segment (at the back of the row) every other pair.
+// Until the next rebuild no atom moves more than skin / 2 from where the list
+// was built, so a far pair is never a core pair: whether it carries a force
+// this step is decided by its shell-batch hash first, and only the selected
+// quarter (freq = 4) is gathered and tested against the shell window.  Near
+// pairs are classified in full (fixed-point screen, FP64 predicate inside the
+// guard bands) as the reference's FilterRBLNeighborCandidates does
+// (rbl_full_neighbor_list_op.hip.cu:237-304).
+//
+// MIXED = false: plain FP64 (pair vector and force math in FP64 from the FP64
+// positions).  MIXED = true: FP32 force math on the exact fixed-point pair
+// vector.  SEL selects the batch test: 0 any freq (divisibility by
+// multiplication), 1 freq a power of two (mask), 2 freq <= 4 (two bits of a
+// partial hash).
+//
+// One warp per atom i.  A segment is walked in batches of U x 32 candidates:
+// the index loads and gathers of a batch are issued before any is consumed,
+// classification and the hash are branch-free, and force-carrying pairs are
+// appended to a per-warp queue (index plus two flag bits) that is drained 32
+// pairs at a time from its tail.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned smem_addr(const void* p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_row_copy(int* dst, const int* src, unsigned bytes,
-                                              unsigned long long* bar) {
-  // order earlier generic-proxy reads of dst before the async-proxy write
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Wait for phase `parity` of bar; false after a bounded number of tries.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-  for (int it = 0; it < (1 << 22); ++it)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-// Bytes of a candidate row copy: 16-byte multiple, at least 16, within the row.
-__device__ __forceinline__ unsigned row_bytes(int cnt, int cap) {
-  unsigned b = ((unsigned)cnt * 4u + 15u) & ~15u;
-  b = b < 16u ? 16u : b;
-  const unsigned capb = (unsigned)cap * 4u;
-  return b > capb ? capb : b;
-}
-
-// Per-warp queue of force-carrying pairs: only j (with the shell flag in the
-// sign bit) is queued; the drain gathers what the 32 pairs need at once (the
-// fixed-point record in the mixed form, FP64 position and charge in the plain
-// form), which keeps the queue small and the block's shared memory low.
-constexpr int RBL_UNROLL = 4;                    // 32-candidate chunks per batch
-constexpr int RBL_QCAP = 32 + 32 * RBL_UNROLL;   // queue stays below 32 between batches
-
-struct QueueF64 {
-  int j[PAIR_WARPS][RBL_QCAP];
-};
-using QueueMixed = QueueF64;  // the drain re-reads the (L1-resident) fixed-point record
+constexpr int RBL_NEAR_U = 3;  // 32-candidate chunks per near batch
+constexpr int RBL_QCAP = 32 + 32 * (RBL_NEAR_U > 4 ? RBL_NEAR_U : 4);  // far batches: 128
+constexpr int QF_SHELL = (int)0x80000000;  // shell pair: force times freq
+constexpr int QF_CHECK = 0x40000000;       // far pair: shell window still to be tested
+constexpr int QF_INDEX = 0x3fffffff;       // atom index (n < 2^30)
 
 // LJ 12-6 force/r in FP32 with one fast reciprocal (mixed form only).
 __device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
@@ -210,38 +178,39 @@ __device__ __forceinline__ float lj_f32_fast(float eps_ij, float s6, float d2) {
   return -24.f * eps_ij * ((2.f * sd6 - 1.f) * sd6) * r2i;
 }
 
-// ---------------------------------------------------------------------------
-// Fused RBL filter + pair force.  MIXED = false: plain FP64 (pair vector and
-// force math in FP64 from the FP64 positions).  MIXED = true: FP32 force math
-// on the exact fixed-point pair vector.  SEL selects the batch test: 0 any
-// freq (divisibility by multiplication), 1 freq a power of two (mask), 2
-// freq <= 4 (two bits of a partial hash).
-//
-// The warp walks atom i's candidate row in batches of RBL_UNROLL x 32: index
-// loads and neighbour-record gathers of a batch are all issued before any is
-// consumed; classification and the shell hash are branch-free; pairs inside a
-// threshold guard band are settled once per batch with the FP64 predicate;
-// force-carrying pairs are appended to a per-warp queue and consumed 32 at a
-// time from its tail.
-// ---------------------------------------------------------------------------
-template <bool MIXED, int SEL, bool PREFETCH, bool CUBIC>
+template <int SEL>
+__device__ __forceinline__ bool batch_selected(unsigned long long key, unsigned long long fmask,
+                                               const DivTest& div) {
+  if (SEL == 2) return rbl_selected_low2(key, (unsigned)fmask);
+  const unsigned long long h = rbl_mix(key);
+  return SEL == 1 ? (h & fmask) == 0ULL : divisible(h, div);
+}
+
+// Pull the used lines of a split row toward L2 (32 ints = one 128-byte line a lane).
+__device__ __forceinline__ void prefetch_row(const Rows& rows, int i, int lane) {
+  int nf, nb;
+  row_extent(rows, i, nf, nb);
+  const int* r = rows.idx + (size_t)i * rows.cap;
+  for (int k = lane * 32; k < nf; k += 32 * 32)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(r + k));
+  const int b0 = (rows.cap - nb) & ~31;  // rows start on 128-byte lines (cap % 32 == 0)
+  for (int k = b0 + lane * 32; k < rows.cap && nb > 0; k += 32 * 32)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(r + k));
+}
+
+template <bool MIXED, int SEL, bool CUBIC>
 __global__ void __launch_bounds__(PAIR_BLOCK, MIXED ? 4 : 3)  // no spills in either form
 k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
             const double* __restrict__ y, const double* __restrict__ z,
             const double* __restrict__ q, const int* __restrict__ type,
             const unsigned long long* __restrict__ key_a,
             const unsigned long long* __restrict__ key_b, int epoch_arg,
-            const int* __restrict__ epoch_dev, const int* __restrict__ cand_count,
-            const int* __restrict__ cand, int cap, double* __restrict__ fx,
-            double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart,
-            int* __restrict__ status) {
+            const int* __restrict__ epoch_dev, Rows rows, double* __restrict__ fx,
+            double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart) {
   using T = typename std::conditional<MIXED, float, double>::type;
   const int epoch = epoch_dev ? *epoch_dev : epoch_arg;  // device copy inside a step graph
-  using Queue = typename std::conditional<MIXED, QueueMixed, QueueF64>::type;
-  extern __shared__ __align__(128) int s_rows[];  // PREFETCH: [PAIR_WARPS][2][cap]
-  __shared__ __align__(8) unsigned long long s_bar[PAIR_WARPS][2];
   __shared__ TypeTables tt;
-  __shared__ Queue qu;
+  __shared__ int s_q[PAIR_WARPS][RBL_QCAP];
   __shared__ double s_acc[PAIR_WARPS][3];
   __shared__ float f_eps[MAX_TYPES_SMEM * MAX_TYPES_SMEM], f_s6[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
   load_type_tables(tt, pp);
@@ -260,24 +229,8 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
   double acc0 = 0, acc1 = 0, acc2 = 0;
   const int nt = pp.ntypes;
   const int wstride = gridDim.x * PAIR_WARPS;
-  const int i0 = blockIdx.x * PAIR_WARPS + warp;
-  int* rowbuf = s_rows + (size_t)warp * 2 * cap;
-  int cnt_next = 0;
-  if (PREFETCH) {
-    if (lane == 0) {
-      mbar_init(&s_bar[warp][0], 1);
-      mbar_init(&s_bar[warp][1], 1);
-      mbar_fence_init();
-    }
-    __syncwarp();
-    if (i0 < n) {
-      const int c0 = min(cand_count[i0], cap);
-      if (lane == 0) bulk_row_copy(rowbuf, cand + (size_t)i0 * cap, row_bytes(c0, cap), &s_bar[warp][0]);
-      if (i0 + wstride < n) cnt_next = min(cand_count[i0 + wstride], cap);
-    }
-  }
-  int t = 0;
-  for (int i = i0; i < n; i += wstride, ++t) {
+  int* const wq = s_q[warp];
+  for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += wstride) {
     const uint4 ai = atoms[i];
     const double xi = x[i], yi = y[i], zi = z[i];
     const T qi = MIXED ? (T)__uint_as_float(ai.w) : (T)q[i];
@@ -285,92 +238,95 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
     const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
     // a row never holds more than cap entries; a larger count marks an
     // overflowed list (a rebuild inside a step graph), which the host replays
-    const int cnt = min(cand_count[i], cap);
-    const int* row = cand + (size_t)i * cap;
-    if (!PREFETCH) {  // pull the next atom's row toward L2 while this one is processed
-      const int inext = i + wstride;
-      if (inext < n && lane * 32 < cap)
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(cand + (size_t)inext * cap + lane * 32));
-    }
-    if (PREFETCH) {
-      const int b = t & 1;
-      const int inext = i + wstride;
-      if (inext < n) {  // prefetch the next row into the other buffer
-        if (lane == 0)
-          bulk_row_copy(rowbuf + (size_t)(b ^ 1) * cap, cand + (size_t)inext * cap,
-                        row_bytes(cnt_next, cap), &s_bar[warp][b ^ 1]);
-        cnt_next = inext + wstride < n ? min(cand_count[inext + wstride], cap) : 0;
-      }
-      if (!mbar_wait_bounded(&s_bar[warp][b], (unsigned)((t >> 1) & 1))) {
-        if (lane == 0) atomicOr(status, 4);  // a row copy never completed
-        if (inext < n)  // let the prefetch just issued land before leaving (bounded)
-          mbar_wait_bounded(&s_bar[warp][b ^ 1], (unsigned)(((t + 1) >> 1) & 1));
-        break;
-      }
-      row = rowbuf + (size_t)b * cap;
-    }
+    int nf, nb;
+    row_extent(rows, i, nf, nb);
+    const int* row = rows.idx + (size_t)i * rows.cap;
+    const int* far_row = row + (rows.cap - nb);
+    if (i + wstride < n) prefetch_row(rows, i + wstride, lane);
     int qn = 0;
     T fxa = 0, fya = 0, fza = 0;
 
     // force from queue slot `slot` (all 32 lanes take one pair each)
     auto pair_force = [&](int slot) {
-      const int c = qu.j[warp][slot];
-      const int j = c & 0x7fffffff;
+      const int c = wq[slot];
+      const int j = c & QF_INDEX;
       const int tj = __ldg(type + j);
       if (MIXED) {
         const uint4 aj = __ldg(atoms + j);  // exact wrapped fixed-point difference r_j - r_i
-        const float4 v = make_float4((float)(int)(aj.x - ai.x) * pp.sf[0],
-                                     (float)(int)(aj.y - ai.y) * pp.sf[1],
-                                     (float)(int)(aj.z - ai.z) * pp.sf[2], __uint_as_float(aj.w));
-        const float d2 = fmaf(v.x, v.x, fmaf(v.y, v.y, v.z * v.z));
-        const float qq = (float)qi * v.w;
+        const float ex = (float)(int)(aj.x - ai.x), ey = (float)(int)(aj.y - ai.y),
+                    ez = (float)(int)(aj.z - ai.z);
+        const float vx = ex * pp.sf[0], vy = ey * pp.sf[1], vz = ez * pp.sf[2];
+        const float d2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
+        bool ok = true;
+        if (c & QF_CHECK) {  // far pair: inside the shell window this step?
+          const float d2s =
+              CUBIC ? fmaf(ex, ex, fmaf(ey, ey, ez * ez))
+                    : fmaf(ex * pp.sw[0], ex * pp.sw[0],
+                           fmaf(ey * pp.sw[1], ey * pp.sw[1], (ez * pp.sw[2]) * (ez * pp.sw[2])));
+          bool unsure;
+          ok = classify_screen(pp, d2s, &unsure).shell_window;
+          if (unsure) ok = classify_exact(exact_d2(pp, x, y, z, i, j), pp).shell_window;
+        }
+        const float qq = (float)qi * __uint_as_float(aj.w);
         float f = lj_f32_fast(f_eps[ti * nt + tj], f_s6[ti * nt + tj], d2);
         if (qq != 0.f) f += coul_f32(alpha_f, sqa_f, qqr2e_f, qq, d2);
         if (c < 0) f *= (float)freq_t;
-        fxa += (T)(f * v.x);
-        fya += (T)(f * v.y);
-        fza += (T)(f * v.z);
+        f = ok ? f : 0.f;
+        fxa += (T)(f * vx);
+        fya += (T)(f * vy);
+        fza += (T)(f * vz);
       } else {
-        // r_j - r_i, MinImageDistance (box.h:51-73)
-        const double ddx = min_image1(__ldg(x + j) - xi, pp.box.len[0], pp.box.half[0]);
-        const double ddy = min_image1(__ldg(y + j) - yi, pp.box.len[1], pp.box.half[1]);
-        const double ddz = min_image1(__ldg(z + j) - zi, pp.box.len[2], pp.box.half[2]);
-        const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        // i minus j with the single-shift minimum image and no FMA: the
+        // list predicate's own r^2 (CaculateDistance), so the window test of a
+        // far pair is exact; the force takes r_j - r_i = -(dx, dy, dz)
+        const double dx = min_image1(__dsub_rn(xi, __ldg(x + j)), pp.box.len[0], pp.box.half[0]);
+        const double dy = min_image1(__dsub_rn(yi, __ldg(y + j)), pp.box.len[1], pp.box.half[1]);
+        const double dz = min_image1(__dsub_rn(zi, __ldg(z + j)), pp.box.len[2], pp.box.half[2]);
+        const double d2 =
+            __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        const bool ok = !(c & QF_CHECK) || classify_exact(d2, pp).shell_window;
         const double qq = (double)qi * __ldg(q + j);
         double f = lj_f64(tt.eps[ti * nt + tj], tt.s6[ti * nt + tj], d2);
         if (qq != 0.0) f += coul_f64(pp.alpha, pp.sqrt_alpha, pp.qqr2e, qq, d2);
         if (c < 0) f *= (double)freq_t;
-        fxa += (T)(f * ddx);
-        fya += (T)(f * ddy);
-        fza += (T)(f * ddz);
+        f = ok ? f : 0.0;
+        fxa -= (T)(f * dx);
+        fya -= (T)(f * dy);
+        fza -= (T)(f * dz);
       }
     };
+    auto drain_full = [&]() {
+      __syncwarp();
+      while (qn >= 32) {  // full batches from the tail of the queue
+        qn -= 32;
+        pair_force(qn + lane);
+      }
+      __syncwarp();
+    };
 
-    for (int k0 = 0; k0 < cnt; k0 += 32 * RBL_UNROLL) {
-      int jj[RBL_UNROLL];
-      uint4 aa[RBL_UNROLL];
+    // near segment: full classification
+    for (int k0 = 0; k0 < nf; k0 += 32 * RBL_NEAR_U) {
+      int jj[RBL_NEAR_U];
+      uint4 aa[RBL_NEAR_U];
+      unsigned long long kb[RBL_NEAR_U];
 #pragma unroll
-      for (int u = 0; u < RBL_UNROLL; ++u) {
+      for (int u = 0; u < RBL_NEAR_U; ++u) {
         const int k = k0 + u * 32 + lane;
-        jj[u] = k < cnt ? row[k] : i;
+        jj[u] = k < nf ? __ldg(row + k) : i;
       }
 #pragma unroll
-      for (int u = 0; u < RBL_UNROLL; ++u) aa[u] = __ldg(atoms + jj[u]);
+      for (int u = 0; u < RBL_NEAR_U; ++u) {
+        aa[u] = __ldg(atoms + jj[u]);
+        kb[u] = __ldg(key_b + jj[u]);
+      }
       unsigned core_bits = 0, shell_bits = 0, sel_bits = 0, unsure_bits = 0;
 #pragma unroll
-      for (int u = 0; u < RBL_UNROLL; ++u) {
+      for (int u = 0; u < RBL_NEAR_U; ++u) {
         const bool valid = jj[u] != i;
         bool unsure;
         const Classified c = classify_screen(
             pp, CUBIC ? fixed_d2(ai, aa[u]) : fixed_d2_weighted(pp, ai, aa[u]), &unsure);
-        // shell batch hash (RblShellSampleSelected)
-        bool sel;
-        if (SEL == 2) {
-          sel = rbl_selected_low2(ea ^ __ldg(key_b + jj[u]), (unsigned)fmask);
-        } else {
-          const unsigned long long h = rbl_mix(ea ^ __ldg(key_b + jj[u]));
-          sel = SEL == 1 ? (h & fmask) == 0ULL : divisible(h, pp.div);
-        }
+        const bool sel = batch_selected<SEL>(ea ^ kb[u], fmask, pp.div);
         core_bits |= (unsigned)(valid && c.core_active) << u;
         shell_bits |= (unsigned)(valid && c.shell_window) << u;
         sel_bits |= (unsigned)sel << u;
@@ -378,7 +334,7 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
       }
       if (__any_sync(0xffffffffu, unsure_bits != 0)) {  // rare: FP64 predicate decides
 #pragma unroll
-        for (int u = 0; u < RBL_UNROLL; ++u) {
+        for (int u = 0; u < RBL_NEAR_U; ++u) {
           if (unsure_bits & (1u << u)) {
             const Classified c = classify_exact(exact_d2(pp, x, y, z, i, jj[u]), pp);
             core_bits = (core_bits & ~(1u << u)) | ((unsigned)c.core_active << u);
@@ -388,21 +344,48 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
       }
       const unsigned push_bits = core_bits | (shell_bits & sel_bits);
 #pragma unroll
-      for (int u = 0; u < RBL_UNROLL; ++u) {
+      for (int u = 0; u < RBL_NEAR_U; ++u) {
         const bool push = (push_bits >> u) & 1u;
         const unsigned m = __ballot_sync(0xffffffffu, push);
-        if (push) {
-          const int pos = qn + __popc(m & lt);
-          qu.j[warp][pos] = ((core_bits >> u) & 1u) ? jj[u] : (jj[u] | (int)0x80000000);
-        }
+        if (push) wq[qn + __popc(m & lt)] = ((core_bits >> u) & 1u) ? jj[u] : (jj[u] | QF_SHELL);
         qn += __popc(m);
       }
-      __syncwarp();
-      while (qn >= 32) {  // full batches from the tail of the queue
-        qn -= 32;
-        pair_force(qn + lane);
+      drain_full();
+    }
+
+    // far segment: batch hash first; selected pairs are queued with the
+    // window test still to do.  The segment is read from the 16-byte boundary
+    // at or below its start, four entries a lane (one 128-entry batch per
+    // warp load); entries before the segment start are skipped.
+    {
+      const int fs = rows.cap - nb;  // first far entry
+      const int fb = fs & ~3;        // rows start on 128-byte lines (cap % 32 == 0)
+      const int4* f4 = reinterpret_cast<const int4*>(row + fb);
+      for (int k0 = 0; fb + k0 < rows.cap; k0 += 128) {
+        const int p0 = fb + k0 + 4 * lane;  // row position of this lane's first entry
+        int4 e = make_int4(i, i, i, i);
+        if (p0 < rows.cap) e = __ldg(f4 + (k0 >> 2) + lane);
+        const int jj[4] = {p0 >= fs ? e.x : i, p0 + 1 >= fs ? e.y : i, p0 + 2 >= fs ? e.z : i,
+                           p0 + 3 >= fs ? e.w : i};
+        unsigned long long kb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) kb[u] = __ldg(key_b + jj[u]);
+        unsigned sb = 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          sb |= (unsigned)((jj[u] != i) & batch_selected<SEL>(ea ^ kb[u], fmask, pp.div)) << u;
+        // queue slots: exclusive prefix over lanes of the per-lane counts (0..4)
+        const unsigned c = __popc(sb);
+        const unsigned b0 = __ballot_sync(0xffffffffu, c & 1u),
+                       b1 = __ballot_sync(0xffffffffu, c & 2u),
+                       b2 = __ballot_sync(0xffffffffu, c & 4u);
+        int pos = qn + __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if ((sb >> u) & 1u) wq[pos++] = jj[u] | QF_SHELL | QF_CHECK;
+        qn += __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2);
+        drain_full();
       }
-      __syncwarp();
     }
     if (lane < qn) pair_force(lane);
     __syncwarp();
@@ -437,8 +420,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK)
 k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
                    const double* __restrict__ x, const double* __restrict__ y,
                    const double* __restrict__ z, const double* __restrict__ q,
-                   const int* __restrict__ type, const int* __restrict__ cand_count,
-                   const int* __restrict__ cand, int cap, double* __restrict__ fx,
+                   const int* __restrict__ type, Rows rows, double* __restrict__ fx,
                    double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart,
                    double* __restrict__ epart) {
   __shared__ TypeTables tt;
@@ -458,8 +440,10 @@ k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
     const uint4 ai = atoms[i];
     const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
     const int ti = type[i];
-    const int cnt = min(cand_count[i], cap);
-    const int* row = cand + (size_t)i * cap;
+    int nf, nb;
+    row_extent(rows, i, nf, nb);
+    const int cnt = nf + nb;
+    const int* row = rows.idx + (size_t)i * rows.cap;
     int qn = 0;
     double fxa = 0, fya = 0, fza = 0;
     double ea[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -470,7 +454,7 @@ k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
         int j = 0;
         const int k = k0 + lane;
         if (k < cnt) {
-          j = __ldg(row + k);
+          j = row_at(row, rows.cap, nf, nb, k);
           if (j != i) {
             const uint4 aj = __ldg(atoms + j);
             const float d2s = CUBIC ? fixed_d2(ai, aj) : fixed_d2_weighted(pp, ai, aj);
@@ -583,17 +567,19 @@ __global__ void k_rbl_lists(PairParams pp, int n, const uint4* __restrict__ atom
                             const double* __restrict__ x, const double* __restrict__ y,
                             const double* __restrict__ z,
                             const unsigned long long* __restrict__ key_a,
-                            const unsigned long long* __restrict__ key_b, int epoch,
-                            const int* __restrict__ cand_count, const int* __restrict__ cand,
-                            int cap, int* __restrict__ core_count, int* __restrict__ core,
+                            const unsigned long long* __restrict__ key_b, int epoch, Rows rows,
+                            int* __restrict__ core_count, int* __restrict__ core,
                             int* __restrict__ shell_count, int* __restrict__ shell) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const unsigned long long ea = key_a[i] ^ (unsigned long long)(long long)epoch;
   int nc = 0, ns = 0;
-  const int cnt = min(cand_count[i], cap);
-  for (int t = 0; t < cnt; ++t) {
-    const int j = cand[(size_t)i * cap + t];
+  int nf, nb;
+  row_extent(rows, i, nf, nb);
+  const int cap = rows.cap;
+  const int* row = rows.idx + (size_t)i * cap;
+  for (int t = 0; t < nf + nb; ++t) {
+    const int j = row_at(row, cap, nf, nb, t);
     if (j == i) continue;
     const double d2 = exact_d2(pp, x, y, z, i, j);
     if (d2 < pp.core2_list)
@@ -813,70 +799,46 @@ IntScreen make_screen(double C, double L, double band) {
 }
 
 int rbl_fused_blocks(int n) {
-  // capacity of the per-block partial buffers: enough for rbl_fused_grid
-  const int target = sm_count() * 32;
+  // capacity of the per-block partial buffers: enough for rbl_fused_grid at up
+  // to 16 waves of 8 resident blocks per SM, so a grid is never cut short of a
+  // whole number of waves
+  const int target = sm_count() * 8 * 16;
   int b = (n + PAIR_WARPS - 1) / PAIR_WARPS;
   if (b > target) b = target;
   return b < 1 ? 1 : b;
 }
 
-int rbl_prefetch_smem(int cap) { return PAIR_WARPS * 2 * cap * (int)sizeof(int); }
-constexpr int kRblMaxDynSmem = 160 * 1024;  // prefetch buffers used up to this size
-
 namespace {
 using RblKernel = void (*)(PairParams, int, const uint4*, const double*, const double*,
                            const double*, const double*, const int*, const unsigned long long*,
-                           const unsigned long long*, int, const int*, const int*, const int*, int,
-                           double*, double*, double*, double*, int*);
+                           const unsigned long long*, int, const int*, Rows, double*, double*,
+                           double*, double*);
 
-struct RblChoice {
-  RblKernel kern;
-  int smem;
-};
-
-// The instantiation a launch uses.  FP64 form: candidate rows prefetched into
-// shared memory when both buffers fit.  The mixed form runs faster at the
-// occupancy it keeps without them.  Cubic boxes take the unweighted distance
-// screen.
-RblChoice rbl_choose(bool mixed, int freq, int cap, bool with_status, bool cubic) {
+// The instantiation a launch uses: the batch test from freq, the unweighted
+// distance screen on cubic boxes.
+RblKernel rbl_choose(bool mixed, int freq, bool cubic) {
   const bool pow2 = freq >= 1 && (freq & (freq - 1)) == 0;
   const int sel = pow2 ? (freq <= 4 ? 2 : 1) : 0;
-  const int dyn = rbl_prefetch_smem(cap);
-  const bool prefetch = !mixed && with_status && dyn <= kRblMaxDynSmem;
-  static RblKernel const table[2][3][2][2] = {
-      {{{k_rbl_fused<false, 0, false, false>, k_rbl_fused<false, 0, false, true>},
-        {k_rbl_fused<false, 0, true, false>, k_rbl_fused<false, 0, true, true>}},
-       {{k_rbl_fused<false, 1, false, false>, k_rbl_fused<false, 1, false, true>},
-        {k_rbl_fused<false, 1, true, false>, k_rbl_fused<false, 1, true, true>}},
-       {{k_rbl_fused<false, 2, false, false>, k_rbl_fused<false, 2, false, true>},
-        {k_rbl_fused<false, 2, true, false>, k_rbl_fused<false, 2, true, true>}}},
-      {{{k_rbl_fused<true, 0, false, false>, k_rbl_fused<true, 0, false, true>},
-        {nullptr, nullptr}},
-       {{k_rbl_fused<true, 1, false, false>, k_rbl_fused<true, 1, false, true>},
-        {nullptr, nullptr}},
-       {{k_rbl_fused<true, 2, false, false>, k_rbl_fused<true, 2, false, true>},
-        {nullptr, nullptr}}}};
-  RblChoice c{table[mixed][sel][prefetch][cubic], prefetch ? dyn : 0};
-  if (prefetch) {  // opt in to large dynamic shared memory, once per instantiation
-    static std::atomic<int> done[3][2] = {};
-    if (!done[sel][cubic].exchange(1)) {
-      cudaFuncSetAttribute(c.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kRblMaxDynSmem);
-      cudaFuncSetAttribute(c.kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    }
-  }
-  return c;
+  static RblKernel const table[2][3][2] = {
+      {{k_rbl_fused<false, 0, false>, k_rbl_fused<false, 0, true>},
+       {k_rbl_fused<false, 1, false>, k_rbl_fused<false, 1, true>},
+       {k_rbl_fused<false, 2, false>, k_rbl_fused<false, 2, true>}},
+      {{k_rbl_fused<true, 0, false>, k_rbl_fused<true, 0, true>},
+       {k_rbl_fused<true, 1, false>, k_rbl_fused<true, 1, true>},
+       {k_rbl_fused<true, 2, false>, k_rbl_fused<true, 2, true>}}};
+  return table[mixed][sel][cubic];
 }
 }  // namespace
 
 int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int waves) {
   // waves of resident blocks (default 8): with several waves the block
-  // scheduler evens out the per-atom work (200k atoms, mixed form: 1 wave
-  // 0.59 ms, 3 waves 0.555 ms, 6-12 waves 0.54 ms, 48 waves 0.57 ms)
+  // scheduler evens out the per-atom work
+  (void)cap;
   const int kRblWaves = waves > 0 ? waves : 8;
-  const RblChoice c = rbl_choose(mixed, freq, cap, true, true);  // occupancy of the cubic form
+  const RblKernel k = rbl_choose(mixed, freq, true);  // occupancy of the cubic form
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, c.kern, PAIR_BLOCK, c.smem) !=
-          cudaSuccess || occ < 1) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, PAIR_BLOCK, 0) != cudaSuccess ||
+      occ < 1) {
     cudaGetLastError();
     occ = 1;
   }
@@ -891,44 +853,43 @@ int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms
                      const double* x, const double* y, const double* z, const double* q,
                      const int* type, const unsigned long long* key_a,
                      const unsigned long long* key_b, int epoch, const int* epoch_dev,
-                     const int* cand_count, const int* cand, int cap, double* fx, double* fy,
-                     double* fz, double* fpart, int nblocks, int* status, cudaStream_t st) {
+                     const Rows& rows, double* fx, double* fy, double* fz, double* fpart,
+                     int nblocks, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  const RblChoice c = rbl_choose(mixed, pp.freq, cap, status != nullptr, pp.cubic != 0);
-  c.kern<<<nblocks, PAIR_BLOCK, c.smem, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
-                                              epoch_dev, cand_count, cand, cap, fx, fy, fz, fpart,
-                                              status);
+  if (n > QF_INDEX) {
+    set_error("rbl_fused: at most %d atoms", QF_INDEX);
+    return RBX_ERR_INVALID;
+  }
+  const RblKernel k = rbl_choose(mixed, pp.freq, pp.cubic != 0);
+  k<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
+                                    epoch_dev, rows, fx, fy, fz, fpart);
   count_launch();
   return check_launch(mixed ? "rbl_fused_mixed" : "rbl_fused_f64");
 }
 
 int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, const double* x,
                             const double* y, const double* z, const double* q, const int* type,
-                            const int* cand_count, const int* cand, int cap, double* fx,
-                            double* fy, double* fz, double* fpart, double* epart, int nblocks,
-                            cudaStream_t st) {
+                            const Rows& rows, double* fx, double* fy, double* fz, double* fpart,
+                            double* epart, int nblocks, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
   if (pp.cubic)
-    k_verlet_fused_f64<true><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type,
-                                                             cand_count, cand, cap, fx, fy, fz,
-                                                             fpart, epart);
+    k_verlet_fused_f64<true><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, rows,
+                                                             fx, fy, fz, fpart, epart);
   else
     k_verlet_fused_f64<false><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type,
-                                                              cand_count, cand, cap, fx, fy, fz,
-                                                              fpart, epart);
+                                                              rows, fx, fy, fz, fpart, epart);
   count_launch();
   return check_launch("verlet_fused_f64");
 }
 
 int launch_rbl_lists(const PairParams& pp, int n, const uint4* atoms, const double* x,
                      const double* y, const double* z, const unsigned long long* key_a,
-                     const unsigned long long* key_b, int epoch, const int* cand_count,
-                     const int* cand, int cap, int* core_count, int* core, int* shell_count,
-                     int* shell, cudaStream_t st) {
+                     const unsigned long long* key_b, int epoch, const Rows& rows,
+                     int* core_count, int* core, int* shell_count, int* shell,
+                     cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  k_rbl_lists<<<(n + 127) / 128, 128, 0, st>>>(pp, n, atoms, x, y, z, key_a, key_b, epoch,
-                                               cand_count, cand, cap, core_count, core,
-                                               shell_count, shell);
+  k_rbl_lists<<<(n + 127) / 128, 128, 0, st>>>(pp, n, atoms, x, y, z, key_a, key_b, epoch, rows,
+                                               core_count, core, shell_count, shell);
   count_launch();
   return check_launch("rbl_lists");
 }
