@@ -7,7 +7,8 @@
  *  - Every function returns an rbx_status (0 = RBX_OK); rbx_last_error() gives
  *    the message of the last failure on the calling thread.  No C++ exception
  *    crosses this boundary.
- *  - Op-level functions take caller-owned DEVICE pointers (FP64 SoA, int32
+ *  - Op-level functions take caller-owned DEVICE pointers (FP64 SoA, or FP32
+ *    for the *_f32 twins of the float build; int32
  *    ids, the reference's rbmd::Real / rbmd::Id layout) and a cudaStream_t
  *    passed as void*; they enqueue work and return without synchronising
  *    unless stated.  Argument order follows the reference functor each one
@@ -298,6 +299,81 @@ int rbx_pair_force_verlet(const rbx_box* box, double cut_off, int num_atoms,
                           double* total_ecoul, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* FP32 twins for the reference's default build: rbmd::Real is float unless  */
+/* ENABLE_DOUBLE (cmake/option.cmake:1, src/common/types.h:4-8).  Argument   */
+/* order and meaning as the FP64 entries above and the functors they cite;   */
+/* every Real buffer and scalar is float, ids stay int (rbmd::Id without      */
+/* ENABLE_64BIT_IDS).  Membership tests (list predicates, force windows) are */
+/* evaluated in float as the float build evaluates them, so lists and kept   */
+/* pairs are that build's; values are computed in FP64 (real space, energy)  */
+/* or in the mixed form (structure factor and RBE force: exact integer phase */
+/* on fixed-point coordinates, FP32 sincos, FP64 reductions) and stored in   */
+/* float.                                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* ComputePnumberChargeStructureFactorOp, float build (kspace_calculator_op.h:106-121). */
+int rbx_rbe_structure_factor_f32(const rbx_box* box, int num_atoms, int p_number,
+                                 const float* charge, const float* p_sample_x,
+                                 const float* p_sample_y, const float* p_sample_z,
+                                 const float* px, const float* py, const float* pz,
+                                 float* density_real, float* density_imag, void* stream);
+
+/* ComputeRBEForceOp, float build (kspace_calculator_op.h:123-135). */
+int rbx_rbe_force_f32(const rbx_box* box, int num_atoms, int p_number, float alpha,
+                      float rbe_sum_gauss, float qqr2e, const float* real_array,
+                      const float* imag_array, const float* charge, const float* p_sample_x,
+                      const float* p_sample_y, const float* p_sample_z, const float* px,
+                      const float* py, const float* pz, float* fx, float* fy, float* fz,
+                      void* stream);
+
+/* ComputeRBEForceVirialOp, float build (kspace_calculator_op.hip.cu:573-674). */
+int rbx_rbe_energy_virial_f32(const rbx_box* box, int p, float alpha, float rbe_sum_gauss,
+                              float qqrd2e, float qsqsum, float qsum, const float* real_array,
+                              const float* imag_array, const float* p_sample_x,
+                              const float* p_sample_y, const float* p_sample_z,
+                              float* virial_tensor, float* energy, void* stream);
+
+/* FilterRblNeighborCandidatesOp, float build
+ * (rbl_full_neighbor_list_op.hip.cu:237-334): CaculateDistance in float
+ * (POW = powf), thresholds r_core^2 - EPSILON and cut_off^2 - EPSILON as the
+ * float build forms them. */
+int rbx_rbl_filter_f32(float core_cutoff_2, float force_cutoff_2, int total_atom_num,
+                       const int* atoms_id, const float* px, const float* py, const float* pz,
+                       const int* candidate_start, const int* candidate_end,
+                       const int* candidate_neighbors, const int* max_core_neighbor_num,
+                       const int* core_start, int* core_end, int* core_neighbors,
+                       int random_neighbor_capacity, int* random_neighbors,
+                       int* random_neighbors_num, int* required_random_neighbor_capacity,
+                       const rbx_box* box, int* should_realloc, int selection_frequency,
+                       int sample_epoch, void* stream);
+
+/* LJCutCoulRBLForceOp, float build (lj_cut_coul_kspace_op.hip.cu:569-683). */
+int rbx_pair_force_rbl_f32(const rbx_box* box, float rs, float rc, int num_atoms,
+                           int neighbor_sample_num, int pice_num, float alpha, float qqr2e,
+                           const int* atoms_type, const float* sigma, const float* eps,
+                           const int* start_id, const int* end_id, const int* id_verletlist,
+                           const int* id_random_neighbor, const int* random_neighbor_num,
+                           const float* charge, const float* px, const float* py,
+                           const float* pz, float* fx, float* fy, float* fz, void* stream);
+
+/* Mean-force removal, float build (lj_cut_coul_kspace.cpp:537-563,
+ * force_op.hip.cu:9-45): the mean is summed in FP64; mean_out (device, 3
+ * floats) may be NULL. */
+int rbx_fix_rbl_force_f32(int num_atoms, float* fx, float* fy, float* fz, float* mean_out,
+                          void* stream);
+
+/* LJCutCoulForceOp, float build (lj_cut_coul_kspace_op.hip.cu:256-356):
+ * flat_virial[c*n + i] in float; total_evdwl / total_ecoul (device floats,
+ * may be NULL) are overwritten with FP64 sums. */
+int rbx_pair_force_verlet_f32(const rbx_box* box, float cut_off, int num_atoms, float alpha,
+                              float qqr2e, const int* atoms_type, const float* sigma,
+                              const float* eps, const int* start_id, const int* end_id,
+                              const int* id_verletlist, const float* charge, const float* px,
+                              const float* py, const float* pz, float* fx, float* fy, float* fz,
+                              float* flat_virial, float* total_evdwl, float* total_ecoul,
+                              void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Engine: LJCutCoulKspace (src/force/src/lj_cut_coul_kspace.cpp) with its   */
 /* KSpaceCalculator and neighbor builders, plus the NVE velocity-Verlet step */
 /* (NVEensemble::Solve, src/simulate_pipeline/src/nve_ensemble.cpp:59-91).   */
@@ -374,6 +450,28 @@ rbx_engine* rbx_engine_create_json(const char* json_text, const rbx_box* box,
                                    int num_atoms, int ntypes, const double* sigma,
                                    const double* eps, const double* mass,
                                    const double* charges, int precision, int device);
+
+/* The force plugin itself: LJCutCoulKspace behind RBMD's Force interface
+ * (Init / Execute / EvaluatePotentialEnergy, src/force/include/force.h:10-48),
+ * built from the same JSON as rbx_engine_create_json.  rbx_force_engine gives
+ * the engine it drives (set positions and k-samples through the engine
+ * functions).  rbx_force_execute runs one force evaluation at sample epoch
+ * `epoch` and then EvaluatePotentialEnergy; thermo_step stands for
+ * ThermoStats::ShouldOutput() (with energy_rbe_flag "yes" the RBE energy of a
+ * thermo step is the exact Ewald energy over kmax plus the self energy).
+ * rbx_force_energies: {e_vdwl, e_coul, e_kspace, e_pe} of the last
+ * evaluation, per atom in LJ units as RBMD reports them (totals in other
+ * units); the pair energies only for a Verlet list, or RBL with
+ * energy_rbl_flag "yes" (lj_cut_coul_kspace.cpp:570-572, 867-878). */
+typedef struct rbx_force rbx_force;
+rbx_force* rbx_force_create_json(const char* json_text, const rbx_box* box, int num_atoms,
+                                 int ntypes, const double* sigma, const double* eps,
+                                 const double* mass, const double* charges, int precision,
+                                 int device);
+void rbx_force_destroy(rbx_force* f);
+rbx_engine* rbx_force_engine(rbx_force* f);
+int rbx_force_execute(rbx_force* f, int epoch, int thermo_step);
+int rbx_force_energies(rbx_force* f, double out[4]);
 void rbx_engine_destroy(rbx_engine* e);
 /* Build and load an engine from RBMD's input files the way MDApplication
  * starts (md_application.cpp:175-195, LammpsFullReader::Load,
@@ -514,6 +612,13 @@ int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace);
  * count in LJ units.  Any pointer may be NULL.  RBL and Verlet-list engines
  * (VERLET-SOG reports its energies through rbx_pair_force_verlet_sog). */
 int rbx_engine_pair_energy(rbx_engine* e, double* e_vdwl, double* e_coul, double* virial);
+/* Exact Ewald reciprocal energy over the kmax box plus the self energy
+ * (-qqr2e sqrt(alpha / pi) sum q^2) of the current positions, on the host:
+ * KSpaceCalculator::ComputeKspaceEnergy + ComputeSelfEnergy
+ * (src/force/src/kspace_calculator.cpp:816-907), which RBMD reports as the RBE
+ * k-space energy on thermo steps when coulomb.energy_rbe_flag is "yes"
+ * (:630-645).  FP64 in both precision forms. */
+int rbx_engine_kspace_energy_exact(rbx_engine* e, const int kmax[3], double* energy);
 /* Last RBL lists as (gid_i, gid_j) pairs; sizes in/out. */
 int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core,
                              int* shell_pairs, int64_t* n_shell);

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librbx.so")
 
-CU_SOURCES = ["rbx_capi.cu", "rbx_rbe.cu", "rbx_pair.cu", "rbx_cells.cu", "rbx_engine.cu",
+CU_SOURCES = ["rbx_capi.cu", "rbx_capi_f32.cu", "rbx_rbe.cu", "rbx_pair.cu", "rbx_cells.cu", "rbx_engine.cu",
               "rbx_batch.cu", "rbx_adjoint.cu", "rbx_thermo.cu", "rbx_shake.cu",
               "rbx_special.cu", "rbx_rbsog.cu"]
 CXX_SOURCES = ["host/config_data.cpp", "host/lj_cut_coul_kspace.cpp", "host/lammps_data.cpp",

@@ -236,15 +236,21 @@ void LJCutCoulKspace::Execute() {
 }
 
 // EvaluatePotentialEnergy (lj_cut_coul_kspace.cpp:867-878): k-space energy
-// (KSpaceCalculator::EvaluatePotentialEnergy, kspace_calculator.cpp:375-385),
-// pair energies where RBMD computes them (ComputeLJVerlet every step,
-// ComputeLJCoulEnergy after the RBL force when energy_rbl_flag is "yes",
-// :570-572, :821-865), each divided by the atom count in LJ units.
+// (KSpaceCalculator::EvaluatePotentialEnergy, kspace_calculator.cpp:375-385;
+// for RBE with energy_rbe_flag "yes" on a thermo step the exact Ewald energy
+// plus the self energy, :630-645), pair energies where RBMD computes them
+// (ComputeLJVerlet every step, ComputeLJCoulEnergy after the RBL force when
+// energy_rbl_flag is "yes", :570-572, :821-865), each divided by the atom
+// count in LJ units.
 void LJCutCoulKspace::EvaluatePotentialEnergy() {
   const double per = _lj_units ? 1.0 / (double)_n : 1.0;
   rbx_stats s;
   if (rbx_engine_get_stats(_engine, &s) != RBX_OK) throw std::runtime_error(rbx_last_error());
-  _e_kspace = s.e_kspace * per;
+  double ek = s.e_kspace;
+  if (_kspace.type() == "RBE" && _kspace.energy_rbe_flag() == "yes" && thermo_step)
+    if (rbx_engine_kspace_energy_exact(_engine, _kspace.kmax(), &ek) != RBX_OK)
+      throw std::runtime_error(rbx_last_error());
+  _e_kspace = ek * per;
   const bool verlet = _neighbor_type == "Verlet-List" || _neighbor_type == "VERLET";
   if (verlet || (_neighbor_type == "RBL" && _energy_rbl_flag == "yes")) {
     double ev = 0.0, ec = 0.0;
@@ -262,6 +268,62 @@ using rbx_host::LJCutCoulKspace;
 
 namespace rbx {
 void set_error(const char* fmt, ...);
+}
+
+// The plugin itself behind the C ABI (Force::Init / Execute /
+// EvaluatePotentialEnergy, src/force/include/force.h:10-48).
+struct rbx_force : LJCutCoulKspace {
+  using LJCutCoulKspace::LJCutCoulKspace;
+};
+
+extern "C" rbx_force* rbx_force_create_json(const char* json_text, const rbx_box* box,
+                                            int num_atoms, int ntypes, const double* sigma,
+                                            const double* eps, const double* mass,
+                                            const double* charges, int precision, int device) {
+  if (!json_text || !box || num_atoms <= 0 || ntypes <= 0 || !sigma || !eps || !mass) {
+    rbx::set_error("rbx_force_create_json: null argument or empty system");
+    return nullptr;
+  }
+  try {
+    auto* f = new rbx_force(json_text, *box, num_atoms, ntypes, sigma, eps, mass, charges,
+                            precision, device);
+    try {
+      f->Init();
+    } catch (...) {
+      delete f;
+      throw;
+    }
+    return f;
+  } catch (const std::exception& ex) {
+    rbx::set_error("%s", ex.what());
+    return nullptr;
+  }
+}
+
+extern "C" void rbx_force_destroy(rbx_force* f) { delete f; }
+
+extern "C" rbx_engine* rbx_force_engine(rbx_force* f) { return f ? f->engine() : nullptr; }
+
+extern "C" int rbx_force_execute(rbx_force* f, int epoch, int thermo_step) {
+  if (!f) return RBX_ERR_INVALID;
+  try {
+    f->epoch = epoch;
+    f->thermo_step = thermo_step != 0;
+    f->Execute();
+    return RBX_OK;
+  } catch (const std::exception& ex) {
+    rbx::set_error("%s", ex.what());
+    return RBX_ERR_INVALID;
+  }
+}
+
+extern "C" int rbx_force_energies(rbx_force* f, double out[4]) {
+  if (!f || !out) return RBX_ERR_INVALID;
+  out[0] = f->e_vdwl();
+  out[1] = f->e_coul();
+  out[2] = f->e_kspace();
+  out[3] = f->e_pe();
+  return RBX_OK;
 }
 
 extern "C" rbx_engine* rbx_engine_create_json(const char* json_text, const rbx_box* box,

@@ -66,6 +66,10 @@ class LJCutCoulKspace : public Force {
     return e;
   }
   int epoch = 0;
+  // ThermoStats::ShouldOutput() of the host's pipeline for the next Execute:
+  // with energy_rbe_flag "yes" the RBE k-space energy of a thermo step is the
+  // exact Ewald energy over kmax plus the self energy (kspace_calculator.cpp:630-645)
+  bool thermo_step = true;
   // energies of the last evaluation, per atom in LJ units (totals otherwise);
   // the pair energies only for a Verlet list or RBL with energy_rbl_flag "yes"
   double e_kspace() const { return _e_kspace; }

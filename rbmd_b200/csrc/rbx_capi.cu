@@ -12,6 +12,7 @@
 #include "rbx.h"
 #include "rbx_common.cuh"
 #include "rbx_kernels.h"
+#include "rbx_capi_util.h"
 
 namespace rbx {
 
@@ -151,41 +152,10 @@ int rbl_freq(int n_global, const rbx_box& b, double r_core, double cut_off, int 
   return shell <= sample_num ? 1 : (int)ceil((double)shell / (double)sample_num);
 }
 
-static bool valid_box(const rbx_box* b) {
-  if (!b) return false;
-  for (int d = 0; d < 3; ++d)
-    if (!(b->hi[d] - b->lo[d] > 0.0) || !isfinite(b->hi[d] - b->lo[d])) return false;
-  return true;
-}
 
 }  // namespace rbx
 
 using namespace rbx;
-
-#define RBX_CHECK_BOX(b)                           \
-  do {                                             \
-    if (!valid_box(b)) {                           \
-      set_error("invalid box (hi must exceed lo)"); \
-      return RBX_ERR_INVALID;                      \
-    }                                              \
-  } while (0)
-
-#define RBX_TRY(expr)       \
-  do {                      \
-    const int _rc = (expr); \
-    if (_rc) return _rc;    \
-  } while (0)
-
-template <typename T>
-static int async_alloc(T** p, size_t count, cudaStream_t st) {
-  if (count == 0) count = 1;
-  if (cudaMallocAsync((void**)p, sizeof(T) * count, st) != cudaSuccess) {
-    cudaGetLastError();
-    set_error("cudaMallocAsync of %zu bytes failed", sizeof(T) * count);
-    return RBX_ERR_NOMEM;
-  }
-  return RBX_OK;
-}
 
 extern "C" {
 

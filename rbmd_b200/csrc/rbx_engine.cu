@@ -1178,19 +1178,23 @@ int rbx_engine::get_force_parts(double* f_pair, double* f_kspace) {
 
 // LJ and erfc-Coulomb energies and the virial over every pair within cut_off
 // of the current positions: the Verlet kernel over the candidate rows (their
-// forces go to scratch), per-block partials summed here in block order.
+// forces go to scratch), per-block partials summed here in block order.  A
+// Verlet-list engine whose forces are those of the current positions already
+// holds the partials of that same kernel from its last force evaluation.
 int rbx_engine::pair_energy(double* e_vdwl, double* e_coul, double* virial) {
   cudaSetDevice(device);
   if (prm.neighbor_type == RBX_NEIGHBOR_VERLET_SOG) {
     set_error("pair energy: the VERLET-SOG energies come from rbx_pair_force_verlet_sog");
     return RBX_ERR_INVALID;
   }
-  ETRY(check_rebuild(false));  // rows that hold every pair within cut_off
-  ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
-  const size_t N = (size_t)n;
   const int nvb = verlet_blocks();
-  ETRY(launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, rows(), stage,
-                               stage + N, stage + 2 * N, nullptr, epart, nvb, st));
+  if (!(prm.neighbor_type == RBX_NEIGHBOR_VERLET && have_forces)) {
+    ETRY(check_rebuild(false));  // rows that hold every pair within cut_off
+    ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, st));
+    const size_t N = (size_t)n;
+    ETRY(launch_verlet_fused_f64(pp, n, atoms, x, y, z, q, type, rows(), stage,
+                                 stage + N, stage + 2 * N, nullptr, epart, nvb, st));
+  }
   std::vector<double> h((size_t)nvb * 8);
   ETRY(cuda_ok(cudaMemcpyAsync(h.data(), epart, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
                                st),
@@ -1204,6 +1208,40 @@ int rbx_engine::pair_energy(double* e_vdwl, double* e_coul, double* virial) {
   if (virial)
     for (int k = 0; k < 6; ++k) virial[k] = t[2 + k];
   return RBX_OK;
+}
+
+// Exact Ewald reciprocal energy over the kmax box plus the self energy of the
+// current positions (ComputeKspaceEnergy + ComputeSelfEnergy,
+// kspace_calculator.cpp:630-645, 816-907): what RBMD reports on thermo steps
+// when energy_rbe_flag is "yes".
+int rbx_engine::kspace_energy_exact(const int kmax[3], double* energy) {
+  cudaSetDevice(device);
+  if (!kmax || kmax[0] < 0 || kmax[1] < 0 || kmax[2] < 0 || !energy) {
+    set_error("kspace_energy_exact: invalid kmax or output");
+    return RBX_ERR_INVALID;
+  }
+  const int nk = (2 * kmax[0] + 1) * (2 * kmax[1] + 1) * (2 * kmax[2] + 1) - 1;
+  if (nk <= 0) {
+    *energy = -prm.qqr2e * sqrt(prm.alpha / RBX_PI) * qsq;
+    return RBX_OK;
+  }
+  double* buf = nullptr;  // re, im, k vectors, one energy
+  if (cudaMallocAsync((void**)&buf, sizeof(double) * (5 * (size_t)nk + 1), st) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("kspace_energy_exact: cudaMallocAsync failed");
+    return RBX_ERR_NOMEM;
+  }
+  const size_t N = (size_t)n;
+  int rc = launch_ewald(dbox, n, kmax, prm.alpha, prm.qqr2e, qsq, q, x, y, z, buf, buf + nk,
+                        buf + 2 * (size_t)nk, stage, stage + N, stage + 2 * N,
+                        buf + 5 * (size_t)nk, st);
+  if (!rc)
+    rc = cuda_ok(cudaMemcpyAsync(energy, buf + 5 * (size_t)nk, sizeof(double),
+                                 cudaMemcpyDeviceToHost, st),
+                 "D2H");
+  cudaFreeAsync(buf, st);
+  if (!rc) rc = cuda_ok(cudaStreamSynchronize(st), "kspace energy sync");
+  return rc;
 }
 
 int rbx_engine::get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs,
@@ -1866,6 +1904,11 @@ int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace) 
 int rbx_engine_pair_energy(rbx_engine* e, double* e_vdwl, double* e_coul, double* virial) {
   if (!e) return RBX_ERR_INVALID;
   return e->pair_energy(e_vdwl, e_coul, virial);
+}
+
+int rbx_engine_kspace_energy_exact(rbx_engine* e, const int kmax[3], double* energy) {
+  if (!e) return RBX_ERR_INVALID;
+  return e->kspace_energy_exact(kmax, energy);
 }
 
 int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core, int* shell_pairs,

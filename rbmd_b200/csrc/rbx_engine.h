@@ -227,6 +227,7 @@ struct rbx_engine {
                 double* fx, double* fy, double* fz);
   int get_force_parts(double* f_pair, double* f_kspace);
   int pair_energy(double* e_vdwl, double* e_coul, double* virial);
+  int kspace_energy_exact(const int kmax[3], double* energy);
   int get_rbl_pairs(int* core_pairs, int64_t* n_core, int* shell_pairs, int64_t* n_shell);
   int get_stats(rbx_stats* s);
   int set_images(const int* image);

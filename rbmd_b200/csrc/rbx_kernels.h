@@ -168,6 +168,33 @@ int launch_ref_pair_verlet(const DBox& b, double cut_off, int n, double alpha, d
                            const double* x, const double* y, const double* z, double* fx,
                            double* fy, double* fz, double* flat_virial, double* epart,
                            cudaStream_t st);
+// FP32 overloads of the drop-in ops (the reference's default build,
+// rbmd::Real = float): membership tests in float as that build evaluates
+// them, force values computed in FP64 and stored in float.
+int launch_ref_rbl_filter(float core2, float force2, int n, const int* gid, const float* x,
+                          const float* y, const float* z, const int* cstart, const int* cend,
+                          const int* cand, const int* core_cap, const int* core_start,
+                          int* core_end, int* core, int shell_cap, int* shell, int* shell_num,
+                          int* required, const DBox& b, int* realloc, const DivTest& div,
+                          int epoch, cudaStream_t st);
+int launch_ref_pair_rbl(const DBox& b, float rs, float rc, int n, int pice_num, double alpha,
+                        double qqr2e, const int* type, const float* sigma, const float* eps,
+                        const int* start, const int* end, const int* core, const int* shell,
+                        const int* shell_num, const float* q, const float* x, const float* y,
+                        const float* z, float* fx, float* fy, float* fz, cudaStream_t st);
+int launch_ref_pair_verlet(const DBox& b, float cut_off, int n, double alpha, double qqr2e,
+                           const int* type, const float* sigma, const float* eps,
+                           const int* start, const int* end, const int* nbrs, const float* q,
+                           const float* x, const float* y, const float* z, float* fx,
+                           float* fy, float* fz, float* flat_virial, double* epart,
+                           cudaStream_t st);
+int launch_reduce_cols(int n, int ncols, const float* cols, double* out, double scale,
+                       cudaStream_t st);
+int launch_sub_mean(int n, float* fx, float* fy, float* fz, const double* mean,
+                    cudaStream_t st);
+// Element-wise conversions between float and double device arrays.
+int launch_widen(int n, const float* src, double* dst, cudaStream_t st);
+int launch_narrow(int n, const double* src, float* dst, cudaStream_t st);
 int launch_sum_i32(int n, const int* src, long long* out, cudaStream_t st);
 int launch_reduce_cols(int n, int ncols, const double* cols, double* out, double scale,
                        cudaStream_t st);

@@ -602,25 +602,62 @@ __global__ void k_rbl_keys(int n, const int* __restrict__ gid, unsigned long lon
 // ---------------------------------------------------------------------------
 // Drop-in ops with the reference data layouts.
 // ---------------------------------------------------------------------------
+// The drop-in ops take the reference's rbmd::Real (T): double under
+// ENABLE_DOUBLE, float in the default build.  Every membership test (list
+// predicates, force windows) is evaluated in T with the reference's own
+// expression, so a pair is kept or dropped exactly as the reference build of
+// the same precision keeps or drops it; force values are then computed in
+// FP64 from the T inputs.
+//
+// Single-shift minimum image of MinImageDistance (box.h:51-73): the half-edge
+// test compares against box._length * 0.5, which C++ evaluates in double.
+template <typename T>
+__device__ __forceinline__ T ref_min_image(T d, T len) {
+  if (fabs((double)d) > (double)len * 0.5) d -= (d > 0 ? len : -len);
+  return d;
+}
+// CaculateDistance (full_neighbor_list_op.h:98-106): i minus j, the squares
+// by POW and summed left to right.  In double POW(d, 2) is the product d * d.
+__device__ __forceinline__ double ref_list_d2(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+__device__ __forceinline__ float ref_list_d2(float dx, float dy, float dz) {
+  return __fadd_rn(__fadd_rn(powf(dx, 2.f), powf(dy, 2.f)), powf(dz, 2.f));
+}
+template <typename T>
+struct RefLen {
+  T len[3];
+};
+template <typename T>
+RefLen<T> ref_len(const DBox& b) {
+  RefLen<T> r;
+  for (int d = 0; d < 3; ++d) r.len[d] = (T)b.len[d];
+  return r;
+}
+
 // FilterRBLNeighborCandidates semantics (rbl_full_neighbor_list_op.hip.cu:237-304).
-__global__ void k_ref_rbl_filter(double core2, double force2, int n, const int* __restrict__ gid,
-                                 const double* __restrict__ x, const double* __restrict__ y,
-                                 const double* __restrict__ z, const int* __restrict__ cstart,
+template <typename T>
+__global__ void k_ref_rbl_filter(T core2, T force2, int n, const int* __restrict__ gid,
+                                 const T* __restrict__ x, const T* __restrict__ y,
+                                 const T* __restrict__ z, const int* __restrict__ cstart,
                                  const int* __restrict__ cend, const int* __restrict__ cand,
                                  const int* __restrict__ core_cap,
                                  const int* __restrict__ core_start, int* __restrict__ core_end,
                                  int* __restrict__ core, int shell_cap, int* __restrict__ shell,
                                  int* __restrict__ shell_num, int* __restrict__ required,
-                                 DBox b, int* __restrict__ realloc, DivTest div, int epoch) {
+                                 RefLen<T> b, int* __restrict__ realloc, DivTest div, int epoch) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const unsigned long long ea = rbl_key_a(gid[i]) ^ (unsigned long long)(long long)epoch;
   int nc = 0, ns = 0;
   const int out0 = core_start[i], ccap = core_cap[i];
+  const T xi = x[i], yi = y[i], zi = z[i];
   for (int pos = cstart[i]; pos < cend[i]; ++pos) {
     const int j = cand[pos];
     if (j == i) continue;
-    const double d2 = dist2_list(b, x[i], y[i], z[i], x[j], y[j], z[j]);
+    const T d2 = ref_list_d2(ref_min_image<T>(xi - x[j], b.len[0]),
+                             ref_min_image<T>(yi - y[j], b.len[1]),
+                             ref_min_image<T>(zi - z[j], b.len[2]));
     if (d2 < core2) {
       if (nc < ccap)
         core[out0 + nc] = j;
@@ -637,34 +674,51 @@ __global__ void k_ref_rbl_filter(double core2, double force2, int n, const int* 
   atomicMax(required, ns);
 }
 
+// Pair vector r_j - r_i in T with the minimum image, and its r^2 as the
+// reference's force helpers form it (lj_op.hip.cu:40-54).
+template <typename T>
+struct RefPair {
+  T dx, dy, dz, d2;
+};
+template <typename T>
+__device__ __forceinline__ RefPair<T> ref_pair(const RefLen<T>& b, T xi, T yi, T zi, T xj, T yj,
+                                               T zj) {
+  RefPair<T> p;
+  p.dx = ref_min_image<T>(xj - xi, b.len[0]);
+  p.dy = ref_min_image<T>(yj - yi, b.len[1]);
+  p.dz = ref_min_image<T>(zj - zi, b.len[2]);
+  p.d2 = p.dx * p.dx + p.dy * p.dy + p.dz * p.dz;
+  return p;
+}
+
 // LJCutCoulRBLForce semantics, warp per atom over core CSR + sample-major shell.
+template <typename T>
 __global__ void __launch_bounds__(PAIR_BLOCK)
-k_ref_pair_rbl(DBox b, double rs2, double rc2, int n, int pice, double alpha, double sqa,
-               double qqr2e, const int* __restrict__ type, const double* __restrict__ sigma,
-               const double* __restrict__ eps, const int* __restrict__ start,
+k_ref_pair_rbl(RefLen<T> b, T rs, T rc, int n, int pice, double alpha, double sqa, double qqr2e,
+               const int* __restrict__ type, const T* __restrict__ sigma,
+               const T* __restrict__ eps, const int* __restrict__ start,
                const int* __restrict__ end, const int* __restrict__ core,
                const int* __restrict__ shell, const int* __restrict__ shell_num,
-               const double* __restrict__ q, const double* __restrict__ x,
-               const double* __restrict__ y, const double* __restrict__ z,
-               double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+               const T* __restrict__ q, const T* __restrict__ x, const T* __restrict__ y,
+               const T* __restrict__ z, T* __restrict__ fx, T* __restrict__ fy,
+               T* __restrict__ fz) {
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
   if (i >= n) return;
+  const T rs2 = rs * rs, rc2 = rc * rc, eps_t = (T)RBX_EPSILON;
   const int ti = type[i];
-  const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
-  const double si = sigma[ti], ei = eps[ti];
+  const T xi = x[i], yi = y[i], zi = z[i];
+  const double qi = q[i], si = sigma[ti], ei = eps[ti];
   double s[3] = {0, 0, 0}, c[3] = {0, 0, 0};
   const int a = start[i], e = end[i], ns = shell_num[i];
   for (int t = a + lane; t < e; t += 32) {
     const int j = core[t];
-    const double dx = min_image1(x[j] - xi, b.len[0], b.half[0]);
-    const double dy = min_image1(y[j] - yi, b.len[1], b.half[1]);
-    const double dz = min_image1(z[j] - zi, b.len[2], b.half[2]);
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    if (d2 < rs2 && d2 > RBX_EPSILON) {
-      const double sij = (si + sigma[type[j]]) / 2, eij = sqrt(ei * eps[type[j]]);
+    const RefPair<T> p = ref_pair<T>(b, xi, yi, zi, x[j], y[j], z[j]);
+    if (p.d2 < rs2 && p.d2 > eps_t) {
+      const double dx = p.dx, dy = p.dy, dz = p.dz, d2 = dx * dx + dy * dy + dz * dz;
+      const double sij = (si + (double)sigma[type[j]]) / 2, eij = sqrt(ei * (double)eps[type[j]]);
       double f = lj_f64(eij, pow(sij, 6.0), d2);
-      const double qq = qi * q[j];
+      const double qq = qi * (double)q[j];
       if (qq != 0.0) f += coul_f64(alpha, sqa, qqr2e, qq, d2);
       s[0] += f * dx;
       s[1] += f * dy;
@@ -673,14 +727,12 @@ k_ref_pair_rbl(DBox b, double rs2, double rc2, int n, int pice, double alpha, do
   }
   for (int t = lane; t < ns; t += 32) {
     const int j = shell[(size_t)t * n + i];
-    const double dx = min_image1(x[j] - xi, b.len[0], b.half[0]);
-    const double dy = min_image1(y[j] - yi, b.len[1], b.half[1]);
-    const double dz = min_image1(z[j] - zi, b.len[2], b.half[2]);
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    if (d2 < rc2 && d2 > rs2) {
-      const double sij = (si + sigma[type[j]]) / 2, eij = sqrt(ei * eps[type[j]]);
+    const RefPair<T> p = ref_pair<T>(b, xi, yi, zi, x[j], y[j], z[j]);
+    if (p.d2 < rc2 && p.d2 > rs2) {
+      const double dx = p.dx, dy = p.dy, dz = p.dz, d2 = dx * dx + dy * dy + dz * dz;
+      const double sij = (si + (double)sigma[type[j]]) / 2, eij = sqrt(ei * (double)eps[type[j]]);
       double f = lj_f64(eij, pow(sij, 6.0), d2);
-      const double qq = qi * q[j];
+      const double qq = qi * (double)q[j];
       if (qq != 0.0) f += coul_f64(alpha, sqa, qqr2e, qq, d2);
       f *= (double)pice;
       c[0] += f * dx;
@@ -693,41 +745,42 @@ k_ref_pair_rbl(DBox b, double rs2, double rc2, int n, int pice, double alpha, do
     c[d] = warp_sum(c[d]);
   }
   if (lane == 0) {
-    fx[i] = s[0] + c[0];
-    fy[i] = s[1] + c[1];
-    fz[i] = s[2] + c[2];
+    fx[i] = (T)(s[0] + c[0]);
+    fy[i] = (T)(s[1] + c[1]);
+    fz[i] = (T)(s[2] + c[2]);
   }
 }
 
 // LJCutCoulForce semantics (Verlet), warp per atom, per-atom virial columns
 // and per-atom energies epart[2*n] for a deterministic reduction.
+template <typename T>
 __global__ void __launch_bounds__(PAIR_BLOCK)
-k_ref_pair_verlet(DBox b, double cut2, int n, double alpha, double sqa, double qqr2e,
-                  const int* __restrict__ type, const double* __restrict__ sigma,
-                  const double* __restrict__ eps, const int* __restrict__ start,
+k_ref_pair_verlet(RefLen<T> b, T cut_off, int n, double alpha, double sqa, double qqr2e,
+                  const int* __restrict__ type, const T* __restrict__ sigma,
+                  const T* __restrict__ eps, const int* __restrict__ start,
                   const int* __restrict__ end, const int* __restrict__ nbrs,
-                  const double* __restrict__ q, const double* __restrict__ x,
-                  const double* __restrict__ y, const double* __restrict__ z,
-                  double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-                  double* __restrict__ vir, double* __restrict__ epart) {
+                  const T* __restrict__ q, const T* __restrict__ x, const T* __restrict__ y,
+                  const T* __restrict__ z, T* __restrict__ fx, T* __restrict__ fy,
+                  T* __restrict__ fz, T* __restrict__ vir, double* __restrict__ epart) {
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
   if (i >= n) return;
+  const T cut2 = cut_off * cut_off;
   const int ti = type[i];
-  const double xi = x[i], yi = y[i], zi = z[i], qi = q[i];
+  const T xi = x[i], yi = y[i], zi = z[i];
+  const double qi = q[i];
   double a[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int t = start[i] + lane; t < end[i]; t += 32) {
     const int j = nbrs[t];
-    const double dx = min_image1(x[j] - xi, b.len[0], b.half[0]);
-    const double dy = min_image1(y[j] - yi, b.len[1], b.half[1]);
-    const double dz = min_image1(z[j] - zi, b.len[2], b.half[2]);
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    if (!(d2 < cut2)) continue;
-    const double sij = (sigma[ti] + sigma[type[j]]) / 2, eij = sqrt(eps[ti] * eps[type[j]]);
+    const RefPair<T> p = ref_pair<T>(b, xi, yi, zi, x[j], y[j], z[j]);
+    if (!(p.d2 < cut2)) continue;
+    const double dx = p.dx, dy = p.dy, dz = p.dz, d2 = dx * dx + dy * dy + dz * dz;
+    const double sij = ((double)sigma[ti] + (double)sigma[type[j]]) / 2,
+                 eij = sqrt((double)eps[ti] * (double)eps[type[j]]);
     const double s6 = pow(sij, 6.0), d6 = d2 * d2 * d2, sd6 = s6 / d6;
     double f = -24 * eij * ((2 * sd6 - 1) * sd6) / d2;
     a[3] += 0.5 * (4 * eij * (s6 / d6 - 1) * sd6);
-    const double qq = qi * q[j];
+    const double qq = qi * (double)q[j];
     if (qq != 0.0) {
       const double dis = sqrt(d2), ec = erfc(sqa * dis);
       f += -qqr2e * qq * (ec / d2 + 2 * sqa * exp(-alpha * d2) / (1.7724538509055160273 * dis)) / dis;
@@ -745,24 +798,25 @@ k_ref_pair_verlet(DBox b, double cut2, int n, double alpha, double sqa, double q
   }
   for (int c = 0; c < 11; ++c) a[c] = warp_sum(a[c]);
   if (lane == 0) {
-    fx[i] = a[0];
-    fy[i] = a[1];
-    fz[i] = a[2];
+    fx[i] = (T)a[0];
+    fy[i] = (T)a[1];
+    fz[i] = (T)a[2];
     if (epart) {
       epart[i] = a[3];
       epart[(size_t)n + i] = a[4];
     }
     if (vir)
-      for (int c = 0; c < 6; ++c) vir[(size_t)c * n + i] = a[5 + c];
+      for (int c = 0; c < 6; ++c) vir[(size_t)c * n + i] = (T)a[5 + c];
   }
 }
 
 // Deterministic column sums: out[c] = scale * sum_i cols[c*n + i] (one block per column).
-__global__ void k_reduce_cols(int n, const double* __restrict__ cols, double* __restrict__ out,
+template <typename T>
+__global__ void k_reduce_cols(int n, const T* __restrict__ cols, double* __restrict__ out,
                               double scale) {
   __shared__ double sh[8];
   double s = 0.0;
-  const double* col = cols + (size_t)blockIdx.x * n;
+  const T* col = cols + (size_t)blockIdx.x * n;
   for (int i = threadIdx.x; i < n; i += 256) s += col[i];
   s = block_sum_det<256>(s, sh);
   if (threadIdx.x == 0) out[blockIdx.x] = s * scale;
@@ -777,13 +831,14 @@ __global__ void k_sum_i32(int n, const int* __restrict__ src, long long* __restr
   if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long*)out, (unsigned long long)s);
 }
 
-__global__ void k_sub_mean(int n, double* __restrict__ fx, double* __restrict__ fy,
-                           double* __restrict__ fz, const double* __restrict__ mean) {
+template <typename T>
+__global__ void k_sub_mean(int n, T* __restrict__ fx, T* __restrict__ fy, T* __restrict__ fz,
+                           const double* __restrict__ mean) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  fx[i] -= mean[0];
-  fy[i] -= mean[1];
-  fz[i] -= mean[2];
+  fx[i] = (T)((double)fx[i] - mean[0]);
+  fy[i] = (T)((double)fy[i] - mean[1]);
+  fz[i] = (T)((double)fz[i] - mean[2]);
 }
 
 // ---------------------------------------------------------------------------
@@ -902,56 +957,123 @@ int launch_rbl_keys(int n, const int* gid, unsigned long long* key_a, unsigned l
   return check_launch("rbl_keys");
 }
 
+template <typename T>
+int launch_ref_rbl_filter_t(T core2, T force2, int n, const int* gid, const T* x, const T* y,
+                            const T* z, const int* cstart, const int* cend, const int* cand,
+                            const int* core_cap, const int* core_start, int* core_end, int* core,
+                            int shell_cap, int* shell, int* shell_num, int* required,
+                            const DBox& b, int* realloc, const DivTest& div, int epoch,
+                            cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_ref_rbl_filter<T><<<(n + 127) / 128, 128, 0, st>>>(
+      core2, force2, n, gid, x, y, z, cstart, cend, cand, core_cap, core_start, core_end, core,
+      shell_cap, shell, shell_num, required, ref_len<T>(b), realloc, div, epoch);
+  count_launch();
+  return check_launch("ref_rbl_filter");
+}
 int launch_ref_rbl_filter(double core2, double force2, int n, const int* gid, const double* x,
                           const double* y, const double* z, const int* cstart, const int* cend,
                           const int* cand, const int* core_cap, const int* core_start,
                           int* core_end, int* core, int shell_cap, int* shell, int* shell_num,
                           int* required, const DBox& b, int* realloc, const DivTest& div,
                           int epoch, cudaStream_t st) {
-  if (n <= 0) return RBX_OK;
-  k_ref_rbl_filter<<<(n + 127) / 128, 128, 0, st>>>(core2, force2, n, gid, x, y, z, cstart, cend,
-                                                    cand, core_cap, core_start, core_end, core,
-                                                    shell_cap, shell, shell_num, required, b,
-                                                    realloc, div, epoch);
-  count_launch();
-  return check_launch("ref_rbl_filter");
+  return launch_ref_rbl_filter_t<double>(core2, force2, n, gid, x, y, z, cstart, cend, cand,
+                                         core_cap, core_start, core_end, core, shell_cap, shell,
+                                         shell_num, required, b, realloc, div, epoch, st);
+}
+int launch_ref_rbl_filter(float core2, float force2, int n, const int* gid, const float* x,
+                          const float* y, const float* z, const int* cstart, const int* cend,
+                          const int* cand, const int* core_cap, const int* core_start,
+                          int* core_end, int* core, int shell_cap, int* shell, int* shell_num,
+                          int* required, const DBox& b, int* realloc, const DivTest& div,
+                          int epoch, cudaStream_t st) {
+  return launch_ref_rbl_filter_t<float>(core2, force2, n, gid, x, y, z, cstart, cend, cand,
+                                        core_cap, core_start, core_end, core, shell_cap, shell,
+                                        shell_num, required, b, realloc, div, epoch, st);
 }
 
+template <typename T>
+int launch_ref_pair_rbl_t(const DBox& b, T rs, T rc, int n, int pice_num, double alpha,
+                          double qqr2e, const int* type, const T* sigma, const T* eps,
+                          const int* start, const int* end, const int* core, const int* shell,
+                          const int* shell_num, const T* q, const T* x, const T* y, const T* z,
+                          T* fx, T* fy, T* fz, cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_ref_pair_rbl<T><<<(n + PAIR_WARPS - 1) / PAIR_WARPS, PAIR_BLOCK, 0, st>>>(
+      ref_len<T>(b), rs, rc, n, pice_num, alpha, sqrt(alpha), qqr2e, type, sigma, eps, start,
+      end, core, shell, shell_num, q, x, y, z, fx, fy, fz);
+  count_launch();
+  return check_launch("ref_pair_rbl");
+}
 int launch_ref_pair_rbl(const DBox& b, double rs, double rc, int n, int pice_num, double alpha,
                         double qqr2e, const int* type, const double* sigma, const double* eps,
                         const int* start, const int* end, const int* core, const int* shell,
                         const int* shell_num, const double* q, const double* x, const double* y,
                         const double* z, double* fx, double* fy, double* fz, cudaStream_t st) {
-  if (n <= 0) return RBX_OK;
-  k_ref_pair_rbl<<<(n + PAIR_WARPS - 1) / PAIR_WARPS, PAIR_BLOCK, 0, st>>>(
-      b, rs * rs, rc * rc, n, pice_num, alpha, sqrt(alpha), qqr2e, type, sigma, eps, start, end,
-      core, shell, shell_num, q, x, y, z, fx, fy, fz);
-  count_launch();
-  return check_launch("ref_pair_rbl");
+  return launch_ref_pair_rbl_t<double>(b, rs, rc, n, pice_num, alpha, qqr2e, type, sigma, eps,
+                                       start, end, core, shell, shell_num, q, x, y, z, fx, fy, fz,
+                                       st);
+}
+int launch_ref_pair_rbl(const DBox& b, float rs, float rc, int n, int pice_num, double alpha,
+                        double qqr2e, const int* type, const float* sigma, const float* eps,
+                        const int* start, const int* end, const int* core, const int* shell,
+                        const int* shell_num, const float* q, const float* x, const float* y,
+                        const float* z, float* fx, float* fy, float* fz, cudaStream_t st) {
+  return launch_ref_pair_rbl_t<float>(b, rs, rc, n, pice_num, alpha, qqr2e, type, sigma, eps,
+                                      start, end, core, shell, shell_num, q, x, y, z, fx, fy, fz,
+                                      st);
 }
 
+template <typename T>
+int launch_ref_pair_verlet_t(const DBox& b, T cut_off, int n, double alpha, double qqr2e,
+                             const int* type, const T* sigma, const T* eps, const int* start,
+                             const int* end, const int* nbrs, const T* q, const T* x, const T* y,
+                             const T* z, T* fx, T* fy, T* fz, T* flat_virial, double* epart,
+                             cudaStream_t st) {
+  if (n <= 0) return RBX_OK;
+  k_ref_pair_verlet<T><<<(n + PAIR_WARPS - 1) / PAIR_WARPS, PAIR_BLOCK, 0, st>>>(
+      ref_len<T>(b), cut_off, n, alpha, sqrt(alpha), qqr2e, type, sigma, eps, start, end, nbrs,
+      q, x, y, z, fx, fy, fz, flat_virial, epart);
+  count_launch();
+  return check_launch("ref_pair_verlet");
+}
 int launch_ref_pair_verlet(const DBox& b, double cut_off, int n, double alpha, double qqr2e,
                            const int* type, const double* sigma, const double* eps,
                            const int* start, const int* end, const int* nbrs, const double* q,
                            const double* x, const double* y, const double* z, double* fx,
                            double* fy, double* fz, double* flat_virial, double* epart,
                            cudaStream_t st) {
-  if (n <= 0) return RBX_OK;
-  k_ref_pair_verlet<<<(n + PAIR_WARPS - 1) / PAIR_WARPS, PAIR_BLOCK, 0, st>>>(
-      b, cut_off * cut_off, n, alpha, sqrt(alpha), qqr2e, type, sigma, eps, start, end, nbrs, q,
-      x, y, z, fx, fy, fz, flat_virial, epart);
-  count_launch();
-  return check_launch("ref_pair_verlet");
+  return launch_ref_pair_verlet_t<double>(b, cut_off, n, alpha, qqr2e, type, sigma, eps, start,
+                                          end, nbrs, q, x, y, z, fx, fy, fz, flat_virial, epart,
+                                          st);
+}
+int launch_ref_pair_verlet(const DBox& b, float cut_off, int n, double alpha, double qqr2e,
+                           const int* type, const float* sigma, const float* eps,
+                           const int* start, const int* end, const int* nbrs, const float* q,
+                           const float* x, const float* y, const float* z, float* fx,
+                           float* fy, float* fz, float* flat_virial, double* epart,
+                           cudaStream_t st) {
+  return launch_ref_pair_verlet_t<float>(b, cut_off, n, alpha, qqr2e, type, sigma, eps, start,
+                                         end, nbrs, q, x, y, z, fx, fy, fz, flat_virial, epart,
+                                         st);
 }
 
-int launch_reduce_cols(int n, int ncols, const double* cols, double* out, double scale,
-                       cudaStream_t st) {
+template <typename T>
+int launch_reduce_cols_t(int n, int ncols, const T* cols, double* out, double scale,
+                         cudaStream_t st) {
   if (ncols <= 0) return RBX_OK;
-  k_reduce_cols<<<ncols, 256, 0, st>>>(n, cols, out, scale);
+  k_reduce_cols<T><<<ncols, 256, 0, st>>>(n, cols, out, scale);
   count_launch();
   return check_launch("reduce_cols");
 }
-
+int launch_reduce_cols(int n, int ncols, const double* cols, double* out, double scale,
+                       cudaStream_t st) {
+  return launch_reduce_cols_t<double>(n, ncols, cols, out, scale, st);
+}
+int launch_reduce_cols(int n, int ncols, const float* cols, double* out, double scale,
+                       cudaStream_t st) {
+  return launch_reduce_cols_t<float>(n, ncols, cols, out, scale, st);
+}
 int launch_sum_i32(int n, const int* src, long long* out, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
   k_sum_i32<<<grid_for(n, 256, sm_count() * 4), 256, 0, st>>>(n, src, out);
@@ -959,12 +1081,20 @@ int launch_sum_i32(int n, const int* src, long long* out, cudaStream_t st) {
   return check_launch("sum_i32");
 }
 
-int launch_sub_mean(int n, double* fx, double* fy, double* fz, const double* mean,
-                    cudaStream_t st) {
+template <typename T>
+int launch_sub_mean_t(int n, T* fx, T* fy, T* fz, const double* mean, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  k_sub_mean<<<(n + 255) / 256, 256, 0, st>>>(n, fx, fy, fz, mean);
+  k_sub_mean<T><<<(n + 255) / 256, 256, 0, st>>>(n, fx, fy, fz, mean);
   count_launch();
   return check_launch("sub_mean");
+}
+int launch_sub_mean(int n, double* fx, double* fy, double* fz, const double* mean,
+                    cudaStream_t st) {
+  return launch_sub_mean_t<double>(n, fx, fy, fz, mean, st);
+}
+int launch_sub_mean(int n, float* fx, float* fy, float* fz, const double* mean,
+                    cudaStream_t st) {
+  return launch_sub_mean_t<float>(n, fx, fy, fz, mean, st);
 }
 
 }  // namespace rbx

@@ -108,6 +108,10 @@ EXPORTS = [
     "rbx_engine_set_shake", "rbx_engine_get_shake", "rbx_engine_set_special", "rbx_special_build",
     "rbx_rbsog_params", "rbx_rbsog_sample", "rbx_rbsog_force", "rbx_pair_force_verlet_sog",
     "rbx_engine_autotune", "rbx_batch_autotune",
+    "rbx_rbe_structure_factor_f32", "rbx_rbe_force_f32", "rbx_rbe_energy_virial_f32",
+    "rbx_rbl_filter_f32", "rbx_pair_force_rbl_f32", "rbx_fix_rbl_force_f32",
+    "rbx_pair_force_verlet_f32", "rbx_engine_kspace_energy_exact", "rbx_force_create_json",
+    "rbx_force_destroy", "rbx_force_engine", "rbx_force_execute", "rbx_force_energies",
 ]
 
 
@@ -229,6 +233,24 @@ def lib():
     L.rbx_batch_stream.argtypes = [vp]
     L.rbx_nlist_should_reuse.argtypes = [B, ip] + [vp] * 6 + [dp, C.POINTER(C.c_int),
                                                              C.POINTER(C.c_double), vp]
+    L.rbx_engine_kspace_energy_exact.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.rbx_force_create_json.restype = vp
+    L.rbx_force_create_json.argtypes = [C.c_char_p, B, ip, ip, vp, vp, vp, vp, ip, ip]
+    L.rbx_force_destroy.restype = None
+    L.rbx_force_destroy.argtypes = [vp]
+    L.rbx_force_engine.restype = vp
+    L.rbx_force_engine.argtypes = [vp]
+    L.rbx_force_execute.argtypes = [vp, ip, ip]
+    L.rbx_force_energies.argtypes = [vp, C.POINTER(C.c_double)]
+    fp = C.c_float  # FP32 twins: float scalars
+    L.rbx_rbe_structure_factor_f32.argtypes = [B, ip, ip] + [vp] * 9 + [vp]
+    L.rbx_rbe_force_f32.argtypes = [B, ip, ip, fp, fp, fp] + [vp] * 12 + [vp]
+    L.rbx_rbe_energy_virial_f32.argtypes = [B, ip, fp, fp, fp, fp, fp] + [vp] * 7 + [vp]
+    L.rbx_rbl_filter_f32.argtypes = ([fp, fp, ip] + [vp] * 11 + [ip] + [vp] * 3 +
+                                     [B, vp, ip, ip, vp])
+    L.rbx_pair_force_rbl_f32.argtypes = [B, fp, fp, ip, ip, ip, fp, fp] + [vp] * 14 + [vp]
+    L.rbx_fix_rbl_force_f32.argtypes = [ip, vp, vp, vp, vp, vp]
+    L.rbx_pair_force_verlet_f32.argtypes = [B, fp, ip, fp, fp] + [vp] * 15 + [vp]
     _lib = L
     return L
 
@@ -387,6 +409,65 @@ def pair_force_verlet(box, cut_off, alpha, qqr2e, typ, sigma, eps, start, end, n
                                       _stream(stream)), "rbx_pair_force_verlet")
 
 
+# FP32 twins (the reference's default float build): float tensors and scalars,
+# same argument order as the FP64 wrappers above.
+def rbe_structure_factor_f32(box, q, mx, my, mz, x, y, z, re, im, stream=None):
+    check(lib().rbx_rbe_structure_factor_f32(C.byref(box), q.numel(), mx.numel(), _ptr(q),
+                                             _ptr(mx), _ptr(my), _ptr(mz), _ptr(x), _ptr(y),
+                                             _ptr(z), _ptr(re), _ptr(im), _stream(stream)),
+          "rbx_rbe_structure_factor_f32")
+
+
+def rbe_force_f32(box, alpha, S, qqr2e, re, im, q, mx, my, mz, x, y, z, fx, fy, fz, stream=None):
+    check(lib().rbx_rbe_force_f32(C.byref(box), q.numel(), mx.numel(), alpha, S, qqr2e,
+                                  _ptr(re), _ptr(im), _ptr(q), _ptr(mx), _ptr(my), _ptr(mz),
+                                  _ptr(x), _ptr(y), _ptr(z), _ptr(fx), _ptr(fy), _ptr(fz),
+                                  _stream(stream)), "rbx_rbe_force_f32")
+
+
+def rbe_energy_virial_f32(box, alpha, S, qqr2e, qsq, qsum, re, im, mx, my, mz, virial, energy,
+                          stream=None):
+    check(lib().rbx_rbe_energy_virial_f32(C.byref(box), mx.numel(), alpha, S, qqr2e, qsq, qsum,
+                                          _ptr(re), _ptr(im), _ptr(mx), _ptr(my), _ptr(mz),
+                                          _ptr(virial), _ptr(energy), _stream(stream)),
+          "rbx_rbe_energy_virial_f32")
+
+
+def rbl_filter_f32(core2, force2, gid, x, y, z, cstart, cend, cand, core_cap, core_start,
+                   core_end, core, shell_cap, shell, shell_num, required, box, realloc, freq,
+                   epoch, stream=None):
+    check(lib().rbx_rbl_filter_f32(core2, force2, gid.numel(), _ptr(gid), _ptr(x), _ptr(y),
+                                   _ptr(z), _ptr(cstart), _ptr(cend), _ptr(cand), _ptr(core_cap),
+                                   _ptr(core_start), _ptr(core_end), _ptr(core), shell_cap,
+                                   _ptr(shell), _ptr(shell_num), _ptr(required), C.byref(box),
+                                   _ptr(realloc), freq, epoch, _stream(stream)),
+          "rbx_rbl_filter_f32")
+
+
+def pair_force_rbl_f32(box, rs, rc, sample_num, pice, alpha, qqr2e, typ, sigma, eps, start, end,
+                       core, shell, shell_num, q, x, y, z, fx, fy, fz, stream=None):
+    check(lib().rbx_pair_force_rbl_f32(C.byref(box), rs, rc, q.numel(), sample_num, pice, alpha,
+                                       qqr2e, _ptr(typ), _ptr(sigma), _ptr(eps), _ptr(start),
+                                       _ptr(end), _ptr(core), _ptr(shell), _ptr(shell_num),
+                                       _ptr(q), _ptr(x), _ptr(y), _ptr(z), _ptr(fx), _ptr(fy),
+                                       _ptr(fz), _stream(stream)), "rbx_pair_force_rbl_f32")
+
+
+def fix_rbl_force_f32(fx, fy, fz, mean=None, stream=None):
+    check(lib().rbx_fix_rbl_force_f32(fx.numel(), _ptr(fx), _ptr(fy), _ptr(fz), _ptr(mean),
+                                      _stream(stream)), "rbx_fix_rbl_force_f32")
+
+
+def pair_force_verlet_f32(box, cut_off, alpha, qqr2e, typ, sigma, eps, start, end, nbrs, q, x, y,
+                          z, fx, fy, fz, flat_virial, evdwl, ecoul, stream=None):
+    check(lib().rbx_pair_force_verlet_f32(C.byref(box), cut_off, q.numel(), alpha, qqr2e,
+                                          _ptr(typ), _ptr(sigma), _ptr(eps), _ptr(start),
+                                          _ptr(end), _ptr(nbrs), _ptr(q), _ptr(x), _ptr(y),
+                                          _ptr(z), _ptr(fx), _ptr(fy), _ptr(fz),
+                                          _ptr(flat_virial), _ptr(evdwl), _ptr(ecoul),
+                                          _stream(stream)), "rbx_pair_force_verlet_f32")
+
+
 # ---------------------------------------------------------------------------
 # engine
 # ---------------------------------------------------------------------------
@@ -532,6 +613,14 @@ class Engine:
               "rbx_engine_pair_energy")
         return ev[0], ec[0], vir
 
+    def kspace_energy_exact(self, kmax):
+        """Exact Ewald reciprocal energy over kmax plus the self energy."""
+        km = (C.c_int * 3)(*[int(k) for k in kmax])
+        out = C.c_double(0.0)
+        check(lib().rbx_engine_kspace_energy_exact(self._h, km, C.byref(out)),
+              "rbx_engine_kspace_energy_exact")
+        return out.value
+
     def rbl_pairs(self):
         nc, ns = C.c_int64(0), C.c_int64(0)
         check(lib().rbx_engine_get_rbl_pairs(self._h, None, C.byref(nc), None, C.byref(ns)),
@@ -656,6 +745,53 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+class Force(Engine):
+    """The LJCutCoulKspace plugin behind RBMD's Force interface
+    (rbx_force_*): built from the JSON config, Execute + EvaluatePotentialEnergy
+    per call, energies as RBMD reports them.  The engine methods act on the
+    engine the plugin drives."""
+
+    def __init__(self, sys, json_text, *, precision=PLAIN_FP64, device=0):
+        L = lib()
+        self.n = int(sys["n"])
+        self.box = Box.make(sys["lo"], sys["hi"])
+        self._sigma = np.ascontiguousarray(sys["sigma"], dtype=np.float64)
+        self._eps = np.ascontiguousarray(sys["eps"], dtype=np.float64)
+        self._mass = np.ascontiguousarray(sys["mass"], dtype=np.float64)
+        q = np.ascontiguousarray(sys["q"], dtype=np.float64)
+        f = L.rbx_force_create_json(json_text.encode(), C.byref(self.box), self.n,
+                                    len(self._sigma), _np_ptr(self._sigma), _np_ptr(self._eps),
+                                    _np_ptr(self._mass), _np_ptr(q), precision, device)
+        if not f:
+            raise RbxError(f"rbx_force_create_json failed: {last_error()}")
+        self._f = C.c_void_p(f)
+        self._h = C.c_void_p(L.rbx_force_engine(self._f))
+        pos = np.ascontiguousarray(sys["pos"], dtype=np.float64)
+        vel = np.ascontiguousarray(sys["vel"], dtype=np.float64)
+        cols = [np.ascontiguousarray(pos[:, d]) for d in range(3)] + \
+               [np.ascontiguousarray(vel[:, d]) for d in range(3)]
+        gid = np.ascontiguousarray(sys["gid"], dtype=np.int32)
+        typ = np.ascontiguousarray(sys["type"], dtype=np.int32)
+        self._gid, self._typ, self._q = gid, typ, q
+        check(L.rbx_engine_set_state(self._h, _np_ptr(gid), _np_ptr(typ), _np_ptr(q),
+                                     *[_np_ptr(c) for c in cols]), "rbx_engine_set_state")
+
+    def execute(self, epoch=0, thermo_step=True):
+        check(lib().rbx_force_execute(self._f, epoch, int(bool(thermo_step))), "rbx_force_execute")
+
+    def energies(self):
+        """{e_vdwl, e_coul, e_kspace, e_pe} of the last execute."""
+        out = (C.c_double * 4)()
+        check(lib().rbx_force_energies(self._f, out), "rbx_force_energies")
+        return dict(zip(("e_vdwl", "e_coul", "e_kspace", "e_pe"), list(out)))
+
+    def close(self):
+        if getattr(self, "_f", None):
+            lib().rbx_force_destroy(self._f)  # owns its engine
+            self._f = None
+            self._h = None
 
 
 class Batch:
