@@ -298,7 +298,8 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
   const float lo_i = live ? lo_band - uu : -INFINITY;
   const float hi_i = live ? hi_band - uu : -INFINITY;
   const bool split = far != nullptr;
-  const float near_i = near2 - uu;  // far pairs: d above this
+  // far pairs: d above this (never, without a split)
+  const float near_i = split && live ? near2 - uu : INFINITY;
   // box of the group's centre atoms relative to the cell centre, rounded outwards
   float glo[3], ghi[3];
   {
@@ -365,13 +366,14 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
         __syncwarp();  // the previous chunk's readers are done
         buf[warp][lane] = v;
         __syncwarp();
-        unsigned acc = 0, maybe = 0;
+        unsigned acc = 0, maybe = 0, farm = 0;  // farm: build distance certainly >= r_near
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
           const float4 q = buf[warp][t];  // broadcast
           const float d = fmaf(ax, q.x, fmaf(ay, q.y, fmaf(az, q.z, q.w)));
           acc |= d < lo_i ? 1u << t : 0u;
           maybe |= d < hi_i ? 1u << t : 0u;
+          farm |= d > near_i ? 1u << t : 0u;
         }
         if (nc == c && k == g) {  // the centre atom itself
           acc &= ~(1u << lane);
@@ -389,18 +391,10 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
         while (acc) {  // hits in cell order, each lane into its own row
           const int t = __ffs(acc) - 1;
           acc &= acc - 1;
-          bool to_back = false;
-          if (split) {  // build distance d + |u|^2 certainly at least r_near
-            const float4 q = buf[warp][t];
-            const float d = fmaf(ax, q.x, fmaf(ay, q.y, fmaf(az, q.z, q.w)));
-            to_back = d > near_i;
-          }
-          if (cnt < cap) {
-            if (to_back)
-              row[cap - 1 - nback++] = first + t;
-            else
-              row[cnt - nback] = first + t;
-          }
+          // one store to the front or the back of the row (no branch)
+          const bool to_back = (farm >> t) & 1u;
+          if (cnt < cap) row[to_back ? cap - 1 - nback : cnt - nback] = first + t;
+          nback += (cnt < cap) & to_back;
           ++cnt;
         }
       }
