@@ -192,14 +192,15 @@ int rbx_rbsog_force(const rbx_box* box, int level, double cut_off, double qqr2e,
  * ComputeLJCutCoulForceUserKernel with lj126 and CoulCutForceUser,
  * lj_cut_coul_kspace_op.hip.cu:196-254, 357-470): LJ 12-6 plus the
  * short-range SOG Coulomb inside cut_off.  sigma / eps per type (host);
- * energy (host, may be NULL) receives {E_LJ, E_coul}, half-counted.  The
- * per-atom virial is not computed. */
+ * energy (host, may be NULL) receives {E_LJ, E_coul}, half-counted;
+ * flat_virial (device, may be NULL) the per-atom virial flat_virial[c*n + i]
+ * (xx, yy, zz, xy, xz, yz) of ComputeVirial (lj_op.hip.cu:76-88). */
 int rbx_pair_force_verlet_sog(const rbx_box* box, int level, double cut_off, double qqr2e,
                               int num_atoms, int ntypes, const double* sigma, const double* eps,
                               const int* type, const double* charge, const double* px,
                               const double* py, const double* pz, int cap, const int* cand_count,
                               const int* cand, double* fx, double* fy, double* fz,
-                              double* energy, void* stream);
+                              double* energy, double* flat_virial, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Neighbor-list ops (device pointers)                                       */
@@ -381,6 +382,11 @@ int rbx_pair_force_verlet_f32(const rbx_box* box, float cut_off, int num_atoms, 
 
 typedef struct rbx_engine rbx_engine;
 
+/* Largest number of atom types an engine takes: the per-type-pair LJ tables
+ * (2 x ntypes^2 doubles, and floats in the mixed form) live in each pair
+ * kernel block's shared memory.  The force adjoint takes at most 16 types. */
+#define RBX_MAX_TYPES 64
+
 typedef enum { RBX_PLAIN_FP64 = 0, RBX_MIXED = 1 } rbx_precision;
 /* neighbor.type: "Verlet-List", "RBL", "VERLET-SOG" (Verlet list with the
  * short-range SOG Coulomb of RBSOG in place of erfc) */
@@ -411,7 +417,7 @@ typedef struct {
   double qqr2e;             /* from init_configuration.read_data.unit */
   double dt;                /* execution.timestep */
   int precision;            /* rbx_precision */
-  int ntypes;
+  int ntypes;               /* 1 .. RBX_MAX_TYPES */
   const double* sigma;      /* host, ntypes */
   const double* eps;        /* host, ntypes */
   const double* mass;       /* host, ntypes */

@@ -87,7 +87,7 @@ def lib():
                                               C.POINTER(C.c_double)]),
             "orc_pair_force_verlet_sog": (None, [C.c_int, C.c_double, B, C.c_double, C.c_int,
                                                  _ip, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int,
-                                                 _ip, _ip, _dp, _dp, _dp, _dp]),
+                                                 _ip, _ip, _dp, _dp, _dp, _dp, _dp]),
             "orc_dist2": (C.c_double, [B] + [C.c_double] * 6),
             "orc_cell_grid": (C.c_int, [B, C.c_double, _ip]),
             "orc_cells_sort": (C.c_int, [C.c_int, B, C.c_double, _dp, _dp, _dp, _ip, _ip,
@@ -288,14 +288,19 @@ def rbsog_far_exact(level, cut_off, box, qqr2e, q, x, y, z, mcut):
     return np.stack(f, axis=1), sf.value
 
 
-def pair_force_verlet_sog(level, cut_off, box, qqr2e, typ, sigma, eps, q, x, y, z, count, rows):
-    """LJCutCoulForceUserOp (lj_cut_coul_kspace_op.hip.cu:196-254, 357-470)."""
+def pair_force_verlet_sog(level, cut_off, box, qqr2e, typ, sigma, eps, q, x, y, z, count, rows,
+                          virial=False):
+    """LJCutCoulForceUserOp (lj_cut_coul_kspace_op.hip.cu:196-254, 357-470): forces,
+    {E_LJ, E_coul}, and with virial=True the per-atom virial [6][n] (xx, yy, zz, xy, xz, yz)."""
     n, cap = rows.shape
     f = [np.zeros(n) for _ in range(3)]
     en = np.zeros(2)
+    vir = np.zeros(6 * n)
     lib().orc_pair_force_verlet_sog(level, cut_off, C.byref(box), qqr2e, n, _i(typ), _d(sigma),
                                     _d(eps), _d(q), _d(x), _d(y), _d(z), cap, _i(count), _i(rows),
-                                    *f, en)
+                                    *f, en, vir)
+    if virial:
+        return np.stack(f, axis=1), en, vir.reshape(6, n)
     return np.stack(f, axis=1), en
 
 

@@ -1925,14 +1925,15 @@ void orc_pair_force_verlet_sog(int level, double cut_off, const orc_box* box, do
                                int n, const int* type, const double* sigma, const double* eps,
                                const double* q, const double* x, const double* y,
                                const double* z, int cap, const int* count, const int* cand,
-                               double* fx, double* fy, double* fz, double* energy) {
+                               double* fx, double* fy, double* fz, double* energy,
+                               double* flat_virial) {
   orc_sog s;
   if (sog_setup(level, cut_off, box, &s)) return;
   const double cut2 = cut_off * cut_off;
   double elj = 0.0, ecl = 0.0;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : elj, ecl)
   for (int i = 0; i < n; ++i) {
-    double f[3] = {0, 0, 0};
+    double f[3] = {0, 0, 0}, v[6] = {0, 0, 0, 0, 0, 0};
     for (int t = 0; t < count[i]; ++t) {
       const int j = cand[(size_t)i * cap + t];
       double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
@@ -1952,6 +1953,13 @@ void orc_pair_force_verlet_sog(int level, double cut_off, const orc_box* box, do
       f[0] += dx * fp;
       f[1] += dy * fp;
       f[2] += dz * fp;
+      /* ComputeVirial (lj_op.hip.cu:76-88) of the pair force */
+      v[0] += -0.5 * dx * dx * fp;
+      v[1] += -0.5 * dy * dy * fp;
+      v[2] += -0.5 * dz * dz * fp;
+      v[3] += -0.5 * dx * dy * fp;
+      v[4] += -0.5 * dx * dz * fp;
+      v[5] += -0.5 * dy * dz * fp;
       elj += 0.5 * (4 * eij * (s6 / d6 - 1) * sd6);
       const double norm = 2.0 * log(s.b) / sqrt(2.0 * M_PI * s.sigma * s.sigma);
       double sume = norm * s.w0 * exp(-d2 / (2.0 * s.sigma * s.sigma));
@@ -1963,6 +1971,8 @@ void orc_pair_force_verlet_sog(int level, double cut_off, const orc_box* box, do
     fx[i] = f[0];
     fy[i] = f[1];
     fz[i] = f[2];
+    if (flat_virial)
+      for (int c = 0; c < 6; ++c) flat_virial[(size_t)c * n + i] = v[c];
   }
   if (energy) {
     energy[0] = elj;

@@ -819,7 +819,7 @@ int rbx_pair_force_verlet_sog(const rbx_box* box, int level, double cut_off, dou
                               const int* type, const double* charge, const double* px,
                               const double* py, const double* pz, int cap, const int* cand_count,
                               const int* cand, double* fx, double* fy, double* fz,
-                              double* energy, void* stream) {
+                              double* energy, double* flat_virial, void* stream) {
   RBX_CHECK_BOX(box);
   if (num_atoms < 0 || ntypes <= 0 || !sigma || !eps || cap < 0) {
     set_error("rbx_pair_force_verlet_sog: invalid arguments");
@@ -858,7 +858,7 @@ int rbx_pair_force_verlet_sog(const rbx_box* box, int level, double cut_off, dou
     sp.lj_eps = tabs;
     sp.lj_s6 = tabs + he.size();
     rc = launch_verlet_sog(sp, num_atoms, px, py, pz, charge, type, cand_count, cand, cap, fx, fy,
-                           fz, epart, st);
+                           fz, epart, st, flat_virial);
   }
   if (!rc) rc = cuda_ok(cudaStreamSynchronize(st), "rbx_pair_force_verlet_sog");
   if (!rc && energy) {

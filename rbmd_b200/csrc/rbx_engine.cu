@@ -143,8 +143,8 @@ int rbx_engine::init() {
     set_error("neighbor type must be Verlet-List, RBL or VERLET-SOG");
     return RBX_ERR_CONFIG;
   }
-  if (prm.ntypes <= 0 || prm.ntypes > 16) {
-    set_error("ntypes must be in [1, 16]");
+  if (prm.ntypes <= 0 || prm.ntypes > RBX_MAX_TYPES) {
+    set_error("ntypes must be in [1, %d]", RBX_MAX_TYPES);
     return RBX_ERR_CONFIG;
   }
   for (int d = 0; d < 3; ++d)
@@ -246,7 +246,8 @@ int rbx_engine::init() {
   pp.sqrt_alpha = sqrt(prm.alpha);
   pp.qqr2e = prm.qqr2e;
   pp.freq = freq;
-  nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, freq, n, cap, nfpart, tun.rbl_waves);
+  nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, freq, n, cap, nfpart, tun.rbl_waves,
+                        prm.ntypes);
   pp.div = div;
   pp.ntypes = prm.ntypes;
   pp.lj_eps = lj_eps;
@@ -428,7 +429,8 @@ int rbx_engine::rebuild() {
     release(cand);
     cap = ((int)(maxc * 1.2) + 31) / 32 * 32;
     ETRY(alloc(&cand, (size_t)n * cap));
-    nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart, tun.rbl_waves);
+    nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart, tun.rbl_waves,
+                          prm.ntypes);
     graph_dirty = host_graph_dirty = true;  // the list moved
     ++graph_version;
     ETRY(launch_fill_i32(1, dflags + 1, 0, st));
@@ -557,7 +559,8 @@ int rbx_engine::apply_tuning(const Tuning& t) {
   tun = t;
   if (P > 0) nparts = t.rho_parts > 0 ? std::min(t.rho_parts, nparts_cap) : rbe_partial_blocks(n);
   if (prm.neighbor_type == RBX_NEIGHBOR_RBL)
-    nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart, tun.rbl_waves);
+    nrbl = rbl_fused_grid(prm.precision == RBX_MIXED, pp.freq, n, cap, nfpart, tun.rbl_waves,
+                          prm.ntypes);
   graph_dirty = host_graph_dirty = true;
   ++graph_version;
   return RBX_OK;
@@ -669,7 +672,7 @@ int rbx_engine::autotune(bool force, rbx_tuning* out) {
     if (!rc && prm.neighbor_type == RBX_NEIGHBOR_RBL) {
       std::vector<Cand> c;
       for (int waves : {2, 4, 8, 16}) {
-        const int nb = rbl_fused_grid(mixed, pp.freq, n, cap, nfpart, waves);
+        const int nb = rbl_fused_grid(mixed, pp.freq, n, cap, nfpart, waves, prm.ntypes);
         float ms = 0.f;
         rc = time_it(
             [&]() {
@@ -1370,20 +1373,20 @@ int rbx_engine::force_vjp(const double* g, double* d_eps, double* d_sigma, doubl
   ETRY(cuda_ok(cudaMemcpyAsync(eps_t, eps.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, st),
                "H2D"));
   ETRY(launch_gather_vec3(n, orig, stage, gx, gy, gz, st));
+  // mixed form: FP32 pair and k-space terms (exact fixed-point phases, the k
+  // table of the last force evaluation), FP64 sums; plain FP64 otherwise
+  const bool mixed = prm.precision == RBX_MIXED;
   ETRY(launch_adj_pair(pp, n, x, y, z, q, type, sig_t, eps_t, key_a, key_b, epoch, rows(), gx,
-                       gy, gz, mean_g, rx, ry, rz, dq, ppart, nb_pair, st));
+                       gy, gz, mean_g, rx, ry, rz, dq, ppart, nb_pair, st, mixed));
   if (P > 0) {
-    if (prm.precision == RBX_MIXED) {  // the k table from an FP64 rho(k) of the same samples
-      ETRY(launch_rbe_rho_partial_f64(dbox, n, P, mx, my, mz, q, x, y, z, part_re, part_im,
-                                      nparts, st));
-      ETRY(launch_rbe_finalize(dbox, P, nparts, part_re, part_im, mx, my, mz, prm.alpha, S,
-                               prm.qqr2e, qsq, qsum, rho_re, rho_im, nullptr, nullptr, tab, 0,
-                               nullptr, n, nullptr, nullptr, st));
-    }
     const double V = dbox.len[0] * dbox.len[1] * dbox.len[2];
     const double cscale = -4.0 * M_PI * prm.qqr2e * S / ((double)P * V);
-    ETRY(launch_adj_kspace(n, P, cscale, tab, q, x, y, z, gx, gy, gz, part_re, part_im, nparts,
-                           kterm, rx, ry, rz, dq, kpart, st));
+    if (mixed)
+      ETRY(launch_adj_kspace_mixed(n, P, cscale, tab, atoms, gx, gy, gz, part_re, part_im,
+                                   nparts, kterm, rx, ry, rz, dq, kpart, st));
+    else
+      ETRY(launch_adj_kspace(n, P, cscale, tab, q, x, y, z, gx, gy, gz, part_re, part_im, nparts,
+                             kterm, rx, ry, rz, dq, kpart, st));
   }
   std::vector<double> hp((size_t)nb_pair * npar), hk(P > 0 ? nb_k : 0);
   ETRY(cuda_ok(cudaMemcpyAsync(hp.data(), ppart, sizeof(double) * hp.size(),

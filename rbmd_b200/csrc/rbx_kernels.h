@@ -127,7 +127,10 @@ struct PairParams {
 int rbl_fused_blocks(int n);
 // Grid of the fused RBL kernel for this form: one wave of resident blocks,
 // at most max_blocks (the capacity of the per-block partial buffer).
-int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int waves = 8);
+int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int waves = 8,
+                   int ntypes = 1);
+// Dynamic shared memory of the pair kernels' per-type-pair LJ tables.
+size_t type_table_bytes(int ntypes, bool mixed);
 // Rows may be split (near / far segments, the far pairs certainly outside
 // r_core until the next rebuild) or not (far null: every pair classified).
 int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms,
@@ -229,7 +232,8 @@ int launch_adj_pair(const PairParams& pp, int n, const double* x, const double* 
                     const unsigned long long* key_b, int epoch, const Rows& rows,
                     const double* gx, const double* gy,
                     const double* gz, const double mean_g[3], double* d_rx, double* d_ry,
-                    double* d_rz, double* d_q, double* part, int nblocks, cudaStream_t st);
+                    double* d_rz, double* d_q, double* part, int nblocks, cudaStream_t st,
+                    bool f32 = false);
 // k-space part, added to d_r and d_q; part_gk[adj_k_blocks(n)] = block sums of g . K.
 // cscale = -4 pi qqr2e S / (P V); ab: 2p scratch; part_a/b: p * nparts scratch.
 int adj_k_blocks(int n);
@@ -238,6 +242,11 @@ int launch_adj_kspace(int n, int p, double cscale, const KTab* tab, const double
                       const double* gy, const double* gz, double* part_a, double* part_b,
                       int nparts, double* ab, double* d_rx, double* d_ry, double* d_rz,
                       double* d_q, double* part_gk, cudaStream_t st);
+// Mixed form: phases from the fixed-point records, FP32 terms, FP64 sums.
+int launch_adj_kspace_mixed(int n, int p, double cscale, const KTab* tab, const uint4* atoms,
+                            const double* gx, const double* gy, const double* gz, double* part_a,
+                            double* part_b, int nparts, double* ab, double* d_rx, double* d_ry,
+                            double* d_rz, double* d_q, double* part_gk, cudaStream_t st);
 // [n][3] interleaved host-order rows -> three cell-order arrays (orig[i] = host index).
 int launch_gather_vec3(int n, const int* orig, const double* src, double* x, double* y, double* z,
                        cudaStream_t st);
@@ -279,10 +288,11 @@ int verlet_sog_blocks(int n);
 int launch_verlet_sog_mixed(const SogPairParams& sp, const float sf[3], int n, const uint4* atoms,
                             const int* type, const int* cand_count, const int* cand, int cap,
                             double* fx, double* fy, double* fz, cudaStream_t st);
+// flat_virial (may be null): per-atom virial [6][n] (xx, yy, zz, xy, xz, yz).
 int launch_verlet_sog(const SogPairParams& sp, int n, const double* x, const double* y,
                       const double* z, const double* q, const int* type, const int* cand_count,
                       const int* cand, int cap, double* fx, double* fy, double* fz, double* epart,
-                      cudaStream_t st);
+                      cudaStream_t st, double* flat_virial = nullptr);
 
 // Nose-Hoover chain (rbx_thermo.cu): parameters and the device state layout.
 constexpr int NH_CHAIN = 3;

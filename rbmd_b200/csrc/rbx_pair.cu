@@ -30,7 +30,6 @@ namespace rbx {
 constexpr int PAIR_BLOCK = 256;
 constexpr int PAIR_WARPS = PAIR_BLOCK / 32;
 constexpr int QCAP = 64;
-constexpr int MAX_TYPES_SMEM = 16;  // ntypes^2 <= 256 pair entries in shared memory
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -67,18 +66,54 @@ __device__ __forceinline__ float coul_f32(float alpha, float sqrt_alpha, float q
   return -qqr2e * qq * g * rinv;
 }
 
+// Per-type-pair LJ tables (eps_ij and sigma_ij^6, ntypes^2 entries each) in
+// dynamic shared memory: FP64, then FP32 copies for the mixed form.
 struct TypeTables {
-  double eps[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
-  double s6[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
+  double* eps;
+  double* s6;
+  float* f_eps;
+  float* f_s6;
 };
 
-__device__ __forceinline__ void load_type_tables(TypeTables& t, const PairParams& pp) {
+size_t type_table_bytes(int ntypes, bool mixed) {
+  return (size_t)ntypes * ntypes * (2 * sizeof(double) + (mixed ? 2 * sizeof(float) : 0));
+}
+
+// Carve the tables out of the dynamic shared memory and fill them (all
+// threads of the block call this).
+__device__ __forceinline__ TypeTables load_type_tables(const PairParams& pp, bool mixed) {
+  extern __shared__ __align__(16) unsigned char s_types[];
   const int nt2 = pp.ntypes * pp.ntypes;
+  TypeTables t;
+  t.eps = reinterpret_cast<double*>(s_types);
+  t.s6 = t.eps + nt2;
+  t.f_eps = reinterpret_cast<float*>(t.s6 + nt2);
+  t.f_s6 = t.f_eps + nt2;
   for (int e = threadIdx.x; e < nt2; e += blockDim.x) {
-    t.eps[e] = pp.lj_eps[e];
-    t.s6[e] = pp.lj_s6[e];
+    const double ep = pp.lj_eps[e], s6 = pp.lj_s6[e];
+    t.eps[e] = ep;
+    t.s6[e] = s6;
+    if (mixed) {
+      t.f_eps[e] = (float)ep;
+      t.f_s6[e] = (float)s6;
+    }
   }
   __syncthreads();
+  return t;
+}
+
+// Opt a kernel in to the dynamic shared memory its type tables need.
+template <typename K>
+int type_table_smem(K kern, int ntypes, bool mixed, size_t* bytes) {
+  *bytes = type_table_bytes(ntypes, mixed);
+  if (*bytes > 48 * 1024 &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    set_error("pair kernels: %d atom types need %zu bytes of shared memory", ntypes, *bytes);
+    return RBX_ERR_INVALID;
+  }
+  return RBX_OK;
 }
 
 // Block partial of the per-atom forces, accumulated by lane 0 of each warp in
@@ -209,18 +244,11 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
             double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart) {
   using T = typename std::conditional<MIXED, float, double>::type;
   const int epoch = epoch_dev ? *epoch_dev : epoch_arg;  // device copy inside a step graph
-  __shared__ TypeTables tt;
   __shared__ int s_q[PAIR_WARPS][RBL_QCAP];
   __shared__ double s_acc[PAIR_WARPS][3];
-  __shared__ float f_eps[MAX_TYPES_SMEM * MAX_TYPES_SMEM], f_s6[MAX_TYPES_SMEM * MAX_TYPES_SMEM];
-  load_type_tables(tt, pp);
-  if (MIXED) {
-    for (int e = threadIdx.x; e < pp.ntypes * pp.ntypes; e += blockDim.x) {
-      f_eps[e] = (float)tt.eps[e];
-      f_s6[e] = (float)tt.s6[e];
-    }
-    __syncthreads();
-  }
+  const TypeTables tt = load_type_tables(pp, MIXED);
+  const float* const f_eps = tt.f_eps;
+  const float* const f_s6 = tt.f_s6;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = lanemask_lt();
   const unsigned long long fmask = (unsigned long long)(pp.freq - 1);
@@ -423,14 +451,13 @@ k_verlet_fused_f64(PairParams pp, int n, const uint4* __restrict__ atoms,
                    const int* __restrict__ type, Rows rows, double* __restrict__ fx,
                    double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart,
                    double* __restrict__ epart) {
-  __shared__ TypeTables tt;
   __shared__ struct {
     double dx[PAIR_WARPS][QCAP], dy[PAIR_WARPS][QCAP], dz[PAIR_WARPS][QCAP];
     int j[PAIR_WARPS][QCAP];
   } qu;
   __shared__ double s_acc[PAIR_WARPS][3];
   __shared__ double s_e[PAIR_WARPS][8];
-  load_type_tables(tt, pp);
+  const TypeTables tt = load_type_tables(pp, false);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = lanemask_lt();
   double acc0 = 0, acc1 = 0, acc2 = 0;
@@ -844,6 +871,12 @@ __global__ void k_sub_mean(int n, T* __restrict__ fx, T* __restrict__ fy, T* __r
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
+#define RBX_TRY_K(expr)     \
+  do {                      \
+    const int _rc = (expr); \
+    if (_rc) return _rc;    \
+  } while (0)
+
 IntScreen make_screen(double C, double L, double band) {
   // |d|^2 s^2 < C  <=>  |d|^2 < C / s^2, s = L / 2^32; band in r^2 units
   const double scale = 18446744073709551616.0 / (L * L);
@@ -885,14 +918,16 @@ RblKernel rbl_choose(bool mixed, int freq, bool cubic) {
 }
 }  // namespace
 
-int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int waves) {
+int rbl_fused_grid(bool mixed, int freq, int n, int cap, int max_blocks, int waves, int ntypes) {
   // waves of resident blocks (default 8): with several waves the block
   // scheduler evens out the per-atom work
   (void)cap;
   const int kRblWaves = waves > 0 ? waves : 8;
   const RblKernel k = rbl_choose(mixed, freq, true);  // occupancy of the cubic form
+  size_t smem = 0;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, PAIR_BLOCK, 0) != cudaSuccess ||
+  if (type_table_smem(k, ntypes, mixed, &smem) != RBX_OK ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, PAIR_BLOCK, smem) != cudaSuccess ||
       occ < 1) {
     cudaGetLastError();
     occ = 1;
@@ -916,7 +951,9 @@ int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms
     return RBX_ERR_INVALID;
   }
   const RblKernel k = rbl_choose(mixed, pp.freq, pp.cubic != 0);
-  k<<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
+  size_t smem = 0;
+  RBX_TRY_K(type_table_smem(k, pp.ntypes, mixed, &smem));
+  k<<<nblocks, PAIR_BLOCK, smem, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
                                     epoch_dev, rows, fx, fy, fz, fpart);
   count_launch();
   return check_launch(mixed ? "rbl_fused_mixed" : "rbl_fused_f64");
@@ -927,12 +964,16 @@ int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, con
                             const Rows& rows, double* fx, double* fy, double* fz, double* fpart,
                             double* epart, int nblocks, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  if (pp.cubic)
-    k_verlet_fused_f64<true><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type, rows,
-                                                             fx, fy, fz, fpart, epart);
-  else
-    k_verlet_fused_f64<false><<<nblocks, PAIR_BLOCK, 0, st>>>(pp, n, atoms, x, y, z, q, type,
-                                                              rows, fx, fy, fz, fpart, epart);
+  size_t smem = 0;
+  if (pp.cubic) {
+    RBX_TRY_K(type_table_smem(k_verlet_fused_f64<true>, pp.ntypes, false, &smem));
+    k_verlet_fused_f64<true><<<nblocks, PAIR_BLOCK, smem, st>>>(pp, n, atoms, x, y, z, q, type,
+                                                                rows, fx, fy, fz, fpart, epart);
+  } else {
+    RBX_TRY_K(type_table_smem(k_verlet_fused_f64<false>, pp.ntypes, false, &smem));
+    k_verlet_fused_f64<false><<<nblocks, PAIR_BLOCK, smem, st>>>(pp, n, atoms, x, y, z, q, type,
+                                                                 rows, fx, fy, fz, fpart, epart);
+  }
   count_launch();
   return check_launch("verlet_fused_f64");
 }

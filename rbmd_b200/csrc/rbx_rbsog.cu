@@ -159,13 +159,16 @@ k_rbsog_energy_sum(int p, const double* __restrict__ kterm, double self_energy,
 // -qqr2e qi qj (1/r^3 + sum_(i<6) c_i r^(2i)); energy 4 eps (s6/r6 - 1) s6/r6 / 2
 // and qqr2e qi qj (1/r - sum_l w_l exp(-r^2 / (2 sigma^2 b^(2l)))) / 2.  A warp
 // per atom over its candidate row, FP64, per-atom sums in lane order.
-template <bool ENERGY>
+// VIRIAL: the per-atom virial flat_virial[c * n + i] of ComputeVirial
+// (lj_op.hip.cu:76-88), -r_a r_b f / 2 summed over the atom's pairs.
+template <bool ENERGY, bool VIRIAL>
 __global__ void __launch_bounds__(SOG_PAIR_BLOCK)
 k_verlet_sog(SogPairParams sp, int n, const double* __restrict__ x, const double* __restrict__ y,
              const double* __restrict__ z, const double* __restrict__ q,
              const int* __restrict__ type, const int* __restrict__ cand_count,
              const int* __restrict__ cand, int cap, double* __restrict__ fx,
-             double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ epart) {
+             double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ epart,
+             double* __restrict__ vir) {
   __shared__ double se[2][SOG_PAIR_BLOCK / 32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int i = blockIdx.x * (SOG_PAIR_BLOCK / 32) + wib;
@@ -175,7 +178,7 @@ k_verlet_sog(SogPairParams sp, int n, const double* __restrict__ x, const double
     const int ti = type[i];
     const double cut2 = sp.cut_off * sp.cut_off;
     const int cnt = min(cand_count[i], cap);
-    double f[3] = {0, 0, 0};
+    double f[3] = {0, 0, 0}, v[6] = {0, 0, 0, 0, 0, 0};
     for (int t = lane; t < cnt; t += 32) {
       const int j = cand[(size_t)i * cap + t];
       double dx = x[j] - xi, dy = y[j] - yi, dz = z[j] - zi;
@@ -200,6 +203,14 @@ k_verlet_sog(SogPairParams sp, int n, const double* __restrict__ x, const double
       f[0] += fp * dx;
       f[1] += fp * dy;
       f[2] += fp * dz;
+      if (VIRIAL) {
+        v[0] += -0.5 * dx * dx * fp;
+        v[1] += -0.5 * dy * dy * fp;
+        v[2] += -0.5 * dz * dz * fp;
+        v[3] += -0.5 * dx * dy * fp;
+        v[4] += -0.5 * dx * dz * fp;
+        v[5] += -0.5 * dy * dz * fp;
+      }
       if (ENERGY) {
         elj += 0.5 * (4 * eps * (s6 / d6 - 1) * sd6);
         double sume = sp.norm * sp.w0 * exp(-d2 / (2.0 * sp.sigma * sp.sigma));
@@ -212,10 +223,14 @@ k_verlet_sog(SogPairParams sp, int n, const double* __restrict__ x, const double
       }
     }
     for (int d = 0; d < 3; ++d) f[d] = warp_sum(f[d]);
+    if (VIRIAL)
+      for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
     if (lane == 0) {
       fx[i] = f[0];
       fy[i] = f[1];
       fz[i] = f[2];
+      if (VIRIAL)
+        for (int c = 0; c < 6; ++c) vir[(size_t)c * n + i] = v[c];
     }
   }
   if (ENERGY) {
@@ -242,8 +257,10 @@ k_verlet_sog_mixed(SogPairParams sp, float sfx, float sfy, float sfz, int n,
                    const uint4* __restrict__ atoms, const int* __restrict__ type,
                    const int* __restrict__ cand_count, const int* __restrict__ cand, int cap,
                    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
-  __shared__ float s_eps[256], s_s6[256];
+  extern __shared__ __align__(16) float s_tab[];  // eps_ij, then sigma_ij^6 (ntypes^2 each)
   const int nt2 = sp.ntypes * sp.ntypes;
+  float* const s_eps = s_tab;
+  float* const s_s6 = s_tab + nt2;
   for (int t = threadIdx.x; t < nt2; t += SOG_PAIR_BLOCK) {
     s_eps[t] = (float)sp.lj_eps[t];
     s_s6[t] = (float)sp.lj_s6[t];
@@ -326,15 +343,17 @@ int verlet_sog_blocks(int n) { return (n + SOG_PAIR_BLOCK / 32 - 1) / (SOG_PAIR_
 int launch_verlet_sog(const SogPairParams& sp, int n, const double* x, const double* y,
                       const double* z, const double* q, const int* type, const int* cand_count,
                       const int* cand, int cap, double* fx, double* fy, double* fz, double* epart,
-                      cudaStream_t st) {
+                      cudaStream_t st, double* flat_virial) {
   if (n <= 0) return RBX_OK;
   const int grid = verlet_sog_blocks(n);
+  auto go = [&](auto kern) {
+    kern<<<grid, SOG_PAIR_BLOCK, 0, st>>>(sp, n, x, y, z, q, type, cand_count, cand, cap, fx, fy,
+                                          fz, epart, flat_virial);
+  };
   if (epart)
-    k_verlet_sog<true><<<grid, SOG_PAIR_BLOCK, 0, st>>>(sp, n, x, y, z, q, type, cand_count, cand,
-                                                        cap, fx, fy, fz, epart);
+    flat_virial ? go(k_verlet_sog<true, true>) : go(k_verlet_sog<true, false>);
   else
-    k_verlet_sog<false><<<grid, SOG_PAIR_BLOCK, 0, st>>>(sp, n, x, y, z, q, type, cand_count,
-                                                         cand, cap, fx, fy, fz, nullptr);
+    flat_virial ? go(k_verlet_sog<false, true>) : go(k_verlet_sog<false, false>);
   count_launch();
   return check_launch("verlet_sog");
 }
@@ -346,11 +365,16 @@ int launch_verlet_sog_mixed(const SogPairParams& sp, const float sf[3], int n, c
                             const int* type, const int* cand_count, const int* cand, int cap,
                             double* fx, double* fy, double* fz, cudaStream_t st) {
   if (n <= 0) return RBX_OK;
-  if (sp.ntypes * sp.ntypes > 256) {
-    set_error("VERLET-SOG mixed form: at most 16 atom types");
+  const size_t smem = (size_t)2 * sp.ntypes * sp.ntypes * sizeof(float);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(k_verlet_sog_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("VERLET-SOG mixed form: %d atom types need %zu bytes of shared memory",
+              sp.ntypes, smem);
     return RBX_ERR_INVALID;
   }
-  k_verlet_sog_mixed<<<verlet_sog_blocks(n), SOG_PAIR_BLOCK, 0, st>>>(
+  k_verlet_sog_mixed<<<verlet_sog_blocks(n), SOG_PAIR_BLOCK, smem, st>>>(
       sp, sf[0], sf[1], sf[2], n, atoms, type, cand_count, cand, cap, fx, fy, fz);
   count_launch();
   return check_launch("verlet_sog_mixed");

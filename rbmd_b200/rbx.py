@@ -20,6 +20,8 @@ _lib = None
 RBX_OK = 0
 PLAIN_FP64 = 0
 MIXED = 1
+# largest atom-type count an engine takes (RBX_MAX_TYPES of include/rbx.h)
+MAX_TYPES = 64
 NEIGHBOR_VERLET = 0
 NEIGHBOR_RBL = 1
 NEIGHBOR_VERLET_SOG = 2
@@ -216,7 +218,7 @@ def lib():
     L.rbx_rbsog_force.argtypes = [B, ip, dp, dp, dp, dp, ip, ip] + [vp] * 10 + [
         C.POINTER(C.c_double), vp]
     L.rbx_pair_force_verlet_sog.argtypes = [B, ip, dp, dp, ip, ip, vp, vp] + [vp] * 5 + [
-        ip, vp, vp, vp, vp, vp, vp, vp]
+        ip, vp, vp, vp, vp, vp, vp, vp, vp]
     L.rbx_lammps_read.restype = vp
     L.rbx_lammps_read.argtypes = [C.c_char_p, C.c_char_p, vp]
     L.rbx_lammps_free.argtypes = [vp]
@@ -939,8 +941,9 @@ def rbsog_force(box, level, cut_off, qqr2e, S, qsqsum, q, mx, my, mz, x, y, z, f
 
 
 def pair_force_verlet_sog(box, level, cut_off, qqr2e, sigma, eps, typ, q, x, y, z, count, rows,
-                          fx, fy, fz, stream=None):
-    """VERLET-SOG pair force over row-major candidate rows [n, cap]; returns (E_LJ, E_coul)."""
+                          fx, fy, fz, flat_virial=None, stream=None):
+    """VERLET-SOG pair force over row-major candidate rows [n, cap]; returns (E_LJ, E_coul).
+    flat_virial (device, 6 n doubles, optional) receives the per-atom virial."""
     sg = np.ascontiguousarray(sigma, np.float64)
     ep = np.ascontiguousarray(eps, np.float64)
     en = np.zeros(2)
@@ -948,5 +951,6 @@ def pair_force_verlet_sog(box, level, cut_off, qqr2e, sigma, eps, typ, q, x, y, 
                                           _np_ptr(sg), _np_ptr(ep), _ptr(typ), _ptr(q), _ptr(x),
                                           _ptr(y), _ptr(z), rows.shape[1], _ptr(count), _ptr(rows),
                                           _ptr(fx), _ptr(fy), _ptr(fz), _np_ptr(en),
-                                          _stream(stream)), "rbx_pair_force_verlet_sog")
+                                          _ptr(flat_virial), _stream(stream)),
+          "rbx_pair_force_verlet_sog")
     return en

@@ -59,16 +59,21 @@ def test_verlet_sog_pair_force_matches_oracle(cuda, rbx, oracle, sys4k):
     xs, ys, zs = x[perm], y[perm], z[perm]
     cnt, rows = oracle.full_list(box, 5.3, xs, ys, zs, cell, cs, ce)
     typ, q = s["type"][perm].astype(np.int32), s["q"][perm]
-    want, ew = oracle.pair_force_verlet_sog(2, 5.0, box, 1.0, typ, s["sigma"], s["eps"], q,
-                                            xs, ys, zs, cnt, rows)
+    want, ew, wv = oracle.pair_force_verlet_sog(2, 5.0, box, 1.0, typ, s["sigma"], s["eps"], q,
+                                                xs, ys, zs, cnt, rows, virial=True)
     T = lambda a: _t(cuda, a)  # noqa: E731
     F = [cuda.zeros(s["n"], dtype=cuda.float64, device="cuda") for _ in range(3)]
+    vir = cuda.zeros(6 * s["n"], dtype=cuda.float64, device="cuda")
     en = rbx.pair_force_verlet_sog(rbx.Box.make(s["lo"], s["hi"]), 2, 5.0, 1.0, s["sigma"],
                                    s["eps"], T(typ), T(q), T(xs), T(ys), T(zs), T(cnt), T(rows),
-                                   *F)
+                                   *F, flat_virial=vir)
     got = np.stack([a.cpu().numpy() for a in F], 1)
     assert systems.rel_rms(got, want) < 1e-10
     assert np.allclose(en, ew, rtol=1e-10)
+    # per-atom virial (ComputeVirial of the pair force), and its total
+    gv = vir.cpu().numpy().reshape(6, s["n"])
+    assert np.abs(gv - wv).max() < 1e-10 * np.abs(wv).max()
+    assert np.abs(gv.sum(1) - wv.sum(1)).max() < 1e-10 * np.abs(wv.sum(1)).max()
 
 
 def _sog_system(n=4000, seed=29, level=2):
