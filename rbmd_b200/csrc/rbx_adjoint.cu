@@ -1,5 +1,7 @@
 // rbx_adjoint.cu -- adjoint (vector-Jacobian product) of the RBL + RBE force
-// for force-field fitting, plain FP64.
+// for force-field fitting: plain FP64 for FP64 engines; FP32 pair terms and
+// FP32 k-space terms on exact fixed-point phases with FP64 sums for engines
+// in the mixed form.
 //
 // For an upstream g = dL/dF it gives dL/d(eps_t, sigma_t) per type, dL/dq_i,
 // dL/dalpha and dL/dr_i (the Hessian-vector product), for the lists, batch
@@ -60,7 +62,36 @@ __device__ __forceinline__ PairTerms pair_terms(double e, double sg, double qq, 
   return t;
 }
 
+// The same pair terms in FP32 (mixed form), returned widened to FP64 for the
+// FP64 sums of the adjoint.
+__device__ __forceinline__ PairTerms pair_terms_f32(float e, float sg, float qq, float r2,
+                                                    float alpha, float qqr2e) {
+  const float ui = 1.0f / r2;
+  const float s2 = sg * sg, s6 = s2 * s2 * s2;
+  const float u = s6 * ui * ui * ui;
+  const float f_lj = -24.0f * e * (2.0f * u * u - u) * ui;
+  const float ui2 = ui * ui, ui4 = ui2 * ui2;
+  const float fp_lj = 24.0f * e * (14.0f * s6 * s6 * ui4 * ui4 - 4.0f * s6 * ui4 * ui);
+  const float r = sqrtf(r2);
+  const float b = sqrtf(alpha);
+  const float ex = expf(-alpha * r2);
+  const float ec = erfcf(b * r);
+  const float two_b_pi = 2.0f * b / 1.77245385090551602729f;
+  const float h = -qqr2e * (ec * ui + two_b_pi * ex / r) / r;
+  const float dh_dr = qqr2e * (3.0f * ec * ui2 + two_b_pi * ex * (3.0f * ui + 2.0f * alpha) / r);
+  PairTerms t;
+  t.h = h;
+  t.dh_da = qqr2e * two_b_pi * ex;
+  t.f = f_lj + qq * h;
+  t.fp = fp_lj + qq * dh_dr / (2.0f * r);
+  t.df_de = f_lj / e;
+  t.df_ds = -144.0f * e * (4.0f * u * u - u) * ui / sg;
+  return t;
+}
+
 // Block partials: [block][2 * ntypes + 1] = d_eps[0..nt), d_sigma[0..nt), d_alpha.
+// F32: pair terms in FP32 (mixed form), sums in FP64 either way.
+template <bool F32>
 __global__ void __launch_bounds__(ADJ_BLOCK)
 k_adj_pair(PairParams pp, int n, const double* __restrict__ x, const double* __restrict__ y,
            const double* __restrict__ z, const double* __restrict__ q,
@@ -109,7 +140,10 @@ k_adj_pair(PairParams pp, int n, const double* __restrict__ x, const double* __r
       const double e = sqrt(eps_t[tm] * eps_t[tj]);
       const double sg = 0.5 * (sigma_t[tm] + sigma_t[tj]);
       const double qj = q[j];
-      const PairTerms pt = pair_terms(e, sg, qm * qj, r2, pp.alpha, pp.qqr2e);
+      const PairTerms pt =
+          F32 ? pair_terms_f32((float)e, (float)sg, (float)(qm * qj), (float)r2, (float)pp.alpha,
+                               (float)pp.qqr2e)
+              : pair_terms(e, sg, qm * qj, r2, pp.alpha, pp.qqr2e);
       if (in_m) {  // pair (m, j) of m's force: parameters and -c on r_m
         const double gd = gpx * dx + gpy * dy + gpz * dz;
         const double w = s * gd;
@@ -224,6 +258,81 @@ k_adj_k_scatter(int n, int p, double cscale, const KTab* __restrict__ tab,
   if (threadIdx.x == 0) part_gk[blockIdx.x] = gk_sum;
 }
 
+// Mixed form of the k-space passes: the phase k.r_i = 2 pi (m . u_i) / 2^32 from
+// the 32-bit fixed-point record u_i exactly in integer arithmetic, sin and
+// cos on the SFU, every term in FP32 and every sum in FP64.
+__global__ void __launch_bounds__(ADJK_BLOCK)
+k_adj_k_ab_mixed(int n, int p, int chunk, const KTab* __restrict__ tab,
+                 const uint4* __restrict__ atoms, const double* __restrict__ gx,
+                 const double* __restrict__ gy, const double* __restrict__ gz,
+                 double* __restrict__ part_a, double* __restrict__ part_b) {
+  const int k = blockIdx.y * ADJK_BLOCK + threadIdx.x;
+  if (k >= p) return;
+  const KTab t = tab[k];
+  const unsigned m0 = (unsigned)t.m[0], m1 = (unsigned)t.m[1], m2 = (unsigned)t.m[2];
+  const float kx = (float)t.kx, ky = (float)t.ky, kz = (float)t.kz;
+  const float ang = (float)(2.0 * RBX_PI / 4294967296.0);
+  const int a0 = blockIdx.x * chunk, a1 = min(n, a0 + chunk);
+  double sa = 0.0, sb = 0.0;
+  for (int i = a0; i < a1; ++i) {
+    const uint4 a = atoms[i];
+    const unsigned ph = m0 * a.x + m1 * a.y + m2 * a.z;
+    float sn, cs;
+    __sincosf((float)(int)ph * ang, &sn, &cs);
+    const float w = __uint_as_float(a.w) *
+                    ((float)gx[i] * kx + (float)gy[i] * ky + (float)gz[i] * kz);
+    sa += (double)(w * cs);
+    sb += (double)(w * sn);
+  }
+  part_a[(size_t)k * gridDim.x + blockIdx.x] = sa;
+  part_b[(size_t)k * gridDim.x + blockIdx.x] = sb;
+}
+
+__global__ void __launch_bounds__(ADJK_BLOCK)
+k_adj_k_scatter_mixed(int n, int p, double cscale, const KTab* __restrict__ tab,
+                      const double* __restrict__ ab, const uint4* __restrict__ atoms,
+                      const double* __restrict__ gx, const double* __restrict__ gy,
+                      const double* __restrict__ gz, double* __restrict__ d_rx,
+                      double* __restrict__ d_ry, double* __restrict__ d_rz,
+                      double* __restrict__ d_q, double* __restrict__ part_gk) {
+  __shared__ double s_sum[ADJK_BLOCK / 32];
+  const int i = blockIdx.x * ADJK_BLOCK + threadIdx.x;
+  double gk_sum = 0.0;
+  if (i < n) {
+    const uint4 a = atoms[i];
+    const float qi = __uint_as_float(a.w);
+    const float gix = (float)gx[i], giy = (float)gy[i], giz = (float)gz[i];
+    const float ang = (float)(2.0 * RBX_PI / 4294967296.0);
+    double rx = 0.0, ry = 0.0, rz = 0.0, dq = 0.0;
+    for (int k = 0; k < p; ++k) {
+      const KTab t = tab[k];
+      const float kx = (float)t.kx, ky = (float)t.ky, kz = (float)t.kz;
+      const float ck = (float)(cscale / (t.kx * t.kx + t.ky * t.ky + t.kz * t.kz));
+      const unsigned ph =
+          (unsigned)t.m[0] * a.x + (unsigned)t.m[1] * a.y + (unsigned)t.m[2] * a.z;
+      float sn, cs;
+      __sincosf((float)(int)ph * ang, &sn, &cs);
+      const float gk = gix * kx + giy * ky + giz * kz;
+      const float ta = (float)t.a, tb = (float)t.b;
+      const float ak = (float)ab[2 * k], bk = (float)ab[2 * k + 1];
+      const float g1 = gk * (cs * tb - sn * ta);
+      dq += (double)(g1 + ck * (ak * sn - bk * cs));
+      const float coef = -gk * (sn * tb + cs * ta) + ck * (ak * cs + bk * sn);
+      rx += (double)(coef * kx);
+      ry += (double)(coef * ky);
+      rz += (double)(coef * kz);
+      gk_sum += (double)g1;
+    }
+    d_rx[i] += (double)qi * rx;
+    d_ry[i] += (double)qi * ry;
+    d_rz[i] += (double)qi * rz;
+    d_q[i] += dq;
+    gk_sum *= (double)qi;
+  }
+  gk_sum = block_sum_det<ADJK_BLOCK>(gk_sum, s_sum);
+  if (threadIdx.x == 0) part_gk[blockIdx.x] = gk_sum;
+}
+
 // Fixed-order reduction of part[k][nb] into out[2 * k + which].
 __global__ void k_adj_reduce_k(int p, int nb, const double* __restrict__ part_a,
                                const double* __restrict__ part_b, double* __restrict__ ab) {
@@ -272,12 +381,14 @@ int launch_adj_pair(const PairParams& pp, int n, const double* x, const double* 
                     const unsigned long long* key_b, int epoch, const Rows& rows,
                     const double* gx, const double* gy,
                     const double* gz, const double mean_g[3], double* d_rx, double* d_ry,
-                    double* d_rz, double* d_q, double* part, int nblocks, cudaStream_t st) {
+                    double* d_rz, double* d_q, double* part, int nblocks, cudaStream_t st,
+                    bool f32) {
   if (pp.ntypes > ADJ_MAX_TYPES) {
     set_error("adjoint: at most %d atom types", ADJ_MAX_TYPES);
     return RBX_ERR_INVALID;
   }
-  k_adj_pair<<<nblocks, ADJ_BLOCK, 0, st>>>(pp, n, x, y, z, q, type, sigma_t, eps_t, key_a, key_b,
+  auto kern = f32 ? k_adj_pair<true> : k_adj_pair<false>;
+  kern<<<nblocks, ADJ_BLOCK, 0, st>>>(pp, n, x, y, z, q, type, sigma_t, eps_t, key_a, key_b,
                                             epoch, rows, gx, gy, gz, mean_g[0],
                                             mean_g[1], mean_g[2], d_rx, d_ry, d_rz, d_q, part);
   count_launch();
@@ -307,6 +418,28 @@ int launch_adj_kspace(int n, int p, double cscale, const KTab* tab, const double
                                                           gy, gz, d_rx, d_ry, d_rz, d_q, part_gk);
   count_launch();
   return check_launch("adj_k_scatter");
+}
+
+int launch_adj_kspace_mixed(int n, int p, double cscale, const KTab* tab, const uint4* atoms,
+                            const double* gx, const double* gy, const double* gz, double* part_a,
+                            double* part_b, int nparts, double* ab, double* d_rx, double* d_ry,
+                            double* d_rz, double* d_q, double* part_gk, cudaStream_t st) {
+  if (p <= 0 || n <= 0) return RBX_OK;
+  const int chunk = (n + nparts - 1) / nparts;
+  const int nb = (n + chunk - 1) / chunk;
+  k_adj_k_ab_mixed<<<dim3(nb, (p + ADJK_BLOCK - 1) / ADJK_BLOCK), ADJK_BLOCK, 0, st>>>(
+      n, p, chunk, tab, atoms, gx, gy, gz, part_a, part_b);
+  count_launch();
+  int rc = check_launch("adj_k_ab_mixed");
+  if (rc) return rc;
+  k_adj_reduce_k<<<p, 128, 0, st>>>(p, nb, part_a, part_b, ab);
+  count_launch();
+  rc = check_launch("adj_reduce_k");
+  if (rc) return rc;
+  k_adj_k_scatter_mixed<<<adj_k_blocks(n), ADJK_BLOCK, 0, st>>>(
+      n, p, cscale, tab, ab, atoms, gx, gy, gz, d_rx, d_ry, d_rz, d_q, part_gk);
+  count_launch();
+  return check_launch("adj_k_scatter_mixed");
 }
 
 }  // namespace rbx

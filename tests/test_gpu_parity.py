@@ -838,7 +838,8 @@ def test_force_vjp_matches_oracle_adjoint(cuda, rbx, oracle, prec):
     """The engine's adjoint (rbx_engine_force_vjp) against the FP64 adjoint
     reference, itself pinned to central differences of the oracle's force:
     parameter gradients per type, dL/dq per atom and dL/dr (Hessian-vector
-    product), with the same lists, batch and k-samples."""
+    product), with the same lists, batch and k-samples.  Plain FP64 within
+    1e-9; the mixed form's FP32 adjoint (FP64 sums) within 2e-5."""
     from oracle import adjoint as A
 
     s = systems.lj_electrolyte(4000, seed=41)
@@ -871,11 +872,14 @@ def test_force_vjp_matches_oracle_adjoint(cuda, rbx, oracle, prec):
     want_q[perm] = d_q
     want_r = np.zeros((s["n"], 3))
     want_r[perm] = d_r
-    assert np.allclose(got["eps"], d_eps, rtol=1e-9, atol=1e-9 * np.abs(d_eps).max())
-    assert np.allclose(got["sigma"], d_sig, rtol=1e-9, atol=1e-9 * np.abs(d_sig).max())
-    assert abs(got["alpha"] - d_alpha) < 1e-9 * abs(d_alpha)
-    assert systems.rel_rms(got["charge"][:, None], want_q[:, None]) < 1e-9
-    assert systems.rel_rms(got["pos"], want_r) < 1e-9
+    # plain FP64 engine: FP64 adjoint; mixed engine: FP32 pair and k-space
+    # terms (exact fixed-point phases) with FP64 sums
+    tol = 1e-9 if prec == 0 else 2e-5
+    assert np.allclose(got["eps"], d_eps, rtol=tol, atol=tol * np.abs(d_eps).max())
+    assert np.allclose(got["sigma"], d_sig, rtol=tol, atol=tol * np.abs(d_sig).max())
+    assert abs(got["alpha"] - d_alpha) < tol * abs(d_alpha)
+    assert systems.rel_rms(got["charge"][:, None], want_q[:, None]) < tol
+    assert systems.rel_rms(got["pos"], want_r) < tol
 
 
 def test_force_vjp_against_engine_finite_differences(cuda, rbx):
