@@ -14,8 +14,11 @@ import pytest
 
 from rbmd_b200 import systems
 
-# RBMD's example inputs, read when the RBMD sources are present
-EXAMPLES = os.path.join(os.environ.get("RBMD_SOURCE", "/root/reference"), "examples")
+# RBMD's example inputs, read when the RBMD sources are present: $RBMD_SOURCE,
+# else a "reference" directory beside this repository
+_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXAMPLES = os.path.join(os.environ.get("RBMD_SOURCE") or
+                        os.path.join(os.path.dirname(_ROOT), "reference"), "examples")
 
 
 def _parse(path):
