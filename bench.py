@@ -983,7 +983,7 @@ def main():
     ap.add_argument("--batched", action="store_true",
                     help="batched-replica measurement instead of the headline line")
     ap.add_argument("--replicas", type=int, default=256)
-    ap.add_argument("--batch-nmin", type=int, default=4000)
+    ap.add_argument("--batch-nmin", type=int, default=953)
     ap.add_argument("--batch-nmax", type=int, default=20000)
     ap.add_argument("--batch-seed", type=int, default=4)
     ap.add_argument("--gradient", action="store_true",

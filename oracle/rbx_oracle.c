@@ -579,8 +579,16 @@ int64_t orc_full_list(int n, const orc_box* box, double neighbor_cutoff,
 #pragma omp parallel for schedule(dynamic, 64) reduction(max : maxc)
   for (int i = 0; i < n; ++i) {
     int cnt = 0;
+    int seen[27], nseen = 0;
     for (int s = 0; s < 27; ++s) {
       const int nc = stencil_cell(dims, cell_of[i], s);
+      /* fewer than three cells along an axis: the stencil wraps onto a cell
+       * it has visited (the reference's WrapFullNeighborStencilIndex then
+       * lists those pairs twice); each pair is listed once here */
+      int dup = 0;
+      for (int k = 0; k < nseen; ++k) dup |= seen[k] == nc;
+      if (dup) continue;
+      seen[nseen++] = nc;
       for (int j = cell_start[nc]; j < cell_end[nc]; ++j) {
         if (j == i) continue;
         const double d2 = orc_dist2(box, x[i], y[i], z[i], x[j], y[j], z[j]);

@@ -408,6 +408,68 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
 }
 
 // ---------------------------------------------------------------------------
+// Candidate rows for boxes with fewer than three cells of edge cut_off + skin
+// along some axis (edge between two and three times cut_off + skin): every
+// atom j != i is tested with the reference's FP64 predicate (CaculateDistance:
+// i minus j, single-shift minimum image, no FMA), so each pair is listed once.
+// (The reference's 27-cell stencil wraps onto the same cell twice along such
+// an axis, WrapFullNeighborStencilIndex in full_neighbor_list_op.hip.cu:9-17,
+// 45-80, and lists those pairs twice.)  A warp per atom; hits are appended in
+// index order through a ballot prefix, far pairs (see FarSplit) to the back.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+k_full_list_small(DBox b, double cut2, double near2, int n, const double* __restrict__ x,
+                  const double* __restrict__ y, const double* __restrict__ z, int cap,
+                  int* __restrict__ count, int* __restrict__ nbrs, int* __restrict__ overflow,
+                  int* __restrict__ far) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (i >= n) return;
+  const unsigned lt = (1u << lane) - 1u;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  int nf = 0, nb = 0;  // near (front) and far (back) entries found
+  int* row = nbrs + (size_t)i * cap;
+  for (int j0 = 0; j0 < n; j0 += 32) {
+    const int j = j0 + lane;
+    double d2 = INFINITY;
+    if (j < n && j != i) d2 = dist2_list(b, xi, yi, zi, x[j], y[j], z[j]);
+    const bool hit = d2 < cut2;
+    const bool is_far = hit && !(d2 < near2);
+    const unsigned mh = __ballot_sync(0xffffffffu, hit && !is_far);
+    const unsigned mf = __ballot_sync(0xffffffffu, is_far);
+    if (hit && !is_far) {
+      const int pos = nf + __popc(mh & lt);
+      if (pos < cap) row[pos] = j;
+    } else if (is_far) {
+      const int k = nb + __popc(mf & lt);
+      if (k < cap) row[cap - 1 - k] = j;
+    }
+    nf += __popc(mh);
+    nb += __popc(mf);
+  }
+  if (lane == 0) {
+    count[i] = nf + nb;
+    if (far) far[i] = nb;
+    if (nf + nb > cap) atomicOr(overflow, 1);
+  }
+}
+
+int launch_full_list_small(const DBox& b, double cutoff, int n, const double* x, const double* y,
+                           const double* z, int cap, int* count, int* nbrs, int* overflow,
+                           cudaStream_t st, const FarSplit* split) {
+  if (n <= 0) return RBX_OK;
+  // near threshold raised by 1e-9 relative: FP64 rounding never moves a pair
+  // that could come within r_core before the next rebuild to the far segment
+  const double near2 =
+      split ? split->r_near * split->r_near * (1.0 + 1e-9) : (double)INFINITY;
+  k_full_list_small<<<(n + 3) / 4, 128, 0, st>>>(b, cutoff * cutoff, near2, n, x, y, z, cap,
+                                                 count, nbrs, overflow,
+                                                 split ? split->far : nullptr);
+  count_launch();
+  return check_launch("full_list_small");
+}
+
+// ---------------------------------------------------------------------------
 // Gathers / scatters and integration.
 // ---------------------------------------------------------------------------
 __global__ void k_fill_i32(int n, int* __restrict__ p, int v) {
@@ -614,6 +676,8 @@ int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, con
                      const FarSplit* split) {
   const int ncell = dims[0] * dims[1] * dims[2];
   if (n <= 0) return RBX_OK;
+  if (dims[0] < 3 || dims[1] < 3 || dims[2] < 3)
+    return launch_full_list_small(b, cutoff, n, x, y, z, cap, count, nbrs, overflow, st, split);
   const double cut2 = cutoff * cutoff;
   double emax = 0.0;
   for (int d = 0; d < 3; ++d) emax = fmax(emax, b.len[d] / dims[d]);

@@ -153,7 +153,10 @@ int rbx_engine::init() {
                 prm.cut_off + prm.skin, 0.5 * dbox.len[d], d);
       return RBX_ERR_CONFIG;
     }
-  ETRY(rbx_cell_grid(&box, prm.cut_off + prm.skin, dims));
+  // cells of edge >= cut_off + skin, floor(L / (cut_off + skin)) per axis (at
+  // least two, by the check above); with fewer than three along an axis the
+  // candidate rows come from the all-pairs builder instead of the stencil
+  for (int d = 0; d < 3; ++d) dims[d] = (int)floor(dbox.len[d] / (prm.cut_off + prm.skin));
   ncell = dims[0] * dims[1] * dims[2];
   freq = rbl ? rbl_freq(n, box, prm.r_core, prm.cut_off, prm.neighbor_sample_num) : 1;
   div = make_divtest(freq);
