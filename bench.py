@@ -685,7 +685,10 @@ def run_water(args):
 
     from rbmd_b200 import rbx, systems
 
-    s = systems.water(args.water_mol, seed=7, kspace_p=args.water_p, dt=args.water_dt)
+    coulomb = args.water_coulomb
+    P = args.water_p if coulomb == "RBE" else -(-args.water_p // 16) * 16  # RBSOG: multiple of 16
+    s = systems.water(args.water_mol, seed=7, kspace_p=P, dt=args.water_dt,
+                      rbsog_level=args.rbsog_level)
     p = s["params"]
     L = np.asarray(s["hi"]) - np.asarray(s["lo"])
     damp = args.water_damp
@@ -693,7 +696,7 @@ def run_water(args):
     tdof = 2.0 * s["n"] - 3  # 3N - 3 - N with SHAKE (Computedof)
 
     def make(sysd, precision, seed=77):
-        e = rbx.Engine(sysd, precision=precision, seed=seed)
+        e = rbx.Engine(sysd, precision=precision, seed=seed, coulomb=coulomb)
         e.set_shake(s["clusters"], systems.WATER_BOND, systems.WATER_ANGLE)
         e.set_special(ns, sp, (0.0, 0.0, 0.0))
         return e
@@ -711,7 +714,9 @@ def run_water(args):
     # force accuracy of the mixed form, same state and k-samples
     from oracle import oracle as O
 
-    m = O.rbe_sample_philox(O.Box.make(s["lo"], s["hi"]), p["alpha"], args.water_p, 5, 0)
+    wbox = O.Box.make(s["lo"], s["hi"])
+    m = (O.rbe_sample_philox(wbox, p["alpha"], P, 5, 0) if coulomb == "RBE" else
+         O.rbsog_sample_philox(args.rbsog_level, p["cut_off"], wbox, P, 5, 0))
     forces = {}
     for prec in (rbx.PLAIN_FP64, rbx.MIXED):
         e = make(s_eq, prec)
@@ -755,7 +760,7 @@ def run_water(args):
                      "temperature_end": e.thermostat()["temperature"]}
         e.close()
     line = {
-        "metric": "rigid water (CVFF special bonds, RBL + RBE, SHAKE, NVT): atom-steps/s",
+        "metric": f"rigid water (CVFF special bonds, RBL + {coulomb}, SHAKE, NVT): atom-steps/s",
         "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": out["mixed"]["ms_per_step"],
         "higher_is_better": True, "scaling": "weak",
@@ -763,7 +768,10 @@ def run_water(args):
         "data": "synthetic",
         "config": {"workload": f"{args.water_mol} rigid 3-site waters ({s['n']} atoms), L = "
                                f"{float(L[0]):.2f} A, REAL, cut_off 10 r_core 6.5 skin 2, "
-                               f"RBE alpha 0.09 P={args.water_p}, special_bonds [0 0 0], SHAKE "
+                               + (f"RBE alpha 0.09 P={P}" if coulomb == "RBE" else
+                                  f"RBSOG rbsog_level {args.rbsog_level} P={P} (+6 direct "
+                                  f"vectors), real-space alpha 0.09")
+                               + ", special_bonds [0 0 0], SHAKE "
                                f"(1.0 A, 109.47 deg), Nose-Hoover 298 K / {damp} fs, "
                                f"dt = {args.water_dt} fs",
                    "equilibration_steps": args.water_equil, "temperature_after_equil": t_equil},
@@ -996,6 +1004,8 @@ def main():
                     help="rigid-water (CVFF, SHAKE, NVT) measurement instead of the headline line")
     ap.add_argument("--water-mol", type=int, default=24327)
     ap.add_argument("--water-p", type=int, default=300)
+    ap.add_argument("--water-coulomb", choices=("RBE", "RBSOG"), default="RBE",
+                    help="k-space of the water run; RBSOG rounds P up to a multiple of 16")
     ap.add_argument("--water-dt", type=float, default=0.5)
     ap.add_argument("--water-damp", type=float, default=10.0)
     ap.add_argument("--water-equil", type=int, default=2000)
