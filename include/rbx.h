@@ -182,12 +182,30 @@ int rbx_rbsog_sample(const rbx_box* box, int level, double cut_off, int p, uint6
  * fac = 1).  S = 0 uses RBSOGSetup's S (the reference's forces), S < 0
  * the full normalisation S_full (an unbiased far field), S > 0 that value;
  * qsqsum = sum q^2.  Device arrays;
- * energy (host, may be NULL).  The virial is not computed. */
+ * energy (host, may be NULL).  The virial is rbx_rbsog_virial. */
 int rbx_rbsog_force(const rbx_box* box, int level, double cut_off, double qqr2e, double S,
                     double qsqsum, int num_atoms, int p, const double* charge, const double* mx,
                     const double* my, const double* mz, const double* px, const double* py,
                     const double* pz, double* fx, double* fy, double* fz, double* energy,
                     void* stream);
+/* The NPT gather map of the p samples (the virial's chain in
+ * RBSOGSampleKSpace, kspace_calculator.cpp:1242-1301): an independence
+ * Metropolis chain over the samples with target Gaussian_modify(m) |k|^4 and
+ * proposal Gaussian(m) |k|^2; idx_npt[0] = 0, idx_npt[i] = i when accepted,
+ * else idx_npt[i - 1].  The uniforms are Philox4x32-10 draws of counter
+ * {i, 0x4e505400, step} under key seed (the sampler's key).  Device arrays. */
+int rbx_rbsog_npt_chain(const rbx_box* box, int level, double cut_off, int p, const double* mx,
+                        const double* my, const double* mz, uint64_t seed, int64_t step,
+                        int* idx_npt, void* stream);
+/* RBSOG k-space virial[6] (host; xx, yy, zz, xy, xz, yz) of the p samples with
+ * their gather map idx_npt (device) plus the six |m| = 1 vectors, at a fixed
+ * box (fac = fac_npt = 1): ComputeRBSOGSampleVirialKernel +
+ * ComputeRBSOGDirectVirialKernel (kspace_calculator_op.hip.cu:1133-1190,
+ * 1308-1355).  S as rbx_rbsog_force; S_npt <= 0 uses RBSOGSetup's S_npt. */
+int rbx_rbsog_virial(const rbx_box* box, int level, double cut_off, double qqr2e, double S,
+                     double S_npt, int num_atoms, int p, const double* charge, const double* mx,
+                     const double* my, const double* mz, const int* idx_npt, const double* px,
+                     const double* py, const double* pz, double* virial, void* stream);
 /* VERLET-SOG pair force over a full candidate list (LJCutCoulForceUserOp:
  * ComputeLJCutCoulForceUserKernel with lj126 and CoulCutForceUser,
  * lj_cut_coul_kspace_op.hip.cu:196-254, 357-470): LJ 12-6 plus the
@@ -440,7 +458,8 @@ typedef struct {
   int candidate_capacity;   /* row capacity of the candidate list */
   int64_t candidates;       /* candidate pairs in the list at the last rebuild */
   double e_kspace;          /* last RBE energy (only if requested) */
-  double virial_kspace[6];
+  double virial_kspace[6];  /* last k-space virial (xx, yy, zz, xy, xz, yz); RBSOG:
+                               sampled + direct with the NPT gather chain */
 } rbx_stats;
 
 rbx_engine* rbx_engine_create(const rbx_params* params, const rbx_box* box,
@@ -629,6 +648,9 @@ int rbx_engine_kspace_energy_exact(rbx_engine* e, const int kmax[3], double* ene
 int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core,
                              int* shell_pairs, int64_t* n_shell);
 int rbx_engine_get_stats(rbx_engine* e, rbx_stats* out);
+/* RBSOG engines: *p = P, and with idx_npt (host int[P], may be NULL) the NPT
+ * gather map (see rbx_rbsog_npt_chain) of the last force evaluation's samples. */
+int rbx_engine_rbsog_npt_map(rbx_engine* e, int* p, int* idx_npt);
 /* Stream the engine launches on (cudaStream_t as void*). */
 void* rbx_engine_stream(rbx_engine* e);
 /* Mean device time per step since profiling was switched on, per phase, in

@@ -74,7 +74,20 @@ def lib():
             "orc_rbe_sample_philox": (C.c_int, [C.c_int, B, C.c_double, C.c_uint64,
                                                 C.c_int64, _dp, _dp, _dp]),
             "orc_rbe_sample_mh": (None, [C.c_int, B, C.c_double, C.c_uint64, _dp, _dp, _dp]),
-            "orc_rbsog_params": (C.c_int, [C.c_int, C.c_double, B, _dp, _dp, _ip, _dp]),
+            "orc_rbsog_params": (C.c_int, [C.c_int, C.c_double, B, _dp, _dp, _ip, _dp, _dp,
+                                           _dp]),
+            "orc_rbsog_npt_uniforms": (None, [C.c_uint64, C.c_int64, C.c_int, _dp]),
+            "orc_shake_a_op": (C.c_int, [C.c_int, B, _ip, _ip, _dp, C.c_int, C.c_double,
+                                         C.c_double, C.c_int, _ip, C.c_double, C.c_double, _dp,
+                                         _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_void_p]),
+            "orc_shake_b_op": (C.c_int, [C.c_int, B, _ip, _ip, _dp, C.c_int, C.c_double,
+                                         C.c_double, C.c_int, _ip, C.c_double, C.c_double, _dp,
+                                         _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+            "orc_rbsog_idx_npt": (C.c_int, [C.c_int, C.c_double, B, C.c_int, _dp, _dp, _dp, _dp,
+                                            _ip]),
+            "orc_rbsog_virial": (C.c_int, [C.c_int, C.c_double, B, C.c_double, C.c_double,
+                                           C.c_double, C.c_int, C.c_int, _dp, _dp, _dp, _dp,
+                                           _ip, _dp, _dp, _dp, _dp]),
             "orc_rbsog_sample_philox": (C.c_int, [C.c_int, C.c_double, B, C.c_int, C.c_uint64,
                                                   C.c_int64, _dp, _dp, _dp]),
             "orc_rbsog_sample_mh": (C.c_int, [C.c_int, C.c_double, B, C.c_int, C.c_uint64,
@@ -244,14 +257,76 @@ def rbsog_params(level, cut_off, box):
     """RBSOGInit / RBSOGSetup / LJCoulSOGInit parameters (kspace_calculator.cpp:988-1140)."""
     sc = np.zeros(13)
     coef = np.zeros(128)
+    coef_npt = np.zeros(128)
     dm = np.zeros(18, dtype=np.int32)
     dfb = np.zeros(6)
-    if lib().orc_rbsog_params(level, cut_off, C.byref(box), sc, coef, dm, dfb) != 0:
+    dfb_npt = np.zeros(6)
+    if lib().orc_rbsog_params(level, cut_off, C.byref(box), sc, coef, dm, dfb, coef_npt,
+                              dfb_npt) != 0:
         raise ValueError("rbsog_level outside [0, 4]")
     mmax = int(sc[0])
     return {"mmax": mmax, "b": sc[1], "sigma": sc[2], "w0": sc[3], "S": sc[4], "S_npt": sc[5],
             "self_coeff": sc[6], "taylor": sc[7:13].copy(), "coef": coef[:mmax].copy(),
-            "direct_m": dm.reshape(6, 3), "direct_fb": dfb}
+            "coef_npt": coef_npt[:mmax].copy(), "direct_m": dm.reshape(6, 3), "direct_fb": dfb,
+            "direct_fb_npt": dfb_npt}
+
+
+def rbsog_idx_npt(level, cut_off, box, m, u):
+    """The NPT gather chain of RBSOGSampleKSpace (kspace_calculator.cpp:1242-1301) on the
+    samples m with the uniforms u."""
+    p = len(m[0])
+    idx = np.zeros(p, dtype=np.int32)
+    lib().orc_rbsog_idx_npt(level, cut_off, C.byref(box), p, *[_d(v) for v in m],
+                            _d(np.asarray(u, dtype=np.float64)), idx)
+    return idx
+
+
+def rbsog_npt_uniforms(seed, step, p):
+    """The uniforms the device NPT chain draws for (seed, step)."""
+    u = np.zeros(p)
+    lib().orc_rbsog_npt_uniforms(seed, step, p, u)
+    return u
+
+
+def shake_a(box, gid, typ, mass, dt, fmt2v, clusters, bond, angle_deg, pos, vel, force):
+    """ShakeAOp at op level: half kick + drift of (pos, vel) with force, then the
+    constraint of the (H, O, H) global-id clusters; returns (pos, vel, images, failures)."""
+    n = len(gid)
+    p = [np.ascontiguousarray(pos[:, d], dtype=np.float64).copy() for d in range(3)]
+    v = [np.ascontiguousarray(vel[:, d], dtype=np.float64).copy() for d in range(3)]
+    f = [np.ascontiguousarray(force[:, d], dtype=np.float64) for d in range(3)]
+    img = np.zeros(3 * n, dtype=np.int32)
+    cl = np.ascontiguousarray(clusters, dtype=np.int32)
+    fails = lib().orc_shake_a_op(n, C.byref(box), _i(np.asarray(gid, dtype=np.int32)),
+                                 _i(np.asarray(typ, dtype=np.int32)),
+                                 _d(np.asarray(mass, dtype=np.float64)), len(mass), dt, fmt2v,
+                                 len(cl), _i(cl), bond, angle_deg, *p, *v, *f,
+                                 img.ctypes.data_as(C.c_void_p))
+    return np.stack(p, 1), np.stack(v, 1), img.reshape(3, n), fails
+
+
+def shake_b(box, gid, typ, mass, dt, fmt2v, clusters, bond, angle_deg, pos, vel, force):
+    """ShakeBOp at op level: half kick of vel with force, then RATTLE; returns (vel, failures)."""
+    n = len(gid)
+    p = [np.ascontiguousarray(pos[:, d], dtype=np.float64) for d in range(3)]
+    v = [np.ascontiguousarray(vel[:, d], dtype=np.float64).copy() for d in range(3)]
+    f = [np.ascontiguousarray(force[:, d], dtype=np.float64) for d in range(3)]
+    cl = np.ascontiguousarray(clusters, dtype=np.int32)
+    fails = lib().orc_shake_b_op(n, C.byref(box), _i(np.asarray(gid, dtype=np.int32)),
+                                 _i(np.asarray(typ, dtype=np.int32)),
+                                 _d(np.asarray(mass, dtype=np.float64)), len(mass), dt, fmt2v,
+                                 len(cl), _i(cl), bond, angle_deg, *p, *v, *f)
+    return np.stack(v, 1), fails
+
+
+def rbsog_virial(level, cut_off, box, qqr2e, q, m, idx, x, y, z, S=0.0, S_npt=0.0):
+    """RBSOG k-space virial [6] (xx, yy, zz, xy, xz, yz): sampled part with the NPT terms over
+    K[idx] plus the direct vectors (kspace_calculator_op.hip.cu:1133-1190, 1308-1355)."""
+    v = np.zeros(6)
+    lib().orc_rbsog_virial(level, cut_off, C.byref(box), qqr2e, S, S_npt, len(q), len(m[0]),
+                           _d(q), *[_d(c) for c in m], _i(np.asarray(idx, dtype=np.int32)),
+                           _d(x), _d(y), _d(z), v)
+    return v
 
 
 def rbsog_sample_philox(level, cut_off, box, p, seed, step):

@@ -1343,6 +1343,83 @@ static void shake_b(orc_engine* e) {
     }
   }
 }
+/* ShakeAOp / ShakeBOp at op level (shake_controller_op.hip.cu:1188-1238) for
+ * atoms i = 0..n-1 with global ids gid[i], on caller arrays:
+ * A: from the positions p (in the box) and velocities v before the step and
+ * the forces f, the half kick and drift of the unconstrained update, then the
+ * constraint; writes p (wrapped into the box, image counters img[3][n]
+ * updated) and v.  B: RATTLE of v at positions p with the forces f of the new
+ * positions after the second half kick; writes v.  Clusters are (H, O, H)
+ * global-id triples; the constraint geometry is bond / angle_deg.  Returns
+ * the number of clusters whose iteration failed. */
+static void shk_view(orc_engine* e, int n, const orc_box* box, const int* gid, const int* type,
+                     const double* mass, int ntypes, double dt, double fmt2v) {
+  memset(e, 0, sizeof(*e));
+  e->n = n;
+  e->box = *box;
+  e->dt = dt;
+  e->fmt2v = fmt2v;
+  e->gid = (int*)gid;
+  e->type = (int*)type;
+  for (int t = 0; t < ntypes && t < 64; ++t) e->mass[t] = mass[t];
+}
+
+int orc_shake_a_op(int n, const orc_box* box, const int* gid, const int* type, const double* mass,
+                   int ntypes, double dt, double fmt2v, int nc, const int* clusters, double bond,
+                   double angle_deg, double* px, double* py, double* pz, double* vx, double* vy,
+                   double* vz, const double* fx, const double* fy, const double* fz, int* img) {
+  orc_engine e;
+  shk_view(&e, n, box, gid, type, mass, ntypes, dt, fmt2v);
+  e.x = px; e.y = py; e.z = pz;
+  e.vx = vx; e.vy = vy; e.vz = vz;
+  e.fx = (double*)fx; e.fy = (double*)fy; e.fz = (double*)fz;
+  if (orc_engine_set_shake(&e, nc, clusters, bond, angle_deg) != 0) return -1;
+  engine_kick(&e);
+  memcpy(e.xs, px, sizeof(double) * (size_t)n);
+  memcpy(e.ys, py, sizeof(double) * (size_t)n);
+  memcpy(e.zs, pz, sizeof(double) * (size_t)n);
+  const double L[3] = {box_len(box, 0), box_len(box, 1), box_len(box, 2)};
+  double* pos[3] = {px, py, pz};
+  const double* vel[3] = {vx, vy, vz};
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) {
+      double s = pos[d][i] + vel[d][i] * dt;
+      if (s >= box->hi[d]) { s -= L[d]; if (img) img[d * n + i]++; }
+      if (s < box->lo[d]) { s += L[d]; if (img) img[d * n + i]--; }
+      pos[d][i] = s;
+    }
+  shake_a(&e);
+  const int fails = e.shake_failures;
+  free(e.shake_gid);
+  free(e.where);
+  free(e.xs);
+  free(e.ys);
+  free(e.zs);
+  return fails;
+}
+
+int orc_shake_b_op(int n, const orc_box* box, const int* gid, const int* type, const double* mass,
+                   int ntypes, double dt, double fmt2v, int nc, const int* clusters, double bond,
+                   double angle_deg, const double* px, const double* py, const double* pz,
+                   double* vx, double* vy, double* vz, const double* fx, const double* fy,
+                   const double* fz) {
+  orc_engine e;
+  shk_view(&e, n, box, gid, type, mass, ntypes, dt, fmt2v);
+  e.x = (double*)px; e.y = (double*)py; e.z = (double*)pz;
+  e.vx = vx; e.vy = vy; e.vz = vz;
+  e.fx = (double*)fx; e.fy = (double*)fy; e.fz = (double*)fz;
+  if (orc_engine_set_shake(&e, nc, clusters, bond, angle_deg) != 0) return -1;
+  engine_kick(&e);
+  shake_b(&e);
+  const int fails = e.shake_failures;
+  free(e.shake_gid);
+  free(e.where);
+  free(e.xs);
+  free(e.ys);
+  free(e.zs);
+  return fails;
+}
+
 static void engine_drift(orc_engine* e) {
   const double L[3] = {box_len(&e->box, 0), box_len(&e->box, 1), box_len(&e->box, 2)};
 #pragma omp parallel for schedule(static)
@@ -1520,7 +1597,7 @@ typedef struct {
   double b, sigma, w0, S, S_npt, self_coeff, taylor[6];
   double coef[128], coef_npt[128];
   int dm[18];
-  double dfb[6];
+  double dfb[6], dfb_npt[6];
 } orc_sog;
 
 static double sog_g1(double r) { return exp(-r * r / 2.0) / sqrt(2 * M_PI); }
@@ -1602,6 +1679,7 @@ static int sog_setup(int level, double cut_off, const orc_box* box, orc_sog* s) 
         s->dm[3 * nd] = i;
         s->dm[3 * nd + 1] = j;
         s->dm[3 * nd + 2] = k;
+        s->dfb_npt[nd] = sog_ghat(s, s->coef_npt, Kx * Kx + Ky * Ky + Kz * Kz);
         s->dfb[nd++] = sog_ghat(s, s->coef, Kx * Kx + Ky * Ky + Kz * Kz);
       }
   s->self_coeff = (logb / (sqrt(2 * M_PI) * s->sigma)) *
@@ -1621,7 +1699,7 @@ static int sog_setup(int level, double cut_off, const orc_box* box, orc_sog* s) 
 }
 
 int orc_rbsog_params(int level, double cut_off, const orc_box* box, double* scal,
-                     double* coef, int* dm, double* dfb) {
+                     double* coef, int* dm, double* dfb, double* coef_npt, double* dfb_npt) {
   orc_sog s;
   if (sog_setup(level, cut_off, box, &s)) return -1;
   /* scal: mmax, b, sigma, w0, S, S_npt, self_coeff, taylor[6] */
@@ -1632,6 +1710,106 @@ int orc_rbsog_params(int level, double cut_off, const orc_box* box, double* scal
   if (coef) memcpy(coef, s.coef, sizeof(double) * (size_t)s.mmax);
   if (dm) memcpy(dm, s.dm, sizeof s.dm);
   if (dfb) memcpy(dfb, s.dfb, sizeof s.dfb);
+  if (coef_npt) memcpy(coef_npt, s.coef_npt, sizeof(double) * (size_t)s.mmax);
+  if (dfb_npt) memcpy(dfb_npt, s.dfb_npt, sizeof s.dfb_npt);
+  return 0;
+}
+
+/* The NPT gather chain of RBSOGSampleKSpace (kspace_calculator.cpp:1242-1301):
+ * idx[0] = 0; sample i proposes itself against the sample idx[i - 1] and is
+ * accepted when u[i] < min(1, pup qup / (pdown qdown)) with
+ * p(m) = Gaussian_modify(m) |k|^4 (coef_npt) and q(m) = Gaussian(m) |k|^2
+ * (coef); u[i] are the caller's uniforms on [0, 1). */
+int orc_rbsog_idx_npt(int level, double cut_off, const orc_box* box, int p, const double* mx,
+                      const double* my, const double* mz, const double* u, int* idx) {
+  orc_sog s;
+  if (sog_setup(level, cut_off, box, &s)) return -1;
+  if (p <= 0) return 0;
+  const double L[3] = {box_len(box, 0), box_len(box, 1), box_len(box, 2)};
+  idx[0] = 0;
+  for (int i = 1; i < p; ++i) {
+    const int o = idx[i - 1];
+    const double mn[3] = {mx[i], my[i], mz[i]}, mo[3] = {mx[o], my[o], mz[o]};
+    double k2n = 0.0, k2o = 0.0, K2n = 0.0, K2o = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      k2n += pow((mn[d] + 0.00) * 2 * M_PI / L[d], 2);
+      k2o += pow((mo[d] + 0.00) * 2 * M_PI / L[d], 2);
+      const double kn = (2 * M_PI / L[d]) * mn[d], ko = (2 * M_PI / L[d]) * mo[d];
+      K2n += kn * kn;
+      K2o += ko * ko;
+    }
+    const double pup = sog_ghat(&s, s.coef_npt, k2n) * (K2n * K2n);
+    const double qup = sog_ghat(&s, s.coef, k2o) * K2o;
+    const double pdown = sog_ghat(&s, s.coef_npt, k2o) * (K2o * K2o);
+    const double qdown = sog_ghat(&s, s.coef, k2n) * K2n;
+    const double r = pup * qup / (pdown * qdown);
+    const double acce = r > 1.0 ? 1.0 : r;
+    idx[i] = u[i] < acce ? i : o;
+  }
+  return 0;
+}
+
+/* RBSOG k-space virial [6] (xx, yy, zz, xy, xz, yz) at a fixed box (fac =
+ * fac_npt = 1): ComputeRBSOGSampleVirialKernel (kspace_calculator_op.hip.cu:
+ * 1133-1190) over the P samples with K_npt = K[idx[j]], plus
+ * ComputeRBSOGDirectVirialKernel (:1308-1355) over the 6 direct vectors.
+ * S, S_npt <= 0 take RBSOGSetup's values. */
+int orc_rbsog_virial(int level, double cut_off, const orc_box* box, double qqr2e, double S,
+                     double S_npt, int n, int p, const double* q, const double* mx,
+                     const double* my, const double* mz, const int* idx, const double* x,
+                     const double* y, const double* z, double* virial) {
+  orc_sog s;
+  if (sog_setup(level, cut_off, box, &s)) return -1;
+  const double L[3] = {box_len(box, 0), box_len(box, 1), box_len(box, 2)};
+  const double V = L[0] * L[1] * L[2];
+  const double Su = S > 0 ? S : s.S, Sn = S_npt > 0 ? S_npt : s.S_npt;
+  const int pt = p + 6;
+  double* K = (double*)malloc(sizeof(double) * 3 * (size_t)(pt > 0 ? pt : 1));
+  double* r2 = (double*)calloc((size_t)(pt > 0 ? pt : 1), sizeof(double));
+  for (int k = 0; k < pt; ++k) {
+    const double m[3] = {k < p ? mx[k] : s.dm[3 * (k - p)], k < p ? my[k] : s.dm[3 * (k - p) + 1],
+                         k < p ? mz[k] : s.dm[3 * (k - p) + 2]};
+    for (int d = 0; d < 3; ++d) K[3 * k + d] = m[d] * (2 * M_PI / L[d]);
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < pt; ++k) {
+    double re = 0.0, im = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double ph = K[3 * k] * x[i] + K[3 * k + 1] * y[i] + K[3 * k + 2] * z[i];
+      re += q[i] * cos(ph);
+      im += q[i] * sin(ph);
+    }
+    r2[k] = re * re + im * im;
+  }
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  const double mv = (Su / p) * qqr2e / (2.0 * V), mn = -(Sn / p) * qqr2e / (4.0 * V);
+  for (int j = 0; j < p; ++j) {
+    const double* Kj = K + 3 * j;
+    const double* Kn = K + 3 * idx[j];
+    const double k2 = Kj[0] * Kj[0] + Kj[1] * Kj[1] + Kj[2] * Kj[2];
+    const double kn2 = Kn[0] * Kn[0] + Kn[1] * Kn[1] + Kn[2] * Kn[2];
+    const double c1 = r2[j] / k2, c2 = r2[idx[j]] / (kn2 * kn2);
+    v[0] += c1 * mv + c2 * mn * Kn[0] * Kn[0];
+    v[1] += c1 * mv + c2 * mn * Kn[1] * Kn[1];
+    v[2] += c1 * mv + c2 * mn * Kn[2] * Kn[2];
+    v[3] += c2 * mn * Kn[0] * Kn[1];
+    v[4] += c2 * mn * Kn[0] * Kn[2];
+    v[5] += c2 * mn * Kn[1] * Kn[2];
+  }
+  const double c1v = qqr2e / (2.0 * V), c2v = -qqr2e / (4.0 * V);
+  for (int d = 0; d < 6; ++d) {
+    const double* Kd = K + 3 * (p + d);
+    const double a = c1v * s.dfb[d] * r2[p + d], b2 = c2v * s.dfb_npt[d] * r2[p + d];
+    v[0] += a + b2 * Kd[0] * Kd[0];
+    v[1] += a + b2 * Kd[1] * Kd[1];
+    v[2] += a + b2 * Kd[2] * Kd[2];
+    v[3] += b2 * Kd[0] * Kd[1];
+    v[4] += b2 * Kd[0] * Kd[2];
+    v[5] += b2 * Kd[1] * Kd[2];
+  }
+  memcpy(virial, v, sizeof v);
+  free(K);
+  free(r2);
   return 0;
 }
 
@@ -1700,6 +1878,20 @@ static int sog_first_above(const double* cdf, int cnt, double target) {
 
 static double sog_u53(uint32_t hi, uint32_t lo) {
   return (double)(((((uint64_t)hi) << 32) | lo) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* Uniforms of the device NPT chain: Philox4x32-10 of counter
+ * {i, 0x4e505400, step lo, step hi} under the sampler's key, u = the top 53
+ * bits of the first two words. */
+void orc_rbsog_npt_uniforms(uint64_t seed, int64_t step, int p, double* u) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int i = 0; i < p; ++i) {
+    const uint32_t c0[4] = {(uint32_t)i, 0x4e505400u, (uint32_t)step,
+                            (uint32_t)((uint64_t)step >> 32)};
+    uint32_t c[4];
+    orc_philox4x32_10(c0, key, c);
+    u[i] = sog_u53(c[0], c[1]);
+  }
 }
 
 int orc_rbsog_sample_philox(int level, double cut_off, const orc_box* box, int p, uint64_t seed,

@@ -61,4 +61,40 @@ int ref_ewald_force(const double* lo, const double* hi, int n, const int* kmax, 
   return ref_sync();
 }
 
+/* RBSOG far field as ComputeRBSOG runs it (kspace_calculator.cpp:1331-1530):
+ * ρ(k) of the P sampled vectors (ComputePnumberChargeStructureFactorSOGOp),
+ * ComputeRBSOGSampleForceOp (force, energy_parts[0], virial with the NPT
+ * terms over K_npt = K[idx_npt]), then ρ(k) of the direct vectors and
+ * ComputeRBSOGDirectForceOp (force, energy, virial), both accumulating into the
+ * same energy and virial buffers as the host code passes them.  K, K_npt and
+ * the direct vectors are Cartesian (2π m / L); fac / fac_npt as
+ * ComputeRBSOGFactorOp leaves them at a fixed box (all ones).  Outputs go to
+ * separate force arrays per part. */
+int ref_rbsog(const double* lo, const double* hi, int n, int p, double qqr2e, double S0,
+              double S_npt, const rbmd::Real* kx, const rbmd::Real* ky, const rbmd::Real* kz,
+              const rbmd::Real* knx, const rbmd::Real* kny, const rbmd::Real* knz,
+              const int* idx_npt, const rbmd::Real* fac, const rbmd::Real* fac_npt, int nd,
+              const rbmd::Real* dx, const rbmd::Real* dy, const rbmd::Real* dz,
+              const rbmd::Real* fb, const rbmd::Real* fb_npt, const rbmd::Real* q,
+              const rbmd::Real* x, const rbmd::Real* y, const rbmd::Real* z, rbmd::Real* rho_re,
+              rbmd::Real* rho_im, rbmd::Real* drho_re, rbmd::Real* drho_im, rbmd::Real* fsx,
+              rbmd::Real* fsy, rbmd::Real* fsz, rbmd::Real* fdx, rbmd::Real* fdy,
+              rbmd::Real* fdz, rbmd::Real* virial_sample, rbmd::Real* virial_direct,
+              rbmd::Real* energy_parts) {
+  const Box box = ref_make_box(lo, hi);
+  op::ComputePnumberChargeStructureFactorSOGOp<device::DEVICE_GPU>()(box, n, p, q, kx, ky, kz, x,
+                                                                     y, z, rho_re, rho_im);
+  op::ComputeRBSOGSampleForceOp<device::DEVICE_GPU>()(
+      box, n, p, (rbmd::Real)qqr2e, (rbmd::Real)S0, (rbmd::Real)S_npt, kx, ky, kz, knx, kny, knz,
+      idx_npt, fac, fac_npt, rho_re, rho_im, q, x, y, z, fsx, fsy, fsz, virial_sample,
+      energy_parts);
+  op::ComputeDirectChargeStructureFactorOp<device::DEVICE_GPU>()(n, nd, dx, dy, dz, q, x, y, z,
+                                                                 drho_re, drho_im);
+  op::ComputeRBSOGDirectForceOp<device::DEVICE_GPU>()(box, n, nd, (rbmd::Real)qqr2e, dx, dy, dz,
+                                                      fb, fb_npt, drho_re, drho_im, q, x, y, z,
+                                                      fdx, fdy, fdz, virial_direct,
+                                                      energy_parts + 1);
+  return ref_sync();
+}
+
 }  // extern "C"

@@ -135,6 +135,7 @@ RbsogSetup rbsog_setup(int level, double cut_off, const rbx_box& box) {
                        Kz = (2 * M_PI / L[2]) * (k + 0.00);
           s.direct_m.insert(s.direct_m.end(), {i, j, k});
           s.direct_fb.push_back(gaussian_k(Kx * Kx + Ky * Ky + Kz * Kz, s, s.coef));
+          s.direct_fb_npt.push_back(gaussian_k(Kx * Kx + Ky * Ky + Kz * Kz, s, s.coef_npt));
         }
   s.self_coeff = (logb / (std::sqrt(2 * M_PI) * s.sigma)) *
                  (s.w0 + (1 - std::pow(s.b, -s.mmax + 0.0)) / (s.b - 1));

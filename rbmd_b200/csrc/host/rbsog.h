@@ -18,6 +18,7 @@ struct RbsogSetup {
   // the |m|^2 <= Kcut = 1 vectors summed directly, and their weights G^(k)
   std::vector<int> direct_m;           // [6][3]
   std::vector<double> direct_fb;       // [6]
+  std::vector<double> direct_fb_npt;   // [6], with coef_npt (virial)
   // exact sampler of p(m) ~ G^(m) |k|^2: a mixture over (Gaussian l, axis d)
   // of separable densities; per (l, axis, kind) a cumulative table over the
   // order m = 0, +1, -1, +2, -2, ... (kind 0: g_l(m), kind 1: k^2 g_l(m))

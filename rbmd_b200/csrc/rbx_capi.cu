@@ -814,6 +814,131 @@ int rbx_rbsog_force(const rbx_box* box, int level, double cut_off, double qqr2e,
   return rc;
 }
 
+static SogGauss sog_gauss_upload(const rbx_host::RbsogSetup& s, double** coef, cudaStream_t st,
+                                 int* rc) {
+  *rc = async_alloc(coef, 2 * (size_t)s.mmax, st);
+  if (*rc) return SogGauss{};
+  cudaMemcpyAsync(*coef, s.coef.data(), sizeof(double) * s.mmax, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(*coef + s.mmax, s.coef_npt.data(), sizeof(double) * s.mmax,
+                  cudaMemcpyHostToDevice, st);
+  return SogGauss{*coef, *coef + s.mmax, s.mmax, s.b * s.b, s.sigma * s.sigma};
+}
+
+int rbx_rbsog_npt_chain(const rbx_box* box, int level, double cut_off, int p, const double* mx,
+                        const double* my, const double* mz, uint64_t seed, int64_t step,
+                        int* idx_npt, void* stream) {
+  RBX_CHECK_BOX(box);
+  if (p <= 0 || !mx || !my || !mz || !idx_npt) {
+    set_error("rbx_rbsog_npt_chain: need p > 0 and the arrays");
+    return RBX_ERR_INVALID;
+  }
+  rbx_host::RbsogSetup s;
+  RBX_TRY(rbsog_setup_checked(level, cut_off, box, &s));
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  double* coef = nullptr;
+  int* mult = nullptr;
+  int rc = 0;
+  const SogGauss g = sog_gauss_upload(s, &coef, st, &rc);
+  if (!rc) rc = async_alloc(&mult, (size_t)p, st);
+  if (!rc)
+    rc = launch_rbsog_npt_chain(make_dbox(*box), p, mx, my, mz, g, seed, (uint64_t)step, nullptr,
+                                idx_npt, mult, st);
+  if (!rc) rc = cuda_ok(cudaStreamSynchronize(st), "rbx_rbsog_npt_chain");
+  for (void* ptr : {(void*)coef, (void*)mult})
+    if (ptr) cudaFreeAsync(ptr, st);
+  return rc;
+}
+
+int rbx_rbsog_virial(const rbx_box* box, int level, double cut_off, double qqr2e, double S,
+                     double S_npt, int num_atoms, int p, const double* charge, const double* mx,
+                     const double* my, const double* mz, const int* idx_npt, const double* px,
+                     const double* py, const double* pz, double* virial, void* stream) {
+  RBX_CHECK_BOX(box);
+  if (num_atoms < 0 || p <= 0 || !mx || !my || !mz || !idx_npt || !virial) {
+    set_error("rbx_rbsog_virial: need num_atoms >= 0, p > 0 and the arrays");
+    return RBX_ERR_INVALID;
+  }
+  rbx_host::RbsogSetup s;
+  RBX_TRY(rbsog_setup_checked(level, cut_off, box, &s));
+  for (int c = 0; c < 6; ++c) virial[c] = 0.0;
+  if (num_atoms == 0) return RBX_OK;
+  RBX_TRY(require_device());
+  cudaStream_t st = (cudaStream_t)stream;
+  const DBox b = make_dbox(*box);
+  const double V = b.len[0] * b.len[1] * b.len[2];
+  const double Suse = S > 0 ? S : (S < 0 ? s.S_full : s.S);
+  const double Snpt = S_npt > 0 ? S_npt : s.S_npt;
+  const int nd = (int)s.direct_fb.size(), pt = p + nd;
+  // multiplicity of each sample in the gather map
+  std::vector<int> hidx(p), mult(p, 0);
+  int rc = cuda_ok(cudaMemcpyAsync(hidx.data(), idx_npt, sizeof(int) * p, cudaMemcpyDeviceToHost,
+                                   st), "D2H");
+  if (!rc) rc = cuda_ok(cudaStreamSynchronize(st), "rbx_rbsog_virial");
+  if (rc) return rc;
+  for (int i = 0; i < p; ++i) {
+    if (hidx[i] < 0 || hidx[i] >= p) {
+      set_error("rbx_rbsog_virial: idx_npt[%d] = %d outside [0, %d)", i, hidx[i], p);
+      return RBX_ERR_INVALID;
+    }
+    ++mult[hidx[i]];
+  }
+  std::vector<double4> w(pt);
+  std::vector<double> wv(pt), dm(3 * (size_t)nd);
+  for (int k = 0; k < p; ++k) {
+    w[k] = make_double4(0.0, 0.0, Suse * qqr2e / (2.0 * p * V), 0.0);
+    wv[k] = -Snpt * qqr2e / (4.0 * p * V);
+  }
+  for (int k = 0; k < nd; ++k) {
+    w[p + k] = make_double4(0.0, 0.0, 0.0, qqr2e * s.direct_fb[k] / (2.0 * V));
+    wv[p + k] = -qqr2e * s.direct_fb_npt[k] / (4.0 * V);
+    for (int d = 0; d < 3; ++d) dm[3 * k + d] = s.direct_m[3 * k + d];
+  }
+  const int nparts = rbe_partial_blocks(num_atoms);
+  double *m3 = nullptr, *pre = nullptr, *pim = nullptr, *kterm = nullptr, *vw = nullptr,
+         *vout = nullptr;
+  double4* wd = nullptr;
+  int* dmult = nullptr;
+  rc = async_alloc(&m3, 3 * (size_t)pt, st);
+  if (!rc) rc = async_alloc(&wd, (size_t)pt, st);
+  if (!rc) rc = async_alloc(&pre, (size_t)pt * nparts, st);
+  if (!rc) rc = async_alloc(&pim, (size_t)pt * nparts, st);
+  if (!rc) rc = async_alloc(&kterm, 7 * (size_t)pt, st);
+  if (!rc) rc = async_alloc(&vw, (size_t)pt, st);
+  if (!rc) rc = async_alloc(&vout, 6, st);
+  if (!rc) rc = async_alloc(&dmult, (size_t)p, st);
+  if (!rc) {
+    double* mxs[3] = {m3, m3 + pt, m3 + 2 * pt};
+    const double* src[3] = {mx, my, mz};
+    std::vector<double> cols(3 * (size_t)nd);
+    for (int d = 0; d < 3; ++d)
+      for (int k = 0; k < nd; ++k) cols[(size_t)d * nd + k] = dm[3 * k + d];
+    for (int d = 0; d < 3; ++d) {
+      cudaMemcpyAsync(mxs[d], src[d], sizeof(double) * p, cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(mxs[d] + p, cols.data() + (size_t)d * nd, sizeof(double) * nd,
+                      cudaMemcpyHostToDevice, st);
+    }
+    cudaMemcpyAsync(wd, w.data(), sizeof(double4) * pt, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(vw, wv.data(), sizeof(double) * pt, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dmult, mult.data(), sizeof(int) * p, cudaMemcpyHostToDevice, st);
+    rc = launch_rbe_rho_partial_f64(b, num_atoms, pt, mxs[0], mxs[1], mxs[2], charge, px, py, pz,
+                                    pre, pim, nparts, st);
+    const SogVirial sv{p, dmult, vw, kterm + pt, vout};
+    if (!rc)
+      rc = launch_rbsog_finalize(b, pt, nparts, pre, pim, mxs[0], mxs[1], mxs[2], wd, nullptr,
+                                 nullptr, nullptr, kterm, 0.0, nullptr, 0, nullptr, 0, nullptr, st,
+                                 &sv);
+    if (!rc) {
+      cudaMemcpyAsync(virial, vout, sizeof(double) * 6, cudaMemcpyDeviceToHost, st);
+      rc = cuda_ok(cudaStreamSynchronize(st), "rbx_rbsog_virial");
+    }
+  }
+  for (void* ptr : {(void*)m3, (void*)wd, (void*)pre, (void*)pim, (void*)kterm, (void*)vw,
+                    (void*)vout, (void*)dmult})
+    if (ptr) cudaFreeAsync(ptr, st);
+  return rc;
+}
+
 int rbx_pair_force_verlet_sog(const rbx_box* box, int level, double cut_off, double qqr2e,
                               int num_atoms, int ntypes, const double* sigma, const double* eps,
                               const int* type, const double* charge, const double* px,

@@ -503,11 +503,15 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
                                       nparts, st, tun.rho_kpt));
   }
   const int mean_parts = rbl ? nrbl + (spec_natoms ? SPEC_PARTS : 0) : 0;
-  if (sog)
+  if (sog) {
+    if (P > 0)
+      ETRY(launch_rbsog_npt_chain(dbox, P, mx, my, mz, sog_gauss, prm.random_seed,
+                                  (uint64_t)(int64_t)epoch, epoch_dev, sog_idx, sog_mult, st));
+    const SogVirial sv{P, sog_mult, sog_wv, kterm + 2 * (size_t)Pk, virk};
     ETRY(launch_rbsog_finalize(dbox, Pk, nparts, part_re, part_im, mx, my, mz, sog_w, rho_re,
                                rho_im, tab, kterm, -sog_self * qsq * prm.qqr2e, ek, mean_parts,
-                               fpart, n, rbl ? mean : nullptr, st));
-  else
+                               fpart, n, rbl ? mean : nullptr, st, &sv));
+  } else
     ETRY(launch_rbe_finalize(dbox, P, P > 0 ? nparts : 0, part_re, part_im, mx, my, mz,
                              prm.alpha, S, prm.qqr2e, qsq, qsum, P > 0 ? rho_re : nullptr,
                              rho_im, P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr,
@@ -757,6 +761,16 @@ int rbx_engine::init_rbsog() {
       dmi.push_back(s.direct_m[3 * k + d]);
     }
   }
+  // NPT weights of the virial: sampled -S_npt qqr2e / (4 P V) (times the
+  // chain's multiplicity / |k|^4), direct -qqr2e G_npt(k) / (4 V)
+  std::vector<double> wv(Pk);
+  for (int k = 0; k < P; ++k) wv[k] = -s.S_npt * qe / (4.0 * P * V);
+  for (int k = 0; k < 6; ++k) wv[P + k] = -qe * s.direct_fb_npt[k] / (4.0 * V);
+  ETRY(alloc(&sog_wv, (size_t)Pk));
+  ETRY(alloc(&sog_coef, (size_t)s.mmax));
+  ETRY(alloc(&sog_coef_npt, (size_t)s.mmax));
+  ETRY(alloc(&sog_idx, (size_t)(P > 0 ? P : 1)));
+  ETRY(alloc(&sog_mult, (size_t)(P > 0 ? P : 1)));
   ETRY(alloc(&sog_w, (size_t)Pk));
   ETRY(alloc(&sog_cdf, s.comp_cdf.size()));
   ETRY(alloc(&sog_tab, s.tables.size()));
@@ -767,6 +781,10 @@ int rbx_engine::init_rbsog() {
     return cuda_ok(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "H2D");
   };
   ETRY(up(sog_w, w.data(), sizeof(double4) * Pk));
+  ETRY(up(sog_wv, wv.data(), sizeof(double) * Pk));
+  ETRY(up(sog_coef, s.coef.data(), sizeof(double) * s.mmax));
+  ETRY(up(sog_coef_npt, s.coef_npt.data(), sizeof(double) * s.mmax));
+  sog_gauss = SogGauss{sog_coef, sog_coef_npt, s.mmax, s.b * s.b, s.sigma * s.sigma};
   ETRY(up(sog_cdf, s.comp_cdf.data(), sizeof(double) * s.comp_cdf.size()));
   ETRY(up(sog_tab, s.tables.data(), sizeof(double) * s.tables.size()));
   ETRY(up(sog_tot, s.tab_tot.data(), sizeof(double) * s.tab_tot.size()));
@@ -1926,6 +1944,20 @@ int rbx_engine_get_rbl_pairs(rbx_engine* e, int* core_pairs, int64_t* n_core, in
 int rbx_engine_get_stats(rbx_engine* e, rbx_stats* out) {
   if (!e || !out) return RBX_ERR_INVALID;
   return e->get_stats(out);
+}
+
+int rbx_engine_rbsog_npt_map(rbx_engine* e, int* p, int* idx_npt) {
+  if (!e || !p) return RBX_ERR_INVALID;
+  if (!e->sog || e->P <= 0) {
+    set_error("rbx_engine_rbsog_npt_map: not an RBSOG engine with samples");
+    return RBX_ERR_INVALID;
+  }
+  *p = e->P;
+  if (!idx_npt) return RBX_OK;
+  cudaSetDevice(e->device);
+  ETRY(cuda_ok(cudaStreamSynchronize(e->st), "rbx_engine_rbsog_npt_map"));
+  return cuda_ok(cudaMemcpy(idx_npt, e->sog_idx, sizeof(int) * e->P, cudaMemcpyDeviceToHost),
+                 "D2H");
 }
 
 void* rbx_engine_stream(rbx_engine* e) { return e ? (void*)e->st : nullptr; }

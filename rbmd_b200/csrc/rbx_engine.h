@@ -31,6 +31,11 @@ struct rbx_engine {
   double *sog_cdf = nullptr, *sog_tab = nullptr, *sog_tot = nullptr;
   int *sog_off = nullptr, *sog_cnt = nullptr;
   rbx::RbsogTables sog_tables{};
+  // k-space virial: the NPT gather chain over the samples (map, multiplicities),
+  // per-k NPT weights, the Gaussian weights the chain reads
+  double *sog_coef = nullptr, *sog_coef_npt = nullptr, *sog_wv = nullptr;
+  int *sog_idx = nullptr, *sog_mult = nullptr;
+  rbx::SogGauss sog_gauss{};
   rbx::SogPairParams sogp{};
   int init_rbsog();
   double S = 0.0, qsq = 0.0, qsum = 0.0;

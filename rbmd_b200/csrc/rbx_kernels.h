@@ -276,12 +276,37 @@ int launch_rbsog_sample(int p, const RbsogTables& t, uint64_t seed, uint64_t ste
                         int* status, cudaStream_t st);
 // w[k] = {wa, wb, ea, eb}: c_k = (wa / k^2 + wb) / V, e_k = (ea / k^2 + eb) |rho|^2.
 // energy (may be null) needs kterm [p]; E = sum_k e_k + self_energy.
+// Virial (optional): vir = {psamp, mult, vw, vterm, out}.  Sample k < psamp
+// adds e_k to each diagonal entry plus mult[k] vw[k] |rho_k|^2 / |k|^4 k_a k_b;
+// a direct vector k >= psamp adds e_k to the diagonal plus
+// vw[k] |rho_k|^2 k_a k_b; the per-k terms vterm [p][6] are summed in k order
+// into out[6] (xx, yy, zz, xy, xz, yz).
+struct SogVirial {
+  int psamp;
+  const int* mult;
+  const double* vw;
+  double* vterm;
+  double* out;
+};
 int launch_rbsog_finalize(const DBox& b, int p, int nparts, const double* part_re,
                           const double* part_im, const double* mx, const double* my,
                           const double* mz, const double4* w, double* rho_re, double* rho_im,
                           KTab* tab, double* kterm, double self_energy, double* energy,
                           int mean_parts, const double* fpart, int n_atoms, double* mean_out,
-                          cudaStream_t st);
+                          cudaStream_t st, const SogVirial* vir = nullptr);
+// The NPT gather chain of RBSOGSampleKSpace over the p samples: one block;
+// r_i = G_npt(m_i) |k_i|^4 / (G(m_i) |k_i|^2) and a Philox uniform u_i per
+// sample, then idx_0 = 0, idx_i = i when u_i r_(idx_(i-1)) < r_i else
+// idx_(i-1).  mult[k] = #{i : idx_i = k}; idx (may be null) the map itself.
+struct SogGauss {
+  const double* coef;      // [mmax] Gaussian weights
+  const double* coef_npt;  // [mmax] their NPT counterparts
+  int mmax;
+  double b2, sig2;         // b^2, sigma^2
+};
+int launch_rbsog_npt_chain(const DBox& b, int p, const double* mx, const double* my,
+                           const double* mz, const SogGauss& g, uint64_t seed, uint64_t step,
+                           const int* step_dev, int* idx, int* mult, cudaStream_t st);
 int verlet_sog_blocks(int n);
 // epart (may be null) receives [blocks][2] = {E_LJ, E_coul} per-block sums.
 // Mixed form: fixed-point records, FP32 pair terms, no energies.

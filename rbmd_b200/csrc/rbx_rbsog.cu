@@ -87,9 +87,77 @@ k_rbsog_sample(int p, RbsogTables t, uint32_t key0, uint32_t key1, uint64_t step
   atomicOr(status, 1);
 }
 
+// G^(k) = sum_l coef_l exp(-b^(2l) sigma^2 |k|^2 / 2) (KSpaceCalculator::Gaussian
+// and Gaussian_modify, kspace_calculator.cpp:1559-1590).
+__device__ double sog_ghat(const double* __restrict__ coef, int mmax, double b2, double sig2,
+                           double k2) {
+  double sum = 0.0, bl = 1.0;
+  for (int l = 0; l < mmax; ++l) {
+    sum += coef[l] * exp(-(bl * sig2) * k2 / 2.0);
+    bl *= b2;
+  }
+  return sum;
+}
+
+constexpr int SOG_CHAIN_BLOCK = 256;
+constexpr int SOG_CHAIN_CHUNK = 1024;
+constexpr uint32_t SOG_NPT_STREAM = 0x4e505400u;  // Philox counter word of the NPT uniforms
+
+// The NPT gather chain (RBSOGSampleKSpace, kspace_calculator.cpp:1242-1301):
+// an independence Metropolis chain over the samples themselves, with target
+// G_npt(m) |k|^4 and proposal density G(m) |k|^2 (the density the samples
+// follow).  Chunks of 1024 samples: every thread forms ratios and uniforms
+// into shared memory, then thread 0 walks the chunk.  Accepting i when
+// u_i r_cur < r_i is u_i < min(1, r_i / r_cur) without the division.
+__global__ void __launch_bounds__(SOG_CHAIN_BLOCK)
+k_rbsog_npt_chain(int p, const double* __restrict__ mx, const double* __restrict__ my,
+                  const double* __restrict__ mz, double Lx, double Ly, double Lz, SogGauss g,
+                  uint32_t key0, uint32_t key1, uint64_t step_arg, const int* __restrict__ step_dev,
+                  int* __restrict__ idx, int* __restrict__ mult) {
+  __shared__ double s_r[SOG_CHAIN_CHUNK], s_u[SOG_CHAIN_CHUNK];
+  const uint64_t step = step_dev ? (uint64_t)(int64_t)*step_dev : step_arg;
+  int cur = 0;
+  double rcur = 0.0;
+  for (int base = 0; base < p; base += SOG_CHAIN_CHUNK) {
+    const int m = min(SOG_CHAIN_CHUNK, p - base);
+    __syncthreads();  // thread 0 is done with the previous chunk
+    for (int t = threadIdx.x; t < m; t += SOG_CHAIN_BLOCK) {
+      const int i = base + t;
+      const double kx = 2 * RBX_PI * mx[i] / Lx, ky = 2 * RBX_PI * my[i] / Ly,
+                   kz = 2 * RBX_PI * mz[i] / Lz;
+      const double k2 = kx * kx + ky * ky + kz * kz;
+      s_r[t] = sog_ghat(g.coef_npt, g.mmax, g.b2, g.sig2, k2) * (k2 * k2) /
+               (sog_ghat(g.coef, g.mmax, g.b2, g.sig2, k2) * k2);
+      uint32_t c[4] = {(uint32_t)i, SOG_NPT_STREAM, (uint32_t)step, (uint32_t)(step >> 32)};
+      philox4x32_10(c, key0, key1);
+      s_u[t] = u53(c[0], c[1]);
+      mult[i] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int t = 0; t < m; ++t) {
+        const int i = base + t;
+        const double r = s_r[t];
+        if (i == 0) {
+          rcur = r;
+        } else if (s_u[t] * rcur < r) {
+          mult[cur] = i - cur;
+          cur = i;
+          rcur = r;
+        }
+        if (idx) idx[i] = cur;
+      }
+    }
+  }
+  if (threadIdx.x == 0 && p > 0) mult[cur] = p - cur;
+}
+
 // Block k < p: rho(k) from the partial sums (fixed order), the force-table
 // entry with c_k = (wa_k / |k|^2 + wb_k) / V and the energy term
 // (ea_k / |k|^2 + eb_k) |rho|^2; blocks p..p+2: mean of the pair-force sums.
+// With vir, the per-k virial terms (ComputeRBSOGSampleVirialKernel :1133-1190,
+// ComputeRBSOGDirectVirialKernel :1308-1355): the energy term on the
+// diagonal plus the NPT term g_k k_a k_b.
 __global__ void __launch_bounds__(SOG_FK_BLOCK)
 k_rbsog_finalize(int p, int nparts, const double* __restrict__ part_re,
                  const double* __restrict__ part_im, const double* __restrict__ mx,
@@ -97,7 +165,8 @@ k_rbsog_finalize(int p, int nparts, const double* __restrict__ part_re,
                  double Ly, double Lz, const double4* __restrict__ w,
                  double* __restrict__ rho_re, double* __restrict__ rho_im,
                  KTab* __restrict__ tab, double* __restrict__ kterm, int mean_parts,
-                 const double* __restrict__ fpart, double n_atoms, double* __restrict__ mean_out) {
+                 const double* __restrict__ fpart, double n_atoms, double* __restrict__ mean_out,
+                 SogVirial vir) {
   __shared__ double sh[SOG_FK_BLOCK / 32];
   const int blk = blockIdx.x;
   if (blk >= p) {
@@ -126,7 +195,19 @@ k_rbsog_finalize(int p, int nparts, const double* __restrict__ part_re,
                kz = 2 * RBX_PI * mz[k] / Lz;
   const double k2 = kx * kx + ky * ky + kz * kz;
   const double4 wk = w[k];
-  if (kterm) kterm[k] = (wk.z / k2 + wk.w) * (r * r + im * im);
+  const double r2 = r * r + im * im;
+  if (kterm) kterm[k] = (wk.z / k2 + wk.w) * r2;
+  if (vir.vterm) {
+    const double e = (wk.z / k2 + wk.w) * r2;
+    const double gk = k < vir.psamp ? vir.mult[k] * vir.vw[k] * r2 / (k2 * k2) : vir.vw[k] * r2;
+    double* v = vir.vterm + 6 * (size_t)k;
+    v[0] = e + gk * kx * kx;
+    v[1] = e + gk * ky * ky;
+    v[2] = e + gk * kz * kz;
+    v[3] = gk * kx * ky;
+    v[4] = gk * kx * kz;
+    v[5] = gk * ky * kz;
+  }
   if (tab) {
     const double c = (wk.x / k2 + wk.y) / V;
     KTab t;
@@ -143,14 +224,26 @@ k_rbsog_finalize(int p, int nparts, const double* __restrict__ part_re,
   }
 }
 
-// Energy: one warp adds the per-k terms in increasing k, then the self term.
+// Energy: one warp adds the per-k terms in increasing k, then the self term;
+// the virial terms likewise when vterm is given.
 __global__ void __launch_bounds__(32)
 k_rbsog_energy_sum(int p, const double* __restrict__ kterm, double self_energy,
-                   double* __restrict__ energy) {
-  double t = 0.0;
-  for (int k = threadIdx.x; k < p; k += 32) t += kterm[k];
-  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-  if (threadIdx.x == 0) *energy = t + self_energy;
+                   double* __restrict__ energy, const double* __restrict__ vterm,
+                   double* __restrict__ virial) {
+  if (energy) {
+    double t = 0.0;
+    for (int k = threadIdx.x; k < p; k += 32) t += kterm[k];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) *energy = t + self_energy;
+  }
+  if (vterm) {
+    for (int c = 0; c < 6; ++c) {
+      double t = 0.0;
+      for (int k = threadIdx.x; k < p; k += 32) t += vterm[6 * (size_t)k + c];
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      if (threadIdx.x == 0) virial[c] = t;
+    }
+  }
 }
 
 // VERLET-SOG pair force (ComputeLJCutCoulForceUserKernel with lj126 and
@@ -320,22 +413,34 @@ int launch_rbsog_finalize(const DBox& b, int p, int nparts, const double* part_r
                           const double* mz, const double4* w, double* rho_re, double* rho_im,
                           KTab* tab, double* kterm, double self_energy, double* energy,
                           int mean_parts, const double* fpart, int n_atoms, double* mean_out,
-                          cudaStream_t st) {
+                          cudaStream_t st, const SogVirial* vir) {
   const int grid = p + (mean_out ? 3 : 0);
+  const SogVirial v = vir ? *vir : SogVirial{0, nullptr, nullptr, nullptr, nullptr};
   if (grid > 0) {
     k_rbsog_finalize<<<grid, SOG_FK_BLOCK, 0, st>>>(
         p, nparts, part_re, part_im, mx, my, mz, b.len[0], b.len[1], b.len[2], w, rho_re, rho_im,
-        tab, energy ? kterm : nullptr, mean_parts, fpart, (double)n_atoms, mean_out);
+        tab, energy ? kterm : nullptr, mean_parts, fpart, (double)n_atoms, mean_out, v);
     count_launch();
     const int rc = check_launch("rbsog_finalize");
     if (rc) return rc;
   }
-  if (energy) {
-    k_rbsog_energy_sum<<<1, 32, 0, st>>>(p, kterm, self_energy, energy);
+  if (energy || v.vterm) {
+    k_rbsog_energy_sum<<<1, 32, 0, st>>>(p, kterm, self_energy, energy, v.vterm, v.out);
     count_launch();
     return check_launch("rbsog_energy_sum");
   }
   return RBX_OK;
+}
+
+int launch_rbsog_npt_chain(const DBox& b, int p, const double* mx, const double* my,
+                           const double* mz, const SogGauss& g, uint64_t seed, uint64_t step,
+                           const int* step_dev, int* idx, int* mult, cudaStream_t st) {
+  if (p <= 0) return RBX_OK;
+  k_rbsog_npt_chain<<<1, SOG_CHAIN_BLOCK, 0, st>>>(p, mx, my, mz, b.len[0], b.len[1], b.len[2],
+                                                   g, (uint32_t)seed, (uint32_t)(seed >> 32),
+                                                   step, step_dev, idx, mult);
+  count_launch();
+  return check_launch("rbsog_npt_chain");
 }
 
 int verlet_sog_blocks(int n) { return (n + SOG_PAIR_BLOCK / 32 - 1) / (SOG_PAIR_BLOCK / 32); }

@@ -114,6 +114,7 @@ EXPORTS = [
     "rbx_rbl_filter_f32", "rbx_pair_force_rbl_f32", "rbx_fix_rbl_force_f32",
     "rbx_pair_force_verlet_f32", "rbx_engine_kspace_energy_exact", "rbx_force_create_json",
     "rbx_force_destroy", "rbx_force_engine", "rbx_force_execute", "rbx_force_energies",
+    "rbx_rbsog_npt_chain", "rbx_rbsog_virial", "rbx_engine_rbsog_npt_map",
 ]
 
 
@@ -217,6 +218,9 @@ def lib():
     L.rbx_rbsog_sample.argtypes = [B, ip, dp, ip, C.c_uint64, C.c_int64, vp, vp, vp, vp]
     L.rbx_rbsog_force.argtypes = [B, ip, dp, dp, dp, dp, ip, ip] + [vp] * 10 + [
         C.POINTER(C.c_double), vp]
+    L.rbx_rbsog_npt_chain.argtypes = [B, ip, dp, ip, vp, vp, vp, C.c_uint64, C.c_int64, vp, vp]
+    L.rbx_rbsog_virial.argtypes = [B, ip, dp, dp, dp, dp, ip, ip] + [vp] * 8 + [vp, vp]
+    L.rbx_engine_rbsog_npt_map.argtypes = [vp, C.POINTER(C.c_int), vp]
     L.rbx_pair_force_verlet_sog.argtypes = [B, ip, dp, dp, ip, ip, vp, vp] + [vp] * 5 + [
         ip, vp, vp, vp, vp, vp, vp, vp, vp]
     L.rbx_lammps_read.restype = vp
@@ -638,6 +642,14 @@ class Engine:
         check(lib().rbx_engine_get_stats(self._h, C.byref(s)), "get_stats")
         return s
 
+    def rbsog_npt_map(self) -> np.ndarray:
+        """RBSOG engines: the NPT gather map of the last evaluation's samples."""
+        p = C.c_int()
+        check(lib().rbx_engine_rbsog_npt_map(self._h, C.byref(p), None), "rbsog_npt_map")
+        out = np.zeros(p.value, dtype=np.int32)
+        check(lib().rbx_engine_rbsog_npt_map(self._h, C.byref(p), _np_ptr(out)), "rbsog_npt_map")
+        return out
+
     @property
     def stream(self) -> int:
         return int(lib().rbx_engine_stream(self._h) or 0)
@@ -938,6 +950,23 @@ def rbsog_force(box, level, cut_off, qqr2e, S, qsqsum, q, mx, my, mz, x, y, z, f
                                 _ptr(y), _ptr(z), _ptr(fx), _ptr(fy), _ptr(fz), C.byref(e),
                                 _stream(stream)), "rbx_rbsog_force")
     return e.value
+
+
+def rbsog_npt_chain(box, level, cut_off, mx, my, mz, seed, step, idx, stream=None):
+    """The NPT gather map of the samples (device int32 idx, filled in place)."""
+    check(lib().rbx_rbsog_npt_chain(C.byref(box), level, cut_off, mx.numel(), _ptr(mx), _ptr(my),
+                                    _ptr(mz), seed, step, _ptr(idx), _stream(stream)),
+          "rbx_rbsog_npt_chain")
+
+
+def rbsog_virial(box, level, cut_off, qqr2e, S, S_npt, q, mx, my, mz, idx, x, y, z, stream=None):
+    """RBSOG k-space virial [6] (sampled with the gather map idx + direct)."""
+    v = np.zeros(6)
+    check(lib().rbx_rbsog_virial(C.byref(box), level, cut_off, qqr2e, S, S_npt, q.numel(),
+                                 mx.numel(), _ptr(q), _ptr(mx), _ptr(my), _ptr(mz), _ptr(idx),
+                                 _ptr(x), _ptr(y), _ptr(z), _np_ptr(v), _stream(stream)),
+          "rbx_rbsog_virial")
+    return v
 
 
 def pair_force_verlet_sog(box, level, cut_off, qqr2e, sigma, eps, typ, q, x, y, z, count, rows,

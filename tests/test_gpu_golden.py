@@ -80,3 +80,51 @@ def test_engine_against_reference(cuda, rbx, path, precision):
     assert systems.rel_rms(fp, ref_p) < tol
     assert systems.rel_rms(fp + fk, ref_p + ref_k) < tol
     e.close()
+
+
+def test_cells_and_list_against_reference(cuda, rbx):
+    """rbx_cells_sort / rbx_full_list against RBMD's LinkedCell and full-list
+    kernels (tests/golden/ref_cells_n3328.npz, cells of edge cut_off + skin):
+    the cell of every atom, atoms per cell and the pair set."""
+    import hashlib
+
+    torch = cuda
+    path = os.path.join(HERE, "golden", "ref_cells_n3328.npz")
+    if not os.path.exists(path):
+        pytest.skip("cells fixture not generated")
+    f = dict(np.load(path))
+    n = int(f["n"])
+    box = rbx.Box.make(f["lo"], f["hi"])
+    dims = rbx.cell_grid(box, 5.3)
+    assert list(dims) == f["c1_dims"].tolist()
+    ncell = int(np.prod(dims))
+    X = [torch.as_tensor(np.ascontiguousarray(f[k])).to("cuda", torch.float64) for k in "xyz"]
+    perm = torch.zeros(n, dtype=torch.int32, device="cuda")
+    cos = torch.zeros(n, dtype=torch.int32, device="cuda")
+    cst = torch.zeros(ncell + 1, dtype=torch.int32, device="cuda")
+    scratch = torch.zeros(rbx.cells_scratch_bytes(n, ncell), dtype=torch.uint8, device="cuda")
+    rbx.cells_sort(box, 5.3, *X, perm, cos, cst, scratch)
+    hp, hc, hs = perm.cpu().numpy(), cos.cpu().numpy(), cst.cpu().numpy()
+    cell = np.empty(n, dtype=np.int32)
+    cell[hp] = hc
+    assert np.array_equal(cell, f["c1_cell"])
+    assert np.array_equal(np.diff(hs), f["c1_cell_count"])
+    xs = [torch.as_tensor(np.ascontiguousarray(f[k][hp])).to("cuda", torch.float64) for k in "xyz"]
+    cap = 800
+    cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
+    nb = torch.full((n, cap), -1, dtype=torch.int32, device="cuda")
+    ovf = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rbx.full_list(box, 5.3, *xs, cst, cap, cnt, nb, ovf)
+    torch.cuda.synchronize()
+    assert ovf.item() == 0
+    gc, gn = cnt.cpu().numpy(), nb.cpu().numpy()
+    want = np.empty(n, dtype=np.int64)
+    want[hp] = gc
+    assert np.array_equal(want, f["c1_list_count"].astype(np.int64))
+    gid = np.asarray(f["gid"], dtype=np.int64)[hp]
+    owner = np.repeat(np.arange(n), gc)
+    flat = np.concatenate([gn[i, :gc[i]] for i in range(n)])
+    pairs = np.stack([gid[owner], gid[flat]], 1)
+    pairs = pairs[np.lexsort((pairs[:, 1], pairs[:, 0]))]
+    assert hashlib.sha256(np.ascontiguousarray(pairs).tobytes()).hexdigest() == \
+        str(f["c1_list_digest"])

@@ -156,3 +156,50 @@ def test_engine_rbsog_graph_matches_launches(cuda, rbx):
         assert np.array_equal(a[key], b[key]), key
     assert sa.rebuilds == sb.rebuilds
     assert sa.e_kspace == sb.e_kspace
+
+
+def test_rbsog_npt_chain_and_virial(cuda, rbx, oracle, sys4k):
+    """The NPT gather chain on the device equals the oracle's restatement of
+    RBSOGSampleKSpace's chain on the same uniforms; the k-space virial
+    (sampled with the gather map + direct, kspace_calculator_op.hip.cu:
+    1133-1190, 1308-1355) within 1e-10 of the oracle's."""
+    s = sys4k
+    box = oracle.Box.make(s["lo"], s["hi"])
+    rbox = rbx.Box.make(s["lo"], s["hi"])
+    P, seed, step = 112, 31, 3
+    m = oracle.rbsog_sample_philox(2, 5.0, box, P, 5, 0)
+    want_idx = oracle.rbsog_idx_npt(2, 5.0, box, m, oracle.rbsog_npt_uniforms(seed, step, P))
+    assert 1 < len(np.unique(want_idx)) < P  # the chain both accepts and rejects
+    M = [_t(cuda, v) for v in m]
+    idx = cuda.zeros(P, dtype=cuda.int32, device="cuda")
+    rbx.rbsog_npt_chain(rbox, 2, 5.0, *M, seed, step, idx)
+    assert np.array_equal(idx.cpu().numpy(), want_idx)
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    v = rbx.rbsog_virial(rbox, 2, 5.0, 1.0, 0.0, 0.0, _t(cuda, s["q"]), *M, idx, _t(cuda, x),
+                         _t(cuda, y), _t(cuda, z))
+    want = oracle.rbsog_virial(2, 5.0, box, 1.0, s["q"], m, want_idx, x, y, z)
+    assert np.abs(v - want).max() < 1e-10 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_engine_rbsog_virial(cuda, rbx, oracle, prec):
+    """The engine's k-space virial (rbx_stats.virial_kspace) with injected
+    samples: its gather map equals the oracle's chain for the engine's seed
+    and epoch, and the virial the oracle's on that map (1e-10 FP64, 1e-6 mixed
+    relative to the largest component)."""
+    s = _sog_system(seed=43)
+    p = s["params"]
+    box = oracle.Box.make(s["lo"], s["hi"])
+    m = oracle.rbsog_sample_philox(2, p["cut_off"], box, 112, 7, 0)
+    e = rbx.Engine(s, precision=prec, neighbor="VERLET-SOG", coulomb="RBSOG", seed=31)
+    e.set_k_samples(*m)
+    e.compute_forces(5)
+    idx = e.rbsog_npt_map()
+    want_idx = oracle.rbsog_idx_npt(2, p["cut_off"], box, m, oracle.rbsog_npt_uniforms(31, 5, 112))
+    assert np.array_equal(idx, want_idx)
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    want = oracle.rbsog_virial(2, p["cut_off"], box, p["qqr2e"], s["q"], m, want_idx, x, y, z)
+    got = np.asarray(e.stats().virial_kspace[:])
+    tol = 1e-10 if prec == 0 else 1e-6
+    assert np.abs(got - want).max() < tol * np.abs(want).max()
+    e.close()

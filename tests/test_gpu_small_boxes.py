@@ -3,9 +3,10 @@ edges between 2 and 3 times cut_off + skin (953 <= N < 3216 atoms for the
 cubic LJ electrolyte at rho* = 0.8; below N = 953 the edge is shorter than
 2 (cut_off + skin) and the engine rejects the box).  The candidate rows come
 from an all-pairs builder with the FP64 list predicate, each pair once (the
-reference's 27-cell stencil wraps onto the same cell twice along such an
-axis and lists those pairs twice; the oracle's stencil visits each distinct
-cell once).
+reference's (2c + 1)^3 stencil over cells of edge (cut_off + skin) / c wraps
+onto the same cell more than once along an axis with fewer than 2c + 1 cells
+and lists those pairs repeatedly, tests/test_golden_rows.py; the oracle's
+stencil visits each distinct cell once).
 
 Checked: RBL + RBE forces in both forms against the oracle (1e-9 / 1e-5
 relative RMS), exact RBL pair sets, the Verlet-list pair energies, steps
