@@ -412,10 +412,13 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
 // along some axis (edge between two and three times cut_off + skin): every
 // atom j != i is tested with the reference's FP64 predicate (CaculateDistance:
 // i minus j, single-shift minimum image, no FMA), so each pair is listed once.
-// (The reference's 27-cell stencil wraps onto the same cell twice along such
-// an axis, WrapFullNeighborStencilIndex in full_neighbor_list_op.hip.cu:9-17,
-// 45-80, and lists those pairs twice.)  A warp per atom; hits are appended in
-// index order through a ballot prefix, far pairs (see FarSplit) to the back.
+// (The reference's cells have edge (cut_off + skin) / c, c = 1 for a Verlet
+// list and ceil((cut_off + skin) / r_core) for RBL (linked_cell_locator.cpp:
+// 26-40), and its (2c + 1)^3 stencil wraps onto the same cell more than once
+// along an axis with fewer than 2c + 1 cells, WrapFullNeighborStencilIndex in
+// full_neighbor_list_op.hip.cu:9-80, listing those pairs repeatedly.)  A warp
+// per atom; hits are appended in index order through a ballot prefix, far
+// pairs (see FarSplit) to the back.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128)
 k_full_list_small(DBox b, double cut2, double near2, int n, const double* __restrict__ x,
@@ -536,14 +539,15 @@ __global__ void k_kick(int n, const double* __restrict__ fx, const double* __res
 
 // UpdatePositionFlag + ApplyPBC (update_position_op.hip.cu:22-46, box.h:133-169),
 // fused with the skin check DisplacementSq (base_neighbor_list_builder.cpp:102-116)
-// and, for the mixed form, the fixed-point record {ux, uy, uz, q_f32}.
+// and, for the mixed form, the fixed-point record {ux, uy, uz, q_f32}.  With
+// kick.fx the first half kick of the step comes first (k_kick's arithmetic).
 __global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double* __restrict__ y,
-                        double* __restrict__ z, const double* __restrict__ vx,
-                        const double* __restrict__ vy, const double* __restrict__ vz,
+                        double* __restrict__ z, double* __restrict__ vx,
+                        double* __restrict__ vy, double* __restrict__ vz,
                         const double* __restrict__ x0, const double* __restrict__ y0,
                         const double* __restrict__ z0, unsigned long long* __restrict__ max_d2,
                         uint4* __restrict__ atoms, const double* __restrict__ q,
-                        ImageRefs img, Pos3 old) {
+                        ImageRefs img, Pos3 old, KickArgs kick) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0.0;
   if (i < n) {
@@ -552,7 +556,17 @@ __global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double
       old.y[i] = y[i];
       old.z[i] = z[i];
     }
-    double p[3] = {x[i] + vx[i] * dt, y[i] + vy[i] * dt, z[i] + vz[i] * dt};
+    double v[3] = {vx[i], vy[i], vz[i]};
+    if (kick.fx) {
+      const double s = kick.inv_mass[kick.type[i]] * kick.half_dt;
+      v[0] += kick.fx[i] * s;
+      v[1] += kick.fy[i] * s;
+      v[2] += kick.fz[i] * s;
+      vx[i] = v[0];
+      vy[i] = v[1];
+      vz[i] = v[2];
+    }
+    double p[3] = {x[i] + v[0] * dt, y[i] + v[1] * dt, z[i] + v[2] * dt};
     for (int d = 0; d < 3; ++d) {  // periodic wrap, counted in the image flags
       int w = 0;
       if (p[d] >= b.lo[d] + b.len[d]) {
@@ -808,12 +822,14 @@ int launch_kick(int n, const double* fx, const double* fy, const double* fz, con
 }
 
 int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* z,
-                 const double* vx, const double* vy, const double* vz, const double* x0,
+                 double* vx, double* vy, double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
-                 uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st) {
+                 uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st,
+                 const KickArgs* kick) {
   if (n <= 0) return RBX_OK;
+  const KickArgs k = kick ? *kick : KickArgs{nullptr, nullptr, nullptr, nullptr, nullptr, 0.0};
   k_drift<<<(n + 255) / 256, 256, 0, st>>>(b, n, dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2_bits,
-                                           atoms, q, img, old);
+                                           atoms, q, img, old, k);
   count_launch();
   return check_launch("drift");
 }

@@ -854,11 +854,11 @@ int rbx_engine::step_plain(int nsteps) {
       cudaEventRecord(e[0], st);
     }
     if (nh_on) ETRY(nh_initial(nullptr, epoch + 1, st));
-    ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
     ETRY(cuda_ok(cudaMemsetAsync(max_d2, 0, sizeof(unsigned long long), st), "memset"));
+    const KickArgs kick{fx, fy, fz, type, inv_mass, 0.5 * prm.dt};
     ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
                      ImageRefs{{img[0], img[1], img[2]}}, Pos3{shake_nc ? xs : nullptr, ys, zs},
-                     st));
+                     st, &kick));
     if (shake_nc) ETRY(shake_a(st));
     if (e) cudaEventRecord(e[1], st);
     ++epoch;
@@ -916,11 +916,11 @@ int rbx_engine::capture_step_into(cudaGraph_t g) {
 // First part of a step: half kick, drift with the skin check (+ SHAKE).
 int rbx_engine::capture_step_head() {
   if (nh_on) ETRY(nh_initial(dflags + 4, 1, st));  // the device epoch is still the last step's
-  ETRY(launch_kick(n, fx, fy, fz, type, inv_mass, 0.5 * prm.dt, vx, vy, vz, st));
   ETRY(launch_zero_u64(max_d2, st));
+  const KickArgs kick{fx, fy, fz, type, inv_mass, 0.5 * prm.dt};
   ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
                      ImageRefs{{img[0], img[1], img[2]}}, Pos3{shake_nc ? xs : nullptr, ys, zs},
-                     st));
+                     st, &kick));
   if (shake_nc) ETRY(shake_a(st));
   return RBX_OK;
 }

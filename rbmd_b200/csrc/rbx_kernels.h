@@ -384,10 +384,19 @@ struct Pos3 {
 struct ImageRefs {
   int* c[3];
 };
+// kick (may be null): the step's first half kick v += F inv_mass[type] half_dt
+// done in the same pass, before the drift.
+struct KickArgs {
+  const double *fx, *fy, *fz;
+  const int* type;
+  const double* inv_mass;
+  double half_dt;
+};
 int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* z,
-                 const double* vx, const double* vy, const double* vz, const double* x0,
+                 double* vx, double* vy, double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
-                 uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st);
+                 uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st,
+                 const KickArgs* kick = nullptr);
 // CVFF special-bond correction of the RBL pair force (rbx_special.cu): its
 // SPEC_PARTS per-block force sums follow the fused kernel's in fpart.
 constexpr int SPEC_PARTS = 1184;  // 8 blocks per SM of 148: about one atom per thread

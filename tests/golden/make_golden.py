@@ -256,10 +256,9 @@ def group_cells(libs, out_dir):
             cap = n * 1200
             nbr = np.zeros(cap, dtype=np.int32)
             realloc = C.c_int()
+            hp = [C.c_void_p(a.ctypes.data) for a in (cell, cs, ce, cnt, nbr)]  # host arrays
             rc = L.ref_cells_full_list(lo, hi, C.c_double(5.3), c, C.c_double(5.3 * 5.3), n, p(x),
-                                       p(y), p(zz), cell.ctypes.data, cs.ctypes.data,
-                                       ce.ctypes.data, cnt.ctypes.data, nbr.ctypes.data,
-                                       C.c_longlong(cap), C.byref(realloc))
+                                       p(y), p(zz), *hp, C.c_longlong(cap), C.byref(realloc))
             assert rc == 0 and realloc.value == 0, (rc, realloc.value)
             gid = np.asarray(s["gid"], dtype=np.int64)
             owner = np.repeat(np.arange(n), cnt)
