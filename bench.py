@@ -399,7 +399,7 @@ def config_runs(local):
         return {"value": n * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps}
 
     out = {}
-    for name, n, p, steps in (("p400", 200000, 400, 50), ("cfg0_n4000", 4000, 100, 1000)):
+    for name, n, p, steps in (("p400", 200000, 400, 50), ("n4000", 4000, 100, 1000)):
         mx = run(n, p, rbx.MIXED, steps, 5)
         f64 = run(n, p, rbx.PLAIN_FP64, steps, 5)
         out[name] = {"n": n, "p": p, "mixed": mx, "fp64_plain": f64,
@@ -573,7 +573,7 @@ def run_ours(args):
 
 
 def run_batched(args):
-    """Batched replicas (the cfg-4 recipe): R independent LJ electrolytes with
+    """Batched replicas: R independent LJ electrolytes with
     log-uniform atom counts, mixed form, all advanced by one CUDA graph launch
     per step (rbx_batch), against the same replicas stepped one engine at a
     time: plain FP64 launch by launch (the one-replica-per-launch baseline)

@@ -4,7 +4,7 @@ The fused filter + pair-force kernel picks its shell-batch test from the
 selection frequency (GetRblParams, rbl_full_neighbor_list_builder.cpp:193-228):
 freq in {1, 2, 4} reads two bits of a partial SplitMix64 hash, other powers
 of two a mask, any other freq a divisibility test by multiplication.  On the
-cfg-0 LJ electrolyte (rho* = 0.8, r_core 2.5, cut_off 5: n_c - n_s = 367)
+4,000-atom LJ electrolyte (rho* = 0.8, r_core 2.5, cut_off 5: n_c - n_s = 367)
 neighbor_sample_num 400 / 200 / 150 / 100 / 90 / 60 / 50 / 40 gives
 freq 1 / 2 / 3 / 4 / 5 / 7 / 8 / 10, which reaches all three paths.
 

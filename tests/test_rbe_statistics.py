@@ -27,7 +27,7 @@ import pytest
 from rbmd_b200 import systems
 
 M = 100          # samplings
-KMAX = (10, 10, 10)  # exp(-k^2 / 4 alpha) < 1e-9 beyond m = 10 for cfg 0 (L = 17.1, alpha = 0.16)
+KMAX = (10, 10, 10)  # exp(-k^2 / 4 alpha) < 1e-9 beyond m = 10 for the 4,000-atom box (L = 17.1, alpha = 0.16)
 
 
 def _stats(samples, ref):
@@ -42,7 +42,7 @@ def _stats(samples, ref):
 
 
 @pytest.fixture(scope="module")
-def cfg0(oracle):
+def electrolyte_n4000(oracle):
     s = systems.lj_electrolyte(4000, seed=2024)
     p = s["params"]
     box = oracle.Box.make(s["lo"], s["hi"])
@@ -60,8 +60,8 @@ def _oracle_rbe(oracle, box, S, qqr2e, xyzq, m):
 
 
 @pytest.fixture(scope="module")
-def oracle_stats(oracle, cfg0):
-    s, box, xyzq, f_ewald, S = cfg0
+def oracle_stats(oracle, electrolyte_n4000):
+    s, box, xyzq, f_ewald, S = electrolyte_n4000
     p = s["params"]
     mh = [_oracle_rbe(oracle, box, S, p["qqr2e"], xyzq,
                       oracle.rbe_sample_mh(box, p["alpha"], p["kspace_p"], 1000 + k))
@@ -90,10 +90,11 @@ def test_reference_and_philox_sampler_errors_agree(oracle_stats):
 
 
 @pytest.mark.gpu
-def test_gpu_rbe_error_matches_reference_statistics(cuda, rbx, oracle, cfg0, oracle_stats):
+def test_gpu_rbe_error_matches_reference_statistics(cuda, rbx, oracle, electrolyte_n4000,
+                                                    oracle_stats):
     import torch
 
-    s, box, (x, y, z, q), f_ewald, S = cfg0
+    s, box, (x, y, z, q), f_ewald, S = electrolyte_n4000
     p = s["params"]
     mh, _ = oracle_stats
     rbox = rbx.Box.make(s["lo"], s["hi"])
