@@ -48,10 +48,10 @@ sys.path.insert(0, ROOT)
 METRIC = "RBE+LJ atom-steps/s @200k atoms: mixed vs FP64 plain at <=1e-5 rel force err"
 UNIT = "atom-steps/s"
 # DRAM bytes (read + written) per atom of one mixed k_rbl_fused launch, from an ncu
-# capture of the same workload at N = 100,000 (271.1 MB per launch: the candidate rows
-# streamed once, plus neighbour-record and key gathers that miss L2).  Rows and gathers
-# grow with N, so the traffic is scaled by N.
-RBL_TRAFFIC_BYTES_PER_ATOM = 2711.1
+# capture of the same workload at N = 100,000 (215.1 MB per launch: the split candidate
+# rows streamed once, plus neighbour-record and key gathers that miss L2).  Rows and
+# gathers grow with N, so the traffic is scaled by N.
+RBL_TRAFFIC_BYTES_PER_ATOM = 2151.0
 
 
 def _peaks():

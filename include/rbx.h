@@ -635,7 +635,10 @@ int rbx_engine_get_force_parts(rbx_engine* e, double* f_pair, double* f_kspace);
  * when neighbor.energy_rbl_flag is "yes" and inside the force op for a Verlet
  * list.  FP64 in both precision forms.  Totals: RBMD divides them by the atom
  * count in LJ units.  Any pointer may be NULL.  RBL and Verlet-list engines
- * (VERLET-SOG reports its energies through rbx_pair_force_verlet_sog). */
+ * (VERLET-SOG reports its energies through rbx_pair_force_verlet_sog).  As in
+ * RBMD's LJCutCoulEnergyOp, no CVFF special-bond weights are applied: with
+ * rbx_engine_set_special the energies and virial still include the excluded
+ * and scaled pairs that the force weights. */
 int rbx_engine_pair_energy(rbx_engine* e, double* e_vdwl, double* e_coul, double* virial);
 /* Exact Ewald reciprocal energy over the kmax box plus the self energy
  * (-qqr2e sqrt(alpha / pi) sum q^2) of the current positions, on the host:
