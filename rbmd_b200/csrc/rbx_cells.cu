@@ -103,7 +103,10 @@ __global__ void k_cell_assign(DBox b, CellGeom g, int dx, int dy, int dz, int n,
     return (unsigned)(v < 0 ? 0 : (v > 3 ? 3 : v));
   };
   sub[i] = n < (1 << SUB_SHIFT) ? morton2(sub4(fx, cx), sub4(fy, cy), sub4(fz, cz)) : 0u;
-  atomicAdd(counts + c, 1);
+  // atoms still in the order of the last sort share cells along a warp: one
+  // atomic per distinct cell of the warp
+  const unsigned same = __match_any_sync(__activemask(), c);
+  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(counts + c, __popc(same));
 }
 
 // Exclusive scan of counts into start[0..ncell] (one block of 1024 threads).
@@ -153,7 +156,15 @@ __global__ void k_cell_scatter(int n, const int* __restrict__ cell,
                                unsigned* __restrict__ tmp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  tmp[atomicAdd(fill + cell[i], 1)] = (sub[i] << SUB_SHIFT) | (unsigned)i;
+  // one atomic per distinct cell of the warp; the order inside a cell is set
+  // by the segment sort that follows
+  const int c = cell[i];
+  const unsigned same = __match_any_sync(__activemask(), c);
+  const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(fill + c, __popc(same));
+  base = __shfl_sync(same, base, leader);
+  tmp[base + __popc(same & ((1u << lane) - 1u))] = (sub[i] << SUB_SHIFT) | (unsigned)i;
 }
 
 // One block per cell: bitonic sort of the cell's keys (sub-cell, old index).

@@ -203,3 +203,23 @@ def test_engine_rbsog_virial(cuda, rbx, oracle, prec):
     tol = 1e-10 if prec == 0 else 1e-6
     assert np.abs(got - want).max() < tol * np.abs(want).max()
     e.close()
+
+
+def test_rbsog_virial_edge_cases(cuda, rbx, oracle, sys4k):
+    """One sample (the gather map is [0]) and no atoms (a zero virial)."""
+    s = sys4k
+    box = oracle.Box.make(s["lo"], s["hi"])
+    rbox = rbx.Box.make(s["lo"], s["hi"])
+    m = oracle.rbsog_sample_philox(2, 5.0, box, 1, 3, 7)
+    M = [_t(cuda, v) for v in m]
+    idx = cuda.full((1,), 5, dtype=cuda.int32, device="cuda")
+    rbx.rbsog_npt_chain(rbox, 2, 5.0, *M, 3, 7, idx)
+    assert idx.item() == 0
+    x, y, z = (np.ascontiguousarray(s["pos"][:, d]) for d in range(3))
+    v = rbx.rbsog_virial(rbox, 2, 5.0, 1.0, 0.0, 0.0, _t(cuda, s["q"]), *M, idx, _t(cuda, x),
+                         _t(cuda, y), _t(cuda, z))
+    want = oracle.rbsog_virial(2, 5.0, box, 1.0, s["q"], m, np.zeros(1, dtype=np.int32), x, y, z)
+    assert np.abs(v - want).max() < 1e-10 * np.abs(want).max()
+    e = cuda.zeros(0, dtype=cuda.float64, device="cuda")
+    assert np.array_equal(rbx.rbsog_virial(rbox, 2, 5.0, 1.0, 0.0, 0.0, e, *M, idx, e, e, e),
+                          np.zeros(6))
