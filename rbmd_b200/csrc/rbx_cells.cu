@@ -279,6 +279,8 @@ k_chunk_boxes(const double* __restrict__ x, const double* __restrict__ y,
   for (int t = base + nch + threadIdx.x; t < next; t += blockDim.x) cell_of[t] = -1;
 }
 
+// SPLIT: RBL rows with a far segment; without it (Verlet lists) no far test.
+template <bool SPLIT>
 __global__ void __launch_bounds__(NL_BLOCK, 5)
 k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, float lo_band,
             float hi_band, int nidx, const double* __restrict__ x, const double* __restrict__ y,
@@ -308,9 +310,8 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
               az = live ? -2.f * uz : 0.f;
   const float lo_i = live ? lo_band - uu : -INFINITY;
   const float hi_i = live ? hi_band - uu : -INFINITY;
-  const bool split = far != nullptr;
-  // far pairs: d above this (never, without a split)
-  const float near_i = split && live ? near2 - uu : INFINITY;
+  // far pairs: d above this
+  const float near_i = live ? near2 - uu : INFINITY;
   // box of the group's centre atoms relative to the cell centre, rounded outwards
   float glo[3], ghi[3];
   {
@@ -384,7 +385,7 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
           const float d = fmaf(ax, q.x, fmaf(ay, q.y, fmaf(az, q.z, q.w)));
           acc |= d < lo_i ? 1u << t : 0u;
           maybe |= d < hi_i ? 1u << t : 0u;
-          farm |= d > near_i ? 1u << t : 0u;
+          if (SPLIT) farm |= d > near_i ? 1u << t : 0u;
         }
         if (nc == c && k == g) {  // the centre atom itself
           acc &= ~(1u << lane);
@@ -403,7 +404,7 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
           const int t = __ffs(acc) - 1;
           acc &= acc - 1;
           // one store to the front or the back of the row (no branch)
-          const bool to_back = (farm >> t) & 1u;
+          const bool to_back = SPLIT && ((farm >> t) & 1u);
           if (cnt < cap) row[to_back ? cap - 1 - nback : cnt - nback] = first + t;
           nback += (cnt < cap) & to_back;
           ++cnt;
@@ -413,7 +414,7 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
   }
   if (live) {
     count[i] = cnt;
-    if (split) far[i] = nback;
+    if (SPLIT) far[i] = nback;
     if (cnt > cap) atomicOr(overflow, 1);
   }
 }
@@ -728,9 +729,14 @@ int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, con
   count_launch();
   // far threshold in r^2, raised by the FP32 error of the test value
   const float near2 = split ? (float)(split->r_near * split->r_near + band) : INFINITY;
-  k_full_list<<<(t + NL_WARPS - 1) / NL_WARPS, NL_BLOCK, 0, st>>>(
-      b, dims[0], dims[1], dims[2], cut2, cut2_up, lo_band, hi_band, t, x, y, z, cell_start,
-      box_lo, box_hi, cell_of, cap, count, nbrs, overflow, near2, split ? split->far : nullptr);
+  if (split)
+    k_full_list<true><<<(t + NL_WARPS - 1) / NL_WARPS, NL_BLOCK, 0, st>>>(
+        b, dims[0], dims[1], dims[2], cut2, cut2_up, lo_band, hi_band, t, x, y, z, cell_start,
+        box_lo, box_hi, cell_of, cap, count, nbrs, overflow, near2, split->far);
+  else
+    k_full_list<false><<<(t + NL_WARPS - 1) / NL_WARPS, NL_BLOCK, 0, st>>>(
+        b, dims[0], dims[1], dims[2], cut2, cut2_up, lo_band, hi_band, t, x, y, z, cell_start,
+        box_lo, box_hi, cell_of, cap, count, nbrs, overflow, near2, nullptr);
   count_launch();
   return check_launch("full_list");
 }
