@@ -553,13 +553,16 @@ __global__ void k_kick(int n, const double* __restrict__ fx, const double* __res
 // fused with the skin check DisplacementSq (base_neighbor_list_builder.cpp:102-116)
 // and, for the mixed form, the fixed-point record {ux, uy, uz, q_f32}.  With
 // kick.fx the first half kick of the step comes first (k_kick's arithmetic).
+// With decide.ctr (inside a step graph) the last block to finish takes the
+// step's rebuild decision as k_step_decide does, then clears the maximum and
+// the block counter for the next step.
 __global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double* __restrict__ y,
                         double* __restrict__ z, double* __restrict__ vx,
                         double* __restrict__ vy, double* __restrict__ vz,
                         const double* __restrict__ x0, const double* __restrict__ y0,
                         const double* __restrict__ z0, unsigned long long* __restrict__ max_d2,
                         uint4* __restrict__ atoms, const double* __restrict__ q,
-                        ImageRefs img, Pos3 old, KickArgs kick) {
+                        ImageRefs img, Pos3 old, KickArgs kick, DecideArgs decide) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0.0;
   if (i < n) {
@@ -610,6 +613,21 @@ __global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double
     }
   }
   if (max_d2) warp_max_atomic(d2, max_d2);
+  if (decide.ctr) {
+    __syncthreads();  // every warp of the block has folded its maximum in
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(decide.ctr, 1u) == gridDim.x - 1) {  // the last block
+        __threadfence();
+        const unsigned long long m = atomicAdd(max_d2, 0ULL);
+        *decide.epoch += 1;
+        cudaGraphSetConditional(decide.cond,
+                                __longlong_as_double((long long)m) > decide.thr2 ? 1u : 0u);
+        *max_d2 = 0ULL;
+        *decide.ctr = 0u;
+      }
+    }
+  }
 }
 
 __global__ void k_to_fixed(DBox b, int n, const double* __restrict__ x,
@@ -842,11 +860,12 @@ int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* 
                  double* vx, double* vy, double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
                  uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st,
-                 const KickArgs* kick) {
+                 const KickArgs* kick, const DecideArgs* decide) {
   if (n <= 0) return RBX_OK;
   const KickArgs k = kick ? *kick : KickArgs{nullptr, nullptr, nullptr, nullptr, nullptr, 0.0};
+  const DecideArgs d = decide ? *decide : DecideArgs{nullptr, 0.0, nullptr, {}};
   k_drift<<<(n + 255) / 256, 256, 0, st>>>(b, n, dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2_bits,
-                                           atoms, q, img, old, k);
+                                           atoms, q, img, old, k, d);
   count_launch();
   return check_launch("drift");
 }

@@ -188,8 +188,8 @@ int rbx_engine::init() {
   ETRY(alloc(&cell_start, (size_t)ncell + 1));
   ETRY(alloc(&cell_scratch, cells_scratch_bytes(n, ncell)));
   ETRY(alloc(&list_scratch, full_list_scratch_bytes(n, ncell)));
-  ETRY(alloc(&dflags, 8));
-  ETRY(cuda_ok(cudaMemsetAsync(dflags, 0, sizeof(int) * 8, st), "memset"));
+  ETRY(alloc(&dflags, 12));  // [8], [9]: block counters of the drift and the RBE finalize
+  ETRY(cuda_ok(cudaMemsetAsync(dflags, 0, sizeof(int) * 12, st), "memset"));
   ETRY(alloc(&max_d2, 1));
   ETRY(alloc(&cand_total, 1));
   nfpart = rbl_fused_blocks(n);
@@ -486,21 +486,24 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
   const bool mixed = prm.precision == RBX_MIXED;
   const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
   if (P > 0) {
-    if (!k_injected) {
-      ETRY(cuda_ok(cudaMemsetAsync(dflags + 2, 0, sizeof(int), st), "memset"));
-      if (sog)
-        ETRY(launch_rbsog_sample(P, sog_tables, prm.random_seed, (uint64_t)(int64_t)epoch,
-                                 epoch_dev, mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
-      else
-        ETRY(launch_rbe_sample(P, sample_tables, tcnt, ttot, prm.random_seed, epoch, epoch_dev,
-                               mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
-    }
+    // a failed draw raises dflags[2] until check_sampler reads it; RBE samples
+    // are drawn inside the structure-factor kernel (no launch of their own)
+    const SampleArgs sa = make_sample_args(sample_tables, tcnt, ttot, prm.random_seed, epoch,
+                                           epoch_dev, mx, my, mz, mixed ? mi : nullptr,
+                                           dflags + 2);
+    const bool draw_in_rho = !k_injected && !sog && n > 0;
+    if (!k_injected && sog)
+      ETRY(launch_rbsog_sample(P, sog_tables, prm.random_seed, (uint64_t)(int64_t)epoch,
+                               epoch_dev, mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
+    else if (!k_injected && !draw_in_rho)
+      ETRY(launch_rbe_sample(P, sample_tables, tcnt, ttot, prm.random_seed, epoch, epoch_dev,
+                             mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
     if (mixed)
       ETRY(launch_rbe_rho_partial_mixed(n, Pk, mi, atoms, part_re, part_im, nparts, st,
-                                        tun.rho_kpt));
+                                        tun.rho_kpt, draw_in_rho ? &sa : nullptr));
     else
       ETRY(launch_rbe_rho_partial_f64(dbox, n, Pk, mx, my, mz, q, x, y, z, part_re, part_im,
-                                      nparts, st, tun.rho_kpt));
+                                      nparts, st, tun.rho_kpt, draw_in_rho ? &sa : nullptr));
   }
   const int mean_parts = rbl ? nrbl + (spec_natoms ? SPEC_PARTS : 0) : 0;
   if (sog) {
@@ -515,7 +518,8 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
     ETRY(launch_rbe_finalize(dbox, P, P > 0 ? nparts : 0, part_re, part_im, mx, my, mz,
                              prm.alpha, S, prm.qqr2e, qsq, qsum, P > 0 ? rho_re : nullptr,
                              rho_im, P > 0 ? ek : nullptr, virk, P > 0 ? tab : nullptr,
-                             mean_parts, fpart, n, rbl ? mean : nullptr, kterm, st));
+                             mean_parts, fpart, n, rbl ? mean : nullptr, kterm, st,
+                             (unsigned*)(dflags + 9)));
   RbeForceOut o;
   o.f_pair_x = fpx;
   o.f_pair_y = fpy;
@@ -822,9 +826,12 @@ int rbx_engine::check_sampler() {
     set_error("real-space kernel: a candidate-row copy did not complete (status %d)", h[1]);
     return RBX_ERR_CUDA;
   }
-  if (h[0] && P > 0 && !k_injected) {
-    set_error("k-sampler: a sample needed more than 64 draws to avoid m = 0");
-    return RBX_ERR_SAMPLER;
+  if (h[0]) {
+    ETRY(cuda_ok(cudaMemset(dflags + 2, 0, sizeof(int)), "memset"));  // reported once
+    if (P > 0 && !k_injected) {
+      set_error("k-sampler: a sample needed more than 64 draws to avoid m = 0");
+      return RBX_ERR_SAMPLER;
+    }
   }
   return RBX_OK;
 }
@@ -907,32 +914,49 @@ int rbx_engine::capture_step_graph() {
 // after what st has captured so far, its body is captured on st_body.
 int rbx_engine::capture_step_into(cudaGraph_t g) {
   const unsigned long long l0 = rbx_launch_count();
-  ETRY(capture_step_head());
-  ETRY(capture_step_tail(g));
+  cudaGraphConditionalHandle cond;
+  ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault),
+               "cudaGraphConditionalHandleCreate"));
+  bool decided = false;
+  ETRY(capture_step_head(&cond, &decided));
+  ETRY(capture_step_tail(g, &cond, decided));
   graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
   return RBX_OK;
 }
 
 // First part of a step: half kick, drift with the skin check (+ SHAKE).
-int rbx_engine::capture_step_head() {
+// Without SHAKE (which moves atoms after the drift) the drift kernel takes the
+// rebuild decision when given the step's conditional handle; max_d2 and its
+// block counter are then cleared by the kernel itself after each decision
+// (and by graph_run_begin before the first step).
+int rbx_engine::capture_step_head(const cudaGraphConditionalHandle* cond, bool* decided) {
   if (nh_on) ETRY(nh_initial(dflags + 4, 1, st));  // the device epoch is still the last step's
-  ETRY(launch_zero_u64(max_d2, st));
+  const bool fold = cond && !shake_nc && n > 0;
+  if (!fold) ETRY(launch_zero_u64(max_d2, st));
   const KickArgs kick{fx, fy, fz, type, inv_mass, 0.5 * prm.dt};
+  const double thr = prm.skin * 0.5;
+  const DecideArgs dec{(unsigned*)(dflags + 8), thr * thr, dflags + 4, fold ? *cond : 0};
   ETRY(launch_drift(dbox, n, prm.dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2, atoms, q,
                      ImageRefs{{img[0], img[1], img[2]}}, Pos3{shake_nc ? xs : nullptr, ys, zs},
-                     st, &kick));
+                     st, &kick, fold ? &dec : nullptr));
   if (shake_nc) ETRY(shake_a(st));
+  if (decided) *decided = fold;
   return RBX_OK;
 }
 
 // Rest of a step, captured on st into g: rebuild decision and the rebuild
 // under an IF node, forces, second half kick (+ RATTLE, thermostat).
-int rbx_engine::capture_step_tail(cudaGraph_t g) {
+int rbx_engine::capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandle* cond_in,
+                                  bool decided) {
   cudaGraphConditionalHandle cond;
-  ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault),
-               "cudaGraphConditionalHandleCreate"));
+  if (cond_in) {
+    cond = *cond_in;
+  } else {
+    ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault),
+                 "cudaGraphConditionalHandleCreate"));
+  }
   const double thr = prm.skin * 0.5;
-  ETRY(launch_step_decide(max_d2, thr * thr, dflags + 4, cond, st));
+  if (!decided) ETRY(launch_step_decide(max_d2, thr * thr, dflags + 4, cond, st));
   // the conditional node after everything captured so far on st
   cudaStreamCaptureStatus cs;
   cudaGraph_t capg = nullptr;
@@ -1016,6 +1040,9 @@ int rbx_engine::graph_run_begin(cudaStream_t s) {
                  "D2D"));
   run_init[0] = epoch;  // [4] epoch, [5] rebuilds inside the graph
   run_init[1] = 0;
+  // the maximum displacement and the drift's block counter start from zero
+  ETRY(cuda_ok(cudaMemsetAsync(max_d2, 0, sizeof(unsigned long long), s), "memset"));
+  ETRY(cuda_ok(cudaMemsetAsync(dflags + 8, 0, sizeof(int), s), "memset"));
   return cuda_ok(cudaMemcpyAsync(dflags + 4, run_init, sizeof(int) * 2, cudaMemcpyHostToDevice, s),
                  "H2D");
 }

@@ -212,8 +212,12 @@ struct rbx_engine {
   rbx::ArraySet state_set(bool save) const;
   int capture_step_graph();
   int capture_step_into(cudaGraph_t g);
-  int capture_step_head();               // kick, drift (+ SHAKE) on st
-  int capture_step_tail(cudaGraph_t g);  // decide, rebuild (IF node), forces, ... on st
+  // kick, drift (+ SHAKE) on st; with cond (same graph as the tail) the drift
+  // kernel takes the rebuild decision itself, and *decided says whether it does
+  int capture_step_head(const cudaGraphConditionalHandle* cond = nullptr, bool* decided = nullptr);
+  // decide (unless decided), rebuild (IF node on cond, or a new handle), forces, ... on st
+  int capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandle* cond = nullptr,
+                        bool decided = false);
   int capture_host_graphs();
   void release_host_graphs();
   int graph_run_begin(cudaStream_t s);

@@ -36,19 +36,37 @@ struct RbeForceOut {
 
 // ---- k-space (rbx_rbe.cu) ----
 int rbe_partial_blocks(int n);
+// The RBE k-sampler's inputs (launch_rbe_sample) for drawing the samples
+// inside the structure-factor kernels: tables null = read the samples instead.
+struct SampleArgs {
+  const double* tables;  // the three cumulative per-axis tables, concatenated
+  int c0, c1, c2;
+  double t0, t1, t2;
+  uint32_t key0, key1;   // the seed
+  uint64_t step_arg;
+  const int* step_dev;   // device step (inside a step graph), else step_arg
+  double *mx, *my, *mz;  // samples out (block column 0)
+  int* mi;               // integer copy (may be null)
+  int* status;           // raised on a failed draw
+};
+SampleArgs make_sample_args(const double* tables, const int cnt[3], const double tot[3],
+                            uint64_t seed, int64_t step, const int* step_dev, double* mx,
+                            double* my, double* mz, int* mi, int* status);
 int launch_rbe_rho_partial_f64(const DBox& b, int n, int p, const double* mx, const double* my,
                                const double* mz, const double* q, const double* x,
                                const double* y, const double* z, double* part_re,
-                               double* part_im, int nblocks, cudaStream_t st, int kpt = 4);
+                               double* part_im, int nblocks, cudaStream_t st, int kpt = 4,
+                               const SampleArgs* sample = nullptr);
 int launch_rbe_rho_partial_mixed(int n, int p, const int* mi, const uint4* atoms,
                                  double* part_re, double* part_im, int nblocks, cudaStream_t st,
-                                 int kpt = 4);
+                                 int kpt = 4, const SampleArgs* sample = nullptr);
 int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
                         const double* part_im, const double* mx, const double* my,
                         const double* mz, double alpha, double S, double qqr2e, double qsq,
                         double qsum, double* rho_re, double* rho_im, double* energy,
                         double* virial, KTab* tab, int mean_parts, const double* fpart,
-                        int n_atoms, double* mean_out, double* kterm, cudaStream_t st);
+                        int n_atoms, double* mean_out, double* kterm, cudaStream_t st,
+                        unsigned* sum_ctr = nullptr);
 // kterm: scratch of 8 p doubles for the per-k energy/virial terms (parallel
 // finalize); when null and energy is requested, one block does the finalize.
 int launch_rbe_force_f64(int n, int p, const KTab* tab, const double* q, const double* x,
@@ -392,11 +410,20 @@ struct KickArgs {
   const double* inv_mass;
   double half_dt;
 };
+// decide (may be null; inside a step graph only): the step's rebuild decision
+// taken by the drift's last block (k_step_decide's test on max_d2 > thr2,
+// epoch += 1), which then clears max_d2 and ctr (zero before the first step).
+struct DecideArgs {
+  unsigned* ctr;
+  double thr2;
+  int* epoch;
+  cudaGraphConditionalHandle cond;
+};
 int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* z,
                  double* vx, double* vy, double* vz, const double* x0,
                  const double* y0, const double* z0, unsigned long long* max_d2_bits,
                  uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st,
-                 const KickArgs* kick = nullptr);
+                 const KickArgs* kick = nullptr, const DecideArgs* decide = nullptr);
 // CVFF special-bond correction of the RBL pair force (rbx_special.cu): its
 // SPEC_PARTS per-block force sums follow the fused kernel's in fpart.
 constexpr int SPEC_PARTS = 1184;  // 8 blocks per SM of 148: about one atom per thread

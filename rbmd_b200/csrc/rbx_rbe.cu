@@ -29,6 +29,76 @@ namespace rbx {
 constexpr int RBE_BLOCK = 256;
 constexpr int RBE_WARPS = RBE_BLOCK / 32;
 
+__device__ __forceinline__ int table_pick(const double* cdf, int cnt, double total, uint64_t u53) {
+  const double target = (double)u53 * (1.0 / 9007199254740992.0) * total;
+  int lo = 0, hi = cnt - 1;  // first index with target < cdf[idx], else cnt - 1
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (target < cdf[mid])
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  const int idx = lo;
+  if (idx == 0) return 0;
+  return (idx & 1) ? (idx + 1) / 2 : -(idx / 2);
+}
+
+// One RBE k-sample s of MD step `step` (RBESampleMH's density, drawn exactly
+// per axis): Philox4x32-10 of counter {s, attempt, step} under key (k0, k1),
+// the three inverse-CDF picks, |m| = 0 redrawn (at most 64 attempts).  false
+// when every attempt gave m = 0.
+__device__ __forceinline__ bool rbe_draw(int s, const SampleArgs& sa, const double* w0,
+                                         uint64_t step, int m[3]) {
+  const double* w1 = w0 + sa.c0;
+  const double* w2 = w1 + sa.c1;
+  for (int a = 0; a < 64; ++a) {
+    uint32_t c[4] = {(uint32_t)s, (uint32_t)(2 * a), (uint32_t)step, (uint32_t)(step >> 32)};
+    philox4x32_10(c, sa.key0, sa.key1);
+    uint32_t d[4] = {(uint32_t)s, (uint32_t)(2 * a + 1), (uint32_t)step, (uint32_t)(step >> 32)};
+    philox4x32_10(d, sa.key0, sa.key1);
+    m[0] = table_pick(w0, sa.c0, sa.t0, ((((uint64_t)c[0]) << 32) | c[1]) >> 11);
+    m[1] = table_pick(w1, sa.c1, sa.t1, ((((uint64_t)c[2]) << 32) | c[3]) >> 11);
+    m[2] = table_pick(w2, sa.c2, sa.t2, ((((uint64_t)d[0]) << 32) | d[1]) >> 11);
+    if (m[0] != 0 || m[1] != 0 || m[2] != 0) return true;
+  }
+  return false;
+}
+
+// With sa.tables the k-vectors of the block's k-group are drawn here (warp 0,
+// into shared memory) instead of read: block column 0 also writes them out
+// (double and integer copies) and raises sa.status on a failed draw.
+template <int KPT>
+__device__ __forceinline__ void rbe_group_samples(const SampleArgs& sa, int p, int kbase,
+                                                  int (*s_m)[32 * KPT]) {
+  if (threadIdx.x < 32) {
+    const uint64_t step = sa.step_dev ? (uint64_t)(int64_t)*sa.step_dev : sa.step_arg;
+#pragma unroll 1
+    for (int t = 0; t < KPT; ++t) {
+      const int slot = threadIdx.x + 32 * t, k = kbase + slot;
+      int m[3] = {0, 0, 0};
+      if (k < p) {
+        const bool ok = rbe_draw(k, sa, sa.tables, step, m);
+        if (blockIdx.x == 0) {
+          if (!ok) atomicOr(sa.status, 1);
+          sa.mx[k] = m[0];
+          sa.my[k] = m[1];
+          sa.mz[k] = m[2];
+          if (sa.mi) {
+            sa.mi[3 * k] = m[0];
+            sa.mi[3 * k + 1] = m[1];
+            sa.mi[3 * k + 2] = m[2];
+          }
+        }
+      }
+      s_m[0][slot] = m[0];
+      s_m[1][slot] = m[1];
+      s_m[2][slot] = m[2];
+    }
+  }
+  __syncthreads();
+}
+
 template <int KPT>
 __global__ void __launch_bounds__(RBE_BLOCK)
 k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kzs,
@@ -36,20 +106,25 @@ k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kz
                       const double* __restrict__ mz, const double* __restrict__ q,
                       const double* __restrict__ x, const double* __restrict__ y,
                       const double* __restrict__ z, double* __restrict__ part_re,
-                      double* __restrict__ part_im) {
+                      double* __restrict__ part_im, SampleArgs sa) {
   __shared__ double s_re[RBE_WARPS][(32 * KPT)];
   __shared__ double s_im[RBE_WARPS][(32 * KPT)];
+  __shared__ int s_m[3][32 * KPT];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int kbase = blockIdx.y * (32 * KPT);
+  if (sa.tables) rbe_group_samples<KPT>(sa, p, kbase, s_m);
   double kx[KPT], ky[KPT], kz[KPT], sr[KPT], si[KPT];
 #pragma unroll
   for (int t = 0; t < KPT; ++t) {
     const int k = kbase + lane + 32 * t;
     const bool ok = k < p;
+    const double m0 = sa.tables ? (double)s_m[0][lane + 32 * t] : (ok ? mx[k] : 0.0);
+    const double m1 = sa.tables ? (double)s_m[1][lane + 32 * t] : (ok ? my[k] : 0.0);
+    const double m2 = sa.tables ? (double)s_m[2][lane + 32 * t] : (ok ? mz[k] : 0.0);
     // k = 2 pi m / L, evaluated as (2 pi * m) / L like the reference.
-    kx[t] = ok ? (2 * RBX_PI * mx[k]) / kxs : 0.0;
-    ky[t] = ok ? (2 * RBX_PI * my[k]) / kys : 0.0;
-    kz[t] = ok ? (2 * RBX_PI * mz[k]) / kzs : 0.0;
+    kx[t] = ok ? (2 * RBX_PI * m0) / kxs : 0.0;
+    ky[t] = ok ? (2 * RBX_PI * m1) / kys : 0.0;
+    kz[t] = ok ? (2 * RBX_PI * m2) / kzs : 0.0;
     sr[t] = 0.0;
     si[t] = 0.0;
   }
@@ -104,20 +179,22 @@ template <int KPT>
 __global__ void __launch_bounds__(RBE_BLOCK)
 k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
                         const uint4* __restrict__ atoms, double* __restrict__ part_re,
-                        double* __restrict__ part_im) {
+                        double* __restrict__ part_im, SampleArgs sa) {
   __shared__ double s_re[RBE_WARPS][(32 * KPT)];
   __shared__ double s_im[RBE_WARPS][(32 * KPT)];
+  __shared__ int s_m[3][32 * KPT];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int kbase = blockIdx.y * (32 * KPT);
+  if (sa.tables) rbe_group_samples<KPT>(sa, p, kbase, s_m);
   int m0[KPT], m1[KPT], m2[KPT];
   float hr[KPT], lr[KPT], hi[KPT], li[KPT];
 #pragma unroll
   for (int t = 0; t < KPT; ++t) {
     const int k = kbase + lane + 32 * t;
     const bool ok = k < p;
-    m0[t] = ok ? mi[3 * k] : 0;
-    m1[t] = ok ? mi[3 * k + 1] : 0;
-    m2[t] = ok ? mi[3 * k + 2] : 0;
+    m0[t] = sa.tables ? s_m[0][lane + 32 * t] : (ok ? mi[3 * k] : 0);
+    m1[t] = sa.tables ? s_m[1][lane + 32 * t] : (ok ? mi[3 * k + 1] : 0);
+    m2[t] = sa.tables ? s_m[2][lane + 32 * t] : (ok ? mi[3 * k + 2] : 0);
     hr[t] = lr[t] = hi[t] = li[t] = 0.f;
   }
   const float ang = (float)(2.0 * RBX_PI / 4294967296.0);
@@ -274,9 +351,48 @@ k_rbe_finalize(int p, int nparts, const double* __restrict__ part_re,
 // Parallel finalize: block k < p reduces the partials of k-vector k (fixed
 // strided order, then a fixed tree) and writes rho(k), the force table entry
 // and its seven energy/virial terms to kterm[k][0..6]; blocks p..p+2 reduce
-// the per-block pair-force sums into the mean force.  k_rbe_energy_sum then
-// adds the per-k terms in increasing k (one warp, fixed order).
+// the per-block pair-force sums into the mean force.  The per-k terms are then
+// added in increasing k by one warp in a fixed order: k_rbe_energy_sum, or,
+// with es.ctr, the last block of this kernel to finish.
 constexpr int FK_BLOCK = 128;
+
+struct EnergySum {
+  unsigned* ctr;  // block counter, zero before the launch; cleared again by the last block
+  double alpha, V, qqr2e, qsq, qsum;
+  double* energy;
+  double* virial;
+};
+
+__device__ __forceinline__ void rbe_energy_sum_warp(int p, const double* __restrict__ kterm,
+                                                    const EnergySum& es, bool coherent) {
+  const int lane = threadIdx.x & 31;
+  double t[7] = {0, 0, 0, 0, 0, 0, 0};
+  // each lane adds its k in increasing order; the seven loads of a k are independent
+  for (int k = lane; k < p; k += 32) {
+    const double* r = kterm + (size_t)k * 8;
+#pragma unroll
+    for (int c = 0; c < 7; ++c) t[c] += coherent ? __ldcg(r + c) : r[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 7; ++c)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t[c] += __shfl_down_sync(0xffffffffu, t[c], o);
+  if (lane == 0) {
+    const double MY_PIS = 1.77245385090551602729, MY_PI2 = 1.57079632679489661923;
+    const double etot =
+        t[0] - (sqrt(es.alpha) * es.qsq / MY_PIS + MY_PI2 * es.qsum * es.qsum / (es.alpha * es.V));
+    *es.energy = etot * es.qqr2e;
+    for (int c = 0; c < 6; ++c) es.virial[c] = t[1 + c] * es.qqr2e;
+  }
+}
+
+__device__ void rbe_finalize_one(int k, int p, int nparts, const double* __restrict__ part_re,
+                                 const double* __restrict__ part_im, const double* __restrict__ mx,
+                                 const double* __restrict__ my, const double* __restrict__ mz,
+                                 double Lx, double Ly, double Lz, double alpha, double S,
+                                 double qqr2e, double* __restrict__ rho_re,
+                                 double* __restrict__ rho_im, KTab* __restrict__ tab,
+                                 double* __restrict__ kterm, double* sh);
 
 __global__ void __launch_bounds__(FK_BLOCK)
 k_rbe_finalize_k(int p, int nparts, const double* __restrict__ part_re,
@@ -285,8 +401,10 @@ k_rbe_finalize_k(int p, int nparts, const double* __restrict__ part_re,
                  double Ly, double Lz, double alpha, double S, double qqr2e,
                  double* __restrict__ rho_re, double* __restrict__ rho_im,
                  KTab* __restrict__ tab, double* __restrict__ kterm, int mean_parts,
-                 const double* __restrict__ fpart, double n_atoms, double* __restrict__ mean_out) {
+                 const double* __restrict__ fpart, double n_atoms, double* __restrict__ mean_out,
+                 EnergySum es) {
   __shared__ double sh[FK_BLOCK / 32];
+  __shared__ bool s_last;
   const int blk = blockIdx.x;
   if (blk >= p) {  // mean of the pair-force block sums, one component per block
     const int d = blk - p;
@@ -294,9 +412,30 @@ k_rbe_finalize_k(int p, int nparts, const double* __restrict__ part_re,
     for (int b = threadIdx.x; b < mean_parts; b += FK_BLOCK) s += fpart[(size_t)b * 3 + d];
     s = block_sum_det<FK_BLOCK>(s, sh);
     if (threadIdx.x == 0) mean_out[d] = s / n_atoms;
-    return;
+  } else {
+    rbe_finalize_one(blk, p, nparts, part_re, part_im, mx, my, mz, Lx, Ly, Lz, alpha, S, qqr2e,
+                     rho_re, rho_im, tab, kterm, sh);
   }
-  const int k = blk;
+  if (!es.ctr) return;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(es.ctr, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x < 32) rbe_energy_sum_warp(p, kterm, es, true);
+  if (threadIdx.x == 0) *es.ctr = 0u;
+}
+
+// Block k's part of the finalize (all threads of the block call it).
+__device__ void rbe_finalize_one(int k, int p, int nparts, const double* __restrict__ part_re,
+                                 const double* __restrict__ part_im, const double* __restrict__ mx,
+                                 const double* __restrict__ my, const double* __restrict__ mz,
+                                 double Lx, double Ly, double Lz, double alpha, double S,
+                                 double qqr2e, double* __restrict__ rho_re,
+                                 double* __restrict__ rho_im, KTab* __restrict__ tab,
+                                 double* __restrict__ kterm, double* sh) {
   double r = 0.0, im = 0.0;
   const double* pr = part_re + (size_t)k * nparts;
   const double* pi = part_im + (size_t)k * nparts;
@@ -346,27 +485,8 @@ k_rbe_finalize_k(int p, int nparts, const double* __restrict__ part_re,
 }
 
 __global__ void __launch_bounds__(32)
-k_rbe_energy_sum(int p, const double* __restrict__ kterm, double alpha, double V, double qqr2e,
-                 double qsq, double qsum, double* __restrict__ energy,
-                 double* __restrict__ virial) {
-  const int lane = threadIdx.x;
-  double t[7] = {0, 0, 0, 0, 0, 0, 0};
-  // each lane adds its k in increasing order; the seven loads of a k are independent
-  for (int k = lane; k < p; k += 32) {
-    const double* r = kterm + (size_t)k * 8;
-#pragma unroll
-    for (int c = 0; c < 7; ++c) t[c] += r[c];
-  }
-#pragma unroll
-  for (int c = 0; c < 7; ++c)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t[c] += __shfl_down_sync(0xffffffffu, t[c], o);
-  if (lane == 0) {
-    const double MY_PIS = 1.77245385090551602729, MY_PI2 = 1.57079632679489661923;
-    const double etot = t[0] - (sqrt(alpha) * qsq / MY_PIS + MY_PI2 * qsum * qsum / (alpha * V));
-    *energy = etot * qqr2e;
-    for (int c = 0; c < 6; ++c) virial[c] = t[1 + c] * qqr2e;
-  }
+k_rbe_energy_sum(int p, const double* __restrict__ kterm, EnergySum es) {
+  rbe_energy_sum_warp(p, kterm, es, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -517,20 +637,6 @@ k_rbe_force_mixed(int n, int p, const KTab* __restrict__ tab, const uint4* __res
 // cdf[t] = w[0] + ... + w[t], accumulated left to right on the host exactly as
 // the oracle's linear scan accumulates, so the first t with target < cdf[t]
 // (binary search) is the oracle's pick.
-__device__ __forceinline__ int table_pick(const double* cdf, int cnt, double total, uint64_t u53) {
-  const double target = (double)u53 * (1.0 / 9007199254740992.0) * total;
-  int lo = 0, hi = cnt - 1;  // first index with target < cdf[idx], else cnt - 1
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (target < cdf[mid])
-      hi = mid;
-    else
-      lo = mid + 1;
-  }
-  const int idx = lo;
-  if (idx == 0) return 0;
-  return (idx & 1) ? (idx + 1) / 2 : -(idx / 2);
-}
 
 constexpr int kSampleSmemTables = 6144;  // staged table entries (48 KB)
 constexpr int SAMPLE_BLOCK = 128;
@@ -553,32 +659,30 @@ k_rbe_sample(int p, const double* __restrict__ tables, int c0, int c1, int c2, d
   if (s >= p) return;
   // the MD step: a device copy inside a step graph
   const uint64_t step = step_dev ? (uint64_t)(int64_t)*step_dev : step_arg;
-  const double* w0 = staged ? s_tab : tables;
-  const double* w1 = w0 + c0;
-  const double* w2 = w0 + c0 + c1;
-  for (int a = 0; a < 64; ++a) {
-    uint32_t c[4] = {(uint32_t)s, (uint32_t)(2 * a), (uint32_t)step, (uint32_t)(step >> 32)};
-    philox4x32_10(c, key0, key1);
-    uint32_t d[4] = {(uint32_t)s, (uint32_t)(2 * a + 1), (uint32_t)step, (uint32_t)(step >> 32)};
-    philox4x32_10(d, key0, key1);
-    const int m0 = table_pick(w0, c0, t0, ((((uint64_t)c[0]) << 32) | c[1]) >> 11);
-    const int m1 = table_pick(w1, c1, t1, ((((uint64_t)c[2]) << 32) | c[3]) >> 11);
-    const int m2 = table_pick(w2, c2, t2, ((((uint64_t)d[0]) << 32) | d[1]) >> 11);
-    if (m0 != 0 || m1 != 0 || m2 != 0) {
-      if (mx) {
-        mx[s] = m0;
-        my[s] = m1;
-        mz[s] = m2;
-      }
-      if (mi) {
-        mi[3 * s] = m0;
-        mi[3 * s + 1] = m1;
-        mi[3 * s + 2] = m2;
-      }
-      return;
-    }
+  SampleArgs sa{};
+  sa.c0 = c0;
+  sa.c1 = c1;
+  sa.c2 = c2;
+  sa.t0 = t0;
+  sa.t1 = t1;
+  sa.t2 = t2;
+  sa.key0 = key0;
+  sa.key1 = key1;
+  int m[3];
+  if (!rbe_draw(s, sa, staged ? s_tab : tables, step, m)) {
+    atomicOr(status, 1);
+    return;
   }
-  atomicOr(status, 1);
+  if (mx) {
+    mx[s] = m[0];
+    my[s] = m[1];
+    mz[s] = m[2];
+  }
+  if (mi) {
+    mi[3 * s] = m[0];
+    mi[3 * s + 1] = m[1];
+    mi[3 * s + 2] = m[2];
+  }
 }
 
 // Integer copy of injected samples (for the mixed kernels).
@@ -684,14 +788,16 @@ int rbe_partial_blocks(int n) {
 int launch_rbe_rho_partial_f64(const DBox& b, int n, int p, const double* mx, const double* my,
                                const double* mz, const double* q, const double* x,
                                const double* y, const double* z, double* part_re,
-                               double* part_im, int nblocks, cudaStream_t st, int kpt) {
+                               double* part_im, int nblocks, cudaStream_t st, int kpt,
+                               const SampleArgs* sample) {
   if (n <= 0 || p <= 0) return RBX_OK;
   const int chunk = (n + nblocks - 1) / nblocks;
   dim3 grid(nblocks, (p + 32 * kpt - 1) / (32 * kpt));
+  const SampleArgs sa = sample ? *sample : SampleArgs{};
 #define RHO_F64(K)                                                                             \
   k_rbe_rho_partial_f64<K><<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, b.len[0], b.len[1],       \
                                                        b.len[2], mx, my, mz, q, x, y, z,       \
-                                                       part_re, part_im)
+                                                       part_re, part_im, sa)
   switch (kpt) {
     case 1: RHO_F64(1); break;
     case 2: RHO_F64(2); break;
@@ -705,12 +811,14 @@ int launch_rbe_rho_partial_f64(const DBox& b, int n, int p, const double* mx, co
 
 int launch_rbe_rho_partial_mixed(int n, int p, const int* mi, const uint4* atoms,
                                  double* part_re, double* part_im, int nblocks, cudaStream_t st,
-                                 int kpt) {
+                                 int kpt, const SampleArgs* sample) {
   if (n <= 0 || p <= 0) return RBX_OK;
   const int chunk = (n + nblocks - 1) / nblocks;
   dim3 grid(nblocks, (p + 32 * kpt - 1) / (32 * kpt));
+  const SampleArgs sa = sample ? *sample : SampleArgs{};
 #define RHO_MIX(K) \
-  k_rbe_rho_partial_mixed<K><<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, mi, atoms, part_re, part_im)
+  k_rbe_rho_partial_mixed<K><<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, mi, atoms, part_re, part_im, \
+                                                         sa)
   switch (kpt) {
     case 1: RHO_MIX(1); break;
     case 2: RHO_MIX(2); break;
@@ -727,7 +835,8 @@ int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
                         const double* mz, double alpha, double S, double qqr2e, double qsq,
                         double qsum, double* rho_re, double* rho_im, double* energy,
                         double* virial, KTab* tab, int mean_parts, const double* fpart,
-                        int n_atoms, double* mean_out, double* kterm, cudaStream_t st) {
+                        int n_atoms, double* mean_out, double* kterm, cudaStream_t st,
+                        unsigned* sum_ctr) {
   if (energy && !kterm) {  // no per-k scratch: one block does it all
     k_rbe_finalize<<<1, FIN_WIDE, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
                                             b.len[1], b.len[2], alpha, S, qqr2e, qsq, qsum,
@@ -737,18 +846,22 @@ int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
     return check_launch("rbe_finalize");
   }
   const int grid = p + (mean_out ? 3 : 0);
+  EnergySum es{nullptr, alpha, b.len[0] * b.len[1] * b.len[2], qqr2e, qsq, qsum, energy, virial};
+  // the energy sum in the finalize's last block when a counter is given
+  const bool fold = energy && sum_ctr && grid > 0 && p > 0;
   if (grid > 0) {
+    EnergySum ek = es;
+    ek.ctr = fold ? sum_ctr : nullptr;
     k_rbe_finalize_k<<<grid, FK_BLOCK, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
                                                 b.len[1], b.len[2], alpha, S, qqr2e, rho_re,
                                                 rho_im, tab, energy ? kterm : nullptr, mean_parts,
-                                                fpart, (double)n_atoms, mean_out);
+                                                fpart, (double)n_atoms, mean_out, ek);
     count_launch();
     const int rc = check_launch("rbe_finalize_k");
     if (rc) return rc;
   }
-  if (energy) {
-    k_rbe_energy_sum<<<1, 32, 0, st>>>(p, kterm, alpha, b.len[0] * b.len[1] * b.len[2], qqr2e, qsq,
-                                      qsum, energy, virial);
+  if (energy && !fold) {
+    k_rbe_energy_sum<<<1, 32, 0, st>>>(p, kterm, es);
     count_launch();
   }
   return check_launch("rbe_energy_sum");
@@ -816,6 +929,29 @@ int launch_rbe_sample(int p, const double* tables, const int cnt[3], const doubl
       (uint32_t)(seed >> 32), (uint64_t)step, step_dev, mx, my, mz, mi, status);
   count_launch();
   return check_launch("rbe_sample");
+}
+
+SampleArgs make_sample_args(const double* tables, const int cnt[3], const double tot[3],
+                            uint64_t seed, int64_t step, const int* step_dev, double* mx,
+                            double* my, double* mz, int* mi, int* status) {
+  SampleArgs sa{};
+  sa.tables = tables;
+  sa.c0 = cnt[0];
+  sa.c1 = cnt[1];
+  sa.c2 = cnt[2];
+  sa.t0 = tot[0];
+  sa.t1 = tot[1];
+  sa.t2 = tot[2];
+  sa.key0 = (uint32_t)seed;
+  sa.key1 = (uint32_t)(seed >> 32);
+  sa.step_arg = (uint64_t)step;
+  sa.step_dev = step_dev;
+  sa.mx = mx;
+  sa.my = my;
+  sa.mz = mz;
+  sa.mi = mi;
+  sa.status = status;
+  return sa;
 }
 
 int launch_m_to_int(int p, const double* mx, const double* my, const double* mz, int* mi,
