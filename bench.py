@@ -16,7 +16,9 @@ e2e        mixed form through rbx_engine_step_host: host x, v in (pinned), one
 roofline   the fused RBL filter + pair-force kernel against measured HBM
            bandwidth; its algorithmic bytes per launch are the candidate
            indices read (4 B each) plus 44 B of per-atom traffic (count,
-           atom record, type, two hash keys, force out).
+           atom record, type, two hash keys, force out).  roofline.issue: the
+           same launch against the SM issue limit (warp instructions per launch
+           from an ncu count per candidate), the bound that holds it.
 cpu_baseline  the FP64 host oracle (same step, OpenMP over all host cores).
 parity_vs_oracle  both forms against the FP64 oracle at the same size: force,
            pair and k-space force errors, k-space energy and virial, pair
@@ -52,6 +54,11 @@ UNIT = "atom-steps/s"
 # rows streamed once, plus neighbour-record and key gathers that miss L2).  Rows and
 # gathers grow with N, so the traffic is scaled by N.
 RBL_TRAFFIC_BYTES_PER_ATOM = 2151.0
+# Warp instructions per 32 candidates of the same launch (186.7 M for 47.9 M candidates in
+# the N = 100,000 capture), and the SM issue limit they are compared with: one warp
+# instruction per cycle per SM sub-partition, four per SM.
+RBL_WARP_INSTR_PER_32_CAND = 124.7
+ISSUE_SLOTS_PER_SM_CYCLE = 4
 
 
 def _peaks():
@@ -532,6 +539,19 @@ def run_ours(args):
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at N=100000, "
                               "scaled by N",
             "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": phm[2]}
+    # the bound that holds the kernel: instruction issue (warp instructions per
+    # launch from the ncu count per candidate, against the SM count x 4 issue
+    # slots x the median SM clock sampled in the timed region)
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+    if sm_mhz:
+        instr = RBL_WARP_INSTR_PER_32_CAND * stats2.candidates / 32.0
+        issue_peak = torch.cuda.get_device_properties(0).multi_processor_count * \
+            ISSUE_SLOTS_PER_SM_CYCLE * sm_mhz * 1e6
+        roof["issue"] = {"achieved": instr / t_pair, "peak": issue_peak,
+                         "unit": "warp instructions/s", "frac": instr / t_pair / issue_peak,
+                         "warp_instructions_per_launch": instr,
+                         "source": "ncu smsp__inst_executed.sum per candidate at N=100000"}
     # ten steps hold about two list rebuilds (one every ~5 steps), like the GPU average
     base = cpu_baseline(n, p, 10, 1) if not args.no_cpu_baseline else None
     line = {
@@ -556,7 +576,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": 6 * 8 * n, "d2h_bytes_per_step": 9 * 8 * n},
         "gpu_launches": launches,
         "roofline": roof,
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "cpu_baseline": base,
     }
     if ws == 1 and not args.no_extras:  # the other configs and RBMD's kernels, one GPU
