@@ -595,9 +595,10 @@ def run_ours(args):
 def run_batched(args):
     """Batched replicas: R independent LJ electrolytes with
     log-uniform atom counts, mixed form, all advanced by one CUDA graph launch
-    per step (rbx_batch), against the same replicas stepped one engine at a
-    time: plain FP64 launch by launch (the one-replica-per-launch baseline)
-    and mixed with each engine's own step graph."""
+    per step (rbx_batch) in the phase-batched design (value) and in the
+    one-branch-per-replica design, against the same replicas stepped one
+    engine at a time: plain FP64 launch by launch (the one-replica-per-launch
+    baseline) and mixed with each engine's own step graph."""
     import torch
 
     from rbmd_b200 import rbx, systems
@@ -637,13 +638,23 @@ def run_batched(args):
         torch.cuda.synchronize()
         return ev0.elapsed_time(ev1)
 
-    ms_default = time_batch()
+    def time_design(mode):
+        b.set_mode(mode)
+        b.step(args.warmup)  # the first step captures the graph
+        return time_batch(), b.design
+
+    # the phase-batched graph (one launch per phase over all replicas; value)
+    # and the graph of one branch per replica, with the built-in launch
+    # shapes, then autotuned (per-replica shapes: the phased graph then takes
+    # one launch per shape and phase)
+    ms_batch, design = time_design(rbx.Batch.AUTO)
+    ms_branch_default, _ = time_design(rbx.Batch.BRANCHES)
     # autotuner: one timing per size bin, the other replicas of the bin reuse it
     t_tune = time.perf_counter()
     b.autotune()
     t_tune = time.perf_counter() - t_tune
-    b.step(args.warmup)
-    ms_batch = time_batch()
+    ms_branch, _ = time_design(rbx.Batch.BRANCHES)
+    ms_tuned, _ = time_design(rbx.Batch.AUTO)
     b.close()
     close(es)
 
@@ -682,9 +693,15 @@ def run_batched(args):
                                              "timing": "host wall clock, one graph launch per "
                                                        "engine and step"},
         "batched_over_fp64_baseline": value / (total * base_steps / t64),
-        "autotune": {"untuned_value": total * args.steps / (ms_default / 1e3),
+        "design": {1: "phased: one launch per phase over all replicas, a conditional rebuild "
+                      "node per replica",
+                   2: "branches: one graph branch per replica"}.get(design, str(design)),
+        "branch_graph": {"value": total * args.steps / (ms_branch_default / 1e3),
+                         "ms_per_step": ms_branch_default / args.steps,
+                         "autotuned_value": total * args.steps / (ms_branch / 1e3)},
+        "autotune": {"phased_autotuned_value": total * args.steps / (ms_tuned / 1e3),
                      "tuning_seconds": t_tune,
-                     "note": "value is with the autotuned launch shapes"},
+                     "note": "value and branch_graph.value use the built-in launch shapes"},
     }
     print(json.dumps(line), flush=True)
     return 0

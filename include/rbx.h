@@ -742,21 +742,41 @@ int rbx_lammps_write_charge(const char* path, const rbx_box* box, int n, int nty
 
 /* ---- Batches of replicas ------------------------------------------------
  * Independent engines on one device advanced together: each rbx_batch_step
- * MD step is one CUDA graph launch in which every replica's step is a
- * parallel branch (kick, drift, its own rebuild decision and conditional
- * rebuild, forces, second kick).  The engines stay owned by the caller and
+ * MD step is one CUDA graph launch.  Two designs of that graph:
+ *   RBX_BATCH_PHASED: one kernel launch per phase of the step over the blocks
+ *     of every replica (drift with the first half kick and the rebuild
+ *     decision; fused RBL force; structure factor with the k-sampling;
+ *     finalize; RBE force with the second half kick), each replica's rebuild
+ *     under its own conditional node between the drift and the RBL phase.
+ *     For RBL engines in the mixed form with RBE k-space, NVE, no SHAKE and
+ *     no special bonds;
+ *   RBX_BATCH_BRANCHES: every replica's own step graph as a parallel branch.
+ * RBX_BATCH_AUTO (the default) takes the phased design when every replica
+ * allows it, else the branches.  The engines stay owned by the caller and
  * must outlive the batch; each must have skin > 0 and profiling off.  Results
- * equal stepping each engine alone.  No counterpart in the reference (one
- * system per process). */
+ * equal stepping each engine alone, in either design.  No counterpart in the
+ * reference (one system per process). */
+#define RBX_BATCH_AUTO 0
+#define RBX_BATCH_PHASED 1
+#define RBX_BATCH_BRANCHES 2
 typedef struct rbx_batch rbx_batch;
 rbx_batch* rbx_batch_create(rbx_engine* const* engines, int count);
 /* Autotune every engine of a batch (rbx_engine_autotune without forcing:
- * replicas of one size bin share one timing); before the first rbx_batch_step. */
+ * replicas of one size bin share one timing); before the first rbx_batch_step.
+ * In the phased design replicas whose tuned launch shapes differ take
+ * separate launches of a phase. */
 int rbx_batch_autotune(rbx_batch* b);
 void rbx_batch_destroy(rbx_batch* b);
 int rbx_batch_step(rbx_batch* b, int nsteps);
 /* The stream the batch graph runs on (cudaStream_t). */
 void* rbx_batch_stream(rbx_batch* b);
+/* Request a design (RBX_BATCH_AUTO, _PHASED or _BRANCHES; the graph is
+ * captured again at the next step).  With RBX_BATCH_PHASED a batch whose
+ * replicas do not all allow it fails at rbx_batch_step. */
+int rbx_batch_set_mode(rbx_batch* b, int mode);
+/* The design of the captured graph (RBX_BATCH_PHASED or RBX_BATCH_BRANCHES),
+ * -1 before the first step after creation or a change of mode. */
+int rbx_batch_design(const rbx_batch* b);
 
 #ifdef __cplusplus
 }

@@ -556,14 +556,43 @@ __global__ void k_kick(int n, const double* __restrict__ fx, const double* __res
 // With decide.ctr (inside a step graph) the last block to finish takes the
 // step's rebuild decision as k_step_decide does, then clears the maximum and
 // the block counter for the next step.
-__global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double* __restrict__ y,
-                        double* __restrict__ z, double* __restrict__ vx,
-                        double* __restrict__ vy, double* __restrict__ vz,
-                        const double* __restrict__ x0, const double* __restrict__ y0,
-                        const double* __restrict__ z0, unsigned long long* __restrict__ max_d2,
-                        uint4* __restrict__ atoms, const double* __restrict__ q,
-                        ImageRefs img, Pos3 old, KickArgs kick, DecideArgs decide) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+struct DriftArgs {
+  DBox b;
+  int n;
+  double dt;
+  double *x, *y, *z, *vx, *vy, *vz;
+  const double *x0, *y0, *z0;
+  unsigned long long* max_d2;
+  uint4* atoms;
+  const double* q;
+  ImageRefs img;
+  Pos3 old;
+  KickArgs kick;
+  DecideArgs decide;
+};
+
+// Block bx of a grid of gx blocks.
+__device__ __forceinline__ void drift_body(const DriftArgs& A, int bx, int gx) {
+  const DBox& b = A.b;
+  const int n = A.n;
+  const double dt = A.dt;
+  double* __restrict__ x = A.x;
+  double* __restrict__ y = A.y;
+  double* __restrict__ z = A.z;
+  double* __restrict__ vx = A.vx;
+  double* __restrict__ vy = A.vy;
+  double* __restrict__ vz = A.vz;
+  const double* __restrict__ x0 = A.x0;
+  const double* __restrict__ y0 = A.y0;
+  const double* __restrict__ z0 = A.z0;
+  unsigned long long* __restrict__ max_d2 = A.max_d2;
+  uint4* __restrict__ atoms = A.atoms;
+  const double* __restrict__ q = A.q;
+  const ImageRefs& img = A.img;
+  const Pos3& old = A.old;
+  const KickArgs& kick = A.kick;
+  const DecideArgs& decide = A.decide;
+  const int i = bx * blockDim.x + threadIdx.x;
   double d2 = 0.0;
   if (i < n) {
     if (old.x) {  // positions before the drift, for SHAKE
@@ -617,7 +646,7 @@ __global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double
     __syncthreads();  // every warp of the block has folded its maximum in
     if (threadIdx.x == 0) {
       __threadfence();
-      if (atomicAdd(decide.ctr, 1u) == gridDim.x - 1) {  // the last block
+      if (atomicAdd(decide.ctr, 1u) == (unsigned)gx - 1) {  // the last block
         __threadfence();
         const unsigned long long m = atomicAdd(max_d2, 0ULL);
         *decide.epoch += 1;
@@ -628,6 +657,15 @@ __global__ void k_drift(DBox b, int n, double dt, double* __restrict__ x, double
       }
     }
   }
+}
+
+__global__ void __launch_bounds__(256) k_drift(DriftArgs a) { drift_body(a, blockIdx.x, gridDim.x); }
+
+__global__ void __launch_bounds__(256)
+k_drift_batch(const DriftArgs* __restrict__ a, const int* __restrict__ start, int nrep) {
+  const int r = batch_replica(start, nrep, blockIdx.x);
+  const int b0 = __ldg(start + r);
+  drift_body(a[r], blockIdx.x - b0, __ldg(start + r + 1) - b0);
 }
 
 __global__ void k_to_fixed(DBox b, int n, const double* __restrict__ x,
@@ -862,12 +900,37 @@ int launch_drift(const DBox& b, int n, double dt, double* x, double* y, double* 
                  uint4* atoms, const double* q, ImageRefs img, Pos3 old, cudaStream_t st,
                  const KickArgs* kick, const DecideArgs* decide) {
   if (n <= 0) return RBX_OK;
-  const KickArgs k = kick ? *kick : KickArgs{nullptr, nullptr, nullptr, nullptr, nullptr, 0.0};
-  const DecideArgs d = decide ? *decide : DecideArgs{nullptr, 0.0, nullptr, {}};
-  k_drift<<<(n + 255) / 256, 256, 0, st>>>(b, n, dt, x, y, z, vx, vy, vz, x0, y0, z0, max_d2_bits,
-                                           atoms, q, img, old, k, d);
+  DriftArgs a;
+  a.b = b;
+  a.n = n;
+  a.dt = dt;
+  a.x = x;
+  a.y = y;
+  a.z = z;
+  a.vx = vx;
+  a.vy = vy;
+  a.vz = vz;
+  a.x0 = x0;
+  a.y0 = y0;
+  a.z0 = z0;
+  a.max_d2 = max_d2_bits;
+  a.atoms = atoms;
+  a.q = q;
+  a.img = img;
+  a.old = old;
+  a.kick = kick ? *kick : KickArgs{nullptr, nullptr, nullptr, nullptr, nullptr, 0.0};
+  a.decide = decide ? *decide : DecideArgs{nullptr, 0.0, nullptr, {}};
+  const int grid = (n + 255) / 256;
+  if (batch_recorder()) return record_phase(PH_DRIFT, 0, grid, 256, 0, &a, sizeof a);
+  k_drift<<<grid, 256, 0, st>>>(a);
   count_launch();
   return check_launch("drift");
+}
+
+int launch_drift_batch(const void* args, const int* start, int nrep, int total, cudaStream_t st) {
+  k_drift_batch<<<total, 256, 0, st>>>(static_cast<const DriftArgs*>(args), start, nrep);
+  count_launch();
+  return check_launch("drift_batch");
 }
 
 int launch_to_fixed(const DBox& b, int n, const double* x, const double* y, const double* z,

@@ -974,6 +974,15 @@ int rbx_engine::capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandl
   cudaGraph_t body = np.conditional.phGraph_out[0];
   ETRY(cuda_ok(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
                "cudaStreamUpdateCaptureDependencies"));
+  ETRY(capture_rebuild_body(body));
+  ETRY(real_space(dflags + 4));
+  ETRY(kspace_and_combine(true, dflags + 4));
+  if (shake_nc) ETRY(shake_b(st));
+  if (nh_on) ETRY(nh_final(st));
+  return RBX_OK;
+}
+
+int rbx_engine::capture_rebuild_body(cudaGraph_t body) {
   const unsigned long long b0 = rbx_launch_count();
   ETRY(cuda_ok(cudaStreamBeginCaptureToGraph(st_body, body, nullptr, nullptr, 0,
                                              cudaStreamCaptureModeThreadLocal),
@@ -984,10 +993,40 @@ int rbx_engine::capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandl
   ETRY(brc);
   ETRY(cuda_ok(be, "cudaStreamEndCapture (rebuild body)"));
   graph_rebuild_launches = rbx_launch_count() - b0;
-  ETRY(real_space(dflags + 4));
-  ETRY(kspace_and_combine(true, dflags + 4));
-  if (shake_nc) ETRY(shake_b(st));
-  if (nh_on) ETRY(nh_final(st));
+  return RBX_OK;
+}
+
+// The launchers record instead of launching while rec is installed; the
+// recording runs inside a capture of st into a graph that is thrown away, so
+// a launch without a batched form (counted by rbx_launch_count) never runs.
+int rbx_engine::record_phased_step(BatchRecorder* rec, cudaGraphConditionalHandle cond) {
+  const bool ok = prm.neighbor_type == RBX_NEIGHBOR_RBL && prm.precision == RBX_MIXED && !sog &&
+                  !sog_pair && !shake_nc && !nh_on && !spec_natoms && n > 0 && P > 0 &&
+                  !profiling;
+  if (!ok) {
+    set_error("phase-batched step: needs an RBL engine in the mixed form with RBE k-space, "
+              "NVE, no SHAKE and no special bonds");
+    return RBX_ERR_INVALID;
+  }
+  ETRY(cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
+               "cudaStreamBeginCapture"));
+  batch_recorder() = rec;
+  const unsigned long long l0 = rbx_launch_count();
+  bool decided = false;
+  int rc = capture_step_head(&cond, &decided);
+  if (!rc) rc = real_space(dflags + 4);
+  if (!rc) rc = kspace_and_combine(true, dflags + 4);
+  batch_recorder() = nullptr;
+  const bool foreign = rbx_launch_count() != l0;
+  cudaGraph_t scratch = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &scratch);
+  if (scratch) cudaGraphDestroy(scratch);
+  ETRY(rc);
+  ETRY(cuda_ok(e, "cudaStreamEndCapture (phase recording)"));
+  if (foreign || !decided) {
+    set_error("phase-batched step: a kernel of the step has no batched form");
+    return RBX_ERR_INVALID;
+  }
   return RBX_OK;
 }
 

@@ -215,6 +215,11 @@ struct rbx_engine {
   // kick, drift (+ SHAKE) on st; with cond (same graph as the tail) the drift
   // kernel takes the rebuild decision itself, and *decided says whether it does
   int capture_step_head(const cudaGraphConditionalHandle* cond = nullptr, bool* decided = nullptr);
+  // the rebuild, captured on st_body into the body graph of an IF node
+  int capture_rebuild_body(cudaGraph_t body);
+  // a graph step without its rebuild, recorded for a phase-batched graph
+  // (rbx_batch.cu); RBX_ERR_INVALID when a kernel of the step has no batched form
+  int record_phased_step(rbx::BatchRecorder* rec, cudaGraphConditionalHandle cond);
   // decide (unless decided), rebuild (IF node on cond, or a new handle), forces, ... on st
   int capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandle* cond = nullptr,
                         bool decided = false);

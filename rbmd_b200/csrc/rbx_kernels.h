@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "rbx_common.cuh"
 
 namespace rbx {
@@ -451,5 +453,56 @@ int launch_to_fixed(const DBox& b, int n, const double* x, const double* y, cons
 int launch_max_disp(const DBox& b, int n, const double* x, const double* y, const double* z,
                     const double* x0, const double* y0, const double* z0,
                     unsigned long long* max_d2_bits, cudaStream_t st);
+
+// ---- phase-batched replicas (rbx_batch.cu) ----
+// While a recorder is installed on the calling thread, the launchers of the
+// step kernels that have a batched form -- drift, fused RBL, mixed structure
+// factor, finalize, mixed RBE force -- append their argument block to it
+// instead of launching.  A batch then launches each phase once over the
+// blocks of every replica: block b belongs to replica r when start[r] <= b <
+// start[r + 1], and runs as block b - start[r] of that replica's own grid.
+enum PhaseKind { PH_DRIFT = 0, PH_RBL = 1, PH_RHO = 2, PH_FINALIZE = 3, PH_FORCE = 4 };
+struct PhaseRecord {
+  int kind = 0;
+  int variant = 0;  // template instance of the kernel
+  int blocks = 0;   // the replica's grid
+  int threads = 0;
+  size_t smem = 0;
+  std::vector<unsigned char> args;
+};
+struct BatchRecorder {
+  std::vector<PhaseRecord> recs;
+};
+BatchRecorder*& batch_recorder();  // the calling thread's recorder (null: launch)
+int record_phase(int kind, int variant, int blocks, int threads, size_t smem, const void* args,
+                 size_t bytes);
+// One launch of phase `kind` over nrep replicas: args holds their argument
+// blocks back to back, start[0..nrep] their first blocks (device arrays).
+int launch_phase_batch(int kind, int variant, const void* args, const int* start, int nrep,
+                       int total, int threads, size_t smem, cudaStream_t st);
+int launch_drift_batch(const void* args, const int* start, int nrep, int total, cudaStream_t st);
+int launch_rbl_batch(int variant, const void* args, const int* start, int nrep, int total,
+                     size_t smem, cudaStream_t st);
+int launch_rho_mixed_batch(int variant, const void* args, const int* start, int nrep, int total,
+                           cudaStream_t st);
+int launch_finalize_batch(const void* args, const int* start, int nrep, int total,
+                          cudaStream_t st);
+int launch_force_mixed_batch(int variant, const void* args, const int* start, int nrep,
+                             int total, cudaStream_t st);
+
+#ifdef __CUDACC__
+// Replica of block b (binary search over start[0..nrep), start[0] = 0).
+__device__ __forceinline__ int batch_replica(const int* __restrict__ start, int nrep, int b) {
+  int lo = 0, hi = nrep - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(start + mid) <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+#endif
 
 }  // namespace rbx

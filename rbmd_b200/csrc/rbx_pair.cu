@@ -118,12 +118,13 @@ int type_table_smem(K kern, int ntypes, bool mixed, size_t* bytes) {
 
 // Block partial of the per-atom forces, accumulated by lane 0 of each warp in
 // atom order and combined over warps in warp order.
-__device__ __forceinline__ void write_block_partial(double (*s_acc)[3], double* fpart) {
+__device__ __forceinline__ void write_block_partial(double (*s_acc)[3], double* fpart,
+                                                    int bx = -1) {
   __syncthreads();
   if (threadIdx.x < 3) {
     double s = 0.0;
     for (int w = 0; w < PAIR_WARPS; ++w) s += s_acc[w][threadIdx.x];
-    fpart[(size_t)blockIdx.x * 3 + threadIdx.x] = s;
+    fpart[(size_t)(bx < 0 ? (int)blockIdx.x : bx) * 3 + threadIdx.x] = s;
   }
 }
 
@@ -233,15 +234,30 @@ __device__ __forceinline__ void prefetch_row(const Rows& rows, int i, int lane) 
     asm volatile("prefetch.global.L2 [%0];" ::"l"(r + k));
 }
 
+struct RblArgs {
+  PairParams pp;
+  int n;
+  const uint4* atoms;
+  const double *x, *y, *z, *q;
+  const int* type;
+  const unsigned long long *key_a, *key_b;
+  int epoch_arg;
+  const int* epoch_dev;
+  Rows rows;
+  double *fx, *fy, *fz, *fpart;
+};
+
+// Block bx of a grid of gx blocks.  (The pointers are parameters, not copies
+// of struct fields, so that their __restrict__ qualifiers hold.)
 template <bool MIXED, int SEL, bool CUBIC>
-__global__ void __launch_bounds__(PAIR_BLOCK, MIXED ? 4 : 3)  // no spills in either form
-k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
-            const double* __restrict__ y, const double* __restrict__ z,
-            const double* __restrict__ q, const int* __restrict__ type,
-            const unsigned long long* __restrict__ key_a,
-            const unsigned long long* __restrict__ key_b, int epoch_arg,
-            const int* __restrict__ epoch_dev, Rows rows, double* __restrict__ fx,
-            double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart) {
+__device__ __forceinline__ void rbl_fused_body(
+    const PairParams& pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
+    const double* __restrict__ y, const double* __restrict__ z, const double* __restrict__ q,
+    const int* __restrict__ type, const unsigned long long* __restrict__ key_a,
+    const unsigned long long* __restrict__ key_b, int epoch_arg,
+    const int* __restrict__ epoch_dev, const Rows& rows, double* __restrict__ fx,
+    double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart, int bx,
+    int gx) {
   using T = typename std::conditional<MIXED, float, double>::type;
   const int epoch = epoch_dev ? *epoch_dev : epoch_arg;  // device copy inside a step graph
   __shared__ int s_q[PAIR_WARPS][RBL_QCAP];
@@ -256,9 +272,9 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
   const T freq_t = (T)pp.freq;
   double acc0 = 0, acc1 = 0, acc2 = 0;
   const int nt = pp.ntypes;
-  const int wstride = gridDim.x * PAIR_WARPS;
+  const int wstride = gx * PAIR_WARPS;
   int* const wq = s_q[warp];
-  for (int i = blockIdx.x * PAIR_WARPS + warp; i < n; i += wstride) {
+  for (int i = bx * PAIR_WARPS + warp; i < n; i += wstride) {
     const uint4 ai = atoms[i];
     const double xi = x[i], yi = y[i], zi = z[i];
     const T qi = MIXED ? (T)__uint_as_float(ai.w) : (T)q[i];
@@ -269,7 +285,6 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
     int nf, nb;
     row_extent(rows, i, nf, nb);
     const int* row = rows.idx + (size_t)i * rows.cap;
-    const int* far_row = row + (rows.cap - nb);
     if (i + wstride < n) prefetch_row(rows, i + wstride, lane);
     int qn = 0;
     T fxa = 0, fya = 0, fza = 0;
@@ -433,7 +448,37 @@ k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double*
     s_acc[warp][1] = acc1;
     s_acc[warp][2] = acc2;
   }
-  if (fpart) write_block_partial(s_acc, fpart);
+  if (fpart) write_block_partial(s_acc, fpart, bx);
+}
+
+template <bool MIXED, int SEL, bool CUBIC>
+__global__ void __launch_bounds__(PAIR_BLOCK, MIXED ? 4 : 3)  // no spills in either form
+k_rbl_fused(PairParams pp, int n, const uint4* __restrict__ atoms, const double* __restrict__ x,
+            const double* __restrict__ y, const double* __restrict__ z,
+            const double* __restrict__ q, const int* __restrict__ type,
+            const unsigned long long* __restrict__ key_a,
+            const unsigned long long* __restrict__ key_b, int epoch_arg,
+            const int* __restrict__ epoch_dev, Rows rows, double* __restrict__ fx,
+            double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ fpart) {
+  rbl_fused_body<MIXED, SEL, CUBIC>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch_arg,
+                                    epoch_dev, rows, fx, fy, fz, fpart, blockIdx.x, gridDim.x);
+}
+
+template <bool MIXED, int SEL, bool CUBIC>
+__global__ void __launch_bounds__(PAIR_BLOCK, MIXED ? 4 : 3)
+k_rbl_fused_batch(const RblArgs* __restrict__ a, const int* __restrict__ start, int nrep) {
+  // the replica's arguments in shared memory: read where used, not held in registers
+  static_assert(sizeof(RblArgs) % 4 == 0 && sizeof(RblArgs) <= 4 * PAIR_BLOCK, "RblArgs size");
+  __shared__ __align__(16) RblArgs s_a;
+  const int r = batch_replica(start, nrep, blockIdx.x);
+  const int b0 = __ldg(start + r);
+  if (threadIdx.x < sizeof(RblArgs) / 4)
+    reinterpret_cast<int*>(&s_a)[threadIdx.x] = __ldg(reinterpret_cast<const int*>(a + r) + threadIdx.x);
+  __syncthreads();
+  rbl_fused_body<MIXED, SEL, CUBIC>(s_a.pp, s_a.n, s_a.atoms, s_a.x, s_a.y, s_a.z, s_a.q,
+                                    s_a.type, s_a.key_a, s_a.key_b, s_a.epoch_arg, s_a.epoch_dev,
+                                    s_a.rows, s_a.fx, s_a.fy, s_a.fz, s_a.fpart, blockIdx.x - b0,
+                                    __ldg(start + r + 1) - b0);
 }
 
 // ---------------------------------------------------------------------------
@@ -901,20 +946,35 @@ using RblKernel = void (*)(PairParams, int, const uint4*, const double*, const d
                            const double*, const double*, const int*, const unsigned long long*,
                            const unsigned long long*, int, const int*, Rows, double*, double*,
                            double*, double*);
+using RblBatchKernel = void (*)(const RblArgs*, const int*, int);
 
 // The instantiation a launch uses: the batch test from freq, the unweighted
-// distance screen on cubic boxes.
-RblKernel rbl_choose(bool mixed, int freq, bool cubic) {
+// distance screen on cubic boxes; variant = (mixed * 3 + sel) * 2 + cubic.
+int rbl_variant(bool mixed, int freq, bool cubic) {
   const bool pow2 = freq >= 1 && (freq & (freq - 1)) == 0;
   const int sel = pow2 ? (freq <= 4 ? 2 : 1) : 0;
-  static RblKernel const table[2][3][2] = {
-      {{k_rbl_fused<false, 0, false>, k_rbl_fused<false, 0, true>},
-       {k_rbl_fused<false, 1, false>, k_rbl_fused<false, 1, true>},
-       {k_rbl_fused<false, 2, false>, k_rbl_fused<false, 2, true>}},
-      {{k_rbl_fused<true, 0, false>, k_rbl_fused<true, 0, true>},
-       {k_rbl_fused<true, 1, false>, k_rbl_fused<true, 1, true>},
-       {k_rbl_fused<true, 2, false>, k_rbl_fused<true, 2, true>}}};
-  return table[mixed][sel][cubic];
+  return ((mixed ? 3 : 0) + sel) * 2 + (cubic ? 1 : 0);
+}
+RblKernel rbl_kernel(int v) {
+  static RblKernel const table[12] = {
+      k_rbl_fused<false, 0, false>, k_rbl_fused<false, 0, true>, k_rbl_fused<false, 1, false>,
+      k_rbl_fused<false, 1, true>,  k_rbl_fused<false, 2, false>, k_rbl_fused<false, 2, true>,
+      k_rbl_fused<true, 0, false>,  k_rbl_fused<true, 0, true>,  k_rbl_fused<true, 1, false>,
+      k_rbl_fused<true, 1, true>,   k_rbl_fused<true, 2, false>, k_rbl_fused<true, 2, true>};
+  return table[v];
+}
+RblBatchKernel rbl_batch_kernel(int v) {
+  static RblBatchKernel const table[12] = {
+      k_rbl_fused_batch<false, 0, false>, k_rbl_fused_batch<false, 0, true>,
+      k_rbl_fused_batch<false, 1, false>, k_rbl_fused_batch<false, 1, true>,
+      k_rbl_fused_batch<false, 2, false>, k_rbl_fused_batch<false, 2, true>,
+      k_rbl_fused_batch<true, 0, false>,  k_rbl_fused_batch<true, 0, true>,
+      k_rbl_fused_batch<true, 1, false>,  k_rbl_fused_batch<true, 1, true>,
+      k_rbl_fused_batch<true, 2, false>,  k_rbl_fused_batch<true, 2, true>};
+  return table[v];
+}
+RblKernel rbl_choose(bool mixed, int freq, bool cubic) {
+  return rbl_kernel(rbl_variant(mixed, freq, cubic));
 }
 }  // namespace
 
@@ -950,13 +1010,44 @@ int launch_rbl_fused(bool mixed, const PairParams& pp, int n, const uint4* atoms
     set_error("rbl_fused: at most %d atoms", QF_INDEX);
     return RBX_ERR_INVALID;
   }
-  const RblKernel k = rbl_choose(mixed, pp.freq, pp.cubic != 0);
+  const int v = rbl_variant(mixed, pp.freq, pp.cubic != 0);
+  const RblKernel k = rbl_kernel(v);
   size_t smem = 0;
   RBX_TRY_K(type_table_smem(k, pp.ntypes, mixed, &smem));
+  RblArgs a;
+  a.pp = pp;
+  a.n = n;
+  a.atoms = atoms;
+  a.x = x;
+  a.y = y;
+  a.z = z;
+  a.q = q;
+  a.type = type;
+  a.key_a = key_a;
+  a.key_b = key_b;
+  a.epoch_arg = epoch;
+  a.epoch_dev = epoch_dev;
+  a.rows = rows;
+  a.fx = fx;
+  a.fy = fy;
+  a.fz = fz;
+  a.fpart = fpart;
+  if (batch_recorder()) {
+    RBX_TRY_K(type_table_smem(rbl_batch_kernel(v), pp.ntypes, mixed, &smem));
+    return record_phase(PH_RBL, v, nblocks, PAIR_BLOCK, smem, &a, sizeof a);
+  }
   k<<<nblocks, PAIR_BLOCK, smem, st>>>(pp, n, atoms, x, y, z, q, type, key_a, key_b, epoch,
                                     epoch_dev, rows, fx, fy, fz, fpart);
   count_launch();
   return check_launch(mixed ? "rbl_fused_mixed" : "rbl_fused_f64");
+}
+
+int launch_rbl_batch(int variant, const void* args, const int* start, int nrep, int total,
+                     size_t smem, cudaStream_t st) {
+  rbl_batch_kernel(variant)<<<total, PAIR_BLOCK, smem, st>>>(static_cast<const RblArgs*>(args),
+                                                             start, nrep);
+  count_launch();
+  return check_launch("rbl_fused_batch");
 }
 
 int launch_verlet_fused_f64(const PairParams& pp, int n, const uint4* atoms, const double* x,

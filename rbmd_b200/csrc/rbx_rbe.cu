@@ -70,7 +70,7 @@ __device__ __forceinline__ bool rbe_draw(int s, const SampleArgs& sa, const doub
 // (double and integer copies) and raises sa.status on a failed draw.
 template <int KPT>
 __device__ __forceinline__ void rbe_group_samples(const SampleArgs& sa, int p, int kbase,
-                                                  int (*s_m)[32 * KPT]) {
+                                                  int (*s_m)[32 * KPT], bool col0) {
   if (threadIdx.x < 32) {
     const uint64_t step = sa.step_dev ? (uint64_t)(int64_t)*sa.step_dev : sa.step_arg;
 #pragma unroll 1
@@ -79,7 +79,7 @@ __device__ __forceinline__ void rbe_group_samples(const SampleArgs& sa, int p, i
       int m[3] = {0, 0, 0};
       if (k < p) {
         const bool ok = rbe_draw(k, sa, sa.tables, step, m);
-        if (blockIdx.x == 0) {
+        if (col0) {
           if (!ok) atomicOr(sa.status, 1);
           sa.mx[k] = m[0];
           sa.my[k] = m[1];
@@ -112,7 +112,7 @@ k_rbe_rho_partial_f64(int n, int p, int chunk, double kxs, double kys, double kz
   __shared__ int s_m[3][32 * KPT];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int kbase = blockIdx.y * (32 * KPT);
-  if (sa.tables) rbe_group_samples<KPT>(sa, p, kbase, s_m);
+  if (sa.tables) rbe_group_samples<KPT>(sa, p, kbase, s_m, blockIdx.x == 0);
   double kx[KPT], ky[KPT], kz[KPT], sr[KPT], si[KPT];
 #pragma unroll
   for (int t = 0; t < KPT; ++t) {
@@ -175,17 +175,30 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
 // (hi, lo) pair.
 constexpr int RBE_TILE = 32;
 
+struct RhoMixedArgs {
+  int n, p, chunk;
+  const int* mi;
+  const uint4* atoms;
+  double *part_re, *part_im;
+  SampleArgs sa;
+  int gx;  // atom chunks (the grid is gx x k-groups)
+};
+
+// Block (bx, by) of the replica's grid.
 template <int KPT>
-__global__ void __launch_bounds__(RBE_BLOCK)
-k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
-                        const uint4* __restrict__ atoms, double* __restrict__ part_re,
-                        double* __restrict__ part_im, SampleArgs sa) {
+__device__ __forceinline__ void rho_mixed_body(const RhoMixedArgs& A, int bx, int by) {
+  const int n = A.n, p = A.p, chunk = A.chunk, gx = A.gx;
+  const int* __restrict__ mi = A.mi;
+  const uint4* __restrict__ atoms = A.atoms;
+  double* __restrict__ part_re = A.part_re;
+  double* __restrict__ part_im = A.part_im;
+  const SampleArgs& sa = A.sa;
   __shared__ double s_re[RBE_WARPS][(32 * KPT)];
   __shared__ double s_im[RBE_WARPS][(32 * KPT)];
   __shared__ int s_m[3][32 * KPT];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int kbase = blockIdx.y * (32 * KPT);
-  if (sa.tables) rbe_group_samples<KPT>(sa, p, kbase, s_m);
+  const int kbase = by * (32 * KPT);
+  if (sa.tables) rbe_group_samples<KPT>(sa, p, kbase, s_m, bx == 0);
   int m0[KPT], m1[KPT], m2[KPT];
   float hr[KPT], lr[KPT], hi[KPT], li[KPT];
 #pragma unroll
@@ -198,7 +211,7 @@ k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
     hr[t] = lr[t] = hi[t] = li[t] = 0.f;
   }
   const float ang = (float)(2.0 * RBX_PI / 4294967296.0);
-  const int a0 = blockIdx.x * chunk;
+  const int a0 = bx * chunk;
   const int a1 = min(n, a0 + chunk);
   const int sub = (chunk + RBE_WARPS - 1) / RBE_WARPS;
   const int w0 = a0 + warp * sub, w1 = min(a1, w0 + sub);
@@ -244,9 +257,23 @@ k_rbe_rho_partial_mixed(int n, int p, int chunk, const int* __restrict__ mi,
       r += s_re[w][s];
       im += s_im[w][s];
     }
-    part_re[(size_t)k * gridDim.x + blockIdx.x] = r;
-    part_im[(size_t)k * gridDim.x + blockIdx.x] = im;
+    part_re[(size_t)k * gx + bx] = r;
+    part_im[(size_t)k * gx + bx] = im;
   }
+}
+
+template <int KPT>
+__global__ void __launch_bounds__(RBE_BLOCK) k_rbe_rho_partial_mixed(RhoMixedArgs a) {
+  rho_mixed_body<KPT>(a, blockIdx.x, blockIdx.y);
+}
+
+template <int KPT>
+__global__ void __launch_bounds__(RBE_BLOCK)
+k_rbe_rho_partial_mixed_batch(const RhoMixedArgs* __restrict__ a, const int* __restrict__ start,
+                              int nrep) {
+  const int r = batch_replica(start, nrep, blockIdx.x);
+  const int b = blockIdx.x - __ldg(start + r), gx = a[r].gx;
+  rho_mixed_body<KPT>(a[r], b % gx, b / gx);
 }
 
 // ---------------------------------------------------------------------------
@@ -394,18 +421,32 @@ __device__ void rbe_finalize_one(int k, int p, int nparts, const double* __restr
                                  double* __restrict__ rho_im, KTab* __restrict__ tab,
                                  double* __restrict__ kterm, double* sh);
 
-__global__ void __launch_bounds__(FK_BLOCK)
-k_rbe_finalize_k(int p, int nparts, const double* __restrict__ part_re,
-                 const double* __restrict__ part_im, const double* __restrict__ mx,
-                 const double* __restrict__ my, const double* __restrict__ mz, double Lx,
-                 double Ly, double Lz, double alpha, double S, double qqr2e,
-                 double* __restrict__ rho_re, double* __restrict__ rho_im,
-                 KTab* __restrict__ tab, double* __restrict__ kterm, int mean_parts,
-                 const double* __restrict__ fpart, double n_atoms, double* __restrict__ mean_out,
-                 EnergySum es) {
+struct FinalizeArgs {
+  int p, nparts;
+  const double *part_re, *part_im, *mx, *my, *mz;
+  double Lx, Ly, Lz, alpha, S, qqr2e;
+  double *rho_re, *rho_im;
+  KTab* tab;
+  double* kterm;
+  int mean_parts;
+  const double* fpart;
+  double n_atoms;
+  double* mean_out;
+  EnergySum es;
+};
+
+// Block blk of a grid of gx blocks.
+__device__ __forceinline__ void finalize_k_body(const FinalizeArgs& A, int blk, int gx) {
+  const int p = A.p, nparts = A.nparts, mean_parts = A.mean_parts;
+  const double* __restrict__ part_re = A.part_re;
+  const double* __restrict__ part_im = A.part_im;
+  const double* __restrict__ fpart = A.fpart;
+  double* __restrict__ kterm = A.kterm;
+  double* __restrict__ mean_out = A.mean_out;
+  const double n_atoms = A.n_atoms;
+  const EnergySum& es = A.es;
   __shared__ double sh[FK_BLOCK / 32];
   __shared__ bool s_last;
-  const int blk = blockIdx.x;
   if (blk >= p) {  // mean of the pair-force block sums, one component per block
     const int d = blk - p;
     double s = 0.0;
@@ -413,19 +454,31 @@ k_rbe_finalize_k(int p, int nparts, const double* __restrict__ part_re,
     s = block_sum_det<FK_BLOCK>(s, sh);
     if (threadIdx.x == 0) mean_out[d] = s / n_atoms;
   } else {
-    rbe_finalize_one(blk, p, nparts, part_re, part_im, mx, my, mz, Lx, Ly, Lz, alpha, S, qqr2e,
-                     rho_re, rho_im, tab, kterm, sh);
+    rbe_finalize_one(blk, p, nparts, part_re, part_im, A.mx, A.my, A.mz, A.Lx, A.Ly, A.Lz,
+                     A.alpha, A.S, A.qqr2e, A.rho_re, A.rho_im, A.tab, kterm, sh);
   }
   if (!es.ctr) return;
   if (threadIdx.x == 0) {
     __threadfence();
-    s_last = atomicAdd(es.ctr, 1u) == gridDim.x - 1;
+    s_last = atomicAdd(es.ctr, 1u) == (unsigned)gx - 1;
   }
   __syncthreads();
   if (!s_last) return;
   __threadfence();
   if (threadIdx.x < 32) rbe_energy_sum_warp(p, kterm, es, true);
   if (threadIdx.x == 0) *es.ctr = 0u;
+}
+
+__global__ void __launch_bounds__(FK_BLOCK) k_rbe_finalize_k(FinalizeArgs a) {
+  finalize_k_body(a, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(FK_BLOCK)
+k_rbe_finalize_k_batch(const FinalizeArgs* __restrict__ a, const int* __restrict__ start,
+                       int nrep) {
+  const int r = batch_replica(start, nrep, blockIdx.x);
+  const int b0 = __ldg(start + r);
+  finalize_k_body(a[r], blockIdx.x - b0, __ldg(start + r + 1) - b0);
 }
 
 // Block k's part of the finalize (all threads of the block call it).
@@ -584,12 +637,21 @@ struct KTabF {
   float a, b, kx, ky, kz;
 };
 
+struct ForceMixedArgs {
+  int n, p;
+  const KTab* tab;
+  const uint4* atoms;
+  ForceEpilogue ep;
+};
+
 template <int FB>
-__global__ void __launch_bounds__(FB)
-k_rbe_force_mixed(int n, int p, const KTab* __restrict__ tab, const uint4* __restrict__ atoms,
-                  ForceEpilogue ep) {
+__device__ __forceinline__ void force_mixed_body(const ForceMixedArgs& A, int bx) {
+  const int n = A.n, p = A.p;
+  const KTab* __restrict__ tab = A.tab;
+  const uint4* __restrict__ atoms = A.atoms;
+  const ForceEpilogue& ep = A.ep;
   __shared__ KTabF s_tab[FRC_TABLE];
-  const int i = blockIdx.x * FB + threadIdx.x;
+  const int i = bx * FB + threadIdx.x;
   const bool live = i < n;
   const uint4 a = live ? atoms[i] : make_uint4(0, 0, 0, 0);
   const float ang = (float)(2.0 * RBX_PI / 4294967296.0);
@@ -628,6 +690,19 @@ k_rbe_force_mixed(int n, int p, const KTab* __restrict__ tab, const uint4* __res
     const double qi = (double)__uint_as_float(a.w);
     force_epilogue(ep, i, (double)fx * qi, (double)fy * qi, (double)fz * qi);
   }
+}
+
+template <int FB>
+__global__ void __launch_bounds__(FB) k_rbe_force_mixed(ForceMixedArgs a) {
+  force_mixed_body<FB>(a, blockIdx.x);
+}
+
+template <int FB>
+__global__ void __launch_bounds__(FB)
+k_rbe_force_mixed_batch(const ForceMixedArgs* __restrict__ a, const int* __restrict__ start,
+                        int nrep) {
+  const int r = batch_replica(start, nrep, blockIdx.x);
+  force_mixed_body<FB>(a[r], blockIdx.x - __ldg(start + r));
 }
 
 // ---------------------------------------------------------------------------
@@ -815,10 +890,20 @@ int launch_rbe_rho_partial_mixed(int n, int p, const int* mi, const uint4* atoms
   if (n <= 0 || p <= 0) return RBX_OK;
   const int chunk = (n + nblocks - 1) / nblocks;
   dim3 grid(nblocks, (p + 32 * kpt - 1) / (32 * kpt));
-  const SampleArgs sa = sample ? *sample : SampleArgs{};
-#define RHO_MIX(K) \
-  k_rbe_rho_partial_mixed<K><<<grid, RBE_BLOCK, 0, st>>>(n, p, chunk, mi, atoms, part_re, part_im, \
-                                                         sa)
+  RhoMixedArgs a;
+  a.n = n;
+  a.p = p;
+  a.chunk = chunk;
+  a.mi = mi;
+  a.atoms = atoms;
+  a.part_re = part_re;
+  a.part_im = part_im;
+  a.sa = sample ? *sample : SampleArgs{};
+  a.gx = nblocks;
+  if (kpt != 1 && kpt != 2 && kpt != 8) kpt = 4;
+  if (batch_recorder())
+    return record_phase(PH_RHO, kpt, (int)(grid.x * grid.y), RBE_BLOCK, 0, &a, sizeof a);
+#define RHO_MIX(K) k_rbe_rho_partial_mixed<K><<<grid, RBE_BLOCK, 0, st>>>(a)
   switch (kpt) {
     case 1: RHO_MIX(1); break;
     case 2: RHO_MIX(2); break;
@@ -850,12 +935,38 @@ int launch_rbe_finalize(const DBox& b, int p, int nparts, const double* part_re,
   // the energy sum in the finalize's last block when a counter is given
   const bool fold = energy && sum_ctr && grid > 0 && p > 0;
   if (grid > 0) {
-    EnergySum ek = es;
-    ek.ctr = fold ? sum_ctr : nullptr;
-    k_rbe_finalize_k<<<grid, FK_BLOCK, 0, st>>>(p, nparts, part_re, part_im, mx, my, mz, b.len[0],
-                                                b.len[1], b.len[2], alpha, S, qqr2e, rho_re,
-                                                rho_im, tab, energy ? kterm : nullptr, mean_parts,
-                                                fpart, (double)n_atoms, mean_out, ek);
+    FinalizeArgs a;
+    a.p = p;
+    a.nparts = nparts;
+    a.part_re = part_re;
+    a.part_im = part_im;
+    a.mx = mx;
+    a.my = my;
+    a.mz = mz;
+    a.Lx = b.len[0];
+    a.Ly = b.len[1];
+    a.Lz = b.len[2];
+    a.alpha = alpha;
+    a.S = S;
+    a.qqr2e = qqr2e;
+    a.rho_re = rho_re;
+    a.rho_im = rho_im;
+    a.tab = tab;
+    a.kterm = energy ? kterm : nullptr;
+    a.mean_parts = mean_parts;
+    a.fpart = fpart;
+    a.n_atoms = (double)n_atoms;
+    a.mean_out = mean_out;
+    a.es = es;
+    a.es.ctr = fold ? sum_ctr : nullptr;
+    if (batch_recorder()) {
+      if (energy && !fold) {
+        set_error("rbe_finalize: a batched finalize needs the energy sum folded in");
+        return RBX_ERR_INVALID;
+      }
+      return record_phase(PH_FINALIZE, 0, grid, FK_BLOCK, 0, &a, sizeof a);
+    }
+    k_rbe_finalize_k<<<grid, FK_BLOCK, 0, st>>>(a);
     count_launch();
     const int rc = check_launch("rbe_finalize_k");
     if (rc) return rc;
@@ -907,15 +1018,57 @@ int launch_rbe_force_f64(int n, int p, const KTab* tab, const double* q, const d
 int launch_rbe_force_mixed(int n, int p, const KTab* tab, const uint4* atoms,
                            const RbeForceOut& out, cudaStream_t st, int block) {
   if (n <= 0) return RBX_OK;
-  const ForceEpilogue ep = make_ep(out);
+  ForceMixedArgs a;
+  a.n = n;
+  a.p = p;
+  a.tab = tab;
+  a.atoms = atoms;
+  a.ep = make_ep(out);
+  if (block != 128 && block != 512) block = 256;
+  if (batch_recorder())
+    return record_phase(PH_FORCE, block, (n + block - 1) / block, block, 0, &a, sizeof a);
   if (block == 128)
-    k_rbe_force_mixed<128><<<(n + 127) / 128, 128, 0, st>>>(n, p, tab, atoms, ep);
+    k_rbe_force_mixed<128><<<(n + 127) / 128, 128, 0, st>>>(a);
   else if (block == 512)
-    k_rbe_force_mixed<512><<<(n + 511) / 512, 512, 0, st>>>(n, p, tab, atoms, ep);
+    k_rbe_force_mixed<512><<<(n + 511) / 512, 512, 0, st>>>(a);
   else
-    k_rbe_force_mixed<256><<<(n + 255) / 256, 256, 0, st>>>(n, p, tab, atoms, ep);
+    k_rbe_force_mixed<256><<<(n + 255) / 256, 256, 0, st>>>(a);
   count_launch();
   return check_launch("rbe_force_mixed");
+}
+
+int launch_rho_mixed_batch(int variant, const void* args, const int* start, int nrep, int total,
+                           cudaStream_t st) {
+  const RhoMixedArgs* a = static_cast<const RhoMixedArgs*>(args);
+  switch (variant) {
+    case 1: k_rbe_rho_partial_mixed_batch<1><<<total, RBE_BLOCK, 0, st>>>(a, start, nrep); break;
+    case 2: k_rbe_rho_partial_mixed_batch<2><<<total, RBE_BLOCK, 0, st>>>(a, start, nrep); break;
+    case 8: k_rbe_rho_partial_mixed_batch<8><<<total, RBE_BLOCK, 0, st>>>(a, start, nrep); break;
+    default: k_rbe_rho_partial_mixed_batch<4><<<total, RBE_BLOCK, 0, st>>>(a, start, nrep); break;
+  }
+  count_launch();
+  return check_launch("rbe_rho_partial_mixed_batch");
+}
+
+int launch_finalize_batch(const void* args, const int* start, int nrep, int total,
+                          cudaStream_t st) {
+  k_rbe_finalize_k_batch<<<total, FK_BLOCK, 0, st>>>(static_cast<const FinalizeArgs*>(args),
+                                                     start, nrep);
+  count_launch();
+  return check_launch("rbe_finalize_k_batch");
+}
+
+int launch_force_mixed_batch(int variant, const void* args, const int* start, int nrep,
+                             int total, cudaStream_t st) {
+  const ForceMixedArgs* a = static_cast<const ForceMixedArgs*>(args);
+  if (variant == 128)
+    k_rbe_force_mixed_batch<128><<<total, 128, 0, st>>>(a, start, nrep);
+  else if (variant == 512)
+    k_rbe_force_mixed_batch<512><<<total, 512, 0, st>>>(a, start, nrep);
+  else
+    k_rbe_force_mixed_batch<256><<<total, 256, 0, st>>>(a, start, nrep);
+  count_launch();
+  return check_launch("rbe_force_mixed_batch");
 }
 
 int launch_rbe_sample(int p, const double* tables, const int cnt[3], const double tot[3],

@@ -109,7 +109,7 @@ EXPORTS = [
     "rbx_lammps_gauss_velocities", "rbx_engine_set_nose_hoover", "rbx_engine_get_thermostat",
     "rbx_engine_set_shake", "rbx_engine_get_shake", "rbx_engine_set_special", "rbx_special_build",
     "rbx_rbsog_params", "rbx_rbsog_sample", "rbx_rbsog_force", "rbx_pair_force_verlet_sog",
-    "rbx_engine_autotune", "rbx_batch_autotune",
+    "rbx_engine_autotune", "rbx_batch_autotune", "rbx_batch_set_mode", "rbx_batch_design",
     "rbx_rbe_structure_factor_f32", "rbx_rbe_force_f32", "rbx_rbe_energy_virial_f32",
     "rbx_rbl_filter_f32", "rbx_pair_force_rbl_f32", "rbx_fix_rbl_force_f32",
     "rbx_pair_force_verlet_f32", "rbx_engine_kspace_energy_exact", "rbx_force_create_json",
@@ -237,6 +237,8 @@ def lib():
     L.rbx_batch_step.argtypes = [vp, ip]
     L.rbx_batch_stream.restype = vp
     L.rbx_batch_stream.argtypes = [vp]
+    L.rbx_batch_set_mode.argtypes = [vp, ip]
+    L.rbx_batch_design.argtypes = [vp]
     L.rbx_nlist_should_reuse.argtypes = [B, ip] + [vp] * 6 + [dp, C.POINTER(C.c_int),
                                                              C.POINTER(C.c_double), vp]
     L.rbx_engine_kspace_energy_exact.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
@@ -823,8 +825,20 @@ class Batch:
         """rbx_batch_autotune: tune each replica (one timing per size bin)."""
         check(lib().rbx_batch_autotune(self._h), "rbx_batch_autotune")
 
+    AUTO, PHASED, BRANCHES = 0, 1, 2  # RBX_BATCH_* graph designs
+
     def step(self, nsteps=1):
         check(lib().rbx_batch_step(self._h, nsteps), "rbx_batch_step")
+
+    def set_mode(self, mode):
+        """rbx_batch_set_mode: AUTO, PHASED (one launch per phase over all
+        replicas) or BRANCHES (one graph branch per replica)."""
+        check(lib().rbx_batch_set_mode(self._h, mode), "rbx_batch_set_mode")
+
+    @property
+    def design(self) -> int:
+        """rbx_batch_design: PHASED or BRANCHES once captured, else -1."""
+        return lib().rbx_batch_design(self._h)
 
     @property
     def stream(self) -> int:
