@@ -288,7 +288,7 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
             const float4* __restrict__ box_lo, const float4* __restrict__ box_hi,
             const int* __restrict__ cell_of, int cap, int* __restrict__ count,
             int* __restrict__ nbrs, int* __restrict__ overflow, float near2,
-            int* __restrict__ far) {
+            int* __restrict__ far, long long* __restrict__ total) {
   __shared__ float4 buf[NL_WARPS][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int w = blockIdx.x * NL_WARPS + warp;
@@ -417,6 +417,10 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
     if (SPLIT) far[i] = nback;
     if (cnt > cap) atomicOr(overflow, 1);
   }
+  if (total) {  // the warp's rows (cnt is 0 on lanes without a centre atom)
+    const int s = __reduce_add_sync(0xffffffffu, cnt);
+    if (lane == 0) atomicAdd((unsigned long long*)total, (unsigned long long)s);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(128)
 k_full_list_small(DBox b, double cut2, double near2, int n, const double* __restrict__ x,
                   const double* __restrict__ y, const double* __restrict__ z, int cap,
                   int* __restrict__ count, int* __restrict__ nbrs, int* __restrict__ overflow,
-                  int* __restrict__ far) {
+                  int* __restrict__ far, long long* __restrict__ total) {
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (i >= n) return;
@@ -466,12 +470,13 @@ k_full_list_small(DBox b, double cut2, double near2, int n, const double* __rest
     count[i] = nf + nb;
     if (far) far[i] = nb;
     if (nf + nb > cap) atomicOr(overflow, 1);
+    if (total) atomicAdd((unsigned long long*)total, (unsigned long long)(nf + nb));
   }
 }
 
 int launch_full_list_small(const DBox& b, double cutoff, int n, const double* x, const double* y,
                            const double* z, int cap, int* count, int* nbrs, int* overflow,
-                           cudaStream_t st, const FarSplit* split) {
+                           cudaStream_t st, const FarSplit* split, long long* total) {
   if (n <= 0) return RBX_OK;
   // near threshold raised by 1e-9 relative: FP64 rounding never moves a pair
   // that could come within r_core before the next rebuild to the far segment
@@ -479,7 +484,7 @@ int launch_full_list_small(const DBox& b, double cutoff, int n, const double* x,
       split ? split->r_near * split->r_near * (1.0 + 1e-9) : (double)INFINITY;
   k_full_list_small<<<(n + 3) / 4, 128, 0, st>>>(b, cutoff * cutoff, near2, n, x, y, z, cap,
                                                  count, nbrs, overflow,
-                                                 split ? split->far : nullptr);
+                                                 split ? split->far : nullptr, total);
   count_launch();
   return check_launch("full_list_small");
 }
@@ -489,6 +494,18 @@ int launch_full_list_small(const DBox& b, double cutoff, int n, const double* x,
 // ---------------------------------------------------------------------------
 __global__ void k_fill_i32(int n, int* __restrict__ p, int v) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// Zero the cell counts; with book (an engine rebuild), also its flags and
+// candidate total, and count the rebuild.
+__global__ void k_cells_reset(int ncell, int* __restrict__ counts, RebuildBook book) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncell; i += gridDim.x * blockDim.x)
+    counts[i] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (book.flags) book.flags[0] = book.flags[1] = 0;
+    if (book.total) *book.total = 0;
+    if (book.counter) *book.counter += 1;
+  }
 }
 
 // One pass over a set of per-atom arrays: dst[a][i] = src[a][perm[i]] (perm
@@ -710,7 +727,7 @@ size_t cells_scratch_bytes(int n, int ncell) {
 
 int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, const double* y,
                       const double* z, int* perm, int* cell_of_sorted, int* cell_start,
-                      void* scratch, int* status, cudaStream_t st) {
+                      void* scratch, int* status, cudaStream_t st, const RebuildBook* book) {
   const int ncell = dims[0] * dims[1] * dims[2];
   auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
   char* p = (char*)scratch;
@@ -723,7 +740,8 @@ int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, 
   unsigned* sub = (unsigned*)p;
   p += al(sizeof(int) * (size_t)n);
   unsigned* tmp = (unsigned*)p;
-  k_fill_i32<<<grid_for(ncell, 256, sm_count() * 4), 256, 0, st>>>(ncell, counts, 0);
+  k_cells_reset<<<grid_for(ncell, 256, sm_count() * 4), 256, 0, st>>>(
+      ncell, counts, book ? *book : RebuildBook{nullptr, nullptr, nullptr});
   count_launch();
   if (n > 0) {
     CellGeom g;
@@ -755,11 +773,12 @@ size_t full_list_scratch_bytes(int n, int ncell) {
 int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
                      const double* y, const double* z, const int* cell_start, int cap,
                      int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st,
-                     const FarSplit* split) {
+                     const FarSplit* split, long long* total) {
   const int ncell = dims[0] * dims[1] * dims[2];
   if (n <= 0) return RBX_OK;
   if (dims[0] < 3 || dims[1] < 3 || dims[2] < 3)
-    return launch_full_list_small(b, cutoff, n, x, y, z, cap, count, nbrs, overflow, st, split);
+    return launch_full_list_small(b, cutoff, n, x, y, z, cap, count, nbrs, overflow, st, split,
+                                  total);
   const double cut2 = cutoff * cutoff;
   double emax = 0.0;
   for (int d = 0; d < 3; ++d) emax = fmax(emax, b.len[d] / dims[d]);
@@ -788,11 +807,11 @@ int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, con
   if (split)
     k_full_list<true><<<(t + NL_WARPS - 1) / NL_WARPS, NL_BLOCK, 0, st>>>(
         b, dims[0], dims[1], dims[2], cut2, cut2_up, lo_band, hi_band, t, x, y, z, cell_start,
-        box_lo, box_hi, cell_of, cap, count, nbrs, overflow, near2, split->far);
+        box_lo, box_hi, cell_of, cap, count, nbrs, overflow, near2, split->far, total);
   else
     k_full_list<false><<<(t + NL_WARPS - 1) / NL_WARPS, NL_BLOCK, 0, st>>>(
         b, dims[0], dims[1], dims[2], cut2, cut2_up, lo_band, hi_band, t, x, y, z, cell_start,
-        box_lo, box_hi, cell_of, cap, count, nbrs, overflow, near2, nullptr);
+        box_lo, box_hi, cell_of, cap, count, nbrs, overflow, near2, nullptr, total);
   count_launch();
   return check_launch("full_list");
 }

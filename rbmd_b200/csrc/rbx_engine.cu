@@ -386,20 +386,19 @@ ArraySet rbx_engine::state_set(bool save) const {
 // in_graph: also the candidate total and the device rebuild counter, with no
 // host decision (the host checks the flags after the graph has run).
 int rbx_engine::rebuild_launches(cudaStream_t s, bool in_graph) {
-  ETRY(launch_fill_i32(2, dflags, 0, s));  // cell-sort status, list overflow
+  // the cell sort's first kernel clears the cell-sort status, the list
+  // overflow and the candidate total (and counts a rebuild inside a graph);
+  // the list builder sums the candidates
+  const RebuildBook book{dflags, (long long*)cand_total, in_graph ? dflags + 5 : nullptr};
   ETRY(launch_cells_sort(dbox, dims, n, x, y, z, perm, cell_of_sorted, cell_start, cell_scratch,
-                         dflags, s));
+                         dflags, s, &book));
   ETRY(launch_move_set(n, perm, permute_set(true), s));
   ETRY(launch_move_set(n, nullptr, permute_set(false), s));
   if (where) ETRY(launch_inverse_perm(n, orig, where, s));  // SHAKE / special rows
   ETRY(launch_to_fixed(dbox, n, x, y, z, q, atoms, s));
   ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
-                        cand_count, cand, dflags + 1, list_scratch, s, far_split()));
-  if (in_graph) {
-    ETRY(launch_zero_u64((unsigned long long*)cand_total, s));
-    ETRY(launch_sum_i32(n, cand_count, cand_total, s));
-    ETRY(launch_add_i32(dflags + 5, 1, s));
-  }
+                        cand_count, cand, dflags + 1, list_scratch, s, far_split(),
+                        (long long*)cand_total));
   return RBX_OK;
 }
 
@@ -418,8 +417,7 @@ int rbx_engine::rebuild() {
     if (!(h[1] & 1)) {
       have_cache = true;
       ++rebuilds;
-      ETRY(launch_zero_u64((unsigned long long*)cand_total, st));
-      return launch_sum_i32(n, cand_count, cand_total, st);
+      return RBX_OK;
     }
     // grow the row capacity and build the list again
     int maxc = 0;
@@ -437,8 +435,10 @@ int rbx_engine::rebuild() {
     graph_dirty = host_graph_dirty = true;  // the list moved
     ++graph_version;
     ETRY(launch_fill_i32(1, dflags + 1, 0, st));
+    ETRY(launch_zero_u64((unsigned long long*)cand_total, st));
     ETRY(launch_full_list(dbox, dims, prm.cut_off + prm.skin, n, x, y, z, cell_start, cap,
-                          cand_count, cand, dflags + 1, list_scratch, st, far_split()));
+                          cand_count, cand, dflags + 1, list_scratch, st, far_split(),
+                          (long long*)cand_total));
   }
   set_error("candidate list capacity did not converge");
   return RBX_ERR_CAPACITY;

@@ -225,9 +225,19 @@ int launch_sub_mean(int n, double* fx, double* fy, double* fz, const double* mea
                     cudaStream_t st);
 
 // ---- cells, lists, integration (rbx_cells.cu) ----
+// Bookkeeping of an engine rebuild folded into its kernels (each member may be
+// null): the cell sort's first kernel zeroes flags[0..1] (sort status, list
+// overflow) and *total and adds one to *counter; the list builder then adds
+// every row's candidate count to *total.
+struct RebuildBook {
+  int* flags;
+  long long* total;
+  int* counter;
+};
 int launch_cells_sort(const DBox& b, const int dims[3], int n, const double* x, const double* y,
                       const double* z, int* perm, int* cell_of_sorted, int* cell_start,
-                      void* scratch, int* status, cudaStream_t st);
+                      void* scratch, int* status, cudaStream_t st,
+                      const RebuildBook* book = nullptr);
 size_t cells_scratch_bytes(int n, int ncell);
 // Scratch of launch_full_list: per-chunk boxes and cells, full_list_scratch_bytes(n, ncell).
 size_t full_list_scratch_bytes(int n, int ncell);
@@ -242,7 +252,7 @@ struct FarSplit {
 int launch_full_list(const DBox& b, const int dims[3], double cutoff, int n, const double* x,
                      const double* y, const double* z, const int* cell_start, int cap,
                      int* count, int* nbrs, int* overflow, void* scratch, cudaStream_t st,
-                     const FarSplit* split = nullptr);
+                     const FarSplit* split = nullptr, long long* total = nullptr);
 // Force adjoint (rbx_adjoint.cu).  Pair part: per-atom dL/dr, dL/dq and
 // per-block partials [nblocks][2 ntypes + 1] (d_eps, d_sigma, d_alpha).
 int adj_pair_blocks(int n);
