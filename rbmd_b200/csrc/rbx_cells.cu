@@ -658,9 +658,23 @@ __device__ __forceinline__ void drift_body(const DriftArgs& A, int bx, int gx) {
       atoms[i] = a;
     }
   }
-  if (max_d2) warp_max_atomic(d2, max_d2);
+  if (max_d2) {  // block maximum, then one atomic per block
+    __shared__ unsigned long long s_max[32];
+    unsigned long long bits = (unsigned long long)__double_as_longlong(d2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long t = __shfl_xor_sync(0xffffffffu, bits, o);
+      bits = t > bits ? t : bits;
+    }
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = bits;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) bits = s_max[w] > bits ? s_max[w] : bits;
+      atomicMax(max_d2, bits);
+    }
+  }
   if (decide.ctr) {
-    __syncthreads();  // every warp of the block has folded its maximum in
+    __syncthreads();  // the block's maximum is folded in (by thread 0, below)
     if (threadIdx.x == 0) {
       __threadfence();
       if (atomicAdd(decide.ctr, 1u) == (unsigned)gx - 1) {  // the last block

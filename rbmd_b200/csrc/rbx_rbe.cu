@@ -65,36 +65,43 @@ __device__ __forceinline__ bool rbe_draw(int s, const SampleArgs& sa, const doub
   return false;
 }
 
-// With sa.tables the k-vectors of the block's k-group are drawn here (warp 0,
-// into shared memory) instead of read: block column 0 also writes them out
+// With sa.tables the k-vectors of the block's k-group are drawn here (one
+// per thread, into shared memory) instead of read, from the cumulative tables
+// staged in shared memory when they fit: block column 0 also writes them out
 // (double and integer copies) and raises sa.status on a failed draw.
+constexpr int SAMPLE_TAB_SMEM = 768;  // table entries staged in shared memory
+
 template <int KPT>
 __device__ __forceinline__ void rbe_group_samples(const SampleArgs& sa, int p, int kbase,
                                                   int (*s_m)[32 * KPT], bool col0) {
-  if (threadIdx.x < 32) {
-    const uint64_t step = sa.step_dev ? (uint64_t)(int64_t)*sa.step_dev : sa.step_arg;
-#pragma unroll 1
-    for (int t = 0; t < KPT; ++t) {
-      const int slot = threadIdx.x + 32 * t, k = kbase + slot;
-      int m[3] = {0, 0, 0};
-      if (k < p) {
-        const bool ok = rbe_draw(k, sa, sa.tables, step, m);
-        if (col0) {
-          if (!ok) atomicOr(sa.status, 1);
-          sa.mx[k] = m[0];
-          sa.my[k] = m[1];
-          sa.mz[k] = m[2];
-          if (sa.mi) {
-            sa.mi[3 * k] = m[0];
-            sa.mi[3 * k + 1] = m[1];
-            sa.mi[3 * k + 2] = m[2];
-          }
+  __shared__ double s_cdf[SAMPLE_TAB_SMEM];
+  const int ent = sa.c0 + sa.c1 + sa.c2;
+  const bool staged = ent <= SAMPLE_TAB_SMEM;
+  if (staged)
+    for (int e = threadIdx.x; e < ent; e += blockDim.x) s_cdf[e] = sa.tables[e];
+  __syncthreads();
+  const double* w0 = staged ? s_cdf : sa.tables;
+  const uint64_t step = sa.step_dev ? (uint64_t)(int64_t)*sa.step_dev : sa.step_arg;
+  for (int slot = threadIdx.x; slot < 32 * KPT; slot += blockDim.x) {
+    const int k = kbase + slot;
+    int m[3] = {0, 0, 0};
+    if (k < p) {
+      const bool ok = rbe_draw(k, sa, w0, step, m);
+      if (col0) {
+        if (!ok) atomicOr(sa.status, 1);
+        sa.mx[k] = m[0];
+        sa.my[k] = m[1];
+        sa.mz[k] = m[2];
+        if (sa.mi) {
+          sa.mi[3 * k] = m[0];
+          sa.mi[3 * k + 1] = m[1];
+          sa.mi[3 * k + 2] = m[2];
         }
       }
-      s_m[0][slot] = m[0];
-      s_m[1][slot] = m[1];
-      s_m[2][slot] = m[2];
     }
+    s_m[0][slot] = m[0];
+    s_m[1][slot] = m[1];
+    s_m[2][slot] = m[2];
   }
   __syncthreads();
 }
