@@ -604,8 +604,11 @@ def run_batched(args):
     from rbmd_b200 import rbx, systems
 
     rng = np.random.default_rng(args.batch_seed)
-    sizes = np.exp(rng.uniform(np.log(args.batch_nmin), np.log(args.batch_nmax),
-                               args.replicas)).astype(int)
+    if args.batch_nmin == args.batch_nmax:  # equal replicas
+        sizes = np.full(args.replicas, args.batch_nmin)
+    else:
+        sizes = np.exp(rng.uniform(np.log(args.batch_nmin), np.log(args.batch_nmax),
+                                   args.replicas)).astype(int)
     syss = [systems.lj_electrolyte(int(n), seed=1000 + r, kspace_p=args.p)
             for r, n in enumerate(sizes)]
     total = int(sizes.sum())
@@ -682,9 +685,10 @@ def run_batched(args):
         "ms_per_step": ms_batch / args.steps, "higher_is_better": True, "scaling": "weak",
         "dtype": "mixed(u32 fixed-point, f32 SFU, f64 reductions/integrator)",
         "data": "synthetic",
-        "config": {"workload": f"{args.replicas} LJ electrolytes rho*=0.8 10% ions, N log-uniform "
-                               f"[{args.batch_nmin}, {args.batch_nmax}] (seed {args.batch_seed}), "
-                               f"RBL + RBE(P={args.p}), NVE dt=0.005",
+        "config": {"workload": f"{args.replicas} LJ electrolytes rho*=0.8 10% ions, " + (
+                       f"N = {args.batch_nmin} each" if args.batch_nmin == args.batch_nmax else
+                       f"N log-uniform [{args.batch_nmin}, {args.batch_nmax}] "
+                       f"(seed {args.batch_seed})") + f", RBL + RBE(P={args.p}), NVE dt=0.005",
                    "total_atoms": total, "replicas": args.replicas},
         "one_replica_per_launch_fp64": {"value": total * base_steps / t64, "steps": base_steps,
                                         "timing": "host wall clock around launch-by-launch steps"},
