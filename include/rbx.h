@@ -752,7 +752,7 @@ int rbx_lammps_write_charge(const char* path, const rbx_box* box, int n, int nty
  *     no special bonds;
  *   RBX_BATCH_BRANCHES: every replica's own step graph as a parallel branch.
  * RBX_BATCH_AUTO (the default) takes the phased design for replicas of fewer
- * than 12,000 atoms on average when every replica allows it, else the
+ * than 5,000 atoms on average when every replica allows it, else the
  * branches.  The engines stay owned by the caller and
  * must outlive the batch; each must have skin > 0 and profiling off.  Results
  * equal stepping each engine alone, in either design.  No counterpart in the

@@ -218,11 +218,12 @@ struct rbx_batch {
   }
 
   // AUTO: the phased graph for replicas of fewer than kPhasedMeanAtoms atoms
-  // on average (one launch per phase pays off over many small replicas:
-  // 910 x 2,000 atoms 4.4x the branches; 256 x 7,100 atoms 1.04x), else the
-  // branches (91 x 20,000 atoms: branches 1.07x the phased graph, whose
-  // force phases wait for every replica's rebuild).
-  static constexpr int kPhasedMeanAtoms = 12000;
+  // on average, else the branches.  One launch per phase pays off over many
+  // small replicas (910 x 2,000 atoms: 5.1x the branches, whose thousand-node
+  // graph is bound by node scheduling); at 256 x 7,100 atoms the designs are
+  // level, and with larger replicas the branches win (the phased force
+  // launches wait for every replica's rebuild).
+  static constexpr int kPhasedMeanAtoms = 5000;
   int capture() {
     long long atoms = 0;
     for (rbx_engine* e : eng) atoms += e->n;
