@@ -400,7 +400,22 @@ k_full_list(DBox b, int dimx, int dimy, int dimz, double cut2, float cut2_up, fl
             if (dist2_list(b, xi, yi, zi, x[j], y[j], z[j]) < cut2) acc |= 1u << t;
           }
         }
-        while (acc) {  // hits in cell order, each lane into its own row
+        if (cnt + __popc(acc) <= cap) {
+          // every hit of the chunk fits: next front and back slots as offsets,
+          // the counts recovered after the loop
+          int foff = cnt - nback, boff = cap - 1 - nback;
+          while (acc) {  // hits in cell order, each lane into its own row
+            const int t = __ffs(acc) - 1;
+            acc &= acc - 1;
+            const bool to_back = SPLIT && ((farm >> t) & 1u);
+            row[to_back ? boff : foff] = first + t;
+            boff -= to_back;
+            foff += !to_back;
+          }
+          nback = cap - 1 - boff;
+          cnt = foff + nback;
+        }
+        while (acc) {  // the row fills up: stop storing at cap entries
           const int t = __ffs(acc) - 1;
           acc &= acc - 1;
           // one store to the front or the back of the row (no branch)
