@@ -85,3 +85,24 @@ def test_phased_mode_needs_eligible_replicas(cuda, rbx):
     b.close()
     for e in mixed + plain:
         e.close()
+
+
+def test_auto_design_follows_replica_size(cuda, rbx):
+    # AUTO: phased below 5,000 atoms per replica on average, branches above;
+    # an explicit mode overrides it, with the same trajectories either way
+    big = _engines(rbx, [(6000, 41), (7000, 42)], rbx.MIXED)
+    ref = _engines(rbx, [(6000, 41), (7000, 42)], rbx.MIXED)
+    b = rbx.Batch(big)
+    b.step(4)
+    assert b.design == rbx.Batch.BRANCHES
+    b.set_mode(rbx.Batch.PHASED)
+    b.step(6)
+    assert b.design == rbx.Batch.PHASED
+    for e in ref:
+        e.step(4)
+        e.step(6)
+    for e1, e2 in zip(big, ref):
+        _assert_same(e1, e2)
+    b.close()
+    for e in big + ref:
+        e.close()
