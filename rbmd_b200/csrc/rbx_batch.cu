@@ -175,7 +175,8 @@ struct rbx_batch {
                                 L.total, L.threads, L.smem, st);
     };
     size_t li = 0;
-    for (; li < launches.size() && launches[li].kind == PH_DRIFT && !rc; ++li) rc = run(launches[li]);
+    for (; li < launches.size() && launches[li].kind == PH_DRIFT && !rc; ++li)
+      rc = run(launches[li]);
     unsigned long long rebuild_launches = 0;
     if (!rc) {  // every replica's rebuild under its own IF node, after the drift
       cudaStreamCaptureStatus cs;

@@ -705,7 +705,9 @@ __device__ __forceinline__ void drift_body(const DriftArgs& A, int bx, int gx) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_drift(DriftArgs a) { drift_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_drift(DriftArgs a) {
+  drift_body(a, blockIdx.x, gridDim.x);
+}
 
 __global__ void __launch_bounds__(256)
 k_drift_batch(const DriftArgs* __restrict__ a, const int* __restrict__ start, int nrep) {

@@ -475,7 +475,8 @@ k_rbl_fused_batch(const RblArgs* __restrict__ a, const int* __restrict__ start, 
   const int r = batch_replica(start, nrep, blockIdx.x);
   const int b0 = __ldg(start + r);
   if (threadIdx.x < sizeof(RblArgs) / 4)
-    reinterpret_cast<int*>(&s_a)[threadIdx.x] = __ldg(reinterpret_cast<const int*>(a + r) + threadIdx.x);
+    reinterpret_cast<int*>(&s_a)[threadIdx.x] =
+        __ldg(reinterpret_cast<const int*>(a + r) + threadIdx.x);
   __syncthreads();
   rbl_fused_body<MIXED, SEL, CUBIC>(s_a.pp, s_a.n, s_a.atoms, s_a.x, s_a.y, s_a.z, s_a.q,
                                     s_a.type, s_a.key_a, s_a.key_b, s_a.epoch_arg, s_a.epoch_dev,
