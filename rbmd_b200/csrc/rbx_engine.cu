@@ -72,6 +72,9 @@ rbx_engine::~rbx_engine() {
   release_host_graphs();
   if (ev_side) cudaEventDestroy(ev_side);
   if (st_side) cudaStreamDestroy(st_side);
+  for (cudaEvent_t e : ev_ks)
+    if (e) cudaEventDestroy(e);
+  if (st_ks) cudaStreamDestroy(st_ks);
   if (st_body) cudaStreamDestroy(st_body);
   if (st) cudaStreamDestroy(st);
 }
@@ -117,6 +120,9 @@ int rbx_engine::init() {
   ETRY(cuda_ok(cudaStreamCreateWithFlags(&st_body, cudaStreamNonBlocking), "cudaStreamCreate"));
   ETRY(cuda_ok(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking), "cudaStreamCreate"));
   ETRY(cuda_ok(cudaEventCreateWithFlags(&ev_side, cudaEventDisableTiming), "cudaEventCreate"));
+  ETRY(cuda_ok(cudaStreamCreateWithFlags(&st_ks, cudaStreamNonBlocking), "cudaStreamCreate"));
+  for (cudaEvent_t& e : ev_ks)
+    ETRY(cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate"));
   dbox = make_dbox(box);
   const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
   if (!(prm.cut_off > 0.0) || prm.skin < 0.0 || (rbl && !(prm.r_core > 0.0)) ||
@@ -483,8 +489,12 @@ int rbx_engine::real_space(const int* epoch_dev) {
 }
 
 int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
+  ETRY(kspace_rho(st, epoch_dev));
+  return kspace_finish(kick, epoch_dev);
+}
+
+int rbx_engine::kspace_rho(cudaStream_t s, const int* epoch_dev) {
   const bool mixed = prm.precision == RBX_MIXED;
-  const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
   if (P > 0) {
     // a failed draw raises dflags[2] until check_sampler reads it; RBE samples
     // are drawn inside the structure-factor kernel (no launch of their own)
@@ -494,22 +504,29 @@ int rbx_engine::kspace_and_combine(bool kick, const int* epoch_dev) {
     const bool draw_in_rho = !k_injected && !sog && n > 0;
     if (!k_injected && sog)
       ETRY(launch_rbsog_sample(P, sog_tables, prm.random_seed, (uint64_t)(int64_t)epoch,
-                               epoch_dev, mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
+                               epoch_dev, mx, my, mz, mixed ? mi : nullptr, dflags + 2, s));
     else if (!k_injected && !draw_in_rho)
       ETRY(launch_rbe_sample(P, sample_tables, tcnt, ttot, prm.random_seed, epoch, epoch_dev,
-                             mx, my, mz, mixed ? mi : nullptr, dflags + 2, st));
+                             mx, my, mz, mixed ? mi : nullptr, dflags + 2, s));
     if (mixed)
-      ETRY(launch_rbe_rho_partial_mixed(n, Pk, mi, atoms, part_re, part_im, nparts, st,
+      ETRY(launch_rbe_rho_partial_mixed(n, Pk, mi, atoms, part_re, part_im, nparts, s,
                                         tun.rho_kpt, draw_in_rho ? &sa : nullptr));
     else
       ETRY(launch_rbe_rho_partial_f64(dbox, n, Pk, mx, my, mz, q, x, y, z, part_re, part_im,
-                                      nparts, st, tun.rho_kpt, draw_in_rho ? &sa : nullptr));
+                                      nparts, s, tun.rho_kpt, draw_in_rho ? &sa : nullptr));
+    // the RBSOG virial's gather chain reads only the samples
+    if (sog)
+      ETRY(launch_rbsog_npt_chain(dbox, P, mx, my, mz, sog_gauss, prm.random_seed,
+                                  (uint64_t)(int64_t)epoch, epoch_dev, sog_idx, sog_mult, s));
   }
+  return RBX_OK;
+}
+
+int rbx_engine::kspace_finish(bool kick, const int* epoch_dev) {
+  const bool mixed = prm.precision == RBX_MIXED;
+  const bool rbl = prm.neighbor_type == RBX_NEIGHBOR_RBL;
   const int mean_parts = rbl ? nrbl + (spec_natoms ? SPEC_PARTS : 0) : 0;
   if (sog) {
-    if (P > 0)
-      ETRY(launch_rbsog_npt_chain(dbox, P, mx, my, mz, sog_gauss, prm.random_seed,
-                                  (uint64_t)(int64_t)epoch, epoch_dev, sog_idx, sog_mult, st));
     const SogVirial sv{P, sog_mult, sog_wv, kterm + 2 * (size_t)Pk, virk};
     ETRY(launch_rbsog_finalize(dbox, Pk, nparts, part_re, part_im, mx, my, mz, sog_w, rho_re,
                                rho_im, tab, kterm, -sog_self * qsq * prm.qqr2e, ek, mean_parts,
@@ -975,8 +992,16 @@ int rbx_engine::capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandl
   ETRY(cuda_ok(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
                "cudaStreamUpdateCaptureDependencies"));
   ETRY(capture_rebuild_body(body));
+  // the k-sampling and the structure factor read only the positions (after
+  // the rebuild's reordering): a branch beside the real-space force, joined
+  // before the finalize, which needs both
+  ETRY(cuda_ok(cudaEventRecord(ev_ks[0], st), "cudaEventRecord"));
+  ETRY(cuda_ok(cudaStreamWaitEvent(st_ks, ev_ks[0], 0), "cudaStreamWaitEvent"));
+  ETRY(kspace_rho(st_ks, dflags + 4));
+  ETRY(cuda_ok(cudaEventRecord(ev_ks[1], st_ks), "cudaEventRecord"));
   ETRY(real_space(dflags + 4));
-  ETRY(kspace_and_combine(true, dflags + 4));
+  ETRY(cuda_ok(cudaStreamWaitEvent(st, ev_ks[1], 0), "cudaStreamWaitEvent"));
+  ETRY(kspace_finish(true, dflags + 4));
   if (shake_nc) ETRY(shake_b(st));
   if (nh_on) ETRY(nh_final(st));
   return RBX_OK;

@@ -178,6 +178,10 @@ struct rbx_engine {
   cudaGraphExec_t hexec[2] = {nullptr, nullptr};
   cudaStream_t st_side = nullptr;
   cudaEvent_t ev_side = nullptr;
+  // inside a step graph the k-sampling and the structure factor run on a
+  // branch of their own (st_ks), beside the real-space force
+  cudaStream_t st_ks = nullptr;
+  cudaEvent_t ev_ks[2] = {nullptr, nullptr};
   unsigned long long host_step_launches = 0;
   int* run_init = nullptr;   // pinned: device epoch / counter seeds of a graph run
   int* run_flags = nullptr;  // pinned: dflags[0..5] after a graph run
@@ -233,6 +237,10 @@ struct rbx_engine {
   int check_rebuild(bool disp_from_drift);
   int real_space(const int* epoch_dev = nullptr);
   int kspace_and_combine(bool kick, const int* epoch_dev = nullptr);
+  // its two parts: the k-sampling and structure-factor partial sums on stream
+  // s, then the finalize and the force scatter (+ combine, kick) on st
+  int kspace_rho(cudaStream_t s, const int* epoch_dev);
+  int kspace_finish(bool kick, const int* epoch_dev);
   int compute_forces(int epoch);
   int check_sampler();
   int step(int nsteps);
