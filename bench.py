@@ -652,6 +652,13 @@ def run_batched(args):
     # one launch per shape and phase)
     ms_batch, design = time_design(rbx.Batch.AUTO)
     ms_branch_default, _ = time_design(rbx.Batch.BRANCHES)
+    ms_phased = ms_batch if design == rbx.Batch.PHASED else None
+    if ms_phased is None:  # AUTO took the branches: time the phased graph too
+        try:
+            ms_phased, _ = time_design(rbx.Batch.PHASED)
+        except rbx.RbxError:
+            ms_phased = None
+    b.set_mode(rbx.Batch.AUTO)
     # autotuner: one timing per size bin, the other replicas of the bin reuse it
     t_tune = time.perf_counter()
     b.autotune()
@@ -703,6 +710,9 @@ def run_batched(args):
         "branch_graph": {"value": total * args.steps / (ms_branch_default / 1e3),
                          "ms_per_step": ms_branch_default / args.steps,
                          "autotuned_value": total * args.steps / (ms_branch / 1e3)},
+        "phased_graph": None if ms_phased is None else {
+            "value": total * args.steps / (ms_phased / 1e3),
+            "ms_per_step": ms_phased / args.steps},
         "autotune": {"phased_autotuned_value": total * args.steps / (ms_tuned / 1e3),
                      "tuning_seconds": t_tune,
                      "note": "value and branch_graph.value use the built-in launch shapes"},

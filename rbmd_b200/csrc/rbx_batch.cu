@@ -248,7 +248,7 @@ struct rbx_batch {
     for (size_t r = 0; r < eng.size() && !rc; ++r) {
       rbx_engine* e = eng[r];
       rc = ok(cudaStreamWaitEvent(e->st, fork, 0), "cudaStreamWaitEvent");  // branch r
-      if (!rc) rc = e->capture_step_into(graph);
+      if (!rc) rc = e->capture_step_into(graph, false);
       if (!rc) rc = ok(cudaEventRecord(join[r], e->st), "cudaEventRecord");
       if (!rc) rc = ok(cudaStreamWaitEvent(st, join[r], 0), "cudaStreamWaitEvent");  // join
     }

@@ -929,14 +929,14 @@ int rbx_engine::capture_step_graph() {
 // Record one MD step on st, which must be capturing into g (its own graph or
 // a batch graph): the conditional handle is created on g, the IF node goes
 // after what st has captured so far, its body is captured on st_body.
-int rbx_engine::capture_step_into(cudaGraph_t g) {
+int rbx_engine::capture_step_into(cudaGraph_t g, bool fork_kspace) {
   const unsigned long long l0 = rbx_launch_count();
   cudaGraphConditionalHandle cond;
   ETRY(cuda_ok(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault),
                "cudaGraphConditionalHandleCreate"));
   bool decided = false;
   ETRY(capture_step_head(&cond, &decided));
-  ETRY(capture_step_tail(g, &cond, decided));
+  ETRY(capture_step_tail(g, &cond, decided, fork_kspace));
   graph_step_launches = rbx_launch_count() - l0 - graph_rebuild_launches;
   return RBX_OK;
 }
@@ -964,7 +964,7 @@ int rbx_engine::capture_step_head(const cudaGraphConditionalHandle* cond, bool* 
 // Rest of a step, captured on st into g: rebuild decision and the rebuild
 // under an IF node, forces, second half kick (+ RATTLE, thermostat).
 int rbx_engine::capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandle* cond_in,
-                                  bool decided) {
+                                  bool decided, bool fork_kspace) {
   cudaGraphConditionalHandle cond;
   if (cond_in) {
     cond = *cond_in;
@@ -992,16 +992,21 @@ int rbx_engine::capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandl
   ETRY(cuda_ok(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
                "cudaStreamUpdateCaptureDependencies"));
   ETRY(capture_rebuild_body(body));
-  // the k-sampling and the structure factor read only the positions (after
-  // the rebuild's reordering): a branch beside the real-space force, joined
-  // before the finalize, which needs both
-  ETRY(cuda_ok(cudaEventRecord(ev_ks[0], st), "cudaEventRecord"));
-  ETRY(cuda_ok(cudaStreamWaitEvent(st_ks, ev_ks[0], 0), "cudaStreamWaitEvent"));
-  ETRY(kspace_rho(st_ks, dflags + 4));
-  ETRY(cuda_ok(cudaEventRecord(ev_ks[1], st_ks), "cudaEventRecord"));
-  ETRY(real_space(dflags + 4));
-  ETRY(cuda_ok(cudaStreamWaitEvent(st, ev_ks[1], 0), "cudaStreamWaitEvent"));
-  ETRY(kspace_finish(true, dflags + 4));
+  if (fork_kspace) {
+    // the k-sampling and the structure factor read only the positions (after
+    // the rebuild's reordering): a branch beside the real-space force, joined
+    // before the finalize, which needs both
+    ETRY(cuda_ok(cudaEventRecord(ev_ks[0], st), "cudaEventRecord"));
+    ETRY(cuda_ok(cudaStreamWaitEvent(st_ks, ev_ks[0], 0), "cudaStreamWaitEvent"));
+    ETRY(kspace_rho(st_ks, dflags + 4));
+    ETRY(cuda_ok(cudaEventRecord(ev_ks[1], st_ks), "cudaEventRecord"));
+    ETRY(real_space(dflags + 4));
+    ETRY(cuda_ok(cudaStreamWaitEvent(st, ev_ks[1], 0), "cudaStreamWaitEvent"));
+    ETRY(kspace_finish(true, dflags + 4));
+  } else {
+    ETRY(real_space(dflags + 4));
+    ETRY(kspace_and_combine(true, dflags + 4));
+  }
   if (shake_nc) ETRY(shake_b(st));
   if (nh_on) ETRY(nh_final(st));
   return RBX_OK;

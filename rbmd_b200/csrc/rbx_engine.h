@@ -215,7 +215,7 @@ struct rbx_engine {
   rbx::ArraySet permute_set(bool to_shadow) const;
   rbx::ArraySet state_set(bool save) const;
   int capture_step_graph();
-  int capture_step_into(cudaGraph_t g);
+  int capture_step_into(cudaGraph_t g, bool fork_kspace = true);
   // kick, drift (+ SHAKE) on st; with cond (same graph as the tail) the drift
   // kernel takes the rebuild decision itself, and *decided says whether it does
   int capture_step_head(const cudaGraphConditionalHandle* cond = nullptr, bool* decided = nullptr);
@@ -225,8 +225,11 @@ struct rbx_engine {
   // (rbx_batch.cu); RBX_ERR_INVALID when a kernel of the step has no batched form
   int record_phased_step(rbx::BatchRecorder* rec, cudaGraphConditionalHandle cond);
   // decide (unless decided), rebuild (IF node on cond, or a new handle), forces, ... on st
+  // fork_kspace: the k-sampling and structure factor on a branch beside the
+  // real-space force (off inside a batch graph of one branch per replica,
+  // where the replicas' branches already run side by side)
   int capture_step_tail(cudaGraph_t g, const cudaGraphConditionalHandle* cond = nullptr,
-                        bool decided = false);
+                        bool decided = false, bool fork_kspace = true);
   int capture_host_graphs();
   void release_host_graphs();
   int graph_run_begin(cudaStream_t s);
