@@ -186,17 +186,13 @@ int rbx_engine::init() {
   for (unsigned long long*& p : snapu) ETRY(alloc(&p, N));
   int** iptrs[] = {&type, &gid, &orig, &tmpi, &perm, &cell_of_sorted, &cand_count};
   for (int** p : iptrs) ETRY(alloc(p, N));
-  // RBL rows are split at r_core + skin (far pairs take the batch hash before
-  // any gather), except in the plain FP64 form when most of the far pairs the
-  // hash selects would lie beyond cut_off at the step (a wide skin): those are
-  // queued before their window test and pay the FP64 pair math for nothing,
-  // so the FP64 form then classifies every candidate in full
-  if (prm.neighbor_type == RBX_NEIGHBOR_RBL) {
-    const double rl = prm.cut_off + prm.skin, rn = prm.r_core + prm.skin, rc = prm.cut_off;
-    const double beyond =
-        rl > rn ? (rl * rl * rl - rc * rc * rc) / (rl * rl * rl - rn * rn * rn) : 0.0;
-    if (prm.precision == RBX_MIXED || beyond <= 0.5) ETRY(alloc(&cand_far, N));
-  }
+  // RBL rows of the mixed form are split at r_core + skin (far pairs take the
+  // batch hash before any gather).  The plain FP64 form keeps one segment:
+  // its split kernel queues the selected far pairs before their window test,
+  // and those beyond cut_off at the step pay the FP64 pair math for nothing,
+  // while the unsplit list builds faster
+  if (prm.neighbor_type == RBX_NEIGHBOR_RBL && prm.precision == RBX_MIXED)
+    ETRY(alloc(&cand_far, N));
   ETRY(alloc(&key_a, N));
   ETRY(alloc(&key_b, N));
   ETRY(alloc(&tmpu, N));
