@@ -227,10 +227,10 @@ k_cell_segsort(int ncell, int n, const int* __restrict__ start, const unsigned* 
 // reference's FP64 predicate, so the list equals the FP64 reference list as a
 // set; rows come out in stencil order, then in cell order.
 //
-// Split rows (RBL engines): a pair whose build distance is certainly at least
-// r_near = r_core + skin cannot come within r_core before the next rebuild (no
-// atom moves more than skin/2 before one), so the fused RBL kernel tests it
-// with its batch hash first.  Such far pairs are written from the end of the
+// Split rows (RBL engines in the mixed form): a pair whose build distance is
+// certainly at least r_near = r_core + skin cannot come within r_core before
+// the next rebuild (no atom moves more than skin/2 before one), so the fused
+// RBL kernel tests it with its batch hash first.  Such far pairs are written from the end of the
 // row backwards; every other candidate from the front.  count[i] is the
 // number of candidates (above cap: overflow), far[i] the number written to
 // the back; the front holds min(count, cap) - far[i] entries, all written.
